@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""Benchmark of the dense density-matrix step on the 512-H2O box (ndim 11776).
+
+One step = one SCF iteration's density step: packed H, S -> filter (1e-5) ->
+Cholesky orthogonalisation -> trace-correcting purification -> packed P.
+
+  value  device-resident packed inputs (libptbgpu ptbgpu_tc_purify_device),
+         seconds per step from the library's CUDA events on its stream;
+  e2e    the C-ABI call with pinned host buffers (ptbgpu_tc_purify), host->device
+         and device->host copies inside the timed region.
+
+Inputs (2 x 555 MB packed, plus ~8 GB of working matrices per step) are far
+larger than the 126 MB L2, so no L2 flush is needed between steps.
+N > 1 runs independent replicas (the dense step does not shard); the per-step
+time reported is the maximum over ranks.
+
+--impl reference times the reference's dense FP64 density step (the check-mode
+solve2: LAPACK dsygvd + Fermi occupations + P = C f C^T, restated in the CPU
+oracle with scipy's multithreaded OpenBLAS) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+METRIC = "P-build s/SCF iter & TFLOP/s: mixed-prec vs FP64 GPU at max|dP|<=1e-6"
+UNIT = "s/SCF-iter"
+FILTER = 1e-5
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained", 1400.0), d.get("hbm_gbs", 6650.0), "measured"
+    return 1590.0, 1400.0, 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, world, local, pg
+
+
+def reduce_max(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], device="cuda", dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def cpu_baseline_sample(sysobj, target_s: float = 20.0):
+    """The oracle's dense FP64 density step (solve2: dsygvd + occupations + C f C^T)
+    on a bounded leading sample of the basis, scaled by n^3 to the full ndim."""
+    from oracle import ptb_oracle as O
+    n_full = sysobj.ndim
+    Hf = O.blowsym(n_full, O.filter_matrix_sym(sysobj.Hvec, FILTER))
+    Sf = O.blowsym(n_full, O.filter_matrix_sym(sysobj.Svec, FILTER))
+    n = 1536
+    t = 0.0
+    while True:
+        t0 = time.perf_counter()
+        Pv, e, focc, fail = O.solve2(1, n, min(sysobj.nel, n), 0, 300.0, O.packsym(Hf[:n, :n]), O.packsym(Sf[:n, :n]))
+        t = time.perf_counter() - t0
+        if t * 8 > target_s or 2 * n > n_full:
+            break
+        n *= 2
+    scale = (n_full / n) ** 3
+    return t * scale, n, t
+
+
+def run_reference(args, rank):
+    from ptb_b200 import synth
+    if rank != 0:
+        return
+    s = synth.water_cluster(512, seed=1)
+    times = []
+    for i in range(args.warmup + args.steps):
+        est, n, t = cpu_baseline_sample(s, target_s=8.0)
+        if i >= args.warmup:
+            times.append(est)
+    v = statistics.median(times)
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "dense density step, 512-H2O box (1536 atoms, ndim 11776, nel 4096), filter 1e-5",
+                   "global_batch": 1, "seq_len": 11776, "parallelism": "replicas"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"oracle solve2 (dsygvd + Fermi + C f C^T, OpenBLAS {cores} threads) on the "
+                                   f"leading {n} basis functions, {t:.2f} s, scaled by (11776/{n})^3"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local, pg):
+    import torch
+
+    from ptb_b200 import PREC_FP64, PREC_MIXED, Context, Options, synth
+
+    peak_burst, peak_sust, hbm, peak_kind = load_peaks()
+    s = synth.water_cluster(512, seed=1)
+    n, nel = s.ndim, s.nel
+    npk = n * (n + 1) // 2
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    dH = torch.from_numpy(s.Hvec).to(dev)
+    dS = torch.from_numpy(s.Svec).to(dev)
+    dP = torch.empty(npk, dtype=torch.float64, device=dev)
+    hH = torch.from_numpy(s.Hvec).pin_memory()
+    hS = torch.from_numpy(s.Svec).pin_memory()
+    hP = torch.empty(npk, dtype=torch.float64).pin_memory()
+    hHn, hSn, hPn = hH.numpy(), hS.numpy(), hP.numpy()
+    prec = PREC_FP64 if args.precision == "fp64" else PREC_MIXED
+    opts = Options(filter=FILTER, precision=prec)
+    ctx = Context(local)
+    torch.cuda.synchronize()
+
+    def dev_step(o=opts):
+        return ctx.tc_purify_device(n, nel, dH.data_ptr(), dS.data_ptr(), dP.data_ptr(), o)
+
+    for _ in range(args.warmup):
+        dev_step()
+    torch.cuda.synchronize()
+    barrier(pg)
+    stats = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier(pg)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            stats.append(dev_step())
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        barrier(pg)
+        # end-to-end through the host C-ABI (pinned host buffers)
+        e2e = []
+        for _ in range(max(1, min(args.steps, 3))):
+            P_host, st = ctx.tc_purify(n, nel, hHn, hSn, opts)
+            e2e.append(st)
+        torch.cuda.synchronize()
+    clocks = clk.summary()
+    ms_dev = sum(st.ms_total for st in stats) / len(stats)
+    ms_dev = reduce_max(pg, ms_dev)
+    ms_e2e = reduce_max(pg, sum(st.ms_total for st in e2e) / len(e2e))
+
+    # accuracy against the plain FP64 GPU path, and its time (the 10x comparator)
+    fp64 = {}
+    if args.compare_fp64 and rank == 0:
+        Pmix = dP.cpu().numpy().copy()
+        st64 = ctx.tc_purify_device(n, nel, dH.data_ptr(), dS.data_ptr(), dP.data_ptr(),
+                                    Options(filter=FILTER, precision=PREC_FP64))
+        P64 = dP.cpu().numpy()
+        fp64 = {"s_per_step": st64.ms_total / 1e3, "iterations": st64.iterations,
+                "max_abs_dP_mixed_vs_fp64": float(np.max(np.abs(Pmix - P64)))}
+        chk = ctx.check_density(n, Pmix, ctx.filter_matrix_sym(s.Svec, n, FILTER),
+                                ctx.filter_matrix_sym(s.Hvec, n, FILTER))
+        chk64 = ctx.check_density(n, P64, ctx.filter_matrix_sym(s.Svec, n, FILTER),
+                                  ctx.filter_matrix_sym(s.Hvec, n, FILTER))
+        fp64.update({"nel_mixed": chk.nel, "band_energy_mixed": chk.band_energy,
+                     "band_energy_fp64": chk64.band_energy,
+                     "dE_band_mixed_vs_fp64": chk.band_energy - chk64.band_energy,
+                     "idempotency_frob_mixed": chk.idempotency_frob,
+                     "speedup_mixed_vs_fp64": (st64.ms_total / 1e3) / (ms_dev / 1e3)})
+
+    last = stats[-1]
+    # roofline of the dominant kernel: the tcgen05 product (both epilogues)
+    tc_ms = (sum(x.ms_tc_sp2 + x.ms_tc_full for x in stats)) / len(stats)
+    tc_n = (sum(x.n_tc_sp2 + x.n_tc_full for x in stats)) / len(stats)
+    # algorithmic flops: SP2 step = symmetric square, n^2 (n+1) ~ n^3; general product 2 n^3
+    alg = last.n_tc_sp2 * float(n) ** 3 + last.n_tc_full * 2.0 * float(n) ** 3
+    ldp = ((n + 255) // 256) * 256
+    nt_up = sum(1 for bi in range(ldp // 128) for bj in range(ldp // 256) if bj * 256 + 255 >= bi * 128)
+    executed = 3 * 2.0 * 128 * 256 * ldp * (last.n_tc_sp2 * nt_up + last.n_tc_full * (ldp // 128) * (ldp // 256))
+    achieved = alg / (last.ms_tc_sp2 + last.ms_tc_full) / 1e9 if (last.ms_tc_sp2 + last.ms_tc_full) > 0 else 0.0
+    exec_tf = executed / (last.ms_tc_sp2 + last.ms_tc_full) / 1e9 if (last.ms_tc_sp2 + last.ms_tc_full) > 0 else 0.0
+    traffic = None
+    tp = ROOT / "profiles" / "traffic.json"
+    if tp.exists():
+        traffic = json.loads(tp.read_text()).get("tc_product_bytes_per_launch")
+
+    if rank != 0:
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        est, ns, t = cpu_baseline_sample(s)
+        cpu = {"value": est, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"oracle solve2 (dsygvd + Fermi + C f C^T, OpenBLAS) on the leading {ns} basis "
+                         f"functions: {t:.2f} s, scaled by (11776/{ns})^3"}
+    line = {
+        "metric": METRIC, "value": ms_dev / 1e3, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_dev, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16x3+f64" if prec == PREC_MIXED else "f64", "data": "synthetic",
+        "config": {"workload": "dense density step, 512-H2O box (1536 atoms, ndim 11776, nel 4096), filter 1e-5, "
+                               "trace-correcting purification",
+                   "global_batch": world, "seq_len": n, "parallelism": f"replicas x{world}",
+                   "l2": "inputs and working set far larger than L2 (no flush)"},
+        "tflops_algorithmic": last.flops / (last.ms_solve / 1e3) / 1e12 if last.ms_solve > 0 else None,
+        "iterations": last.iterations,
+        "e2e": {"value": ms_e2e / 1e3, "unit": UNIT, "h2d_bytes_per_step": 2 * npk * 8, "d2h_bytes_per_step": npk * 8},
+        "gpu_launches": int(sum(x.kernel_launches for x in stats)),
+        "roofline": {"bound": "tensor", "kernel": "k_tc_product (tcgen05 bf16x3)",
+                     "achieved": achieved, "peak": peak_sust, "unit": "TFLOP/s",
+                     "frac": achieved / peak_sust if peak_sust else None, "traffic": traffic,
+                     "peak_kind": f"{peak_kind} bf16 sustained",
+                     "executed_tflops": exec_tf, "executed_frac": exec_tf / peak_sust if peak_sust else None,
+                     "launches_per_step": tc_n, "ms_per_step_in_kernel": tc_ms},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "wall_s_timed": wall,
+    }
+    if fp64:
+        line["fp64_gpu"] = fp64
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--no-compare-fp64", dest="compare_fp64", action="store_false")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, rank)
+        return
+    rank, world, local, pg = dist_setup(args.gpus)
+    try:
+        run_ours(args, rank, world, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

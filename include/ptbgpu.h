@@ -1,0 +1,178 @@
+/*
+ * ptbgpu.h -- C-ABI of the B200 density-matrix step for PTB.
+ *
+ * Drop-in boundary for the Fortran SCF driver (twoscf, source/pgtb.f90:345-670):
+ * every entry point takes host pointers in the reference's packed layout
+ * (FP64, 1-based ij = i(i-1)/2 + j for j <= i: column i, rows <= i;
+ * source/solve.f:149-200) and default Fortran integers as int64_t (the
+ * reference builds with -i8, source/Makefile:35-37).  The library copies in
+ * and out; it keeps no caller pointer after a call returns.
+ *
+ * Every function returns 0 on success or one of the PTBGPU_E* codes below;
+ * ptbgpu_last_error() returns the message of the last failure on a context.
+ * A context is not re-entrant: one host thread drives it at a time.
+ */
+#ifndef PTBGPU_H
+#define PTBGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PTBGPU_OK               0
+#define PTBGPU_EINVAL           1   /* bad argument (size, mode, null pointer)          */
+#define PTBGPU_ECUDA            2   /* CUDA runtime / cuBLAS / cuSOLVER failure           */
+#define PTBGPU_ENOTSPD          3   /* overlap (sub)matrix not positive definite          */
+#define PTBGPU_ENAN             4   /* NaN during an iteration ("error stop" in the ref.) */
+#define PTBGPU_EITER            5   /* iteration cap reached without convergence          */
+#define PTBGPU_ENOTIMPL         6   /* mode the reference stops on ("not implemented")     */
+#define PTBGPU_ETIMEOUT         7   /* a bounded device-side wait gave up                 */
+#define PTBGPU_ENOMEM           8   /* device allocation failed                           */
+
+/* ---- mode codes (source/purification_settings.f90:6-27) ---------------- */
+#define PTBGPU_MODE_FULL                 1
+#define PTBGPU_MODE_SUBMATRIX            2
+#define PTBGPU_COLUMNS_SINGLE            1
+#define PTBGPU_COLUMNS_ATOMS             2
+#define PTBGPU_COLUMNS_FULL_MATRIX       3
+#define PTBGPU_COLUMNS_KMEANS            4
+#define PTBGPU_SUBMATRIX_SIGN            1
+#define PTBGPU_SUBMATRIX_SYGV            2
+#define PTBGPU_TYPE_MCWEENY              1
+#define PTBGPU_TYPE_PADE                 2
+#define PTBGPU_TYPE_NEWTON               3
+#define PTBGPU_TYPE_DIAG                 4
+#define PTBGPU_METRIC_INV                1
+#define PTBGPU_METRIC_INV_SQRT           2
+#define PTBGPU_METRIC_SQRT               3
+
+/* ---- precision of the trace-correcting purification -------------------- */
+#define PTBGPU_PREC_FP64                 0  /* every product in FP64 (comparator path)      */
+#define PTBGPU_PREC_MIXED                1  /* bf16x3 tensor-core iterations + FP64 refinement */
+
+typedef struct ptbgpu_ctx ptbgpu_ctx;
+
+/* POD mirror of tPurificationSet (source/purification_settings.f90:29-86). */
+typedef struct {
+    int64_t mode;               /* 1 full, 2 submatrix                    */
+    int64_t type;               /* 1 mcweeny, 2 pade, 3 newton, 4 diag    */
+    int64_t cycles;             /* purification cycles (default 40)       */
+    int64_t prlvl;              /* print level (default 1)                */
+    int64_t nel;                /* electrons (set by the caller)          */
+    int64_t submatrix_mode;     /* 1 sign, 2 sygv                         */
+    int64_t submatrix_columns;  /* 1..4                                   */
+    int64_t metric_type;        /* 1 inv, 2 inv_sqrt, 3 sqrt              */
+    int64_t metric_cycles;      /* default 50                             */
+    int64_t metric_iterative;   /* logical                                */
+    int64_t chempot_cycles;     /* default 60                             */
+    double  chempot_guess;      /* default -1.5                           */
+    double  chempot_increment;  /* default 0.1                            */
+} ptbgpu_pur_settings;
+
+/* Options that have no counterpart in the reference's argument lists. */
+typedef struct {
+    double  filter;             /* >0: zero |A_ij| < filter in H and S first (source/pgtb.f90:567-585) */
+    int64_t precision;          /* PTBGPU_PREC_*                                  */
+    int64_t print_level;        /* 0 silent, 1 the reference's progress lines     */
+    int64_t max_iter;           /* cap on trace-correcting iterations (0 = 100)   */
+    double  electronic_temp;    /* solve2 Fermi temperature in K (0 = 300)        */
+    double  glob_par15;         /* solve2 orbital-energy shift for mode >= 2      */
+    double  glob_par17;
+} ptbgpu_opts;
+
+/* What a call reports back (all optional for the caller). */
+typedef struct {
+    double  mu;                 /* chemical potential (Eh) / last bisection midpoint  */
+    double  nel;                /* electron count of the result, tr(PS)              */
+    double  band_energy;        /* tr(PH) with the filtered H                        */
+    double  idempotency_ref;    /* |sum(1/2 PSP - P)| as source/metrics.f90:356      */
+    double  idempotency_frob;   /* ||1/2 PSP - P||_F                                 */
+    int64_t nsm;                /* number of submatrices                             */
+    int64_t sum_dims;           /* sum of submatrix dimensions                       */
+    int64_t max_dim;            /* largest submatrix dimension                       */
+    int64_t iterations;         /* purification iterations (all passes)              */
+    int64_t mu_iterations;      /* chemical-potential steps                          */
+    int64_t info;               /* first nonzero LAPACK-style info, 0 otherwise      */
+    double  ms_total;           /* device time of the call (CUDA events)             */
+    double  ms_h2d;
+    double  ms_solve;
+    double  ms_d2h;
+    double  flops;              /* algorithmic FLOPs of the call                     */
+    double  ms_tc_sp2;          /* summed device time of the SP2 tensor-core products */
+    int64_t n_tc_sp2;           /* their launches                                     */
+    double  ms_tc_full;         /* summed device time of the general tensor-core products */
+    int64_t n_tc_full;
+    int64_t kernel_launches;    /* launches of this library's own kernels in the call */
+} ptbgpu_stats;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+/* Replaces nothing in the reference (its accel_lib context, source/cuda_context.f90:1-24,
+ * is an unbuilt stub).  One context per device and host thread. */
+int  ptbgpu_init(int device, ptbgpu_ctx** ctx);
+int  ptbgpu_finalize(ptbgpu_ctx* ctx);
+int  ptbgpu_last_error(const ptbgpu_ctx* ctx, char* buf, size_t len);
+void ptbgpu_default_settings(ptbgpu_pur_settings* s);   /* type-bound defaults, purification_settings.f90:29-86 */
+void ptbgpu_default_opts(ptbgpu_opts* o);
+
+/* ---- matrix utilities --------------------------------------------------- */
+/* filter_matrix_sym(A, n, filter), source/pgtb.f90:1532-1547: in place on a
+ * host packed array, |A_ij| < filter -> 0. */
+int ptbgpu_filter_packed(ptbgpu_ctx* ctx, int64_t n, double* Apk, double filter);
+
+/* check_density / get_nel / band_structure / idempotent
+ * (source/metrics.f90:144-179, 202-230, 253-277, 316-360) on packed host data;
+ * Hpk may be NULL.  Fills st->nel, band_energy, idempotency_*. */
+int ptbgpu_check_density(ptbgpu_ctx* ctx, int64_t ndim, const double* Ppk, const double* Spk,
+                         const double* Hpk, ptbgpu_stats* st);
+
+/* ---- the density-matrix step -------------------------------------------- */
+/* sm_stupid_simple(ndim,nelref,Hvec,Svec,Pvec,n,xyz,aoat,submatrix_columns,submatrix_mode),
+ * source/sm.f90:34-409.  partition (nat entries, 1-based cluster per atom) is
+ * required for columns mode 4 in place of the reference's k-means; NULL otherwise.
+ * Filtering (opts->filter) is applied to copies of H and S first. */
+int ptbgpu_sm_density(ptbgpu_ctx* ctx, int64_t ndim, int64_t nelref,
+                      const double* Hpk, const double* Spk, double* Ppk,
+                      int64_t nat, const double* xyz, const int64_t* aoat,
+                      int64_t submatrix_columns, int64_t submatrix_mode,
+                      const int64_t* partition, const ptbgpu_opts* opts, ptbgpu_stats* st);
+
+/* purification(pur, ndim, H, S, P) -> purification_wrapper, source/purification.f90:28-80:
+ * metric, chemical-potential search and the selected purification type in FP64. */
+int ptbgpu_purify(ptbgpu_ctx* ctx, const ptbgpu_pur_settings* pur, int64_t ndim,
+                  const double* Hpk, const double* Spk, double* Ppk,
+                  const ptbgpu_opts* opts, ptbgpu_stats* st);
+
+/* Trace-correcting (SP2) purification, the B200 fast path for the dense
+ * density step; replaces the mu search of purification_search
+ * (source/purification.f90:232-353) with trace correction.  nel must be even.
+ * opts->precision selects FP64 or bf16x3 + FP64 refinement. */
+int ptbgpu_tc_purify(ptbgpu_ctx* ctx, int64_t ndim, int64_t nel,
+                     const double* Hpk, const double* Spk, double* Ppk,
+                     const ptbgpu_opts* opts, ptbgpu_stats* st);
+
+/* Same with device-resident packed arrays (no host copies); stream is a
+ * cudaStream_t or NULL for the context's own stream. */
+int ptbgpu_tc_purify_device(ptbgpu_ctx* ctx, int64_t ndim, int64_t nel,
+                            const double* dHpk, const double* dSpk, double* dPpk,
+                            const ptbgpu_opts* opts, ptbgpu_stats* st);
+
+/* solve2(mode,ndim,nel,nopen,homo,et,focc,H,S,P,e,U,fail), source/pgtb.f90:1066-1170:
+ * dense generalized eigensolve + Fermi smearing, the check-mode oracle.
+ * e (ndim) and focc (ndim) may be NULL. */
+int ptbgpu_solve2(ptbgpu_ctx* ctx, int64_t mode, int64_t ndim, int64_t nel, int64_t nopen,
+                  const double* Hpk, const double* Spk, double* Ppk, double* e, double* focc,
+                  const ptbgpu_opts* opts, ptbgpu_stats* st);
+
+/* ---- kernel-level entry points (parity tests and benchmarks) ------------ */
+/* C = X * X for a symmetric n x n FP64 matrix X (row-major), computed with the
+ * bf16x3 tcgen05 kernel (hi/lo split, FP32 accumulation); C is FP32 row-major. */
+int ptbgpu_symsq_bf16x3(ptbgpu_ctx* ctx, int64_t n, const double* X, float* C);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PTBGPU_H */

@@ -1,0 +1,303 @@
+"""Host-side mirror of the reference's density-step interface over the C-ABI.
+
+The functions keep the reference's names and argument meaning:
+
+* ``sm_stupid_simple``  -> source/sm.f90:34 (submatrix method)
+* ``purification``      -> source/purification.f90:28 (purification_wrapper)
+* ``solve2``            -> source/pgtb.f90:1066 (dense FP64 diagonalisation)
+* ``filter_matrix_sym`` -> source/pgtb.f90:1532
+* ``check_density`` / ``get_nel`` / ``band_structure`` / ``idempotent``
+                        -> source/metrics.f90:144-360
+plus ``tc_purify`` (trace-correcting purification, the B200 fast path of the
+dense step).  Arrays are numpy float64 in the reference's packed layout;
+default Fortran integers are int64.  Every call goes through libptbgpu.so;
+there is no CPU fallback: a missing library or device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from .settings import PurificationSettings
+
+_LIB = None
+_PKG = Path(__file__).resolve().parent
+
+# status codes (include/ptbgpu.h)
+OK, EINVAL, ECUDA, ENOTSPD, ENAN, EITER, ENOTIMPL, ETIMEOUT, ENOMEM = range(9)
+PREC_FP64, PREC_MIXED, PREC_MIXED_NOREFINE = 0, 1, 2
+
+
+class PtbGpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class _Settings(C.Structure):
+    _fields_ = [("mode", C.c_int64), ("type", C.c_int64), ("cycles", C.c_int64), ("prlvl", C.c_int64),
+                ("nel", C.c_int64), ("submatrix_mode", C.c_int64), ("submatrix_columns", C.c_int64),
+                ("metric_type", C.c_int64), ("metric_cycles", C.c_int64), ("metric_iterative", C.c_int64),
+                ("chempot_cycles", C.c_int64), ("chempot_guess", C.c_double), ("chempot_increment", C.c_double)]
+
+
+class _Opts(C.Structure):
+    _fields_ = [("filter", C.c_double), ("precision", C.c_int64), ("print_level", C.c_int64),
+                ("max_iter", C.c_int64), ("electronic_temp", C.c_double), ("glob_par15", C.c_double),
+                ("glob_par17", C.c_double)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [("mu", C.c_double), ("nel", C.c_double), ("band_energy", C.c_double),
+                ("idempotency_ref", C.c_double), ("idempotency_frob", C.c_double), ("nsm", C.c_int64),
+                ("sum_dims", C.c_int64), ("max_dim", C.c_int64), ("iterations", C.c_int64),
+                ("mu_iterations", C.c_int64), ("info", C.c_int64), ("ms_total", C.c_double),
+                ("ms_h2d", C.c_double), ("ms_solve", C.c_double), ("ms_d2h", C.c_double), ("flops", C.c_double),
+                ("ms_tc_sp2", C.c_double), ("n_tc_sp2", C.c_int64), ("ms_tc_full", C.c_double),
+                ("n_tc_full", C.c_int64), ("kernel_launches", C.c_int64)]
+
+
+EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_default_settings",
+            "ptbgpu_default_opts", "ptbgpu_filter_packed", "ptbgpu_check_density", "ptbgpu_sm_density",
+            "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_solve2",
+            "ptbgpu_symsq_bf16x3")
+
+
+def library_path() -> Path:
+    return Path(os.environ.get("PTBGPU_LIB", _PKG / "libptbgpu.so"))
+
+
+def load_library():
+    """Loads libptbgpu.so (built by ptb_b200.build); raises if it is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not path.exists():
+        raise PtbGpuError(ECUDA, f"{path} not found: build it with `python -m ptb_b200.build`")
+    lib = C.CDLL(str(path))
+    P = C.POINTER
+    d = P(C.c_double)
+    i64 = C.c_int64
+    lib.ptbgpu_init.argtypes = [C.c_int, P(C.c_void_p)]
+    lib.ptbgpu_finalize.argtypes = [C.c_void_p]
+    lib.ptbgpu_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+    lib.ptbgpu_default_settings.argtypes = [P(_Settings)]
+    lib.ptbgpu_default_settings.restype = None
+    lib.ptbgpu_default_opts.argtypes = [P(_Opts)]
+    lib.ptbgpu_default_opts.restype = None
+    lib.ptbgpu_filter_packed.argtypes = [C.c_void_p, i64, d, C.c_double]
+    lib.ptbgpu_check_density.argtypes = [C.c_void_p, i64, d, d, d, P(_Stats)]
+    lib.ptbgpu_sm_density.argtypes = [C.c_void_p, i64, i64, d, d, d, i64, d, P(i64), i64, i64, P(i64),
+                                      P(_Opts), P(_Stats)]
+    lib.ptbgpu_purify.argtypes = [C.c_void_p, P(_Settings), i64, d, d, d, P(_Opts), P(_Stats)]
+    lib.ptbgpu_tc_purify.argtypes = [C.c_void_p, i64, i64, d, d, d, P(_Opts), P(_Stats)]
+    lib.ptbgpu_tc_purify_device.argtypes = [C.c_void_p, i64, i64, C.c_void_p, C.c_void_p, C.c_void_p, P(_Opts),
+                                            P(_Stats)]
+    lib.ptbgpu_solve2.argtypes = [C.c_void_p, i64, i64, i64, i64, d, d, d, d, d, P(_Opts), P(_Stats)]
+    lib.ptbgpu_symsq_bf16x3.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
+    for name in EXPORTED:
+        f = getattr(lib, name)
+        if f.restype is not None and name not in ("ptbgpu_default_settings", "ptbgpu_default_opts"):
+            f.restype = C.c_int
+    _LIB = lib
+    return lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def npacked(n: int) -> int:
+    return n * (n + 1) // 2
+
+
+@dataclass
+class Stats:
+    mu: float = 0.0
+    nel: float = 0.0
+    band_energy: float = 0.0
+    idempotency_ref: float = 0.0
+    idempotency_frob: float = 0.0
+    nsm: int = 0
+    sum_dims: int = 0
+    max_dim: int = 0
+    iterations: int = 0
+    mu_iterations: int = 0
+    info: int = 0
+    ms_total: float = 0.0
+    ms_h2d: float = 0.0
+    ms_solve: float = 0.0
+    ms_d2h: float = 0.0
+    flops: float = 0.0
+    ms_tc_sp2: float = 0.0
+    n_tc_sp2: int = 0
+    ms_tc_full: float = 0.0
+    n_tc_full: int = 0
+    kernel_launches: int = 0
+
+    @classmethod
+    def from_c(cls, s: _Stats) -> "Stats":
+        return cls(**{k: getattr(s, k) for k, _ in _Stats._fields_})
+
+
+@dataclass
+class Options:
+    """Options without a counterpart in the reference's argument lists."""
+    filter: float = 0.0
+    precision: int = PREC_MIXED
+    print_level: int = 0
+    max_iter: int = 100
+    electronic_temp: float = 300.0
+    glob_par15: float = 0.0
+    glob_par17: float = 0.0
+
+    def to_c(self) -> _Opts:
+        return _Opts(self.filter, self.precision, self.print_level, self.max_iter, self.electronic_temp,
+                     self.glob_par15, self.glob_par17)
+
+
+class Context:
+    """One library context (device buffers, stream, cuBLAS/cuSOLVER handles)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load_library()
+        h = C.c_void_p()
+        rc = self._lib.ptbgpu_init(int(device), C.byref(h))
+        if rc != OK:
+            raise PtbGpuError(rc, f"ptbgpu_init(device={device}) failed")
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ptbgpu_finalize(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != OK:
+            buf = C.create_string_buffer(1024)
+            self._lib.ptbgpu_last_error(self._h, buf, 1024)
+            raise PtbGpuError(rc, buf.value.decode(errors="replace"))
+
+    # ---- reference entry points ------------------------------------------
+    def filter_matrix_sym(self, A: np.ndarray, n: int, filter: float) -> np.ndarray:
+        """source/pgtb.f90:1532-1547, returns the filtered packed copy."""
+        out = _f64(A).copy()
+        self._check(self._lib.ptbgpu_filter_packed(self._h, int(n), _dptr(out), float(filter)))
+        return out
+
+    def check_density(self, ndim: int, P: np.ndarray, S: np.ndarray, H: np.ndarray | None = None) -> Stats:
+        """get_nel, band_structure and idempotent (source/metrics.f90:144-360) on packed data."""
+        st = _Stats()
+        P, S = _f64(P), _f64(S)
+        Hp = _dptr(_f64(H)) if H is not None else None
+        self._check(self._lib.ptbgpu_check_density(self._h, int(ndim), _dptr(P), _dptr(S), Hp, C.byref(st)))
+        return Stats.from_c(st)
+
+    def sm_stupid_simple(self, ndim: int, nelref: int, Hvec: np.ndarray, Svec: np.ndarray, n: int,
+                         xyz: np.ndarray, aoat: np.ndarray, submatrix_columns: int, submatrix_mode: int,
+                         partition: np.ndarray | None = None, opts: Options | None = None):
+        """Submatrix density step, source/sm.f90:34-409.  Returns (Pvec, Stats)."""
+        H, S = _f64(Hvec), _f64(Svec)
+        P = np.zeros(npacked(ndim))
+        xyz_a = _f64(xyz)
+        ao = _i64(aoat)
+        part = _i64(partition) if partition is not None else None
+        st = _Stats()
+        o = (opts or Options()).to_c()
+        self._check(self._lib.ptbgpu_sm_density(
+            self._h, int(ndim), int(nelref), _dptr(H), _dptr(S), _dptr(P), int(n), _dptr(xyz_a),
+            ao.ctypes.data_as(C.POINTER(C.c_int64)), int(submatrix_columns), int(submatrix_mode),
+            part.ctypes.data_as(C.POINTER(C.c_int64)) if part is not None else None, C.byref(o), C.byref(st)))
+        return P, Stats.from_c(st)
+
+    def purification(self, pur: PurificationSettings, ndim: int, H: np.ndarray, S: np.ndarray,
+                     opts: Options | None = None):
+        """purification_wrapper, source/purification.f90:28-80.  Returns (Pvec, Stats)."""
+        Hh, Sh = _f64(H), _f64(S)
+        P = np.zeros(npacked(ndim))
+        st = _Stats()
+        cs = pur.to_c(_Settings)
+        o = (opts or Options()).to_c()
+        self._check(self._lib.ptbgpu_purify(self._h, C.byref(cs), int(ndim), _dptr(Hh), _dptr(Sh), _dptr(P),
+                                            C.byref(o), C.byref(st)))
+        return P, Stats.from_c(st)
+
+    def tc_purify(self, ndim: int, nel: int, H: np.ndarray, S: np.ndarray, opts: Options | None = None):
+        """Trace-correcting purification (FP64 or bf16x3 + FP64 refinement).  Returns (Pvec, Stats)."""
+        Hh, Sh = _f64(H), _f64(S)
+        P = np.zeros(npacked(ndim))
+        st = _Stats()
+        o = (opts or Options()).to_c()
+        self._check(self._lib.ptbgpu_tc_purify(self._h, int(ndim), int(nel), _dptr(Hh), _dptr(Sh), _dptr(P),
+                                               C.byref(o), C.byref(st)))
+        return P, Stats.from_c(st)
+
+    def tc_purify_device(self, ndim: int, nel: int, dH: int, dS: int, dP: int, opts: Options | None = None):
+        """Same on device-resident packed arrays (raw device pointers)."""
+        st = _Stats()
+        o = (opts or Options()).to_c()
+        self._check(self._lib.ptbgpu_tc_purify_device(self._h, int(ndim), int(nel), C.c_void_p(dH),
+                                                      C.c_void_p(dS), C.c_void_p(dP), C.byref(o), C.byref(st)))
+        return Stats.from_c(st)
+
+    def solve2(self, mode: int, ndim: int, nel: int, nopen: int, H: np.ndarray, S: np.ndarray,
+               opts: Options | None = None):
+        """Dense FP64 diagonalisation + Fermi smearing, source/pgtb.f90:1066-1170.
+
+        Returns (Pvec, e, focc, Stats)."""
+        Hh, Sh = _f64(H), _f64(S)
+        P = np.zeros(npacked(ndim))
+        e = np.zeros(ndim)
+        focc = np.zeros(ndim)
+        st = _Stats()
+        o = (opts or Options()).to_c()
+        self._check(self._lib.ptbgpu_solve2(self._h, int(mode), int(ndim), int(nel), int(nopen), _dptr(Hh),
+                                            _dptr(Sh), _dptr(P), _dptr(e), _dptr(focc), C.byref(o), C.byref(st)))
+        return P, e, focc, Stats.from_c(st)
+
+    # ---- kernel level ------------------------------------------------------
+    def symsq_bf16x3(self, X: np.ndarray) -> np.ndarray:
+        """C = X X (symmetric X) on the tcgen05 kernel with bf16x3 operands; FP32 result."""
+        Xh = _f64(X)
+        n = Xh.shape[0]
+        out = np.zeros((n, n), dtype=np.float32)
+        self._check(self._lib.ptbgpu_symsq_bf16x3(self._h, int(n), _dptr(Xh),
+                                                  out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+
+# module-level conveniences with the reference's names -----------------------
+def get_nel(ctx: Context, ndim: int, P: np.ndarray, S: np.ndarray) -> float:
+    """tr(PS) of packed P, S (source/metrics.f90:202-230)."""
+    return ctx.check_density(ndim, P, S).nel
+
+
+def band_structure(ctx: Context, ndim: int, P: np.ndarray, H: np.ndarray, S: np.ndarray) -> float:
+    """tr(PH) of packed P, H (source/metrics.f90:253-277)."""
+    return ctx.check_density(ndim, P, S, H).band_energy

@@ -1,0 +1,224 @@
+// extern "C" entry points: argument checks, host <-> device copies of the
+// packed arrays, CUDA-event timing, and translation of internal errors into
+// status codes plus a message readable through ptbgpu_last_error().
+#include <cstring>
+
+#include "common.cuh"
+
+namespace ptb {
+void tc_purify_entry(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, const double* dS, double* dP,
+                     const ptbgpu_opts* o, ptbgpu_stats* st);
+void symsq_entry(ptbgpu_ctx* c, int64_t n, const double* hX, float* hC);
+void purify_ref_device(ptbgpu_ctx* c, const ptbgpu_pur_settings& pur, int64_t n, const double* dH,
+                       const double* dS, double* dP, const ptbgpu_opts* o, ptbgpu_stats* st);
+void solve2_device(ptbgpu_ctx* c, int64_t mode, int64_t n, int64_t nel, int64_t nopen, const double* dH,
+                   const double* dS, double* dP, double* he, double* hfocc, const ptbgpu_opts* o, ptbgpu_stats* st);
+void check_density_device(ptbgpu_ctx* c, int64_t n, const double* dP, const double* dS, const double* dH,
+                          ptbgpu_stats* st);
+void sm_density_device(ptbgpu_ctx* c, int64_t ndim, int64_t nelref, const double* dH, const double* dS, double* dP,
+                       int64_t nat, const double* xyz, const int64_t* aoat, int64_t columns, int64_t mode,
+                       const int64_t* partition, const ptbgpu_opts* o, ptbgpu_stats* st);
+}  // namespace ptb
+
+namespace {
+
+using namespace ptb;
+
+template <class F>
+int guarded(ptbgpu_ctx* c, F&& f) {
+    if (!c) return PTBGPU_EINVAL;
+    try {
+        PTB_CUDA(cudaSetDevice(c->device));
+        launch_counter() = 0;
+        c->evused = 0;
+        c->timed.clear();
+        f();
+        c->last_error.clear();
+        return PTBGPU_OK;
+    } catch (const Error& e) {
+        c->last_error = e.msg;
+        (void)cudaGetLastError();
+        if (c->stream) cudaStreamSynchronize(c->stream);
+        return e.code;
+    } catch (const std::exception& e) {
+        c->last_error = e.what();
+        return PTBGPU_ECUDA;
+    }
+}
+
+// Device copies of up to three packed inputs and one packed output.
+struct PackedIO {
+    ptbgpu_ctx* c;
+    int64_t n;
+    double* d[3] = {nullptr, nullptr, nullptr};
+    PackedIO(ptbgpu_ctx* cc, int64_t nn) : c(cc), n(nn) {
+        for (int k = 0; k < 3; ++k) {
+            DevBuf& b = c->buf(B_PK0 + k);
+            b.reserve(sizeof(double) * (size_t)npacked(n));
+            d[k] = b.as<double>();
+        }
+    }
+    void in(int k, const double* h) {
+        PTB_CUDA(cudaMemcpyAsync(d[k], h, sizeof(double) * (size_t)npacked(n), cudaMemcpyHostToDevice, c->stream));
+    }
+    void out(int k, double* h) {
+        PTB_CUDA(cudaMemcpyAsync(h, d[k], sizeof(double) * (size_t)npacked(n), cudaMemcpyDeviceToHost, c->stream));
+    }
+};
+
+// Records ms_h2d / ms_solve / ms_d2h / ms_total with CUDA events on the context stream.
+struct PhaseTimer {
+    ptbgpu_ctx* c;
+    explicit PhaseTimer(ptbgpu_ctx* cc) : c(cc) { PTB_CUDA(cudaEventRecord(c->ev[0], c->stream)); }
+    void mark(int k) { PTB_CUDA(cudaEventRecord(c->ev[k], c->stream)); }
+    void finish(ptbgpu_stats* st) {
+        PTB_CUDA(cudaEventRecord(c->ev[3], c->stream));
+        PTB_CUDA(cudaEventSynchronize(c->ev[3]));
+        if (!st) return;
+        float a = 0, b = 0, d = 0;
+        PTB_CUDA(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
+        PTB_CUDA(cudaEventElapsedTime(&b, c->ev[1], c->ev[2]));
+        PTB_CUDA(cudaEventElapsedTime(&d, c->ev[2], c->ev[3]));
+        st->ms_h2d = a;
+        st->ms_solve = b;
+        st->ms_d2h = d;
+        st->ms_total = a + b + d;
+        for (const auto& t : c->timed) {
+            float ms = 0.f;
+            PTB_CUDA(cudaEventElapsedTime(&ms, t.a, t.b));
+            if (t.kind == 0) {
+                st->ms_tc_sp2 += ms;
+                st->n_tc_sp2 += 1;
+            } else {
+                st->ms_tc_full += ms;
+                st->n_tc_full += 1;
+            }
+        }
+        st->kernel_launches = launch_counter();
+    }
+};
+
+void clear_stats(ptbgpu_stats* st) {
+    if (st) memset(st, 0, sizeof(*st));
+}
+
+}  // namespace
+
+extern "C" {
+
+int ptbgpu_filter_packed(ptbgpu_ctx* c, int64_t n, double* Apk, double filter) {
+    return guarded(c, [&] {
+        PTB_CHECK(n > 0 && Apk, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, n);
+        io.in(0, Apk);
+        filter_packed(c->stream, n, io.d[0], filter);
+        io.out(0, Apk);
+        PTB_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int ptbgpu_check_density(ptbgpu_ctx* c, int64_t ndim, const double* Ppk, const double* Spk, const double* Hpk,
+                         ptbgpu_stats* st) {
+    return guarded(c, [&] {
+        PTB_CHECK(ndim > 0 && Ppk && Spk && st, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, ndim);
+        io.in(0, Ppk);
+        io.in(1, Spk);
+        if (Hpk) io.in(2, Hpk);
+        check_density_device(c, ndim, io.d[0], io.d[1], Hpk ? io.d[2] : nullptr, st);
+        PTB_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int ptbgpu_sm_density(ptbgpu_ctx* c, int64_t ndim, int64_t nelref, const double* Hpk, const double* Spk,
+                      double* Ppk, int64_t nat, const double* xyz, const int64_t* aoat, int64_t columns,
+                      int64_t mode, const int64_t* partition, const ptbgpu_opts* opts, ptbgpu_stats* st) {
+    clear_stats(st);
+    return guarded(c, [&] {
+        PTB_CHECK(ndim > 0 && Hpk && Spk && Ppk && aoat, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, ndim);
+        PhaseTimer t(c);
+        io.in(0, Hpk);
+        io.in(1, Spk);
+        t.mark(1);
+        sm_density_device(c, ndim, nelref, io.d[0], io.d[1], io.d[2], nat, xyz, aoat, columns, mode, partition,
+                          opts, st);
+        t.mark(2);
+        io.out(2, Ppk);
+        t.finish(st);
+    });
+}
+
+int ptbgpu_purify(ptbgpu_ctx* c, const ptbgpu_pur_settings* pur, int64_t ndim, const double* Hpk,
+                  const double* Spk, double* Ppk, const ptbgpu_opts* opts, ptbgpu_stats* st) {
+    clear_stats(st);
+    return guarded(c, [&] {
+        PTB_CHECK(pur && ndim > 0 && Hpk && Spk && Ppk, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, ndim);
+        PhaseTimer t(c);
+        io.in(0, Hpk);
+        io.in(1, Spk);
+        t.mark(1);
+        purify_ref_device(c, *pur, ndim, io.d[0], io.d[1], io.d[2], opts, st);
+        t.mark(2);
+        io.out(2, Ppk);
+        t.finish(st);
+    });
+}
+
+int ptbgpu_tc_purify(ptbgpu_ctx* c, int64_t ndim, int64_t nel, const double* Hpk, const double* Spk, double* Ppk,
+                     const ptbgpu_opts* opts, ptbgpu_stats* st) {
+    clear_stats(st);
+    return guarded(c, [&] {
+        PTB_CHECK(ndim > 0 && Hpk && Spk && Ppk, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, ndim);
+        PhaseTimer t(c);
+        io.in(0, Hpk);
+        io.in(1, Spk);
+        t.mark(1);
+        tc_purify_entry(c, ndim, nel, io.d[0], io.d[1], io.d[2], opts, st);
+        t.mark(2);
+        io.out(2, Ppk);
+        t.finish(st);
+    });
+}
+
+int ptbgpu_tc_purify_device(ptbgpu_ctx* c, int64_t ndim, int64_t nel, const double* dH, const double* dS,
+                            double* dP, const ptbgpu_opts* opts, ptbgpu_stats* st) {
+    clear_stats(st);
+    return guarded(c, [&] {
+        PTB_CHECK(ndim > 0 && dH && dS && dP, PTBGPU_EINVAL, "bad arguments");
+        PhaseTimer t(c);
+        t.mark(1);
+        tc_purify_entry(c, ndim, nel, dH, dS, dP, opts, st);
+        t.mark(2);
+        t.finish(st);
+    });
+}
+
+int ptbgpu_solve2(ptbgpu_ctx* c, int64_t mode, int64_t ndim, int64_t nel, int64_t nopen, const double* Hpk,
+                  const double* Spk, double* Ppk, double* e, double* focc, const ptbgpu_opts* opts,
+                  ptbgpu_stats* st) {
+    clear_stats(st);
+    return guarded(c, [&] {
+        PTB_CHECK(ndim > 0 && Hpk && Spk && Ppk, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, ndim);
+        PhaseTimer t(c);
+        io.in(0, Hpk);
+        io.in(1, Spk);
+        t.mark(1);
+        solve2_device(c, mode, ndim, nel, nopen, io.d[0], io.d[1], io.d[2], e, focc, opts, st);
+        t.mark(2);
+        io.out(2, Ppk);
+        t.finish(st);
+    });
+}
+
+int ptbgpu_symsq_bf16x3(ptbgpu_ctx* c, int64_t n, const double* X, float* C) {
+    return guarded(c, [&] {
+        PTB_CHECK(n > 0 && X && C, PTBGPU_EINVAL, "bad arguments");
+        symsq_entry(c, n, X, C);
+    });
+}
+
+}  // extern "C"

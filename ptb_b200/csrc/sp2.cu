@@ -1,0 +1,581 @@
+// Trace-correcting (SP2) purification of the dense density-matrix step.
+//
+// Both precisions share the orthogonalisation: S = L L^T (Cholesky),
+// A = L^-1 H L^-T, Gershgorin bounds [e_min, e_max] of A,
+// X_0 = (e_max I - A) / (e_max - e_min), and at the end P = 2 L^-T X L^-1.
+// Each SP2 step maps X -> X^2 or X -> 2X - X^2, whichever lands tr X closer
+// to N = nel/2 (tr X^2 = ||X||_F^2 for symmetric X is known before the
+// product, so the branch is decided first).
+//
+// PTBGPU_PREC_FP64: every product is an FP64 SYRK (the comparator path).
+//
+// PTBGPU_PREC_MIXED:
+//   pass 1   SP2 products on the tcgen05 kernel with bf16x3 operands and FP32
+//            accumulation; the epilogue applies the branch, writes the next
+//            iterate (FP32 + bf16 hi/lo planes, kept for every step: the
+//            trajectory) and per-tile trace / sum-of-squares partials; a
+//            one-block kernel reduces them and decides the next branch and
+//            convergence on the device.
+//   cleanup  a few FP64 SP2 steps make the pass-1 result P~ idempotent to
+//            rounding (its subspace still carries the bf16x3 error).
+//   refine   first-order density-matrix perturbation theory around P~: with
+//            C = [A, P~] (one FP64 product) the off-diagonal part of A in the
+//            P~ basis is A1 = [C, P~] (small, so a bf16x3 product suffices);
+//            its response is propagated through the recorded branch sequence
+//            over the stored trajectory, X1 <- X0_k X1 + X1 X0_k (or
+//            2 X1 - (...)), again with bf16x3 products; P = P~ + X1.
+//            The error left is second order in the pass-1 error.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "tc_gemm.cuh"
+
+namespace ptb {
+
+namespace {
+
+constexpr int kMaxIt = 255;
+
+struct SP2State {
+    int active;      // 1 while pass 1 runs; product/decision launches are no-ops at 0
+    int next;        // index of the iterate the next decision evaluates
+    int converged;
+    int status;      // 0 or a PTBGPU_E* code
+    int sq_cur;      // branch for the step about to run
+    int pad[3];
+    double trX[kMaxIt + 1];
+    double trX2[kMaxIt + 1];
+    double err[kMaxIt + 1];
+    int sq[kMaxIt + 1];
+};
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// X_0 = (e_max I - A)/(e_max - e_min) from column-major FP64 A (n x n), into
+// zero-padded FP32 / bf16 hi / bf16 lo planes (ldp x ldp); per-block partials
+// of tr X_0 and ||X_0||^2 into stats[2*block].
+__global__ void k_x0_init(int64_t n, int64_t ldp, const double* __restrict__ A, double emax, double scale,
+                          float* __restrict__ xf, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
+                          double* __restrict__ stats) {
+    double tr = 0.0, ss = 0.0;
+    for (int64_t j = blockIdx.x; j < ldp; j += gridDim.x) {
+        for (int64_t i = threadIdx.x; i < ldp; i += blockDim.x) {
+            float v = 0.0f;
+            if (i < n && j < n) {
+                double d = ((i == j) ? emax : 0.0) - A[i + j * n];
+                v = (float)(d * scale);
+            }
+            const int64_t k = i + j * ldp;
+            xf[k] = v;
+            __nv_bfloat16 h = __float2bfloat16_rn(v);
+            hi[k] = h;
+            lo[k] = __float2bfloat16_rn(v - __bfloat162float(h));
+            const double dv = v;
+            if (i == j) tr += dv;
+            ss += dv * dv;
+        }
+    }
+    __shared__ double sh[2][32];
+    tr = warp_sum(tr);
+    ss = warp_sum(ss);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sh[0][w] = tr;
+        sh[1][w] = ss;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+            a += sh[0][q];
+            b += sh[1][q];
+        }
+        stats[2 * blockIdx.x] = a;
+        stats[2 * blockIdx.x + 1] = b;
+    }
+}
+
+// Reduce the partials of iterate k in a fixed order and decide the next step.
+__global__ void k_decide(SP2State* st, const double* __restrict__ stats, int nparts, double N, double tol_abs,
+                         double e_switch, int maxit) {
+    if (!st->active) return;
+    __shared__ double sh[2][256];
+    double a = 0.0, b = 0.0;
+    for (int p = threadIdx.x; p < nparts; p += blockDim.x) {
+        a += stats[2 * p];
+        b += stats[2 * p + 1];
+    }
+    sh[0][threadIdx.x] = a;
+    sh[1][threadIdx.x] = b;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + s];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    const int k = st->next;
+    const double trX = sh[0][0], trX2 = sh[1][0];
+    const double e = trX - trX2;
+    st->trX[k] = trX;
+    st->trX2[k] = trX2;
+    st->err[k] = e;
+    if (!(e == e)) {
+        st->status = PTBGPU_ENAN;
+        st->active = 0;
+        return;
+    }
+    const int sq = fabs(trX2 - N) <= fabs(2.0 * trX - trX2 - N) ? 1 : 0;
+    st->sq[k] = sq;
+    st->sq_cur = sq;
+    const double ae = fabs(e);
+    const bool conv = ae < tol_abs || (k >= 2 && ae < e_switch && ae >= fabs(st->err[k - 2]));
+    if (conv) {
+        st->converged = 1;
+        st->active = 0;
+    } else if (k >= maxit || k >= kMaxIt) {
+        st->status = PTBGPU_EITER;
+        st->active = 0;
+    } else {
+        st->next = k + 1;
+    }
+}
+
+// out(i,j) = alpha (W_ij + W_ji) + beta X_ij over the ldp x ldp FP32 planes
+// (row-major W), 32x32 tile pairs through shared memory; also writes the bf16
+// hi/lo planes of the result.  blockDim = (32, 8).
+__global__ void k_sym_update(int64_t ldp, const float* __restrict__ W, const float* __restrict__ X, float alpha,
+                             float beta, float* __restrict__ out, __nv_bfloat16* __restrict__ hi,
+                             __nv_bfloat16* __restrict__ lo) {
+    __shared__ float t[32][33];
+    const int64_t bi = blockIdx.y, bj = blockIdx.x;
+    if (bi > bj) return;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int64_t i0 = bi * 32, j0 = bj * 32;
+    // stage W(j-block rows, i-block cols) transposed: t[c][r] = W[j0 + r][i0 + c]
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) t[tx][ty + k] = W[(j0 + ty + k) * ldp + i0 + tx];
+    __syncthreads();
+    // element (i, j) = (i0 + ty + k, j0 + tx): W[i][j] + W[j][i]
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const int64_t i = i0 + ty + k, j = j0 + tx;
+        const float s = W[i * ldp + j] + t[ty + k][tx];
+        const float v = alpha * s + (beta != 0.0f ? beta * X[i * ldp + j] : 0.0f);
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+        out[i * ldp + j] = v;
+        hi[i * ldp + j] = h;
+        lo[i * ldp + j] = l;
+        t[ty + k][tx] = v;   // each thread rewrites only the slot it read
+    }
+    __syncthreads();
+    if (bi == bj) return;
+    // mirrored tile: element (j, i) with j = j0 + ty + k, i = i0 + tx
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const int64_t j = j0 + ty + k, i = i0 + tx;
+        const float v = t[tx][ty + k];
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        out[j * ldp + i] = v;
+        hi[j * ldp + i] = h;
+        lo[j * ldp + i] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+}
+
+// FP32 plane (ldp) -> FP64 column-major n x n, optionally added to y: y = a*x + b*y
+__global__ void k_f2d(int64_t n, int64_t ldp, const float* __restrict__ x, double a, double b,
+                      double* __restrict__ y) {
+    for (int64_t j = blockIdx.x; j < n; j += gridDim.x)
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const double v = a * (double)x[i + j * ldp];
+            y[i + j * n] = (b == 0.0) ? v : v + b * y[i + j * n];
+        }
+}
+
+// C = W - W^T (column-major FP64), 32x32 tiles.  blockDim = (32, 8).
+__global__ void k_antisym(int64_t n, const double* __restrict__ W, double* __restrict__ C) {
+    __shared__ double t[32][33];
+    const int64_t bi = blockIdx.y, bj = blockIdx.x;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int64_t i0 = bi * 32, j0 = bj * 32;
+    // t[c][r] = W(j0 + c, i0 + r)  (i.e. W^T entries)
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const int64_t row = j0 + tx, col = i0 + ty + k;
+        t[tx][ty + k] = (row < n && col < n) ? W[row + col * n] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const int64_t row = i0 + tx, col = j0 + ty + k;
+        if (row < n && col < n) C[row + col * n] = W[row + col * n] - t[ty + k][tx];
+    }
+}
+
+int grid1(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(n, 148 * 16)); }
+
+// A tensor-core product bracketed by CUDA events on the launching stream; the
+// C-ABI layer sums the elapsed times per kind into the call's stats.
+void timed_product(ptbgpu_ctx* c, int epi, int64_t ldp, const void* a0, const void* a1, const void* b0,
+                   const void* b1, const tc::ProdList& prods, const int2* tiles, int ntiles, const tc::EpiParams& ep) {
+    cudaEvent_t a = c->take_event(), b = c->take_event();
+    PTB_CUDA(cudaEventRecord(a, c->stream));
+    tc::launch_product(c->stream, epi, ldp, a0, a1, b0, b1, prods, tiles, ntiles, ep);
+    PTB_CUDA(cudaEventRecord(b, c->stream));
+    c->timed.push_back({epi == tc::EPI_SP2 ? 0 : 1, a, b});
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+struct Prologue {
+    double emin, emax;
+};
+
+// H (packed) -> A = L^-1 H L^-T in B_H; S (packed) -> L in B_S.  Both column-major, ld = n.
+Prologue orthogonalise(ptbgpu_ctx* c, int64_t n, const double* dHpk, const double* dSpk, double filter) {
+    DevBuf& bh = c->buf(B_H);
+    DevBuf& bs = c->buf(B_S);
+    bh.reserve(sizeof(double) * n * n);
+    bs.reserve(sizeof(double) * n * n);
+    double* H = bh.as<double>();
+    double* S = bs.as<double>();
+    unpack_sym(c->stream, n, n, dHpk, H, filter);
+    unpack_sym(c->stream, n, n, dSpk, S, filter);
+    const int info = dpotrf_lower(c, n, n, S);
+    PTB_CHECK(info == 0, PTBGPU_ENOTSPD, "overlap matrix not positive definite (potrf info=%d)", info);
+    const double one = 1.0;
+    PTB_CUBLAS(cublasDtrsm(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                           (int)n, (int)n, &one, S, (int)n, H, (int)n));
+    PTB_CUBLAS(cublasDtrsm(c->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT,
+                           (int)n, (int)n, &one, S, (int)n, H, (int)n));
+    symmetrize_upper(c->stream, n, n, H);
+    Prologue p;
+    gershgorin_bounds(c, n, n, H, &p.emin, &p.emax);
+    PTB_CHECK(std::isfinite(p.emin) && std::isfinite(p.emax) && p.emax > p.emin, PTBGPU_ENAN,
+              "invalid spectral bounds [%g, %g]", p.emin, p.emax);
+    return p;
+}
+
+// P = 2 L^-T X L^-1 (X in place, column-major n x n), then packed into dPpk.
+void back_transform(ptbgpu_ctx* c, int64_t n, double* X, double* dPpk) {
+    const double* L = c->buf(B_S).as<double>();
+    const double two = 2.0, one = 1.0;
+    PTB_CUBLAS(cublasDtrsm(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT,
+                           (int)n, (int)n, &two, L, (int)n, X, (int)n));
+    PTB_CUBLAS(cublasDtrsm(c->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                           (int)n, (int)n, &one, L, (int)n, X, (int)n));
+    pack_cols(c->stream, n, n, X, dPpk);
+}
+
+// One FP64 SP2 step on X (column-major n x n, symmetric) using W as scratch;
+// returns the idempotency error tr X - tr X^2 of the input and whether it squared.
+struct StepInfo {
+    double trX, trX2, err;
+    bool sq;
+};
+StepInfo fp64_step(ptbgpu_ctx* c, int64_t n, double N, double*& X, double*& W) {
+    StepInfo s;
+    s.trX = trace_dev(c, n, n, X);
+    const double f = frob_dev(c, n, n, X);
+    s.trX2 = f * f;
+    s.err = s.trX - s.trX2;
+    PTB_CHECK(std::isfinite(s.err), PTBGPU_ENAN, "NaN during purification");
+    s.sq = std::fabs(s.trX2 - N) <= std::fabs(2.0 * s.trX - s.trX2 - N);
+    dsyrk_sq(c, n, n, X, W);                         // W = X^2
+    if (!s.sq) axpby_diag(c->stream, n, n, 2.0, X, -1.0, W, 0.0);   // W = 2X - X^2
+    std::swap(X, W);
+    return s;
+}
+
+void sp2_fp64(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int maxit, double* dPpk,
+              ptbgpu_stats* st, int prl) {
+    double* X = c->buf(B_H).as<double>();
+    DevBuf& bw = c->buf(B_W0);
+    bw.reserve(sizeof(double) * n * n);
+    double* W = bw.as<double>();
+    const double scale = 1.0 / (pro.emax - pro.emin);
+    axpby_diag(c->stream, n, n, 0.0, nullptr, -scale, X, pro.emax * scale);
+    const double N = 0.5 * (double)nel;
+    std::vector<double> hist;
+    int it = 0;
+    bool done = false;
+    for (it = 1; it <= maxit; ++it) {
+        StepInfo s = fp64_step(c, n, N, X, W);
+        const double e = std::fabs(s.err);
+        hist.push_back(e);
+        log_line(prl, 2, " SP2 (fp64) iter %3d  trX %.10f  err %.3e  %s", it, s.trX, s.err, s.sq ? "X^2" : "2X-X^2");
+        if (e < 1e-13 * (double)n || (hist.size() > 2 && e < 1e-2 && e >= hist[hist.size() - 3])) {
+            done = true;
+            break;
+        }
+    }
+    PTB_CHECK(done, PTBGPU_EITER, "trace-correcting purification did not converge in %d iterations", maxit);
+    back_transform(c, n, X, dPpk);
+    if (st) {
+        st->iterations = it;
+        st->flops += (double)it * (double)n * n * n;   // SYRK-equivalent products
+    }
+}
+
+void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int maxit, bool refine,
+               double* dPpk, ptbgpu_stats* st, int prl) {
+    cudaStream_t s = c->stream;
+    const int64_t ldp = round_up(n, tc::tile_n());
+    const size_t plane = sizeof(__nv_bfloat16) * (size_t)ldp * ldp;
+    const size_t fplane = sizeof(float) * (size_t)ldp * ldp;
+
+    // trajectory slots (hi+lo per iterate), bounded by free memory
+    size_t free_b = 0, total_b = 0;
+    PTB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t other = 6 * fplane + 4 * plane + (size_t)(64 << 20);
+    int slots = (int)std::min<int64_t>(maxit + 1, kMaxIt + 1);
+    if (free_b > other) slots = (int)std::min<size_t>(slots, (free_b - other) * 6 / 10 / (2 * plane));
+    PTB_CHECK(slots >= 8, PTBGPU_ENOMEM, "not enough device memory for the purification trajectory");
+    DevBuf& btraj = c->buf(B_TRAJ);
+    btraj.reserve(2 * plane * (size_t)slots);
+    auto traj_hi = [&](int k) { return (__nv_bfloat16*)((char*)btraj.ptr + 2 * plane * (size_t)k); };
+    auto traj_lo = [&](int k) { return (__nv_bfloat16*)((char*)btraj.ptr + 2 * plane * (size_t)k + plane); };
+    c->buf(B_XF0).reserve(fplane);
+    c->buf(B_XF1).reserve(fplane);
+    float* xf[2] = {c->buf(B_XF0).as<float>(), c->buf(B_XF1).as<float>()};
+
+    // tiles and per-tile stats
+    std::vector<int2> up = tc::make_tiles(ldp, true);
+    std::vector<int2> all = tc::make_tiles(ldp, false);
+    DevBuf& bt = c->buf(B_TILES);
+    bt.reserve(sizeof(int2) * (up.size() + all.size()));
+    int2* tiles_up = bt.as<int2>();
+    int2* tiles_all = tiles_up + up.size();
+    PTB_CUDA(cudaMemcpyAsync(tiles_up, up.data(), sizeof(int2) * up.size(), cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemcpyAsync(tiles_all, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s));
+    const int x0_blocks = grid1(ldp);
+    DevBuf& bstats = c->buf(B_STATS);
+    bstats.reserve(sizeof(double) * 2 * std::max<size_t>(up.size(), (size_t)x0_blocks));
+    double* stats = bstats.as<double>();
+    if (!c->sp2_state) PTB_CUDA(cudaMalloc(&c->sp2_state, sizeof(SP2State)));
+    SP2State* state = (SP2State*)c->sp2_state;
+    PTB_CUDA(cudaMemsetAsync(state, 0, sizeof(SP2State), s));
+    const int one = 1;
+    PTB_CUDA(cudaMemcpyAsync(&state->active, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemsetAsync(&c->flags->timeout, 0, sizeof(int), s));
+
+    const double* A = c->buf(B_H).as<double>();
+    const double scale = 1.0 / (pro.emax - pro.emin);
+    const double N = 0.5 * (double)nel;
+    const double tol_abs = 1e-6 * (double)n;   // floor of bf16x3 iterations
+    const double e_switch = 1.0;
+    k_x0_init<<<x0_blocks, 256, 0, s>>>(n, ldp, A, pro.emax, scale, xf[0], traj_hi(0), traj_lo(0), stats);
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+    k_decide<<<1, 256, 0, s>>>(state, stats, x0_blocks, N, tol_abs, e_switch, std::min(maxit, slots - 1));
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+
+    tc::ProdList split3{3, {0, 0, 1, 0}, {0, 1, 0, 0}};
+    tc::EpiParams ep{};
+    ep.active = &state->active;
+    ep.sq_flag = &state->sq_cur;
+    ep.err = &c->flags->timeout;
+    ep.ld = ldp;
+    ep.stats = stats;
+    const int cap = std::min(maxit, slots - 1);
+    int launched = 0;
+    SP2State* hs = (SP2State*)c->pinned;   // only the 8-int header is read back while iterating
+    for (int k = 0; k < cap; ++k) {
+        ep.xcur = xf[k & 1];
+        ep.out = xf[(k + 1) & 1];
+        ep.hi = traj_hi(k + 1);
+        ep.lo = traj_lo(k + 1);
+        timed_product(c, tc::EPI_SP2, ldp, traj_hi(k), traj_lo(k), traj_hi(k), traj_lo(k), split3, tiles_up,
+                           (int)up.size(), ep);
+        k_decide<<<1, 256, 0, s>>>(state, stats, (int)up.size(), N, tol_abs, e_switch, cap);
+        count_launch();
+        PTB_CUDA(cudaGetLastError());
+        ++launched;
+        if ((k & 3) == 3 || k + 1 == cap) {
+            PTB_CUDA(cudaMemcpyAsync(hs, state, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
+            PTB_CUDA(cudaStreamSynchronize(s));
+            if (!hs->active) break;
+        }
+    }
+    std::vector<SP2State> hstate(1);
+    PTB_CUDA(cudaMemcpyAsync(hstate.data(), state, sizeof(SP2State), cudaMemcpyDeviceToHost, s));
+    int tmo = 0;
+    PTB_CUDA(cudaMemcpyAsync(&tmo, &c->flags->timeout, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PTB_CUDA(cudaStreamSynchronize(s));
+    const SP2State& H = hstate[0];
+    PTB_CHECK(tmo == 0, PTBGPU_ETIMEOUT, "tensor-core product gave up waiting (site %d)", tmo);
+    PTB_CHECK(H.status == 0, H.status, "pass-1 purification failed (status %d at iterate %d)", H.status, H.next);
+    PTB_CHECK(H.converged, PTBGPU_EITER, "pass-1 purification did not converge in %d iterations", cap);
+    const int K = H.next;   // index of the final pass-1 iterate
+    for (int k = 0; k <= K && prl >= 2; ++k)
+        log_line(prl, 2, " SP2 (bf16x3) iter %3d  trX %.10f  err %.3e  %s", k, H.trX[k], H.err[k],
+                 k < K ? (H.sq[k] ? "X^2" : "2X-X^2") : "final");
+
+    // FP64 cleanup of the pass-1 result
+    DevBuf& bw0 = c->buf(B_W0);
+    DevBuf& bw1 = c->buf(B_W1);
+    bw0.reserve(sizeof(double) * n * n);
+    bw1.reserve(sizeof(double) * n * n);
+    double* X = bw0.as<double>();
+    double* W = bw1.as<double>();
+    k_f2d<<<grid1(n), 256, 0, s>>>(n, ldp, xf[K & 1], 1.0, 0.0, X);
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+    std::vector<double> hist;
+    int nclean = 0;
+    for (nclean = 1; nclean <= 8; ++nclean) {
+        StepInfo si = fp64_step(c, n, N, X, W);
+        const double e = std::fabs(si.err);
+        hist.push_back(e);
+        log_line(prl, 2, " SP2 (fp64 cleanup) %d  err %.3e", nclean, si.err);
+        if (e < 1e-13 * (double)n || (hist.size() > 2 && e >= hist[hist.size() - 3])) break;
+    }
+    nclean = std::min(nclean, 8);
+    double flops = (double)K * 3.0 * (double)n * n * n /*bf16x3, symmetric half*/ +
+                   (double)nclean * (double)n * n * n;
+
+    if (refine) {
+        // C = A P~ - P~ A (FP64)
+        DevBuf& bw2 = c->buf(B_W2);
+        bw2.reserve(sizeof(double) * n * n);
+        double* Wc = bw2.as<double>();
+        dgemm_nn(c, n, n, 1.0, A, X, 0.0, W);
+        const unsigned nb = (unsigned)((n + 31) / 32);
+        k_antisym<<<dim3(nb, nb), dim3(32, 8), 0, s>>>(n, W, Wc);
+        count_launch();
+        PTB_CUDA(cudaGetLastError());
+        // bf16x3 planes of C and P~ (padded), V = C^T P~ = -C P~ on the tensor cores
+        c->buf(B_X1HI).reserve(2 * plane);
+        c->buf(B_X1LO).reserve(2 * plane);
+        c->buf(B_MISC0).reserve(fplane);   // W (FP32, row-major)
+        c->buf(B_X1F0).reserve(fplane);
+        c->buf(B_X1F1).reserve(fplane);
+        DevBuf& bp = c->buf(B_MISC1);
+        bp.reserve(2 * plane);
+        __nv_bfloat16* chi = (__nv_bfloat16*)c->buf(B_X1HI).ptr;
+        __nv_bfloat16* clo = chi + (size_t)ldp * ldp;
+        __nv_bfloat16* phi = (__nv_bfloat16*)bp.ptr;
+        __nv_bfloat16* plo = phi + (size_t)ldp * ldp;
+        float* wf = c->buf(B_MISC0).as<float>();
+        float* x1f[2] = {c->buf(B_X1F0).as<float>(), c->buf(B_X1F1).as<float>()};
+        // X1 hi planes live in B_X1LO; its lo planes take over the C planes once
+        // the product V below has consumed them (stream order).
+        __nv_bfloat16* x1hi[2] = {(__nv_bfloat16*)c->buf(B_X1LO).ptr,
+                                  (__nv_bfloat16*)c->buf(B_X1LO).ptr + (size_t)ldp * ldp};
+        __nv_bfloat16* x1lo[2] = {chi, clo};
+        d2f_split(s, n, ldp, Wc, nullptr, chi, clo);
+        d2f_split(s, n, ldp, X, nullptr, phi, plo);
+        tc::EpiParams epf{};
+        epf.err = &c->flags->timeout;
+        epf.ld = ldp;
+        epf.out = wf;
+        timed_product(c, tc::EPI_FULL, ldp, chi, clo, phi, plo, split3, tiles_all, (int)all.size(), epf);
+        // The planes hold C^T (column-major C read row-major), so wf = C^T P~ = -C P~.
+        // A1 = C P~ - P~ C = -(wf + wf^T) and X1_0 = -A1 / (e_max - e_min) = (wf + wf^T) * scale.
+        const unsigned nbp = (unsigned)(ldp / 32);
+        k_sym_update<<<dim3(nbp, nbp), dim3(32, 8), 0, s>>>(ldp, wf, nullptr, (float)scale, 0.0f, x1f[0], x1hi[0],
+                                                            x1lo[0]);
+        count_launch();
+        PTB_CUDA(cudaGetLastError());
+        // replay the branch sequence over the stored trajectory
+        for (int k = 0; k < K; ++k) {
+            const int a = k & 1, b = a ^ 1;
+            timed_product(c, tc::EPI_FULL, ldp, traj_hi(k), traj_lo(k), x1hi[a], x1lo[a], split3, tiles_all,
+                               (int)all.size(), epf);
+            const bool sq = H.sq[k] != 0;
+            k_sym_update<<<dim3(nbp, nbp), dim3(32, 8), 0, s>>>(ldp, wf, x1f[a], sq ? 1.0f : -1.0f,
+                                                                sq ? 0.0f : 2.0f, x1f[b], x1hi[b], x1lo[b]);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+        }
+        // P_o = P~ + X1_K
+        k_f2d<<<grid1(n), 256, 0, s>>>(n, ldp, x1f[K & 1], 1.0, 1.0, X);
+        count_launch();
+        PTB_CUDA(cudaGetLastError());
+        flops += 2.0 * (double)n * n * n /*FP64 commutator*/ + (double)(K + 1) * 3.0 * 2.0 * (double)n * n * n;
+        PTB_CUDA(cudaMemcpyAsync(&tmo, &c->flags->timeout, sizeof(int), cudaMemcpyDeviceToHost, s));
+        PTB_CUDA(cudaStreamSynchronize(s));
+        PTB_CHECK(tmo == 0, PTBGPU_ETIMEOUT, "tensor-core product gave up waiting (site %d)", tmo);
+    }
+    back_transform(c, n, X, dPpk);
+    if (st) {
+        st->iterations = K + nclean;
+        st->flops += flops;
+    }
+}
+
+void tc_purify_device(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, const double* dS, double* dP,
+                      const ptbgpu_opts* o, ptbgpu_stats* st) {
+    PTB_CHECK(n > 0 && nel > 0 && nel <= 2 * n, PTBGPU_EINVAL, "bad sizes ndim=%lld nel=%lld", (long long)n,
+              (long long)nel);
+    PTB_CHECK(nel % 2 == 0, PTBGPU_EINVAL, "trace-correcting purification needs an even electron count");
+    ptbgpu_opts def;
+    ptbgpu_default_opts(&def);
+    if (!o) o = &def;
+    const int maxit = o->max_iter > 0 ? (int)std::min<int64_t>(o->max_iter, kMaxIt) : 100;
+    const int prl = (int)o->print_level;
+    Prologue pro = orthogonalise(c, n, dH, dS, o->filter);
+    if (st) st->flops += (1.0 / 3.0 + 4.0) * (double)n * n * n;   // potrf + 4 trsm
+    if (o->precision == PTBGPU_PREC_FP64)
+        sp2_fp64(c, n, nel, pro, maxit, dP, st, prl);
+    else
+        sp2_mixed(c, n, nel, pro, maxit, o->precision != 2, dP, st, prl);
+}
+
+}  // namespace
+
+void tc_purify_entry(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, const double* dS, double* dP,
+                     const ptbgpu_opts* o, ptbgpu_stats* st) {
+    tc_purify_device(c, n, nel, dH, dS, dP, o, st);
+}
+
+// C = X X with the bf16x3 kernel (every tile, EPI_FULL), for kernel-level tests.
+void symsq_entry(ptbgpu_ctx* c, int64_t n, const double* hX, float* hC) {
+    cudaStream_t s = c->stream;
+    const int64_t ldp = round_up(n, tc::tile_n());
+    const size_t plane = sizeof(__nv_bfloat16) * (size_t)ldp * ldp;
+    DevBuf& bx = c->buf(B_W0);
+    bx.reserve(sizeof(double) * n * n);
+    PTB_CUDA(cudaMemcpyAsync(bx.ptr, hX, sizeof(double) * n * n, cudaMemcpyHostToDevice, s));
+    DevBuf& bp = c->buf(B_MISC1);
+    bp.reserve(2 * plane);
+    __nv_bfloat16* hi = (__nv_bfloat16*)bp.ptr;
+    __nv_bfloat16* lo = hi + (size_t)ldp * ldp;
+    d2f_split(s, n, ldp, bx.as<double>(), nullptr, hi, lo);
+    DevBuf& bc = c->buf(B_MISC0);
+    bc.reserve(sizeof(float) * (size_t)ldp * ldp);
+    std::vector<int2> all = tc::make_tiles(ldp, false);
+    DevBuf& bt = c->buf(B_TILES);
+    bt.reserve(sizeof(int2) * all.size());
+    PTB_CUDA(cudaMemcpyAsync(bt.ptr, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemsetAsync(&c->flags->timeout, 0, sizeof(int), s));
+    tc::ProdList split3{3, {0, 0, 1, 0}, {0, 1, 0, 0}};
+    tc::EpiParams ep{};
+    ep.err = &c->flags->timeout;
+    ep.ld = ldp;
+    ep.out = bc.as<float>();
+    tc::launch_product(s, tc::EPI_FULL, ldp, hi, lo, hi, lo, split3, bt.as<int2>(), (int)all.size(), ep);
+    PTB_CUDA(cudaMemcpy2DAsync(hC, sizeof(float) * n, bc.ptr, sizeof(float) * ldp, sizeof(float) * n, n,
+                               cudaMemcpyDeviceToHost, s));
+    int tmo = 0;
+    PTB_CUDA(cudaMemcpyAsync(&tmo, &c->flags->timeout, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PTB_CUDA(cudaStreamSynchronize(s));
+    PTB_CHECK(tmo == 0, PTBGPU_ETIMEOUT, "tensor-core product gave up waiting (site %d)", tmo);
+}
+
+}  // namespace ptb

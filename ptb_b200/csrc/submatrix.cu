@@ -1,0 +1,658 @@
+// Submatrix method, sm_stupid_simple (source/sm.f90:34-409), on the device.
+//
+//  1. column grouping (host, source/sm.f90:92-162): owned columns per submatrix
+//  2. pattern scan: row i joins submatrix k iff H(i,c) > 0 or S(i,c) > 0 or
+//     i == c for an owned column c (strictly positive, source/sm.f90:210-228);
+//     one coalesced pass over H and S, flags[k][i]
+//  3. ordered compaction of the flags into the sorted index maps (CSR) and the
+//     position of every owned column inside its map
+//  4. submatrices bucketed by padded size M (multiple of 32); H_k, S_k gathered
+//     into M x M batches, padded with H = 1e3 I, S = I (eigenvalues far above
+//     the mu bracket, eigenvectors outside the real block: they carry no
+//     electrons and no density);  S_k = L L^T, C = L^-1 H_k L^-T, C = V w V^T,
+//     U = L^-T V  (the generalized problem of la_sygvd, source/sm.f90:296-299)
+//  5. fe_j = sum_{c owned} (S_k U)_{ic,j} U_{ic,j}  (source/sm.f90:305-310)
+//  6. mu bisection on [-10, 10] with occupations 2 / 1 / 0 for e < / = / > mu,
+//     stop on |a-b| < 1e-3 or |nel - nelref| < 1e-5 (REAL(4) literals), then
+//     one final pass at the same mu (source/sm.f90:191-383) - one block
+//  7. final density: P(map(i), c) = sum_j U_ij occ_j U_{ic,j} for owned c,
+//     written directly into the packed result for map(i) <= c (packsym keeps
+//     column c, rows <= c; rows outside the map stay zero, source/sm.f90:201-203,
+//     343-362, 387).
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+
+namespace ptb {
+
+namespace {
+
+constexpr double kPadDiag = 1.0e3;
+
+// (2) flags[k*n + i] |= (H(i,c) > 0 || S(i,c) > 0 || i == c) for column c of submatrix owner[c]
+__global__ void k_pattern(int64_t n, const double* __restrict__ H, const double* __restrict__ S,
+                          const int* __restrict__ owner, uint8_t* __restrict__ flags) {
+    for (int64_t c = blockIdx.x; c < n; c += gridDim.x) {
+        const int k = owner[c];
+        if (k < 0) continue;
+        uint8_t* f = flags + (int64_t)k * n;
+        const double* hc = H + c * n;
+        const double* sc = S + c * n;
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x)
+            if (hc[i] > 0.0 || sc[i] > 0.0 || i == c) f[i] = 1;
+    }
+}
+
+__global__ void k_count(int64_t n, const uint8_t* __restrict__ flags, int* __restrict__ counts) {
+    const int k = blockIdx.x;
+    int cnt = 0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) cnt += flags[(int64_t)k * n + i];
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    __shared__ int sh[32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        counts[k] = t;
+    }
+}
+
+// (3) ordered compaction; 256 threads per block (one submatrix per block).
+__global__ void k_fill(int64_t n, const uint8_t* __restrict__ flags, const int64_t* __restrict__ offs,
+                       const int* __restrict__ owner, int* __restrict__ maps, int* __restrict__ ipos) {
+    const int k = blockIdx.x;
+    const uint8_t* f = flags + (int64_t)k * n;
+    int* mp = maps + offs[k];
+    __shared__ int warp_tot[8];
+    __shared__ int base;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t c0 = 0; c0 < n; c0 += blockDim.x) {
+        const int64_t i = c0 + threadIdx.x;
+        const bool on = i < n && f[i];
+        const unsigned m = __ballot_sync(0xffffffffu, on);
+        const int before = __popc(m & ((1u << lane) - 1u));
+        if (lane == 0) warp_tot[w] = __popc(m);
+        __syncthreads();
+        int wbase = 0;
+        for (int q = 0; q < w; ++q) wbase += warp_tot[q];
+        if (on) {
+            const int p = base + wbase + before;
+            mp[p] = (int)i;
+            if (owner[i] == k) ipos[i] = p;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int q = 0; q < 8; ++q) t += warp_tot[q];
+            base += t;
+        }
+        __syncthreads();
+    }
+}
+
+struct Prob {
+    int k;          // submatrix index
+    int m;          // real dimension
+    int64_t moff;   // offset of its map in maps[]
+    int64_t eoff;   // offset of its eigenpairs in e[] / fe[]
+};
+
+// (4) gather H_k, S_k into the padded M x M batch (column-major per problem).
+__global__ void k_gather(int M, const Prob* __restrict__ probs, const int* __restrict__ maps, int64_t n,
+                         const double* __restrict__ H, const double* __restrict__ S, double* __restrict__ Hb,
+                         double* __restrict__ Sb) {
+    const Prob p = probs[blockIdx.z];
+    const int* mp = maps + p.moff;
+    double* hb = Hb + (int64_t)blockIdx.z * M * M;
+    double* sb = Sb + (int64_t)blockIdx.z * M * M;
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    for (int j = blockIdx.y * 8 + threadIdx.y; j < M; j += gridDim.y * 8) {
+        if (i >= M) continue;
+        double h, s;
+        if (i < p.m && j < p.m) {
+            const int64_t gi = mp[i], gj = mp[j];
+            h = H[gi + gj * n];
+            s = S[gi + gj * n];
+        } else {
+            h = (i == j) ? kPadDiag : 0.0;
+            s = (i == j) ? 1.0 : 0.0;
+        }
+        hb[i + (int64_t)j * M] = h;
+        sb[i + (int64_t)j * M] = s;
+    }
+}
+
+// (5) fe_j for problem blockIdx.x: the owned rows of S_k are staged in shared
+// memory FE_CH at a time (S_k(ic, l) = S(c, map(l))); warp per eigenvector
+// column j, lanes over l (coalesced reads of U's column j).
+constexpr int FE_CH = 4;
+__global__ void k_fe(int M, const Prob* __restrict__ probs, const int* __restrict__ maps,
+                     const int64_t* __restrict__ own_off, const int* __restrict__ own_cols,
+                     const int* __restrict__ ipos, int64_t n, const double* __restrict__ S,
+                     const double* __restrict__ Ub, const double* __restrict__ w, double* __restrict__ e_out,
+                     double* __restrict__ fe_out) {
+    extern __shared__ double sm[];
+    double* srow = sm;                 // FE_CH x M
+    double* fes = sm + FE_CH * M;      // M
+    const Prob p = probs[blockIdx.x];
+    const int* mp = maps + p.moff;
+    const double* U = Ub + (int64_t)blockIdx.x * M * M;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int j = threadIdx.x; j < p.m; j += blockDim.x) fes[j] = 0.0;
+    const int64_t o0 = own_off[p.k], o1 = own_off[p.k + 1];
+    for (int64_t ob = o0; ob < o1; ob += FE_CH) {
+        const int nc = (int)((o1 - ob) < FE_CH ? (o1 - ob) : FE_CH);
+        __syncthreads();
+        for (int t = 0; t < nc; ++t) {
+            const int64_t c = own_cols[ob + t];
+            for (int l = threadIdx.x; l < p.m; l += blockDim.x) srow[t * M + l] = S[c + (int64_t)mp[l] * n];
+        }
+        __syncthreads();
+        for (int j = wp; j < p.m; j += nw) {
+            const double* uj = U + (int64_t)j * M;
+            double add = 0.0;
+            for (int t = 0; t < nc; ++t) {
+                double sdot = 0.0;
+                for (int l = lane; l < p.m; l += 32) sdot += srow[t * M + l] * uj[l];
+                for (int o = 16; o > 0; o >>= 1) sdot += __shfl_xor_sync(0xffffffffu, sdot, o);
+                add += sdot * uj[ipos[own_cols[ob + t]]];
+            }
+            if (lane == 0) fes[j] += add;
+        }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < p.m; j += blockDim.x) {
+        e_out[p.eoff + j] = w[(int64_t)blockIdx.x * M + j];
+        fe_out[p.eoff + j] = fes[j];
+    }
+}
+
+// fe for one large submatrix from T = S_k U (column-major m x m): thread per j.
+__global__ void k_fe_large(int m, const double* __restrict__ T, const double* __restrict__ U,
+                           const int* __restrict__ own_cols, int64_t o0, int64_t o1, const int* __restrict__ ipos,
+                           const double* __restrict__ w, double* __restrict__ e_out, double* __restrict__ fe_out) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+        double f = 0.0;
+        for (int64_t oc = o0; oc < o1; ++oc) {
+            const int64_t ic = ipos[own_cols[oc]];
+            f += T[ic + (int64_t)j * m] * U[ic + (int64_t)j * m];
+        }
+        e_out[j] = w[j];
+        fe_out[j] = f;
+    }
+}
+
+// Z(j, t) = occ_j U(ic_t, j) for the owned columns t of one large submatrix.
+__global__ void k_occ_rows(int m, const double* __restrict__ U, const double* __restrict__ w, double mu,
+                           const int* __restrict__ own_cols, int64_t o0, int64_t nown, const int* __restrict__ ipos,
+                           double* __restrict__ Z) {
+    for (int64_t t = blockIdx.y; t < nown; t += gridDim.y) {
+        const int64_t ic = ipos[own_cols[o0 + t]];
+        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+            const double ev = w[j];
+            const double occ = ev < mu ? 2.0 : (ev == mu ? 1.0 : 0.0);
+            Z[j + t * (int64_t)m] = occ * U[ic + (int64_t)j * m];
+        }
+    }
+}
+
+// Scatter P_k(:, owned) (m x nown, column-major) into the packed result.
+__global__ void k_scatter_cols(int m, const double* __restrict__ Pc, const int* __restrict__ mp,
+                               const int* __restrict__ own_cols, int64_t o0, int64_t nown, double* __restrict__ Ppk) {
+    for (int64_t t = blockIdx.y; t < nown; t += gridDim.y) {
+        const int64_t c = own_cols[o0 + t];
+        double* col = Ppk + c * (c + 1) / 2;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+            const int64_t gi = mp[i];
+            if (gi <= c) col[gi] = Pc[i + t * (int64_t)m];
+        }
+    }
+}
+
+struct MuResult {
+    double mu;
+    double nel;
+    int iters;
+    int converged;
+    double trace_mu[100];
+    double trace_nel[100];
+};
+
+__device__ double block_sum_fixed(double v, double* sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// (6) the mu bisection, one block of 1024 threads, fixed summation order.
+__global__ void k_mu_bisect(int64_t total, const double* __restrict__ e, const double* __restrict__ fe,
+                            double nelref, double tol_mu, double tol_nel, MuResult* out) {
+    __shared__ double sh[1024];
+    double mua = -10.0, mub = 10.0, mu = 0.0, nel = 0.0;
+    bool finaliter = false;
+    int it = 0;
+    for (int muiter = 1; muiter <= 100; ++muiter) {
+        mu = 0.5 * (mua + mub);
+        double part = 0.0;
+        for (int64_t q = threadIdx.x; q < total; q += blockDim.x) {
+            const double ev = e[q];
+            const double occ = ev < mu ? 2.0 : (ev == mu ? 1.0 : 0.0);
+            part += fe[q] * occ;
+        }
+        nel = block_sum_fixed(part, sh);
+        if (finaliter) break;
+        if (threadIdx.x == 0) {
+            out->trace_mu[muiter - 1] = mu;
+            out->trace_nel[muiter - 1] = nel;
+        }
+        it = muiter;
+        if (fabs(mua - mub) < tol_mu || fabs(nel - nelref) < tol_nel) finaliter = true;
+        if (!finaliter) {
+            if (nel > nelref) mub = mu;
+            else mua = mu;
+        }
+    }
+    if (threadIdx.x == 0) {
+        out->mu = mu;
+        out->nel = nel;
+        out->iters = it;
+        out->converged = finaliter ? 1 : 0;
+    }
+}
+
+// (7) P(map(i), c) for owned column c of problem blockIdx.x; threads over i.
+__global__ void k_final(int M, const Prob* __restrict__ probs, const int* __restrict__ maps,
+                        const int64_t* __restrict__ own_off, const int* __restrict__ own_cols,
+                        const int* __restrict__ ipos, const double* __restrict__ Ub, const double* __restrict__ w,
+                        double mu, double* __restrict__ Ppk) {
+    extern __shared__ double wv[];   // occ_j U(ic, j)
+    const Prob p = probs[blockIdx.x];
+    const int* mp = maps + p.moff;
+    const double* U = Ub + (int64_t)blockIdx.x * M * M;
+    const double* ev = w + (int64_t)blockIdx.x * M;
+    for (int64_t oc = own_off[p.k] + blockIdx.y; oc < own_off[p.k + 1]; oc += gridDim.y) {
+        const int64_t c = own_cols[oc];
+        const int ic = ipos[c];
+        __syncthreads();
+        for (int j = threadIdx.x; j < p.m; j += blockDim.x) {
+            const double occ = ev[j] < mu ? 2.0 : (ev[j] == mu ? 1.0 : 0.0);
+            wv[j] = occ * U[ic + (int64_t)j * M];
+        }
+        __syncthreads();
+        double* col = Ppk + c * (c + 1) / 2;
+        for (int i = threadIdx.x; i < p.m; i += blockDim.x) {
+            const int64_t gi = mp[i];
+            if (gi > c) continue;
+            double s = 0.0;
+            for (int j = 0; j < p.m; ++j) s += U[i + (int64_t)j * M] * wv[j];
+            col[gi] = s;
+        }
+    }
+}
+
+// Column grouping, source/sm.f90:92-162 (mode 4 from the supplied partition,
+// column order as source/sm.f90:483-496).
+std::vector<std::vector<int>> group_columns(int64_t ndim, const int64_t* aoat, int64_t nat, int64_t mode,
+                                            const int64_t* partition) {
+    std::vector<std::vector<int>> comb;
+    if (mode == PTBGPU_COLUMNS_SINGLE) {
+        comb.resize(ndim);
+        for (int64_t i = 0; i < ndim; ++i) comb[i] = {(int)i};
+    } else if (mode == PTBGPU_COLUMNS_ATOMS) {
+        comb.push_back({0});
+        for (int64_t i = 1; i < ndim; ++i) {
+            if (aoat[i] == aoat[i - 1]) comb.back().push_back((int)i);
+            else comb.push_back({(int)i});
+        }
+    } else if (mode == PTBGPU_COLUMNS_FULL_MATRIX) {
+        comb.resize(1);
+        comb[0].resize(ndim);
+        std::iota(comb[0].begin(), comb[0].end(), 0);
+    } else if (mode == PTBGPU_COLUMNS_KMEANS) {
+        PTB_CHECK(partition != nullptr && nat > 0, PTBGPU_EINVAL,
+                  "columns mode 4 needs an atom -> cluster partition");
+        int64_t nsm = 0;
+        for (int64_t a = 0; a < nat; ++a) {
+            PTB_CHECK(partition[a] >= 1, PTBGPU_EINVAL, "partition ids are 1-based");
+            nsm = std::max(nsm, partition[a]);
+        }
+        std::vector<std::vector<int>> by_atom(nat + 1);
+        for (int64_t j = 0; j < ndim; ++j) {
+            PTB_CHECK(aoat[j] >= 1 && aoat[j] <= nat, PTBGPU_EINVAL, "aoat out of range");
+            by_atom[aoat[j]].push_back((int)j);
+        }
+        comb.resize(nsm);
+        for (int64_t k = 1; k <= nsm; ++k)
+            for (int64_t a = 1; a <= nat; ++a)
+                if (partition[a - 1] == k) comb[k - 1].insert(comb[k - 1].end(), by_atom[a].begin(), by_atom[a].end());
+        comb.erase(std::remove_if(comb.begin(), comb.end(), [](const std::vector<int>& v) { return v.empty(); }),
+                   comb.end());
+    } else {
+        fail(PTBGPU_ENOTIMPL, "not implemented");
+    }
+    return comb;
+}
+
+template <class T>
+T* upload(ptbgpu_ctx* c, int id, const std::vector<T>& v) {
+    DevBuf& b = c->buf(id);
+    b.reserve(sizeof(T) * std::max<size_t>(v.size(), 1));
+    if (!v.empty())
+        PTB_CUDA(cudaMemcpyAsync(b.ptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, c->stream));
+    return b.as<T>();
+}
+
+}  // namespace
+
+void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* dH, const double* dS, double* dP,
+                       int64_t nat, const double* xyz, const int64_t* aoat, int64_t columns, int64_t mode,
+                       const int64_t* partition, const ptbgpu_opts* o, ptbgpu_stats* st) {
+    (void)xyz;
+    const int prl = o ? (int)o->print_level : 0;
+    const double filter = o ? o->filter : 0.0;
+    if (mode == PTBGPU_SUBMATRIX_SIGN) fail(PTBGPU_ENOTIMPL, "submatrix_mode.eq.1 not implemented");
+    PTB_CHECK(mode == PTBGPU_SUBMATRIX_SYGV, PTBGPU_ENOTIMPL, "not implemented submatrix_mode %lld", (long long)mode);
+    PTB_CHECK(n > 0 && n < (int64_t)1 << 31, PTBGPU_EINVAL, "bad ndim");
+    cudaStream_t s = c->stream;
+    log_line(prl, 1, " Stupid simple implementation of the submatrix method: %lld %lld", (long long)columns,
+             (long long)mode);
+
+    // full, filtered H and S
+    DevBuf& bh = c->buf(B_H);
+    DevBuf& bs = c->buf(B_S);
+    bh.reserve(sizeof(double) * n * n);
+    bs.reserve(sizeof(double) * n * n);
+    double* H = bh.as<double>();
+    double* S = bs.as<double>();
+    unpack_sym(s, n, n, dH, H, filter);
+    unpack_sym(s, n, n, dS, S, filter);
+
+    // (1) grouping
+    std::vector<std::vector<int>> comb = group_columns(n, aoat, nat, columns, partition);
+    const int nsm = (int)comb.size();
+    std::vector<int> owner(n, -1), own_cols;
+    std::vector<int64_t> own_off(nsm + 1, 0);
+    for (int k = 0; k < nsm; ++k) {
+        own_off[k + 1] = own_off[k] + (int64_t)comb[k].size();
+        for (int col : comb[k]) {
+            owner[col] = k;
+            own_cols.push_back(col);
+        }
+    }
+    int* d_owner = upload(c, B_SM0, owner);
+    int* d_own_cols = upload(c, B_SM1, own_cols);
+    int64_t* d_own_off = upload(c, B_SM2, own_off);
+
+    // (2) pattern scan
+    DevBuf& bf = c->buf(B_SM3);
+    bf.reserve((size_t)nsm * n);
+    PTB_CUDA(cudaMemsetAsync(bf.ptr, 0, (size_t)nsm * n, s));
+    k_pattern<<<(int)std::min<int64_t>(n, 148 * 8), 256, 0, s>>>(n, H, S, d_owner, bf.as<uint8_t>());
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+    DevBuf& bc = c->buf(B_SM4);
+    bc.reserve(sizeof(int) * nsm);
+    k_count<<<nsm, 256, 0, s>>>(n, bf.as<uint8_t>(), bc.as<int>());
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+    std::vector<int> counts(nsm);
+    PTB_CUDA(cudaMemcpyAsync(counts.data(), bc.ptr, sizeof(int) * nsm, cudaMemcpyDeviceToHost, s));
+    PTB_CUDA(cudaStreamSynchronize(s));
+    std::vector<int64_t> moff(nsm + 1, 0);
+    for (int k = 0; k < nsm; ++k) moff[k + 1] = moff[k] + counts[k];
+    int64_t* d_moff = upload(c, B_SM5, moff);
+    DevBuf& bm = c->buf(B_SM6);
+    bm.reserve(sizeof(int) * std::max<int64_t>(moff[nsm], 1));
+    DevBuf& bip = c->buf(B_SM7);
+    bip.reserve(sizeof(int) * n);
+    k_fill<<<nsm, 256, 0, s>>>(n, bf.as<uint8_t>(), d_moff, d_owner, bm.as<int>(), bip.as<int>());
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+    const int* d_maps = bm.as<int>();
+    const int* d_ipos = bip.as<int>();
+
+    int64_t sumdims = moff[nsm];
+    int maxdim = *std::max_element(counts.begin(), counts.end());
+    double effort_full = std::pow((double)n, 2.5), effort_sms = 0.0;
+    for (int k = 0; k < nsm; ++k) effort_sms += std::pow((double)counts[k], 2.5);
+    log_line(prl, 1, " number of submatrices= %d", nsm);
+    log_line(prl, 1, " average sm dim= %lld", (long long)(sumdims / nsm));
+    log_line(prl, 1, " effort for full matrix ops= %g", effort_full);
+    log_line(prl, 1, " sums of efforts for submatrices= %g", effort_sms);
+    log_line(prl, 1, " ratio %g", effort_sms / effort_full);
+
+    // (4) buckets by padded size; submatrices above kBatchMax take the large path
+    constexpr int kBatchMax = 1024;
+    std::map<int, std::vector<Prob>> buckets;
+    std::vector<Prob> large;
+    int64_t eoff = 0;
+    for (int k = 0; k < nsm; ++k) {
+        Prob p{k, counts[k], moff[k], eoff};
+        eoff += counts[k];
+        if (counts[k] > kBatchMax) large.push_back(p);
+        else buckets[(int)round_up(counts[k], 32)].push_back(p);
+    }
+    const int64_t total = eoff;
+    DevBuf& be = c->buf(B_MISC0);
+    DevBuf& bfe = c->buf(B_MISC1);
+    be.reserve(sizeof(double) * total);
+    bfe.reserve(sizeof(double) * total);
+
+    struct Bucket {
+        int M = 0, count = 0;
+        bool is_large = false;
+        Prob single{};
+        DevBuf probs, U, w;
+    };
+    std::vector<Bucket> bks(buckets.size() + large.size());
+    DevBuf sb, ptrs, infos, ws, tbuf;
+    double flops = 0.0;
+    cusolverDnParams_t params;
+    PTB_CUSOLVER(cusolverDnCreateParams(&params));
+    auto cleanup = [&] {
+        cusolverDnDestroyParams(params);
+        for (Bucket& bk : bks) {
+            bk.probs.release();
+            bk.U.release();
+            bk.w.release();
+        }
+        sb.release();
+        ptrs.release();
+        infos.release();
+        ws.release();
+        tbuf.release();
+    };
+    static bool fe_attr = false;
+    if (!fe_attr) {
+        PTB_CUDA(cudaFuncSetAttribute(k_fe, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        PTB_CUDA(cudaFuncSetAttribute(k_final, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        fe_attr = true;
+    }
+    const double one = 1.0, zero = 0.0;
+    try {
+        size_t bi = 0;
+        for (auto& kv : buckets) {
+            const int M = kv.first;
+            std::vector<Prob>& pv = kv.second;
+            const int B = (int)pv.size();
+            Bucket& bk = bks[bi++];
+            bk.M = M;
+            bk.count = B;
+            bk.probs.reserve(sizeof(Prob) * B);
+            PTB_CUDA(cudaMemcpyAsync(bk.probs.ptr, pv.data(), sizeof(Prob) * B, cudaMemcpyHostToDevice, s));
+            bk.U.reserve(sizeof(double) * (size_t)B * M * M);
+            bk.w.reserve(sizeof(double) * (size_t)B * M);
+            sb.reserve(sizeof(double) * (size_t)B * M * M);
+            double* Hb = bk.U.as<double>();
+            double* Sb = sb.as<double>();
+            dim3 gg((M + 31) / 32, (unsigned)std::max(1, std::min(M / 8, 64)), B);
+            k_gather<<<gg, dim3(32, 8), 0, s>>>(M, bk.probs.as<Prob>(), d_maps, n, H, S, Hb, Sb);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            std::vector<double*> hp(2 * (size_t)B);
+            for (int q = 0; q < B; ++q) {
+                hp[q] = Sb + (size_t)q * M * M;
+                hp[B + q] = Hb + (size_t)q * M * M;
+            }
+            ptrs.reserve(sizeof(double*) * hp.size());
+            PTB_CUDA(cudaMemcpyAsync(ptrs.ptr, hp.data(), sizeof(double*) * hp.size(), cudaMemcpyHostToDevice, s));
+            infos.reserve(sizeof(int) * B);
+            double** dS_arr = ptrs.as<double*>();
+            double** dH_arr = dS_arr + B;
+            PTB_CUSOLVER(cusolverDnDpotrfBatched(c->solver, CUBLAS_FILL_MODE_LOWER, M, dS_arr, M, infos.as<int>(), B));
+            std::vector<int> hinfo(B);
+            PTB_CUDA(cudaMemcpyAsync(hinfo.data(), infos.ptr, sizeof(int) * B, cudaMemcpyDeviceToHost, s));
+            PTB_CUDA(cudaStreamSynchronize(s));
+            for (int q = 0; q < B; ++q)
+                PTB_CHECK(hinfo[q] == 0, PTBGPU_ENOTSPD, "overlap submatrix %d not positive definite (info=%d)",
+                          pv[q].k + 1, hinfo[q]);
+            PTB_CUBLAS(cublasDtrsmBatched(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                                          CUBLAS_DIAG_NON_UNIT, M, M, &one, dS_arr, M, dH_arr, M, B));
+            PTB_CUBLAS(cublasDtrsmBatched(c->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                                          CUBLAS_DIAG_NON_UNIT, M, M, &one, dS_arr, M, dH_arr, M, B));
+            size_t wsd = 0, wsh = 0;
+            cusolverStatus_t bst = cusolverDnXsyevBatched_bufferSize(
+                c->solver, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, M, CUDA_R_64F, Hb, M,
+                CUDA_R_64F, bk.w.ptr, CUDA_R_64F, &wsd, &wsh, B);
+            if (bst == CUSOLVER_STATUS_SUCCESS) {
+                ws.reserve(std::max<size_t>(wsd, 16));
+                std::vector<char> hws(std::max<size_t>(wsh, 16));
+                bst = cusolverDnXsyevBatched(c->solver, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, M,
+                                             CUDA_R_64F, Hb, M, CUDA_R_64F, bk.w.ptr, CUDA_R_64F, ws.ptr, wsd,
+                                             hws.data(), wsh, infos.as<int>(), B);
+                PTB_CUDA(cudaStreamSynchronize(s));
+            }
+            if (bst != CUSOLVER_STATUS_SUCCESS) {
+                // per-matrix eigensolves of the reduced problems (same layout)
+                for (int q = 0; q < B; ++q) {
+                    dsyevd(c, M, M, Hb + (size_t)q * M * M, bk.w.as<double>() + (size_t)q * M);
+                }
+                PTB_CUDA(cudaMemsetAsync(infos.ptr, 0, sizeof(int) * B, s));
+            }
+            PTB_CUDA(cudaMemcpyAsync(hinfo.data(), infos.ptr, sizeof(int) * B, cudaMemcpyDeviceToHost, s));
+            PTB_CUDA(cudaStreamSynchronize(s));
+            for (int q = 0; q < B; ++q)
+                PTB_CHECK(hinfo[q] == 0, PTBGPU_EITER, "eigensolver failed on submatrix %d (info=%d)", pv[q].k + 1,
+                          hinfo[q]);
+            PTB_CUBLAS(cublasDtrsmBatched(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                                          CUBLAS_DIAG_NON_UNIT, M, M, &one, dS_arr, M, dH_arr, M, B));
+            k_fe<<<B, 256, sizeof(double) * (FE_CH + 1) * M, s>>>(M, bk.probs.as<Prob>(), d_maps, d_own_off,
+                                                                  d_own_cols, d_ipos, n, S, Hb, bk.w.as<double>(),
+                                                                  be.as<double>(), bfe.as<double>());
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            for (const Prob& p : pv) flops += 9.0 * std::pow((double)p.m, 3);
+        }
+        // large submatrices: one generalized eigensolve each (dsygvd), fe from T = S_k U
+        for (const Prob& p : large) {
+            Bucket& bk = bks[bi++];
+            bk.is_large = true;
+            bk.single = p;
+            const int m = p.m;
+            bk.M = m;
+            bk.count = 1;
+            bk.probs.reserve(sizeof(Prob));
+            PTB_CUDA(cudaMemcpyAsync(bk.probs.ptr, &p, sizeof(Prob), cudaMemcpyHostToDevice, s));
+            bk.U.reserve(sizeof(double) * (size_t)m * m);
+            bk.w.reserve(sizeof(double) * (size_t)m);
+            sb.reserve(sizeof(double) * (size_t)m * m);
+            tbuf.reserve(sizeof(double) * (size_t)m * m);
+            double* U = bk.U.as<double>();
+            double* Sk = sb.as<double>();
+            dim3 gg((m + 31) / 32, 64, 1);
+            k_gather<<<gg, dim3(32, 8), 0, s>>>(m, bk.probs.as<Prob>(), d_maps, n, H, S, U, Sk);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            const int info = dsygvd(c, m, m, U, Sk, bk.w.as<double>());
+            PTB_CHECK(info == 0, PTBGPU_ENOTSPD, "dsygvd failed on submatrix %d (info=%d)", p.k + 1, info);
+            k_gather<<<gg, dim3(32, 8), 0, s>>>(m, bk.probs.as<Prob>(), d_maps, n, H, S, tbuf.as<double>(), Sk);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &one, Sk, m, U, m, &zero,
+                                   tbuf.as<double>(), m));
+            k_fe_large<<<(m + 255) / 256, 256, 0, s>>>(m, tbuf.as<double>(), U, d_own_cols, own_off[p.k],
+                                                       own_off[p.k + 1], d_ipos, bk.w.as<double>(),
+                                                       be.as<double>() + p.eoff, bfe.as<double>() + p.eoff);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            flops += 9.0 * std::pow((double)m, 3);
+        }
+
+        // (6) mu bisection
+        DevBuf bmu;
+        bmu.reserve(sizeof(MuResult));
+        const double tol_mu = (double)1e-3f, tol_nel = (double)1e-5f;
+        k_mu_bisect<<<1, 1024, 0, s>>>(total, be.as<double>(), bfe.as<double>(), (double)nelref, tol_mu, tol_nel,
+                                       bmu.as<MuResult>());
+        count_launch();
+        PTB_CUDA(cudaGetLastError());
+        MuResult mr;
+        PTB_CUDA(cudaMemcpyAsync(&mr, bmu.ptr, sizeof(MuResult), cudaMemcpyDeviceToHost, s));
+        PTB_CUDA(cudaStreamSynchronize(s));
+        bmu.release();
+        for (int it = 0; it < mr.iters; ++it)
+            log_line(prl, 1, " muiter %d mu %.15g %.15g of %lld", it + 1, mr.trace_mu[it], mr.trace_nel[it],
+                     (long long)nelref);
+        PTB_CHECK(mr.converged, PTBGPU_EITER, "chemical potential bisection did not converge");
+        log_line(prl, 1, " iteration of chemical potential converged");
+
+        // (7) final density into the packed result
+        PTB_CUDA(cudaMemsetAsync(dP, 0, sizeof(double) * (size_t)npacked(n), s));
+        for (Bucket& bk : bks) {
+            if (!bk.is_large) {
+                dim3 g(bk.count, 4);
+                k_final<<<g, 256, sizeof(double) * bk.M, s>>>(bk.M, bk.probs.as<Prob>(), d_maps, d_own_off,
+                                                             d_own_cols, d_ipos, bk.U.as<double>(), bk.w.as<double>(),
+                                                             mr.mu, dP);
+                count_launch();
+                PTB_CUDA(cudaGetLastError());
+                continue;
+            }
+            const Prob& p = bk.single;
+            const int m = p.m;
+            const int64_t o0 = own_off[p.k], nown = own_off[p.k + 1] - o0;
+            tbuf.reserve(sizeof(double) * (size_t)m * nown * 2);
+            double* Z = tbuf.as<double>();
+            double* Pc = Z + (size_t)m * nown;
+            dim3 g((m + 255) / 256, (unsigned)std::min<int64_t>(nown, 65535));
+            k_occ_rows<<<g, 256, 0, s>>>(m, bk.U.as<double>(), bk.w.as<double>(), mr.mu, d_own_cols, o0, nown, d_ipos,
+                                        Z);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, (int)nown, m, &one, bk.U.as<double>(), m, Z,
+                                   m, &zero, Pc, m));
+            k_scatter_cols<<<g, 256, 0, s>>>(m, Pc, d_maps + p.moff, d_own_cols, o0, nown, dP);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+        }
+        PTB_CUDA(cudaStreamSynchronize(s));
+        if (st) {
+            st->mu = mr.mu;
+            st->nel = mr.nel;
+            st->mu_iterations = mr.iters;
+            st->nsm = nsm;
+            st->sum_dims = sumdims;
+            st->max_dim = maxdim;
+            st->flops += flops;
+        }
+    } catch (...) {
+        cleanup();
+        throw;
+    }
+    cleanup();
+}
+
+}  // namespace ptb

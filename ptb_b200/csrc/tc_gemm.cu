@@ -1,0 +1,446 @@
+// tcgen05 tensor-core products for the trace-correcting purification.
+//
+// C = sum_p A_{a(p)} * B_{b(p)}^T over a short list of bf16 operand planes,
+// accumulated in FP32 in tensor memory.  With planes {X_hi, X_lo} and the
+// products (hi,hi) + (hi,lo) + (lo,hi) this is the "bf16x3" split product of
+// an FP32 matrix (about 16 significant bits per operand; the dropped lo*lo
+// term is 2^-16 relative).
+//
+// One CTA computes a 128 x 256 tile (cta_group::1, UMMA 128x256x16):
+//   warp 0      TMA producer: per 64-wide K block, 2 A tiles (128x64) and 2 B
+//               tiles (256x64) into a 2-stage ring, 128B-swizzled, completion
+//               on a "full" mbarrier with a transaction count;
+//   warp 1      MMA issuer (one thread): 4 K16 steps x 3 products per stage,
+//               tcgen05.commit releases the stage on its "empty" mbarrier;
+//   warp 2      allocates / frees the 256 TMEM columns of the accumulator;
+//   warps 4..7  epilogue: tcgen05.ld of their 32 lanes (rows), fused update.
+//
+// Epilogues:
+//   EPI_FULL  every tile; C written row-major as FP32 (general product).
+//   EPI_SP2   symmetric X*X: only tiles touching the upper triangle run; the
+//             element (r,c), c >= r, becomes X' = C (branch "square") or
+//             2X - C, written to (r,c) and (c,r) as FP32 and as the bf16 hi/lo
+//             planes of the next product; per-tile trace and sum of squares
+//             (= tr X'^2 for symmetric X') go to a stats array that the
+//             decision kernel reduces in a fixed order (deterministic).
+//
+// Every mbarrier wait is bounded (2 s of globaltimer); on expiry the CTA sets
+// an error word, drains the copies it issued and frees its TMEM.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "common.cuh"
+#include "tc_gemm.cuh"
+
+namespace ptb {
+namespace tc {
+
+namespace {
+
+constexpr int BM = 128;
+constexpr int BN = 256;
+constexpr int KB = 64;                        // K elements per stage (128 bytes of bf16)
+constexpr int STAGES = 2;
+constexpr int NPLANE = 2;                     // A planes and B planes per stage
+constexpr int A_TILE_BYTES = BM * KB * 2;     // 16 KB
+constexpr int B_TILE_BYTES = BN * KB * 2;     // 32 KB
+constexpr int STAGE_BYTES = NPLANE * (A_TILE_BYTES + B_TILE_BYTES);
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int THREADS = 256;
+constexpr uint64_t kTimeoutNs = 2000000000ull;
+
+// ---- PTX wrappers ---------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait: true when the phase of the given parity completed.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = gtimer();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (gtimer() - t0 > kTimeoutNs) return false;
+    }
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0,
+                                            int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1)
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+          "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+          "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// UMMA shared-memory descriptor, K-major operand in the 128B-swizzle canonical
+// layout: rows of 128 bytes, 8-row (1024 B) swizzle atoms, SBO = 1024 B,
+// LBO unused (16 B), descriptor version 1, layout type 2 (SWIZZLE_128B).
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1u << 16;
+    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)2u << 61;
+    return d;
+}
+// Instruction descriptor for kind::f16: D fp32, A/B bf16, both K-major, M=128, N=BN.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                            ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void set_err(int* err, int site) {
+    if (err) atomicCAS(err, 0, site);
+}
+
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& h, __nv_bfloat16& l) {
+    h = __float2bfloat16_rn(v);
+    l = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+// ---- the kernel -----------------------------------------------------------
+template <int EPI>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_tc_product(const __grid_constant__ TmaPlanes maps, const ProdList prods, const int2* __restrict__ tiles,
+                 int nk, EpiParams ep) {
+    if (ep.active && *ep.active == 0) return;   // uniform early exit (converged iteration)
+
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t base_raw = smem_u32(smem_raw);
+    const uint32_t base = (base_raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - base_raw);
+    const uint32_t bar0 = base + STAGES * STAGE_BYTES;
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+    const uint32_t accum_bar = bar0 + 8u * (2 * STAGES);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + STAGES * STAGE_BYTES + 8 * (2 * STAGES + 1));
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+    double* red = reinterpret_cast<double*>(gbase + STAGES * STAGE_BYTES + 128);   // 8 doubles
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int2 tile = tiles[blockIdx.x];
+    const int bi = tile.x, bj = tile.y;
+
+    auto a_tile = [&](int s, int p) { return base + s * STAGE_BYTES + p * A_TILE_BYTES; };
+    auto b_tile = [&](int s, int p) {
+        return base + s * STAGE_BYTES + NPLANE * A_TILE_BYTES + p * B_TILE_BYTES;
+    };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(accum_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"((uint32_t)BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer ----------------
+        int issued_phase[STAGES];
+        for (int s = 0; s < STAGES; ++s) issued_phase[s] = -1;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % STAGES, round = kb / STAGES;
+            if (round > 0 && !mbar_wait(empty_bar(s), (round - 1) & 1)) {
+                set_err(ep.err, 11);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            mbar_expect_tx(full_bar(s), STAGE_BYTES);
+            for (int p = 0; p < NPLANE; ++p)
+                tma_load_2d(a_tile(s, p), &maps.a[p], full_bar(s), kb * KB, bi * BM);
+            for (int p = 0; p < NPLANE; ++p)
+                tma_load_2d(b_tile(s, p), &maps.b[p], full_bar(s), kb * KB, bj * BN);
+            issued_phase[s] = round & 1;
+        }
+        // drain: every copy this thread issued has landed before the CTA may exit
+        for (int s = 0; s < STAGES; ++s)
+            if (issued_phase[s] >= 0 && !mbar_wait(full_bar(s), (uint32_t)issued_phase[s])) set_err(ep.err, 12);
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer ----------------
+        bool ok = true;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % STAGES, round = kb / STAGES;
+            if (!mbar_wait(full_bar(s), round & 1)) {
+                set_err(ep.err, 21);
+                *(volatile int*)abort_flag = 1;
+                ok = false;
+                break;
+            }
+            if (*(volatile int*)abort_flag) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+#pragma unroll
+            for (int k = 0; k < KB / 16; ++k) {
+                for (int p = 0; p < prods.n; ++p) {
+                    const uint64_t ad = sdesc_sw128(a_tile(s, prods.a[p]) + k * 32);
+                    const uint64_t bd = sdesc_sw128(b_tile(s, prods.b[p]) + k * 32);
+                    umma_bf16(tmem, ad, bd, kIdesc, (kb | k | p) != 0);
+                }
+            }
+            umma_commit(empty_bar(s));
+        }
+        umma_commit(accum_bar);   // also issued on abort so the wait below ends
+        if (!ok) mbar_wait(accum_bar, 0);
+    } else if (warp >= 4) {
+        // ---------------- epilogue ----------------
+        const int q = warp - 4;                   // TMEM lane quarter
+        const int64_t ld = ep.ld;
+        const int64_t r = (int64_t)bi * BM + q * 32 + lane;
+        double tr = 0.0, ss = 0.0;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(accum_bar, 0));
+        if (!ok && lane == 0) {
+            set_err(ep.err, 31);
+            *(volatile int*)abort_flag = 1;
+        }
+        const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
+        tc_fence_after();
+        if (ok && !aborted) {
+            const bool square = (EPI == EPI_SP2) ? (*ep.sq_flag != 0) : true;
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                uint32_t v[32];
+                __syncwarp();   // lanes may have taken different paths in the previous chunk
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
+                const int64_t cbase = (int64_t)bj * BN + c0;
+                if (EPI == EPI_FULL) {
+                    float4* dst = reinterpret_cast<float4*>(ep.out + r * ld + cbase);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                        dst[j] = make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
+                                             __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]));
+                    continue;
+                }
+                if (cbase + 31 < r) continue;       // chunk entirely below the diagonal
+                if (cbase >= r) {
+                    // whole chunk in the upper triangle: vector path
+                    const float4* xin = reinterpret_cast<const float4*>(ep.xcur + r * ld + cbase);
+                    float4* xo = reinterpret_cast<float4*>(ep.out + r * ld + cbase);
+                    uint4* ho = reinterpret_cast<uint4*>(ep.hi + r * ld + cbase);
+                    uint4* lo = reinterpret_cast<uint4*>(ep.lo + r * ld + cbase);
+#pragma unroll
+                    for (int j8 = 0; j8 < 4; ++j8) {
+                        float val[8];
+                        const float4 x0 = xin[2 * j8], x1 = xin[2 * j8 + 1];
+                        const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+                        __align__(16) __nv_bfloat16 hh[8], ll[8];
+#pragma unroll
+                        for (int t = 0; t < 8; ++t) {
+                            const float cv = __uint_as_float(v[8 * j8 + t]);
+                            val[t] = square ? cv : 2.0f * xs[t] - cv;
+                            split_bf16(val[t], hh[t], ll[t]);
+                            const int64_t c = cbase + 8 * j8 + t;
+                            const double dv = (double)val[t];
+                            if (c == r) {
+                                tr += dv;
+                                ss += dv * dv;
+                            } else {
+                                ss += 2.0 * dv * dv;
+                                ep.out[c * ld + r] = val[t];
+                                ep.hi[c * ld + r] = hh[t];
+                                ep.lo[c * ld + r] = ll[t];
+                            }
+                        }
+                        xo[2 * j8] = make_float4(val[0], val[1], val[2], val[3]);
+                        xo[2 * j8 + 1] = make_float4(val[4], val[5], val[6], val[7]);
+                        ho[j8] = *reinterpret_cast<const uint4*>(hh);
+                        lo[j8] = *reinterpret_cast<const uint4*>(ll);
+                    }
+                } else {
+                    // chunk straddles the diagonal: scalar path, c >= r only
+#pragma unroll 4
+                    for (int j = 0; j < 32; ++j) {
+                        const int64_t c = cbase + j;
+                        if (c < r) continue;
+                        const float cv = __uint_as_float(v[j]);
+                        const float val = square ? cv : 2.0f * ep.xcur[r * ld + c] - cv;
+                        __nv_bfloat16 h, l;
+                        split_bf16(val, h, l);
+                        const double dv = (double)val;
+                        ep.out[r * ld + c] = val;
+                        ep.hi[r * ld + c] = h;
+                        ep.lo[r * ld + c] = l;
+                        if (c == r) {
+                            tr += dv;
+                            ss += dv * dv;
+                        } else {
+                            ss += 2.0 * dv * dv;
+                            ep.out[c * ld + r] = val;
+                            ep.hi[c * ld + r] = h;
+                            ep.lo[c * ld + r] = l;
+                        }
+                    }
+                }
+            }
+        }
+        if (EPI == EPI_SP2) {
+            for (int o = 16; o > 0; o >>= 1) {
+                tr += __shfl_xor_sync(0xffffffffu, tr, o);
+                ss += __shfl_xor_sync(0xffffffffu, ss, o);
+            }
+            if (lane == 0) {
+                red[2 * q] = tr;
+                red[2 * q + 1] = ss;
+            }
+            asm volatile("bar.sync 1, 128;" ::: "memory");   // epilogue warps only
+            if (q == 0 && lane == 0) {
+                ep.stats[2 * blockIdx.x] = red[0] + red[2] + red[4] + red[6];
+                ep.stats[2 * blockIdx.x + 1] = red[1] + red[3] + red[5] + red[7];
+            }
+        }
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 2) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN));
+    }
+}
+
+// ---- host side ------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    PTB_CHECK(fn != nullptr, PTBGPU_ECUDA, "cuTensorMapEncodeTiled unavailable");
+    return fn;
+}
+
+void encode_plane(CUtensorMap* map, const void* plane, int64_t ld, int box_rows) {
+    PTB_CHECK(((uintptr_t)plane & 15) == 0, PTBGPU_EINVAL, "operand plane not 16-byte aligned");
+    PTB_CHECK(ld % 256 == 0, PTBGPU_EINVAL, "operand leading dimension must be a multiple of 256");
+    cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)ld};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    cuuint32_t box[2] = {(cuuint32_t)KB, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = get_encode()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(plane), dims,
+                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    PTB_CHECK(r == CUDA_SUCCESS, PTBGPU_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+}
+
+}  // namespace
+
+int tile_n() { return BN; }
+
+// Tile lists: row blocks of 128, column blocks of 256, grouped by 16 row
+// blocks so that consecutive CTAs share operand panels in L2.
+std::vector<int2> make_tiles(long long ld, bool upper_only) {
+    const int nbi = (int)(ld / BM), nbj = (int)(ld / BN);
+    std::vector<int2> t;
+    const int G = 16;
+    for (int g0 = 0; g0 < nbi; g0 += G)
+        for (int bj = 0; bj < nbj; ++bj)
+            for (int bi = g0; bi < std::min(nbi, g0 + G); ++bi)
+                if (!upper_only || (int64_t)bj * BN + BN - 1 >= (int64_t)bi * BM) t.push_back(make_int2(bi, bj));
+    return t;
+}
+
+void launch_product(cudaStream_t s, int epi, long long ld, const void* a0, const void* a1, const void* b0,
+                    const void* b1, const ProdList& prods, const int2* tiles_dev, int ntiles,
+                    const EpiParams& ep) {
+    static bool attr_set[2] = {false, false};
+    TmaPlanes maps;
+    encode_plane(&maps.a[0], a0, ld, BM);
+    encode_plane(&maps.a[1], a1, ld, BM);
+    encode_plane(&maps.b[0], b0, ld, BN);
+    encode_plane(&maps.b[1], b1, ld, BN);
+    const int nk = (int)(ld / KB);
+    if (epi == EPI_SP2) {
+        if (!attr_set[1]) {
+            PTB_CUDA(cudaFuncSetAttribute(k_tc_product<EPI_SP2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          SMEM_BYTES));
+            attr_set[1] = true;
+        }
+        k_tc_product<EPI_SP2><<<ntiles, THREADS, SMEM_BYTES, s>>>(maps, prods, tiles_dev, nk, ep);
+        count_launch();
+    } else {
+        if (!attr_set[0]) {
+            PTB_CUDA(cudaFuncSetAttribute(k_tc_product<EPI_FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          SMEM_BYTES));
+            attr_set[0] = true;
+        }
+        k_tc_product<EPI_FULL><<<ntiles, THREADS, SMEM_BYTES, s>>>(maps, prods, tiles_dev, nk, ep);
+        count_launch();
+    }
+    PTB_CUDA(cudaGetLastError());
+}
+
+}  // namespace tc
+}  // namespace ptb

@@ -1,0 +1,112 @@
+"""tPurificationSet mirror and the .PUR settings parser.
+
+Follows source/purification_settings.f90:6-218: the same mode codes and
+defaults, the same ``key = value`` / bare-flag grammar, the same errors on
+invalid values, and the same quirk that ``chempot_increment`` is truncated by
+``int()`` (source/purification_settings.f90:193-195).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+FULL, SUBMATRIX = 1, 2
+SINGLE_COLUMNS, ATOMS_COLUMNS, FULL_MATRIX, KMEANS_R_HEURISTIC = 1, 2, 3, 4
+SUBMATRIX_SIGN, SUBMATRIX_SYGV = 1, 2
+MCWEENY, SIGN_ITER_PADE, SIGN_ITER_NEWTON, SIGN_DIAGONALIZATION = 1, 2, 3, 4
+INV, INV_SQRT, SQRT_ = 1, 2, 3
+
+_MODE = {"full": FULL, "submatrix": SUBMATRIX}
+_COLUMNS = {"single_columns": SINGLE_COLUMNS, "atoms_columns": ATOMS_COLUMNS,
+            "full_matrix": FULL_MATRIX, "kmeans_r_heuristic": KMEANS_R_HEURISTIC}
+_SMMODE = {"submatrix_sign": SUBMATRIX_SIGN, "submatrix_sygv": SUBMATRIX_SYGV}
+_TYPE = {"mcweeny": MCWEENY, "pade": SIGN_ITER_PADE, "newton": SIGN_ITER_NEWTON,
+         "diag": SIGN_DIAGONALIZATION}
+_METRIC = {"inverse": INV, "inverse_sqrt": INV_SQRT, "sqrt": SQRT_}
+
+
+class PurSettingsError(ValueError):
+    pass
+
+
+@dataclass
+class PurificationSettings:
+    mode: int = FULL
+    type: int = SIGN_DIAGONALIZATION
+    cycles: int = 40
+    prlvl: int = 1
+    dev: bool = True
+    check: bool = False
+    nel: int = 0
+    submatrix_mode: int = SUBMATRIX_SYGV
+    submatrix_columns: int = ATOMS_COLUMNS
+    metric_type: int = INV_SQRT
+    metric_cycles: int = 50
+    metric_iterative: bool = False
+    chempot_cycles: int = 60
+    chempot_guess: float = -1.5
+    chempot_increment: float = 0.1
+
+    def to_c(self, struct_type):
+        return struct_type(self.mode, self.type, self.cycles, self.prlvl, self.nel, self.submatrix_mode,
+                           self.submatrix_columns, self.metric_type, self.metric_cycles,
+                           int(self.metric_iterative), self.chempot_cycles, self.chempot_guess,
+                           self.chempot_increment)
+
+    # initialize_purification, source/purification_settings.f90:91-218
+    def read(self, text: str) -> "PurificationSettings":
+        for raw in text.splitlines():
+            toks = raw.split()
+            if not toks:
+                continue
+            arg1 = toks[0]
+            if arg1.startswith("!"):
+                continue
+            if len(toks) >= 2 and toks[1] == "=":
+                arg3 = toks[2] if len(toks) > 2 else ""
+                num = _first_float(toks[2:])
+                if arg1 == "mode":
+                    self.mode = _pick(_MODE, arg3, "Error: .PUR contains invalid type definition")
+                elif arg1 == "submatrix_columns":
+                    self.submatrix_columns = _pick(_COLUMNS, arg3, "Error: .PUR contains invalid type definition")
+                elif arg1 == "submatrix_mode":
+                    self.submatrix_mode = _pick(_SMMODE, arg3, "Error: .PUR contains invalid type definition")
+                elif arg1 == "type":
+                    self.type = _pick(_TYPE, arg3, "Error: .PUR contains invalid type definition")
+                elif arg1 == "metric":
+                    self.metric_type = _pick(_METRIC, arg3, "Error: .PUR contains invalid metric definition.")
+                elif arg1 == "cycles" and num is not None:
+                    self.cycles = int(num)
+                elif arg1 == "chempot_cycles" and num is not None:
+                    self.chempot_cycles = int(num)
+                elif arg1 == "chempot_increment" and num is not None:
+                    self.chempot_increment = float(int(num))
+                elif arg1 == "pr" and num is not None:
+                    self.prlvl = int(num)
+            else:
+                if arg1 == "dev":
+                    self.dev = True
+                elif arg1 == "check":
+                    self.check = True
+                elif arg1 == "iterative_inversion":
+                    self.metric_iterative = True
+        return self
+
+    @classmethod
+    def from_file(cls, path) -> "PurificationSettings":
+        with open(path) as f:
+            return cls().read(f.read())
+
+
+def _pick(table, key, msg):
+    if key not in table:
+        raise PurSettingsError(msg)
+    return table[key]
+
+
+def _first_float(toks):
+    for t in toks:
+        try:
+            return float(t.replace("d", "e").replace("D", "e"))
+        except ValueError:
+            continue
+    return None
