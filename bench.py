@@ -314,6 +314,10 @@ def main():
         rank = int(os.environ.get("RANK", "0"))
         run_reference(args, rank)
         return
+    # libptbgpu first: its cuBLAS / cuSOLVER dependencies then resolve to the CUDA
+    # toolkit it was built against rather than to the copies bundled with torch.
+    from ptb_b200 import load_library
+    load_library()
     rank, world, local, pg = dist_setup(args.gpus)
     try:
         run_ours(args, rank, world, local, pg)

@@ -205,6 +205,21 @@ __global__ void k_f2d(int64_t n, int64_t ldp, const float* __restrict__ x, doubl
         }
 }
 
+// Per-block partial traces of an FP32 plane (64 blocks, fixed order).
+__global__ void k_trace_f32(int64_t n, int64_t ldp, const float* __restrict__ x, double* __restrict__ out) {
+    __shared__ double sh[256];
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += (double)x[i + i * ldp];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+
 // C = W - W^T (column-major FP64), 32x32 tiles.  blockDim = (32, 8).
 __global__ void k_antisym(int64_t n, const double* __restrict__ W, double* __restrict__ C) {
     __shared__ double t[32][33];
@@ -344,7 +359,8 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     const size_t other = 6 * fplane + 4 * plane + (size_t)(64 << 20);
     int slots = (int)std::min<int64_t>(maxit + 1, kMaxIt + 1);
     if (free_b > other) slots = (int)std::min<size_t>(slots, (free_b - other) * 6 / 10 / (2 * plane));
-    PTB_CHECK(slots >= 8, PTBGPU_ENOMEM, "not enough device memory for the purification trajectory");
+    PTB_CHECK(slots >= std::min(8, maxit + 1), PTBGPU_ENOMEM,
+              "not enough device memory for the purification trajectory");
     DevBuf& btraj = c->buf(B_TRAJ);
     btraj.reserve(2 * plane * (size_t)slots);
     auto traj_hi = [&](int k) { return (__nv_bfloat16*)((char*)btraj.ptr + 2 * plane * (size_t)k); };
@@ -503,8 +519,21 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
             count_launch();
             PTB_CUDA(cudaGetLastError());
         }
-        // P_o = P~ + X1_K
-        k_f2d<<<grid1(n), 256, 0, s>>>(n, ldp, x1f[K & 1], 1.0, 1.0, X);
+        // P_o = P~ (1 - tau/N) + X1_K with tau = tr X1_K: the exact first-order
+        // response is traceless; its bf16x3 rounding noise is removed from the
+        // trace in FP64 along P~ (a uniform shift of the occupied eigenvalues by
+        // tau/N), so tr P_o = N to FP64 rounding.
+        DevBuf& btau = c->buf(B_MISC2);
+        btau.reserve(sizeof(double) * 64);
+        k_trace_f32<<<64, 256, 0, s>>>(n, ldp, x1f[K & 1], btau.as<double>());
+        count_launch();
+        PTB_CUDA(cudaGetLastError());
+        double tparts[64];
+        PTB_CUDA(cudaMemcpyAsync(tparts, btau.ptr, sizeof(tparts), cudaMemcpyDeviceToHost, s));
+        PTB_CUDA(cudaStreamSynchronize(s));
+        double tau = 0.0;
+        for (double v : tparts) tau += v;
+        k_f2d<<<grid1(n), 256, 0, s>>>(n, ldp, x1f[K & 1], 1.0, 1.0 - tau / N, X);
         count_launch();
         PTB_CUDA(cudaGetLastError());
         flops += 2.0 * (double)n * n * n /*FP64 commutator*/ + (double)(K + 1) * 3.0 * 2.0 * (double)n * n * n;
