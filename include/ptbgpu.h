@@ -82,6 +82,8 @@ typedef struct {
     double  electronic_temp;    /* solve2 Fermi temperature in K (0 = 300)        */
     double  glob_par15;         /* solve2 orbital-energy shift for mode >= 2      */
     double  glob_par17;
+    int64_t split3_iters;       /* PREC_MIXED: leading iterations whose products use the
+                                   three-plane bf16 split (~24 bits); 0 = all, -1 = none */
 } ptbgpu_opts;
 
 /* What a call reports back (all optional for the caller). */
@@ -117,6 +119,9 @@ int  ptbgpu_finalize(ptbgpu_ctx* ctx);
 int  ptbgpu_last_error(const ptbgpu_ctx* ctx, char* buf, size_t len);
 void ptbgpu_default_settings(ptbgpu_pur_settings* s);   /* type-bound defaults, purification_settings.f90:29-86 */
 void ptbgpu_default_opts(ptbgpu_opts* o);
+/* No counterpart in the reference: device name and the CUDA runtime, driver,
+ * cuBLAS and cuSOLVER versions the context is bound to, as one text line. */
+int  ptbgpu_runtime_info(const ptbgpu_ctx* ctx, char* buf, size_t len);
 
 /* ---- matrix utilities --------------------------------------------------- */
 /* filter_matrix_sym(A, n, filter), source/pgtb.f90:1532-1547: in place on a
@@ -171,6 +176,8 @@ int ptbgpu_solve2(ptbgpu_ctx* ctx, int64_t mode, int64_t ndim, int64_t nel, int6
 /* C = X * X for a symmetric n x n FP64 matrix X (row-major), computed with the
  * bf16x3 tcgen05 kernel (hi/lo split, FP32 accumulation); C is FP32 row-major. */
 int ptbgpu_symsq_bf16x3(ptbgpu_ctx* ctx, int64_t n, const double* X, float* C);
+/* The same with the three-plane split (hi, mid, lo) and six products, ~24-bit operands. */
+int ptbgpu_symsq_bf16x6(ptbgpu_ctx* ctx, int64_t n, const double* X, float* C);
 
 #ifdef __cplusplus
 }

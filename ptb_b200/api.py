@@ -48,7 +48,7 @@ class _Settings(C.Structure):
 class _Opts(C.Structure):
     _fields_ = [("filter", C.c_double), ("precision", C.c_int64), ("print_level", C.c_int64),
                 ("max_iter", C.c_int64), ("electronic_temp", C.c_double), ("glob_par15", C.c_double),
-                ("glob_par17", C.c_double)]
+                ("glob_par17", C.c_double), ("split3_iters", C.c_int64)]
 
 
 class _Stats(C.Structure):
@@ -64,7 +64,7 @@ class _Stats(C.Structure):
 EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_default_settings",
             "ptbgpu_default_opts", "ptbgpu_filter_packed", "ptbgpu_check_density", "ptbgpu_sm_density",
             "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_solve2",
-            "ptbgpu_symsq_bf16x3")
+            "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_runtime_info")
 
 
 def library_path() -> Path:
@@ -79,7 +79,12 @@ def load_library():
     path = library_path()
     if not path.exists():
         raise PtbGpuError(ECUDA, f"{path} not found: build it with `python -m ptb_b200.build`")
-    lib = C.CDLL(str(path))
+    # RTLD_DEEPBIND: the library and the cuBLAS / cuSOLVER it was linked against
+    # resolve their symbols inside their own tree first, so copies of the same
+    # libraries that other packages (torch) load into the global scope are not
+    # mixed into our calls.  Load this module before importing such packages.
+    mode = C.RTLD_LOCAL | getattr(os, "RTLD_NOW", 2) | getattr(os, "RTLD_DEEPBIND", 8)
+    lib = C.CDLL(str(path), mode=mode)
     P = C.POINTER
     d = P(C.c_double)
     i64 = C.c_int64
@@ -100,6 +105,8 @@ def load_library():
                                             P(_Stats)]
     lib.ptbgpu_solve2.argtypes = [C.c_void_p, i64, i64, i64, i64, d, d, d, d, d, P(_Opts), P(_Stats)]
     lib.ptbgpu_symsq_bf16x3.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
+    lib.ptbgpu_symsq_bf16x6.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
+    lib.ptbgpu_runtime_info.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     for name in EXPORTED:
         f = getattr(lib, name)
         if f.restype is not None and name not in ("ptbgpu_default_settings", "ptbgpu_default_opts"):
@@ -163,10 +170,11 @@ class Options:
     electronic_temp: float = 300.0
     glob_par15: float = 0.0
     glob_par17: float = 0.0
+    split3_iters: int = 0
 
     def to_c(self) -> _Opts:
         return _Opts(self.filter, self.precision, self.print_level, self.max_iter, self.electronic_temp,
-                     self.glob_par15, self.glob_par17)
+                     self.glob_par15, self.glob_par17, self.split3_iters)
 
 
 class Context:
@@ -203,6 +211,12 @@ class Context:
             buf = C.create_string_buffer(1024)
             self._lib.ptbgpu_last_error(self._h, buf, 1024)
             raise PtbGpuError(rc, buf.value.decode(errors="replace"))
+
+    def runtime_info(self) -> str:
+        """Device and the CUDA runtime / driver / cuBLAS / cuSOLVER versions in use."""
+        buf = C.create_string_buffer(512)
+        self._check(self._lib.ptbgpu_runtime_info(self._h, buf, 512))
+        return buf.value.decode()
 
     # ---- reference entry points ------------------------------------------
     def filter_matrix_sym(self, A: np.ndarray, n: int, filter: float) -> np.ndarray:
@@ -284,11 +298,17 @@ class Context:
     # ---- kernel level ------------------------------------------------------
     def symsq_bf16x3(self, X: np.ndarray) -> np.ndarray:
         """C = X X (symmetric X) on the tcgen05 kernel with bf16x3 operands; FP32 result."""
+        return self._symsq(X, self._lib.ptbgpu_symsq_bf16x3)
+
+    def symsq_bf16x6(self, X: np.ndarray) -> np.ndarray:
+        """C = X X with the three-plane split (bf16x6 products); FP32 result."""
+        return self._symsq(X, self._lib.ptbgpu_symsq_bf16x6)
+
+    def _symsq(self, X, fn):
         Xh = _f64(X)
         n = Xh.shape[0]
         out = np.zeros((n, n), dtype=np.float32)
-        self._check(self._lib.ptbgpu_symsq_bf16x3(self._h, int(n), _dptr(Xh),
-                                                  out.ctypes.data_as(C.POINTER(C.c_float))))
+        self._check(fn(self._h, int(n), _dptr(Xh), out.ctypes.data_as(C.POINTER(C.c_float))))
         return out
 
 

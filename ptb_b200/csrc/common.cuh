@@ -136,6 +136,7 @@ void axpby_diag(cudaStream_t s, int64_t n, int64_t ld, double alpha, const doubl
 void symmetrize_upper(cudaStream_t s, int64_t n, int64_t ld, double* a);   // a_ji := a_ij for i<j (row-major upper)
 void copy_mat(cudaStream_t s, int64_t n, int64_t ld_src, const double* src, int64_t ld_dst, double* dst);
 void d2f_split(cudaStream_t s, int64_t n, int64_t ldp, const double* x, float* xf, void* hi, void* lo);
+void d2f_split3(cudaStream_t s, int64_t ldp, const float* xf, const void* hi, void* mid, void* lo);
 
 // cuBLAS / cuSOLVER wrappers on row-major symmetric work (see dense_ops.cu)
 void dgemm_nn(ptbgpu_ctx* c, int64_t n, int64_t ld, double alpha, const double* A, const double* B,

@@ -126,6 +126,22 @@ int ptbgpu_last_error(const ptbgpu_ctx* c, char* buf, size_t len) {
     return PTBGPU_OK;
 }
 
+int ptbgpu_runtime_info(const ptbgpu_ctx* c, char* buf, size_t len) {
+    if (!c || !buf || len == 0) return PTBGPU_EINVAL;
+    int rt = 0, drv = 0, cub = 0, maj = 0, min = 0, pat = 0;
+    cudaRuntimeGetVersion(&rt);
+    cudaDriverGetVersion(&drv);
+    cublasGetVersion(c->blas, &cub);
+    cusolverGetProperty(MAJOR_VERSION, &maj);
+    cusolverGetProperty(MINOR_VERSION, &min);
+    cusolverGetProperty(PATCH_LEVEL, &pat);
+    cudaDeviceProp p{};
+    cudaGetDeviceProperties(&p, c->device);
+    snprintf(buf, len, "device %s (sm_%d%d, %d SMs) cudart %d driver %d cublas %d cusolver %d.%d.%d", p.name,
+             p.major, p.minor, p.multiProcessorCount, rt, drv, cub, maj, min, pat);
+    return PTBGPU_OK;
+}
+
 void ptbgpu_default_settings(ptbgpu_pur_settings* s) {
     if (!s) return;
     s->mode = PTBGPU_MODE_FULL;
@@ -150,6 +166,7 @@ void ptbgpu_default_opts(ptbgpu_opts* o) {
     o->print_level = 0;
     o->max_iter = 100;
     o->electronic_temp = 300.0;
+    o->split3_iters = 0;
 }
 
 }  // extern "C"

@@ -240,6 +240,18 @@ __global__ void k_d2f_split(int64_t n, int64_t ldp, const double* __restrict__ x
         }
 }
 
+// Third split plane: mid = bf16(x - hi), lo = bf16(x - hi - mid) from the FP32 copy.
+__global__ void k_split3(int64_t count, const float* __restrict__ xf, const __nv_bfloat16* __restrict__ hi,
+                         __nv_bfloat16* __restrict__ mid, __nv_bfloat16* __restrict__ lo) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < count;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const float r = xf[k] - __bfloat162float(hi[k]);
+        const __nv_bfloat16 m = __float2bfloat16_rn(r);
+        mid[k] = m;
+        lo[k] = __float2bfloat16_rn(r - __bfloat162float(m));
+    }
+}
+
 int grid_for(int64_t work, int per = kThreads) {
     int64_t g = (work + per - 1) / per;
     return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
@@ -401,6 +413,14 @@ void copy_mat(cudaStream_t s, int64_t n, int64_t lds, const double* src, int64_t
 void d2f_split(cudaStream_t s, int64_t n, int64_t ldp, const double* x, float* xf, void* hi, void* lo) {
     k_d2f_split<<<grid_for(ldp, 1), kThreads, 0, s>>>(n, ldp, x, xf, (__nv_bfloat16*)hi,
                                                      (__nv_bfloat16*)lo);
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+}
+
+void d2f_split3(cudaStream_t s, int64_t ldp, const float* xf, const void* hi, void* mid, void* lo) {
+    const int64_t cnt = ldp * ldp;
+    k_split3<<<grid_for(cnt), kThreads, 0, s>>>(cnt, xf, (const __nv_bfloat16*)hi, (__nv_bfloat16*)mid,
+                                                (__nv_bfloat16*)lo);
     count_launch();
     PTB_CUDA(cudaGetLastError());
 }

@@ -65,8 +65,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 // zero-padded FP32 / bf16 hi / bf16 lo planes (ldp x ldp); per-block partials
 // of tr X_0 and ||X_0||^2 into stats[2*block].
 __global__ void k_x0_init(int64_t n, int64_t ldp, const double* __restrict__ A, double emax, double scale,
-                          float* __restrict__ xf, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
-                          double* __restrict__ stats) {
+                          float* __restrict__ xf, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ mid,
+                          __nv_bfloat16* __restrict__ lo, double* __restrict__ stats) {
     double tr = 0.0, ss = 0.0;
     for (int64_t j = blockIdx.x; j < ldp; j += gridDim.x) {
         for (int64_t i = threadIdx.x; i < ldp; i += blockDim.x) {
@@ -77,9 +77,12 @@ __global__ void k_x0_init(int64_t n, int64_t ldp, const double* __restrict__ A, 
             }
             const int64_t k = i + j * ldp;
             xf[k] = v;
-            __nv_bfloat16 h = __float2bfloat16_rn(v);
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            const float r = v - __bfloat162float(h);
+            const __nv_bfloat16 m = __float2bfloat16_rn(r);
             hi[k] = h;
-            lo[k] = __float2bfloat16_rn(v - __bfloat162float(h));
+            mid[k] = m;
+            lo[k] = __float2bfloat16_rn(r - __bfloat162float(m));
             const double dv = v;
             if (i == j) tr += dv;
             ss += dv * dv;
@@ -244,11 +247,11 @@ int grid1(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(n, 148
 
 // A tensor-core product bracketed by CUDA events on the launching stream; the
 // C-ABI layer sums the elapsed times per kind into the call's stats.
-void timed_product(ptbgpu_ctx* c, int epi, int64_t ldp, const void* a0, const void* a1, const void* b0,
-                   const void* b1, const tc::ProdList& prods, const int2* tiles, int ntiles, const tc::EpiParams& ep) {
+void timed_product(ptbgpu_ctx* c, int epi, int np, int64_t ldp, const void* const* pa, const void* const* pb,
+                   const tc::ProdList& prods, const int2* tiles, int ntiles, const tc::EpiParams& ep) {
     cudaEvent_t a = c->take_event(), b = c->take_event();
     PTB_CUDA(cudaEventRecord(a, c->stream));
-    tc::launch_product(c->stream, epi, ldp, a0, a1, b0, b1, prods, tiles, ntiles, ep);
+    tc::launch_product(c->stream, epi, np, ldp, pa, pb, prods, tiles, ntiles, ep);
     PTB_CUDA(cudaEventRecord(b, c->stream));
     c->timed.push_back({epi == tc::EPI_SP2 ? 0 : 1, a, b});
 }
@@ -347,40 +350,44 @@ void sp2_fp64(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int ma
 }
 
 void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int maxit, bool refine,
-               double* dPpk, ptbgpu_stats* st, int prl) {
+               int64_t split3_iters, double* dPpk, ptbgpu_stats* st, int prl) {
     cudaStream_t s = c->stream;
     const int64_t ldp = round_up(n, tc::tile_n());
     const size_t plane = sizeof(__nv_bfloat16) * (size_t)ldp * ldp;
     const size_t fplane = sizeof(float) * (size_t)ldp * ldp;
 
-    // trajectory slots (hi+lo per iterate), bounded by free memory
+    // trajectory slots (hi, mid, lo planes per iterate), bounded by free memory
     size_t free_b = 0, total_b = 0;
     PTB_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t other = 6 * fplane + 4 * plane + (size_t)(64 << 20);
     int slots = (int)std::min<int64_t>(maxit + 1, kMaxIt + 1);
-    if (free_b > other) slots = (int)std::min<size_t>(slots, (free_b - other) * 6 / 10 / (2 * plane));
+    if (free_b > other) slots = (int)std::min<size_t>(slots, (free_b - other) * 6 / 10 / (3 * plane));
     PTB_CHECK(slots >= std::min(8, maxit + 1), PTBGPU_ENOMEM,
               "not enough device memory for the purification trajectory");
     DevBuf& btraj = c->buf(B_TRAJ);
-    btraj.reserve(2 * plane * (size_t)slots);
-    auto traj_hi = [&](int k) { return (__nv_bfloat16*)((char*)btraj.ptr + 2 * plane * (size_t)k); };
-    auto traj_lo = [&](int k) { return (__nv_bfloat16*)((char*)btraj.ptr + 2 * plane * (size_t)k + plane); };
+    btraj.reserve(3 * plane * (size_t)slots);
+    auto traj = [&](int k, int j) { return (__nv_bfloat16*)((char*)btraj.ptr + plane * (3 * (size_t)k + j)); };
+    auto traj_hi = [&](int k) { return traj(k, 0); };
+    auto traj_lo = [&](int k) { return traj(k, 1); };
     c->buf(B_XF0).reserve(fplane);
     c->buf(B_XF1).reserve(fplane);
     float* xf[2] = {c->buf(B_XF0).as<float>(), c->buf(B_XF1).as<float>()};
 
     // tiles and per-tile stats
-    std::vector<int2> up = tc::make_tiles(ldp, true);
-    std::vector<int2> all = tc::make_tiles(ldp, false);
+    std::vector<int2> up = tc::make_tiles(ldp, true, 256);
+    std::vector<int2> up3 = tc::make_tiles(ldp, true, 128);
+    std::vector<int2> all = tc::make_tiles(ldp, false, 256);
     DevBuf& bt = c->buf(B_TILES);
-    bt.reserve(sizeof(int2) * (up.size() + all.size()));
+    bt.reserve(sizeof(int2) * (up.size() + up3.size() + all.size()));
     int2* tiles_up = bt.as<int2>();
-    int2* tiles_all = tiles_up + up.size();
+    int2* tiles_up3 = tiles_up + up.size();
+    int2* tiles_all = tiles_up3 + up3.size();
     PTB_CUDA(cudaMemcpyAsync(tiles_up, up.data(), sizeof(int2) * up.size(), cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemcpyAsync(tiles_up3, up3.data(), sizeof(int2) * up3.size(), cudaMemcpyHostToDevice, s));
     PTB_CUDA(cudaMemcpyAsync(tiles_all, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s));
     const int x0_blocks = grid1(ldp);
     DevBuf& bstats = c->buf(B_STATS);
-    bstats.reserve(sizeof(double) * 2 * std::max<size_t>(up.size(), (size_t)x0_blocks));
+    bstats.reserve(sizeof(double) * 2 * std::max({up.size(), up3.size(), (size_t)x0_blocks}));
     double* stats = bstats.as<double>();
     if (!c->sp2_state) PTB_CUDA(cudaMalloc(&c->sp2_state, sizeof(SP2State)));
     SP2State* state = (SP2State*)c->sp2_state;
@@ -392,16 +399,19 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     const double* A = c->buf(B_H).as<double>();
     const double scale = 1.0 / (pro.emax - pro.emin);
     const double N = 0.5 * (double)nel;
-    const double tol_abs = 1e-6 * (double)n;   // floor of bf16x3 iterations
+    // pass 1 runs to its rounding floor: the two-step non-decrease rule ends it
+    const double tol_abs = 1e-12 * (double)n;
     const double e_switch = 1.0;
-    k_x0_init<<<x0_blocks, 256, 0, s>>>(n, ldp, A, pro.emax, scale, xf[0], traj_hi(0), traj_lo(0), stats);
+    k_x0_init<<<x0_blocks, 256, 0, s>>>(n, ldp, A, pro.emax, scale, xf[0], traj(0, 0), traj(0, 1), traj(0, 2),
+                                        stats);
     count_launch();
     PTB_CUDA(cudaGetLastError());
     k_decide<<<1, 256, 0, s>>>(state, stats, x0_blocks, N, tol_abs, e_switch, std::min(maxit, slots - 1));
     count_launch();
     PTB_CUDA(cudaGetLastError());
 
-    tc::ProdList split3{3, {0, 0, 1, 0}, {0, 1, 0, 0}};
+    tc::ProdList split3{3, {0, 0, 1}, {0, 1, 0}};
+    tc::ProdList split6{6, {0, 0, 1, 0, 2, 1}, {0, 1, 0, 2, 0, 1}};
     tc::EpiParams ep{};
     ep.active = &state->active;
     ep.sq_flag = &state->sq_cur;
@@ -414,11 +424,15 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     for (int k = 0; k < cap; ++k) {
         ep.xcur = xf[k & 1];
         ep.out = xf[(k + 1) & 1];
-        ep.hi = traj_hi(k + 1);
-        ep.lo = traj_lo(k + 1);
-        timed_product(c, tc::EPI_SP2, ldp, traj_hi(k), traj_lo(k), traj_hi(k), traj_lo(k), split3, tiles_up,
-                           (int)up.size(), ep);
-        k_decide<<<1, 256, 0, s>>>(state, stats, (int)up.size(), N, tol_abs, e_switch, cap);
+        ep.hi = traj(k + 1, 0);
+        ep.lo = traj(k + 1, 1);
+        ep.lo2 = traj(k + 1, 2);
+        const bool three = split3_iters < 0 ? false : (split3_iters == 0 || k < split3_iters);
+        const void* pl[3] = {traj(k, 0), traj(k, 1), traj(k, 2)};
+        const int ntl = three ? (int)up3.size() : (int)up.size();
+        timed_product(c, tc::EPI_SP2, three ? 3 : 2, ldp, pl, pl, three ? split6 : split3,
+                      three ? tiles_up3 : tiles_up, ntl, ep);
+        k_decide<<<1, 256, 0, s>>>(state, stats, ntl, N, tol_abs, e_switch, cap);
         count_launch();
         PTB_CUDA(cudaGetLastError());
         ++launched;
@@ -500,7 +514,9 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         epf.err = &c->flags->timeout;
         epf.ld = ldp;
         epf.out = wf;
-        timed_product(c, tc::EPI_FULL, ldp, chi, clo, phi, plo, split3, tiles_all, (int)all.size(), epf);
+        const void* pc[2] = {chi, clo};
+        const void* pp[2] = {phi, plo};
+        timed_product(c, tc::EPI_FULL, 2, ldp, pc, pp, split3, tiles_all, (int)all.size(), epf);
         // The planes hold C^T (column-major C read row-major), so wf = C^T P~ = -C P~.
         // A1 = C P~ - P~ C = -(wf + wf^T) and X1_0 = -A1 / (e_max - e_min) = (wf + wf^T) * scale.
         const unsigned nbp = (unsigned)(ldp / 32);
@@ -511,8 +527,9 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         // replay the branch sequence over the stored trajectory
         for (int k = 0; k < K; ++k) {
             const int a = k & 1, b = a ^ 1;
-            timed_product(c, tc::EPI_FULL, ldp, traj_hi(k), traj_lo(k), x1hi[a], x1lo[a], split3, tiles_all,
-                               (int)all.size(), epf);
+            const void* p0[2] = {traj_hi(k), traj_lo(k)};
+            const void* p1[2] = {x1hi[a], x1lo[a]};
+            timed_product(c, tc::EPI_FULL, 2, ldp, p0, p1, split3, tiles_all, (int)all.size(), epf);
             const bool sq = H.sq[k] != 0;
             k_sym_update<<<dim3(nbp, nbp), dim3(32, 8), 0, s>>>(ldp, wf, x1f[a], sq ? 1.0f : -1.0f,
                                                                 sq ? 0.0f : 2.0f, x1f[b], x1hi[b], x1lo[b]);
@@ -563,7 +580,7 @@ void tc_purify_device(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, c
     if (o->precision == PTBGPU_PREC_FP64)
         sp2_fp64(c, n, nel, pro, maxit, dP, st, prl);
     else
-        sp2_mixed(c, n, nel, pro, maxit, o->precision != 2, dP, st, prl);
+        sp2_mixed(c, n, nel, pro, maxit, o->precision != 2, o->split3_iters, dP, st, prl);
 }
 
 }  // namespace
@@ -573,8 +590,9 @@ void tc_purify_entry(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, co
     tc_purify_device(c, n, nel, dH, dS, dP, o, st);
 }
 
-// C = X X with the bf16x3 kernel (every tile, EPI_FULL), for kernel-level tests.
-void symsq_entry(ptbgpu_ctx* c, int64_t n, const double* hX, float* hC) {
+// C = X X with the split-bf16 kernel (every tile, EPI_FULL) for kernel-level
+// tests: np = 2 planes (bf16x3 products) or 3 planes (bf16x6 products).
+void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, const double* hX, float* hC) {
     cudaStream_t s = c->stream;
     const int64_t ldp = round_up(n, tc::tile_n());
     const size_t plane = sizeof(__nv_bfloat16) * (size_t)ldp * ldp;
@@ -582,24 +600,30 @@ void symsq_entry(ptbgpu_ctx* c, int64_t n, const double* hX, float* hC) {
     bx.reserve(sizeof(double) * n * n);
     PTB_CUDA(cudaMemcpyAsync(bx.ptr, hX, sizeof(double) * n * n, cudaMemcpyHostToDevice, s));
     DevBuf& bp = c->buf(B_MISC1);
-    bp.reserve(2 * plane);
+    bp.reserve(3 * plane);
     __nv_bfloat16* hi = (__nv_bfloat16*)bp.ptr;
-    __nv_bfloat16* lo = hi + (size_t)ldp * ldp;
-    d2f_split(s, n, ldp, bx.as<double>(), nullptr, hi, lo);
+    __nv_bfloat16* mid = hi + (size_t)ldp * ldp;
+    __nv_bfloat16* lo = mid + (size_t)ldp * ldp;
     DevBuf& bc = c->buf(B_MISC0);
     bc.reserve(sizeof(float) * (size_t)ldp * ldp);
-    std::vector<int2> all = tc::make_tiles(ldp, false);
+    float* xf = bc.as<float>();
+    // planes of the FP32-rounded X: hi, mid = bf16(x - hi), lo = bf16(x - hi - mid)
+    d2f_split(s, n, ldp, bx.as<double>(), xf, hi, mid);
+    d2f_split3(s, ldp, xf, hi, mid, lo);
+    std::vector<int2> all = tc::make_tiles(ldp, false, np == 2 ? 256 : 128);
     DevBuf& bt = c->buf(B_TILES);
     bt.reserve(sizeof(int2) * all.size());
     PTB_CUDA(cudaMemcpyAsync(bt.ptr, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s));
     PTB_CUDA(cudaMemsetAsync(&c->flags->timeout, 0, sizeof(int), s));
-    tc::ProdList split3{3, {0, 0, 1, 0}, {0, 1, 0, 0}};
+    tc::ProdList split3{3, {0, 0, 1}, {0, 1, 0}};
+    tc::ProdList split6{6, {0, 0, 1, 0, 2, 1}, {0, 1, 0, 2, 0, 1}};
     tc::EpiParams ep{};
     ep.err = &c->flags->timeout;
     ep.ld = ldp;
-    ep.out = bc.as<float>();
-    tc::launch_product(s, tc::EPI_FULL, ldp, hi, lo, hi, lo, split3, bt.as<int2>(), (int)all.size(), ep);
-    PTB_CUDA(cudaMemcpy2DAsync(hC, sizeof(float) * n, bc.ptr, sizeof(float) * ldp, sizeof(float) * n, n,
+    ep.out = xf;   // the FP32 copy is consumed by the split above (stream order)
+    const void* pl[3] = {hi, mid, lo};
+    timed_product(c, tc::EPI_FULL, np, ldp, pl, pl, np == 2 ? split3 : split6, bt.as<int2>(), (int)all.size(), ep);
+    PTB_CUDA(cudaMemcpy2DAsync(hC, sizeof(float) * n, xf, sizeof(float) * ldp, sizeof(float) * n, n,
                                cudaMemcpyDeviceToHost, s));
     int tmo = 0;
     PTB_CUDA(cudaMemcpyAsync(&tmo, &c->flags->timeout, sizeof(int), cudaMemcpyDeviceToHost, s));

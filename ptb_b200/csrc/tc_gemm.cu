@@ -6,21 +6,26 @@
 // an FP32 matrix (about 16 significant bits per operand; the dropped lo*lo
 // term is 2^-16 relative).
 //
-// One CTA computes a 128 x 256 tile (cta_group::1, UMMA 128x256x16):
-//   warp 0      TMA producer: per 64-wide K block, 2 A tiles (128x64) and 2 B
-//               tiles (256x64) into a 2-stage ring, 128B-swizzled, completion
+// With three planes {hi, mid, lo} (hi = bf16(x), mid = bf16(x - hi),
+// lo = bf16(x - hi - mid)) and the six products hh + hm + mh + hl + lh + mm the
+// operands carry about 24 significant bits ("bf16x6").
+//
+// One CTA computes a 128 x BN tile (cta_group::1, UMMA 128xBNx16); BN = 256
+// with two planes or BN = 128 with three planes, both 96 KB per stage:
+//   warp 0      TMA producer: per 64-wide K block, NP A tiles (128x64) and NP B
+//               tiles (BNx64) into a 2-stage ring, 128B-swizzled, completion
 //               on a "full" mbarrier with a transaction count;
-//   warp 1      MMA issuer (one thread): 4 K16 steps x 3 products per stage,
-//               tcgen05.commit releases the stage on its "empty" mbarrier;
-//   warp 2      allocates / frees the 256 TMEM columns of the accumulator;
+//   warp 1      MMA issuer (one thread): 4 K16 steps x the product list per
+//               stage, tcgen05.commit releases the stage on its "empty" mbarrier;
+//   warp 2      allocates / frees the BN TMEM columns of the accumulator;
 //   warps 4..7  epilogue: tcgen05.ld of their 32 lanes (rows), fused update.
 //
 // Epilogues:
 //   EPI_FULL  every tile; C written row-major as FP32 (general product).
 //   EPI_SP2   symmetric X*X: only tiles touching the upper triangle run; the
 //             element (r,c), c >= r, becomes X' = C (branch "square") or
-//             2X - C, written to (r,c) and (c,r) as FP32 and as the bf16 hi/lo
-//             planes of the next product; per-tile trace and sum of squares
+//             2X - C, written to (r,c) and (c,r) as FP32 and as the bf16
+//             hi/mid/lo planes of the next product; per-tile trace and sum of squares
 //             (= tr X'^2 for symmetric X') go to a stats array that the
 //             decision kernel reduces in a fixed order (deterministic).
 //
@@ -42,15 +47,21 @@ namespace tc {
 namespace {
 
 constexpr int BM = 128;
-constexpr int BN = 256;
 constexpr int KB = 64;                        // K elements per stage (128 bytes of bf16)
 constexpr int STAGES = 2;
-constexpr int NPLANE = 2;                     // A planes and B planes per stage
 constexpr int A_TILE_BYTES = BM * KB * 2;     // 16 KB
-constexpr int B_TILE_BYTES = BN * KB * 2;     // 32 KB
-constexpr int STAGE_BYTES = NPLANE * (A_TILE_BYTES + B_TILE_BYTES);
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr int THREADS = 256;
+
+template <int BN, int NP>
+struct Cfg {
+    static constexpr int B_TILE_BYTES = BN * KB * 2;
+    static constexpr int STAGE_BYTES = NP * (A_TILE_BYTES + B_TILE_BYTES);
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+    // Instruction descriptor for kind::f16: D fp32, A/B bf16, both K-major, M=128, N=BN.
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                      ((uint32_t)(BM >> 4) << 24);
+    static_assert(STAGE_BYTES <= 98304, "stage larger than the 2-stage budget");
+};
 constexpr uint64_t kTimeoutNs = 2000000000ull;
 
 // ---- PTX wrappers ---------------------------------------------------------
@@ -141,25 +152,27 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
     d |= (uint64_t)2u << 61;
     return d;
 }
-// Instruction descriptor for kind::f16: D fp32, A/B bf16, both K-major, M=128, N=BN.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                            ((uint32_t)(BM >> 4) << 24);
 
 __device__ __forceinline__ void set_err(int* err, int site) {
     if (err) atomicCAS(err, 0, site);
 }
 
-__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& h, __nv_bfloat16& l) {
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& h, __nv_bfloat16& m, __nv_bfloat16& l) {
     h = __float2bfloat16_rn(v);
-    l = __float2bfloat16_rn(v - __bfloat162float(h));
+    const float r = v - __bfloat162float(h);
+    m = __float2bfloat16_rn(r);
+    l = __float2bfloat16_rn(r - __bfloat162float(m));
 }
 
 // ---- the kernel -----------------------------------------------------------
-template <int EPI>
+template <int EPI, int BN, int NP>
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_product(const __grid_constant__ TmaPlanes maps, const ProdList prods, const int2* __restrict__ tiles,
                  int nk, EpiParams ep) {
     if (ep.active && *ep.active == 0) return;   // uniform early exit (converged iteration)
+    using C = Cfg<BN, NP>;
+    constexpr int STAGE_BYTES = C::STAGE_BYTES;
+    constexpr int B_TILE_BYTES = C::B_TILE_BYTES;
 
     extern __shared__ uint8_t smem_raw[];
     const uint32_t base_raw = smem_u32(smem_raw);
@@ -179,7 +192,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     auto a_tile = [&](int s, int p) { return base + s * STAGE_BYTES + p * A_TILE_BYTES; };
     auto b_tile = [&](int s, int p) {
-        return base + s * STAGE_BYTES + NPLANE * A_TILE_BYTES + p * B_TILE_BYTES;
+        return base + s * STAGE_BYTES + NP * A_TILE_BYTES + p * B_TILE_BYTES;
     };
 
     if (threadIdx.x == 0) {
@@ -215,9 +228,9 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             if (*(volatile int*)abort_flag) break;
             mbar_expect_tx(full_bar(s), STAGE_BYTES);
-            for (int p = 0; p < NPLANE; ++p)
+            for (int p = 0; p < NP; ++p)
                 tma_load_2d(a_tile(s, p), &maps.a[p], full_bar(s), kb * KB, bi * BM);
-            for (int p = 0; p < NPLANE; ++p)
+            for (int p = 0; p < NP; ++p)
                 tma_load_2d(b_tile(s, p), &maps.b[p], full_bar(s), kb * KB, bj * BN);
             issued_phase[s] = round & 1;
         }
@@ -245,7 +258,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 for (int p = 0; p < prods.n; ++p) {
                     const uint64_t ad = sdesc_sw128(a_tile(s, prods.a[p]) + k * 32);
                     const uint64_t bd = sdesc_sw128(b_tile(s, prods.b[p]) + k * 32);
-                    umma_bf16(tmem, ad, bd, kIdesc, (kb | k | p) != 0);
+                    umma_bf16(tmem, ad, bd, C::IDESC, (kb | k | p) != 0);
                 }
             }
             umma_commit(empty_bar(s));
@@ -286,18 +299,19 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const float4* xin = reinterpret_cast<const float4*>(ep.xcur + r * ld + cbase);
                     float4* xo = reinterpret_cast<float4*>(ep.out + r * ld + cbase);
                     uint4* ho = reinterpret_cast<uint4*>(ep.hi + r * ld + cbase);
-                    uint4* lo = reinterpret_cast<uint4*>(ep.lo + r * ld + cbase);
+                    uint4* mo = reinterpret_cast<uint4*>(ep.lo + r * ld + cbase);
+                    uint4* lo = reinterpret_cast<uint4*>(ep.lo2 + r * ld + cbase);
 #pragma unroll
                     for (int j8 = 0; j8 < 4; ++j8) {
                         float val[8];
                         const float4 x0 = xin[2 * j8], x1 = xin[2 * j8 + 1];
                         const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-                        __align__(16) __nv_bfloat16 hh[8], ll[8];
+                        __align__(16) __nv_bfloat16 hh[8], mm[8], ll[8];
 #pragma unroll
                         for (int t = 0; t < 8; ++t) {
                             const float cv = __uint_as_float(v[8 * j8 + t]);
                             val[t] = square ? cv : 2.0f * xs[t] - cv;
-                            split_bf16(val[t], hh[t], ll[t]);
+                            split_bf16(val[t], hh[t], mm[t], ll[t]);
                             const int64_t c = cbase + 8 * j8 + t;
                             const double dv = (double)val[t];
                             if (c == r) {
@@ -307,12 +321,14 @@ __global__ void __launch_bounds__(THREADS, 1)
                                 ss += 2.0 * dv * dv;
                                 ep.out[c * ld + r] = val[t];
                                 ep.hi[c * ld + r] = hh[t];
-                                ep.lo[c * ld + r] = ll[t];
+                                ep.lo[c * ld + r] = mm[t];
+                                ep.lo2[c * ld + r] = ll[t];
                             }
                         }
                         xo[2 * j8] = make_float4(val[0], val[1], val[2], val[3]);
                         xo[2 * j8 + 1] = make_float4(val[4], val[5], val[6], val[7]);
                         ho[j8] = *reinterpret_cast<const uint4*>(hh);
+                        mo[j8] = *reinterpret_cast<const uint4*>(mm);
                         lo[j8] = *reinterpret_cast<const uint4*>(ll);
                     }
                 } else {
@@ -323,12 +339,13 @@ __global__ void __launch_bounds__(THREADS, 1)
                         if (c < r) continue;
                         const float cv = __uint_as_float(v[j]);
                         const float val = square ? cv : 2.0f * ep.xcur[r * ld + c] - cv;
-                        __nv_bfloat16 h, l;
-                        split_bf16(val, h, l);
+                        __nv_bfloat16 h, m, l;
+                        split_bf16(val, h, m, l);
                         const double dv = (double)val;
                         ep.out[r * ld + c] = val;
                         ep.hi[r * ld + c] = h;
-                        ep.lo[r * ld + c] = l;
+                        ep.lo[r * ld + c] = m;
+                        ep.lo2[r * ld + c] = l;
                         if (c == r) {
                             tr += dv;
                             ss += dv * dv;
@@ -336,7 +353,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                             ss += 2.0 * dv * dv;
                             ep.out[c * ld + r] = val;
                             ep.hi[c * ld + r] = h;
-                            ep.lo[c * ld + r] = l;
+                            ep.lo[c * ld + r] = m;
+                            ep.lo2[c * ld + r] = l;
                         }
                     }
                 }
@@ -397,47 +415,56 @@ void encode_plane(CUtensorMap* map, const void* plane, int64_t ld, int box_rows)
 
 }  // namespace
 
-int tile_n() { return BN; }
+int tile_n() { return 256; }
 
-// Tile lists: row blocks of 128, column blocks of 256, grouped by 16 row
+// Tile lists: row blocks of 128, column blocks of bn, grouped by 16 row
 // blocks so that consecutive CTAs share operand panels in L2.
-std::vector<int2> make_tiles(long long ld, bool upper_only) {
-    const int nbi = (int)(ld / BM), nbj = (int)(ld / BN);
+std::vector<int2> make_tiles(long long ld, bool upper_only, int bn) {
+    const int nbi = (int)(ld / BM), nbj = (int)(ld / bn);
     std::vector<int2> t;
     const int G = 16;
     for (int g0 = 0; g0 < nbi; g0 += G)
         for (int bj = 0; bj < nbj; ++bj)
             for (int bi = g0; bi < std::min(nbi, g0 + G); ++bi)
-                if (!upper_only || (int64_t)bj * BN + BN - 1 >= (int64_t)bi * BM) t.push_back(make_int2(bi, bj));
+                if (!upper_only || (int64_t)bj * bn + bn - 1 >= (int64_t)bi * BM) t.push_back(make_int2(bi, bj));
     return t;
 }
 
-void launch_product(cudaStream_t s, int epi, long long ld, const void* a0, const void* a1, const void* b0,
-                    const void* b1, const ProdList& prods, const int2* tiles_dev, int ntiles,
-                    const EpiParams& ep) {
-    static bool attr_set[2] = {false, false};
+namespace {
+template <int EPI, int BN, int NP>
+void launch_t(cudaStream_t s, const TmaPlanes& maps, const ProdList& prods, const int2* tiles, int ntiles, int nk,
+              const EpiParams& ep) {
+    static bool attr = false;
+    if (!attr) {
+        PTB_CUDA(cudaFuncSetAttribute(k_tc_product<EPI, BN, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      Cfg<BN, NP>::SMEM_BYTES));
+        attr = true;
+    }
+    k_tc_product<EPI, BN, NP><<<ntiles, THREADS, Cfg<BN, NP>::SMEM_BYTES, s>>>(maps, prods, tiles, nk, ep);
+    count_launch();
+}
+}  // namespace
+
+void launch_product(cudaStream_t s, int epi, int np, long long ld, const void* const* a, const void* const* b,
+                    const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep) {
+    PTB_CHECK(np == 2 || np == 3, PTBGPU_EINVAL, "unsupported plane count %d", np);
+    const int bn = np == 2 ? 256 : 128;
+    for (int p = 0; p < prods.n; ++p)
+        PTB_CHECK(prods.a[p] < np && prods.b[p] < np, PTBGPU_EINVAL, "product references a missing plane");
+    PTB_CHECK(epi != EPI_SP2 || (ep.lo2 != nullptr && ep.lo != nullptr), PTBGPU_EINVAL,
+              "the SP2 epilogue writes three planes");
     TmaPlanes maps;
-    encode_plane(&maps.a[0], a0, ld, BM);
-    encode_plane(&maps.a[1], a1, ld, BM);
-    encode_plane(&maps.b[0], b0, ld, BN);
-    encode_plane(&maps.b[1], b1, ld, BN);
+    for (int p = 0; p < np; ++p) {
+        encode_plane(&maps.a[p], a[p], ld, BM);
+        encode_plane(&maps.b[p], b[p], ld, bn);
+    }
     const int nk = (int)(ld / KB);
     if (epi == EPI_SP2) {
-        if (!attr_set[1]) {
-            PTB_CUDA(cudaFuncSetAttribute(k_tc_product<EPI_SP2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          SMEM_BYTES));
-            attr_set[1] = true;
-        }
-        k_tc_product<EPI_SP2><<<ntiles, THREADS, SMEM_BYTES, s>>>(maps, prods, tiles_dev, nk, ep);
-        count_launch();
+        if (np == 2) launch_t<EPI_SP2, 256, 2>(s, maps, prods, tiles_dev, ntiles, nk, ep);
+        else launch_t<EPI_SP2, 128, 3>(s, maps, prods, tiles_dev, ntiles, nk, ep);
     } else {
-        if (!attr_set[0]) {
-            PTB_CUDA(cudaFuncSetAttribute(k_tc_product<EPI_FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          SMEM_BYTES));
-            attr_set[0] = true;
-        }
-        k_tc_product<EPI_FULL><<<ntiles, THREADS, SMEM_BYTES, s>>>(maps, prods, tiles_dev, nk, ep);
-        count_launch();
+        if (np == 2) launch_t<EPI_FULL, 256, 2>(s, maps, prods, tiles_dev, ntiles, nk, ep);
+        else launch_t<EPI_FULL, 128, 3>(s, maps, prods, tiles_dev, ntiles, nk, ep);
     }
     PTB_CUDA(cudaGetLastError());
 }

@@ -11,17 +11,17 @@ namespace tc {
 
 enum : int { EPI_FULL = 0, EPI_SP2 = 1 };
 
-// Tensor maps of the two A-role and two B-role bf16 planes (64-byte aligned).
+// Tensor maps of up to three A-role and three B-role bf16 planes (64-byte aligned).
 struct TmaPlanes {
-    CUtensorMap a[2];
-    CUtensorMap b[2];
+    CUtensorMap a[3];
+    CUtensorMap b[3];
 };
 
 // Which (A plane, B plane) pairs are accumulated per K step.
 struct ProdList {
     int n;
-    int a[4];
-    int b[4];
+    int a[6];
+    int b[6];
 };
 
 struct EpiParams {
@@ -32,15 +32,16 @@ struct EpiParams {
     const float* xcur;        // EPI_SP2: current iterate (FP32)
     float* out;               // EPI_FULL: C;  EPI_SP2: next iterate (FP32)
     __nv_bfloat16* hi;        // EPI_SP2: next iterate, bf16 hi plane
-    __nv_bfloat16* lo;        // EPI_SP2: next iterate, bf16 lo plane
+    __nv_bfloat16* lo;        // EPI_SP2: next iterate, bf16 mid plane  (x - hi)
+    __nv_bfloat16* lo2;       // EPI_SP2: next iterate, bf16 lo plane   (x - hi - mid)
     double* stats;            // EPI_SP2: per-tile {trace, sum of squares}
 };
 
+// Two-plane products run on 128 x 256 tiles, three-plane products on 128 x 128.
 int tile_n();
-std::vector<int2> make_tiles(long long ld, bool upper_only);
-void launch_product(cudaStream_t s, int epi, long long ld, const void* a0, const void* a1, const void* b0,
-                    const void* b1, const ProdList& prods, const int2* tiles_dev, int ntiles,
-                    const EpiParams& ep);
+std::vector<int2> make_tiles(long long ld, bool upper_only, int bn);
+void launch_product(cudaStream_t s, int epi, int np, long long ld, const void* const* a, const void* const* b,
+                    const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep);
 
 }  // namespace tc
 }  // namespace ptb

@@ -47,6 +47,22 @@ def test_symsq_bf16x3_matches_emulation(ctx, n):
     assert np.max(np.abs(C - X @ X)) <= 1e-4 * scale
 
 
+@pytest.mark.parametrize("n", [200, 512, 640])
+def test_symsq_bf16x6_three_plane_split(ctx, n):
+    rng = np.random.default_rng(n + 1)
+    A = rng.uniform(-1, 1, (n, n))
+    X = 0.5 * (A + A.T)
+    C = ctx.symsq_bf16x6(X).astype(np.float64)
+    x32 = X.astype(np.float32).astype(np.float64)
+    exact = x32 @ x32
+    # three planes carry the FP32 operand almost exactly; what is left is FP32 accumulation
+    bound = 2 * n * 2.0 ** -24 * (np.abs(X) @ np.abs(X)) + 1e-30
+    assert np.all(np.abs(C - exact) <= bound)
+    # and it is clearly more accurate than the two-plane product
+    C3 = ctx.symsq_bf16x3(X).astype(np.float64)
+    assert np.max(np.abs(C - exact)) < 0.25 * np.max(np.abs(C3 - exact))
+
+
 def test_filter_packed_bit_exact(ctx, water8):
     s = water8
     out = ctx.filter_matrix_sym(s.Hvec, s.ndim, 1e-3)
