@@ -184,7 +184,7 @@ def run_ours(args, rank, world, local, pg):
     from ptb_b200 import PREC_FP64, PREC_MIXED, Context, Options, synth
 
     peak_burst, peak_sust, hbm, peak_kind = load_peaks()
-    s = synth.water_cluster(512, seed=1)
+    s = synth.water_cluster(args.nmol, seed=1)
     n, nel = s.ndim, s.nel
     npk = n * (n + 1) // 2
     dev = torch.device("cuda", local)
@@ -276,8 +276,8 @@ def run_ours(args, rank, world, local, pg):
         "metric": METRIC, "value": ms_dev / 1e3, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_dev, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16x3+f64" if prec == PREC_MIXED else "f64", "data": "synthetic",
-        "config": {"workload": "dense density step, 512-H2O box (1536 atoms, ndim 11776, nel 4096), filter 1e-5, "
-                               "trace-correcting purification",
+        "config": {"workload": f"dense density step, {args.nmol}-H2O box ({s.nat} atoms, ndim {n}, nel {nel}), "
+                               "filter 1e-5, trace-correcting purification",
                    "global_batch": world, "seq_len": n, "parallelism": f"replicas x{world}",
                    "l2": "inputs and working set far larger than L2 (no flush)"},
         "tflops_algorithmic": last.flops / (last.ms_solve / 1e3) / 1e12 if last.ms_solve > 0 else None,
@@ -309,6 +309,8 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--no-compare-fp64", dest="compare_fp64", action="store_false")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nmol", type=int, default=512,
+                    help="water molecules in the box (512 = the benchmark workload; smaller boxes for profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

@@ -170,7 +170,7 @@ class Options:
     electronic_temp: float = 300.0
     glob_par15: float = 0.0
     glob_par17: float = 0.0
-    split3_iters: int = 0
+    split3_iters: int = 8
 
     def to_c(self) -> _Opts:
         return _Opts(self.filter, self.precision, self.print_level, self.max_iter, self.electronic_temp,

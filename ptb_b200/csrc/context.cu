@@ -166,7 +166,7 @@ void ptbgpu_default_opts(ptbgpu_opts* o) {
     o->print_level = 0;
     o->max_iter = 100;
     o->electronic_temp = 300.0;
-    o->split3_iters = 0;
+    o->split3_iters = 8;
 }
 
 }  // extern "C"
