@@ -37,8 +37,12 @@ int guarded(ptbgpu_ctx* c, F&& f) {
         return PTBGPU_OK;
     } catch (const Error& e) {
         c->last_error = e.msg;
-        (void)cudaGetLastError();
-        if (c->stream) cudaStreamSynchronize(c->stream);
+        // report a pending or sticky device error too: library status codes such
+        // as cuSOLVER's internal error can be the echo of an earlier kernel fault
+        cudaError_t pend = c->stream ? cudaStreamSynchronize(c->stream) : cudaSuccess;
+        cudaError_t last = cudaGetLastError();
+        if (pend != cudaSuccess || last != cudaSuccess)
+            c->last_error += std::string(" [device: ") + cudaGetErrorString(pend != cudaSuccess ? pend : last) + "]";
         return e.code;
     } catch (const std::exception& e) {
         c->last_error = e.what();

@@ -77,8 +77,10 @@ struct ptbgpu_ctx {
     cudaEvent_t ev[4] = {};
     std::string last_error;
     int num_sms = 0;
-    // named scratch buffers (grown on demand, kept for the context's lifetime)
-    std::vector<ptb::DevBuf> bufs;
+    // named scratch buffers (grown on demand, kept for the context's lifetime);
+    // a fixed array so that references handed out by buf() never move
+    static constexpr int kMaxBufs = 64;
+    ptb::DevBuf bufs[kMaxBufs];
     ptb::DevBuf& buf(int id);
     ptb::DeviceFlags* flags = nullptr;   // device
     int* info_dev = nullptr;             // device int for LAPACK-style info

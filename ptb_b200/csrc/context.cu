@@ -60,8 +60,10 @@ cudaEvent_t ptbgpu_ctx::take_event() {
     return evpool[evused++];
 }
 
+static_assert(ptb::B_COUNT <= ptbgpu_ctx::kMaxBufs, "more scratch-buffer ids than slots");
+
 ptb::DevBuf& ptbgpu_ctx::buf(int id) {
-    if ((int)bufs.size() <= id) bufs.resize(id + 1);
+    PTB_CHECK(id >= 0 && id < kMaxBufs, PTBGPU_EINVAL, "scratch buffer id %d out of range", id);
     return bufs[id];
 }
 

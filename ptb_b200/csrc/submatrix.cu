@@ -20,6 +20,7 @@
 //     column c, rows <= c; rows outside the map stay zero, source/sm.f90:201-203,
 //     343-362, 387).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <map>
 #include <numeric>
@@ -369,6 +370,16 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
     cudaStream_t s = c->stream;
     log_line(prl, 1, " Stupid simple implementation of the submatrix method: %lld %lld", (long long)columns,
              (long long)mode);
+    // phase timer (print level >= 2 only: it synchronises the stream at each mark)
+    auto t_last = std::chrono::steady_clock::now();
+    auto mark = [&](const char* what) {
+        if (prl < 2) return;
+        PTB_CUDA(cudaStreamSynchronize(s));
+        auto now = std::chrono::steady_clock::now();
+        log_line(prl, 2, " * submatrix %-28s %10.3f ms", what,
+                 std::chrono::duration<double, std::milli>(now - t_last).count());
+        t_last = now;
+    };
 
     // full, filtered H and S
     DevBuf& bh = c->buf(B_H);
@@ -434,6 +445,7 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
     log_line(prl, 1, " sums of efforts for submatrices= %g", effort_sms);
     log_line(prl, 1, " ratio %g", effort_sms / effort_full);
 
+    mark("unpack, pattern scan, maps");
     // (4) buckets by padded size; submatrices above kBatchMax take the large path
     constexpr int kBatchMax = 1024;
     std::map<int, std::vector<Prob>> buckets;
@@ -530,10 +542,12 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
             if (bst == CUSOLVER_STATUS_SUCCESS) {
                 ws.reserve(std::max<size_t>(wsd, 16));
                 std::vector<char> hws(std::max<size_t>(wsh, 16));
+                mark("reduction (potrf, 2 trsm)");
                 bst = cusolverDnXsyevBatched(c->solver, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, M,
                                              CUDA_R_64F, Hb, M, CUDA_R_64F, bk.w.ptr, CUDA_R_64F, ws.ptr, wsd,
                                              hws.data(), wsh, infos.as<int>(), B);
                 PTB_CUDA(cudaStreamSynchronize(s));
+                mark("batched eigensolve");
             }
             if (bst != CUSOLVER_STATUS_SUCCESS) {
                 // per-matrix eigensolves of the reduced problems (same layout)
@@ -554,7 +568,9 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
                                                                   be.as<double>(), bfe.as<double>());
             count_launch();
             PTB_CUDA(cudaGetLastError());
+            mark("back-transform and fe");
             for (const Prob& p : pv) flops += 9.0 * std::pow((double)p.m, 3);
+            log_line(prl, 2, " * submatrix bucket M=%d: %d problems", M, B);
         }
         // large submatrices: one generalized eigensolve each (dsygvd), fe from T = S_k U
         for (const Prob& p : large) {
