@@ -624,6 +624,7 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
                      (long long)nelref);
         PTB_CHECK(mr.converged, PTBGPU_EITER, "chemical potential bisection did not converge");
         log_line(prl, 1, " iteration of chemical potential converged");
+        mark("mu bisection");
 
         // (7) final density into the packed result
         PTB_CUDA(cudaMemsetAsync(dP, 0, sizeof(double) * (size_t)npacked(n), s));
@@ -655,6 +656,7 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
             PTB_CUDA(cudaGetLastError());
         }
         PTB_CUDA(cudaStreamSynchronize(s));
+        mark("final density");
         if (st) {
             st->mu = mr.mu;
             st->nel = mr.nel;
