@@ -172,6 +172,22 @@ int ptbgpu_solve2(ptbgpu_ctx* ctx, int64_t mode, int64_t ndim, int64_t nel, int6
                   const double* Hpk, const double* Spk, double* Ppk, double* e, double* focc,
                   const ptbgpu_opts* opts, ptbgpu_stats* st);
 
+/* tr(PS) and tr(PH) (the nel and band_energy of ptbgpu_check_density) of
+ * device-resident packed P, S, H without allocating any device memory and
+ * without a context: for callers that own all device memory themselves (a
+ * Fortran SCF driver with its own pool, a device already full with the
+ * matrices of a large box) or cannot afford the device-wide synchronisation of
+ * cudaMalloc/cudaFree.  No counterpart in the reference.  out (host, 2 doubles)
+ * = {tr(PS), tr(PH)}; dHpk may be NULL (out[1] = 0).  Working memory is a
+ * fixed 1 MB array in the library's device image: ndim <= 65536, larger sizes
+ * are rejected with PTBGPU_EINVAL.  The first call on a device looks up that
+ * array's device address; make it before any stream capture.  Calls share the
+ * array: calls whose kernels overlap on the GPU race.  stream is a cudaStream_t
+ * (NULL: the legacy default stream); the call returns after the stream has
+ * finished.  err (may be NULL) receives the message of a failure. */
+int ptbgpu_density_traces_noalloc(int device, int64_t ndim, const double* dPpk, const double* dSpk,
+                                  const double* dHpk, double* out, void* stream, char* err, size_t errlen);
+
 /* ---- kernel-level entry points (parity tests and benchmarks) ------------ */
 /* C = X * X for a symmetric n x n FP64 matrix X (row-major), computed with the
  * bf16x3 tcgen05 kernel (hi/lo split, FP32 accumulation); C is FP32 row-major. */

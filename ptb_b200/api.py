@@ -64,7 +64,8 @@ class _Stats(C.Structure):
 EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_default_settings",
             "ptbgpu_default_opts", "ptbgpu_filter_packed", "ptbgpu_check_density", "ptbgpu_sm_density",
             "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_solve2",
-            "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_runtime_info")
+            "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_runtime_info",
+            "ptbgpu_density_traces_noalloc")
 
 
 def library_path() -> Path:
@@ -107,6 +108,8 @@ def load_library():
     lib.ptbgpu_symsq_bf16x3.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_bf16x6.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_runtime_info.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+    lib.ptbgpu_density_traces_noalloc.argtypes = [C.c_int, i64, C.c_void_p, C.c_void_p, C.c_void_p, d,
+                                                  C.c_void_p, C.c_char_p, C.c_size_t]
     for name in EXPORTED:
         f = getattr(lib, name)
         if f.restype is not None and name not in ("ptbgpu_default_settings", "ptbgpu_default_opts"):
@@ -310,6 +313,22 @@ class Context:
         out = np.zeros((n, n), dtype=np.float32)
         self._check(fn(self._h, int(n), _dptr(Xh), out.ctypes.data_as(C.POINTER(C.c_float))))
         return out
+
+
+def density_traces_noalloc(device: int, ndim: int, dP: int, dS: int, dH: int | None = None,
+                           stream: int | None = None) -> tuple[float, float]:
+    """(tr(PS), tr(PH)) of device-resident packed P, S, H (raw device pointers)
+    through ptbgpu_density_traces_noalloc: no context and no device allocation,
+    for callers that cannot allocate device memory; ndim <= 65536."""
+    lib = load_library()
+    out = np.zeros(2)
+    err = C.create_string_buffer(512)
+    rc = lib.ptbgpu_density_traces_noalloc(int(device), int(ndim), C.c_void_p(dP), C.c_void_p(dS),
+                                           C.c_void_p(dH) if dH else None, _dptr(out),
+                                           C.c_void_p(stream) if stream else None, err, 512)
+    if rc != OK:
+        raise PtbGpuError(rc, err.value.decode(errors="replace"))
+    return float(out[0]), float(out[1])
 
 
 # module-level conveniences with the reference's names -----------------------
