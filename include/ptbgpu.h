@@ -194,6 +194,9 @@ int ptbgpu_density_traces_noalloc(int device, int64_t ndim, const double* dPpk, 
 int ptbgpu_symsq_bf16x3(ptbgpu_ctx* ctx, int64_t n, const double* X, float* C);
 /* The same with the three-plane split (hi, mid, lo) and six products, ~24-bit operands. */
 int ptbgpu_symsq_bf16x6(ptbgpu_ctx* ctx, int64_t n, const double* X, float* C);
+/* Either split with an explicit K block of the kernel: planes 2 or 3, kblock 32,
+ * 64 or 0 (the autotuned choice). */
+int ptbgpu_symsq_split(ptbgpu_ctx* ctx, int64_t n, int64_t planes, int64_t kblock, const double* X, float* C);
 
 #ifdef __cplusplus
 }

@@ -64,7 +64,7 @@ class _Stats(C.Structure):
 EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_default_settings",
             "ptbgpu_default_opts", "ptbgpu_filter_packed", "ptbgpu_check_density", "ptbgpu_sm_density",
             "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_solve2",
-            "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_runtime_info",
+            "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_symsq_split", "ptbgpu_runtime_info",
             "ptbgpu_density_traces_noalloc")
 
 
@@ -107,6 +107,7 @@ def load_library():
     lib.ptbgpu_solve2.argtypes = [C.c_void_p, i64, i64, i64, i64, d, d, d, d, d, P(_Opts), P(_Stats)]
     lib.ptbgpu_symsq_bf16x3.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_bf16x6.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
+    lib.ptbgpu_symsq_split.argtypes = [C.c_void_p, i64, i64, i64, d, P(C.c_float)]
     lib.ptbgpu_runtime_info.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     lib.ptbgpu_density_traces_noalloc.argtypes = [C.c_int, i64, C.c_void_p, C.c_void_p, C.c_void_p, d,
                                                   C.c_void_p, C.c_char_p, C.c_size_t]
@@ -306,6 +307,10 @@ class Context:
     def symsq_bf16x6(self, X: np.ndarray) -> np.ndarray:
         """C = X X with the three-plane split (bf16x6 products); FP32 result."""
         return self._symsq(X, self._lib.ptbgpu_symsq_bf16x6)
+
+    def symsq_split(self, X: np.ndarray, planes: int, kblock: int) -> np.ndarray:
+        """C = X X with an explicit plane count (2 or 3) and kernel K block (32, 64, 0 = tuned)."""
+        return self._symsq(X, lambda h, n, x, o: self._lib.ptbgpu_symsq_split(h, n, planes, kblock, x, o))
 
     def _symsq(self, X, fn):
         Xh = _f64(X)

@@ -8,7 +8,7 @@
 namespace ptb {
 void tc_purify_entry(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, const double* dS, double* dP,
                      const ptbgpu_opts* o, ptbgpu_stats* st);
-void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, const double* hX, float* hC);
+void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, int kblock, const double* hX, float* hC);
 void purify_ref_device(ptbgpu_ctx* c, const ptbgpu_pur_settings& pur, int64_t n, const double* dH,
                        const double* dS, double* dP, const ptbgpu_opts* o, ptbgpu_stats* st);
 void solve2_device(ptbgpu_ctx* c, int64_t mode, int64_t n, int64_t nel, int64_t nopen, const double* dH,
@@ -221,14 +221,22 @@ int ptbgpu_solve2(ptbgpu_ctx* c, int64_t mode, int64_t ndim, int64_t nel, int64_
 int ptbgpu_symsq_bf16x3(ptbgpu_ctx* c, int64_t n, const double* X, float* C) {
     return guarded(c, [&] {
         PTB_CHECK(n > 0 && X && C, PTBGPU_EINVAL, "bad arguments");
-        symsq_entry(c, n, 2, X, C);
+        symsq_entry(c, n, 2, 0, X, C);
     });
 }
 
 int ptbgpu_symsq_bf16x6(ptbgpu_ctx* c, int64_t n, const double* X, float* C) {
     return guarded(c, [&] {
         PTB_CHECK(n > 0 && X && C, PTBGPU_EINVAL, "bad arguments");
-        symsq_entry(c, n, 3, X, C);
+        symsq_entry(c, n, 3, 0, X, C);
+    });
+}
+
+int ptbgpu_symsq_split(ptbgpu_ctx* c, int64_t n, int64_t planes, int64_t kblock, const double* X, float* C) {
+    return guarded(c, [&] {
+        PTB_CHECK(n > 0 && X && C && (planes == 2 || planes == 3) && (kblock == 0 || kblock == 32 || kblock == 64),
+                  PTBGPU_EINVAL, "bad arguments");
+        symsq_entry(c, n, (int)planes, (int)kblock, X, C);
     });
 }
 

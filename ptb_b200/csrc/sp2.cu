@@ -171,25 +171,30 @@ __global__ void k_sym_update(int64_t ldp, const float* __restrict__ W, const flo
 #pragma unroll
     for (int k = 0; k < 32; k += 8) t[tx][ty + k] = W[(j0 + ty + k) * ldp + i0 + tx];
     __syncthreads();
-    // element (i, j) = (i0 + ty + k, j0 + tx): W[i][j] + W[j][i]
+    // element (i, j) = (i0 + ty + k, j0 + tx): W[i][j] + W[j][i]; on a diagonal
+    // tile only the upper triangle is computed here and mirrored below, so the
+    // result is exactly symmetric even when X is not
 #pragma unroll
     for (int k = 0; k < 32; k += 8) {
         const int64_t i = i0 + ty + k, j = j0 + tx;
         const float s = W[i * ldp + j] + t[ty + k][tx];
         const float v = alpha * s + (beta != 0.0f ? beta * X[i * ldp + j] : 0.0f);
-        const __nv_bfloat16 h = __float2bfloat16_rn(v);
-        const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
-        out[i * ldp + j] = v;
-        hi[i * ldp + j] = h;
-        lo[i * ldp + j] = l;
+        if (bi != bj || i <= j) {
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+            out[i * ldp + j] = v;
+            hi[i * ldp + j] = h;
+            lo[i * ldp + j] = l;
+        }
         t[ty + k][tx] = v;   // each thread rewrites only the slot it read
     }
     __syncthreads();
-    if (bi == bj) return;
-    // mirrored tile: element (j, i) with j = j0 + ty + k, i = i0 + tx
+    // mirrored tile: element (j, i) with j = j0 + ty + k, i = i0 + tx (strictly
+    // below the diagonal on a diagonal tile)
 #pragma unroll
     for (int k = 0; k < 32; k += 8) {
         const int64_t j = j0 + ty + k, i = i0 + tx;
+        if (bi == bj && j <= i) continue;
         const float v = t[tx][ty + k];
         const __nv_bfloat16 h = __float2bfloat16_rn(v);
         out[j * ldp + i] = v;
@@ -206,6 +211,22 @@ __global__ void k_f2d(int64_t n, int64_t ldp, const float* __restrict__ x, doubl
             const double v = a * (double)x[i + j * ldp];
             y[i + j * n] = (b == 0.0) ? v : v + b * y[i + j * n];
         }
+}
+
+// bf16 hi/lo planes of an FP32 plane.
+__global__ void k_split2(int64_t count, const float* __restrict__ x, __nv_bfloat16* __restrict__ hi,
+                         __nv_bfloat16* __restrict__ lo) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < count; k += (int64_t)gridDim.x * blockDim.x) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(x[k]);
+        hi[k] = h;
+        lo[k] = __float2bfloat16_rn(x[k] - __bfloat162float(h));
+    }
+}
+
+// y += x over FP32 planes.
+__global__ void k_add_f32(int64_t count, const float* __restrict__ x, float* __restrict__ y) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < count; k += (int64_t)gridDim.x * blockDim.x)
+        y[k] += x[k];
 }
 
 // Per-block partial traces of an FP32 plane (64 blocks, fixed order).
@@ -248,10 +269,11 @@ int grid1(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(n, 148
 // A tensor-core product bracketed by CUDA events on the launching stream; the
 // C-ABI layer sums the elapsed times per kind into the call's stats.
 void timed_product(ptbgpu_ctx* c, int epi, int np, int64_t ldp, const void* const* pa, const void* const* pb,
-                   const tc::ProdList& prods, const int2* tiles, int ntiles, const tc::EpiParams& ep) {
+                   const tc::ProdList& prods, const int2* tiles, int ntiles, const tc::EpiParams& ep,
+                   int kblock = 0) {
     cudaEvent_t a = c->take_event(), b = c->take_event();
     PTB_CUDA(cudaEventRecord(a, c->stream));
-    tc::launch_product(c->stream, epi, np, ldp, pa, pb, prods, tiles, ntiles, ep);
+    tc::launch_product(c->stream, epi, np, ldp, pa, pb, prods, tiles, ntiles, ep, kblock);
     PTB_CUDA(cudaEventRecord(b, c->stream));
     c->timed.push_back({epi == tc::EPI_SP2 ? 0 : 1, a, b});
 }
@@ -473,11 +495,14 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         const double e = std::fabs(si.err);
         hist.push_back(e);
         log_line(prl, 2, " SP2 (fp64 cleanup) %d  err %.3e", nclean, si.err);
+        // until the error reaches FP64 rounding or stops falling over two steps: a
+        // single SP2 step squares the deviation on one side of the spectrum but
+        // doubles it on the other, so a small error on entry is not enough
         if (e < 1e-13 * (double)n || (hist.size() > 2 && e >= hist[hist.size() - 3])) break;
     }
     nclean = std::min(nclean, 8);
-    double flops = (double)K * 3.0 * (double)n * n * n /*bf16x3, symmetric half*/ +
-                   (double)nclean * (double)n * n * n;
+    // algorithmic: every SP2 step is one symmetric square (n^3), pass 1 and cleanup alike
+    double flops = (double)K * (double)n * n * n + (double)nclean * (double)n * n * n;
 
     if (refine) {
         // C = A P~ - P~ A (FP64)
@@ -536,6 +561,49 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
             count_launch();
             PTB_CUDA(cudaGetLastError());
         }
+        // Keep only the blocks of X1 that couple occupied and virtual states of
+        // P~: X1_od = P~ X1 + X1 P~ - 2 P~ X1 P~ = W + W^T - 2 W P~ with W = P~ X1.
+        // The diagonal blocks of the computed X1 are rounding noise of the
+        // products; they would shift the energy at first order, X1_od only at
+        // second.  Both products are of a small quantity, so bf16x3 suffices.
+        {
+            const int a = K & 1, b = a ^ 1;
+            const void* pp2[2] = {phi, plo};
+            const void* px[2] = {x1hi[a], x1lo[a]};
+            timed_product(c, tc::EPI_FULL, 2, ldp, pp2, px, split3, tiles_all, (int)all.size(), epf);   // W
+            k_split2<<<grid1(ldp * ldp / 256), 256, 0, s>>>(ldp * ldp, wf, x1hi[b], x1lo[b]);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            tc::EpiParams epv = epf;
+            epv.out = x1f[b];
+            const void* pw[2] = {x1hi[b], x1lo[b]};
+            timed_product(c, tc::EPI_FULL, 2, ldp, pw, pp2, split3, tiles_all, (int)all.size(), epv);  // W P~
+            k_sym_update<<<dim3(nbp, nbp), dim3(32, 8), 0, s>>>(ldp, wf, x1f[b], 1.0f, -2.0f, x1f[a], x1hi[a],
+                                                                x1lo[a]);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            // Second-order idempotency term of the expansion: for a purely
+            // off-diagonal first-order part X1, (P~ + X1)^2 - (P~ + X1) = Y = X1^2
+            // (block diagonal, positive semi-definite), which lowers the energy at
+            // second order summed over all occupied states.  P2 = -(P~ Y + Y P~ - Y)
+            // removes it: X1 <- X1 + Y - (W2 + W2^T), W2 = P~ Y (traceless, small).
+            const void* px1[2] = {x1hi[a], x1lo[a]};
+            tc::EpiParams epy = epf;
+            epy.out = x1f[b];
+            timed_product(c, tc::EPI_FULL, 2, ldp, px1, px1, split3, tiles_all, (int)all.size(), epy);   // Y
+            k_split2<<<grid1(ldp * ldp / 256), 256, 0, s>>>(ldp * ldp, x1f[b], x1hi[b], x1lo[b]);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            const void* py[2] = {x1hi[b], x1lo[b]};
+            timed_product(c, tc::EPI_FULL, 2, ldp, pp2, py, split3, tiles_all, (int)all.size(), epf);    // W2
+            k_add_f32<<<grid1(ldp * ldp / 256), 256, 0, s>>>(ldp * ldp, x1f[a], x1f[b]);              // Y + X1
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            k_sym_update<<<dim3(nbp, nbp), dim3(32, 8), 0, s>>>(ldp, wf, x1f[b], -1.0f, 1.0f, x1f[a], x1hi[a],
+                                                                x1lo[a]);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+        }
         // P_o = P~ (1 - tau/N) + X1_K with tau = tr X1_K: the exact first-order
         // response is traceless; its bf16x3 rounding noise is removed from the
         // trace in FP64 along P~ (a uniform shift of the occupied eigenvalues by
@@ -553,7 +621,8 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         k_f2d<<<grid1(n), 256, 0, s>>>(n, ldp, x1f[K & 1], 1.0, 1.0 - tau / N, X);
         count_launch();
         PTB_CUDA(cudaGetLastError());
-        flops += 2.0 * (double)n * n * n /*FP64 commutator*/ + (double)(K + 1) * 3.0 * 2.0 * (double)n * n * n;
+        // algorithmic: FP64 commutator 2n^3, then K + 5 general products of 2n^3
+        flops += 2.0 * (double)n * n * n + (double)(K + 5) * 2.0 * (double)n * n * n;
         PTB_CUDA(cudaMemcpyAsync(&tmo, &c->flags->timeout, sizeof(int), cudaMemcpyDeviceToHost, s));
         PTB_CUDA(cudaStreamSynchronize(s));
         PTB_CHECK(tmo == 0, PTBGPU_ETIMEOUT, "tensor-core product gave up waiting (site %d)", tmo);
@@ -592,7 +661,7 @@ void tc_purify_entry(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, co
 
 // C = X X with the split-bf16 kernel (every tile, EPI_FULL) for kernel-level
 // tests: np = 2 planes (bf16x3 products) or 3 planes (bf16x6 products).
-void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, const double* hX, float* hC) {
+void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, int kblock, const double* hX, float* hC) {
     cudaStream_t s = c->stream;
     const int64_t ldp = round_up(n, tc::tile_n());
     const size_t plane = sizeof(__nv_bfloat16) * (size_t)ldp * ldp;
@@ -622,7 +691,8 @@ void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, const double* hX, float* hC) 
     ep.ld = ldp;
     ep.out = xf;   // the FP32 copy is consumed by the split above (stream order)
     const void* pl[3] = {hi, mid, lo};
-    timed_product(c, tc::EPI_FULL, np, ldp, pl, pl, np == 2 ? split3 : split6, bt.as<int2>(), (int)all.size(), ep);
+    timed_product(c, tc::EPI_FULL, np, ldp, pl, pl, np == 2 ? split3 : split6, bt.as<int2>(), (int)all.size(), ep,
+                  kblock);
     PTB_CUDA(cudaMemcpy2DAsync(hC, sizeof(float) * n, xf, sizeof(float) * ldp, sizeof(float) * n, n,
                                cudaMemcpyDeviceToHost, s));
     int tmo = 0;

@@ -11,11 +11,13 @@
 // operands carry about 24 significant bits ("bf16x6").
 //
 // One CTA computes a 128 x BN tile (cta_group::1, UMMA 128xBNx16); BN = 256
-// with two planes or BN = 128 with three planes, both 96 KB per stage:
-//   warp 0      TMA producer: per 64-wide K block, NP A tiles (128x64) and NP B
-//               tiles (BNx64) into a 2-stage ring, 128B-swizzled, completion
-//               on a "full" mbarrier with a transaction count;
-//   warp 1      MMA issuer (one thread): 4 K16 steps x the product list per
+// with two planes or BN = 128 with three planes.  K advances in blocks of KB:
+// 64 (128B swizzle, two 96 KB stages) or 32 (64B swizzle, four 48 KB stages);
+// the launcher times both on the first launch of a shape and keeps the faster.
+//   warp 0      TMA producer: per K block, NP A tiles (128xKB) and NP B tiles
+//               (BNxKB) into the stage ring, swizzled, completion on a "full"
+//               mbarrier with a transaction count;
+//   warp 1      MMA issuer (one thread): KB/16 K16 steps x the product list per
 //               stage, tcgen05.commit releases the stage on its "empty" mbarrier;
 //   warp 2      allocates / frees the BN TMEM columns of the accumulator;
 //   warps 4..7  epilogue: tcgen05.ld of their 32 lanes (rows), fused update.
@@ -36,7 +38,9 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
+#include <tuple>
 
 #include "common.cuh"
 #include "tc_gemm.cuh"
@@ -47,20 +51,28 @@ namespace tc {
 namespace {
 
 constexpr int BM = 128;
-constexpr int KB = 64;                        // K elements per stage (128 bytes of bf16)
-constexpr int STAGES = 2;
-constexpr int A_TILE_BYTES = BM * KB * 2;     // 16 KB
 constexpr int THREADS = 256;
+constexpr int kSmemBudget = 196608;   // operand ring (192 KB); barriers and alignment come on top
 
-template <int BN, int NP>
+// Tile configuration: BN output columns, NP operand planes, KB K elements per
+// stage.  KB = 64 rows are 128 bytes (128B swizzle, 1024-byte atoms); KB = 32
+// rows are 64 bytes (64B swizzle, 512-byte atoms).  The ring holds as many
+// stages as fit in the 192 KB budget: 2 for KB = 64, 4 for KB = 32.
+template <int BN, int NP, int KB>
 struct Cfg {
+    static constexpr int A_TILE_BYTES = BM * KB * 2;
     static constexpr int B_TILE_BYTES = BN * KB * 2;
     static constexpr int STAGE_BYTES = NP * (A_TILE_BYTES + B_TILE_BYTES);
+    static constexpr int STAGES = kSmemBudget / STAGE_BYTES;
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+    static constexpr uint32_t SWIZZLE_LAYOUT = KB == 64 ? 2u : 4u;      // UMMA layout type
+    static constexpr uint32_t SBO = KB == 64 ? 1024u : 512u;            // bytes between 8-row groups
     // Instruction descriptor for kind::f16: D fp32, A/B bf16, both K-major, M=128, N=BN.
     static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                                       ((uint32_t)(BM >> 4) << 24);
-    static_assert(STAGE_BYTES <= 98304, "stage larger than the 2-stage budget");
+    static_assert(KB == 64 || KB == 32, "K block of 64 or 32 elements");
+    static_assert(STAGES >= 2 && STAGES <= 4, "2..4 pipeline stages");
+    static_assert(STAGE_BYTES % 1024 == 0, "stages keep the swizzle atoms aligned");
 };
 constexpr uint64_t kTimeoutNs = 2000000000ull;
 
@@ -140,16 +152,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// UMMA shared-memory descriptor, K-major operand in the 128B-swizzle canonical
-// layout: rows of 128 bytes, 8-row (1024 B) swizzle atoms, SBO = 1024 B,
-// LBO unused (16 B), descriptor version 1, layout type 2 (SWIZZLE_128B).
-__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
+// UMMA shared-memory descriptor, K-major operand in a swizzled canonical
+// layout: start address, LBO unused for swizzled K-major (16 B), SBO = bytes
+// between 8-row groups (1024 for 128B swizzle, 512 for 64B), descriptor
+// version 1, layout type 2 (SWIZZLE_128B) or 4 (SWIZZLE_64B).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t sbo, uint32_t layout) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
     d |= (uint64_t)1u << 16;
-    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
     d |= (uint64_t)1u << 46;
-    d |= (uint64_t)2u << 61;
+    d |= (uint64_t)layout << 61;
     return d;
 }
 
@@ -165,13 +178,15 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& h, __nv_bfloa
 }
 
 // ---- the kernel -----------------------------------------------------------
-template <int EPI, int BN, int NP>
+template <int EPI, int BN, int NP, int KB>
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_product(const __grid_constant__ TmaPlanes maps, const ProdList prods, const int2* __restrict__ tiles,
                  int nk, EpiParams ep) {
     if (ep.active && *ep.active == 0) return;   // uniform early exit (converged iteration)
-    using C = Cfg<BN, NP>;
+    using C = Cfg<BN, NP, KB>;
     constexpr int STAGE_BYTES = C::STAGE_BYTES;
+    constexpr int STAGES = C::STAGES;
+    constexpr int A_TILE_BYTES = C::A_TILE_BYTES;
     constexpr int B_TILE_BYTES = C::B_TILE_BYTES;
 
     extern __shared__ uint8_t smem_raw[];
@@ -256,8 +271,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
             for (int k = 0; k < KB / 16; ++k) {
                 for (int p = 0; p < prods.n; ++p) {
-                    const uint64_t ad = sdesc_sw128(a_tile(s, prods.a[p]) + k * 32);
-                    const uint64_t bd = sdesc_sw128(b_tile(s, prods.b[p]) + k * 32);
+                    const uint64_t ad = sdesc(a_tile(s, prods.a[p]) + k * 32, C::SBO, C::SWIZZLE_LAYOUT);
+                    const uint64_t bd = sdesc(b_tile(s, prods.b[p]) + k * 32, C::SBO, C::SWIZZLE_LAYOUT);
                     umma_bf16(tmem, ad, bd, C::IDESC, (kb | k | p) != 0);
                 }
             }
@@ -304,7 +319,10 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                     for (int j8 = 0; j8 < 4; ++j8) {
                         float val[8];
-                        const float4 x0 = xin[2 * j8], x1 = xin[2 * j8 + 1];
+                        // X is only needed for 2X - X^2: skip its read on the square branch
+                        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                        const float4 x0 = square ? zero4 : xin[2 * j8];
+                        const float4 x1 = square ? zero4 : xin[2 * j8 + 1];
                         const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
                         __align__(16) __nv_bfloat16 hh[8], mm[8], ll[8];
 #pragma unroll
@@ -400,15 +418,16 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     return fn;
 }
 
-void encode_plane(CUtensorMap* map, const void* plane, int64_t ld, int box_rows) {
+void encode_plane(CUtensorMap* map, const void* plane, int64_t ld, int box_rows, int kb) {
     PTB_CHECK(((uintptr_t)plane & 15) == 0, PTBGPU_EINVAL, "operand plane not 16-byte aligned");
     PTB_CHECK(ld % 256 == 0, PTBGPU_EINVAL, "operand leading dimension must be a multiple of 256");
     cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)ld};
     cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-    cuuint32_t box[2] = {(cuuint32_t)KB, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)kb, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
+    const CUtensorMapSwizzle sw = kb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
     CUresult r = get_encode()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(plane), dims,
-                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     PTB_CHECK(r == CUDA_SUCCESS, PTBGPU_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
 }
@@ -431,42 +450,89 @@ std::vector<int2> make_tiles(long long ld, bool upper_only, int bn) {
 }
 
 namespace {
-template <int EPI, int BN, int NP>
+template <int EPI, int BN, int NP, int KB>
 void launch_t(cudaStream_t s, const TmaPlanes& maps, const ProdList& prods, const int2* tiles, int ntiles, int nk,
               const EpiParams& ep) {
+    using C = Cfg<BN, NP, KB>;
     static bool attr = false;
     if (!attr) {
-        PTB_CUDA(cudaFuncSetAttribute(k_tc_product<EPI, BN, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      Cfg<BN, NP>::SMEM_BYTES));
+        PTB_CUDA(cudaFuncSetAttribute(k_tc_product<EPI, BN, NP, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      C::SMEM_BYTES));
         attr = true;
     }
-    k_tc_product<EPI, BN, NP><<<ntiles, THREADS, Cfg<BN, NP>::SMEM_BYTES, s>>>(maps, prods, tiles, nk, ep);
+    k_tc_product<EPI, BN, NP, KB><<<ntiles, THREADS, C::SMEM_BYTES, s>>>(maps, prods, tiles, nk, ep);
     count_launch();
 }
+
+template <int EPI>
+void launch_epi(cudaStream_t s, int np, int kb, const TmaPlanes& maps, const ProdList& prods, const int2* tiles,
+                int ntiles, int nk, const EpiParams& ep) {
+    if (np == 2) {
+        if (kb == 64) launch_t<EPI, 256, 2, 64>(s, maps, prods, tiles, ntiles, nk, ep);
+        else launch_t<EPI, 256, 2, 32>(s, maps, prods, tiles, ntiles, nk, ep);
+    } else {
+        if (kb == 64) launch_t<EPI, 128, 3, 64>(s, maps, prods, tiles, ntiles, nk, ep);
+        else launch_t<EPI, 128, 3, 32>(s, maps, prods, tiles, ntiles, nk, ep);
+    }
+}
+
+// Autotuned K-block choice per (device, epilogue, planes, leading dimension):
+// the first launch of a shape runs both variants back to back (same inputs,
+// same outputs, so running twice is harmless), times them with CUDA events
+// and keeps the faster for the rest of the process.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, long long>, int> g_tuned;
 }  // namespace
 
+int tuned_kblock(int epi, int np, long long ld) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(std::make_tuple(dev, epi, np, ld));
+    return it == g_tuned.end() ? 0 : it->second;
+}
+
 void launch_product(cudaStream_t s, int epi, int np, long long ld, const void* const* a, const void* const* b,
-                    const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep) {
+                    const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep, int kblock) {
     PTB_CHECK(np == 2 || np == 3, PTBGPU_EINVAL, "unsupported plane count %d", np);
+    PTB_CHECK(kblock == 0 || kblock == 32 || kblock == 64, PTBGPU_EINVAL, "K block must be 0, 32 or 64");
     const int bn = np == 2 ? 256 : 128;
     for (int p = 0; p < prods.n; ++p)
         PTB_CHECK(prods.a[p] < np && prods.b[p] < np, PTBGPU_EINVAL, "product references a missing plane");
     PTB_CHECK(epi != EPI_SP2 || (ep.lo2 != nullptr && ep.lo != nullptr), PTBGPU_EINVAL,
               "the SP2 epilogue writes three planes");
-    TmaPlanes maps;
-    for (int p = 0; p < np; ++p) {
-        encode_plane(&maps.a[p], a[p], ld, BM);
-        encode_plane(&maps.b[p], b[p], ld, bn);
+    auto run = [&](int kb) {
+        TmaPlanes maps;
+        for (int p = 0; p < np; ++p) {
+            encode_plane(&maps.a[p], a[p], ld, BM, kb);
+            encode_plane(&maps.b[p], b[p], ld, bn, kb);
+        }
+        const int nk = (int)(ld / kb);
+        if (epi == EPI_SP2) launch_epi<EPI_SP2>(s, np, kb, maps, prods, tiles_dev, ntiles, nk, ep);
+        else launch_epi<EPI_FULL>(s, np, kb, maps, prods, tiles_dev, ntiles, nk, ep);
+        PTB_CUDA(cudaGetLastError());
+    };
+    if (kblock == 0) kblock = tuned_kblock(epi, np, ld);
+    if (kblock != 0) {
+        run(kblock);
+        return;
     }
-    const int nk = (int)(ld / KB);
-    if (epi == EPI_SP2) {
-        if (np == 2) launch_t<EPI_SP2, 256, 2>(s, maps, prods, tiles_dev, ntiles, nk, ep);
-        else launch_t<EPI_SP2, 128, 3>(s, maps, prods, tiles_dev, ntiles, nk, ep);
-    } else {
-        if (np == 2) launch_t<EPI_FULL, 256, 2>(s, maps, prods, tiles_dev, ntiles, nk, ep);
-        else launch_t<EPI_FULL, 128, 3>(s, maps, prods, tiles_dev, ntiles, nk, ep);
-    }
-    PTB_CUDA(cudaGetLastError());
+    cudaEvent_t e[3];
+    for (auto& x : e) PTB_CUDA(cudaEventCreate(&x));
+    PTB_CUDA(cudaEventRecord(e[0], s));
+    run(64);
+    PTB_CUDA(cudaEventRecord(e[1], s));
+    run(32);
+    PTB_CUDA(cudaEventRecord(e[2], s));
+    PTB_CUDA(cudaEventSynchronize(e[2]));
+    float t64 = 0.f, t32 = 0.f;
+    PTB_CUDA(cudaEventElapsedTime(&t64, e[0], e[1]));
+    PTB_CUDA(cudaEventElapsedTime(&t32, e[1], e[2]));
+    for (auto& x : e) cudaEventDestroy(x);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned[std::make_tuple(dev, epi, np, ld)] = t32 < t64 ? 32 : 64;
 }
 
 }  // namespace tc

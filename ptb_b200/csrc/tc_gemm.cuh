@@ -40,8 +40,11 @@ struct EpiParams {
 // Two-plane products run on 128 x 256 tiles, three-plane products on 128 x 128.
 int tile_n();
 std::vector<int2> make_tiles(long long ld, bool upper_only, int bn);
+// kblock: 64 (128B swizzle, 2 stages), 32 (64B swizzle, 4 stages) or 0 = the
+// autotuned choice for this shape (both are timed on its first launch).
 void launch_product(cudaStream_t s, int epi, int np, long long ld, const void* const* a, const void* const* b,
-                    const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep);
+                    const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep, int kblock = 0);
+int tuned_kblock(int epi, int np, long long ld);   // 0 until the shape has been tuned
 
 }  // namespace tc
 }  // namespace ptb

@@ -47,6 +47,21 @@ def test_symsq_bf16x3_matches_emulation(ctx, n):
     assert np.max(np.abs(C - X @ X)) <= 1e-4 * scale
 
 
+@pytest.mark.parametrize("planes", [2, 3])
+@pytest.mark.parametrize("kblock", [32, 64])
+def test_symsq_both_k_blocks(ctx, planes, kblock):
+    """Both K-block variants of the kernel (64B / 128B swizzle) give the same product."""
+    n = 520
+    rng = np.random.default_rng(7)
+    A = rng.uniform(-1, 1, (n, n))
+    X = 0.5 * (A + A.T)
+    C = ctx.symsq_split(X, planes, kblock).astype(np.float64)
+    ref = ctx.symsq_split(X, planes, 64 if kblock == 32 else 32).astype(np.float64)
+    bound = 2 * n * 2.0 ** -24 * (np.abs(X) @ np.abs(X)) + 1e-30
+    assert np.all(np.abs(C - ref) <= bound)
+    assert np.max(np.abs(C - X @ X)) <= 1e-4 * np.max(np.abs(X @ X))
+
+
 @pytest.mark.parametrize("n", [200, 512, 640])
 def test_symsq_bf16x6_three_plane_split(ctx, n):
     rng = np.random.default_rng(n + 1)
