@@ -84,6 +84,10 @@ typedef struct {
     double  glob_par17;
     int64_t split3_iters;       /* PREC_MIXED: leading iterations whose products use the
                                    three-plane bf16 split (~24 bits); 0 = all, -1 = none */
+    int64_t fp64_slices;        /* PREC_MIXED: 6..8 -> the FP64 products around the purification
+                                   (orthogonalisation, cleanup, commutator, back-transform) run on
+                                   the int8 tensor cores with that many 7-bit slices per operand;
+                                   0 -> cuBLAS/cuSOLVER FP64 */
 } ptbgpu_opts;
 
 /* What a call reports back (all optional for the caller). */
@@ -109,6 +113,8 @@ typedef struct {
     double  ms_tc_full;         /* summed device time of the general tensor-core products */
     int64_t n_tc_full;
     int64_t kernel_launches;    /* launches of this library's own kernels in the call */
+    double  ms_oz;              /* summed device time of the int8-sliced FP64 products */
+    int64_t n_oz;
 } ptbgpu_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */
@@ -197,6 +203,15 @@ int ptbgpu_symsq_bf16x6(ptbgpu_ctx* ctx, int64_t n, const double* X, float* C);
 /* Either split with an explicit K block of the kernel: planes 2 or 3, kblock 32,
  * 64 or 0 (the autotuned choice). */
 int ptbgpu_symsq_split(ptbgpu_ctx* ctx, int64_t n, int64_t planes, int64_t kblock, const double* X, float* C);
+/* C = A * B for n x n FP64 row-major host matrices, on the int8 tensor cores
+ * with `slices` (6..8) 7-bit slices per operand row and an int32-exact K loop;
+ * kblock 32 or 64 bytes (0 = default).  tri_a / tri_b: 0 full, 1 lower, 2 upper
+ * triangular (the other part is read as zero and its K blocks are skipped);
+ * symmetric != 0: only the upper triangle of C is computed and mirrored.
+ * n <= (2^31 - 1) / (slices * 127^2) rounded down to a multiple of 128.
+ * ms (may be NULL) receives the device time of the product kernel. */
+int ptbgpu_oz_gemm(ptbgpu_ctx* ctx, int64_t n, int64_t slices, int64_t kblock, int64_t tri_a, int64_t tri_b,
+                   int64_t symmetric, const double* A, const double* B, double* C, double* ms);
 
 #ifdef __cplusplus
 }

@@ -48,7 +48,8 @@ class _Settings(C.Structure):
 class _Opts(C.Structure):
     _fields_ = [("filter", C.c_double), ("precision", C.c_int64), ("print_level", C.c_int64),
                 ("max_iter", C.c_int64), ("electronic_temp", C.c_double), ("glob_par15", C.c_double),
-                ("glob_par17", C.c_double), ("split3_iters", C.c_int64)]
+                ("glob_par17", C.c_double), ("split3_iters", C.c_int64),
+                ("fp64_slices", C.c_int64)]
 
 
 class _Stats(C.Structure):
@@ -58,14 +59,15 @@ class _Stats(C.Structure):
                 ("mu_iterations", C.c_int64), ("info", C.c_int64), ("ms_total", C.c_double),
                 ("ms_h2d", C.c_double), ("ms_solve", C.c_double), ("ms_d2h", C.c_double), ("flops", C.c_double),
                 ("ms_tc_sp2", C.c_double), ("n_tc_sp2", C.c_int64), ("ms_tc_full", C.c_double),
-                ("n_tc_full", C.c_int64), ("kernel_launches", C.c_int64)]
+                ("n_tc_full", C.c_int64), ("kernel_launches", C.c_int64), ("ms_oz", C.c_double),
+                ("n_oz", C.c_int64)]
 
 
 EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_default_settings",
             "ptbgpu_default_opts", "ptbgpu_filter_packed", "ptbgpu_check_density", "ptbgpu_sm_density",
             "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_solve2",
             "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_symsq_split", "ptbgpu_runtime_info",
-            "ptbgpu_density_traces_noalloc")
+            "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm")
 
 
 def library_path() -> Path:
@@ -108,6 +110,7 @@ def load_library():
     lib.ptbgpu_symsq_bf16x3.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_bf16x6.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_split.argtypes = [C.c_void_p, i64, i64, i64, d, P(C.c_float)]
+    lib.ptbgpu_oz_gemm.argtypes = [C.c_void_p, i64, i64, i64, i64, i64, i64, d, d, d, d]
     lib.ptbgpu_runtime_info.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     lib.ptbgpu_density_traces_noalloc.argtypes = [C.c_int, i64, C.c_void_p, C.c_void_p, C.c_void_p, d,
                                                   C.c_void_p, C.c_char_p, C.c_size_t]
@@ -158,6 +161,8 @@ class Stats:
     ms_tc_full: float = 0.0
     n_tc_full: int = 0
     kernel_launches: int = 0
+    ms_oz: float = 0.0
+    n_oz: int = 0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "Stats":
@@ -175,10 +180,11 @@ class Options:
     glob_par15: float = 0.0
     glob_par17: float = 0.0
     split3_iters: int = 8
+    fp64_slices: int = 8
 
     def to_c(self) -> _Opts:
         return _Opts(self.filter, self.precision, self.print_level, self.max_iter, self.electronic_temp,
-                     self.glob_par15, self.glob_par17, self.split3_iters)
+                     self.glob_par15, self.glob_par17, self.split3_iters, self.fp64_slices)
 
 
 class Context:
@@ -311,6 +317,21 @@ class Context:
     def symsq_split(self, X: np.ndarray, planes: int, kblock: int) -> np.ndarray:
         """C = X X with an explicit plane count (2 or 3) and kernel K block (32, 64, 0 = tuned)."""
         return self._symsq(X, lambda h, n, x, o: self._lib.ptbgpu_symsq_split(h, n, planes, kblock, x, o))
+
+    def oz_gemm(self, A: np.ndarray, B: np.ndarray, slices: int = 7, kblock: int = 0, tri_a: int = 0,
+                tri_b: int = 0, symmetric: bool = False, timed: bool = False):
+        """C = A B in FP64 on the int8 tensor cores (slices 6..8 per operand row);
+        tri_*: 0 full, 1 lower, 2 upper triangular operand; symmetric: only the
+        upper triangle of C is computed and mirrored.  timed: returns (C, device
+        milliseconds of the product kernel)."""
+        Ah, Bh = _f64(A), _f64(B)
+        n = Ah.shape[0]
+        out = np.zeros((n, n), dtype=np.float64)
+        ms = C.c_double(0.0)
+        self._check(self._lib.ptbgpu_oz_gemm(self._h, int(n), int(slices), int(kblock), int(tri_a), int(tri_b),
+                                             int(bool(symmetric)), _dptr(Ah), _dptr(Bh), _dptr(out),
+                                             C.byref(ms)))
+        return (out, ms.value) if timed else out
 
     def _symsq(self, X, fn):
         Xh = _f64(X)

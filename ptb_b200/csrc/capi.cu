@@ -9,6 +9,8 @@ namespace ptb {
 void tc_purify_entry(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, const double* dS, double* dP,
                      const ptbgpu_opts* o, ptbgpu_stats* st);
 void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, int kblock, const double* hX, float* hC);
+void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int tri_a, int tri_b, bool sym, const double* hA,
+                   const double* hB, double* hC);
 void purify_ref_device(ptbgpu_ctx* c, const ptbgpu_pur_settings& pur, int64_t n, const double* dH,
                        const double* dS, double* dP, const ptbgpu_opts* o, ptbgpu_stats* st);
 void solve2_device(ptbgpu_ctx* c, int64_t mode, int64_t n, int64_t nel, int64_t nopen, const double* dH,
@@ -93,6 +95,9 @@ struct PhaseTimer {
             if (t.kind == 0) {
                 st->ms_tc_sp2 += ms;
                 st->n_tc_sp2 += 1;
+            } else if (t.kind == 2) {
+                st->ms_oz += ms;
+                st->n_oz += 1;
             } else {
                 st->ms_tc_full += ms;
                 st->n_tc_full += 1;
@@ -237,6 +242,25 @@ int ptbgpu_symsq_split(ptbgpu_ctx* c, int64_t n, int64_t planes, int64_t kblock,
         PTB_CHECK(n > 0 && X && C && (planes == 2 || planes == 3) && (kblock == 0 || kblock == 32 || kblock == 64),
                   PTBGPU_EINVAL, "bad arguments");
         symsq_entry(c, n, (int)planes, (int)kblock, X, C);
+    });
+}
+
+int ptbgpu_oz_gemm(ptbgpu_ctx* c, int64_t n, int64_t slices, int64_t kblock, int64_t tri_a, int64_t tri_b,
+                   int64_t symmetric, const double* A, const double* B, double* Cout, double* ms) {
+    return guarded(c, [&] {
+        PTB_CHECK(n > 0 && A && B && Cout && slices >= 6 && slices <= 8 &&
+                      (kblock == 0 || kblock == 32 || kblock == 64) && tri_a >= 0 && tri_a <= 2 && tri_b >= 0 &&
+                      tri_b <= 2,
+                  PTBGPU_EINVAL, "bad arguments");
+        oz_gemm_entry(c, n, (int)slices, (int)kblock, (int)tri_a, (int)tri_b, symmetric != 0, A, B, Cout);
+        if (ms) {
+            *ms = 0.0;
+            for (const auto& t : c->timed) {
+                float x = 0.f;
+                PTB_CUDA(cudaEventElapsedTime(&x, t.a, t.b));
+                *ms += x;
+            }
+        }
     });
 }
 

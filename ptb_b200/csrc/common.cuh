@@ -93,7 +93,7 @@ struct ptbgpu_ctx {
     std::vector<cudaEvent_t> evpool;
     size_t evused = 0;
     struct Timed {
-        int kind;            // 0 SP2 product, 1 general product
+        int kind;            // 0 SP2 product, 1 general product, 2 int8-sliced FP64 product
         cudaEvent_t a, b;
     };
     std::vector<Timed> timed;
@@ -112,6 +112,8 @@ enum BufId {
     B_X1HI, B_X1LO,                                   // bf16 planes of the DMPT response
     B_STATS, B_TILES, B_SOLVER_WS, B_MISC0, B_MISC1, B_MISC2, B_MISC3,
     B_SM0, B_SM1, B_SM2, B_SM3, B_SM4, B_SM5, B_SM6, B_SM7,
+    B_OZ0, B_OZ1, B_OZE0, B_OZE1, B_OZR, B_OZT, B_OZS,  // int8 slices, row exponents, scratch of the
+                                                        // emulated FP64 products
     B_COUNT
 };
 

@@ -169,6 +169,7 @@ void ptbgpu_default_opts(ptbgpu_opts* o) {
     o->max_iter = 100;
     o->electronic_temp = 300.0;
     o->split3_iters = 8;
+    o->fp64_slices = 8;
 }
 
 }  // extern "C"

@@ -455,6 +455,49 @@ int dpotrf_lower(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A) {
     return info;
 }
 
+namespace {
+// cuSOLVER trtri on one diagonal block (lower, in place).
+void trtri_block(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A) {
+    size_t wd = 0, wh = 0;
+    PTB_CUSOLVER(cusolverDnXtrtri_bufferSize(c->solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, n, CUDA_R_64F,
+                                             A, ld, &wd, &wh));
+    DevBuf& ws = c->buf(B_SOLVER_WS);
+    ws.reserve(std::max<size_t>(wd, 8));
+    std::vector<char> hw(std::max<size_t>(wh, 8));
+    PTB_CUSOLVER(cusolverDnXtrtri(c->solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, n, CUDA_R_64F, A, ld,
+                                  ws.ptr, wd, hw.data(), wh, c->info_dev));
+    int info = 0;
+    PTB_CUDA(cudaMemcpyAsync(&info, c->info_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    PTB_CUDA(cudaStreamSynchronize(c->stream));
+    PTB_CHECK(info == 0, PTBGPU_ENOTSPD, "triangular inverse failed (trtri info=%d)", info);
+}
+
+// Recursive halving: for L = [L11 0; L21 L22], L^-1 = [L11^-1 0; -L22^-1 L21 L11^-1  L22^-1].
+// The off-diagonal block takes two triangular products (cuBLAS trmm, in place),
+// so the n^3/3 flops run at product speed; blocks of <= 1024 go to cuSOLVER.
+void trtri_rec(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A) {
+    if (n <= 1024) {
+        trtri_block(c, n, ld, A);
+        return;
+    }
+    const int64_t n1 = (n / 2 + 127) / 128 * 128, n2 = n - n1;
+    double* L11 = A;
+    double* L21 = A + n1;
+    double* L22 = A + n1 + n1 * ld;
+    trtri_rec(c, n1, ld, L11);
+    trtri_rec(c, n2, ld, L22);
+    const double one = 1.0, mone = -1.0;
+    PTB_CUBLAS(cublasDtrmm(c->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                           (int)n2, (int)n1, &one, L11, (int)ld, L21, (int)ld, L21, (int)ld));
+    PTB_CUBLAS(cublasDtrmm(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                           (int)n2, (int)n1, &mone, L22, (int)ld, L21, (int)ld, L21, (int)ld));
+}
+}  // namespace
+
+// In-place inverse of the lower triangle of A (column-major); the strict upper
+// triangle is not referenced.
+void dtrtri_lower(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A) { trtri_rec(c, n, ld, A); }
+
 void dsyevd(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A, double* w) {
     int lwork = 0;
     PTB_CUSOLVER(cusolverDnDsyevd_bufferSize(c->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER,

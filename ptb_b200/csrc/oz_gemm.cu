@@ -1,0 +1,490 @@
+// FP64 products on the int8 tensor cores (tcgen05 kind::i8, int32 in tensor
+// memory): Ozaki-scheme slicing of the operands and the product kernel.
+//
+// Product kernel, one CTA per 128 x 64 output tile (cta_group::1):
+//   warp 0      TMA producer: per K block of RB bytes, the S A-slices (128 x RB)
+//               and the S B-slices (64 x RB) into a ring of stages (64B or 32B
+//               swizzle), completion on a "full" mbarrier with a byte count;
+//   warp 1      MMA issuer: for every K32 step, the S(S+1)/2 slice pairs
+//               (p, q), p + q <= S - 1, as UMMA 128x64x32 int8 into
+//               accumulator p + q (tensor-memory columns (p + q) * 64 ..);
+//               tcgen05.commit frees the stage;
+//   warp 2      allocates / frees 512 tensor-memory columns;
+//   warps 4..7  epilogue: per row, sum_g 2^(-7(g+2)) G_g in FP64 (smallest
+//               group first), times 2^(e_i + f_j), then the fused output.
+// The int32 sums are exact: a group has at most S pairs of |s| <= 127 terms, so
+// K <= (2^31 - 1) / (S * 127^2) (19020 for S = 7) never overflows.
+//
+// Every mbarrier wait is bounded (2 s); on expiry the CTA records an error
+// site, drains its copies and frees its tensor memory.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "common.cuh"
+#include "oz_gemm.cuh"
+#include "tc_ptx.cuh"
+
+namespace ptb {
+namespace oz {
+
+namespace {
+
+using namespace tc::ptx;
+
+constexpr int THREADS = 256;
+constexpr int kSmemBudget = 196608;
+constexpr int kTmemCols = 512;
+
+template <int S, int RB>
+struct OzCfg {
+    static constexpr int A_TILE = BM * RB;
+    static constexpr int B_TILE = BN * RB;
+    static constexpr int STAGE = S * (A_TILE + B_TILE);
+    static constexpr int STAGES = (kSmemBudget / STAGE) > 4 ? 4 : (kSmemBudget / STAGE);
+    static constexpr int SMEM = STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+    static constexpr uint32_t LAYOUT = RB == 64 ? 4u : 6u;   // SWIZZLE_64B / SWIZZLE_32B
+    static constexpr uint32_t SBO = 8u * RB;                  // bytes between 8-row groups
+    // kind::i8: D s32 (2), A and B signed int8 (1), both K-major, N = 64, M = 128
+    static constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                      ((uint32_t)(BM >> 4) << 24);
+    static_assert(RB == 64 || RB == 32, "64- or 32-byte K blocks");
+    static_assert(S >= 2 && S * BN <= kTmemCols, "S accumulators of 64 columns fit in tensor memory");
+    static_assert(STAGES >= 2, "at least two pipeline stages");
+    static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0, "tiles keep the swizzle atoms aligned");
+};
+
+// 2^e as a double for -1022 <= e <= 1023 (IEEE-754 exponent field).
+__device__ __forceinline__ double pow2i(int e) {
+    return __longlong_as_double((long long)(e + 1023) << 52);
+}
+// x * 2^e for |e| <= 2044, exact while the result is a normal number
+__device__ __forceinline__ double scale2(double x, int e) {
+    const int h = e / 2;
+    return x * pow2i(h) * pow2i(e - h);
+}
+
+// ---- slicing ---------------------------------------------------------------
+__device__ __forceinline__ bool tri_keep(int tri, int64_t i, int64_t k) {
+    return tri == TRI_NONE || (tri == TRI_LOWER ? k <= i : k >= i);
+}
+
+// Row maxima of |M(i,k)| over a 32-row x 128-column tile, merged with
+// atomicMax on the bit patterns (order-preserving for non-negative doubles).
+__global__ void k_oz_rowmax(const double* __restrict__ M, int64_t rs, int64_t cs, int64_t n, int tri,
+                            unsigned long long* __restrict__ rowmax) {
+    const int64_t i0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 128;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (cs == 1) {
+        // rows contiguous: each warp takes 4 rows, lanes run along k
+        for (int rr = 0; rr < 4; ++rr) {
+            const int64_t i = i0 + w * 4 + rr;
+            double m = 0.0;
+            if (i < n) {
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int64_t k = k0 + lane + 32 * t;
+                    if (k < n && tri_keep(tri, i, k)) m = fmax(m, fabs(M[i * rs + k]));
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0 && i < n && m > 0.0) atomicMax(&rowmax[i], (unsigned long long)__double_as_longlong(m));
+        }
+    } else {
+        // columns contiguous: lanes run along i, warps along k
+        __shared__ double red[8][33];
+        const int64_t i = i0 + lane;
+        double m = 0.0;
+        if (i < n) {
+            for (int t = 0; t < 16; ++t) {
+                const int64_t k = k0 + w + 8 * t;
+                if (k < n && tri_keep(tri, i, k)) m = fmax(m, fabs(M[i + k * cs]));
+            }
+        }
+        red[w][lane] = m;
+        __syncthreads();
+        if (w == 0) {
+            for (int t = 1; t < 8; ++t) m = fmax(m, red[t][lane]);
+            if (i < n && m > 0.0) atomicMax(&rowmax[i], (unsigned long long)__double_as_longlong(m));
+        }
+    }
+}
+
+// Slices of a 32-row x 64-column tile; rows/columns beyond n (the padding up
+// to ldp) are written as zero.  e_i: |M(i,k)| < 2^e_i, taken from the
+// exponent field of the row maximum.
+template <int S>
+__global__ void k_oz_slice(const double* __restrict__ M, int64_t rs, int64_t cs, int64_t n, int tri,
+                           const unsigned long long* __restrict__ rowmax, int8_t* __restrict__ planes,
+                           int* __restrict__ exps, int64_t ldp) {
+    __shared__ double t[32][65];
+    const int64_t i0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 64;
+    if (cs == 1) {
+        for (int e = threadIdx.x; e < 32 * 64; e += THREADS) {
+            const int r = e >> 6, kk = e & 63;
+            const int64_t i = i0 + r, k = k0 + kk;
+            t[r][kk] = (i < n && k < n && tri_keep(tri, i, k)) ? M[i * rs + k] : 0.0;
+        }
+    } else {
+        for (int e = threadIdx.x; e < 32 * 64; e += THREADS) {
+            const int r = e & 31, kk = e >> 5;
+            const int64_t i = i0 + r, k = k0 + kk;
+            t[r][kk] = (i < n && k < n && tri_keep(tri, i, k)) ? M[i + k * cs] : 0.0;
+        }
+    }
+    __syncthreads();
+    const int r = threadIdx.x >> 3, kq = (threadIdx.x & 7) * 8;
+    const int64_t i = i0 + r;
+    int e = 0;
+    if (i < n) {
+        const unsigned long long b = rowmax[i];
+        if (b != 0ull) {
+            const int fld = (int)((b >> 52) & 0x7FF);
+            e = fld == 0 ? -1022 : fld - 1022;   // max = m 2^e, 0.5 <= m < 1 (subnormal: max < 2^-1022)
+        }
+    }
+    if (blockIdx.x == 0 && (threadIdx.x & 7) == 0) exps[i] = e;
+    const double sc = pow2i(-e);
+    uint32_t w[S][2];
+#pragma unroll
+    for (int p = 0; p < S; ++p) w[p][0] = w[p][1] = 0u;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        double x = t[r][kq + j] * sc;   // |x| < 1
+#pragma unroll
+        for (int p = 0; p < S; ++p) {
+            x *= 128.0;
+            const double q = trunc(x);   // |q| <= 127
+            x -= q;                      // exact: the fraction of x
+            const uint32_t byte = (uint32_t)(uint8_t)(int8_t)(int)q;
+            w[p][j >> 2] |= byte << (8 * (j & 3));
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < S; ++p)
+        *reinterpret_cast<uint2*>(planes + ((int64_t)p * ldp + i) * ldp + k0 + kq) = make_uint2(w[p][0], w[p][1]);
+}
+
+// ---- product ---------------------------------------------------------------
+struct OzMaps {
+    CUtensorMap a;   // S stacked A planes
+    CUtensorMap b;   // S stacked B planes
+};
+
+template <int EPI, int S, int RB>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_oz_product(const __grid_constant__ OzMaps maps, const int4* __restrict__ tiles, const int* __restrict__ ea,
+                 const int* __restrict__ eb, OzEpi ep) {
+    using C = OzCfg<S, RB>;
+    constexpr int STAGE = C::STAGE;
+    constexpr int STAGES = C::STAGES;
+
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t base_raw = smem_u32(smem_raw);
+    const uint32_t base = (base_raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - base_raw);
+    const uint32_t bar0 = base + STAGES * STAGE;
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+    const uint32_t accum_bar = bar0 + 8u * (2 * STAGES);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + STAGES * STAGE + 8 * (2 * STAGES + 1));
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+    double* red = reinterpret_cast<double*>(gbase + STAGES * STAGE + 128);   // 8 doubles
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int4 tile = tiles[blockIdx.x];
+    const int bi = tile.x, bj = tile.y;
+    const int kb0 = tile.z / RB;
+    const int nk = (tile.w - tile.z) / RB;
+
+    auto a_tile = [&](int s, int p) { return base + s * STAGE + p * C::A_TILE; };
+    auto b_tile = [&](int s, int q) { return base + s * STAGE + S * C::A_TILE + q * C::B_TILE; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(accum_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"((uint32_t)kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer ----------------
+        int issued_phase[STAGES];
+        for (int s = 0; s < STAGES; ++s) issued_phase[s] = -1;
+        for (int it = 0; it < nk; ++it) {
+            const int s = it % STAGES, round = it / STAGES;
+            if (round > 0 && !mbar_wait(empty_bar(s), (round - 1) & 1)) {
+                set_err(ep.err, 111);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            mbar_expect_tx(full_bar(s), STAGE);
+            const int kx = (kb0 + it) * RB;
+            for (int p = 0; p < S; ++p)
+                tma_load_2d(a_tile(s, p), &maps.a, full_bar(s), kx, (int)(p * ep.ldp) + bi * BM);
+            for (int q = 0; q < S; ++q)
+                tma_load_2d(b_tile(s, q), &maps.b, full_bar(s), kx, (int)(q * ep.ldp) + bj * BN);
+            issued_phase[s] = round & 1;
+        }
+        for (int s = 0; s < STAGES; ++s)
+            if (issued_phase[s] >= 0 && !mbar_wait(full_bar(s), (uint32_t)issued_phase[s])) set_err(ep.err, 112);
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer ----------------
+        bool ok = true;
+        for (int it = 0; it < nk; ++it) {
+            const int s = it % STAGES, round = it / STAGES;
+            if (!mbar_wait(full_bar(s), round & 1)) {
+                set_err(ep.err, 121);
+                *(volatile int*)abort_flag = 1;
+                ok = false;
+                break;
+            }
+            if (*(volatile int*)abort_flag) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+#pragma unroll
+            for (int k = 0; k < RB / 32; ++k) {
+#pragma unroll
+                for (int p = 0; p < S; ++p) {
+                    const uint64_t ad = sdesc(a_tile(s, p) + k * 32, C::SBO, C::LAYOUT);
+#pragma unroll
+                    for (int q = 0; q < S - p; ++q) {
+                        const uint64_t bd = sdesc(b_tile(s, q) + k * 32, C::SBO, C::LAYOUT);
+                        // p = 0 opens every accumulator on the first K step; the rest add
+                        umma_i8(tmem + (uint32_t)((p + q) * BN), ad, bd, C::IDESC, (it | k | p) != 0);
+                    }
+                }
+            }
+            umma_commit(empty_bar(s));
+        }
+        umma_commit(accum_bar);
+        if (!ok) mbar_wait(accum_bar, 0);
+    } else if (warp >= 4) {
+        // ---------------- epilogue ----------------
+        const int q4 = warp - 4;
+        const int64_t n = ep.n;
+        const int64_t r = (int64_t)bi * BM + q4 * 32 + lane;
+        double tr = 0.0, ss = 0.0;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(accum_bar, 0));
+        if (!ok && lane == 0) {
+            set_err(ep.err, 131);
+            *(volatile int*)abort_flag = 1;
+        }
+        const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
+        tc_fence_after();
+        if (ok && !aborted) {
+            const int er = r < n ? ea[r] : 0;
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                double acc[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+#pragma unroll 1
+                for (int g = S - 1; g >= 0; --g) {
+                    uint32_t v[32];
+                    __syncwarp();
+                    tmem_ld32(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(g * BN + c0), v);
+                    const double w = pow2i(-7 * (g + 2));
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[j] += (double)(int)v[j] * w;
+                }
+                if (nk == 0) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                }
+                if (r >= n) continue;
+                const int64_t cb = (int64_t)bj * BN + c0;
+                if (EPI == OZ_OUT) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int64_t c = cb + j;
+                        if (c < n) ep.out[r * ep.ors + c * ep.ocs] = ep.alpha * scale2(acc[j], er + eb[c]);
+                    }
+                } else {
+                    if (cb + 31 < r) continue;   // chunk entirely below the diagonal
+                    const int64_t ld = ep.ors;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int64_t c = cb + j;
+                        if (c < r || c >= n) continue;
+                        double val = ep.alpha * scale2(acc[j], er + eb[c]);
+                        if (ep.xin && !ep.square) val = 2.0 * ep.xin[r + c * ld] - val;
+                        ep.out[r + c * ld] = val;
+                        if (c == r) {
+                            tr += val;
+                            ss += val * val;
+                        } else {
+                            ss += 2.0 * val * val;
+                            ep.out[c + r * ld] = val;
+                        }
+                    }
+                }
+            }
+        }
+        if (EPI == OZ_SYM && ep.stats) {
+            for (int o = 16; o > 0; o >>= 1) {
+                tr += __shfl_xor_sync(0xffffffffu, tr, o);
+                ss += __shfl_xor_sync(0xffffffffu, ss, o);
+            }
+            if (lane == 0) {
+                red[2 * q4] = tr;
+                red[2 * q4 + 1] = ss;
+            }
+            asm volatile("bar.sync 1, 128;" ::: "memory");   // epilogue warps only
+            if (q4 == 0 && lane == 0) {
+                ep.stats[2 * blockIdx.x] = red[0] + red[2] + red[4] + red[6];
+                ep.stats[2 * blockIdx.x + 1] = red[1] + red[3] + red[5] + red[7];
+            }
+        }
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 2) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTmemCols));
+    }
+}
+
+// ---- host side ---------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    PTB_CHECK(fn != nullptr, PTBGPU_ECUDA, "cuTensorMapEncodeTiled unavailable");
+    return fn;
+}
+
+void encode_planes(CUtensorMap* map, const Operand& op, int box_rows, int rb) {
+    PTB_CHECK(((uintptr_t)op.planes & 15) == 0, PTBGPU_EINVAL, "slice planes not 16-byte aligned");
+    PTB_CHECK(op.ldp % BM == 0, PTBGPU_EINVAL, "slice leading dimension must be a multiple of 128");
+    cuuint64_t dims[2] = {(cuuint64_t)op.ldp, (cuuint64_t)op.ldp * (cuuint64_t)op.S};
+    cuuint64_t strides[1] = {(cuuint64_t)op.ldp};
+    cuuint32_t box[2] = {(cuuint32_t)rb, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    const CUtensorMapSwizzle sw = rb == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+    CUresult r = get_encode()(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, op.planes, dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    PTB_CHECK(r == CUDA_SUCCESS, PTBGPU_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+}
+
+template <int EPI, int S, int RB>
+void launch_t(cudaStream_t s, const OzMaps& maps, const int4* tiles, int ntiles, const Operand& a,
+              const Operand& b, const OzEpi& ep) {
+    using C = OzCfg<S, RB>;
+    static bool attr = false;
+    if (!attr) {
+        PTB_CUDA(cudaFuncSetAttribute(k_oz_product<EPI, S, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      C::SMEM));
+        attr = true;
+    }
+    k_oz_product<EPI, S, RB><<<ntiles, THREADS, C::SMEM, s>>>(maps, tiles, a.exps, b.exps, ep);
+    count_launch();
+}
+
+template <int EPI, int S>
+void launch_s(cudaStream_t s, int rb, const OzMaps& maps, const int4* tiles, int ntiles, const Operand& a,
+              const Operand& b, const OzEpi& ep) {
+    if (rb == 64) launch_t<EPI, S, 64>(s, maps, tiles, ntiles, a, b, ep);
+    else launch_t<EPI, S, 32>(s, maps, tiles, ntiles, a, b, ep);
+}
+
+template <int EPI>
+void launch_e(cudaStream_t s, int S, int rb, const OzMaps& maps, const int4* tiles, int ntiles, const Operand& a,
+              const Operand& b, const OzEpi& ep) {
+    switch (S) {
+        case 6: launch_s<EPI, 6>(s, rb, maps, tiles, ntiles, a, b, ep); break;
+        case 7: launch_s<EPI, 7>(s, rb, maps, tiles, ntiles, a, b, ep); break;
+        case 8: launch_s<EPI, 8>(s, rb, maps, tiles, ntiles, a, b, ep); break;
+        default: PTB_CHECK(false, PTBGPU_EINVAL, "unsupported slice count %d (6, 7 or 8)", S);
+    }
+}
+
+}  // namespace
+
+int64_t max_k(int S) { return (int64_t)2147483647 / ((int64_t)S * 127 * 127); }
+int64_t padded(int64_t n) { return round_up(n, BM); }
+bool supported(int64_t n, int S) { return S >= 6 && S <= 8 && padded(n) <= max_k(S); }
+
+void slice(cudaStream_t s, const double* M, int64_t rs, int64_t cs, int64_t n, int tri, const Operand& op,
+           unsigned long long* rowmax) {
+    PTB_CHECK(rs == 1 || cs == 1, PTBGPU_EINVAL, "slicing needs rows or columns contiguous");
+    PTB_CHECK(op.ldp >= n && op.ldp % BM == 0, PTBGPU_EINVAL, "bad slice leading dimension");
+    PTB_CUDA(cudaMemsetAsync(rowmax, 0, sizeof(unsigned long long) * (size_t)op.ldp, s));
+    const dim3 g1((unsigned)((n + 127) / 128), (unsigned)((n + 31) / 32));
+    k_oz_rowmax<<<g1, THREADS, 0, s>>>(M, rs, cs, n, tri, rowmax);
+    count_launch();
+    const dim3 g2((unsigned)(op.ldp / 64), (unsigned)(op.ldp / 32));
+    switch (op.S) {
+        case 6: k_oz_slice<6><<<g2, THREADS, 0, s>>>(M, rs, cs, n, tri, rowmax, op.planes, op.exps, op.ldp); break;
+        case 7: k_oz_slice<7><<<g2, THREADS, 0, s>>>(M, rs, cs, n, tri, rowmax, op.planes, op.exps, op.ldp); break;
+        case 8: k_oz_slice<8><<<g2, THREADS, 0, s>>>(M, rs, cs, n, tri, rowmax, op.planes, op.exps, op.ldp); break;
+        default: PTB_CHECK(false, PTBGPU_EINVAL, "unsupported slice count %d (6, 7 or 8)", op.S);
+    }
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+}
+
+std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri) {
+    const int nbi = (int)(ldp / BM), nbj = (int)(ldp / BN);
+    std::vector<int4> t;
+    const int G = 16;
+    for (int g0 = 0; g0 < nbi; g0 += G)
+        for (int bj = 0; bj < nbj; ++bj)
+            for (int bi = g0; bi < std::min(nbi, g0 + G); ++bi) {
+                if (upper && (int64_t)bj * BN + BN - 1 < (int64_t)bi * BM) continue;
+                int64_t k0 = 0, k1 = ldp;
+                if (a_tri == TRI_LOWER) k1 = std::min<int64_t>(k1, (int64_t)(bi + 1) * BM);
+                if (a_tri == TRI_UPPER) k0 = std::max<int64_t>(k0, (int64_t)bi * BM);
+                if (b_tri == TRI_LOWER) k1 = std::min<int64_t>(k1, (int64_t)(bj + 1) * BN);
+                if (b_tri == TRI_UPPER) k0 = std::max<int64_t>(k0, (int64_t)bj * BN);
+                PTB_CHECK(k1 > k0, PTBGPU_EINVAL, "empty K range in a tile");
+                t.push_back(make_int4(bi, bj, (int)k0, (int)k1));
+            }
+    std::stable_sort(t.begin(), t.end(), [](const int4& x, const int4& y) { return x.w - x.z > y.w - y.z; });
+    return t;
+}
+
+void product(cudaStream_t s, int epi, const Operand& a, const Operand& b, const int4* tiles_dev, int ntiles,
+             const OzEpi& ep, int rb) {
+    if (rb == 0) rb = 64;   // measured faster than 32 at ndim 11776 (S = 7 and 8)
+    PTB_CHECK(rb == 32 || rb == 64, PTBGPU_EINVAL, "K block must be 32 or 64 bytes");
+    PTB_CHECK(a.S == b.S && a.ldp == b.ldp && a.ldp == ep.ldp, PTBGPU_EINVAL, "operands do not match");
+    PTB_CHECK(a.ldp <= max_k(a.S), PTBGPU_EINVAL, "dimension %lld too large for exact int32 sums with %d slices",
+              (long long)a.ldp, a.S);
+    PTB_CHECK(epi == OZ_OUT || epi == OZ_SYM, PTBGPU_EINVAL, "bad epilogue");
+    if (ntiles == 0) return;
+    OzMaps maps;
+    encode_planes(&maps.a, a, BM, rb);
+    encode_planes(&maps.b, b, BN, rb);
+    if (epi == OZ_OUT) launch_e<OZ_OUT>(s, a.S, rb, maps, tiles_dev, ntiles, a, b, ep);
+    else launch_e<OZ_SYM>(s, a.S, rb, maps, tiles_dev, ntiles, a, b, ep);
+    PTB_CUDA(cudaGetLastError());
+}
+
+}  // namespace oz
+}  // namespace ptb

@@ -25,6 +25,12 @@
 //            over the stored trajectory, X1 <- X0_k X1 + X1 X0_k (or
 //            2 X1 - (...)), again with bf16x3 products; P = P~ + X1.
 //            The error left is second order in the pass-1 error.
+//
+// The FP64 products of the mixed path (A = L^-1 H L^-T through the explicit
+// triangular inverse, the cleanup squares, the commutator and the
+// back-transform) run on the int8 tensor cores with 7-bit operand slices and
+// exact int32 sums (oz_gemm.cu) when opts->fp64_slices is 6..8; with 0 they are
+// cuBLAS/cuSOLVER FP64 calls, as in the FP64 path.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -32,6 +38,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "oz_gemm.cuh"
 #include "tc_gemm.cuh"
 
 namespace ptb {
@@ -278,6 +285,79 @@ void timed_product(ptbgpu_ctx* c, int epi, int np, int64_t ldp, const void* cons
     c->timed.push_back({epi == tc::EPI_SP2 ? 0 : 1, a, b});
 }
 
+// Device-time phase log of one purification call (print level >= 2): CUDA
+// events on the context stream between phases, reported when the call ends.
+struct PhaseLog {
+    ptbgpu_ctx* c = nullptr;
+    std::vector<std::pair<const char*, cudaEvent_t>> marks;
+    void add(const char* what) {
+        cudaEvent_t e = c->take_event();
+        PTB_CUDA(cudaEventRecord(e, c->stream));
+        marks.push_back({what, e});
+    }
+    void report(int prl) {
+        if (marks.size() < 2) return;
+        PTB_CUDA(cudaEventSynchronize(marks.back().second));
+        for (size_t i = 1; i < marks.size(); ++i) {
+            float ms = 0.f;
+            PTB_CUDA(cudaEventElapsedTime(&ms, marks[i - 1].second, marks[i].second));
+            log_line(prl, 2, " * purification %-34s %9.3f ms", marks[i].first, ms);
+        }
+    }
+};
+thread_local PhaseLog* t_phases = nullptr;   // set for the duration of a call at print level >= 2
+void phase(const char* what) {
+    if (t_phases) t_phases->add(what);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 products on the int8 tensor cores (oz_gemm.cu): context-held operands
+// ---------------------------------------------------------------------------
+oz::Operand oz_operand(ptbgpu_ctx* c, int slot, int64_t n, int S) {
+    const int64_t ldp = oz::padded(n);
+    DevBuf& bp = c->buf(B_OZ0 + slot);
+    DevBuf& be = c->buf(B_OZE0 + slot);
+    bp.reserve((size_t)S * ldp * ldp);
+    be.reserve(sizeof(int) * (size_t)ldp);
+    oz::Operand op;
+    op.planes = bp.as<int8_t>();
+    op.exps = be.as<int>();
+    op.ldp = ldp;
+    op.S = S;
+    return op;
+}
+
+void oz_slice(ptbgpu_ctx* c, const double* M, int64_t rs, int64_t cs, int64_t n, int tri, const oz::Operand& op) {
+    DevBuf& br = c->buf(B_OZR);
+    br.reserve(sizeof(unsigned long long) * (size_t)op.ldp);
+    oz::slice(c->stream, M, rs, cs, n, tri, op, br.as<unsigned long long>());
+}
+
+// One product over a freshly uploaded tile list, bracketed by CUDA events.
+// Returns the tile count (the number of per-tile stats of OZ_SYM).
+int oz_product(ptbgpu_ctx* c, int epi, const oz::Operand& a, const oz::Operand& b, bool upper, int tri_a,
+               int tri_b, oz::OzEpi ep, int rb = 0) {
+    const std::vector<int4> t = oz::make_tiles(a.ldp, upper, tri_a, tri_b);
+    DevBuf& bt = c->buf(B_OZT);
+    bt.reserve(sizeof(int4) * t.size());
+    PTB_CUDA(cudaMemcpyAsync(bt.ptr, t.data(), sizeof(int4) * t.size(), cudaMemcpyHostToDevice, c->stream));
+    ep.ldp = a.ldp;
+    if (!ep.err) ep.err = &c->flags->timeout;
+    cudaEvent_t e0 = c->take_event(), e1 = c->take_event();
+    PTB_CUDA(cudaEventRecord(e0, c->stream));
+    oz::product(c->stream, epi, a, b, bt.as<int4>(), (int)t.size(), ep, rb);
+    PTB_CUDA(cudaEventRecord(e1, c->stream));
+    c->timed.push_back({2, e0, e1});
+    return (int)t.size();
+}
+
+void check_timeout(ptbgpu_ctx* c, const char* what) {
+    int tmo = 0;
+    PTB_CUDA(cudaMemcpyAsync(&tmo, &c->flags->timeout, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    PTB_CUDA(cudaStreamSynchronize(c->stream));
+    PTB_CHECK(tmo == 0, PTBGPU_ETIMEOUT, "%s gave up waiting (site %d)", what, tmo);
+}
+
 // ---------------------------------------------------------------------------
 // host helpers
 // ---------------------------------------------------------------------------
@@ -295,19 +375,100 @@ Prologue orthogonalise(ptbgpu_ctx* c, int64_t n, const double* dHpk, const doubl
     double* S = bs.as<double>();
     unpack_sym(c->stream, n, n, dHpk, H, filter);
     unpack_sym(c->stream, n, n, dSpk, S, filter);
+    phase("unpack H, S");
     const int info = dpotrf_lower(c, n, n, S);
     PTB_CHECK(info == 0, PTBGPU_ENOTSPD, "overlap matrix not positive definite (potrf info=%d)", info);
+    phase("potrf");
     const double one = 1.0;
     PTB_CUBLAS(cublasDtrsm(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
                            (int)n, (int)n, &one, S, (int)n, H, (int)n));
     PTB_CUBLAS(cublasDtrsm(c->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT,
                            (int)n, (int)n, &one, S, (int)n, H, (int)n));
     symmetrize_upper(c->stream, n, n, H);
+    phase("2 trsm (A = L^-1 H L^-T)");
     Prologue p;
     gershgorin_bounds(c, n, n, H, &p.emin, &p.emax);
     PTB_CHECK(std::isfinite(p.emin) && std::isfinite(p.emax) && p.emax > p.emin, PTBGPU_ENAN,
               "invalid spectral bounds [%g, %g]", p.emin, p.emax);
     return p;
+}
+
+// The same on the int8 tensor cores: L^-1 by cuSOLVER trtri (in place in B_S,
+// lower triangle), T = L^-1 H (lower-triangular A operand: K blocks past the
+// diagonal are skipped), A = T L^-T (symmetric: upper tiles, mirrored).
+Prologue orthogonalise_oz(ptbgpu_ctx* c, int64_t n, const double* dHpk, const double* dSpk, double filter, int S) {
+    DevBuf& bh = c->buf(B_H);
+    DevBuf& bs = c->buf(B_S);
+    DevBuf& bt = c->buf(B_W1);
+    bh.reserve(sizeof(double) * n * n);
+    bs.reserve(sizeof(double) * n * n);
+    bt.reserve(sizeof(double) * n * n);
+    double* H = bh.as<double>();
+    double* L = bs.as<double>();
+    double* T = bt.as<double>();
+    unpack_sym(c->stream, n, n, dHpk, H, filter);
+    unpack_sym(c->stream, n, n, dSpk, L, filter);
+    phase("unpack H, S");
+    const int info = dpotrf_lower(c, n, n, L);
+    PTB_CHECK(info == 0, PTBGPU_ENOTSPD, "overlap matrix not positive definite (potrf info=%d)", info);
+    phase("potrf");
+    dtrtri_lower(c, n, n, L);
+    phase("trtri");
+    const oz::Operand opL = oz_operand(c, 0, n, S), op1 = oz_operand(c, 1, n, S);
+    oz_slice(c, L, 1, n, n, oz::TRI_LOWER, opL);   // rows of L^-1 (column-major storage)
+    oz_slice(c, H, 1, n, n, oz::TRI_NONE, op1);    // rows of H (symmetric)
+    phase("slice L^-1, H");
+    oz::OzEpi ep;
+    ep.n = n;
+    ep.out = T;   // T column-major
+    ep.ors = 1;
+    ep.ocs = n;
+    oz_product(c, oz::OZ_OUT, opL, op1, false, oz::TRI_LOWER, oz::TRI_NONE, ep);
+    phase("int8 T = L^-1 H");
+    oz_slice(c, T, 1, n, n, oz::TRI_NONE, op1);    // rows of T
+    phase("slice T");
+    oz::OzEpi es;
+    es.n = n;
+    es.out = H;   // A overwrites H (its slices are no longer read)
+    es.ors = n;
+    oz_product(c, oz::OZ_SYM, op1, opL, true, oz::TRI_NONE, oz::TRI_LOWER, es);
+    phase("int8 A = T L^-T");
+    check_timeout(c, "int8 product (orthogonalisation)");
+    Prologue p;
+    gershgorin_bounds(c, n, n, H, &p.emin, &p.emax);
+    PTB_CHECK(std::isfinite(p.emin) && std::isfinite(p.emax) && p.emax > p.emin, PTBGPU_ENAN,
+              "invalid spectral bounds [%g, %g]", p.emin, p.emax);
+    return p;
+}
+
+// P = 2 L^-T X L^-1 on the int8 tensor cores with L^-1 from orthogonalise_oz:
+// T2 = X L^-1 (B operand = rows of L^-T, upper triangular), then
+// P = 2 L^-T T2 (A operand = rows of L^-T; symmetric result), packed into dPpk.
+// X (column-major, symmetric) is overwritten; W is n x n scratch.
+void back_transform_oz(ptbgpu_ctx* c, int64_t n, double* X, double* W, double* dPpk, int S) {
+    const double* Linv = c->buf(B_S).as<double>();
+    const oz::Operand opLt = oz_operand(c, 0, n, S), op1 = oz_operand(c, 1, n, S);
+    oz_slice(c, Linv, n, 1, n, oz::TRI_UPPER, opLt);   // row j of L^-T = column j of L^-1
+    oz_slice(c, X, 1, n, n, oz::TRI_NONE, op1);
+    phase("slice L^-T, X");
+    oz::OzEpi ep;
+    ep.n = n;
+    ep.out = W;   // T2 column-major
+    ep.ors = 1;
+    ep.ocs = n;
+    oz_product(c, oz::OZ_OUT, op1, opLt, false, oz::TRI_NONE, oz::TRI_UPPER, ep);
+    phase("int8 T2 = X L^-1");
+    oz_slice(c, W, n, 1, n, oz::TRI_NONE, op1);        // rows of T2^T = columns of T2
+    phase("slice T2^T");
+    oz::OzEpi es;
+    es.n = n;
+    es.alpha = 2.0;
+    es.out = X;
+    es.ors = n;
+    oz_product(c, oz::OZ_SYM, opLt, op1, true, oz::TRI_UPPER, oz::TRI_NONE, es);
+    phase("int8 P = 2 L^-T T2");
+    check_timeout(c, "int8 product (back-transform)");
+    pack_cols(c->stream, n, n, X, dPpk);
 }
 
 // P = 2 L^-T X L^-1 (X in place, column-major n x n), then packed into dPpk.
@@ -364,7 +525,9 @@ void sp2_fp64(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int ma
         }
     }
     PTB_CHECK(done, PTBGPU_EITER, "trace-correcting purification did not converge in %d iterations", maxit);
+    phase("SP2 iterations (FP64 syrk)");
     back_transform(c, n, X, dPpk);
+    phase("back-transform and pack");
     if (st) {
         st->iterations = it;
         st->flops += (double)it * (double)n * n * n;   // SYRK-equivalent products
@@ -372,7 +535,7 @@ void sp2_fp64(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int ma
 }
 
 void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int maxit, bool refine,
-               int64_t split3_iters, double* dPpk, ptbgpu_stats* st, int prl) {
+               int64_t split3_iters, int S, double* dPpk, ptbgpu_stats* st, int prl) {
     cudaStream_t s = c->stream;
     const int64_t ldp = round_up(n, tc::tile_n());
     const size_t plane = sizeof(__nv_bfloat16) * (size_t)ldp * ldp;
@@ -470,6 +633,7 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     PTB_CUDA(cudaMemcpyAsync(&tmo, &c->flags->timeout, sizeof(int), cudaMemcpyDeviceToHost, s));
     PTB_CUDA(cudaStreamSynchronize(s));
     const SP2State& H = hstate[0];
+    phase("pass 1 (tcgen05 bf16 SP2)");
     PTB_CHECK(tmo == 0, PTBGPU_ETIMEOUT, "tensor-core product gave up waiting (site %d)", tmo);
     PTB_CHECK(H.status == 0, H.status, "pass-1 purification failed (status %d at iterate %d)", H.status, H.next);
     PTB_CHECK(H.converged, PTBGPU_EITER, "pass-1 purification did not converge in %d iterations", cap);
@@ -490,17 +654,58 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     PTB_CUDA(cudaGetLastError());
     std::vector<double> hist;
     int nclean = 0;
-    for (nclean = 1; nclean <= 8; ++nclean) {
-        StepInfo si = fp64_step(c, n, N, X, W);
-        const double e = std::fabs(si.err);
-        hist.push_back(e);
-        log_line(prl, 2, " SP2 (fp64 cleanup) %d  err %.3e", nclean, si.err);
-        // until the error reaches FP64 rounding or stops falling over two steps: a
-        // single SP2 step squares the deviation on one side of the spectrum but
-        // doubles it on the other, so a small error on entry is not enough
-        if (e < 1e-13 * (double)n || (hist.size() > 2 && e >= hist[hist.size() - 3])) break;
+    if (S > 0) {
+        // int8-sliced squares, X updated in place (the epilogue reads X(r,c), c >= r,
+        // before writing it; the mirrored lower triangle is never read); the error
+        // of each iterate is checked before its square is taken
+        const oz::Operand opX = oz_operand(c, 1, n, S);
+        DevBuf& bst = c->buf(B_OZS);
+        bst.reserve(sizeof(double) * 2 * (size_t)(oz::padded(n) / oz::BM) * (size_t)(oz::padded(n) / oz::BN));
+        std::vector<double> hst;
+        double trX = trace_dev(c, n, n, X);
+        const double f0 = frob_dev(c, n, n, X);
+        double trX2 = f0 * f0;
+        for (;;) {
+            const double err = trX - trX2, e = std::fabs(err);
+            PTB_CHECK(std::isfinite(err), PTBGPU_ENAN, "NaN during purification");
+            hist.push_back(e);
+            log_line(prl, 2, " SP2 (int8 FP64 cleanup) %d  err %.3e", nclean, err);
+            if (e < 1e-13 * (double)n || (hist.size() > 2 && e >= hist[hist.size() - 3]) || nclean >= 8) break;
+            const bool sq = std::fabs(trX2 - N) <= std::fabs(2.0 * trX - trX2 - N);
+            oz_slice(c, X, 1, n, n, oz::TRI_NONE, opX);
+            oz::OzEpi es;
+            es.n = n;
+            es.out = X;
+            es.ors = n;
+            es.xin = X;
+            es.square = sq ? 1 : 0;
+            es.stats = bst.as<double>();
+            const int nt = oz_product(c, oz::OZ_SYM, opX, opX, true, oz::TRI_NONE, oz::TRI_NONE, es);
+            hst.resize(2 * (size_t)nt);
+            PTB_CUDA(cudaMemcpyAsync(hst.data(), es.stats, sizeof(double) * hst.size(), cudaMemcpyDeviceToHost, s));
+            check_timeout(c, "int8 product (cleanup)");
+            trX = 0.0;
+            trX2 = 0.0;
+            for (int t = 0; t < nt; ++t) {
+                trX += hst[2 * t];
+                trX2 += hst[2 * t + 1];
+            }
+            ++nclean;
+        }
+    } else {
+        for (nclean = 1; nclean <= 8; ++nclean) {
+            StepInfo si = fp64_step(c, n, N, X, W);
+            const double e = std::fabs(si.err);
+            hist.push_back(e);
+            log_line(prl, 2, " SP2 (fp64 cleanup) %d  err %.3e", nclean, si.err);
+            // until the error reaches FP64 rounding or stops falling over two steps: a
+            // single SP2 step squares the deviation on one side of the spectrum but
+            // doubles it on the other, so a small error on entry is not enough
+            if (e < 1e-13 * (double)n || (hist.size() > 2 && e >= hist[hist.size() - 3])) break;
+        }
+        nclean = std::min(nclean, 8);
     }
-    nclean = std::min(nclean, 8);
+    phase(S > 0 ? "cleanup (int8 FP64 squares)" : "cleanup (FP64 syrk)");
     // algorithmic: every SP2 step is one symmetric square (n^3), pass 1 and cleanup alike
     double flops = (double)K * (double)n * n * n + (double)nclean * (double)n * n * n;
 
@@ -509,7 +714,21 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         DevBuf& bw2 = c->buf(B_W2);
         bw2.reserve(sizeof(double) * n * n);
         double* Wc = bw2.as<double>();
-        dgemm_nn(c, n, n, 1.0, A, X, 0.0, W);
+        if (S > 0) {
+            const oz::Operand opA = oz_operand(c, 0, n, S), opP = oz_operand(c, 1, n, S);
+            oz_slice(c, A, 1, n, n, oz::TRI_NONE, opA);
+            oz_slice(c, X, 1, n, n, oz::TRI_NONE, opP);
+            oz::OzEpi ep;
+            ep.n = n;
+            ep.out = W;   // W = A P~, column-major
+            ep.ors = 1;
+            ep.ocs = n;
+            oz_product(c, oz::OZ_OUT, opA, opP, false, oz::TRI_NONE, oz::TRI_NONE, ep);
+            phase("int8 W = A P~ (incl. slices)");
+        } else {
+            dgemm_nn(c, n, n, 1.0, A, X, 0.0, W);
+            phase("dgemm W = A P~");
+        }
         const unsigned nb = (unsigned)((n + 31) / 32);
         k_antisym<<<dim3(nb, nb), dim3(32, 8), 0, s>>>(n, W, Wc);
         count_launch();
@@ -549,6 +768,7 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
                                                             x1lo[0]);
         count_launch();
         PTB_CUDA(cudaGetLastError());
+        phase("commutator, planes, A1 product");
         // replay the branch sequence over the stored trajectory
         for (int k = 0; k < K; ++k) {
             const int a = k & 1, b = a ^ 1;
@@ -561,6 +781,7 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
             count_launch();
             PTB_CUDA(cudaGetLastError());
         }
+        phase("DMPT replay (tcgen05 bf16x3)");
         // Keep only the blocks of X1 that couple occupied and virtual states of
         // P~: X1_od = P~ X1 + X1 P~ - 2 P~ X1 P~ = W + W^T - 2 W P~ with W = P~ X1.
         // The diagonal blocks of the computed X1 are rounding noise of the
@@ -604,6 +825,7 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
             count_launch();
             PTB_CUDA(cudaGetLastError());
         }
+        phase("projection, idempotency term");
         // P_o = P~ (1 - tau/N) + X1_K with tau = tr X1_K: the exact first-order
         // response is traceless; its bf16x3 rounding noise is removed from the
         // trace in FP64 along P~ (a uniform shift of the occupied eigenvalues by
@@ -623,11 +845,14 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         PTB_CUDA(cudaGetLastError());
         // algorithmic: FP64 commutator 2n^3, then K + 5 general products of 2n^3
         flops += 2.0 * (double)n * n * n + (double)(K + 5) * 2.0 * (double)n * n * n;
+        phase("trace correction");
         PTB_CUDA(cudaMemcpyAsync(&tmo, &c->flags->timeout, sizeof(int), cudaMemcpyDeviceToHost, s));
         PTB_CUDA(cudaStreamSynchronize(s));
         PTB_CHECK(tmo == 0, PTBGPU_ETIMEOUT, "tensor-core product gave up waiting (site %d)", tmo);
     }
-    back_transform(c, n, X, dPpk);
+    if (S > 0) back_transform_oz(c, n, X, W, dPpk, S);
+    else back_transform(c, n, X, dPpk);
+    phase("back-transform and pack");
     if (st) {
         st->iterations = K + nclean;
         st->flops += flops;
@@ -644,12 +869,26 @@ void tc_purify_device(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, c
     if (!o) o = &def;
     const int maxit = o->max_iter > 0 ? (int)std::min<int64_t>(o->max_iter, kMaxIt) : 100;
     const int prl = (int)o->print_level;
-    Prologue pro = orthogonalise(c, n, dH, dS, o->filter);
+    // int8-sliced FP64 products on the mixed path, when the dimension keeps the int32 sums exact
+    const int S = (o->precision != PTBGPU_PREC_FP64 && o->fp64_slices != 0) ? (int)o->fp64_slices : 0;
+    PTB_CHECK(S == 0 || (S >= 6 && S <= 8), PTBGPU_EINVAL, "fp64_slices must be 0 or 6..8 (got %d)", S);
+    const int Suse = (S > 0 && oz::supported(n, S)) ? S : 0;
+    PhaseLog plog;
+    plog.c = c;
+    struct Scope {
+        PhaseLog* p;
+        explicit Scope(PhaseLog* q) : p(q) { t_phases = q; }
+        ~Scope() { t_phases = nullptr; }
+    } scope(prl >= 2 ? &plog : nullptr);
+    phase("start");
+    Prologue pro = Suse > 0 ? orthogonalise_oz(c, n, dH, dS, o->filter, Suse) : orthogonalise(c, n, dH, dS, o->filter);
+    phase("Gershgorin bounds");
     if (st) st->flops += (1.0 / 3.0 + 4.0) * (double)n * n * n;   // potrf + 4 trsm
     if (o->precision == PTBGPU_PREC_FP64)
         sp2_fp64(c, n, nel, pro, maxit, dP, st, prl);
     else
-        sp2_mixed(c, n, nel, pro, maxit, o->precision != 2, o->split3_iters, dP, st, prl);
+        sp2_mixed(c, n, nel, pro, maxit, o->precision != 2, o->split3_iters, Suse, dP, st, prl);
+    if (prl >= 2) plog.report(prl);
 }
 
 }  // namespace
@@ -699,6 +938,38 @@ void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, int kblock, const double* hX,
     PTB_CUDA(cudaMemcpyAsync(&tmo, &c->flags->timeout, sizeof(int), cudaMemcpyDeviceToHost, s));
     PTB_CUDA(cudaStreamSynchronize(s));
     PTB_CHECK(tmo == 0, PTBGPU_ETIMEOUT, "tensor-core product gave up waiting (site %d)", tmo);
+}
+
+// C = A B (n x n, row-major host FP64) with the int8-sliced kernel, for
+// kernel-level tests.  tri_a / tri_b describe A and B as matrices (1 lower,
+// 2 upper); sym: only the upper triangle of C is computed and mirrored.
+void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int tri_a, int tri_b, bool sym, const double* hA,
+                   const double* hB, double* hC) {
+    PTB_CHECK(oz::supported(n, S), PTBGPU_EINVAL, "n = %lld is too large for exact int32 sums with %d slices",
+              (long long)n, S);
+    cudaStream_t s = c->stream;
+    DevBuf& ba = c->buf(B_W0);
+    DevBuf& bb = c->buf(B_W1);
+    DevBuf& bc = c->buf(B_W2);
+    ba.reserve(sizeof(double) * n * n);
+    bb.reserve(sizeof(double) * n * n);
+    bc.reserve(sizeof(double) * n * n);
+    PTB_CUDA(cudaMemcpyAsync(ba.ptr, hA, sizeof(double) * n * n, cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemcpyAsync(bb.ptr, hB, sizeof(double) * n * n, cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemsetAsync(&c->flags->timeout, 0, sizeof(int), s));
+    const oz::Operand opA = oz_operand(c, 0, n, S), opB = oz_operand(c, 1, n, S);
+    // rows of A: A(i,k) = A[i n + k]; rows of B^T: B^T(j,k) = B(k,j) = B[j + k n]
+    const int ta = tri_a, tb = tri_b == 1 ? oz::TRI_UPPER : tri_b == 2 ? oz::TRI_LOWER : oz::TRI_NONE;
+    oz_slice(c, ba.as<double>(), n, 1, n, ta, opA);
+    oz_slice(c, bb.as<double>(), 1, n, n, tb, opB);
+    oz::OzEpi ep;
+    ep.n = n;
+    ep.out = bc.as<double>();
+    ep.ors = n;
+    ep.ocs = 1;
+    oz_product(c, sym ? oz::OZ_SYM : oz::OZ_OUT, opA, opB, sym, ta, tb, ep, kblock);
+    PTB_CUDA(cudaMemcpyAsync(hC, bc.ptr, sizeof(double) * n * n, cudaMemcpyDeviceToHost, s));
+    check_timeout(c, "int8 product");
 }
 
 }  // namespace ptb
