@@ -254,15 +254,19 @@ def run_ours(args, rank, world, local, pg):
     tc_n = (sum(x.n_tc_sp2 + x.n_tc_full for x in stats)) / len(stats)
     # algorithmic flops: SP2 step = symmetric square, n^2 (n+1) ~ n^3; general product 2 n^3
     alg = last.n_tc_sp2 * float(n) ** 3 + last.n_tc_full * 2.0 * float(n) ** 3
-    ldp = ((n + 255) // 256) * 256
-    nt_up = sum(1 for bi in range(ldp // 128) for bj in range(ldp // 256) if bj * 256 + 255 >= bi * 128)
-    executed = 3 * 2.0 * 128 * 256 * ldp * (last.n_tc_sp2 * nt_up + last.n_tc_full * (ldp // 128) * (ldp // 256))
+    executed = last.tc_flops   # every product of the split, every tile that ran (reported by the library)
     achieved = alg / (last.ms_tc_sp2 + last.ms_tc_full) / 1e9 if (last.ms_tc_sp2 + last.ms_tc_full) > 0 else 0.0
     exec_tf = executed / (last.ms_tc_sp2 + last.ms_tc_full) / 1e9 if (last.ms_tc_sp2 + last.ms_tc_full) > 0 else 0.0
     traffic = None
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
         traffic = json.loads(tp.read_text()).get("tc_product_bytes_per_launch")
+    # the FP64-class products of the mixed path on the int8 tensor cores (Ozaki slices)
+    oz = None
+    if last.n_oz > 0 and last.ms_oz > 0:
+        oz = {"kernel": "k_oz_product (tcgen05 kind::i8, exact int32 slice-pair sums)",
+              "slices": opts.fp64_slices, "launches_per_step": last.n_oz, "ms_per_step_in_kernel": last.ms_oz,
+              "int8_executed_tops": last.oz_ops / (last.ms_oz / 1e3) / 1e12}
 
     if rank != 0:
         return
@@ -275,7 +279,9 @@ def run_ours(args, rank, world, local, pg):
     line = {
         "metric": METRIC, "value": ms_dev / 1e3, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_dev, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16x3+f64" if prec == PREC_MIXED else "f64", "data": "synthetic",
+        "vs_baseline": None,
+        "dtype": ("bf16x3+i8-sliced-f64+f64" if oz else "bf16x3+f64") if prec == PREC_MIXED else "f64",
+        "data": "synthetic",
         "config": {"workload": f"dense density step, {args.nmol}-H2O box ({s.nat} atoms, ndim {n}, nel {nel}), "
                                "filter 1e-5, trace-correcting purification",
                    "global_batch": world, "seq_len": n, "parallelism": f"replicas x{world}",
@@ -294,6 +300,8 @@ def run_ours(args, rank, world, local, pg):
         "clocks": clocks,
         "wall_s_timed": wall,
     }
+    if oz:
+        line["int8_fp64_products"] = oz
     if fp64:
         line["fp64_gpu"] = fp64
     print(json.dumps(line), flush=True)

@@ -115,6 +115,8 @@ typedef struct {
     int64_t kernel_launches;    /* launches of this library's own kernels in the call */
     double  ms_oz;              /* summed device time of the int8-sliced FP64 products */
     int64_t n_oz;
+    double  oz_ops;             /* int8 multiply-adds x 2 those products executed (slice pairs, all tiles) */
+    double  tc_flops;           /* bf16 flops the tcgen05 split products executed (all planes, all tiles) */
 } ptbgpu_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */

@@ -60,7 +60,7 @@ class _Stats(C.Structure):
                 ("ms_h2d", C.c_double), ("ms_solve", C.c_double), ("ms_d2h", C.c_double), ("flops", C.c_double),
                 ("ms_tc_sp2", C.c_double), ("n_tc_sp2", C.c_int64), ("ms_tc_full", C.c_double),
                 ("n_tc_full", C.c_int64), ("kernel_launches", C.c_int64), ("ms_oz", C.c_double),
-                ("n_oz", C.c_int64)]
+                ("n_oz", C.c_int64), ("oz_ops", C.c_double), ("tc_flops", C.c_double)]
 
 
 EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_default_settings",
@@ -163,6 +163,8 @@ class Stats:
     kernel_launches: int = 0
     ms_oz: float = 0.0
     n_oz: int = 0
+    oz_ops: float = 0.0
+    tc_flops: float = 0.0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "Stats":

@@ -34,6 +34,7 @@ int guarded(ptbgpu_ctx* c, F&& f) {
         launch_counter() = 0;
         c->evused = 0;
         c->timed.clear();
+        c->oz_ops = 0.0;
         f();
         c->last_error.clear();
         return PTBGPU_OK;
@@ -104,6 +105,7 @@ struct PhaseTimer {
             }
         }
         st->kernel_launches = launch_counter();
+        st->oz_ops = c->oz_ops;
     }
 };
 

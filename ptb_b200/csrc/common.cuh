@@ -97,6 +97,7 @@ struct ptbgpu_ctx {
         cudaEvent_t a, b;
     };
     std::vector<Timed> timed;
+    double oz_ops = 0.0;   // executed int8 ops of the int8-sliced products since the call started
     cudaEvent_t take_event();
 };
 

@@ -474,9 +474,9 @@ void trtri_block(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A) {
 
 // Recursive halving: for L = [L11 0; L21 L22], L^-1 = [L11^-1 0; -L22^-1 L21 L11^-1  L22^-1].
 // The off-diagonal block takes two triangular products (cuBLAS trmm, in place),
-// so the n^3/3 flops run at product speed; blocks of <= 1024 go to cuSOLVER.
+// so the n^3/3 flops run at product speed; blocks of <= 512 go to cuSOLVER.
 void trtri_rec(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A) {
-    if (n <= 1024) {
+    if (n <= 512) {
         trtri_block(c, n, ld, A);
         return;
     }

@@ -343,6 +343,9 @@ int oz_product(ptbgpu_ctx* c, int epi, const oz::Operand& a, const oz::Operand& 
     PTB_CUDA(cudaMemcpyAsync(bt.ptr, t.data(), sizeof(int4) * t.size(), cudaMemcpyHostToDevice, c->stream));
     ep.ldp = a.ldp;
     if (!ep.err) ep.err = &c->flags->timeout;
+    double kk = 0.0;
+    for (const int4& x : t) kk += (double)(x.w - x.z);
+    c->oz_ops += 2.0 * oz::BM * oz::BN * kk * (double)(a.S * (a.S + 1) / 2);
     cudaEvent_t e0 = c->take_event(), e1 = c->take_event();
     PTB_CUDA(cudaEventRecord(e0, c->stream));
     oz::product(c->stream, epi, a, b, bt.as<int4>(), (int)t.size(), ep, rb);
@@ -350,6 +353,12 @@ int oz_product(ptbgpu_ctx* c, int epi, const oz::Operand& a, const oz::Operand& 
     c->timed.push_back({2, e0, e1});
     return (int)t.size();
 }
+
+// Slices of the orthogonalisation products: one fewer than the cleanup squares
+// (whose errors the SP2 map feeds back and which set the idempotency floor) and
+// the back-transform (which sets tr(PS) directly); an error of A moves the
+// problem, not the electron count, and 7 slices keep ~2^-49 of the row maxima.
+int slices_once(int S) { return std::max(6, S - 1); }
 
 void check_timeout(ptbgpu_ctx* c, const char* what) {
     int tmo = 0;
@@ -591,7 +600,9 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
                                         stats);
     count_launch();
     PTB_CUDA(cudaGetLastError());
-    k_decide<<<1, 256, 0, s>>>(state, stats, x0_blocks, N, tol_abs, e_switch, std::min(maxit, slots - 1));
+    const int cap = std::min(maxit, slots - 1);
+    const int n6 = (int)up3.size(), n3 = (int)up.size();
+    k_decide<<<1, 256, 0, s>>>(state, stats, x0_blocks, N, tol_abs, e_switch, cap);
     count_launch();
     PTB_CUDA(cudaGetLastError());
 
@@ -603,8 +614,10 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     ep.err = &c->flags->timeout;
     ep.ld = ldp;
     ep.stats = stats;
-    const int cap = std::min(maxit, slots - 1);
+    // three-plane products for the leading steps (0 = all, -1 = none)
+    auto three_planes = [&](int k) { return split3_iters < 0 ? false : (split3_iters == 0 || k < split3_iters); };
     int launched = 0;
+    const size_t timed0 = c->timed.size();   // pass-1 step timings start here
     SP2State* hs = (SP2State*)c->pinned;   // only the 8-int header is read back while iterating
     for (int k = 0; k < cap; ++k) {
         ep.xcur = xf[k & 1];
@@ -612,9 +625,9 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         ep.hi = traj(k + 1, 0);
         ep.lo = traj(k + 1, 1);
         ep.lo2 = traj(k + 1, 2);
-        const bool three = split3_iters < 0 ? false : (split3_iters == 0 || k < split3_iters);
         const void* pl[3] = {traj(k, 0), traj(k, 1), traj(k, 2)};
-        const int ntl = three ? (int)up3.size() : (int)up.size();
+        const bool three = three_planes(k);
+        const int ntl = three ? n6 : n3;
         timed_product(c, tc::EPI_SP2, three ? 3 : 2, ldp, pl, pl, three ? split6 : split3,
                       three ? tiles_up3 : tiles_up, ntl, ep);
         k_decide<<<1, 256, 0, s>>>(state, stats, ntl, N, tol_abs, e_switch, cap);
@@ -638,6 +651,13 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     PTB_CHECK(H.status == 0, H.status, "pass-1 purification failed (status %d at iterate %d)", H.status, H.next);
     PTB_CHECK(H.converged, PTBGPU_EITER, "pass-1 purification did not converge in %d iterations", cap);
     const int K = H.next;   // index of the final pass-1 iterate
+    // steps launched after the decision that ended pass 1 did nothing: drop their timings
+    if (timed0 + (size_t)K < c->timed.size()) c->timed.resize(timed0 + (size_t)K);
+    // executed tcgen05 flops (all tiles of every launch that ran, every product of the split)
+    double tc_exec = 0.0;
+    for (int k = 0; k < K; ++k)
+        tc_exec += three_planes(k) ? 2.0 * 6 * 128 * 128 * (double)ldp * n6 : 2.0 * 3 * 128 * 256 * (double)ldp * n3;
+    const double tc_exec_full = 2.0 * 3 * (double)ldp * ldp * ldp;   // one general bf16x3 product
     for (int k = 0; k <= K && prl >= 2; ++k)
         log_line(prl, 2, " SP2 (bf16x3) iter %3d  trX %.10f  err %.3e  %s", k, H.trX[k], H.err[k],
                  k < K ? (H.sq[k] ? "X^2" : "2X-X^2") : "final");
@@ -715,7 +735,10 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         bw2.reserve(sizeof(double) * n * n);
         double* Wc = bw2.as<double>();
         if (S > 0) {
-            const oz::Operand opA = oz_operand(c, 0, n, S), opP = oz_operand(c, 1, n, S);
+            // C is ~1e-6 of |A||P~|: 6 slices (42 bits of the row maxima) leave it
+            // with ~1e-7 relative error, far below what its first-order use needs
+            const int Sc = 6;
+            const oz::Operand opA = oz_operand(c, 0, n, Sc), opP = oz_operand(c, 1, n, Sc);
             oz_slice(c, A, 1, n, n, oz::TRI_NONE, opA);
             oz_slice(c, X, 1, n, n, oz::TRI_NONE, opP);
             oz::OzEpi ep;
@@ -850,11 +873,12 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         PTB_CUDA(cudaStreamSynchronize(s));
         PTB_CHECK(tmo == 0, PTBGPU_ETIMEOUT, "tensor-core product gave up waiting (site %d)", tmo);
     }
-    if (S > 0) back_transform_oz(c, n, X, W, dPpk, S);
+    if (S > 0) back_transform_oz(c, n, X, W, dPpk, S);   // sets tr(PS) directly: full slice count
     else back_transform(c, n, X, dPpk);
     phase("back-transform and pack");
     if (st) {
         st->iterations = K + nclean;
+        st->tc_flops += tc_exec + (refine ? (double)(K + 5) * tc_exec_full : 0.0);
         st->flops += flops;
     }
 }
@@ -881,7 +905,8 @@ void tc_purify_device(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, c
         ~Scope() { t_phases = nullptr; }
     } scope(prl >= 2 ? &plog : nullptr);
     phase("start");
-    Prologue pro = Suse > 0 ? orthogonalise_oz(c, n, dH, dS, o->filter, Suse) : orthogonalise(c, n, dH, dS, o->filter);
+    Prologue pro = Suse > 0 ? orthogonalise_oz(c, n, dH, dS, o->filter, slices_once(Suse))
+                            : orthogonalise(c, n, dH, dS, o->filter);
     phase("Gershgorin bounds");
     if (st) st->flops += (1.0 / 3.0 + 4.0) * (double)n * n * n;   // potrf + 4 trsm
     if (o->precision == PTBGPU_PREC_FP64)
