@@ -196,6 +196,29 @@ int ptbgpu_solve2(ptbgpu_ctx* ctx, int64_t mode, int64_t ndim, int64_t nel, int6
 int ptbgpu_density_traces_noalloc(int device, int64_t ndim, const double* dPpk, const double* dSpk,
                                   const double* dHpk, double* out, void* stream, char* err, size_t errlen);
 
+/* ---- population analysis on the produced P ------------------------------ */
+/* mlpop14(nao, s, s34, s14), source/mlpop.f:142-190: s34 = S^(1-x) and s14 = S^x
+ * in REAL*4 (nao x nao, column-major) from an FP32 eigen-decomposition of the
+ * packed FP64 overlap Spk; x is mull_loew14 (source/parcom.f90:26: 1/3). */
+int ptbgpu_mlpop14(ptbgpu_ctx* ctx, int64_t nao, const double* Spk, double x, float* s34, float* s14);
+/* The same with device-resident Spk and device outputs. */
+int ptbgpu_mlpop14_device(ptbgpu_ctx* ctx, int64_t nao, const double* dSpk, double x, float* d_s34,
+                          float* d_s14);
+/* mlpop2(n, nao, p, s1, s2, q, qsh), source/mlpop.f:198-235: atomic populations
+ * q(n) and shell populations qsh(10, n) (Fortran order) from the diagonal of
+ * s2 P s1, with P packed FP64 and s1 = S^(1-x), s2 = S^x REAL*4 column-major.
+ * aoat(nao) (AO -> atom) and shell2ao(nao) (AO -> shell of its atom), 1-based,
+ * are the bascom module arrays the Fortran routine reads.  The diagonal is
+ * formed from one int8-sliced product (6 slices, exact int32 sums), more
+ * accurate than the reference's REAL*4 ssymm + sgemm. */
+int ptbgpu_mlpop2(ptbgpu_ctx* ctx, int64_t n, int64_t nao, const double* Ppk, const float* s1, const float* s2,
+                  const int64_t* aoat, const int64_t* shell2ao, double* q, double* qsh, ptbgpu_stats* st);
+/* The same with P (e.g. left on the device by ptbgpu_tc_purify_device), s1 and
+ * s2 device-resident; aoat, shell2ao, q and qsh are host arrays. */
+int ptbgpu_mlpop2_device(ptbgpu_ctx* ctx, int64_t n, int64_t nao, const double* dPpk, const float* d_s1,
+                         const float* d_s2, const int64_t* aoat, const int64_t* shell2ao, double* q, double* qsh,
+                         ptbgpu_stats* st);
+
 /* ---- kernel-level entry points (parity tests and benchmarks) ------------ */
 /* C = X * X for a symmetric n x n FP64 matrix X (row-major), computed with the
  * bf16x3 tcgen05 kernel (hi/lo split, FP32 accumulation); C is FP32 row-major. */

@@ -647,3 +647,48 @@ def gershgorin_bounds(A: np.ndarray):
 def sp2_choose_square(trX: float, trX2: float, N: float) -> bool:
     """SP2 branch rule: X^2 if it lands the trace closer to N than 2X - X^2 does."""
     return abs(trX2 - N) <= abs(2.0 * trX - trX2 - N)
+
+
+# ---------------------------------------------------------------------------
+# Mixed Mulliken/Loewdin population analysis (source/mlpop.f)
+# ---------------------------------------------------------------------------
+MULL_LOEW14 = 0.3333333333   # source/parcom.f90:26 (REAL(wp) parameter)
+
+
+def mlpop14(nao: int, Svec: np.ndarray, x: float = MULL_LOEW14):
+    """source/mlpop.f:142-190: s34 = S^(1-x), s14 = S^x in REAL*4.
+
+    blowsym84 (packed FP64 -> full REAL*4), ssyev('V','U'), e1 = e**(1-x) and
+    e2 = e**x (REAL*4 base, REAL(8) exponent, stored REAL*4), then
+    sgemm('N','T') of X with X*diag(e).  Returns float32 (nao, nao) arrays in
+    Fortran index order ([row, col])."""
+    X = blowsym(nao, Svec).astype(np.float32)
+    w, V, info = _lapack.ssyev(X, compute_v=1, lower=0)
+    if info != 0:
+        raise RuntimeError(f"ssyev info={info}")
+    e1 = (w.astype(np.float64) ** (1.0 - x)).astype(np.float32)
+    e2 = (w.astype(np.float64) ** x).astype(np.float32)
+    s34 = (V @ (V * e1[None, :]).T).astype(np.float32)
+    s14 = (V @ (V * e2[None, :]).T).astype(np.float32)
+    return s34, s14
+
+
+def mlpop2(n: int, nao: int, Pvec: np.ndarray, s1: np.ndarray, s2: np.ndarray, aoat: np.ndarray,
+           shell2ao: np.ndarray, dtype=np.float32):
+    """source/mlpop.f:198-235: X = s2 (P s1) with P blown up to REAL*4
+    (blowsym84), ssymm then sgemm, q(aoat(i)) += X(i,i) and
+    qsh(shell2ao(i), aoat(i)) += X(i,i) in REAL*8.  aoat and shell2ao are
+    1-based (bascom).  dtype=np.float64 gives the same formula in FP64 (the
+    error-free value the REAL*4 reference approximates).  Returns q (n,) and
+    qsh (n, 10) (= Fortran qsh(10, n) in memory order)."""
+    x = blowsym(nao, Pvec).astype(dtype)
+    cc = (x @ s1.astype(dtype)).astype(dtype)
+    xx = (s2.astype(dtype) @ cc).astype(dtype)
+    q = np.zeros(n)
+    qsh = np.zeros((n, 10))
+    d = np.diag(xx).astype(np.float64)
+    for i in range(nao):
+        ia = int(aoat[i]) - 1
+        q[ia] += d[i]
+        qsh[ia, int(shell2ao[i]) - 1] += d[i]
+    return q, qsh

@@ -30,6 +30,7 @@ _PKG = Path(__file__).resolve().parent
 # status codes (include/ptbgpu.h)
 OK, EINVAL, ECUDA, ENOTSPD, ENAN, EITER, ENOTIMPL, ETIMEOUT, ENOMEM = range(9)
 PREC_FP64, PREC_MIXED, PREC_MIXED_NOREFINE = 0, 1, 2
+MULL_LOEW14 = 0.3333333333   # Mulliken/Loewdin mixing of the populations, source/parcom.f90:26
 
 
 class PtbGpuError(RuntimeError):
@@ -67,7 +68,8 @@ EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_defau
             "ptbgpu_default_opts", "ptbgpu_filter_packed", "ptbgpu_check_density", "ptbgpu_sm_density",
             "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_solve2",
             "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_symsq_split", "ptbgpu_runtime_info",
-            "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm")
+            "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm", "ptbgpu_mlpop14", "ptbgpu_mlpop14_device",
+            "ptbgpu_mlpop2", "ptbgpu_mlpop2_device")
 
 
 def library_path() -> Path:
@@ -111,6 +113,12 @@ def load_library():
     lib.ptbgpu_symsq_bf16x6.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_split.argtypes = [C.c_void_p, i64, i64, i64, d, P(C.c_float)]
     lib.ptbgpu_oz_gemm.argtypes = [C.c_void_p, i64, i64, i64, i64, i64, i64, d, d, d, d]
+    f = P(C.c_float)
+    lib.ptbgpu_mlpop14.argtypes = [C.c_void_p, i64, d, C.c_double, f, f]
+    lib.ptbgpu_mlpop14_device.argtypes = [C.c_void_p, i64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+    lib.ptbgpu_mlpop2.argtypes = [C.c_void_p, i64, i64, d, f, f, P(i64), P(i64), d, d, P(_Stats)]
+    lib.ptbgpu_mlpop2_device.argtypes = [C.c_void_p, i64, i64, C.c_void_p, C.c_void_p, C.c_void_p, P(i64), P(i64),
+                                         d, d, P(_Stats)]
     lib.ptbgpu_runtime_info.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     lib.ptbgpu_density_traces_noalloc.argtypes = [C.c_int, i64, C.c_void_p, C.c_void_p, C.c_void_p, d,
                                                   C.c_void_p, C.c_char_p, C.c_size_t]
@@ -334,6 +342,47 @@ class Context:
                                              int(bool(symmetric)), _dptr(Ah), _dptr(Bh), _dptr(out),
                                              C.byref(ms)))
         return (out, ms.value) if timed else out
+
+    # ---- population analysis (source/mlpop.f) ----
+    def mlpop14(self, nao: int, Svec: np.ndarray, x: float = MULL_LOEW14):
+        """mlpop14 (source/mlpop.f:142): (s34, s14) = (S^(1-x), S^x) as float32
+        (nao, nao) arrays indexed [row, col] (column-major in memory)."""
+        s34 = np.zeros((nao, nao), dtype=np.float32, order="F")
+        s14 = np.zeros((nao, nao), dtype=np.float32, order="F")
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        self._check(self._lib.ptbgpu_mlpop14(self._h, int(nao), _dptr(_f64(Svec)), float(x), fp(s34), fp(s14)))
+        return s34, s14
+
+    def mlpop2(self, n: int, nao: int, Pvec: np.ndarray, s1: np.ndarray, s2: np.ndarray, aoat: np.ndarray,
+               shell2ao: np.ndarray):
+        """mlpop2 (source/mlpop.f:198): atomic populations q (n,) and shell
+        populations qsh (n, 10) (Fortran qsh(10, n)); s1 = S^(1-x), s2 = S^x
+        indexed [row, col]; aoat / shell2ao 1-based."""
+        f1 = np.asfortranarray(s1, dtype=np.float32)
+        f2 = np.asfortranarray(s2, dtype=np.float32)
+        q = np.zeros(n)
+        qsh = np.zeros((n, 10))
+        st = _Stats()
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
+        a, sh = _i64(aoat), _i64(shell2ao)
+        self._check(self._lib.ptbgpu_mlpop2(self._h, int(n), int(nao), _dptr(_f64(Pvec)), fp(f1), fp(f2), ip(a),
+                                            ip(sh), _dptr(q), _dptr(qsh), C.byref(st)))
+        return q, qsh, Stats.from_c(st)
+
+    def mlpop2_device(self, n: int, nao: int, dP: int, ds1: int, ds2: int, aoat: np.ndarray,
+                      shell2ao: np.ndarray):
+        """mlpop2 on device-resident packed P and column-major float32 s1, s2
+        (raw device pointers)."""
+        q = np.zeros(n)
+        qsh = np.zeros((n, 10))
+        st = _Stats()
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
+        a, sh = _i64(aoat), _i64(shell2ao)
+        self._check(self._lib.ptbgpu_mlpop2_device(self._h, int(n), int(nao), C.c_void_p(dP), C.c_void_p(ds1),
+                                                   C.c_void_p(ds2), ip(a), ip(sh), _dptr(q), _dptr(qsh),
+                                                   C.byref(st)))
+        return q, qsh, Stats.from_c(st)
 
     def _symsq(self, X, fn):
         Xh = _f64(X)

@@ -9,6 +9,8 @@ namespace ptb {
 void tc_purify_entry(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, const double* dS, double* dP,
                      const ptbgpu_opts* o, ptbgpu_stats* st);
 void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, int kblock, const double* hX, float* hC);
+void mlpop14_device(ptbgpu_ctx* c, int64_t n, const double* dSpk, double x, float* s34, float* s14);
+void mlpop2_diag_device(ptbgpu_ctx* c, int64_t n, const double* dPpk, const float* s1, const float* s2, double* xd);
 void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int tri_a, int tri_b, bool sym, const double* hA,
                    const double* hB, double* hC);
 void purify_ref_device(ptbgpu_ctx* c, const ptbgpu_pur_settings& pur, int64_t n, const double* dH,
@@ -111,6 +113,22 @@ struct PhaseTimer {
 
 void clear_stats(ptbgpu_stats* st) {
     if (st) memset(st, 0, sizeof(*st));
+}
+
+// q(aoat(i)) += xd(i), qsh(shell2ao(i), aoat(i)) += xd(i) in AO order, as
+// source/mlpop.f:225-233 (1-based maps; qsh is Fortran qsh(10, n)).
+void accumulate_pops(int64_t nat, int64_t nao, const double* xd, const int64_t* aoat, const int64_t* shell2ao,
+                     double* q, double* qsh) {
+    for (int64_t a = 0; a < nat; ++a) q[a] = 0.0;
+    for (int64_t k = 0; k < 10 * nat; ++k) qsh[k] = 0.0;
+    for (int64_t i = 0; i < nao; ++i) {
+        const int64_t ia = aoat[i] - 1, ish = shell2ao[i] - 1;
+        PTB_CHECK(ia >= 0 && ia < nat && ish >= 0 && ish < 10, PTBGPU_EINVAL,
+                  "aoat(%lld) = %lld or shell2ao = %lld out of range", (long long)(i + 1), (long long)aoat[i],
+                  (long long)shell2ao[i]);
+        q[ia] += xd[i];
+        qsh[ia * 10 + ish] += xd[i];
+    }
 }
 
 }  // namespace
@@ -244,6 +262,71 @@ int ptbgpu_symsq_split(ptbgpu_ctx* c, int64_t n, int64_t planes, int64_t kblock,
         PTB_CHECK(n > 0 && X && C && (planes == 2 || planes == 3) && (kblock == 0 || kblock == 32 || kblock == 64),
                   PTBGPU_EINVAL, "bad arguments");
         symsq_entry(c, n, (int)planes, (int)kblock, X, C);
+    });
+}
+
+int ptbgpu_mlpop14(ptbgpu_ctx* c, int64_t nao, const double* Spk, double x, float* s34, float* s14) {
+    return guarded(c, [&] {
+        PTB_CHECK(nao > 0 && Spk && s34 && s14, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, nao);
+        io.in(0, Spk);
+        DevBuf& b3 = c->buf(B_X1F0);
+        DevBuf& b1 = c->buf(B_X1F1);
+        b3.reserve(sizeof(float) * nao * nao);
+        b1.reserve(sizeof(float) * nao * nao);
+        mlpop14_device(c, nao, io.d[0], x, b3.as<float>(), b1.as<float>());
+        PTB_CUDA(cudaMemcpyAsync(s34, b3.ptr, sizeof(float) * nao * nao, cudaMemcpyDeviceToHost, c->stream));
+        PTB_CUDA(cudaMemcpyAsync(s14, b1.ptr, sizeof(float) * nao * nao, cudaMemcpyDeviceToHost, c->stream));
+        PTB_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int ptbgpu_mlpop14_device(ptbgpu_ctx* c, int64_t nao, const double* dSpk, double x, float* d_s34, float* d_s14) {
+    return guarded(c, [&] {
+        PTB_CHECK(nao > 0 && dSpk && d_s34 && d_s14, PTBGPU_EINVAL, "bad arguments");
+        mlpop14_device(c, nao, dSpk, x, d_s34, d_s14);
+        PTB_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int ptbgpu_mlpop2(ptbgpu_ctx* c, int64_t n, int64_t nao, const double* Ppk, const float* s1, const float* s2,
+                  const int64_t* aoat, const int64_t* shell2ao, double* q, double* qsh, ptbgpu_stats* st) {
+    clear_stats(st);
+    return guarded(c, [&] {
+        PTB_CHECK(n > 0 && nao > 0 && Ppk && s1 && s2 && aoat && shell2ao && q && qsh, PTBGPU_EINVAL,
+                  "bad arguments");
+        PackedIO io(c, nao);
+        DevBuf& b1 = c->buf(B_MISC0);
+        DevBuf& b2 = c->buf(B_MISC1);
+        b1.reserve(sizeof(float) * nao * nao);
+        b2.reserve(sizeof(float) * nao * nao);
+        PhaseTimer t(c);
+        io.in(0, Ppk);
+        PTB_CUDA(cudaMemcpyAsync(b1.ptr, s1, sizeof(float) * nao * nao, cudaMemcpyHostToDevice, c->stream));
+        PTB_CUDA(cudaMemcpyAsync(b2.ptr, s2, sizeof(float) * nao * nao, cudaMemcpyHostToDevice, c->stream));
+        t.mark(1);
+        std::vector<double> xd((size_t)nao);
+        mlpop2_diag_device(c, nao, io.d[0], b1.as<float>(), b2.as<float>(), xd.data());
+        t.mark(2);
+        t.finish(st);
+        accumulate_pops(n, nao, xd.data(), aoat, shell2ao, q, qsh);
+    });
+}
+
+int ptbgpu_mlpop2_device(ptbgpu_ctx* c, int64_t n, int64_t nao, const double* dPpk, const float* d_s1,
+                         const float* d_s2, const int64_t* aoat, const int64_t* shell2ao, double* q, double* qsh,
+                         ptbgpu_stats* st) {
+    clear_stats(st);
+    return guarded(c, [&] {
+        PTB_CHECK(n > 0 && nao > 0 && dPpk && d_s1 && d_s2 && aoat && shell2ao && q && qsh, PTBGPU_EINVAL,
+                  "bad arguments");
+        PhaseTimer t(c);
+        t.mark(1);
+        std::vector<double> xd((size_t)nao);
+        mlpop2_diag_device(c, nao, dPpk, d_s1, d_s2, xd.data());
+        t.mark(2);
+        t.finish(st);
+        accumulate_pops(n, nao, xd.data(), aoat, shell2ao, q, qsh);
     });
 }
 

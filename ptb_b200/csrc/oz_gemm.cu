@@ -417,10 +417,11 @@ template <int EPI>
 void launch_e(cudaStream_t s, int S, int rb, const OzMaps& maps, const int4* tiles, int ntiles, const Operand& a,
               const Operand& b, const OzEpi& ep) {
     switch (S) {
+        case 4: launch_s<EPI, 4>(s, rb, maps, tiles, ntiles, a, b, ep); break;
         case 6: launch_s<EPI, 6>(s, rb, maps, tiles, ntiles, a, b, ep); break;
         case 7: launch_s<EPI, 7>(s, rb, maps, tiles, ntiles, a, b, ep); break;
         case 8: launch_s<EPI, 8>(s, rb, maps, tiles, ntiles, a, b, ep); break;
-        default: PTB_CHECK(false, PTBGPU_EINVAL, "unsupported slice count %d (6, 7 or 8)", S);
+        default: PTB_CHECK(false, PTBGPU_EINVAL, "unsupported slice count %d (4, 6, 7 or 8)", S);
     }
 }
 
@@ -428,7 +429,7 @@ void launch_e(cudaStream_t s, int S, int rb, const OzMaps& maps, const int4* til
 
 int64_t max_k(int S) { return (int64_t)2147483647 / ((int64_t)S * 127 * 127); }
 int64_t padded(int64_t n) { return round_up(n, BM); }
-bool supported(int64_t n, int S) { return S >= 6 && S <= 8 && padded(n) <= max_k(S); }
+bool supported(int64_t n, int S) { return (S == 4 || (S >= 6 && S <= 8)) && padded(n) <= max_k(S); }
 
 void slice(cudaStream_t s, const double* M, int64_t rs, int64_t cs, int64_t n, int tri, const Operand& op,
            unsigned long long* rowmax) {
@@ -440,10 +441,11 @@ void slice(cudaStream_t s, const double* M, int64_t rs, int64_t cs, int64_t n, i
     count_launch();
     const dim3 g2((unsigned)(op.ldp / 64), (unsigned)(op.ldp / 32));
     switch (op.S) {
+        case 4: k_oz_slice<4><<<g2, THREADS, 0, s>>>(M, rs, cs, n, tri, rowmax, op.planes, op.exps, op.ldp); break;
         case 6: k_oz_slice<6><<<g2, THREADS, 0, s>>>(M, rs, cs, n, tri, rowmax, op.planes, op.exps, op.ldp); break;
         case 7: k_oz_slice<7><<<g2, THREADS, 0, s>>>(M, rs, cs, n, tri, rowmax, op.planes, op.exps, op.ldp); break;
         case 8: k_oz_slice<8><<<g2, THREADS, 0, s>>>(M, rs, cs, n, tri, rowmax, op.planes, op.exps, op.ldp); break;
-        default: PTB_CHECK(false, PTBGPU_EINVAL, "unsupported slice count %d (6, 7 or 8)", op.S);
+        default: PTB_CHECK(false, PTBGPU_EINVAL, "unsupported slice count %d (4, 6, 7 or 8)", op.S);
     }
     count_launch();
     PTB_CUDA(cudaGetLastError());

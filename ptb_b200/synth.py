@@ -183,6 +183,25 @@ def basis_layout(symbols):
             np.array(occ, dtype=bool))
 
 
+# Shells of the vDZP-sized synthetic basis, per AO of an atom (1-based, as
+# bascom's shell2ao): H 5 AOs = s, s, p; C/N/O 13 AOs = s, s, p, p, d.
+SHELLS_PER_AO = {5: (1, 2, 3, 3, 3), 13: (1, 2, 3, 3, 3, 4, 4, 4, 5, 5, 5, 5, 5)}
+
+
+def shell2ao(aoat: np.ndarray) -> np.ndarray:
+    """AO -> shell index within its atom (1-based) for an AO -> atom map."""
+    aoat = np.asarray(aoat)
+    out = np.empty(aoat.shape[0], dtype=np.int64)
+    i = 0
+    while i < aoat.shape[0]:
+        j = i
+        while j < aoat.shape[0] and aoat[j] == aoat[i]:
+            j += 1
+        out[i:j] = SHELLS_PER_AO[j - i]
+        i = j
+    return out
+
+
 def _pack_upper(full: np.ndarray) -> np.ndarray:
     n = full.shape[0]
     r, c = np.tril_indices(n)

@@ -192,3 +192,34 @@ def test_fermi_smearing_integer_for_gap():
     occ, ef = O.fermismear(4, 2, 300.0, e)
     assert np.allclose(occ, [1, 1, 0, 0], atol=1e-12)
     assert -0.5 < ef < 0.5
+
+
+def test_mlpop_identity_overlap_is_diagonal_sum():
+    """With S = I, S^(1-x) = S^x = I and the populations are sums of diag(P)
+    per atom and per shell (source/mlpop.f:198-235)."""
+    from ptb_b200 import synth
+    s = synth.water_cluster(4, seed=3)
+    n = s.ndim
+    s34, s14 = O.mlpop14(n, O.packsym(np.eye(n)))
+    assert np.max(np.abs(s34 - np.eye(n))) < 1e-6 and np.max(np.abs(s14 - np.eye(n))) < 1e-6
+    rng = np.random.default_rng(0)
+    P = rng.standard_normal((n, n))
+    P = P + P.T
+    sh = synth.shell2ao(s.aoat)
+    q, qsh = O.mlpop2(s.nat, n, O.packsym(P), np.eye(n, dtype=np.float32), np.eye(n, dtype=np.float32),
+                      s.aoat, sh, dtype=np.float64)
+    d = np.diag(P)
+    for a in range(s.nat):
+        assert abs(q[a] - d[s.aoat == a + 1].sum()) < 1e-12
+    assert abs(qsh.sum() - d.sum()) < 1e-10
+
+
+def test_mlpop_populations_sum_to_trace_ps():
+    from ptb_b200 import synth
+    s = synth.water_cluster(8, seed=5)
+    n = s.ndim
+    H, S = O.blowsym(n, s.Hvec), O.blowsym(n, s.Svec)
+    P, _ = O.dense_projector(H, S, s.nel)
+    s34, s14 = O.mlpop14(n, s.Svec)
+    q, _ = O.mlpop2(s.nat, n, O.packsym(P), s34, s14, s.aoat, synth.shell2ao(s.aoat), dtype=np.float64)
+    assert abs(q.sum() - s.nel) < 1e-3
