@@ -196,6 +196,20 @@ int ptbgpu_solve2(ptbgpu_ctx* ctx, int64_t mode, int64_t ndim, int64_t nel, int6
 int ptbgpu_density_traces_noalloc(int device, int64_t ndim, const double* dPpk, const double* dSpk,
                                   const double* dHpk, double* out, void* stream, char* err, size_t errlen);
 
+/* Columns mode 4 grouping, source/sm.f90:127-154 + clustering_kmeans :459-514
+ * + KMPP source/kmpp.f: k-means++ on the atom positions for 1..min(64, nat)
+ * clusters, keeping the partition with the least sum over submatrices of
+ * dim^2.5 (dim from the H > 0 / S > 0 index-set test on the filtered H, S).
+ * The reference's generator is global Fortran state shared by an OpenMP loop;
+ * here each cluster count draws from its own splitmix64 stream derived from
+ * `seed`, so the partition is reproducible.  partition(nat) receives 1-based
+ * cluster ids (the input ptbgpu_sm_density takes in mode 4); nsm and effort
+ * (may be NULL) the chosen count and its cost.  ptbgpu_sm_density in mode 4
+ * with partition == NULL runs this with seed 42. */
+int ptbgpu_kmeans_partition(ptbgpu_ctx* ctx, int64_t ndim, const double* Hpk, const double* Spk, int64_t nat,
+                            const double* xyz, const int64_t* aoat, uint64_t seed, const ptbgpu_opts* opts,
+                            int64_t* partition, int64_t* nsm, double* effort);
+
 /* ---- population analysis on the produced P ------------------------------ */
 /* mlpop14(nao, s, s34, s14), source/mlpop.f:142-190: s34 = S^(1-x) and s14 = S^x
  * in REAL*4 (nao x nao, column-major) from an FP32 eigen-decomposition of the

@@ -692,3 +692,133 @@ def mlpop2(n: int, nao: int, Pvec: np.ndarray, s1: np.ndarray, s2: np.ndarray, a
         q[ia] += d[i]
         qsh[ia, int(shell2ao[i]) - 1] += d[i]
     return q, qsh
+
+
+# ---------------------------------------------------------------------------
+# Deterministic k-means partition for submatrix columns mode 4
+# (source/sm.f90:127-154,459-514 with source/kmpp.f; the reference draws from
+# the Fortran global RNG inside an OpenMP loop, so its partition is not
+# reproducible -- this restatement fixes the generator: splitmix64 seeded per
+# cluster count)
+# ---------------------------------------------------------------------------
+_M64 = (1 << 64) - 1
+
+
+class SplitMix64:
+    """splitmix64 (Vigna): state += golden gamma, then two xor-shift-multiply
+    rounds; uniform() = top 53 bits / 2^53 in [0, 1)."""
+
+    def __init__(self, seed: int):
+        self.s = seed & _M64
+
+    def uniform(self) -> float:
+        self.s = (self.s + 0x9E3779B97F4A7C15) & _M64
+        z = self.s
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+        z ^= z >> 31
+        return float(z >> 11) * (2.0 ** -53)
+
+
+def kmeans_seed(seed: int, k: int) -> int:
+    return (seed ^ ((k * 0xD1B54A32D192ED03) & _M64)) & _M64
+
+
+def kmeans_pp(xyz: np.ndarray, k: int, seed: int, maxiter: int = 1000):
+    """k-means++ seeding + Lloyd iterations as source/kmpp.f:24-178 (first
+    centre at int(u N), the others with probability proportional to the
+    squared distance to the nearest chosen centre; nearest centre with ties to
+    the lower index; centres = sum * (1/count)).  Returns 0-based labels, or
+    None when a cluster empties (IFAULT = 1 in the reference)."""
+    x = [tuple(float(v) for v in p) for p in np.asarray(xyz, dtype=np.float64)]
+    n = len(x)
+    rng = SplitMix64(kmeans_seed(seed, k))
+    big = 1e33
+    work = [big] * n
+    i1 = min(int(rng.uniform() * n), n - 1)
+    C = [x[i1]]
+    for _ in range(1, k):
+        tot = 0.0
+        c = C[-1]
+        for i in range(n):
+            d2 = (x[i][0] - c[0]) ** 2 + (x[i][1] - c[1]) ** 2 + (x[i][2] - c[2]) ** 2
+            if d2 < work[i]:
+                work[i] = d2
+            tot += work[i]
+        w = rng.uniform() * tot
+        acc = 0.0
+        i1 = n - 1
+        for i in range(n):
+            acc += work[i]
+            if acc > w:
+                i1 = i
+                break
+        C.append(x[i1])
+    z = [-1] * n
+    for _ in range(maxiter):
+        change = False
+        for i in range(n):
+            best, l1 = big, 0
+            for l in range(k):
+                c = C[l]
+                d2 = (x[i][0] - c[0]) ** 2 + (x[i][1] - c[1]) ** 2 + (x[i][2] - c[2]) ** 2
+                if d2 < best:
+                    best, l1 = d2, l
+            if z[i] != l1:
+                z[i] = l1
+                change = True
+        if not change:
+            break
+        cnt = [0] * k
+        sums = [[0.0, 0.0, 0.0] for _ in range(k)]
+        for i in range(n):
+            cnt[z[i]] += 1
+            for j in range(3):
+                sums[z[i]][j] += x[i][j]
+        if min(cnt) == 0:
+            return None
+        C = [tuple(sums[l][j] * (1.0 / cnt[l]) for j in range(3)) for l in range(k)]
+    return np.array(z, dtype=np.int64)
+
+
+def atom_pattern(ndim: int, H: np.ndarray, S: np.ndarray, aoat: np.ndarray, nat: int) -> np.ndarray:
+    """R[i, A] = any column c of atom A with H(i,c) > 0 or S(i,c) > 0 or i == c
+    (the index-set test of source/sm.f90:503-508, per atom)."""
+    F = (H > 0) | (S > 0) | np.eye(ndim, dtype=bool)
+    R = np.zeros((ndim, nat), dtype=bool)
+    at = np.asarray(aoat) - 1
+    for a in range(nat):
+        R[:, a] = F[:, at == a].any(axis=1)
+    return R
+
+
+def kmeans_effort(R: np.ndarray, z: np.ndarray, k: int) -> float:
+    """sum_k m_k^2.5 (source/sm.f90:498-512) with m_k = rows coupled to a
+    column of cluster k; m^2.5 evaluated as m*m*sqrt(m)."""
+    m = np.zeros(k, dtype=np.int64)
+    for i in range(R.shape[0]):
+        ks = np.unique(z[np.nonzero(R[i])[0]])
+        m[ks] += 1
+    e = 0.0
+    for v in m:
+        v = float(v)
+        e += v * v * math.sqrt(v)
+    return e
+
+
+def kmeans_partition(ndim: int, H: np.ndarray, S: np.ndarray, nat: int, xyz: np.ndarray, aoat: np.ndarray,
+                     seed: int = 42):
+    """Mode-4 grouping, source/sm.f90:127-154: k-means for 1..min(64, nat)
+    clusters, keep the least sum m_k^2.5 (ties: fewer clusters).  Returns the
+    1-based atom -> cluster partition, the cluster count and the effort."""
+    R = atom_pattern(ndim, H, S, aoat, nat)
+    best = (math.inf, 0, None)
+    for k in range(1, min(64, nat) + 1):
+        z = kmeans_pp(xyz, k, seed)
+        if z is None:
+            continue
+        e = kmeans_effort(R, z, k)
+        if e < best[0]:
+            best = (e, k, z)
+    e, k, z = best
+    return z + 1, k, e

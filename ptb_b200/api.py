@@ -69,7 +69,7 @@ EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_defau
             "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_solve2",
             "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_symsq_split", "ptbgpu_runtime_info",
             "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm", "ptbgpu_mlpop14", "ptbgpu_mlpop14_device",
-            "ptbgpu_mlpop2", "ptbgpu_mlpop2_device")
+            "ptbgpu_mlpop2", "ptbgpu_mlpop2_device", "ptbgpu_kmeans_partition")
 
 
 def library_path() -> Path:
@@ -113,6 +113,8 @@ def load_library():
     lib.ptbgpu_symsq_bf16x6.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_split.argtypes = [C.c_void_p, i64, i64, i64, d, P(C.c_float)]
     lib.ptbgpu_oz_gemm.argtypes = [C.c_void_p, i64, i64, i64, i64, i64, i64, d, d, d, d]
+    lib.ptbgpu_kmeans_partition.argtypes = [C.c_void_p, i64, d, d, i64, d, P(i64), C.c_uint64, P(_Opts), P(i64),
+                                            P(i64), d]
     f = P(C.c_float)
     lib.ptbgpu_mlpop14.argtypes = [C.c_void_p, i64, d, C.c_double, f, f]
     lib.ptbgpu_mlpop14_device.argtypes = [C.c_void_p, i64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
@@ -269,6 +271,22 @@ class Context:
             ao.ctypes.data_as(C.POINTER(C.c_int64)), int(submatrix_columns), int(submatrix_mode),
             part.ctypes.data_as(C.POINTER(C.c_int64)) if part is not None else None, C.byref(o), C.byref(st)))
         return P, Stats.from_c(st)
+
+    def kmeans_partition(self, ndim: int, Hvec: np.ndarray, Svec: np.ndarray, n: int, xyz: np.ndarray,
+                         aoat: np.ndarray, seed: int = 42, opts: Options | None = None):
+        """Columns mode 4 grouping (source/sm.f90:127-154, clustering_kmeans
+        :459-514): seeded k-means++ for 1..min(64, n) clusters, least sum of
+        dim^2.5.  Returns (1-based atom -> cluster partition, nsm, effort)."""
+        part = np.zeros(n, dtype=np.int64)
+        nsm = C.c_int64(0)
+        eff = C.c_double(0.0)
+        o = (opts or Options()).to_c()
+        ao = _i64(aoat)
+        self._check(self._lib.ptbgpu_kmeans_partition(
+            self._h, int(ndim), _dptr(_f64(Hvec)), _dptr(_f64(Svec)), int(n), _dptr(_f64(xyz)),
+            ao.ctypes.data_as(C.POINTER(C.c_int64)), C.c_uint64(seed), C.byref(o),
+            part.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(nsm), C.byref(eff)))
+        return part, int(nsm.value), float(eff.value)
 
     def purification(self, pur: PurificationSettings, ndim: int, H: np.ndarray, S: np.ndarray,
                      opts: Options | None = None):

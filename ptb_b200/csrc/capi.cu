@@ -9,6 +9,9 @@ namespace ptb {
 void tc_purify_entry(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, const double* dS, double* dP,
                      const ptbgpu_opts* o, ptbgpu_stats* st);
 void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, int kblock, const double* hX, float* hC);
+std::vector<int64_t> kmeans_partition(ptbgpu_ctx* c, int64_t n, const double* dH, const double* dS, int64_t nat,
+                                      const double* xyz, const int64_t* aoat, uint64_t seed, int* nsm_out,
+                                      double* effort_out);
 void mlpop14_device(ptbgpu_ctx* c, int64_t n, const double* dSpk, double x, float* s34, float* s14);
 void mlpop2_diag_device(ptbgpu_ctx* c, int64_t n, const double* dPpk, const float* s1, const float* s2, double* xd);
 void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int tri_a, int tri_b, bool sym, const double* hA,
@@ -262,6 +265,31 @@ int ptbgpu_symsq_split(ptbgpu_ctx* c, int64_t n, int64_t planes, int64_t kblock,
         PTB_CHECK(n > 0 && X && C && (planes == 2 || planes == 3) && (kblock == 0 || kblock == 32 || kblock == 64),
                   PTBGPU_EINVAL, "bad arguments");
         symsq_entry(c, n, (int)planes, (int)kblock, X, C);
+    });
+}
+
+int ptbgpu_kmeans_partition(ptbgpu_ctx* c, int64_t ndim, const double* Hpk, const double* Spk, int64_t nat,
+                            const double* xyz, const int64_t* aoat, uint64_t seed, const ptbgpu_opts* opts,
+                            int64_t* partition, int64_t* nsm, double* effort) {
+    return guarded(c, [&] {
+        PTB_CHECK(ndim > 0 && Hpk && Spk && nat > 0 && xyz && aoat && partition, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, ndim);
+        io.in(0, Hpk);
+        io.in(1, Spk);
+        DevBuf& bh = c->buf(B_H);
+        DevBuf& bs = c->buf(B_S);
+        bh.reserve(sizeof(double) * ndim * ndim);
+        bs.reserve(sizeof(double) * ndim * ndim);
+        const double filter = opts ? opts->filter : 0.0;
+        unpack_sym(c->stream, ndim, ndim, io.d[0], bh.as<double>(), filter);
+        unpack_sym(c->stream, ndim, ndim, io.d[1], bs.as<double>(), filter);
+        int k = 0;
+        double e = 0.0;
+        const std::vector<int64_t> p =
+            kmeans_partition(c, ndim, bh.as<double>(), bs.as<double>(), nat, xyz, aoat, seed, &k, &e);
+        std::copy(p.begin(), p.end(), partition);
+        if (nsm) *nsm = k;
+        if (effort) *effort = e;
     });
 }
 

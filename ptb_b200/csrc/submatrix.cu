@@ -20,10 +20,12 @@
 //     column c, rows <= c; rows outside the map stay zero, source/sm.f90:201-203,
 //     343-362, 387).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <map>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -33,6 +35,9 @@ namespace ptb {
 namespace {
 
 constexpr double kPadDiag = 1.0e3;
+// generator seed of the mode-4 k-means when the caller supplies no partition
+// (the reference seeds its Fortran generator with 42 * (i - 1), source/sm.f90:21-32)
+constexpr uint64_t kKmeansSeed = 42;
 
 // (2) flags[k*n + i] |= (H(i,c) > 0 || S(i,c) > 0 || i == c) for column c of submatrix owner[c]
 __global__ void k_pattern(int64_t n, const double* __restrict__ H, const double* __restrict__ S,
@@ -347,6 +352,171 @@ std::vector<std::vector<int>> group_columns(int64_t ndim, const int64_t* aoat, i
     return comb;
 }
 
+// ---- deterministic k-means partition (columns mode 4) ---------------------
+// source/sm.f90:127-154,459-514 with source/kmpp.f.  The reference draws from
+// the Fortran global generator inside an OpenMP loop, so its partition is not
+// reproducible; here every cluster count k gets its own splitmix64 stream
+// (seed ^ k * const), so the result depends on the seed only.
+
+// splitmix64 (Vigna): add the golden gamma, two xor-shift-multiply rounds.
+struct SplitMix64 {
+    uint64_t s;
+    double uniform() {
+        s += 0x9E3779B97F4A7C15ull;
+        uint64_t z = s;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * 0x1.0p-53;
+    }
+};
+
+// k-means++ seeding and Lloyd iterations on the atom positions (xyz(3, n)),
+// as source/kmpp.f:24-178: first centre at int(u n), the others with
+// probability proportional to the squared distance to the nearest chosen
+// centre, nearest centre with ties to the lower index, centres = sum * (1/count).
+// Returns 0-based labels, or an empty vector when a cluster empties.
+std::vector<int> kmeans_pp(const double* xyz, int64_t n, int k, uint64_t seed) {
+    SplitMix64 rng{seed ^ ((uint64_t)k * 0xD1B54A32D192ED03ull)};
+    const double big = 1e33;
+    auto d2 = [&](int64_t i, const double* c) {
+        const double a = xyz[3 * i] - c[0], b = xyz[3 * i + 1] - c[1], e = xyz[3 * i + 2] - c[2];
+        return a * a + b * b + e * e;
+    };
+    std::vector<double> work(n, big), C(3 * (size_t)k);
+    int64_t i1 = std::min<int64_t>((int64_t)(rng.uniform() * (double)n), n - 1);
+    for (int j = 0; j < 3; ++j) C[j] = xyz[3 * i1 + j];
+    for (int l = 1; l < k; ++l) {
+        double tot = 0.0;
+        const double* c = &C[3 * (l - 1)];
+        for (int64_t i = 0; i < n; ++i) {
+            const double d = d2(i, c);
+            if (d < work[i]) work[i] = d;
+            tot += work[i];
+        }
+        const double w = rng.uniform() * tot;
+        double acc = 0.0;
+        i1 = n - 1;
+        for (int64_t i = 0; i < n; ++i) {
+            acc += work[i];
+            if (acc > w) {
+                i1 = i;
+                break;
+            }
+        }
+        for (int j = 0; j < 3; ++j) C[3 * l + j] = xyz[3 * i1 + j];
+    }
+    std::vector<int> z(n, -1);
+    for (int it = 0; it < 1000; ++it) {
+        bool change = false;
+        for (int64_t i = 0; i < n; ++i) {
+            double best = big;
+            int l1 = 0;
+            for (int l = 0; l < k; ++l) {
+                const double d = d2(i, &C[3 * l]);
+                if (d < best) {
+                    best = d;
+                    l1 = l;
+                }
+            }
+            if (z[i] != l1) {
+                z[i] = l1;
+                change = true;
+            }
+        }
+        if (!change) break;
+        std::vector<int64_t> cnt(k, 0);
+        std::vector<double> sum(3 * (size_t)k, 0.0);
+        for (int64_t i = 0; i < n; ++i) {
+            ++cnt[z[i]];
+            for (int j = 0; j < 3; ++j) sum[3 * z[i] + j] += xyz[3 * i + j];
+        }
+        for (int l = 0; l < k; ++l) {
+            if (cnt[l] == 0) return {};
+            const double w = 1.0 / (double)cnt[l];
+            for (int j = 0; j < 3; ++j) C[3 * l + j] = sum[3 * l + j] * w;
+        }
+    }
+    return z;
+}
+
+// sum_k m_k^2.5 with m_k the rows coupled to a column of cluster k
+// (source/sm.f90:498-512); rows[i] lists the atoms coupled to row i; k <= 64.
+double kmeans_effort(const std::vector<std::vector<int>>& rows, const std::vector<int>& z, int k) {
+    std::vector<int64_t> m(k, 0);
+    for (const auto& r : rows) {
+        uint64_t mask = 0;
+        for (int a : r) mask |= 1ull << z[a];
+        for (int l = 0; l < k; ++l)
+            if (mask >> l & 1ull) ++m[l];
+    }
+    double e = 0.0;
+    for (int l = 0; l < k; ++l) {
+        const double v = (double)m[l];
+        e += v * v * std::sqrt(v);
+    }
+    return e;
+}
+
+}  // namespace
+
+// Mode-4 partition: k-means for 1..min(64, nat) clusters, the least
+// sum m_k^2.5 wins (ties: fewer clusters).  dH, dS: full column-major FP64.
+// The per-atom coupling pattern comes from the device pattern scan; the
+// candidates run on host threads, each with its own generator stream.
+std::vector<int64_t> kmeans_partition(ptbgpu_ctx* c, int64_t n, const double* dH, const double* dS, int64_t nat,
+                                      const double* xyz, const int64_t* aoat, uint64_t seed, int* nsm_out,
+                                      double* effort_out) {
+    PTB_CHECK(nat > 0 && xyz && aoat, PTBGPU_EINVAL, "k-means partition needs nat, xyz and aoat");
+    cudaStream_t s = c->stream;
+    std::vector<int> owner(n);
+    for (int64_t j = 0; j < n; ++j) {
+        PTB_CHECK(aoat[j] >= 1 && aoat[j] <= nat, PTBGPU_EINVAL, "aoat out of range");
+        owner[j] = (int)(aoat[j] - 1);
+    }
+    DevBuf& bo = c->buf(B_SM0);
+    bo.reserve(sizeof(int) * n);
+    PTB_CUDA(cudaMemcpyAsync(bo.ptr, owner.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    DevBuf& bf = c->buf(B_SM3);
+    bf.reserve((size_t)nat * n);
+    PTB_CUDA(cudaMemsetAsync(bf.ptr, 0, (size_t)nat * n, s));
+    k_pattern<<<(int)std::min<int64_t>(n, 148 * 8), 256, 0, s>>>(n, dH, dS, bo.as<int>(), bf.as<uint8_t>());
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+    std::vector<uint8_t> flags((size_t)nat * n);
+    PTB_CUDA(cudaMemcpyAsync(flags.data(), bf.ptr, flags.size(), cudaMemcpyDeviceToHost, s));
+    PTB_CUDA(cudaStreamSynchronize(s));
+    std::vector<std::vector<int>> rows(n);
+    for (int64_t a = 0; a < nat; ++a)
+        for (int64_t i = 0; i < n; ++i)
+            if (flags[a * n + i]) rows[i].push_back((int)a);
+    const int kmax = (int)std::min<int64_t>(64, nat);
+    std::vector<std::vector<int>> labels(kmax + 1);
+    std::vector<double> effort(kmax + 1, HUGE_VAL);
+    std::atomic<int> next{1};
+    auto work = [&] {
+        for (int k = next++; k <= kmax; k = next++) {
+            labels[k] = kmeans_pp(xyz, nat, k, seed);
+            if (!labels[k].empty()) effort[k] = kmeans_effort(rows, labels[k], k);
+        }
+    };
+    const int nthr = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthr; ++t) pool.emplace_back(work);
+    for (auto& t : pool) t.join();
+    int best = 0;
+    for (int k = 1; k <= kmax; ++k)
+        if (effort[k] < (best ? effort[best] : HUGE_VAL)) best = k;
+    PTB_CHECK(best > 0, PTBGPU_EITER, "k-means failed for every cluster count");
+    if (nsm_out) *nsm_out = best;
+    if (effort_out) *effort_out = effort[best];
+    std::vector<int64_t> part(nat);
+    for (int64_t a = 0; a < nat; ++a) part[a] = labels[best][a] + 1;
+    return part;
+}
+
+namespace {
+
 template <class T>
 T* upload(ptbgpu_ctx* c, int id, const std::vector<T>& v) {
     DevBuf& b = c->buf(id);
@@ -361,7 +531,6 @@ T* upload(ptbgpu_ctx* c, int id, const std::vector<T>& v) {
 void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* dH, const double* dS, double* dP,
                        int64_t nat, const double* xyz, const int64_t* aoat, int64_t columns, int64_t mode,
                        const int64_t* partition, const ptbgpu_opts* o, ptbgpu_stats* st) {
-    (void)xyz;
     const int prl = o ? (int)o->print_level : 0;
     const double filter = o ? o->filter : 0.0;
     if (mode == PTBGPU_SUBMATRIX_SIGN) fail(PTBGPU_ENOTIMPL, "submatrix_mode.eq.1 not implemented");
@@ -391,7 +560,16 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
     unpack_sym(s, n, n, dH, H, filter);
     unpack_sym(s, n, n, dS, S, filter);
 
-    // (1) grouping
+    // (1) grouping; mode 4 without a supplied partition runs the seeded k-means
+    std::vector<int64_t> own_part;
+    if (columns == PTBGPU_COLUMNS_KMEANS && partition == nullptr) {
+        int k = 0;
+        double eff = 0.0;
+        own_part = kmeans_partition(c, n, H, S, nat, xyz, aoat, kKmeansSeed, &k, &eff);
+        partition = own_part.data();
+        log_line(prl, 1, " k-means partition: %d clusters, effort %.6e", k, eff);
+        mark("k-means partition");
+    }
     std::vector<std::vector<int>> comb = group_columns(n, aoat, nat, columns, partition);
     const int nsm = (int)comb.size();
     std::vector<int> owner(n, -1), own_cols;
