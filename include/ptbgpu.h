@@ -239,18 +239,22 @@ int ptbgpu_mlpop2_device(ptbgpu_ctx* ctx, int64_t n, int64_t nao, const double* 
 int ptbgpu_symsq_bf16x3(ptbgpu_ctx* ctx, int64_t n, const double* X, float* C);
 /* The same with the three-plane split (hi, mid, lo) and six products, ~24-bit operands. */
 int ptbgpu_symsq_bf16x6(ptbgpu_ctx* ctx, int64_t n, const double* X, float* C);
-/* Either split with an explicit K block of the kernel: planes 2 or 3, kblock 32,
- * 64 or 0 (the autotuned choice). */
-int ptbgpu_symsq_split(ptbgpu_ctx* ctx, int64_t n, int64_t planes, int64_t kblock, const double* X, float* C);
+/* Either split with an explicit kernel: planes 2 or 3; kblock 32 or 64 (one CTA,
+ * that K block), 1032 or 1064 (two planes only: the CTA-pair cta_group::2
+ * kernel with K block 32 or 64), or 0 (the autotuned choice). */
+int ptbgpu_symsq_split(ptbgpu_ctx* ctx, int64_t n, int64_t planes, int64_t kblock, const double* X, float* C,
+                       double* ms);   /* ms (may be NULL): device time of the product launch(es) */
 /* C = A * B for n x n FP64 row-major host matrices, on the int8 tensor cores
  * with `slices` (6..8) 7-bit slices per operand row and an int32-exact K loop;
- * kblock 32 or 64 bytes (0 = default).  tri_a / tri_b: 0 full, 1 lower, 2 upper
+ * kblock 32 or 64 bytes (0 = default); variant 0 default, 1 A slices read
+ * from shared memory by every MMA, 2 A slices copied into tensor memory once
+ * per K step (bit-identical results).  tri_a / tri_b: 0 full, 1 lower, 2 upper
  * triangular (the other part is read as zero and its K blocks are skipped);
  * symmetric != 0: only the upper triangle of C is computed and mirrored.
  * n <= (2^31 - 1) / (slices * 127^2) rounded down to a multiple of 128.
  * ms (may be NULL) receives the device time of the product kernel. */
-int ptbgpu_oz_gemm(ptbgpu_ctx* ctx, int64_t n, int64_t slices, int64_t kblock, int64_t tri_a, int64_t tri_b,
-                   int64_t symmetric, const double* A, const double* B, double* C, double* ms);
+int ptbgpu_oz_gemm(ptbgpu_ctx* ctx, int64_t n, int64_t slices, int64_t kblock, int64_t variant, int64_t tri_a,
+                   int64_t tri_b, int64_t symmetric, const double* A, const double* B, double* C, double* ms);
 
 #ifdef __cplusplus
 }

@@ -111,8 +111,8 @@ def load_library():
     lib.ptbgpu_solve2.argtypes = [C.c_void_p, i64, i64, i64, i64, d, d, d, d, d, P(_Opts), P(_Stats)]
     lib.ptbgpu_symsq_bf16x3.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_bf16x6.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
-    lib.ptbgpu_symsq_split.argtypes = [C.c_void_p, i64, i64, i64, d, P(C.c_float)]
-    lib.ptbgpu_oz_gemm.argtypes = [C.c_void_p, i64, i64, i64, i64, i64, i64, d, d, d, d]
+    lib.ptbgpu_symsq_split.argtypes = [C.c_void_p, i64, i64, i64, d, P(C.c_float), d]
+    lib.ptbgpu_oz_gemm.argtypes = [C.c_void_p, i64, i64, i64, i64, i64, i64, i64, d, d, d, d]
     lib.ptbgpu_kmeans_partition.argtypes = [C.c_void_p, i64, d, d, i64, d, P(i64), C.c_uint64, P(_Opts), P(i64),
                                             P(i64), d]
     f = P(C.c_float)
@@ -342,22 +342,28 @@ class Context:
         """C = X X with the three-plane split (bf16x6 products); FP32 result."""
         return self._symsq(X, self._lib.ptbgpu_symsq_bf16x6)
 
-    def symsq_split(self, X: np.ndarray, planes: int, kblock: int) -> np.ndarray:
-        """C = X X with an explicit plane count (2 or 3) and kernel K block (32, 64, 0 = tuned)."""
-        return self._symsq(X, lambda h, n, x, o: self._lib.ptbgpu_symsq_split(h, n, planes, kblock, x, o))
+    def symsq_split(self, X: np.ndarray, planes: int, kblock: int, timed: bool = False):
+        """C = X X with an explicit plane count (2 or 3) and kernel: K block 32 /
+        64 (one CTA), 1032 / 1064 (CTA pair, two planes), 0 = tuned.  timed:
+        returns (C, device milliseconds of the product launches)."""
+        ms = C.c_double(0.0)
+        out = self._symsq(X, lambda h, n, x, o: self._lib.ptbgpu_symsq_split(h, n, planes, kblock, x, o,
+                                                                              C.byref(ms)))
+        return (out, ms.value) if timed else out
 
     def oz_gemm(self, A: np.ndarray, B: np.ndarray, slices: int = 7, kblock: int = 0, tri_a: int = 0,
-                tri_b: int = 0, symmetric: bool = False, timed: bool = False):
-        """C = A B in FP64 on the int8 tensor cores (slices 6..8 per operand row);
-        tri_*: 0 full, 1 lower, 2 upper triangular operand; symmetric: only the
-        upper triangle of C is computed and mirrored.  timed: returns (C, device
-        milliseconds of the product kernel)."""
+                tri_b: int = 0, symmetric: bool = False, timed: bool = False, variant: int = 0):
+        """C = A B in FP64 on the int8 tensor cores (4 or 6..8 slices per
+        operand row); tri_*: 0 full, 1 lower, 2 upper triangular operand;
+        symmetric: only the upper triangle of C is computed and mirrored;
+        variant: 0 default, 1 A from shared memory, 2 A in tensor memory.
+        timed: returns (C, device milliseconds of the product kernel)."""
         Ah, Bh = _f64(A), _f64(B)
         n = Ah.shape[0]
         out = np.zeros((n, n), dtype=np.float64)
         ms = C.c_double(0.0)
-        self._check(self._lib.ptbgpu_oz_gemm(self._h, int(n), int(slices), int(kblock), int(tri_a), int(tri_b),
-                                             int(bool(symmetric)), _dptr(Ah), _dptr(Bh), _dptr(out),
+        self._check(self._lib.ptbgpu_oz_gemm(self._h, int(n), int(slices), int(kblock), int(variant), int(tri_a),
+                                             int(tri_b), int(bool(symmetric)), _dptr(Ah), _dptr(Bh), _dptr(out),
                                              C.byref(ms)))
         return (out, ms.value) if timed else out
 

@@ -4,6 +4,7 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "tc_gemm.cuh"
 
 namespace ptb {
 void tc_purify_entry(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, const double* dS, double* dP,
@@ -14,7 +15,8 @@ std::vector<int64_t> kmeans_partition(ptbgpu_ctx* c, int64_t n, const double* dH
                                       double* effort_out);
 void mlpop14_device(ptbgpu_ctx* c, int64_t n, const double* dSpk, double x, float* s34, float* s14);
 void mlpop2_diag_device(ptbgpu_ctx* c, int64_t n, const double* dPpk, const float* s1, const float* s2, double* xd);
-void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int tri_a, int tri_b, bool sym, const double* hA,
+void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int variant, int tri_a, int tri_b, bool sym,
+                   const double* hA,
                    const double* hB, double* hC);
 void purify_ref_device(ptbgpu_ctx* c, const ptbgpu_pur_settings& pur, int64_t n, const double* dH,
                        const double* dS, double* dP, const ptbgpu_opts* o, ptbgpu_stats* st);
@@ -260,11 +262,23 @@ int ptbgpu_symsq_bf16x6(ptbgpu_ctx* c, int64_t n, const double* X, float* C) {
     });
 }
 
-int ptbgpu_symsq_split(ptbgpu_ctx* c, int64_t n, int64_t planes, int64_t kblock, const double* X, float* C) {
+int ptbgpu_symsq_split(ptbgpu_ctx* c, int64_t n, int64_t planes, int64_t kblock, const double* X, float* C,
+                       double* ms) {
     return guarded(c, [&] {
-        PTB_CHECK(n > 0 && X && C && (planes == 2 || planes == 3) && (kblock == 0 || kblock == 32 || kblock == 64),
+        // kblock: 0 tuned, 32 / 64 one CTA, 1032 / 1064 CTA pair (two planes only)
+        const bool pair = kblock == tc::kPairKernel + 32 || kblock == tc::kPairKernel + 64;
+        PTB_CHECK(n > 0 && X && C && (planes == 2 || planes == 3) &&
+                      (kblock == 0 || kblock == 32 || kblock == 64 || (pair && planes == 2)),
                   PTBGPU_EINVAL, "bad arguments");
         symsq_entry(c, n, (int)planes, (int)kblock, X, C);
+        if (ms) {
+            *ms = 0.0;
+            for (const auto& t : c->timed) {
+                float x = 0.f;
+                PTB_CUDA(cudaEventElapsedTime(&x, t.a, t.b));
+                *ms += x;
+            }
+        }
     });
 }
 
@@ -358,14 +372,15 @@ int ptbgpu_mlpop2_device(ptbgpu_ctx* c, int64_t n, int64_t nao, const double* dP
     });
 }
 
-int ptbgpu_oz_gemm(ptbgpu_ctx* c, int64_t n, int64_t slices, int64_t kblock, int64_t tri_a, int64_t tri_b,
-                   int64_t symmetric, const double* A, const double* B, double* Cout, double* ms) {
+int ptbgpu_oz_gemm(ptbgpu_ctx* c, int64_t n, int64_t slices, int64_t kblock, int64_t variant, int64_t tri_a,
+                   int64_t tri_b, int64_t symmetric, const double* A, const double* B, double* Cout, double* ms) {
     return guarded(c, [&] {
-        PTB_CHECK(n > 0 && A && B && Cout && slices >= 6 && slices <= 8 &&
-                      (kblock == 0 || kblock == 32 || kblock == 64) && tri_a >= 0 && tri_a <= 2 && tri_b >= 0 &&
-                      tri_b <= 2,
+        PTB_CHECK(n > 0 && A && B && Cout && (slices == 4 || (slices >= 6 && slices <= 8)) &&
+                      (kblock == 0 || kblock == 32 || kblock == 64) && variant >= 0 && variant <= 2 &&
+                      tri_a >= 0 && tri_a <= 2 && tri_b >= 0 && tri_b <= 2,
                   PTBGPU_EINVAL, "bad arguments");
-        oz_gemm_entry(c, n, (int)slices, (int)kblock, (int)tri_a, (int)tri_b, symmetric != 0, A, B, Cout);
+        oz_gemm_entry(c, n, (int)slices, (int)kblock, (int)variant, (int)tri_a, (int)tri_b, symmetric != 0, A, B,
+                      Cout);
         if (ms) {
             *ms = 0.0;
             for (const auto& t : c->timed) {

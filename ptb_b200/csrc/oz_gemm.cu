@@ -37,6 +37,7 @@ using namespace tc::ptx;
 constexpr int THREADS = 256;
 constexpr int kSmemBudget = 196608;
 constexpr int kTmemCols = 512;
+constexpr int kDefaultVariant = V_SMEM_A;
 
 template <int S, int RB>
 struct OzCfg {
@@ -173,6 +174,108 @@ struct OzMaps {
     CUtensorMap b;   // S stacked B planes
 };
 
+template <int W>
+__device__ __forceinline__ void tmem_ldw(uint32_t taddr, uint32_t (&v)[W]) {
+    if constexpr (W == 32) tmem_ld32(taddr, v);
+    else tmem_ld16(taddr, v);
+}
+
+// W columns [c0, c0 + W) of the tile: combine the S group accumulators
+// (columns g * NT + c0 ..) in FP64, smallest group first, rescale by
+// 2^(e_r + f_c) and write the fused output.
+template <int EPI, int S, int NT, int W>
+__device__ __forceinline__ void oz_epilogue_chunk(const OzEpi& ep, uint32_t tmem, int bi, int bj, int q4, int lane,
+                                                  int c0, bool empty_k, int er, const int* __restrict__ eb,
+                                                  double& tr, double& ss) {
+    const int64_t n = ep.n;
+    const int64_t r = (int64_t)bi * BM + q4 * 32 + lane;
+    double acc[W];
+#pragma unroll
+    for (int j = 0; j < W; ++j) acc[j] = 0.0;
+#pragma unroll 1
+    for (int g = S - 1; g >= 0; --g) {
+        uint32_t v[W];
+        __syncwarp();
+        tmem_ldw<W>(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(g * NT + c0), v);
+        const double w = pow2i(-7 * (g + 2));
+#pragma unroll
+        for (int j = 0; j < W; ++j) acc[j] += (double)(int)v[j] * w;
+    }
+    if (empty_k) {
+#pragma unroll
+        for (int j = 0; j < W; ++j) acc[j] = 0.0;
+    }
+    if (r >= n) return;
+    const int64_t cb = (int64_t)bj * NT + c0;
+    if (EPI == OZ_OUT) {
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            const int64_t c = cb + j;
+            if (c < n) ep.out[r * ep.ors + c * ep.ocs] = ep.alpha * scale2(acc[j], er + eb[c]);
+        }
+    } else {
+        if (cb + W - 1 < r) return;   // chunk entirely below the diagonal
+        const int64_t ld = ep.ors;
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            const int64_t c = cb + j;
+            if (c < r || c >= n) continue;
+            double val = ep.alpha * scale2(acc[j], er + eb[c]);
+            if (ep.xin && !ep.square) val = 2.0 * ep.xin[r + c * ld] - val;
+            ep.out[r + c * ld] = val;
+            if (c == r) {
+                tr += val;
+                ss += val * val;
+            } else {
+                ss += 2.0 * val * val;
+                ep.out[c + r * ld] = val;
+            }
+        }
+    }
+}
+
+// Epilogue warps 4..7 (q4 = TMEM lane quarter): wait for the accumulators
+// (bounded), drain them chunk by chunk, reduce the per-tile trace / sum of
+// squares of a symmetric result in a fixed order.
+template <int EPI, int S, int NT>
+__device__ __forceinline__ void oz_epilogue(const OzEpi& ep, uint32_t tmem, uint32_t accum_bar, int* abort_flag,
+                                            double* red, int bi, int bj, int q4, int lane, int nk,
+                                            const int* __restrict__ ea, const int* __restrict__ eb) {
+    static_assert(NT == 64 || NT == 48, "tile widths of 64 or 48 columns");
+    const int64_t r = (int64_t)bi * BM + q4 * 32 + lane;
+    double tr = 0.0, ss = 0.0;
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(accum_bar, 0));
+    if (!ok && lane == 0) {
+        set_err(ep.err, 131);
+        *(volatile int*)abort_flag = 1;
+    }
+    const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
+    tc_fence_after();
+    if (ok && !aborted) {
+        const int er = r < ep.n ? ea[r] : 0;
+        oz_epilogue_chunk<EPI, S, NT, 32>(ep, tmem, bi, bj, q4, lane, 0, nk == 0, er, eb, tr, ss);
+        if constexpr (NT == 64)
+            oz_epilogue_chunk<EPI, S, NT, 32>(ep, tmem, bi, bj, q4, lane, 32, nk == 0, er, eb, tr, ss);
+        else
+            oz_epilogue_chunk<EPI, S, NT, 16>(ep, tmem, bi, bj, q4, lane, 32, nk == 0, er, eb, tr, ss);
+    }
+    if (EPI == OZ_SYM && ep.stats) {
+        for (int o = 16; o > 0; o >>= 1) {
+            tr += __shfl_xor_sync(0xffffffffu, tr, o);
+            ss += __shfl_xor_sync(0xffffffffu, ss, o);
+        }
+        if (lane == 0) {
+            red[2 * q4] = tr;
+            red[2 * q4 + 1] = ss;
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");   // epilogue warps only
+        if (q4 == 0 && lane == 0) {
+            ep.stats[2 * blockIdx.x] = red[0] + red[2] + red[4] + red[6];
+            ep.stats[2 * blockIdx.x + 1] = red[1] + red[3] + red[5] + red[7];
+        }
+    }
+}
+
 template <int EPI, int S, int RB>
 __global__ void __launch_bounds__(THREADS, 1)
     k_oz_product(const __grid_constant__ OzMaps maps, const int4* __restrict__ tiles, const int* __restrict__ ea,
@@ -278,81 +381,154 @@ __global__ void __launch_bounds__(THREADS, 1)
         umma_commit(accum_bar);
         if (!ok) mbar_wait(accum_bar, 0);
     } else if (warp >= 4) {
-        // ---------------- epilogue ----------------
-        const int q4 = warp - 4;
-        const int64_t n = ep.n;
-        const int64_t r = (int64_t)bi * BM + q4 * 32 + lane;
-        double tr = 0.0, ss = 0.0;
-        const bool ok = __all_sync(0xffffffffu, mbar_wait(accum_bar, 0));
-        if (!ok && lane == 0) {
-            set_err(ep.err, 131);
-            *(volatile int*)abort_flag = 1;
+        oz_epilogue<EPI, S, BN>(ep, tmem, accum_bar, abort_flag, red, bi, bj, warp - 4, lane, nk, ea, eb);
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 2) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTmemCols));
+    }
+}
+
+// Same product with the A slices in tensor memory: per K32 step, tcgen05.cp
+// copies the S A-slices (128 rows x 32 bytes each) from the stage into one of
+// two TMEM buffers (columns 384.. and 448..), and the S(S+1)/2 MMAs read A from
+// there and only the B slice from shared memory, which removes the A re-reads
+// that bound the kernel above (each A slice feeds S - p MMAs).  The
+// accumulators are NT columns wide (48 for 7 or 8 slices, 64 for fewer) so
+// that S * NT <= 384.  A buffer is rewritten only after the MMAs that read it
+// have completed (tcgen05.commit to a per-buffer mbarrier, bounded wait).
+template <int EPI, int S, int RB, int NT>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_oz_product_ta(const __grid_constant__ OzMaps maps, const int4* __restrict__ tiles, const int* __restrict__ ea,
+                    const int* __restrict__ eb, OzEpi ep) {
+    constexpr int A_TILE = BM * RB;
+    constexpr int B_TILE = NT * RB;
+    constexpr int STAGE = S * (A_TILE + B_TILE);
+    constexpr int STAGES = (kSmemBudget / STAGE) > 4 ? 4 : (kSmemBudget / STAGE);
+    constexpr uint32_t LAYOUT = RB == 64 ? 4u : 6u;
+    constexpr uint32_t SBO = 8u * RB;
+    constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) |
+                               ((uint32_t)(BM >> 4) << 24);
+    constexpr uint32_t TA = 384;   // first TMEM column of the A buffers (2 x 8 S columns)
+    static_assert(S * NT <= (int)TA && TA + 16 * S <= (uint32_t)kTmemCols, "TMEM budget");
+    static_assert(NT % 16 == 0 && STAGES >= 2, "tile shape");
+    static_assert(A_TILE % (8 * RB) == 0 && B_TILE % (8 * RB) == 0, "tiles keep the swizzle atoms aligned");
+
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t base_raw = smem_u32(smem_raw);
+    const uint32_t base = (base_raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - base_raw);
+    const uint32_t bar0 = base + STAGES * STAGE;
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+    const uint32_t accum_bar = bar0 + 8u * (2 * STAGES);
+    const uint32_t abuf_bar0 = bar0 + 8u * (2 * STAGES + 1);   // two: one per A buffer
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + STAGES * STAGE + 8 * (2 * STAGES + 3));
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+    double* red = reinterpret_cast<double*>(gbase + STAGES * STAGE + 128);   // 8 doubles
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int4 tile = tiles[blockIdx.x];
+    const int bi = tile.x, bj = tile.y;
+    const int kb0 = tile.z / RB;
+    const int nk = (tile.w - tile.z) / RB;
+
+    auto a_tile = [&](int s, int p) { return base + s * STAGE + p * A_TILE; };
+    auto b_tile = [&](int s, int q) { return base + s * STAGE + S * A_TILE + q * B_TILE; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
         }
-        const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
-        tc_fence_after();
-        if (ok && !aborted) {
-            const int er = r < n ? ea[r] : 0;
-            for (int c0 = 0; c0 < BN; c0 += 32) {
-                double acc[32];
+        mbar_init(accum_bar, 1);
+        mbar_init(abuf_bar0, 1);
+        mbar_init(abuf_bar0 + 8u, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"((uint32_t)kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer ----------------
+        int issued_phase[STAGES];
+        for (int s = 0; s < STAGES; ++s) issued_phase[s] = -1;
+        for (int it = 0; it < nk; ++it) {
+            const int s = it % STAGES, round = it / STAGES;
+            if (round > 0 && !mbar_wait(empty_bar(s), (round - 1) & 1)) {
+                set_err(ep.err, 141);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            mbar_expect_tx(full_bar(s), STAGE);
+            const int kx = (kb0 + it) * RB;
+            for (int p = 0; p < S; ++p)
+                tma_load_2d(a_tile(s, p), &maps.a, full_bar(s), kx, (int)(p * ep.ldp) + bi * BM);
+            for (int q = 0; q < S; ++q)
+                tma_load_2d(b_tile(s, q), &maps.b, full_bar(s), kx, (int)(q * ep.ldp) + bj * NT);
+            issued_phase[s] = round & 1;
+        }
+        for (int s = 0; s < STAGES; ++s)
+            if (issued_phase[s] >= 0 && !mbar_wait(full_bar(s), (uint32_t)issued_phase[s])) set_err(ep.err, 142);
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- copy + MMA issuer ----------------
+        bool ok = true;
+        int t = 0;   // K32 step counter over the tile
+        for (int it = 0; it < nk && ok; ++it) {
+            const int s = it % STAGES, round = it / STAGES;
+            if (!mbar_wait(full_bar(s), round & 1)) {
+                set_err(ep.err, 151);
+                *(volatile int*)abort_flag = 1;
+                ok = false;
+                break;
+            }
+            if (*(volatile int*)abort_flag) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
 #pragma unroll
-                for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-#pragma unroll 1
-                for (int g = S - 1; g >= 0; --g) {
-                    uint32_t v[32];
-                    __syncwarp();
-                    tmem_ld32(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(g * BN + c0), v);
-                    const double w = pow2i(-7 * (g + 2));
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) acc[j] += (double)(int)v[j] * w;
+            for (int k = 0; k < RB / 32; ++k, ++t) {
+                const int b = t & 1;
+                if (t >= 2 && !mbar_wait(abuf_bar0 + 8u * b, (uint32_t)(((t - 2) >> 1) & 1))) {
+                    set_err(ep.err, 152);
+                    *(volatile int*)abort_flag = 1;
+                    ok = false;
+                    break;
                 }
-                if (nk == 0) {
+                const uint32_t ta = tmem + TA + (uint32_t)(b * 8 * S);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-                }
-                if (r >= n) continue;
-                const int64_t cb = (int64_t)bj * BN + c0;
-                if (EPI == OZ_OUT) {
+                for (int p = 0; p < S; ++p)
+                    tmem_cp_128x256b(ta + 8u * p, sdesc(a_tile(s, p) + k * 32, SBO, LAYOUT));
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int64_t c = cb + j;
-                        if (c < n) ep.out[r * ep.ors + c * ep.ocs] = ep.alpha * scale2(acc[j], er + eb[c]);
+                for (int p = 0; p < S; ++p) {
+#pragma unroll
+                    for (int q = 0; q < S - p; ++q) {
+                        const uint64_t bd = sdesc(b_tile(s, q) + k * 32, SBO, LAYOUT);
+                        umma_i8_ta(tmem + (uint32_t)((p + q) * NT), ta + 8u * p, bd, IDESC, (t | p) != 0);
                     }
-                } else {
-                    if (cb + 31 < r) continue;   // chunk entirely below the diagonal
-                    const int64_t ld = ep.ors;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int64_t c = cb + j;
-                        if (c < r || c >= n) continue;
-                        double val = ep.alpha * scale2(acc[j], er + eb[c]);
-                        if (ep.xin && !ep.square) val = 2.0 * ep.xin[r + c * ld] - val;
-                        ep.out[r + c * ld] = val;
-                        if (c == r) {
-                            tr += val;
-                            ss += val * val;
-                        } else {
-                            ss += 2.0 * val * val;
-                            ep.out[c + r * ld] = val;
-                        }
-                    }
                 }
+                umma_commit(abuf_bar0 + 8u * b);
             }
+            umma_commit(empty_bar(s));
         }
-        if (EPI == OZ_SYM && ep.stats) {
-            for (int o = 16; o > 0; o >>= 1) {
-                tr += __shfl_xor_sync(0xffffffffu, tr, o);
-                ss += __shfl_xor_sync(0xffffffffu, ss, o);
-            }
-            if (lane == 0) {
-                red[2 * q4] = tr;
-                red[2 * q4 + 1] = ss;
-            }
-            asm volatile("bar.sync 1, 128;" ::: "memory");   // epilogue warps only
-            if (q4 == 0 && lane == 0) {
-                ep.stats[2 * blockIdx.x] = red[0] + red[2] + red[4] + red[6];
-                ep.stats[2 * blockIdx.x + 1] = red[1] + red[3] + red[5] + red[7];
-            }
-        }
+        umma_commit(accum_bar);
+        if (!ok) mbar_wait(accum_bar, 0);
+    } else if (warp >= 4) {
+        oz_epilogue<EPI, S, NT>(ep, tmem, accum_bar, abort_flag, red, bi, bj, warp - 4, lane, nk, ea, eb);
     }
     __syncwarp();
     tc_fence_before();
@@ -406,21 +582,45 @@ void launch_t(cudaStream_t s, const OzMaps& maps, const int4* tiles, int ntiles,
     count_launch();
 }
 
+constexpr int ta_tile_n(int S) { return S >= 7 ? 48 : 64; }
+
+template <int EPI, int S, int RB>
+void launch_ta(cudaStream_t s, const OzMaps& maps, const int4* tiles, int ntiles, const Operand& a,
+               const Operand& b, const OzEpi& ep) {
+    constexpr int NT = ta_tile_n(S);
+    constexpr int STAGE = S * (BM * RB + NT * RB);
+    constexpr int STAGES = (kSmemBudget / STAGE) > 4 ? 4 : (kSmemBudget / STAGE);
+    constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+    static bool attr = false;
+    if (!attr) {
+        PTB_CUDA(cudaFuncSetAttribute(k_oz_product_ta<EPI, S, RB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      SMEM));
+        attr = true;
+    }
+    k_oz_product_ta<EPI, S, RB, NT><<<ntiles, THREADS, SMEM, s>>>(maps, tiles, a.exps, b.exps, ep);
+    count_launch();
+}
+
 template <int EPI, int S>
-void launch_s(cudaStream_t s, int rb, const OzMaps& maps, const int4* tiles, int ntiles, const Operand& a,
-              const Operand& b, const OzEpi& ep) {
-    if (rb == 64) launch_t<EPI, S, 64>(s, maps, tiles, ntiles, a, b, ep);
-    else launch_t<EPI, S, 32>(s, maps, tiles, ntiles, a, b, ep);
+void launch_s(cudaStream_t s, int rb, int variant, const OzMaps& maps, const int4* tiles, int ntiles,
+              const Operand& a, const Operand& b, const OzEpi& ep) {
+    if (variant == V_TMEM_A) {
+        if (rb == 64) launch_ta<EPI, S, 64>(s, maps, tiles, ntiles, a, b, ep);
+        else launch_ta<EPI, S, 32>(s, maps, tiles, ntiles, a, b, ep);
+    } else {
+        if (rb == 64) launch_t<EPI, S, 64>(s, maps, tiles, ntiles, a, b, ep);
+        else launch_t<EPI, S, 32>(s, maps, tiles, ntiles, a, b, ep);
+    }
 }
 
 template <int EPI>
-void launch_e(cudaStream_t s, int S, int rb, const OzMaps& maps, const int4* tiles, int ntiles, const Operand& a,
-              const Operand& b, const OzEpi& ep) {
+void launch_e(cudaStream_t s, int S, int rb, int variant, const OzMaps& maps, const int4* tiles, int ntiles,
+              const Operand& a, const Operand& b, const OzEpi& ep) {
     switch (S) {
-        case 4: launch_s<EPI, 4>(s, rb, maps, tiles, ntiles, a, b, ep); break;
-        case 6: launch_s<EPI, 6>(s, rb, maps, tiles, ntiles, a, b, ep); break;
-        case 7: launch_s<EPI, 7>(s, rb, maps, tiles, ntiles, a, b, ep); break;
-        case 8: launch_s<EPI, 8>(s, rb, maps, tiles, ntiles, a, b, ep); break;
+        case 4: launch_s<EPI, 4>(s, rb, variant, maps, tiles, ntiles, a, b, ep); break;
+        case 6: launch_s<EPI, 6>(s, rb, variant, maps, tiles, ntiles, a, b, ep); break;
+        case 7: launch_s<EPI, 7>(s, rb, variant, maps, tiles, ntiles, a, b, ep); break;
+        case 8: launch_s<EPI, 8>(s, rb, variant, maps, tiles, ntiles, a, b, ep); break;
         default: PTB_CHECK(false, PTBGPU_EINVAL, "unsupported slice count %d (4, 6, 7 or 8)", S);
     }
 }
@@ -451,19 +651,27 @@ void slice(cudaStream_t s, const double* M, int64_t rs, int64_t cs, int64_t n, i
     PTB_CUDA(cudaGetLastError());
 }
 
-std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri) {
-    const int nbi = (int)(ldp / BM), nbj = (int)(ldp / BN);
+int resolve_variant(int variant) { return variant == V_DEFAULT ? kDefaultVariant : variant; }
+
+int tile_n(int S, int variant) { return resolve_variant(variant) == V_TMEM_A ? ta_tile_n(S) : BN; }
+
+std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int bn) {
+    PTB_CHECK(bn == 64 || bn == 48, PTBGPU_EINVAL, "tile width must be 64 or 48");
+    // column tiles may overhang ldp (the operand rows there are padding or the
+    // next plane; those columns are never written)
+    const int nbi = (int)(ldp / BM), nbj = (int)((ldp + bn - 1) / bn);
     std::vector<int4> t;
     const int G = 16;
     for (int g0 = 0; g0 < nbi; g0 += G)
         for (int bj = 0; bj < nbj; ++bj)
             for (int bi = g0; bi < std::min(nbi, g0 + G); ++bi) {
-                if (upper && (int64_t)bj * BN + BN - 1 < (int64_t)bi * BM) continue;
+                if (upper && (int64_t)bj * bn + bn - 1 < (int64_t)bi * BM) continue;
                 int64_t k0 = 0, k1 = ldp;
+                // K ranges in whole 128-blocks: the masked triangle reads as zero beyond
                 if (a_tri == TRI_LOWER) k1 = std::min<int64_t>(k1, (int64_t)(bi + 1) * BM);
                 if (a_tri == TRI_UPPER) k0 = std::max<int64_t>(k0, (int64_t)bi * BM);
-                if (b_tri == TRI_LOWER) k1 = std::min<int64_t>(k1, (int64_t)(bj + 1) * BN);
-                if (b_tri == TRI_UPPER) k0 = std::max<int64_t>(k0, (int64_t)bj * BN);
+                if (b_tri == TRI_LOWER) k1 = std::min<int64_t>(k1, round_up((int64_t)(bj + 1) * bn, BM));
+                if (b_tri == TRI_UPPER) k0 = std::max<int64_t>(k0, (int64_t)bj * bn / BM * BM);
                 PTB_CHECK(k1 > k0, PTBGPU_EINVAL, "empty K range in a tile");
                 t.push_back(make_int4(bi, bj, (int)k0, (int)k1));
             }
@@ -472,7 +680,9 @@ std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri) {
 }
 
 void product(cudaStream_t s, int epi, const Operand& a, const Operand& b, const int4* tiles_dev, int ntiles,
-             const OzEpi& ep, int rb) {
+             const OzEpi& ep, int rb, int variant) {
+    variant = resolve_variant(variant);
+    PTB_CHECK(variant == V_SMEM_A || variant == V_TMEM_A, PTBGPU_EINVAL, "bad kernel variant %d", variant);
     if (rb == 0) rb = 64;   // measured faster than 32 at ndim 11776 (S = 7 and 8)
     PTB_CHECK(rb == 32 || rb == 64, PTBGPU_EINVAL, "K block must be 32 or 64 bytes");
     PTB_CHECK(a.S == b.S && a.ldp == b.ldp && a.ldp == ep.ldp, PTBGPU_EINVAL, "operands do not match");
@@ -482,9 +692,9 @@ void product(cudaStream_t s, int epi, const Operand& a, const Operand& b, const 
     if (ntiles == 0) return;
     OzMaps maps;
     encode_planes(&maps.a, a, BM, rb);
-    encode_planes(&maps.b, b, BN, rb);
-    if (epi == OZ_OUT) launch_e<OZ_OUT>(s, a.S, rb, maps, tiles_dev, ntiles, a, b, ep);
-    else launch_e<OZ_SYM>(s, a.S, rb, maps, tiles_dev, ntiles, a, b, ep);
+    encode_planes(&maps.b, b, tile_n(a.S, variant), rb);
+    if (epi == OZ_OUT) launch_e<OZ_OUT>(s, a.S, rb, variant, maps, tiles_dev, ntiles, a, b, ep);
+    else launch_e<OZ_SYM>(s, a.S, rb, variant, maps, tiles_dev, ntiles, a, b, ep);
     PTB_CUDA(cudaGetLastError());
 }
 

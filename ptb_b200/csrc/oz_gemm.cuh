@@ -64,15 +64,23 @@ int64_t padded(int64_t n);   // round_up(n, 128)
 void slice(cudaStream_t s, const double* M, int64_t rs, int64_t cs, int64_t n, int tri, const Operand& op,
            unsigned long long* rowmax);
 
-// Tiles {bi, bj, k0, k1} over ldp: all, or only those touching the upper
-// triangle; the K range of each tile is cut to the nonzero part of a
-// triangular A (rows of A) or B (rows of B).  Longest K ranges first.
-std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri);
+// Kernel variants: A slices re-read from shared memory by every MMA (64-column
+// tiles), or copied once per K step into tensor memory (48-column tiles for 7
+// or 8 slices, 64 for fewer).  Both give bit-identical results.
+enum Variant : int { V_DEFAULT = 0, V_SMEM_A = 1, V_TMEM_A = 2 };
+int tile_n(int S, int variant = V_DEFAULT);   // output columns per tile
 
-// C(i,j) = sum_k A(i,k) B(j,k) over the listed tiles.  rb: K bytes per stage,
-// 64 (64B swizzle) or 32 (32B swizzle); 0 = the default.
+// Tiles {bi, bj, k0, k1}: 128-row blocks of ldp by bn-column blocks (the last
+// may overhang), all or only those touching the upper triangle; the K range of
+// each tile is cut to the nonzero part (whole 128-blocks) of a triangular A
+// (rows of A) or B (rows of B).  Longest K ranges first.
+std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int bn);
+
+// C(i,j) = sum_k A(i,k) B(j,k) over the listed tiles, which must be built
+// with tile_n(S, variant).  rb: K bytes per stage, 64 (64B swizzle) or 32
+// (32B swizzle); 0 = the default.
 void product(cudaStream_t s, int epi, const Operand& a, const Operand& b, const int4* tiles_dev, int ntiles,
-             const OzEpi& ep, int rb = 0);
+             const OzEpi& ep, int rb = 0, int variant = V_DEFAULT);
 
 }  // namespace oz
 }  // namespace ptb

@@ -160,7 +160,8 @@ void mlpop2_diag_device(ptbgpu_ctx* c, int64_t n, const double* dPpk, const floa
     oa.S = ob.S = S;
     oz::slice(s, P, 1, n, n, oz::TRI_NONE, oa, brm.as<unsigned long long>());
     oz::slice(s, S1, n, 1, n, oz::TRI_NONE, ob, brm.as<unsigned long long>());
-    const std::vector<int4> t = oz::make_tiles(ldp, false, oz::TRI_NONE, oz::TRI_NONE);
+    const int bn = oz::tile_n(S);
+    const std::vector<int4> t = oz::make_tiles(ldp, false, oz::TRI_NONE, oz::TRI_NONE, bn);
     DevBuf& bt = c->buf(B_OZT);
     bt.reserve(sizeof(int4) * t.size());
     PTB_CUDA(cudaMemcpyAsync(bt.ptr, t.data(), sizeof(int4) * t.size(), cudaMemcpyHostToDevice, s));
@@ -179,7 +180,7 @@ void mlpop2_diag_device(ptbgpu_ctx* c, int64_t n, const double* dPpk, const floa
     c->timed.push_back({2, e0, e1});
     double kk = 0.0;
     for (const int4& x : t) kk += (double)(x.w - x.z);
-    c->oz_ops += 2.0 * oz::BM * oz::BN * kk * (double)(S * (S + 1) / 2);
+    c->oz_ops += 2.0 * oz::BM * bn * kk * (double)(S * (S + 1) / 2);
     k_diag_s2c<<<(unsigned)((n + 31) / 32), dim3(32, 8), 0, s>>>(n, s2, Cm, bxd.as<double>());
     count_launch();
     PTB_CUDA(cudaGetLastError());

@@ -275,14 +275,17 @@ int grid1(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(n, 148
 
 // A tensor-core product bracketed by CUDA events on the launching stream; the
 // C-ABI layer sums the elapsed times per kind into the call's stats.
-void timed_product(ptbgpu_ctx* c, int epi, int np, int64_t ldp, const void* const* pa, const void* const* pb,
-                   const tc::ProdList& prods, const int2* tiles, int ntiles, const tc::EpiParams& ep,
-                   int kblock = 0) {
+// Returns the number of per-CTA stats partials the launch wrote.
+int timed_product(ptbgpu_ctx* c, int epi, int np, int64_t ldp, const void* const* pa, const void* const* pb,
+                  const tc::ProdList& prods, const int2* tiles, int ntiles, const tc::EpiParams& ep, int kblock = 0,
+                  const int2* pairs = nullptr, int npairs = 0) {
     cudaEvent_t a = c->take_event(), b = c->take_event();
     PTB_CUDA(cudaEventRecord(a, c->stream));
-    tc::launch_product(c->stream, epi, np, ldp, pa, pb, prods, tiles, ntiles, ep, kblock);
+    const int parts = tc::launch_product(c->stream, epi, np, ldp, pa, pb, prods, tiles, ntiles, ep, kblock, pairs,
+                                         npairs);
     PTB_CUDA(cudaEventRecord(b, c->stream));
     c->timed.push_back({epi == tc::EPI_SP2 ? 0 : 1, a, b});
+    return parts;
 }
 
 // Device-time phase log of one purification call (print level >= 2): CUDA
@@ -336,8 +339,9 @@ void oz_slice(ptbgpu_ctx* c, const double* M, int64_t rs, int64_t cs, int64_t n,
 // One product over a freshly uploaded tile list, bracketed by CUDA events.
 // Returns the tile count (the number of per-tile stats of OZ_SYM).
 int oz_product(ptbgpu_ctx* c, int epi, const oz::Operand& a, const oz::Operand& b, bool upper, int tri_a,
-               int tri_b, oz::OzEpi ep, int rb = 0) {
-    const std::vector<int4> t = oz::make_tiles(a.ldp, upper, tri_a, tri_b);
+               int tri_b, oz::OzEpi ep, int rb = 0, int variant = oz::V_DEFAULT) {
+    const int bn = oz::tile_n(a.S, variant);
+    const std::vector<int4> t = oz::make_tiles(a.ldp, upper, tri_a, tri_b, bn);
     DevBuf& bt = c->buf(B_OZT);
     bt.reserve(sizeof(int4) * t.size());
     PTB_CUDA(cudaMemcpyAsync(bt.ptr, t.data(), sizeof(int4) * t.size(), cudaMemcpyHostToDevice, c->stream));
@@ -345,10 +349,10 @@ int oz_product(ptbgpu_ctx* c, int epi, const oz::Operand& a, const oz::Operand& 
     if (!ep.err) ep.err = &c->flags->timeout;
     double kk = 0.0;
     for (const int4& x : t) kk += (double)(x.w - x.z);
-    c->oz_ops += 2.0 * oz::BM * oz::BN * kk * (double)(a.S * (a.S + 1) / 2);
+    c->oz_ops += 2.0 * oz::BM * bn * kk * (double)(a.S * (a.S + 1) / 2);
     cudaEvent_t e0 = c->take_event(), e1 = c->take_event();
     PTB_CUDA(cudaEventRecord(e0, c->stream));
-    oz::product(c->stream, epi, a, b, bt.as<int4>(), (int)t.size(), ep, rb);
+    oz::product(c->stream, epi, a, b, bt.as<int4>(), (int)t.size(), ep, rb, variant);
     PTB_CUDA(cudaEventRecord(e1, c->stream));
     c->timed.push_back({2, e0, e1});
     return (int)t.size();
@@ -571,17 +575,24 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     std::vector<int2> up = tc::make_tiles(ldp, true, 256);
     std::vector<int2> up3 = tc::make_tiles(ldp, true, 128);
     std::vector<int2> all = tc::make_tiles(ldp, false, 256);
+    std::vector<int2> pup = tc::make_pair_tiles(ldp, true);     // CTA-pair kernel tiles
+    std::vector<int2> pall = tc::make_pair_tiles(ldp, false);
     DevBuf& bt = c->buf(B_TILES);
-    bt.reserve(sizeof(int2) * (up.size() + up3.size() + all.size()));
+    bt.reserve(sizeof(int2) * (up.size() + up3.size() + all.size() + pup.size() + pall.size()));
     int2* tiles_up = bt.as<int2>();
     int2* tiles_up3 = tiles_up + up.size();
     int2* tiles_all = tiles_up3 + up3.size();
+    int2* pairs_up = tiles_all + all.size();
+    int2* pairs_all = pairs_up + pup.size();
     PTB_CUDA(cudaMemcpyAsync(tiles_up, up.data(), sizeof(int2) * up.size(), cudaMemcpyHostToDevice, s));
     PTB_CUDA(cudaMemcpyAsync(tiles_up3, up3.data(), sizeof(int2) * up3.size(), cudaMemcpyHostToDevice, s));
     PTB_CUDA(cudaMemcpyAsync(tiles_all, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemcpyAsync(pairs_up, pup.data(), sizeof(int2) * pup.size(), cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemcpyAsync(pairs_all, pall.data(), sizeof(int2) * pall.size(), cudaMemcpyHostToDevice, s));
+    const int npup = (int)pup.size(), npall = (int)pall.size();
     const int x0_blocks = grid1(ldp);
     DevBuf& bstats = c->buf(B_STATS);
-    bstats.reserve(sizeof(double) * 2 * std::max({up.size(), up3.size(), (size_t)x0_blocks}));
+    bstats.reserve(sizeof(double) * 2 * std::max({up.size(), up3.size(), 2 * pup.size(), (size_t)x0_blocks}));
     double* stats = bstats.as<double>();
     if (!c->sp2_state) PTB_CUDA(cudaMalloc(&c->sp2_state, sizeof(SP2State)));
     SP2State* state = (SP2State*)c->sp2_state;
@@ -627,9 +638,9 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         ep.lo2 = traj(k + 1, 2);
         const void* pl[3] = {traj(k, 0), traj(k, 1), traj(k, 2)};
         const bool three = three_planes(k);
-        const int ntl = three ? n6 : n3;
-        timed_product(c, tc::EPI_SP2, three ? 3 : 2, ldp, pl, pl, three ? split6 : split3,
-                      three ? tiles_up3 : tiles_up, ntl, ep);
+        const int ntl = three ? timed_product(c, tc::EPI_SP2, 3, ldp, pl, pl, split6, tiles_up3, n6, ep)
+                              : timed_product(c, tc::EPI_SP2, 2, ldp, pl, pl, split3, tiles_up, n3, ep, 0, pairs_up,
+                                              npup);
         k_decide<<<1, 256, 0, s>>>(state, stats, ntl, N, tol_abs, e_switch, cap);
         count_launch();
         PTB_CUDA(cudaGetLastError());
@@ -680,7 +691,8 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         // of each iterate is checked before its square is taken
         const oz::Operand opX = oz_operand(c, 1, n, S);
         DevBuf& bst = c->buf(B_OZS);
-        bst.reserve(sizeof(double) * 2 * (size_t)(oz::padded(n) / oz::BM) * (size_t)(oz::padded(n) / oz::BN));
+        // per-tile partials: at most (rows / 128) x ceil(cols / 48) tiles for either kernel variant
+        bst.reserve(sizeof(double) * 2 * (size_t)(oz::padded(n) / oz::BM) * (size_t)((oz::padded(n) + 47) / 48));
         std::vector<double> hst;
         double trX = trace_dev(c, n, n, X);
         const double f0 = frob_dev(c, n, n, X);
@@ -783,7 +795,7 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         epf.out = wf;
         const void* pc[2] = {chi, clo};
         const void* pp[2] = {phi, plo};
-        timed_product(c, tc::EPI_FULL, 2, ldp, pc, pp, split3, tiles_all, (int)all.size(), epf);
+        timed_product(c, tc::EPI_FULL, 2, ldp, pc, pp, split3, tiles_all, (int)all.size(), epf, 0, pairs_all, npall);
         // The planes hold C^T (column-major C read row-major), so wf = C^T P~ = -C P~.
         // A1 = C P~ - P~ C = -(wf + wf^T) and X1_0 = -A1 / (e_max - e_min) = (wf + wf^T) * scale.
         const unsigned nbp = (unsigned)(ldp / 32);
@@ -797,7 +809,7 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
             const int a = k & 1, b = a ^ 1;
             const void* p0[2] = {traj_hi(k), traj_lo(k)};
             const void* p1[2] = {x1hi[a], x1lo[a]};
-            timed_product(c, tc::EPI_FULL, 2, ldp, p0, p1, split3, tiles_all, (int)all.size(), epf);
+            timed_product(c, tc::EPI_FULL, 2, ldp, p0, p1, split3, tiles_all, (int)all.size(), epf, 0, pairs_all, npall);
             const bool sq = H.sq[k] != 0;
             k_sym_update<<<dim3(nbp, nbp), dim3(32, 8), 0, s>>>(ldp, wf, x1f[a], sq ? 1.0f : -1.0f,
                                                                 sq ? 0.0f : 2.0f, x1f[b], x1hi[b], x1lo[b]);
@@ -814,14 +826,14 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
             const int a = K & 1, b = a ^ 1;
             const void* pp2[2] = {phi, plo};
             const void* px[2] = {x1hi[a], x1lo[a]};
-            timed_product(c, tc::EPI_FULL, 2, ldp, pp2, px, split3, tiles_all, (int)all.size(), epf);   // W
+            timed_product(c, tc::EPI_FULL, 2, ldp, pp2, px, split3, tiles_all, (int)all.size(), epf, 0, pairs_all, npall);   // W
             k_split2<<<grid1(ldp * ldp / 256), 256, 0, s>>>(ldp * ldp, wf, x1hi[b], x1lo[b]);
             count_launch();
             PTB_CUDA(cudaGetLastError());
             tc::EpiParams epv = epf;
             epv.out = x1f[b];
             const void* pw[2] = {x1hi[b], x1lo[b]};
-            timed_product(c, tc::EPI_FULL, 2, ldp, pw, pp2, split3, tiles_all, (int)all.size(), epv);  // W P~
+            timed_product(c, tc::EPI_FULL, 2, ldp, pw, pp2, split3, tiles_all, (int)all.size(), epv, 0, pairs_all, npall);  // W P~
             k_sym_update<<<dim3(nbp, nbp), dim3(32, 8), 0, s>>>(ldp, wf, x1f[b], 1.0f, -2.0f, x1f[a], x1hi[a],
                                                                 x1lo[a]);
             count_launch();
@@ -834,12 +846,12 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
             const void* px1[2] = {x1hi[a], x1lo[a]};
             tc::EpiParams epy = epf;
             epy.out = x1f[b];
-            timed_product(c, tc::EPI_FULL, 2, ldp, px1, px1, split3, tiles_all, (int)all.size(), epy);   // Y
+            timed_product(c, tc::EPI_FULL, 2, ldp, px1, px1, split3, tiles_all, (int)all.size(), epy, 0, pairs_all, npall);   // Y
             k_split2<<<grid1(ldp * ldp / 256), 256, 0, s>>>(ldp * ldp, x1f[b], x1hi[b], x1lo[b]);
             count_launch();
             PTB_CUDA(cudaGetLastError());
             const void* py[2] = {x1hi[b], x1lo[b]};
-            timed_product(c, tc::EPI_FULL, 2, ldp, pp2, py, split3, tiles_all, (int)all.size(), epf);    // W2
+            timed_product(c, tc::EPI_FULL, 2, ldp, pp2, py, split3, tiles_all, (int)all.size(), epf, 0, pairs_all, npall);    // W2
             k_add_f32<<<grid1(ldp * ldp / 256), 256, 0, s>>>(ldp * ldp, x1f[a], x1f[b]);              // Y + X1
             count_launch();
             PTB_CUDA(cudaGetLastError());
@@ -944,9 +956,13 @@ void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, int kblock, const double* hX,
     d2f_split(s, n, ldp, bx.as<double>(), xf, hi, mid);
     d2f_split3(s, ldp, xf, hi, mid, lo);
     std::vector<int2> all = tc::make_tiles(ldp, false, np == 2 ? 256 : 128);
+    std::vector<int2> pall = np == 2 ? tc::make_pair_tiles(ldp, false) : std::vector<int2>();
     DevBuf& bt = c->buf(B_TILES);
-    bt.reserve(sizeof(int2) * all.size());
+    bt.reserve(sizeof(int2) * (all.size() + pall.size()));
     PTB_CUDA(cudaMemcpyAsync(bt.ptr, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s));
+    int2* pairs = pall.empty() ? nullptr : bt.as<int2>() + all.size();
+    if (pairs)
+        PTB_CUDA(cudaMemcpyAsync(pairs, pall.data(), sizeof(int2) * pall.size(), cudaMemcpyHostToDevice, s));
     PTB_CUDA(cudaMemsetAsync(&c->flags->timeout, 0, sizeof(int), s));
     tc::ProdList split3{3, {0, 0, 1}, {0, 1, 0}};
     tc::ProdList split6{6, {0, 0, 1, 0, 2, 1}, {0, 1, 0, 2, 0, 1}};
@@ -956,7 +972,7 @@ void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, int kblock, const double* hX,
     ep.out = xf;   // the FP32 copy is consumed by the split above (stream order)
     const void* pl[3] = {hi, mid, lo};
     timed_product(c, tc::EPI_FULL, np, ldp, pl, pl, np == 2 ? split3 : split6, bt.as<int2>(), (int)all.size(), ep,
-                  kblock);
+                  kblock, pairs, (int)pall.size());
     PTB_CUDA(cudaMemcpy2DAsync(hC, sizeof(float) * n, xf, sizeof(float) * ldp, sizeof(float) * n, n,
                                cudaMemcpyDeviceToHost, s));
     int tmo = 0;
@@ -968,8 +984,8 @@ void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, int kblock, const double* hX,
 // C = A B (n x n, row-major host FP64) with the int8-sliced kernel, for
 // kernel-level tests.  tri_a / tri_b describe A and B as matrices (1 lower,
 // 2 upper); sym: only the upper triangle of C is computed and mirrored.
-void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int tri_a, int tri_b, bool sym, const double* hA,
-                   const double* hB, double* hC) {
+void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int variant, int tri_a, int tri_b, bool sym,
+                   const double* hA, const double* hB, double* hC) {
     PTB_CHECK(oz::supported(n, S), PTBGPU_EINVAL, "n = %lld is too large for exact int32 sums with %d slices",
               (long long)n, S);
     cudaStream_t s = c->stream;
@@ -992,7 +1008,7 @@ void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int tri_a, int t
     ep.out = bc.as<double>();
     ep.ors = n;
     ep.ocs = 1;
-    oz_product(c, sym ? oz::OZ_SYM : oz::OZ_OUT, opA, opB, sym, ta, tb, ep, kblock);
+    oz_product(c, sym ? oz::OZ_SYM : oz::OZ_OUT, opA, opB, sym, ta, tb, ep, kblock, variant);
     PTB_CUDA(cudaMemcpyAsync(hC, bc.ptr, sizeof(double) * n * n, cudaMemcpyDeviceToHost, s));
     check_timeout(c, "int8 product");
 }

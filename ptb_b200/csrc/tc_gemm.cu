@@ -86,6 +86,125 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& h, __nv_bfloa
 }
 
 // ---- the kernel -----------------------------------------------------------
+// Epilogue warps 4..7 (q = TMEM lane quarter) of a 128 x BN accumulator in this
+// CTA's tensor memory: wait for it (bounded), drain it with the fused update,
+// and reduce the per-tile trace / sum of squares into stats[2 * stat_index].
+template <int EPI, int BN>
+__device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, uint32_t accum_bar,
+                                            int* abort_flag, double* red, int bi, int bj, int q, int lane,
+                                            int stat_index) {
+    const int64_t ld = ep.ld;
+    const int64_t r = (int64_t)bi * BM + q * 32 + lane;
+    double tr = 0.0, ss = 0.0;
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(accum_bar, 0));
+    if (!ok && lane == 0) {
+        set_err(ep.err, 31);
+        *(volatile int*)abort_flag = 1;
+    }
+    const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
+    tc_fence_after();
+    if (ok && !aborted) {
+        const bool square = (EPI == EPI_SP2) ? (*ep.sq_flag != 0) : true;
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+            uint32_t v[32];
+            __syncwarp();   // lanes may have taken different paths in the previous chunk
+            tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
+            const int64_t cbase = (int64_t)bj * BN + c0;
+            if (EPI == EPI_FULL) {
+                float4* dst = reinterpret_cast<float4*>(ep.out + r * ld + cbase);
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    dst[j] = make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
+                                         __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]));
+                continue;
+            }
+            if (cbase + 31 < r) continue;       // chunk entirely below the diagonal
+            if (cbase >= r) {
+                // whole chunk in the upper triangle: vector path
+                const float4* xin = reinterpret_cast<const float4*>(ep.xcur + r * ld + cbase);
+                float4* xo = reinterpret_cast<float4*>(ep.out + r * ld + cbase);
+                uint4* ho = reinterpret_cast<uint4*>(ep.hi + r * ld + cbase);
+                uint4* mo = reinterpret_cast<uint4*>(ep.lo + r * ld + cbase);
+                uint4* lo = reinterpret_cast<uint4*>(ep.lo2 + r * ld + cbase);
+#pragma unroll
+                for (int j8 = 0; j8 < 4; ++j8) {
+                    float val[8];
+                    // X is only needed for 2X - X^2: skip its read on the square branch
+                    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                    const float4 x0 = square ? zero4 : xin[2 * j8];
+                    const float4 x1 = square ? zero4 : xin[2 * j8 + 1];
+                    const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+                    __align__(16) __nv_bfloat16 hh[8], mm[8], ll[8];
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const float cv = __uint_as_float(v[8 * j8 + t]);
+                        val[t] = square ? cv : 2.0f * xs[t] - cv;
+                        split_bf16(val[t], hh[t], mm[t], ll[t]);
+                        const int64_t c = cbase + 8 * j8 + t;
+                        const double dv = (double)val[t];
+                        if (c == r) {
+                            tr += dv;
+                            ss += dv * dv;
+                        } else {
+                            ss += 2.0 * dv * dv;
+                            ep.out[c * ld + r] = val[t];
+                            ep.hi[c * ld + r] = hh[t];
+                            ep.lo[c * ld + r] = mm[t];
+                            ep.lo2[c * ld + r] = ll[t];
+                        }
+                    }
+                    xo[2 * j8] = make_float4(val[0], val[1], val[2], val[3]);
+                    xo[2 * j8 + 1] = make_float4(val[4], val[5], val[6], val[7]);
+                    ho[j8] = *reinterpret_cast<const uint4*>(hh);
+                    mo[j8] = *reinterpret_cast<const uint4*>(mm);
+                    lo[j8] = *reinterpret_cast<const uint4*>(ll);
+                }
+            } else {
+                // chunk straddles the diagonal: scalar path, c >= r only
+#pragma unroll 4
+                for (int j = 0; j < 32; ++j) {
+                    const int64_t c = cbase + j;
+                    if (c < r) continue;
+                    const float cv = __uint_as_float(v[j]);
+                    const float val = square ? cv : 2.0f * ep.xcur[r * ld + c] - cv;
+                    __nv_bfloat16 h, m, l;
+                    split_bf16(val, h, m, l);
+                    const double dv = (double)val;
+                    ep.out[r * ld + c] = val;
+                    ep.hi[r * ld + c] = h;
+                    ep.lo[r * ld + c] = m;
+                    ep.lo2[r * ld + c] = l;
+                    if (c == r) {
+                        tr += dv;
+                        ss += dv * dv;
+                    } else {
+                        ss += 2.0 * dv * dv;
+                        ep.out[c * ld + r] = val;
+                        ep.hi[c * ld + r] = h;
+                        ep.lo[c * ld + r] = m;
+                        ep.lo2[c * ld + r] = l;
+                    }
+                }
+            }
+        }
+    }
+    if (EPI == EPI_SP2) {
+        for (int o = 16; o > 0; o >>= 1) {
+            tr += __shfl_xor_sync(0xffffffffu, tr, o);
+            ss += __shfl_xor_sync(0xffffffffu, ss, o);
+        }
+        if (lane == 0) {
+            red[2 * q] = tr;
+            red[2 * q + 1] = ss;
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");   // epilogue warps only
+        if (q == 0 && lane == 0) {
+            ep.stats[2 * stat_index] = red[0] + red[2] + red[4] + red[6];
+            ep.stats[2 * stat_index + 1] = red[1] + red[3] + red[5] + red[7];
+        }
+    }
+}
+
 template <int EPI, int BN, int NP, int KB>
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_product(const __grid_constant__ TmaPlanes maps, const ProdList prods, const int2* __restrict__ tiles,
@@ -189,118 +308,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         umma_commit(accum_bar);   // also issued on abort so the wait below ends
         if (!ok) mbar_wait(accum_bar, 0);
     } else if (warp >= 4) {
-        // ---------------- epilogue ----------------
-        const int q = warp - 4;                   // TMEM lane quarter
-        const int64_t ld = ep.ld;
-        const int64_t r = (int64_t)bi * BM + q * 32 + lane;
-        double tr = 0.0, ss = 0.0;
-        const bool ok = __all_sync(0xffffffffu, mbar_wait(accum_bar, 0));
-        if (!ok && lane == 0) {
-            set_err(ep.err, 31);
-            *(volatile int*)abort_flag = 1;
-        }
-        const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
-        tc_fence_after();
-        if (ok && !aborted) {
-            const bool square = (EPI == EPI_SP2) ? (*ep.sq_flag != 0) : true;
-            for (int c0 = 0; c0 < BN; c0 += 32) {
-                uint32_t v[32];
-                __syncwarp();   // lanes may have taken different paths in the previous chunk
-                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
-                const int64_t cbase = (int64_t)bj * BN + c0;
-                if (EPI == EPI_FULL) {
-                    float4* dst = reinterpret_cast<float4*>(ep.out + r * ld + cbase);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        dst[j] = make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
-                                             __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]));
-                    continue;
-                }
-                if (cbase + 31 < r) continue;       // chunk entirely below the diagonal
-                if (cbase >= r) {
-                    // whole chunk in the upper triangle: vector path
-                    const float4* xin = reinterpret_cast<const float4*>(ep.xcur + r * ld + cbase);
-                    float4* xo = reinterpret_cast<float4*>(ep.out + r * ld + cbase);
-                    uint4* ho = reinterpret_cast<uint4*>(ep.hi + r * ld + cbase);
-                    uint4* mo = reinterpret_cast<uint4*>(ep.lo + r * ld + cbase);
-                    uint4* lo = reinterpret_cast<uint4*>(ep.lo2 + r * ld + cbase);
-#pragma unroll
-                    for (int j8 = 0; j8 < 4; ++j8) {
-                        float val[8];
-                        // X is only needed for 2X - X^2: skip its read on the square branch
-                        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-                        const float4 x0 = square ? zero4 : xin[2 * j8];
-                        const float4 x1 = square ? zero4 : xin[2 * j8 + 1];
-                        const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-                        __align__(16) __nv_bfloat16 hh[8], mm[8], ll[8];
-#pragma unroll
-                        for (int t = 0; t < 8; ++t) {
-                            const float cv = __uint_as_float(v[8 * j8 + t]);
-                            val[t] = square ? cv : 2.0f * xs[t] - cv;
-                            split_bf16(val[t], hh[t], mm[t], ll[t]);
-                            const int64_t c = cbase + 8 * j8 + t;
-                            const double dv = (double)val[t];
-                            if (c == r) {
-                                tr += dv;
-                                ss += dv * dv;
-                            } else {
-                                ss += 2.0 * dv * dv;
-                                ep.out[c * ld + r] = val[t];
-                                ep.hi[c * ld + r] = hh[t];
-                                ep.lo[c * ld + r] = mm[t];
-                                ep.lo2[c * ld + r] = ll[t];
-                            }
-                        }
-                        xo[2 * j8] = make_float4(val[0], val[1], val[2], val[3]);
-                        xo[2 * j8 + 1] = make_float4(val[4], val[5], val[6], val[7]);
-                        ho[j8] = *reinterpret_cast<const uint4*>(hh);
-                        mo[j8] = *reinterpret_cast<const uint4*>(mm);
-                        lo[j8] = *reinterpret_cast<const uint4*>(ll);
-                    }
-                } else {
-                    // chunk straddles the diagonal: scalar path, c >= r only
-#pragma unroll 4
-                    for (int j = 0; j < 32; ++j) {
-                        const int64_t c = cbase + j;
-                        if (c < r) continue;
-                        const float cv = __uint_as_float(v[j]);
-                        const float val = square ? cv : 2.0f * ep.xcur[r * ld + c] - cv;
-                        __nv_bfloat16 h, m, l;
-                        split_bf16(val, h, m, l);
-                        const double dv = (double)val;
-                        ep.out[r * ld + c] = val;
-                        ep.hi[r * ld + c] = h;
-                        ep.lo[r * ld + c] = m;
-                        ep.lo2[r * ld + c] = l;
-                        if (c == r) {
-                            tr += dv;
-                            ss += dv * dv;
-                        } else {
-                            ss += 2.0 * dv * dv;
-                            ep.out[c * ld + r] = val;
-                            ep.hi[c * ld + r] = h;
-                            ep.lo[c * ld + r] = m;
-                            ep.lo2[c * ld + r] = l;
-                        }
-                    }
-                }
-            }
-        }
-        if (EPI == EPI_SP2) {
-            for (int o = 16; o > 0; o >>= 1) {
-                tr += __shfl_xor_sync(0xffffffffu, tr, o);
-                ss += __shfl_xor_sync(0xffffffffu, ss, o);
-            }
-            if (lane == 0) {
-                red[2 * q] = tr;
-                red[2 * q + 1] = ss;
-            }
-            asm volatile("bar.sync 1, 128;" ::: "memory");   // epilogue warps only
-            if (q == 0 && lane == 0) {
-                ep.stats[2 * blockIdx.x] = red[0] + red[2] + red[4] + red[6];
-                ep.stats[2 * blockIdx.x + 1] = red[1] + red[3] + red[5] + red[7];
-            }
-        }
+        tc_epilogue<EPI, BN>(ep, tmem, accum_bar, abort_flag, red, bi, bj, warp - 4, lane, (int)blockIdx.x);
     }
     __syncwarp();
     tc_fence_before();
@@ -308,6 +316,150 @@ __global__ void __launch_bounds__(THREADS, 1)
     tc_fence_after();
     if (warp == 2) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN));
+    }
+}
+
+// ---- CTA-pair kernel (two planes) --------------------------------------------
+// A cluster of two CTAs computes a 256 x 256 tile with cta_group::2 UMMA
+// 256x256x16: CTA r holds rows 128r..128r+127 of A and of the accumulator, and
+// columns 128r..128r+127 of the B operand, so every SM loads half the B panel
+// of the one-CTA 128 x 256 tile: 1.5x fewer operand bytes per flop from L2.
+// Each CTA's TMA loads count on the leader's (rank 0) "full" mbarrier, which
+// the leader arms with both CTAs' bytes; the leader's single MMA thread issues
+// the pair's MMAs and its commits arrive on the "empty" and accumulator
+// barriers of both CTAs.  The epilogue is the one-CTA epilogue on each CTA's
+// own 128 rows.
+template <int NP, int KB>
+struct CfgPair {
+    static constexpr int A_TILE_BYTES = BM * KB * 2;          // this CTA's 128 rows of A
+    static constexpr int B_TILE_BYTES = 128 * KB * 2;         // this CTA's 128 rows of B (half of N)
+    static constexpr int STAGE_BYTES = NP * (A_TILE_BYTES + B_TILE_BYTES);
+    static constexpr int STAGES = kSmemBudget / STAGE_BYTES > 6 ? 6 : kSmemBudget / STAGE_BYTES;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr uint32_t SWIZZLE_LAYOUT = KB == 64 ? 2u : 4u;
+    static constexpr uint32_t SBO = KB == 64 ? 1024u : 512u;
+    // kind::f16: D fp32, A/B bf16, K-major, M = 256 (the pair), N = 256
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
+                                      ((uint32_t)(256 >> 4) << 24);
+    static_assert(KB == 64 || KB == 32, "K block of 64 or 32 elements");
+    static_assert(STAGES >= 2, "at least two pipeline stages");
+    static_assert(STAGE_BYTES % 1024 == 0, "stages keep the swizzle atoms aligned");
+};
+
+template <int EPI, int NP, int KB>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
+    k_tc_product_pair(const __grid_constant__ TmaPlanes maps, const ProdList prods, const int2* __restrict__ pairs,
+                      int nk, EpiParams ep) {
+    if (ep.active && *ep.active == 0) return;   // uniform over the grid: both CTAs of a pair return
+    using C = CfgPair<NP, KB>;
+    constexpr int STAGE_BYTES = C::STAGE_BYTES;
+    constexpr int STAGES = C::STAGES;
+
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t base_raw = smem_u32(smem_raw);
+    const uint32_t base = (base_raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - base_raw);
+    const uint32_t bar0 = base + STAGES * STAGE_BYTES;
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+    const uint32_t accum_bar = bar0 + 8u * (2 * STAGES);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + STAGES * STAGE_BYTES + 8 * (2 * STAGES + 1));
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+    double* red = reinterpret_cast<double*>(gbase + STAGES * STAGE_BYTES + 128);   // 8 doubles
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const int2 pt = pairs[blockIdx.x >> 1];
+    const int bi = 2 * pt.x + (int)rank, bj = pt.y;   // this CTA's 128-row block; 256-column block
+
+    auto a_tile = [&](int s, int p) { return base + s * STAGE_BYTES + p * C::A_TILE_BYTES; };
+    auto b_tile = [&](int s, int p) { return base + s * STAGE_BYTES + NP * C::A_TILE_BYTES + p * C::B_TILE_BYTES; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(accum_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(256u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();   // both CTAs' barriers are initialised before any remote arrive
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer (both CTAs) ----------------
+        int issued_phase[STAGES];
+        for (int s = 0; s < STAGES; ++s) issued_phase[s] = -1;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % STAGES, round = kb / STAGES;
+            if (round > 0 && !mbar_wait(empty_bar(s), (round - 1) & 1)) {
+                set_err(ep.err, 41);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            if (rank == 0) mbar_expect_tx(full_bar(s), 2 * STAGE_BYTES);   // both CTAs' bytes
+            const uint32_t fb = mapa_shared(full_bar(s), 0);
+            for (int p = 0; p < NP; ++p) tma_load_2d_pair(a_tile(s, p), &maps.a[p], fb, kb * KB, bi * BM);
+            for (int p = 0; p < NP; ++p)
+                tma_load_2d_pair(b_tile(s, p), &maps.b[p], fb, kb * KB, bj * 256 + (int)rank * 128);
+            issued_phase[s] = round & 1;
+        }
+        // drain: the leader sees every copy of the pair land on its full barriers;
+        // the peer's copies have landed once the leader's MMAs consumed them,
+        // which its accumulator barrier (waited by the epilogue) certifies
+        if (rank == 0)
+            for (int s = 0; s < STAGES; ++s)
+                if (issued_phase[s] >= 0 && !mbar_wait(full_bar(s), (uint32_t)issued_phase[s]))
+                    set_err(ep.err, 42);
+    } else if (warp == 1 && lane == 0 && rank == 0) {
+        // ---------------- MMA issuer (leader CTA) ----------------
+        bool ok = true;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % STAGES, round = kb / STAGES;
+            if (!mbar_wait(full_bar(s), round & 1)) {
+                set_err(ep.err, 51);
+                *(volatile int*)abort_flag = 1;
+                ok = false;
+                break;
+            }
+            if (*(volatile int*)abort_flag) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+#pragma unroll
+            for (int k = 0; k < KB / 16; ++k) {
+                for (int p = 0; p < prods.n; ++p) {
+                    const uint64_t ad = sdesc(a_tile(s, prods.a[p]) + k * 32, C::SBO, C::SWIZZLE_LAYOUT);
+                    const uint64_t bd = sdesc(b_tile(s, prods.b[p]) + k * 32, C::SBO, C::SWIZZLE_LAYOUT);
+                    umma_bf16_pair(tmem, ad, bd, C::IDESC, (kb | k | p) != 0);
+                }
+            }
+            umma_commit_pair(empty_bar(s), (uint16_t)0x3);
+        }
+        umma_commit_pair(accum_bar, (uint16_t)0x3);   // also on abort so the epilogues' waits end
+        if (!ok) mbar_wait(accum_bar, 0);
+    } else if (warp >= 4) {
+        tc_epilogue<EPI, 256>(ep, tmem, accum_bar, abort_flag, red, bi, bj, warp - 4, lane, (int)blockIdx.x);
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();   // the leader's MMAs have finished reading the peer's shared memory
+    tc_fence_after();
+    if (warp == 2) {
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
     }
 }
 
@@ -357,6 +509,18 @@ std::vector<int2> make_tiles(long long ld, bool upper_only, int bn) {
     return t;
 }
 
+// 256 x 256 tiles of the CTA-pair kernel, grouped by 8 tile rows.
+std::vector<int2> make_pair_tiles(long long ld, bool upper_only) {
+    const int nb = (int)(ld / 256);
+    std::vector<int2> t;
+    const int G = 8;
+    for (int g0 = 0; g0 < nb; g0 += G)
+        for (int pj = 0; pj < nb; ++pj)
+            for (int pi = g0; pi < std::min(nb, g0 + G); ++pi)
+                if (!upper_only || pj >= pi) t.push_back(make_int2(pi, pj));
+    return t;
+}
+
 namespace {
 template <int EPI, int BN, int NP, int KB>
 void launch_t(cudaStream_t s, const TmaPlanes& maps, const ProdList& prods, const int2* tiles, int ntiles, int nk,
@@ -372,10 +536,27 @@ void launch_t(cudaStream_t s, const TmaPlanes& maps, const ProdList& prods, cons
     count_launch();
 }
 
+template <int EPI, int KB>
+void launch_pair(cudaStream_t s, const TmaPlanes& maps, const ProdList& prods, const int2* pairs, int npairs, int nk,
+                 const EpiParams& ep) {
+    using C = CfgPair<2, KB>;
+    static bool attr = false;
+    if (!attr) {
+        PTB_CUDA(cudaFuncSetAttribute(k_tc_product_pair<EPI, 2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      C::SMEM_BYTES));
+        attr = true;
+    }
+    k_tc_product_pair<EPI, 2, KB><<<2 * npairs, THREADS, C::SMEM_BYTES, s>>>(maps, prods, pairs, nk, ep);
+    count_launch();
+}
+
 template <int EPI>
-void launch_epi(cudaStream_t s, int np, int kb, const TmaPlanes& maps, const ProdList& prods, const int2* tiles,
-                int ntiles, int nk, const EpiParams& ep) {
-    if (np == 2) {
+void launch_epi(cudaStream_t s, int np, int kb, bool pair, const TmaPlanes& maps, const ProdList& prods,
+                const int2* tiles, int ntiles, int nk, const EpiParams& ep) {
+    if (pair) {
+        if (kb == 64) launch_pair<EPI, 64>(s, maps, prods, tiles, ntiles, nk, ep);
+        else launch_pair<EPI, 32>(s, maps, prods, tiles, ntiles, nk, ep);
+    } else if (np == 2) {
         if (kb == 64) launch_t<EPI, 256, 2, 64>(s, maps, prods, tiles, ntiles, nk, ep);
         else launch_t<EPI, 256, 2, 32>(s, maps, prods, tiles, ntiles, nk, ep);
     } else {
@@ -384,10 +565,11 @@ void launch_epi(cudaStream_t s, int np, int kb, const TmaPlanes& maps, const Pro
     }
 }
 
-// Autotuned K-block choice per (device, epilogue, planes, leading dimension):
-// the first launch of a shape runs both variants back to back (same inputs,
-// same outputs, so running twice is harmless), times them with CUDA events
-// and keeps the faster for the rest of the process.
+// Autotuned kernel choice per (device, epilogue, planes, leading dimension):
+// the first launch of a shape runs every candidate (K block 64 / 32, one CTA
+// or a CTA pair where pair tiles are given) back to back -- same inputs, same
+// outputs, so running them all is harmless -- times them with CUDA events and
+// keeps the fastest for the rest of the process.
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, long long>, int> g_tuned;
 }  // namespace
@@ -400,47 +582,70 @@ int tuned_kblock(int epi, int np, long long ld) {
     return it == g_tuned.end() ? 0 : it->second;
 }
 
-void launch_product(cudaStream_t s, int epi, int np, long long ld, const void* const* a, const void* const* b,
-                    const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep, int kblock) {
+int launch_product(cudaStream_t s, int epi, int np, long long ld, const void* const* a, const void* const* b,
+                   const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep, int kblock,
+                   const int2* pairs_dev, int npairs) {
     PTB_CHECK(np == 2 || np == 3, PTBGPU_EINVAL, "unsupported plane count %d", np);
-    PTB_CHECK(kblock == 0 || kblock == 32 || kblock == 64, PTBGPU_EINVAL, "K block must be 0, 32 or 64");
+    PTB_CHECK(kblock == 0 || kblock == 32 || kblock == 64 || kblock == kPairKernel + 32 ||
+                  kblock == kPairKernel + 64,
+              PTBGPU_EINVAL, "bad kernel choice %d", kblock);
+    PTB_CHECK(kblock < kPairKernel || (np == 2 && pairs_dev != nullptr), PTBGPU_EINVAL,
+              "the CTA-pair kernel needs two planes and pair tiles");
+    PTB_CHECK(ld % 256 == 0, PTBGPU_EINVAL, "leading dimension must be a multiple of 256");
     const int bn = np == 2 ? 256 : 128;
     for (int p = 0; p < prods.n; ++p)
         PTB_CHECK(prods.a[p] < np && prods.b[p] < np, PTBGPU_EINVAL, "product references a missing plane");
     PTB_CHECK(epi != EPI_SP2 || (ep.lo2 != nullptr && ep.lo != nullptr), PTBGPU_EINVAL,
               "the SP2 epilogue writes three planes");
-    auto run = [&](int kb) {
+    // returns the number of per-CTA stats partials the launch writes
+    auto run = [&](int choice) {
+        const bool pair = choice >= kPairKernel;
+        const int kb = pair ? choice - kPairKernel : choice;
         TmaPlanes maps;
         for (int p = 0; p < np; ++p) {
             encode_plane(&maps.a[p], a[p], ld, BM, kb);
-            encode_plane(&maps.b[p], b[p], ld, bn, kb);
+            encode_plane(&maps.b[p], b[p], ld, pair ? 128 : bn, kb);
         }
         const int nk = (int)(ld / kb);
-        if (epi == EPI_SP2) launch_epi<EPI_SP2>(s, np, kb, maps, prods, tiles_dev, ntiles, nk, ep);
-        else launch_epi<EPI_FULL>(s, np, kb, maps, prods, tiles_dev, ntiles, nk, ep);
+        const int2* t = pair ? pairs_dev : tiles_dev;
+        const int nt = pair ? npairs : ntiles;
+        if (epi == EPI_SP2) launch_epi<EPI_SP2>(s, np, kb, pair, maps, prods, t, nt, nk, ep);
+        else launch_epi<EPI_FULL>(s, np, kb, pair, maps, prods, t, nt, nk, ep);
         PTB_CUDA(cudaGetLastError());
+        return pair ? 2 * npairs : ntiles;
     };
     if (kblock == 0) kblock = tuned_kblock(epi, np, ld);
-    if (kblock != 0) {
-        run(kblock);
-        return;
+    if (kblock != 0 && (kblock < kPairKernel || pairs_dev)) return run(kblock);
+    std::vector<int> cand = {64, 32};
+    if (np == 2 && pairs_dev) {
+        cand.push_back(kPairKernel + 64);
+        cand.push_back(kPairKernel + 32);
     }
-    cudaEvent_t e[3];
+    std::vector<cudaEvent_t> e(cand.size() + 1);
     for (auto& x : e) PTB_CUDA(cudaEventCreate(&x));
+    int parts = 0;
     PTB_CUDA(cudaEventRecord(e[0], s));
-    run(64);
-    PTB_CUDA(cudaEventRecord(e[1], s));
-    run(32);
-    PTB_CUDA(cudaEventRecord(e[2], s));
-    PTB_CUDA(cudaEventSynchronize(e[2]));
-    float t64 = 0.f, t32 = 0.f;
-    PTB_CUDA(cudaEventElapsedTime(&t64, e[0], e[1]));
-    PTB_CUDA(cudaEventElapsedTime(&t32, e[1], e[2]));
+    for (size_t i = 0; i < cand.size(); ++i) {
+        parts = run(cand[i]);
+        PTB_CUDA(cudaEventRecord(e[i + 1], s));
+    }
+    PTB_CUDA(cudaEventSynchronize(e.back()));
+    int best = cand[0];
+    float tbest = 1e30f;
+    for (size_t i = 0; i < cand.size(); ++i) {
+        float t = 0.f;
+        PTB_CUDA(cudaEventElapsedTime(&t, e[i], e[i + 1]));
+        if (t < tbest) {
+            tbest = t;
+            best = cand[i];
+        }
+    }
     for (auto& x : e) cudaEventDestroy(x);
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    g_tuned[std::make_tuple(dev, epi, np, ld)] = t32 < t64 ? 32 : 64;
+    g_tuned[std::make_tuple(dev, epi, np, ld)] = best;
+    return parts;   // the buffers hold the last candidate's results
 }
 
 }  // namespace tc

@@ -1,4 +1,4 @@
-// Interface of the tcgen05 split-bf16 product kernel (tc_gemm.cu).
+// Interface of the tcgen05 split-bf16 product kernels (tc_gemm.cu).
 #pragma once
 
 #include <cuda.h>
@@ -10,6 +10,10 @@ namespace ptb {
 namespace tc {
 
 enum : int { EPI_FULL = 0, EPI_SP2 = 1 };
+
+// Kernel choice codes: K block 64 or 32 for the one-CTA kernel, and
+// kPairKernel + K block for the CTA-pair (cta_group::2, 256 x 256) kernel.
+constexpr int kPairKernel = 1000;
 
 // Tensor maps of up to three A-role and three B-role bf16 planes (64-byte aligned).
 struct TmaPlanes {
@@ -34,16 +38,21 @@ struct EpiParams {
     __nv_bfloat16* hi;        // EPI_SP2: next iterate, bf16 hi plane
     __nv_bfloat16* lo;        // EPI_SP2: next iterate, bf16 mid plane  (x - hi)
     __nv_bfloat16* lo2;       // EPI_SP2: next iterate, bf16 lo plane   (x - hi - mid)
-    double* stats;            // EPI_SP2: per-tile {trace, sum of squares}
+    double* stats;            // EPI_SP2: per-CTA {trace, sum of squares}
 };
 
-// Two-plane products run on 128 x 256 tiles, three-plane products on 128 x 128.
+// Two-plane products run on 128 x 256 tiles (one CTA) or 256 x 256 tiles (a
+// CTA pair), three-plane products on 128 x 128.
 int tile_n();
 std::vector<int2> make_tiles(long long ld, bool upper_only, int bn);
-// kblock: 64 (128B swizzle, 2 stages), 32 (64B swizzle, 4 stages) or 0 = the
-// autotuned choice for this shape (both are timed on its first launch).
-void launch_product(cudaStream_t s, int epi, int np, long long ld, const void* const* a, const void* const* b,
-                    const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep, int kblock = 0);
+std::vector<int2> make_pair_tiles(long long ld, bool upper_only);
+// kblock: 64 / 32 (one CTA), kPairKernel + 64 / + 32 (CTA pair, needs two
+// planes and pairs_dev), or 0 = the autotuned choice for this shape (every
+// candidate is timed on its first launch).  Returns the number of per-CTA
+// stats partials written (EPI_SP2 reduces that many).
+int launch_product(cudaStream_t s, int epi, int np, long long ld, const void* const* a, const void* const* b,
+                   const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep, int kblock = 0,
+                   const int2* pairs_dev = nullptr, int npairs = 0);
 int tuned_kblock(int epi, int np, long long ld);   // 0 until the shape has been tuned
 
 }  // namespace tc

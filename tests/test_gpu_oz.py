@@ -127,3 +127,21 @@ def test_fp64_slices_validated(ctx, water8):
     s = water8
     with pytest.raises(PtbGpuError):
         ctx.tc_purify(s.ndim, s.nel, s.Hvec, s.Svec, Options(precision=PREC_MIXED, fp64_slices=3))
+
+
+@pytest.mark.parametrize("S", [4, 6, 7, 8])
+@pytest.mark.parametrize("kblock", [32, 64])
+def test_oz_gemm_tmem_a_variant_is_bit_exact(ctx, S, kblock):
+    """The kernel that keeps the A slices in tensor memory (48- or 64-column
+    tiles) sums the same exact int32 products as the shared-memory one."""
+    n = 700   # not a multiple of 48, 64 or 128: overhanging tiles
+    rng = np.random.default_rng(S * 100 + kblock)
+    A = rng.standard_normal((n, n))
+    B = rng.standard_normal((n, n))
+    X = 0.5 * (A + A.T)
+    for kw in ({}, {"symmetric": True}, {"tri_a": 1, "tri_b": 2}, {"tri_a": 2}, {"tri_b": 1}):
+        M = X if kw.get("symmetric") else A
+        N = X if kw.get("symmetric") else B
+        C1 = ctx.oz_gemm(M, N, slices=S, kblock=kblock, variant=1, **kw)
+        C2 = ctx.oz_gemm(M, N, slices=S, kblock=kblock, variant=2, **kw)
+        assert np.array_equal(C1, C2), kw

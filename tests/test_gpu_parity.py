@@ -62,6 +62,21 @@ def test_symsq_both_k_blocks(ctx, planes, kblock):
     assert np.max(np.abs(C - X @ X)) <= 1e-4 * np.max(np.abs(X @ X))
 
 
+@pytest.mark.parametrize("kblock", [1032, 1064])
+@pytest.mark.parametrize("n", [256, 520, 1100])
+def test_symsq_cta_pair_kernel(ctx, kblock, n):
+    """The cta_group::2 kernel (256 x 256 tiles over two SMs) gives the
+    one-CTA product to FP32 accumulation accuracy, on sizes that pad."""
+    rng = np.random.default_rng(n + kblock)
+    A = rng.uniform(-1, 1, (n, n))
+    X = 0.5 * (A + A.T)
+    C = ctx.symsq_split(X, 2, kblock).astype(np.float64)
+    ref = ctx.symsq_split(X, 2, 64).astype(np.float64)
+    bound = 2 * n * 2.0 ** -24 * (np.abs(X) @ np.abs(X)) + 1e-30
+    assert np.all(np.abs(C - ref) <= bound)
+    assert np.max(np.abs(C - X @ X)) <= 1e-4 * np.max(np.abs(X @ X))
+
+
 @pytest.mark.parametrize("n", [200, 512, 640])
 def test_symsq_bf16x6_three_plane_split(ctx, n):
     rng = np.random.default_rng(n + 1)
@@ -153,8 +168,9 @@ def test_sm_errors(ctx, water8):
     with pytest.raises(PtbGpuError) as ei:
         ctx.sm_stupid_simple(s.ndim, s.nel, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, 2, 1)
     assert ei.value.code == api.ENOTIMPL
+    bad_part = np.zeros(s.nat, dtype=np.int64)   # cluster ids are 1-based
     with pytest.raises(PtbGpuError) as ei:
-        ctx.sm_stupid_simple(s.ndim, s.nel, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, 4, 2, None)
+        ctx.sm_stupid_simple(s.ndim, s.nel, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, 4, 2, bad_part)
     assert ei.value.code == api.EINVAL
     bad = s.Svec.copy()
     bad[0] = -1.0   # S_11 < 0: not positive definite
