@@ -196,6 +196,30 @@ int ptbgpu_solve2(ptbgpu_ctx* ctx, int64_t mode, int64_t ndim, int64_t nel, int6
 int ptbgpu_density_traces_noalloc(int device, int64_t ndim, const double* dPpk, const double* dSpk,
                                   const double* dHpk, double* out, void* stream, char* err, size_t errlen);
 
+/* The submatrix method in phases, for splitting one step over ranks (each rank
+ * one device; no counterpart in the reference, which runs sm_stupid_simple on
+ * one node).  The submatrices are independent; only the chemical-potential
+ * bisection couples them, through the electron count, one scalar per step:
+ *   ptbgpu_sm_plan     filter, grouping, pattern scan and maps on the whole
+ *                      system (every rank, identical); dims(ndim) receives the
+ *                      nsm submatrix dimensions (what a size-balanced assignment
+ *                      of submatrices to ranks needs);
+ *   ptbgpu_sm_prepare  gather, reduction, eigensolve and fe weights of this
+ *                      rank's submatrices (0-based indices);
+ *   ptbgpu_sm_nel      this rank's electron count at mu (sum over ranks = the
+ *                      nel of source/sm.f90:322-340);
+ *   ptbgpu_sm_finish   this rank's owned columns of P at mu, zeros elsewhere,
+ *                      packed (the sum over ranks is the reference's P).
+ * One rank preparing every submatrix and bisecting on the host reproduces
+ * ptbgpu_sm_density exactly.  The plan stays on the context until the next
+ * plan or ptbgpu_finalize. */
+int ptbgpu_sm_plan(ptbgpu_ctx* ctx, int64_t ndim, const double* Hpk, const double* Spk, int64_t nat,
+                   const double* xyz, const int64_t* aoat, int64_t submatrix_columns, int64_t submatrix_mode,
+                   const int64_t* partition, const ptbgpu_opts* opts, int64_t* nsm, int64_t* dims);
+int ptbgpu_sm_prepare(ptbgpu_ctx* ctx, int64_t nlocal, const int64_t* ids, ptbgpu_stats* st);
+int ptbgpu_sm_nel(ptbgpu_ctx* ctx, double mu, double* nel);
+int ptbgpu_sm_finish(ptbgpu_ctx* ctx, int64_t ndim, double mu, double* Ppk);
+
 /* Columns mode 4 grouping, source/sm.f90:127-154 + clustering_kmeans :459-514
  * + KMPP source/kmpp.f: k-means++ on the atom positions for 1..min(64, nat)
  * clusters, keeping the partition with the least sum over submatrices of

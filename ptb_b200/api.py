@@ -69,7 +69,8 @@ EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_defau
             "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_solve2",
             "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_symsq_split", "ptbgpu_runtime_info",
             "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm", "ptbgpu_mlpop14", "ptbgpu_mlpop14_device",
-            "ptbgpu_mlpop2", "ptbgpu_mlpop2_device", "ptbgpu_kmeans_partition")
+            "ptbgpu_mlpop2", "ptbgpu_mlpop2_device", "ptbgpu_kmeans_partition", "ptbgpu_sm_plan",
+            "ptbgpu_sm_prepare", "ptbgpu_sm_nel", "ptbgpu_sm_finish")
 
 
 def library_path() -> Path:
@@ -115,6 +116,11 @@ def load_library():
     lib.ptbgpu_oz_gemm.argtypes = [C.c_void_p, i64, i64, i64, i64, i64, i64, i64, d, d, d, d]
     lib.ptbgpu_kmeans_partition.argtypes = [C.c_void_p, i64, d, d, i64, d, P(i64), C.c_uint64, P(_Opts), P(i64),
                                             P(i64), d]
+    lib.ptbgpu_sm_plan.argtypes = [C.c_void_p, i64, d, d, i64, d, P(i64), i64, i64, P(i64), P(_Opts), P(i64),
+                                   P(i64)]
+    lib.ptbgpu_sm_prepare.argtypes = [C.c_void_p, i64, P(i64), P(_Stats)]
+    lib.ptbgpu_sm_nel.argtypes = [C.c_void_p, C.c_double, d]
+    lib.ptbgpu_sm_finish.argtypes = [C.c_void_p, i64, C.c_double, d]
     f = P(C.c_float)
     lib.ptbgpu_mlpop14.argtypes = [C.c_void_p, i64, d, C.c_double, f, f]
     lib.ptbgpu_mlpop14_device.argtypes = [C.c_void_p, i64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
@@ -271,6 +277,44 @@ class Context:
             ao.ctypes.data_as(C.POINTER(C.c_int64)), int(submatrix_columns), int(submatrix_mode),
             part.ctypes.data_as(C.POINTER(C.c_int64)) if part is not None else None, C.byref(o), C.byref(st)))
         return P, Stats.from_c(st)
+
+    # ---- the submatrix method in phases (one rank's share; ptb_b200.distributed) ----
+    def sm_plan(self, ndim: int, Hvec: np.ndarray, Svec: np.ndarray, n: int, xyz: np.ndarray, aoat: np.ndarray,
+                submatrix_columns: int, submatrix_mode: int, partition: np.ndarray | None = None,
+                opts: Options | None = None) -> np.ndarray:
+        """Grouping, pattern scan and maps of the whole system; returns the
+        submatrix dimensions (nsm,)."""
+        nsm = C.c_int64(0)
+        dims = np.zeros(ndim, dtype=np.int64)
+        o = (opts or Options()).to_c()
+        ao = _i64(aoat)
+        part = _i64(partition) if partition is not None else None
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
+        self._check(self._lib.ptbgpu_sm_plan(
+            self._h, int(ndim), _dptr(_f64(Hvec)), _dptr(_f64(Svec)), int(n), _dptr(_f64(xyz)), ip(ao),
+            int(submatrix_columns), int(submatrix_mode), ip(part) if part is not None else None, C.byref(o),
+            C.byref(nsm), ip(dims)))
+        return dims[:nsm.value].copy()
+
+    def sm_prepare(self, ids) -> "Stats":
+        """Eigenpairs and fe weights of the listed submatrices (0-based)."""
+        v = _i64(np.asarray(ids, dtype=np.int64).reshape(-1))
+        st = _Stats()
+        self._check(self._lib.ptbgpu_sm_prepare(self._h, int(v.shape[0]), v.ctypes.data_as(C.POINTER(C.c_int64)),
+                                                C.byref(st)))
+        return Stats.from_c(st)
+
+    def sm_nel(self, mu: float) -> float:
+        """Electron count of the prepared submatrices at mu."""
+        v = C.c_double(0.0)
+        self._check(self._lib.ptbgpu_sm_nel(self._h, float(mu), C.byref(v)))
+        return v.value
+
+    def sm_finish(self, ndim: int, mu: float) -> np.ndarray:
+        """Owned columns of the prepared submatrices at mu (packed, zeros elsewhere)."""
+        P = np.zeros(npacked(ndim))
+        self._check(self._lib.ptbgpu_sm_finish(self._h, int(ndim), float(mu), _dptr(P)))
+        return P
 
     def kmeans_partition(self, ndim: int, Hvec: np.ndarray, Svec: np.ndarray, n: int, xyz: np.ndarray,
                          aoat: np.ndarray, seed: int = 42, opts: Options | None = None):

@@ -13,6 +13,12 @@ void symsq_entry(ptbgpu_ctx* c, int64_t n, int np, int kblock, const double* hX,
 std::vector<int64_t> kmeans_partition(ptbgpu_ctx* c, int64_t n, const double* dH, const double* dS, int64_t nat,
                                       const double* xyz, const int64_t* aoat, uint64_t seed, int* nsm_out,
                                       double* effort_out);
+void sm_plan_entry(ptbgpu_ctx* c, int64_t n, const double* dH, const double* dS, int64_t nat, const double* xyz,
+                   const int64_t* aoat, int64_t columns, int64_t mode, const int64_t* partition, const ptbgpu_opts* o,
+                   int64_t* nsm, int64_t* dims);
+void sm_prepare_entry(ptbgpu_ctx* c, int64_t nlocal, const int64_t* ids, ptbgpu_stats* st);
+double sm_nel_entry(ptbgpu_ctx* c, double mu);
+void sm_finish_entry(ptbgpu_ctx* c, double mu, double* dP);
 void mlpop14_device(ptbgpu_ctx* c, int64_t n, const double* dSpk, double x, float* s34, float* s14);
 void mlpop2_diag_device(ptbgpu_ctx* c, int64_t n, const double* dPpk, const float* s1, const float* s2, double* xd);
 void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int variant, int tri_a, int tri_b, bool sym,
@@ -279,6 +285,43 @@ int ptbgpu_symsq_split(ptbgpu_ctx* c, int64_t n, int64_t planes, int64_t kblock,
                 *ms += x;
             }
         }
+    });
+}
+
+int ptbgpu_sm_plan(ptbgpu_ctx* c, int64_t ndim, const double* Hpk, const double* Spk, int64_t nat,
+                   const double* xyz, const int64_t* aoat, int64_t columns, int64_t mode, const int64_t* partition,
+                   const ptbgpu_opts* opts, int64_t* nsm, int64_t* dims) {
+    return guarded(c, [&] {
+        PTB_CHECK(ndim > 0 && Hpk && Spk && aoat && nsm && dims, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, ndim);
+        io.in(0, Hpk);
+        io.in(1, Spk);
+        sm_plan_entry(c, ndim, io.d[0], io.d[1], nat, xyz, aoat, columns, mode, partition, opts, nsm, dims);
+    });
+}
+
+int ptbgpu_sm_prepare(ptbgpu_ctx* c, int64_t nlocal, const int64_t* ids, ptbgpu_stats* st) {
+    clear_stats(st);
+    return guarded(c, [&] {
+        PTB_CHECK(nlocal >= 0 && (ids || nlocal == 0), PTBGPU_EINVAL, "bad arguments");
+        sm_prepare_entry(c, nlocal, ids, st);
+    });
+}
+
+int ptbgpu_sm_nel(ptbgpu_ctx* c, double mu, double* nel) {
+    return guarded(c, [&] {
+        PTB_CHECK(nel != nullptr, PTBGPU_EINVAL, "bad arguments");
+        *nel = sm_nel_entry(c, mu);
+    });
+}
+
+int ptbgpu_sm_finish(ptbgpu_ctx* c, int64_t ndim, double mu, double* Ppk) {
+    return guarded(c, [&] {
+        PTB_CHECK(ndim > 0 && Ppk, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, ndim);
+        sm_finish_entry(c, mu, io.d[2]);
+        io.out(2, Ppk);
+        PTB_CUDA(cudaStreamSynchronize(c->stream));
     });
 }
 

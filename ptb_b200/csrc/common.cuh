@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -87,6 +88,9 @@ struct ptbgpu_ctx {
     void* pinned = nullptr;              // small pinned staging area (4 KB)
     // trace-correcting purification state (device)
     void* sp2_state = nullptr;
+    // submatrix method between its phases (plan, prepare, nel, finish): kept
+    // until the next plan or the context's end; its destructor frees its buffers
+    std::shared_ptr<void> sm_plan;
     // launches of this library's kernels since the last call started
     int64_t launches = 0;
     // timed tensor-core launches: event pairs recorded on `stream`

@@ -106,6 +106,7 @@ int ptbgpu_init(int device, ptbgpu_ctx** out) {
 int ptbgpu_finalize(ptbgpu_ctx* c) {
     if (!c) return PTBGPU_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    c->sm_plan.reset();
     for (auto& b : c->bufs) b.release();
     if (c->flags) cudaFree(c->flags);
     if (c->info_dev) cudaFree(c->info_dev);

@@ -528,29 +528,85 @@ T* upload(ptbgpu_ctx* c, int id, const std::vector<T>& v) {
 
 }  // namespace
 
-void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* dH, const double* dS, double* dP,
-                       int64_t nat, const double* xyz, const int64_t* aoat, int64_t columns, int64_t mode,
-                       const int64_t* partition, const ptbgpu_opts* o, ptbgpu_stats* st) {
+namespace {
+
+// One size bucket of prepared submatrices (or one large submatrix).
+struct Bucket {
+    int M = 0, count = 0;
+    bool is_large = false;
+    Prob single{};
+    DevBuf probs, U, w;
+};
+
+// __global__ helper: nel(mu) = sum fe_q occ(e_q, mu) over the prepared
+// eigenpairs, one block of 1024 threads with the same partition and reduction
+// order as k_mu_bisect (so a one-rank host bisection reproduces it exactly).
+__global__ void k_nel_at(int64_t total, const double* __restrict__ e, const double* __restrict__ fe, double mu,
+                         double* __restrict__ out) {
+    __shared__ double sh[1024];
+    double part = 0.0;
+    for (int64_t q = threadIdx.x; q < total; q += blockDim.x) {
+        const double ev = e[q];
+        const double occ = ev < mu ? 2.0 : (ev == mu ? 1.0 : 0.0);
+        part += fe[q] * occ;
+    }
+    const double nel = block_sum_fixed(part, sh);
+    if (threadIdx.x == 0) *out = nel;
+}
+
+}  // namespace
+
+// The submatrix method between its phases.  Device data lives in context
+// buffers (filtered H and S in B_H / B_S, owners, owned columns, map offsets,
+// maps and row positions in B_SM0..B_SM7, eigenvalues and fe weights of the
+// prepared submatrices in B_MISC0 / B_MISC1) and in the buckets below.
+struct SmPlan {
+    int64_t n = 0;
+    int nsm = 0;
+    int prl = 0;
+    std::vector<int64_t> own_off;
+    std::vector<int> counts;
+    std::vector<int64_t> moff;
+    std::vector<Bucket> bks;
+    int64_t total = 0;     // prepared eigenpairs
+    double flops = 0.0;
+    bool prepared = false;
+    ~SmPlan() {
+        for (Bucket& bk : bks) {
+            bk.probs.release();
+            bk.U.release();
+            bk.w.release();
+        }
+    }
+};
+
+namespace {
+
+SmPlan& plan_of(ptbgpu_ctx* c) {
+    PTB_CHECK(c->sm_plan != nullptr, PTBGPU_EINVAL, "no submatrix plan on this context (call the plan phase first)");
+    return *static_cast<SmPlan*>(c->sm_plan.get());
+}
+
+}  // namespace
+
+// (1)-(3): filtered H and S, grouping (mode 4 without a partition runs the
+// seeded k-means), pattern scan, ordered maps.  Replaces any earlier plan.
+SmPlan& sm_plan(ptbgpu_ctx* c, int64_t n, const double* dH, const double* dS, int64_t nat, const double* xyz,
+                const int64_t* aoat, int64_t columns, int64_t mode, const int64_t* partition, const ptbgpu_opts* o) {
     const int prl = o ? (int)o->print_level : 0;
     const double filter = o ? o->filter : 0.0;
     if (mode == PTBGPU_SUBMATRIX_SIGN) fail(PTBGPU_ENOTIMPL, "submatrix_mode.eq.1 not implemented");
     PTB_CHECK(mode == PTBGPU_SUBMATRIX_SYGV, PTBGPU_ENOTIMPL, "not implemented submatrix_mode %lld", (long long)mode);
     PTB_CHECK(n > 0 && n < (int64_t)1 << 31, PTBGPU_EINVAL, "bad ndim");
     cudaStream_t s = c->stream;
+    c->sm_plan.reset();
+    auto owner_plan = std::make_shared<SmPlan>();
+    SmPlan& pl = *owner_plan;
+    pl.n = n;
+    pl.prl = prl;
     log_line(prl, 1, " Stupid simple implementation of the submatrix method: %lld %lld", (long long)columns,
              (long long)mode);
-    // phase timer (print level >= 2 only: it synchronises the stream at each mark)
-    auto t_last = std::chrono::steady_clock::now();
-    auto mark = [&](const char* what) {
-        if (prl < 2) return;
-        PTB_CUDA(cudaStreamSynchronize(s));
-        auto now = std::chrono::steady_clock::now();
-        log_line(prl, 2, " * submatrix %-28s %10.3f ms", what,
-                 std::chrono::duration<double, std::milli>(now - t_last).count());
-        t_last = now;
-    };
 
-    // full, filtered H and S
     DevBuf& bh = c->buf(B_H);
     DevBuf& bs = c->buf(B_S);
     bh.reserve(sizeof(double) * n * n);
@@ -560,7 +616,6 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
     unpack_sym(s, n, n, dH, H, filter);
     unpack_sym(s, n, n, dS, S, filter);
 
-    // (1) grouping; mode 4 without a supplied partition runs the seeded k-means
     std::vector<int64_t> own_part;
     if (columns == PTBGPU_COLUMNS_KMEANS && partition == nullptr) {
         int k = 0;
@@ -568,24 +623,23 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
         own_part = kmeans_partition(c, n, H, S, nat, xyz, aoat, kKmeansSeed, &k, &eff);
         partition = own_part.data();
         log_line(prl, 1, " k-means partition: %d clusters, effort %.6e", k, eff);
-        mark("k-means partition");
     }
     std::vector<std::vector<int>> comb = group_columns(n, aoat, nat, columns, partition);
     const int nsm = (int)comb.size();
+    pl.nsm = nsm;
     std::vector<int> owner(n, -1), own_cols;
-    std::vector<int64_t> own_off(nsm + 1, 0);
+    pl.own_off.assign(nsm + 1, 0);
     for (int k = 0; k < nsm; ++k) {
-        own_off[k + 1] = own_off[k] + (int64_t)comb[k].size();
+        pl.own_off[k + 1] = pl.own_off[k] + (int64_t)comb[k].size();
         for (int col : comb[k]) {
             owner[col] = k;
             own_cols.push_back(col);
         }
     }
     int* d_owner = upload(c, B_SM0, owner);
-    int* d_own_cols = upload(c, B_SM1, own_cols);
-    int64_t* d_own_off = upload(c, B_SM2, own_off);
+    upload(c, B_SM1, own_cols);
+    upload(c, B_SM2, pl.own_off);
 
-    // (2) pattern scan
     DevBuf& bf = c->buf(B_SM3);
     bf.reserve((size_t)nsm * n);
     PTB_CUDA(cudaMemsetAsync(bf.ptr, 0, (size_t)nsm * n, s));
@@ -597,68 +651,91 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
     k_count<<<nsm, 256, 0, s>>>(n, bf.as<uint8_t>(), bc.as<int>());
     count_launch();
     PTB_CUDA(cudaGetLastError());
-    std::vector<int> counts(nsm);
-    PTB_CUDA(cudaMemcpyAsync(counts.data(), bc.ptr, sizeof(int) * nsm, cudaMemcpyDeviceToHost, s));
+    pl.counts.resize(nsm);
+    PTB_CUDA(cudaMemcpyAsync(pl.counts.data(), bc.ptr, sizeof(int) * nsm, cudaMemcpyDeviceToHost, s));
     PTB_CUDA(cudaStreamSynchronize(s));
-    std::vector<int64_t> moff(nsm + 1, 0);
-    for (int k = 0; k < nsm; ++k) moff[k + 1] = moff[k] + counts[k];
-    int64_t* d_moff = upload(c, B_SM5, moff);
+    pl.moff.assign(nsm + 1, 0);
+    for (int k = 0; k < nsm; ++k) pl.moff[k + 1] = pl.moff[k] + pl.counts[k];
+    int64_t* d_moff = upload(c, B_SM5, pl.moff);
     DevBuf& bm = c->buf(B_SM6);
-    bm.reserve(sizeof(int) * std::max<int64_t>(moff[nsm], 1));
+    bm.reserve(sizeof(int) * std::max<int64_t>(pl.moff[nsm], 1));
     DevBuf& bip = c->buf(B_SM7);
     bip.reserve(sizeof(int) * n);
     k_fill<<<nsm, 256, 0, s>>>(n, bf.as<uint8_t>(), d_moff, d_owner, bm.as<int>(), bip.as<int>());
     count_launch();
     PTB_CUDA(cudaGetLastError());
-    const int* d_maps = bm.as<int>();
-    const int* d_ipos = bip.as<int>();
 
-    int64_t sumdims = moff[nsm];
-    int maxdim = *std::max_element(counts.begin(), counts.end());
+    const int64_t sumdims = pl.moff[nsm];
     double effort_full = std::pow((double)n, 2.5), effort_sms = 0.0;
-    for (int k = 0; k < nsm; ++k) effort_sms += std::pow((double)counts[k], 2.5);
+    for (int k = 0; k < nsm; ++k) effort_sms += std::pow((double)pl.counts[k], 2.5);
     log_line(prl, 1, " number of submatrices= %d", nsm);
     log_line(prl, 1, " average sm dim= %lld", (long long)(sumdims / nsm));
     log_line(prl, 1, " effort for full matrix ops= %g", effort_full);
     log_line(prl, 1, " sums of efforts for submatrices= %g", effort_sms);
     log_line(prl, 1, " ratio %g", effort_sms / effort_full);
+    c->sm_plan = owner_plan;
+    return pl;
+}
 
-    mark("unpack, pattern scan, maps");
-    // (4) buckets by padded size; submatrices above kBatchMax take the large path
+// (4)-(5): gather, reduction (potrf + 2 trsm), eigensolve and fe weights of
+// the listed submatrices (0-based, each at most once): buckets of padded size
+// <= 1024 through the batched cuSOLVER / cuBLAS calls, larger ones one dsygvd
+// each.  Their eigenpairs replace any earlier prepared set.
+void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
+    cudaStream_t s = c->stream;
+    const int prl = pl.prl;
+    const int64_t n = pl.n;
+    for (Bucket& bk : pl.bks) {
+        bk.probs.release();
+        bk.U.release();
+        bk.w.release();
+    }
+    pl.bks.clear();
+    pl.prepared = false;
+    pl.flops = 0.0;
+    std::vector<char> seen(pl.nsm, 0);
+    for (int k : ids) {
+        PTB_CHECK(k >= 0 && k < pl.nsm && !seen[k], PTBGPU_EINVAL, "bad or repeated submatrix index %d", k);
+        seen[k] = 1;
+    }
+    const double* H = c->buf(B_H).as<double>();
+    const double* S = c->buf(B_S).as<double>();
+    const int* d_own_cols = c->buf(B_SM1).as<int>();
+    const int64_t* d_own_off = c->buf(B_SM2).as<int64_t>();
+    const int* d_maps = c->buf(B_SM6).as<int>();
+    const int* d_ipos = c->buf(B_SM7).as<int>();
+    auto t_last = std::chrono::steady_clock::now();
+    auto mark = [&](const char* what) {
+        if (prl < 2) return;
+        PTB_CUDA(cudaStreamSynchronize(s));
+        auto now = std::chrono::steady_clock::now();
+        log_line(prl, 2, " * submatrix %-28s %10.3f ms", what,
+                 std::chrono::duration<double, std::milli>(now - t_last).count());
+        t_last = now;
+    };
+
     constexpr int kBatchMax = 1024;
     std::map<int, std::vector<Prob>> buckets;
     std::vector<Prob> large;
     int64_t eoff = 0;
-    for (int k = 0; k < nsm; ++k) {
-        Prob p{k, counts[k], moff[k], eoff};
-        eoff += counts[k];
-        if (counts[k] > kBatchMax) large.push_back(p);
-        else buckets[(int)round_up(counts[k], 32)].push_back(p);
+    for (int k : ids) {
+        Prob p{k, pl.counts[k], pl.moff[k], eoff};
+        eoff += pl.counts[k];
+        if (pl.counts[k] > kBatchMax) large.push_back(p);
+        else buckets[(int)round_up(pl.counts[k], 32)].push_back(p);
     }
-    const int64_t total = eoff;
+    pl.total = eoff;
     DevBuf& be = c->buf(B_MISC0);
     DevBuf& bfe = c->buf(B_MISC1);
-    be.reserve(sizeof(double) * total);
-    bfe.reserve(sizeof(double) * total);
+    be.reserve(sizeof(double) * std::max<int64_t>(eoff, 1));
+    bfe.reserve(sizeof(double) * std::max<int64_t>(eoff, 1));
+    pl.bks.resize(buckets.size() + large.size());
 
-    struct Bucket {
-        int M = 0, count = 0;
-        bool is_large = false;
-        Prob single{};
-        DevBuf probs, U, w;
-    };
-    std::vector<Bucket> bks(buckets.size() + large.size());
     DevBuf sb, ptrs, infos, ws, tbuf;
-    double flops = 0.0;
     cusolverDnParams_t params;
     PTB_CUSOLVER(cusolverDnCreateParams(&params));
     auto cleanup = [&] {
         cusolverDnDestroyParams(params);
-        for (Bucket& bk : bks) {
-            bk.probs.release();
-            bk.U.release();
-            bk.w.release();
-        }
         sb.release();
         ptrs.release();
         infos.release();
@@ -678,7 +755,7 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
             const int M = kv.first;
             std::vector<Prob>& pv = kv.second;
             const int B = (int)pv.size();
-            Bucket& bk = bks[bi++];
+            Bucket& bk = pl.bks[bi++];
             bk.M = M;
             bk.count = B;
             bk.probs.reserve(sizeof(Prob) * B);
@@ -747,12 +824,12 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
             count_launch();
             PTB_CUDA(cudaGetLastError());
             mark("back-transform and fe");
-            for (const Prob& p : pv) flops += 9.0 * std::pow((double)p.m, 3);
+            for (const Prob& p : pv) pl.flops += 9.0 * std::pow((double)p.m, 3);
             log_line(prl, 2, " * submatrix bucket M=%d: %d problems", M, B);
         }
         // large submatrices: one generalized eigensolve each (dsygvd), fe from T = S_k U
         for (const Prob& p : large) {
-            Bucket& bk = bks[bi++];
+            Bucket& bk = pl.bks[bi++];
             bk.is_large = true;
             bk.single = p;
             const int m = p.m;
@@ -777,53 +854,70 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
             PTB_CUDA(cudaGetLastError());
             PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &one, Sk, m, U, m, &zero,
                                    tbuf.as<double>(), m));
-            k_fe_large<<<(m + 255) / 256, 256, 0, s>>>(m, tbuf.as<double>(), U, d_own_cols, own_off[p.k],
-                                                       own_off[p.k + 1], d_ipos, bk.w.as<double>(),
+            k_fe_large<<<(m + 255) / 256, 256, 0, s>>>(m, tbuf.as<double>(), U, d_own_cols, pl.own_off[p.k],
+                                                       pl.own_off[p.k + 1], d_ipos, bk.w.as<double>(),
                                                        be.as<double>() + p.eoff, bfe.as<double>() + p.eoff);
             count_launch();
             PTB_CUDA(cudaGetLastError());
-            flops += 9.0 * std::pow((double)m, 3);
+            pl.flops += 9.0 * std::pow((double)m, 3);
         }
-
-        // (6) mu bisection
-        DevBuf bmu;
-        bmu.reserve(sizeof(MuResult));
-        const double tol_mu = (double)1e-3f, tol_nel = (double)1e-5f;
-        k_mu_bisect<<<1, 1024, 0, s>>>(total, be.as<double>(), bfe.as<double>(), (double)nelref, tol_mu, tol_nel,
-                                       bmu.as<MuResult>());
-        count_launch();
-        PTB_CUDA(cudaGetLastError());
-        MuResult mr;
-        PTB_CUDA(cudaMemcpyAsync(&mr, bmu.ptr, sizeof(MuResult), cudaMemcpyDeviceToHost, s));
         PTB_CUDA(cudaStreamSynchronize(s));
-        bmu.release();
-        for (int it = 0; it < mr.iters; ++it)
-            log_line(prl, 1, " muiter %d mu %.15g %.15g of %lld", it + 1, mr.trace_mu[it], mr.trace_nel[it],
-                     (long long)nelref);
-        PTB_CHECK(mr.converged, PTBGPU_EITER, "chemical potential bisection did not converge");
-        log_line(prl, 1, " iteration of chemical potential converged");
-        mark("mu bisection");
+    } catch (...) {
+        cleanup();
+        throw;
+    }
+    cleanup();
+    pl.prepared = true;
+}
 
-        // (7) final density into the packed result
-        PTB_CUDA(cudaMemsetAsync(dP, 0, sizeof(double) * (size_t)npacked(n), s));
-        for (Bucket& bk : bks) {
+// Electron count of the prepared submatrices at mu (the rank-local term of the
+// bisection in source/sm.f90:322-340).
+double sm_nel(ptbgpu_ctx* c, SmPlan& pl, double mu) {
+    PTB_CHECK(pl.prepared, PTBGPU_EINVAL, "submatrices not prepared");
+    cudaStream_t s = c->stream;
+    DevBuf& bo = c->buf(B_MISC2);
+    bo.reserve(sizeof(double) * 64);
+    k_nel_at<<<1, 1024, 0, s>>>(pl.total, c->buf(B_MISC0).as<double>(), c->buf(B_MISC1).as<double>(), mu,
+                                bo.as<double>());
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+    double v = 0.0;
+    PTB_CUDA(cudaMemcpyAsync(&v, bo.ptr, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PTB_CUDA(cudaStreamSynchronize(s));
+    return v;
+}
+
+// (7): dP := 0, then the owned columns of every prepared submatrix at mu.
+void sm_finish(ptbgpu_ctx* c, SmPlan& pl, double mu, double* dP) {
+    PTB_CHECK(pl.prepared, PTBGPU_EINVAL, "submatrices not prepared");
+    cudaStream_t s = c->stream;
+    const int64_t n = pl.n;
+    const int* d_own_cols = c->buf(B_SM1).as<int>();
+    const int64_t* d_own_off = c->buf(B_SM2).as<int64_t>();
+    const int* d_maps = c->buf(B_SM6).as<int>();
+    const int* d_ipos = c->buf(B_SM7).as<int>();
+    const double one = 1.0, zero = 0.0;
+    PTB_CUDA(cudaMemsetAsync(dP, 0, sizeof(double) * (size_t)npacked(n), s));
+    DevBuf tbuf;
+    try {
+        for (Bucket& bk : pl.bks) {
             if (!bk.is_large) {
                 dim3 g(bk.count, 4);
                 k_final<<<g, 256, sizeof(double) * bk.M, s>>>(bk.M, bk.probs.as<Prob>(), d_maps, d_own_off,
                                                              d_own_cols, d_ipos, bk.U.as<double>(), bk.w.as<double>(),
-                                                             mr.mu, dP);
+                                                             mu, dP);
                 count_launch();
                 PTB_CUDA(cudaGetLastError());
                 continue;
             }
             const Prob& p = bk.single;
             const int m = p.m;
-            const int64_t o0 = own_off[p.k], nown = own_off[p.k + 1] - o0;
+            const int64_t o0 = pl.own_off[p.k], nown = pl.own_off[p.k + 1] - o0;
             tbuf.reserve(sizeof(double) * (size_t)m * nown * 2);
             double* Z = tbuf.as<double>();
             double* Pc = Z + (size_t)m * nown;
             dim3 g((m + 255) / 256, (unsigned)std::min<int64_t>(nown, 65535));
-            k_occ_rows<<<g, 256, 0, s>>>(m, bk.U.as<double>(), bk.w.as<double>(), mr.mu, d_own_cols, o0, nown, d_ipos,
+            k_occ_rows<<<g, 256, 0, s>>>(m, bk.U.as<double>(), bk.w.as<double>(), mu, d_own_cols, o0, nown, d_ipos,
                                         Z);
             count_launch();
             PTB_CUDA(cudaGetLastError());
@@ -834,21 +928,86 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
             PTB_CUDA(cudaGetLastError());
         }
         PTB_CUDA(cudaStreamSynchronize(s));
-        mark("final density");
-        if (st) {
-            st->mu = mr.mu;
-            st->nel = mr.nel;
-            st->mu_iterations = mr.iters;
-            st->nsm = nsm;
-            st->sum_dims = sumdims;
-            st->max_dim = maxdim;
-            st->flops += flops;
-        }
     } catch (...) {
-        cleanup();
+        tbuf.release();
         throw;
     }
-    cleanup();
+    tbuf.release();
 }
+
+// The whole step on one device: plan, every submatrix, the device bisection
+// (source/sm.f90:191-383), the final density.
+void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* dH, const double* dS, double* dP,
+                       int64_t nat, const double* xyz, const int64_t* aoat, int64_t columns, int64_t mode,
+                       const int64_t* partition, const ptbgpu_opts* o, ptbgpu_stats* st) {
+    SmPlan& pl = sm_plan(c, n, dH, dS, nat, xyz, aoat, columns, mode, partition, o);
+    const int prl = pl.prl;
+    std::vector<int> all(pl.nsm);
+    std::iota(all.begin(), all.end(), 0);
+    sm_prepare(c, pl, all);
+    cudaStream_t s = c->stream;
+    DevBuf bmu;
+    bmu.reserve(sizeof(MuResult));
+    const double tol_mu = (double)1e-3f, tol_nel = (double)1e-5f;
+    k_mu_bisect<<<1, 1024, 0, s>>>(pl.total, c->buf(B_MISC0).as<double>(), c->buf(B_MISC1).as<double>(),
+                                   (double)nelref, tol_mu, tol_nel, bmu.as<MuResult>());
+    count_launch();
+    PTB_CUDA(cudaGetLastError());
+    MuResult mr;
+    PTB_CUDA(cudaMemcpyAsync(&mr, bmu.ptr, sizeof(MuResult), cudaMemcpyDeviceToHost, s));
+    PTB_CUDA(cudaStreamSynchronize(s));
+    bmu.release();
+    for (int it = 0; it < mr.iters; ++it)
+        log_line(prl, 1, " muiter %d mu %.15g %.15g of %lld", it + 1, mr.trace_mu[it], mr.trace_nel[it],
+                 (long long)nelref);
+    PTB_CHECK(mr.converged, PTBGPU_EITER, "chemical potential bisection did not converge");
+    log_line(prl, 1, " iteration of chemical potential converged");
+    sm_finish(c, pl, mr.mu, dP);
+    if (st) {
+        st->mu = mr.mu;
+        st->nel = mr.nel;
+        st->mu_iterations = mr.iters;
+        st->nsm = pl.nsm;
+        st->sum_dims = pl.moff[pl.nsm];
+        st->max_dim = *std::max_element(pl.counts.begin(), pl.counts.end());
+        st->flops += pl.flops;
+    }
+}
+
+// ---- phase entry points for the C-ABI (one rank's share of the step) -------
+void sm_plan_entry(ptbgpu_ctx* c, int64_t n, const double* dH, const double* dS, int64_t nat, const double* xyz,
+                   const int64_t* aoat, int64_t columns, int64_t mode, const int64_t* partition, const ptbgpu_opts* o,
+                   int64_t* nsm, int64_t* dims) {
+    SmPlan& pl = sm_plan(c, n, dH, dS, nat, xyz, aoat, columns, mode, partition, o);
+    if (nsm) *nsm = pl.nsm;
+    if (dims)
+        for (int k = 0; k < pl.nsm; ++k) dims[k] = pl.counts[k];
+}
+
+void sm_prepare_entry(ptbgpu_ctx* c, int64_t nlocal, const int64_t* ids, ptbgpu_stats* st) {
+    SmPlan& pl = plan_of(c);
+    std::vector<int> v((size_t)nlocal);
+    for (int64_t q = 0; q < nlocal; ++q) {
+        PTB_CHECK(ids[q] >= 0 && ids[q] < pl.nsm, PTBGPU_EINVAL, "submatrix index %lld out of range",
+                  (long long)ids[q]);
+        v[q] = (int)ids[q];
+    }
+    sm_prepare(c, pl, v);
+    if (st) {
+        st->nsm = nlocal;
+        int64_t sd = 0, md = 0;
+        for (int k : v) {
+            sd += pl.counts[k];
+            md = std::max<int64_t>(md, pl.counts[k]);
+        }
+        st->sum_dims = sd;
+        st->max_dim = md;
+        st->flops += pl.flops;
+    }
+}
+
+double sm_nel_entry(ptbgpu_ctx* c, double mu) { return sm_nel(c, plan_of(c), mu); }
+
+void sm_finish_entry(ptbgpu_ctx* c, double mu, double* dP) { sm_finish(c, plan_of(c), mu, dP); }
 
 }  // namespace ptb

@@ -1,0 +1,88 @@
+"""The submatrix method over ranks (ptb_b200.distributed) on CPU gloo ranks,
+with the oracle standing in for each rank's device share: the size-balanced
+assignment, the bisection with one all-reduce per step and the assembly of P
+must reproduce the one-process oracle."""
+import os
+import socket
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import ptb_oracle as O
+from ptb_b200 import Options, synth
+from ptb_b200.distributed import assign_submatrices, mu_bisect, sm_stupid_simple_sharded
+from shard_oracle import OracleShard
+
+FILTER = 1e-4
+
+
+def _system():
+    return synth.alkane(6, seed=2)
+
+
+def test_assignment_covers_and_balances():
+    rng = np.random.default_rng(3)
+    dims = rng.integers(20, 600, size=57)
+    for nr in (1, 2, 3, 8):
+        parts = assign_submatrices(dims, nr)
+        flat = sorted(k for p in parts for k in p)
+        assert flat == list(range(len(dims)))
+        loads = [sum(float(dims[k]) ** 3 for k in p) for p in parts]
+        assert max(loads) - min(loads) <= float(max(dims)) ** 3
+        assert parts == assign_submatrices(dims, nr)
+
+
+@pytest.mark.parametrize("columns", [1, 2])
+def test_single_process_matches_oracle(columns):
+    s = _system()
+    n = s.ndim
+    o = Options(filter=FILTER)
+    P, info = sm_stupid_simple_sharded(OracleShard(), n, s.nel, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, columns, 2,
+                                       opts=o)
+    ref = O.sm_stupid_simple(n, s.nel, O.filter_matrix_sym(s.Hvec, FILTER), O.filter_matrix_sym(s.Svec, FILTER),
+                             s.nat, s.xyz, s.aoat, columns, 2)
+    assert info.mu == ref.mu
+    assert np.max(np.abs(P - ref.Pvec)) < 1e-13
+
+
+def test_bisection_restates_the_reference():
+    """mu_bisect on a monotone staircase: the reference's stop rule and final pass."""
+    levels = np.linspace(-1.0, 1.0, 41)
+    nel_fn = lambda mu: 2.0 * float(np.sum(levels < mu)) + float(np.sum(levels == mu))
+    mu, nel, trace, ok = mu_bisect(nel_fn, 40.0)
+    assert ok and abs(nel - 40.0) < 1e-5 and len(trace) >= 1
+
+
+def _worker(rank, world, port, out, columns):
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        s = _system()
+        P, info = sm_stupid_simple_sharded(OracleShard(), s.ndim, s.nel, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat,
+                                           columns, 2, opts=Options(filter=FILTER))
+        np.save(os.path.join(out, f"P{rank}.npy"), P)
+        np.save(os.path.join(out, f"ids{rank}.npy"), np.asarray(info.local, dtype=np.int64))
+        np.save(os.path.join(out, f"mu{rank}.npy"), np.array([info.mu]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_match_oracle():
+    columns = 1   # one submatrix per column: the most submatrices to split
+    import torch.multiprocessing as mp
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")   # the two ranks share the host cores
+    with tempfile.TemporaryDirectory() as out:
+        mp.spawn(_worker, args=(2, port, out, columns), nprocs=2, join=True)
+        P0, P1 = np.load(os.path.join(out, "P0.npy")), np.load(os.path.join(out, "P1.npy"))
+        ids0, ids1 = np.load(os.path.join(out, "ids0.npy")), np.load(os.path.join(out, "ids1.npy"))
+        mu0, mu1 = np.load(os.path.join(out, "mu0.npy")), np.load(os.path.join(out, "mu1.npy"))
+    s = _system()
+    ref = O.sm_stupid_simple(s.ndim, s.nel, O.filter_matrix_sym(s.Hvec, FILTER), O.filter_matrix_sym(s.Svec, FILTER),
+                             s.nat, s.xyz, s.aoat, columns, 2)
+    assert len(ids0) > 0 and len(ids1) > 0 and not set(ids0) & set(ids1)
+    assert np.array_equal(P0, P1) and mu0[0] == mu1[0]
+    assert np.max(np.abs(P0 - ref.Pvec)) < 1e-12
