@@ -88,6 +88,10 @@ typedef struct {
                                    (orthogonalisation, cleanup, commutator, back-transform) run on
                                    the int8 tensor cores with that many 7-bit slices per operand;
                                    0 -> cuBLAS/cuSOLVER FP64 */
+    int64_t refine_rounds;      /* PREC_MIXED: cap on the refinement rounds (Newton steps on the
+                                   occupied subspace after the tensor-core purification); 0 = 4 */
+    double  refine_tol;         /* PREC_MIXED: another round runs while the error predicted after
+                                   the last one (orthonormal basis) exceeds this; 0 = 1e-7 */
 } ptbgpu_opts;
 
 /* What a call reports back (all optional for the caller). */
@@ -117,6 +121,9 @@ typedef struct {
     int64_t n_oz;
     double  oz_ops;             /* int8 multiply-adds x 2 those products executed (slice pairs, all tiles) */
     double  tc_flops;           /* bf16 flops the tcgen05 split products executed (all planes, all tiles) */
+    int64_t refine_rounds;      /* PREC_MIXED: refinement rounds run                                   */
+    int64_t fp64_fallback;      /* PREC_MIXED: 1 if the refinement could not reach refine_tol (gap too
+                                   small for the bf16 trajectory) and the purification was redone in FP64 */
 } ptbgpu_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */
@@ -172,6 +179,20 @@ int ptbgpu_tc_purify(ptbgpu_ctx* ctx, int64_t ndim, int64_t nel,
 int ptbgpu_tc_purify_device(ptbgpu_ctx* ctx, int64_t ndim, int64_t nel,
                             const double* dHpk, const double* dSpk, double* dPpk,
                             const ptbgpu_opts* opts, ptbgpu_stats* st);
+
+/* ptbgpu_tc_purify over ninst independent systems (system i: ndim[i], nel[i],
+ * Hpk[i], Spk[i] in, Ppk[i] out), as the PTB driver would loop over many
+ * molecules (the density step of source/pgtb.f90:599-618 once per system).  `workers` host
+ * threads (0 = 4), each with its own worker context and stream on ctx's
+ * device, take systems largest first, so that small systems overlap on the
+ * GPU.  st may be NULL or point to ninst stats; wall_ms (may be NULL) gets the
+ * host wall time of the whole batch.  The first failing system's status is
+ * returned and named in ptbgpu_last_error(ctx); systems not yet started are
+ * skipped then.  Worker contexts are kept for later batches and released by
+ * ptbgpu_finalize(ctx). */
+int ptbgpu_tc_purify_batch(ptbgpu_ctx* ctx, int64_t ninst, const int64_t* ndim, const int64_t* nel,
+                           const double* const* Hpk, const double* const* Spk, double* const* Ppk,
+                           int64_t workers, const ptbgpu_opts* opts, ptbgpu_stats* st, double* wall_ms);
 
 /* solve2(mode,ndim,nel,nopen,homo,et,focc,H,S,P,e,U,fail), source/pgtb.f90:1066-1170:
  * dense generalized eigensolve + Fermi smearing, the check-mode oracle.

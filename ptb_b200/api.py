@@ -50,7 +50,7 @@ class _Opts(C.Structure):
     _fields_ = [("filter", C.c_double), ("precision", C.c_int64), ("print_level", C.c_int64),
                 ("max_iter", C.c_int64), ("electronic_temp", C.c_double), ("glob_par15", C.c_double),
                 ("glob_par17", C.c_double), ("split3_iters", C.c_int64),
-                ("fp64_slices", C.c_int64)]
+                ("fp64_slices", C.c_int64), ("refine_rounds", C.c_int64), ("refine_tol", C.c_double)]
 
 
 class _Stats(C.Structure):
@@ -61,12 +61,13 @@ class _Stats(C.Structure):
                 ("ms_h2d", C.c_double), ("ms_solve", C.c_double), ("ms_d2h", C.c_double), ("flops", C.c_double),
                 ("ms_tc_sp2", C.c_double), ("n_tc_sp2", C.c_int64), ("ms_tc_full", C.c_double),
                 ("n_tc_full", C.c_int64), ("kernel_launches", C.c_int64), ("ms_oz", C.c_double),
-                ("n_oz", C.c_int64), ("oz_ops", C.c_double), ("tc_flops", C.c_double)]
+                ("n_oz", C.c_int64), ("oz_ops", C.c_double), ("tc_flops", C.c_double),
+                ("refine_rounds", C.c_int64), ("fp64_fallback", C.c_int64)]
 
 
 EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_default_settings",
             "ptbgpu_default_opts", "ptbgpu_filter_packed", "ptbgpu_check_density", "ptbgpu_sm_density",
-            "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_solve2",
+            "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_tc_purify_batch", "ptbgpu_solve2",
             "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_symsq_split", "ptbgpu_runtime_info",
             "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm", "ptbgpu_mlpop14", "ptbgpu_mlpop14_device",
             "ptbgpu_mlpop2", "ptbgpu_mlpop2_device", "ptbgpu_kmeans_partition", "ptbgpu_sm_plan",
@@ -109,6 +110,8 @@ def load_library():
     lib.ptbgpu_tc_purify.argtypes = [C.c_void_p, i64, i64, d, d, d, P(_Opts), P(_Stats)]
     lib.ptbgpu_tc_purify_device.argtypes = [C.c_void_p, i64, i64, C.c_void_p, C.c_void_p, C.c_void_p, P(_Opts),
                                             P(_Stats)]
+    lib.ptbgpu_tc_purify_batch.argtypes = [C.c_void_p, i64, P(i64), P(i64), P(d), P(d), P(d), i64, P(_Opts),
+                                           P(_Stats), d]
     lib.ptbgpu_solve2.argtypes = [C.c_void_p, i64, i64, i64, i64, d, d, d, d, d, P(_Opts), P(_Stats)]
     lib.ptbgpu_symsq_bf16x3.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_bf16x6.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
@@ -181,6 +184,8 @@ class Stats:
     n_oz: int = 0
     oz_ops: float = 0.0
     tc_flops: float = 0.0
+    refine_rounds: int = 0
+    fp64_fallback: int = 0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "Stats":
@@ -199,10 +204,13 @@ class Options:
     glob_par17: float = 0.0
     split3_iters: int = 8
     fp64_slices: int = 8
+    refine_rounds: int = 4
+    refine_tol: float = 1e-7
 
     def to_c(self) -> _Opts:
         return _Opts(self.filter, self.precision, self.print_level, self.max_iter, self.electronic_temp,
-                     self.glob_par15, self.glob_par17, self.split3_iters, self.fp64_slices)
+                     self.glob_par15, self.glob_par17, self.split3_iters, self.fp64_slices, self.refine_rounds,
+                     self.refine_tol)
 
 
 class Context:
@@ -361,6 +369,25 @@ class Context:
         self._check(self._lib.ptbgpu_tc_purify_device(self._h, int(ndim), int(nel), C.c_void_p(dH),
                                                       C.c_void_p(dS), C.c_void_p(dP), C.byref(o), C.byref(st)))
         return Stats.from_c(st)
+
+    def tc_purify_batch(self, systems, opts: Options | None = None, workers: int = 0):
+        """tc_purify over many independent systems, `systems` a sequence of
+        (ndim, nel, H, S).  Host worker threads with their own streams overlap
+        the systems on the GPU.  Returns ([Pvec], [Stats], wall milliseconds)."""
+        n = len(systems)
+        m = max(n, 1)
+        ndim = (C.c_int64 * m)(*[int(s[0]) for s in systems])
+        nel = (C.c_int64 * m)(*[int(s[1]) for s in systems])
+        Hs = [_f64(s[2]) for s in systems]
+        Ss = [_f64(s[3]) for s in systems]
+        Ps = [np.zeros(npacked(int(s[0]))) for s in systems]
+        arr = lambda xs: (C.POINTER(C.c_double) * m)(*[_dptr(x) for x in xs])
+        st = (_Stats * max(n, 1))()
+        wall = C.c_double(0.0)
+        o = (opts or Options()).to_c()
+        self._check(self._lib.ptbgpu_tc_purify_batch(self._h, n, ndim, nel, arr(Hs), arr(Ss), arr(Ps),
+                                                     int(workers), C.byref(o), st, C.byref(wall)))
+        return Ps, [Stats.from_c(st[i]) for i in range(n)], wall.value
 
     def solve2(self, mode: int, ndim: int, nel: int, nopen: int, H: np.ndarray, S: np.ndarray,
                opts: Options | None = None):

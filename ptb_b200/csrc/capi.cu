@@ -1,7 +1,13 @@
 // extern "C" entry points: argument checks, host <-> device copies of the
 // packed arrays, CUDA-event timing, and translation of internal errors into
 // status codes plus a message readable through ptbgpu_last_error().
+#include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
 
 #include "common.cuh"
 #include "tc_gemm.cuh"
@@ -234,6 +240,57 @@ int ptbgpu_tc_purify_device(ptbgpu_ctx* c, int64_t ndim, int64_t nel, const doub
         t.mark(2);
         t.finish(st);
     });
+}
+
+int ptbgpu_tc_purify_batch(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const int64_t* nel,
+                           const double* const* Hpk, const double* const* Spk, double* const* Ppk, int64_t workers,
+                           const ptbgpu_opts* opts, ptbgpu_stats* st, double* wall_ms) {
+    if (!c) return PTBGPU_EINVAL;
+    if (ninst < 0 || (ninst > 0 && (!ndim || !nel || !Hpk || !Spk || !Ppk)) || workers < 0) {
+        c->last_error = "bad arguments";
+        return PTBGPU_EINVAL;
+    }
+    const int64_t want = workers == 0 ? 4 : workers;
+    const int nw = (int)std::max<int64_t>(1, std::min<int64_t>(want, std::max<int64_t>(ninst, 1)));
+    // worker contexts: created once per main context, reused by later batches
+    while ((int)c->workers.size() < nw) {
+        ptbgpu_ctx* w = nullptr;
+        const int rc = ptbgpu_init(c->device, &w);
+        if (rc != PTBGPU_OK) {
+            c->last_error = "could not create a worker context";
+            return rc;
+        }
+        c->workers.push_back(w);
+    }
+    // largest systems first, so that the small ones fill in around them
+    std::vector<int64_t> order((size_t)ninst);
+    for (int64_t i = 0; i < ninst; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return ndim[a] > ndim[b]; });
+    std::atomic<int64_t> next{0};
+    std::atomic<int> first_rc{PTBGPU_OK};
+    std::mutex err_mu;
+    std::string err_msg;
+    auto run = [&](ptbgpu_ctx* w) {
+        for (int64_t q = next++; q < ninst && first_rc.load() == PTBGPU_OK; q = next++) {
+            const int64_t i = order[q];
+            const int rc = ptbgpu_tc_purify(w, ndim[i], nel[i], Hpk[i], Spk[i], Ppk[i], opts, st ? &st[i] : nullptr);
+            if (rc != PTBGPU_OK) {
+                int expect = PTBGPU_OK;
+                if (first_rc.compare_exchange_strong(expect, rc)) {
+                    std::lock_guard<std::mutex> lock(err_mu);
+                    err_msg = "system " + std::to_string(i) + ": " + w->last_error;
+                }
+            }
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nw; ++t) pool.emplace_back(run, c->workers[t]);
+    for (auto& t : pool) t.join();
+    if (wall_ms) *wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    const int rc = first_rc.load();
+    c->last_error = rc == PTBGPU_OK ? std::string() : err_msg;
+    return rc;
 }
 
 int ptbgpu_solve2(ptbgpu_ctx* c, int64_t mode, int64_t ndim, int64_t nel, int64_t nopen, const double* Hpk,

@@ -107,6 +107,8 @@ int ptbgpu_finalize(ptbgpu_ctx* c) {
     if (!c) return PTBGPU_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->sm_plan.reset();
+    for (ptbgpu_ctx* w : c->workers) ptbgpu_finalize(w);
+    c->workers.clear();
     for (auto& b : c->bufs) b.release();
     if (c->flags) cudaFree(c->flags);
     if (c->info_dev) cudaFree(c->info_dev);
@@ -171,6 +173,8 @@ void ptbgpu_default_opts(ptbgpu_opts* o) {
     o->electronic_temp = 300.0;
     o->split3_iters = 8;
     o->fp64_slices = 8;
+    o->refine_rounds = 4;
+    o->refine_tol = 1e-7;
 }
 
 }  // extern "C"

@@ -572,12 +572,12 @@ template <int EPI, int S, int RB>
 void launch_t(cudaStream_t s, const OzMaps& maps, const int4* tiles, int ntiles, const Operand& a,
               const Operand& b, const OzEpi& ep) {
     using C = OzCfg<S, RB>;
-    static bool attr = false;
-    if (!attr) {
+    static const bool attr = [] {   // thread-safe one-time setup
         PTB_CUDA(cudaFuncSetAttribute(k_oz_product<EPI, S, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       C::SMEM));
-        attr = true;
-    }
+        return true;
+    }();
+    (void)attr;
     k_oz_product<EPI, S, RB><<<ntiles, THREADS, C::SMEM, s>>>(maps, tiles, a.exps, b.exps, ep);
     count_launch();
 }
@@ -591,12 +591,12 @@ void launch_ta(cudaStream_t s, const OzMaps& maps, const int4* tiles, int ntiles
     constexpr int STAGE = S * (BM * RB + NT * RB);
     constexpr int STAGES = (kSmemBudget / STAGE) > 4 ? 4 : (kSmemBudget / STAGE);
     constexpr int SMEM = STAGES * STAGE + 1024 + 256;
-    static bool attr = false;
-    if (!attr) {
+    static const bool attr = [] {   // thread-safe one-time setup
         PTB_CUDA(cudaFuncSetAttribute(k_oz_product_ta<EPI, S, RB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       SMEM));
-        attr = true;
-    }
+        return true;
+    }();
+    (void)attr;
     k_oz_product_ta<EPI, S, RB, NT><<<ntiles, THREADS, SMEM, s>>>(maps, tiles, a.exps, b.exps, ep);
     count_launch();
 }

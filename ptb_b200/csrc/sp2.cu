@@ -46,6 +46,11 @@ namespace ptb {
 namespace {
 
 constexpr int kMaxIt = 255;
+// Contraction of the refinement rounds per unit response gain g of the first
+// round (measured bounds, see sp2_mixed): the first round leaves at most
+// kRho1 * g of its correction, every later one at most kRho2 * g of its own.
+constexpr double kRho1 = 6.5e-5;
+constexpr double kRho2 = 2.6e-4;
 
 struct SP2State {
     int active;      // 1 while pass 1 runs; product/decision launches are no-ops at 0
@@ -117,7 +122,7 @@ __global__ void k_x0_init(int64_t n, int64_t ldp, const double* __restrict__ A, 
 
 // Reduce the partials of iterate k in a fixed order and decide the next step.
 __global__ void k_decide(SP2State* st, const double* __restrict__ stats, int nparts, double N, double tol_abs,
-                         double e_switch, int maxit) {
+                         double e_asym, double e_stag, int maxit) {
     if (!st->active) return;
     __shared__ double sh[2][256];
     double a = 0.0, b = 0.0;
@@ -151,7 +156,18 @@ __global__ void k_decide(SP2State* st, const double* __restrict__ stats, int npa
     st->sq[k] = sq;
     st->sq_cur = sq;
     const double ae = fabs(e);
-    const bool conv = ae < tol_abs || (k >= 2 && ae < e_switch && ae >= fabs(st->err[k - 2]));
+    // Rounding floor: in the asymptotic regime (every eigenvalue within ~0.1 of
+    // 0 or 1, which e < e_asym implies) two exact steps always lower e, so no
+    // decrease over two steps means rounding; above e_asym states near a small
+    // gap can hold e level for a step or two, so there only six steps that all
+    // stay above the best error before them count (for floors above e_asym).
+    bool conv = ae < tol_abs || (k >= 2 && ae < e_asym && ae >= fabs(st->err[k - 2]));
+    if (!conv && k >= 8 && ae < e_stag) {
+        double before = fabs(st->err[0]), window = ae;
+        for (int j = 1; j <= k - 6; ++j) before = fmin(before, fabs(st->err[j]));
+        for (int j = k - 5; j < k; ++j) window = fmin(window, fabs(st->err[j]));
+        conv = window >= before;
+    }
     if (conv) {
         st->converged = 1;
         st->active = 0;
@@ -236,19 +252,31 @@ __global__ void k_add_f32(int64_t count, const float* __restrict__ x, float* __r
         y[k] += x[k];
 }
 
-// Per-block partial traces of an FP32 plane (64 blocks, fixed order).
-__global__ void k_trace_f32(int64_t n, int64_t ldp, const float* __restrict__ x, double* __restrict__ out) {
-    __shared__ double sh[256];
-    double s = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        s += (double)x[i + i * ldp];
-    sh[threadIdx.x] = s;
+// Per-block partials of the trace and of max |x_ij| over the leading n x n
+// block of a row-major FP32 ldp x ldp matrix: out[2b] = trace, out[2b+1] = max.
+__global__ void k_trace_maxabs_f32(int64_t n, int64_t ldp, const float* __restrict__ x, double* __restrict__ out) {
+    __shared__ double st[256], sm[256];
+    double t = 0.0;
+    float m = 0.0f;
+    for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const float* row = x + i * ldp;
+        for (int64_t j = threadIdx.x; j < n; j += blockDim.x) m = fmaxf(m, fabsf(row[j]));
+        if (threadIdx.x == 0) t += (double)row[i];
+    }
+    st[threadIdx.x] = t;
+    sm[threadIdx.x] = (double)m;
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        if ((int)threadIdx.x < w) {
+            st[threadIdx.x] += st[threadIdx.x + w];
+            sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        }
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+    if (threadIdx.x == 0) {
+        out[2 * blockIdx.x] = st[0];
+        out[2 * blockIdx.x + 1] = sm[0];
+    }
 }
 
 // C = W - W^T (column-major FP64), 32x32 tiles.  blockDim = (32, 8).
@@ -515,7 +543,9 @@ StepInfo fp64_step(ptbgpu_ctx* c, int64_t n, double N, double*& X, double*& W) {
     return s;
 }
 
-void sp2_fp64(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int maxit, double* dPpk,
+// FP64 trace-correcting purification of A (B_H, overwritten); the back-transform
+// uses L from the cuBLAS prologue (S == 0) or L^-1 from the int8 one (S slices).
+void sp2_fp64(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int maxit, int S, double* dPpk,
               ptbgpu_stats* st, int prl) {
     double* X = c->buf(B_H).as<double>();
     DevBuf& bw = c->buf(B_W0);
@@ -539,7 +569,8 @@ void sp2_fp64(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int ma
     }
     PTB_CHECK(done, PTBGPU_EITER, "trace-correcting purification did not converge in %d iterations", maxit);
     phase("SP2 iterations (FP64 syrk)");
-    back_transform(c, n, X, dPpk);
+    if (S > 0) back_transform_oz(c, n, X, W, dPpk, S);
+    else back_transform(c, n, X, dPpk);
     phase("back-transform and pack");
     if (st) {
         st->iterations = it;
@@ -547,8 +578,9 @@ void sp2_fp64(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int ma
     }
 }
 
-void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int maxit, bool refine,
-               int64_t split3_iters, int S, double* dPpk, ptbgpu_stats* st, int prl) {
+bool sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int maxit, bool refine,
+               int refine_rounds, double refine_tol, int64_t split3_iters, int S, double* dPpk, ptbgpu_stats* st,
+               int prl) {
     cudaStream_t s = c->stream;
     const int64_t ldp = round_up(n, tc::tile_n());
     const size_t plane = sizeof(__nv_bfloat16) * (size_t)ldp * ldp;
@@ -606,14 +638,14 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     const double N = 0.5 * (double)nel;
     // pass 1 runs to its rounding floor: the two-step non-decrease rule ends it
     const double tol_abs = 1e-12 * (double)n;
-    const double e_switch = 1.0;
+    const double e_asym = 0.1, e_stag = 0.01 * (double)n;
     k_x0_init<<<x0_blocks, 256, 0, s>>>(n, ldp, A, pro.emax, scale, xf[0], traj(0, 0), traj(0, 1), traj(0, 2),
                                         stats);
     count_launch();
     PTB_CUDA(cudaGetLastError());
     const int cap = std::min(maxit, slots - 1);
     const int n6 = (int)up3.size(), n3 = (int)up.size();
-    k_decide<<<1, 256, 0, s>>>(state, stats, x0_blocks, N, tol_abs, e_switch, cap);
+    k_decide<<<1, 256, 0, s>>>(state, stats, x0_blocks, N, tol_abs, e_asym, e_stag, cap);
     count_launch();
     PTB_CUDA(cudaGetLastError());
 
@@ -641,7 +673,7 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         const int ntl = three ? timed_product(c, tc::EPI_SP2, 3, ldp, pl, pl, split6, tiles_up3, n6, ep)
                               : timed_product(c, tc::EPI_SP2, 2, ldp, pl, pl, split3, tiles_up, n3, ep, 0, pairs_up,
                                               npup);
-        k_decide<<<1, 256, 0, s>>>(state, stats, ntl, N, tol_abs, e_switch, cap);
+        k_decide<<<1, 256, 0, s>>>(state, stats, ntl, N, tol_abs, e_asym, e_stag, cap);
         count_launch();
         PTB_CUDA(cudaGetLastError());
         ++launched;
@@ -683,65 +715,87 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     k_f2d<<<grid1(n), 256, 0, s>>>(n, ldp, xf[K & 1], 1.0, 0.0, X);
     count_launch();
     PTB_CUDA(cudaGetLastError());
-    std::vector<double> hist;
-    int nclean = 0;
-    if (S > 0) {
-        // int8-sliced squares, X updated in place (the epilogue reads X(r,c), c >= r,
-        // before writing it; the mirrored lower triangle is never read); the error
-        // of each iterate is checked before its square is taken
-        const oz::Operand opX = oz_operand(c, 1, n, S);
-        DevBuf& bst = c->buf(B_OZS);
-        // per-tile partials: at most (rows / 128) x ceil(cols / 48) tiles for either kernel variant
-        bst.reserve(sizeof(double) * 2 * (size_t)(oz::padded(n) / oz::BM) * (size_t)((oz::padded(n) + 47) / 48));
-        std::vector<double> hst;
-        double trX = trace_dev(c, n, n, X);
-        const double f0 = frob_dev(c, n, n, X);
-        double trX2 = f0 * f0;
-        for (;;) {
-            const double err = trX - trX2, e = std::fabs(err);
-            PTB_CHECK(std::isfinite(err), PTBGPU_ENAN, "NaN during purification");
-            hist.push_back(e);
-            log_line(prl, 2, " SP2 (int8 FP64 cleanup) %d  err %.3e", nclean, err);
-            if (e < 1e-13 * (double)n || (hist.size() > 2 && e >= hist[hist.size() - 3]) || nclean >= 8) break;
-            const bool sq = std::fabs(trX2 - N) <= std::fabs(2.0 * trX - trX2 - N);
-            oz_slice(c, X, 1, n, n, oz::TRI_NONE, opX);
-            oz::OzEpi es;
-            es.n = n;
-            es.out = X;
-            es.ors = n;
-            es.xin = X;
-            es.square = sq ? 1 : 0;
-            es.stats = bst.as<double>();
-            const int nt = oz_product(c, oz::OZ_SYM, opX, opX, true, oz::TRI_NONE, oz::TRI_NONE, es);
-            hst.resize(2 * (size_t)nt);
-            PTB_CUDA(cudaMemcpyAsync(hst.data(), es.stats, sizeof(double) * hst.size(), cudaMemcpyDeviceToHost, s));
-            check_timeout(c, "int8 product (cleanup)");
-            trX = 0.0;
-            trX2 = 0.0;
-            for (int t = 0; t < nt; ++t) {
-                trX += hst[2 * t];
-                trX2 += hst[2 * t + 1];
+    // SP2 steps in FP64 precision until the idempotency error reaches FP64
+    // rounding or stops falling over two steps (at most 8); returns the steps
+    auto cleanup = [&]() -> int {
+        std::vector<double> hist;
+        int nclean = 0;
+        if (S > 0) {
+            // int8-sliced squares, X updated in place (the epilogue reads X(r,c), c >= r,
+            // before writing it; the mirrored lower triangle is never read); the error
+            // of each iterate is checked before its square is taken
+            const oz::Operand opX = oz_operand(c, 1, n, S);
+            DevBuf& bst = c->buf(B_OZS);
+            // per-tile partials: at most (rows / 128) x ceil(cols / 48) tiles for either kernel variant
+            bst.reserve(sizeof(double) * 2 * (size_t)(oz::padded(n) / oz::BM) * (size_t)((oz::padded(n) + 47) / 48));
+            std::vector<double> hst;
+            double trX = trace_dev(c, n, n, X);
+            const double f0 = frob_dev(c, n, n, X);
+            double trX2 = f0 * f0;
+            for (;;) {
+                const double err = trX - trX2, e = std::fabs(err);
+                PTB_CHECK(std::isfinite(err), PTBGPU_ENAN, "NaN during purification");
+                hist.push_back(e);
+                log_line(prl, 2, " SP2 (int8 FP64 cleanup) %d  err %.3e", nclean, err);
+                if (e < 1e-13 * (double)n || (hist.size() > 2 && e >= hist[hist.size() - 3]) || nclean >= 8) break;
+                const bool sq = std::fabs(trX2 - N) <= std::fabs(2.0 * trX - trX2 - N);
+                oz_slice(c, X, 1, n, n, oz::TRI_NONE, opX);
+                oz::OzEpi es;
+                es.n = n;
+                es.out = X;
+                es.ors = n;
+                es.xin = X;
+                es.square = sq ? 1 : 0;
+                es.stats = bst.as<double>();
+                const int nt = oz_product(c, oz::OZ_SYM, opX, opX, true, oz::TRI_NONE, oz::TRI_NONE, es);
+                hst.resize(2 * (size_t)nt);
+                PTB_CUDA(cudaMemcpyAsync(hst.data(), es.stats, sizeof(double) * hst.size(), cudaMemcpyDeviceToHost, s));
+                check_timeout(c, "int8 product (cleanup)");
+                trX = 0.0;
+                trX2 = 0.0;
+                for (int t = 0; t < nt; ++t) {
+                    trX += hst[2 * t];
+                    trX2 += hst[2 * t + 1];
+                }
+                ++nclean;
             }
-            ++nclean;
+        } else {
+            for (nclean = 1; nclean <= 8; ++nclean) {
+                StepInfo si = fp64_step(c, n, N, X, W);
+                const double e = std::fabs(si.err);
+                hist.push_back(e);
+                log_line(prl, 2, " SP2 (fp64 cleanup) %d  err %.3e", nclean, si.err);
+                // until the error reaches FP64 rounding or stops falling over two steps: a
+                // single SP2 step squares the deviation on one side of the spectrum but
+                // doubles it on the other, so a small error on entry is not enough
+                if (e < 1e-13 * (double)n || (hist.size() > 2 && e >= hist[hist.size() - 3])) break;
+            }
+            nclean = std::min(nclean, 8);
         }
-    } else {
-        for (nclean = 1; nclean <= 8; ++nclean) {
-            StepInfo si = fp64_step(c, n, N, X, W);
-            const double e = std::fabs(si.err);
-            hist.push_back(e);
-            log_line(prl, 2, " SP2 (fp64 cleanup) %d  err %.3e", nclean, si.err);
-            // until the error reaches FP64 rounding or stops falling over two steps: a
-            // single SP2 step squares the deviation on one side of the spectrum but
-            // doubles it on the other, so a small error on entry is not enough
-            if (e < 1e-13 * (double)n || (hist.size() > 2 && e >= hist[hist.size() - 3])) break;
-        }
-        nclean = std::min(nclean, 8);
-    }
+        return nclean;
+    };
+    int nclean = cleanup();
     phase(S > 0 ? "cleanup (int8 FP64 squares)" : "cleanup (FP64 syrk)");
     // algorithmic: every SP2 step is one symmetric square (n^3), pass 1 and cleanup alike
     double flops = (double)K * (double)n * n * n + (double)nclean * (double)n * n * n;
 
-    if (refine) {
+    // Refinement rounds: each one is a Newton step on the occupied subspace (the
+    // first-order response to the part of A that couples the occupied and
+    // virtual spaces of P~); the error left is second order in the correction.
+    // The replay linearises along the bf16x3 pass-1 trajectory, which is exact
+    // for a Hamiltonian a rounding away from A; near the gap that relative error
+    // grows like range / gap, so the rounds contract the error linearly with a
+    // factor that grows with the first round's response gain g1 = max|X1| /
+    // max|X1_0|.  Measured on water clusters, an alkane chain and cubic-lattice
+    // systems (range/gap 25 to 1e4): the next correction stays below kRho1 * g1
+    // of the first one and below max(kRho2 * g1, last ratio) of a later one.
+    // Another round, after an FP64 cleanup of the corrected X, runs while that
+    // predicted error exceeds refine_tol, up to refine_rounds.  If the rounds
+    // cannot get there (contraction above 1/2, or the cap reached with the
+    // prediction above 10 refine_tol) the caller redoes the purification in FP64.
+    int rounds = 0;
+    double g1 = 0.0, prev_x1max = 0.0, resid = 0.0, rho = 0.0;
+    while (refine) {
         // C = A P~ - P~ A (FP64)
         DevBuf& bw2 = c->buf(B_W2);
         bw2.reserve(sizeof(double) * n * n);
@@ -801,6 +855,13 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         const unsigned nbp = (unsigned)(ldp / 32);
         k_sym_update<<<dim3(nbp, nbp), dim3(32, 8), 0, s>>>(ldp, wf, nullptr, (float)scale, 0.0f, x1f[0], x1hi[0],
                                                             x1lo[0]);
+        count_launch();
+        PTB_CUDA(cudaGetLastError());
+        // max |X1_0| (second half of the partials buffer, read with the final ones)
+        constexpr int kParts = 296;
+        DevBuf& btau = c->buf(B_MISC2);
+        btau.reserve(sizeof(double) * 4 * kParts);
+        k_trace_maxabs_f32<<<kParts, 256, 0, s>>>(n, ldp, x1f[0], btau.as<double>() + 2 * kParts);
         count_launch();
         PTB_CUDA(cudaGetLastError());
         phase("commutator, planes, A1 product");
@@ -865,16 +926,18 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         // response is traceless; its bf16x3 rounding noise is removed from the
         // trace in FP64 along P~ (a uniform shift of the occupied eigenvalues by
         // tau/N), so tr P_o = N to FP64 rounding.
-        DevBuf& btau = c->buf(B_MISC2);
-        btau.reserve(sizeof(double) * 64);
-        k_trace_f32<<<64, 256, 0, s>>>(n, ldp, x1f[K & 1], btau.as<double>());
+        k_trace_maxabs_f32<<<kParts, 256, 0, s>>>(n, ldp, x1f[K & 1], btau.as<double>());
         count_launch();
         PTB_CUDA(cudaGetLastError());
-        double tparts[64];
+        double tparts[4 * kParts];
         PTB_CUDA(cudaMemcpyAsync(tparts, btau.ptr, sizeof(tparts), cudaMemcpyDeviceToHost, s));
         PTB_CUDA(cudaStreamSynchronize(s));
-        double tau = 0.0;
-        for (double v : tparts) tau += v;
+        double tau = 0.0, x1max = 0.0, x10max = 0.0;
+        for (int p = 0; p < kParts; ++p) {
+            tau += tparts[2 * p];
+            x1max = std::max(x1max, tparts[2 * p + 1]);
+            x10max = std::max(x10max, tparts[2 * kParts + 2 * p + 1]);
+        }
         k_f2d<<<grid1(n), 256, 0, s>>>(n, ldp, x1f[K & 1], 1.0, 1.0 - tau / N, X);
         count_launch();
         PTB_CUDA(cudaGetLastError());
@@ -884,15 +947,44 @@ void sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         PTB_CUDA(cudaMemcpyAsync(&tmo, &c->flags->timeout, sizeof(int), cudaMemcpyDeviceToHost, s));
         PTB_CUDA(cudaStreamSynchronize(s));
         PTB_CHECK(tmo == 0, PTBGPU_ETIMEOUT, "tensor-core product gave up waiting (site %d)", tmo);
+        ++rounds;
+        // error left after this round, predicted from the size of its correction
+        const double gain = x10max > 0.0 ? x1max / x10max : 0.0;
+        if (rounds == 1) {
+            g1 = gain;
+            rho = x10max > 0.0 ? std::min(1.0, kRho1 * g1) : 1.0;
+        } else {
+            rho = std::min(1.0, std::max(kRho2 * g1, prev_x1max > 0.0 ? x1max / prev_x1max : 1.0));
+        }
+        prev_x1max = x1max;
+        resid = x1max * rho;
+        log_line(prl, 2, " refinement round %d  max|X1| %.3e  max|X1_0| %.3e  gain %.3e  predicted %.3e  tau %.3e",
+                 rounds, x1max, x10max, gain, resid, tau);
+        if (!(resid > refine_tol)) break;
+        if (rounds >= refine_rounds || std::min(1.0, kRho2 * g1) > 0.5) {
+            if (resid > 10.0 * refine_tol) {
+                log_line(prl, 1, " refinement cannot reach %.1e (predicted %.2e after %d rounds): FP64 purification",
+                         refine_tol, resid, rounds);
+                if (st) st->refine_rounds = rounds;
+                return false;
+            }
+            break;
+        }
+        const int more = cleanup();
+        nclean += more;
+        flops += (double)more * (double)n * n * n;
+        phase(S > 0 ? "cleanup (int8 FP64 squares)" : "cleanup (FP64 syrk)");
     }
     if (S > 0) back_transform_oz(c, n, X, W, dPpk, S);   // sets tr(PS) directly: full slice count
     else back_transform(c, n, X, dPpk);
     phase("back-transform and pack");
     if (st) {
         st->iterations = K + nclean;
-        st->tc_flops += tc_exec + (refine ? (double)(K + 5) * tc_exec_full : 0.0);
+        st->refine_rounds = rounds;
+        st->tc_flops += tc_exec + (double)rounds * (double)(K + 5) * tc_exec_full;
         st->flops += flops;
     }
+    return true;
 }
 
 void tc_purify_device(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, const double* dS, double* dP,
@@ -909,6 +1001,10 @@ void tc_purify_device(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, c
     const int S = (o->precision != PTBGPU_PREC_FP64 && o->fp64_slices != 0) ? (int)o->fp64_slices : 0;
     PTB_CHECK(S == 0 || (S >= 6 && S <= 8), PTBGPU_EINVAL, "fp64_slices must be 0 or 6..8 (got %d)", S);
     const int Suse = (S > 0 && oz::supported(n, S)) ? S : 0;
+    PTB_CHECK(o->refine_rounds >= 0 && o->refine_rounds <= 16 && o->refine_tol >= 0.0, PTBGPU_EINVAL,
+              "refine_rounds must be 0..16 and refine_tol >= 0");
+    const int rounds = o->refine_rounds > 0 ? (int)o->refine_rounds : 4;
+    const double rtol = o->refine_tol > 0.0 ? o->refine_tol : 1e-7;
     PhaseLog plog;
     plog.c = c;
     struct Scope {
@@ -921,10 +1017,14 @@ void tc_purify_device(ptbgpu_ctx* c, int64_t n, int64_t nel, const double* dH, c
                             : orthogonalise(c, n, dH, dS, o->filter);
     phase("Gershgorin bounds");
     if (st) st->flops += (1.0 / 3.0 + 4.0) * (double)n * n * n;   // potrf + 4 trsm
-    if (o->precision == PTBGPU_PREC_FP64)
-        sp2_fp64(c, n, nel, pro, maxit, dP, st, prl);
-    else
-        sp2_mixed(c, n, nel, pro, maxit, o->precision != 2, o->split3_iters, Suse, dP, st, prl);
+    if (o->precision == PTBGPU_PREC_FP64) {
+        sp2_fp64(c, n, nel, pro, maxit, 0, dP, st, prl);
+    } else if (!sp2_mixed(c, n, nel, pro, maxit, o->precision != 2, rounds, rtol, o->split3_iters, Suse, dP, st,
+                          prl)) {
+        // A (B_H) is still intact: the mixed path only reads it
+        sp2_fp64(c, n, nel, pro, maxit, Suse, dP, st, prl);
+        if (st) st->fp64_fallback = 1;
+    }
     if (prl >= 2) plog.report(prl);
 }
 

@@ -742,12 +742,12 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
         ws.release();
         tbuf.release();
     };
-    static bool fe_attr = false;
-    if (!fe_attr) {
+    static const bool fe_attr = [] {   // thread-safe one-time setup
         PTB_CUDA(cudaFuncSetAttribute(k_fe, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         PTB_CUDA(cudaFuncSetAttribute(k_final, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        fe_attr = true;
-    }
+        return true;
+    }();
+    (void)fe_attr;
     const double one = 1.0, zero = 0.0;
     try {
         size_t bi = 0;

@@ -526,12 +526,12 @@ template <int EPI, int BN, int NP, int KB>
 void launch_t(cudaStream_t s, const TmaPlanes& maps, const ProdList& prods, const int2* tiles, int ntiles, int nk,
               const EpiParams& ep) {
     using C = Cfg<BN, NP, KB>;
-    static bool attr = false;
-    if (!attr) {
+    static const bool attr = [] {   // thread-safe one-time setup
         PTB_CUDA(cudaFuncSetAttribute(k_tc_product<EPI, BN, NP, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       C::SMEM_BYTES));
-        attr = true;
-    }
+        return true;
+    }();
+    (void)attr;
     k_tc_product<EPI, BN, NP, KB><<<ntiles, THREADS, C::SMEM_BYTES, s>>>(maps, prods, tiles, nk, ep);
     count_launch();
 }
@@ -540,12 +540,12 @@ template <int EPI, int KB>
 void launch_pair(cudaStream_t s, const TmaPlanes& maps, const ProdList& prods, const int2* pairs, int npairs, int nk,
                  const EpiParams& ep) {
     using C = CfgPair<2, KB>;
-    static bool attr = false;
-    if (!attr) {
+    static const bool attr = [] {   // thread-safe one-time setup
         PTB_CUDA(cudaFuncSetAttribute(k_tc_product_pair<EPI, 2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       C::SMEM_BYTES));
-        attr = true;
-    }
+        return true;
+    }();
+    (void)attr;
     k_tc_product_pair<EPI, 2, KB><<<2 * npairs, THREADS, C::SMEM_BYTES, s>>>(maps, prods, pairs, nk, ep);
     count_launch();
 }
