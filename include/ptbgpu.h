@@ -301,6 +301,28 @@ int ptbgpu_symsq_split(ptbgpu_ctx* ctx, int64_t n, int64_t planes, int64_t kbloc
 int ptbgpu_oz_gemm(ptbgpu_ctx* ctx, int64_t n, int64_t slices, int64_t kblock, int64_t variant, int64_t tri_a,
                    int64_t tri_b, int64_t symmetric, const double* A, const double* B, double* C, double* ms);
 
+/* ---- consumer of P in the next SCF iteration ---------------------------- */
+/* The iteration-2 XC long-range damping of twoscf (source/pgtb.f90:482-513) on
+ * the packed arrays: xab(lin(a,b)) = (1 + erf(-1.8 (rab - r)/r))/2 with
+ * r = rad(a) + rad(b) over atom pairs, then Hpk(k) += Ppk(k) (hao(i) + hao(j))
+ * xab(lin(aoat(j), aoat(i))) for j < i and Hpk(k) += 2 Ppk(k) xdiag(i) hao(i)
+ * xab(lin(aoat(i), aoat(i))) on the diagonal.  rad(nat) is the special radius
+ * shell_cnf3(10,at) + (cn - avcn(at)) shell_resp(10,at,1); hao(ndim) is
+ * shell_cnf2(shell2ao(i), at(aoat(i))) * gq(aoat(i)); xdiag(ndim) is
+ * shell_xi(8, at(aoat(i))); rab is the packed atom-pair distance array
+ * (nat(nat+1)/2).  aoat(i) outside 1..nat -> PTBGPU_EINVAL.  ms_update (may be
+ * NULL) gets the device time of the AO-pair update. */
+int ptbgpu_xc_damping(ptbgpu_ctx* ctx, int64_t nat, int64_t ndim, const int64_t* aoat, const double* rab,
+                      const double* rad, const double* hao, const double* xdiag, const double* Ppk, double* Hpk,
+                      double* ms_update);
+/* The same with Ppk and Hpk device-resident (e.g. P left on the device by
+ * ptbgpu_tc_purify_device, H to be passed on to the next density step);
+ * aoat, rab, rad, hao, xdiag are host arrays.  dPpk and dHpk must start on a
+ * 16-byte boundary (PTBGPU_EINVAL otherwise). */
+int ptbgpu_xc_damping_device(ptbgpu_ctx* ctx, int64_t nat, int64_t ndim, const int64_t* aoat, const double* rab,
+                             const double* rad, const double* hao, const double* xdiag, const double* dPpk,
+                             double* dHpk, double* ms_update);
+
 #ifdef __cplusplus
 }
 #endif

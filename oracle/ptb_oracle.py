@@ -822,3 +822,70 @@ def kmeans_partition(ndim: int, H: np.ndarray, S: np.ndarray, nat: int, xyz: np.
             best = (e, k, z)
     e, k, z = best
     return z + 1, k, e
+
+
+# ---------------------------------------------------------------------------
+# Iteration-2 XC long-range damping, the consumer of P in the next SCF
+# iteration (source/pgtb.f90:482-513)
+# ---------------------------------------------------------------------------
+def xc_damping_loops(nat: int, ndim: int, aoat, rab, rad, hao, xdiag, Pvec, Hvec) -> np.ndarray:
+    """The reference's two loops verbatim in Python (small cases only): xab over
+    atom pairs (source/pgtb.f90:485-495), then the AO-pair update (:496-513).
+    rad(a) stands for hi = shell_cnf3(10,at) + (cn - avcn) shell_resp(10,at,1),
+    hao(i) for shell_cnf2(ish,ati) gq(ia), xdiag(i) for shell_xi(8,ati)."""
+    xab = np.zeros(nat * (nat + 1) // 2)
+    k = 0
+    for i in range(nat):
+        for j in range(i + 1):
+            r = rad[i] + rad[j]
+            t8 = (rab[k] - r) / r
+            xab[k] = 0.5 * (1.0 + math.erf(-1.8 * t8))
+            k += 1
+    H = np.array(Hvec, dtype=np.float64, copy=True)
+    k = 0
+    for i in range(ndim):
+        ia = int(aoat[i])
+        hi = hao[i]
+        for j in range(i):
+            ib = int(aoat[j])
+            hj = hao[j]
+            H[k] = H[k] + Pvec[k] * (hi + hj) * xab[lin(ib, ia) - 1]
+            k += 1
+        H[k] = H[k] + 2.0 * Pvec[k] * xdiag[i] * hi * xab[lin(ia, ia) - 1]
+        k += 1
+    return H
+
+
+def xc_damping(nat: int, ndim: int, aoat, rab, rad, hao, xdiag, Pvec, Hvec) -> np.ndarray:
+    """Vectorised form of xc_damping_loops (same operations, same order)."""
+    from scipy.special import erf
+    rad = np.asarray(rad, dtype=np.float64)
+    ca, rb = _packed_cols_rows(nat)
+    r = rad[ca] + rad[rb]
+    t8 = (np.asarray(rab, dtype=np.float64) - r) / r
+    xab = 0.5 * (1.0 + erf(-1.8 * t8))
+    ci, rj = _packed_cols_rows(ndim)
+    a = np.asarray(aoat, dtype=np.int64) - 1
+    ia, ib = a[ci], a[rj]
+    hi, lo = np.maximum(ia, ib), np.minimum(ia, ib)
+    x = xab[hi * (hi + 1) // 2 + lo]
+    hao = np.asarray(hao, dtype=np.float64)
+    xdiag = np.asarray(xdiag, dtype=np.float64)
+    P = np.asarray(Pvec, dtype=np.float64)
+    off = P * (hao[ci] + hao[rj]) * x
+    dia = 2.0 * P * xdiag[ci] * hao[ci] * x
+    return np.asarray(Hvec, dtype=np.float64) + np.where(rj < ci, off, dia)
+
+
+def _packed_cols_rows(n: int):
+    """0-based (column, row) of every packed element in storage order."""
+    cols = np.repeat(np.arange(n, dtype=np.int64), np.arange(1, n + 1))
+    starts = cols * (cols + 1) // 2
+    rows = np.arange(n * (n + 1) // 2, dtype=np.int64) - starts
+    return cols, rows
+
+
+def lin(i1: int, i2: int) -> int:
+    """1-based packed address of (i1, i2), source/lin.f:5-11."""
+    a, b = max(i1, i2), min(i1, i2)
+    return b + a * (a - 1) // 2

@@ -71,7 +71,8 @@ EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_defau
             "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_symsq_split", "ptbgpu_runtime_info",
             "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm", "ptbgpu_mlpop14", "ptbgpu_mlpop14_device",
             "ptbgpu_mlpop2", "ptbgpu_mlpop2_device", "ptbgpu_kmeans_partition", "ptbgpu_sm_plan",
-            "ptbgpu_sm_prepare", "ptbgpu_sm_nel", "ptbgpu_sm_finish")
+            "ptbgpu_sm_prepare", "ptbgpu_sm_nel", "ptbgpu_sm_finish", "ptbgpu_xc_damping",
+            "ptbgpu_xc_damping_device")
 
 
 def library_path() -> Path:
@@ -113,6 +114,8 @@ def load_library():
     lib.ptbgpu_tc_purify_batch.argtypes = [C.c_void_p, i64, P(i64), P(i64), P(d), P(d), P(d), i64, P(_Opts),
                                            P(_Stats), d]
     lib.ptbgpu_solve2.argtypes = [C.c_void_p, i64, i64, i64, i64, d, d, d, d, d, P(_Opts), P(_Stats)]
+    lib.ptbgpu_xc_damping.argtypes = [C.c_void_p, i64, i64, P(i64), d, d, d, d, d, d, d]
+    lib.ptbgpu_xc_damping_device.argtypes = [C.c_void_p, i64, i64, P(i64), d, d, d, d, C.c_void_p, C.c_void_p, d]
     lib.ptbgpu_symsq_bf16x3.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_bf16x6.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_split.argtypes = [C.c_void_p, i64, i64, i64, d, P(C.c_float), d]
@@ -388,6 +391,29 @@ class Context:
         self._check(self._lib.ptbgpu_tc_purify_batch(self._h, n, ndim, nel, arr(Hs), arr(Ss), arr(Ps),
                                                      int(workers), C.byref(o), st, C.byref(wall)))
         return Ps, [Stats.from_c(st[i]) for i in range(n)], wall.value
+
+    def xc_damping(self, nat: int, ndim: int, aoat, rab, rad, hao, xdiag, P: np.ndarray, H: np.ndarray,
+                   timed: bool = False):
+        """Iteration-2 XC long-range damping, source/pgtb.f90:482-513: returns H + the
+        P-dependent term (packed); timed: (H, device ms of the AO-pair update)."""
+        a = np.ascontiguousarray(aoat, dtype=np.int64)
+        Hout = _f64(H).copy()
+        ms = C.c_double(0.0)
+        self._check(self._lib.ptbgpu_xc_damping(self._h, int(nat), int(ndim), a.ctypes.data_as(C.POINTER(C.c_int64)),
+                                                _dptr(_f64(rab)), _dptr(_f64(rad)), _dptr(_f64(hao)),
+                                                _dptr(_f64(xdiag)), _dptr(_f64(P)), _dptr(Hout), C.byref(ms)))
+        return (Hout, ms.value) if timed else Hout
+
+    def xc_damping_device(self, nat: int, ndim: int, aoat, rab, rad, hao, xdiag, dP: int, dH: int) -> float:
+        """Same on device-resident packed P and H (raw device pointers, H updated in
+        place); returns the device ms of the AO-pair update."""
+        a = np.ascontiguousarray(aoat, dtype=np.int64)
+        ms = C.c_double(0.0)
+        self._check(self._lib.ptbgpu_xc_damping_device(self._h, int(nat), int(ndim),
+                                                       a.ctypes.data_as(C.POINTER(C.c_int64)), _dptr(_f64(rab)),
+                                                       _dptr(_f64(rad)), _dptr(_f64(hao)), _dptr(_f64(xdiag)),
+                                                       C.c_void_p(dP), C.c_void_p(dH), C.byref(ms)))
+        return ms.value
 
     def solve2(self, mode: int, ndim: int, nel: int, nopen: int, H: np.ndarray, S: np.ndarray,
                opts: Options | None = None):

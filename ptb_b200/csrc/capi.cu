@@ -27,6 +27,8 @@ double sm_nel_entry(ptbgpu_ctx* c, double mu);
 void sm_finish_entry(ptbgpu_ctx* c, double mu, double* dP);
 void mlpop14_device(ptbgpu_ctx* c, int64_t n, const double* dSpk, double x, float* s34, float* s14);
 void mlpop2_diag_device(ptbgpu_ctx* c, int64_t n, const double* dPpk, const float* s1, const float* s2, double* xd);
+float xc_damping_device(ptbgpu_ctx* c, int64_t nat, int64_t ndim, const int64_t* aoat, const double* rab,
+                        const double* rad, const double* hao, const double* xdiag, const double* dP, double* dH);
 void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int variant, int tri_a, int tri_b, bool sym,
                    const double* hA,
                    const double* hB, double* hC);
@@ -469,6 +471,30 @@ int ptbgpu_mlpop2_device(ptbgpu_ctx* c, int64_t n, int64_t nao, const double* dP
         t.mark(2);
         t.finish(st);
         accumulate_pops(n, nao, xd.data(), aoat, shell2ao, q, qsh);
+    });
+}
+
+int ptbgpu_xc_damping(ptbgpu_ctx* c, int64_t nat, int64_t ndim, const int64_t* aoat, const double* rab,
+                      const double* rad, const double* hao, const double* xdiag, const double* Ppk, double* Hpk,
+                      double* ms_update) {
+    return guarded(c, [&] {
+        PTB_CHECK(nat > 0 && ndim > 0 && Ppk && Hpk, PTBGPU_EINVAL, "bad arguments");
+        PackedIO io(c, ndim);
+        io.in(0, Ppk);
+        io.in(1, Hpk);
+        const float ms = xc_damping_device(c, nat, ndim, aoat, rab, rad, hao, xdiag, io.d[0], io.d[1]);
+        io.out(1, Hpk);
+        PTB_CUDA(cudaStreamSynchronize(c->stream));
+        if (ms_update) *ms_update = ms;
+    });
+}
+
+int ptbgpu_xc_damping_device(ptbgpu_ctx* c, int64_t nat, int64_t ndim, const int64_t* aoat, const double* rab,
+                             const double* rad, const double* hao, const double* xdiag, const double* dPpk,
+                             double* dHpk, double* ms_update) {
+    return guarded(c, [&] {
+        const float ms = xc_damping_device(c, nat, ndim, aoat, rab, rad, hao, xdiag, dPpk, dHpk);
+        if (ms_update) *ms_update = ms;
     });
 }
 

@@ -223,3 +223,40 @@ def test_mlpop_populations_sum_to_trace_ps():
     s34, s14 = O.mlpop14(n, s.Svec)
     q, _ = O.mlpop2(s.nat, n, O.packsym(P), s34, s14, s.aoat, synth.shell2ao(s.aoat), dtype=np.float64)
     assert abs(q.sum() - s.nel) < 1e-3
+
+
+def test_xc_damping_vectorised_matches_loops():
+    """The vectorised XC damping oracle equals the reference's loops
+    (source/pgtb.f90:485-513) up to erf's last bit."""
+    rng = np.random.default_rng(3)
+    nat, ndim = 7, 30
+    aoat = np.sort(np.concatenate([np.arange(1, nat + 1), rng.integers(1, nat + 1, ndim - nat)]))
+    rab = rng.uniform(0.5, 8.0, nat * (nat + 1) // 2)
+    rad = rng.uniform(1.0, 3.0, nat)
+    hao, xd = rng.normal(size=ndim), rng.normal(size=ndim)
+    P = rng.normal(size=ndim * (ndim + 1) // 2)
+    H = rng.normal(size=P.size)
+    a = O.xc_damping_loops(nat, ndim, aoat, rab, rad, hao, xd, P, H)
+    b = O.xc_damping(nat, ndim, aoat, rab, rad, hao, xd, P, H)
+    np.testing.assert_allclose(b, a, rtol=1e-14, atol=1e-15)
+
+
+def test_xc_damping_known_values():
+    """rab equal to the radius sum gives xab = 1/2; P = 0 leaves H unchanged;
+    one AO per atom reduces the update to closed forms."""
+    nat = ndim = 3
+    aoat = np.array([1, 2, 3])
+    rad = np.array([1.0, 2.0, 3.0])
+    ca = [0, 1, 1, 2, 2, 2]
+    rb = [0, 0, 1, 0, 1, 2]
+    rab = np.array([rad[a] + rad[b] for a, b in zip(ca, rb)])
+    hao = np.array([0.5, 1.5, -2.0])
+    xd = np.array([3.0, 4.0, 5.0])
+    P = np.arange(1.0, 7.0)
+    H = np.zeros(6)
+    out = O.xc_damping(nat, ndim, aoat, rab, rad, hao, xd, P, H)
+    want = [2 * P[0] * xd[0] * hao[0] * 0.5, P[1] * (hao[1] + hao[0]) * 0.5, 2 * P[2] * xd[1] * hao[1] * 0.5,
+            P[3] * (hao[2] + hao[0]) * 0.5, P[4] * (hao[2] + hao[1]) * 0.5, 2 * P[5] * xd[2] * hao[2] * 0.5]
+    np.testing.assert_allclose(out, want, rtol=1e-15)
+    assert np.array_equal(O.xc_damping(nat, ndim, aoat, rab, rad, hao, xd, np.zeros(6), P), P)
+    assert O.lin(2, 3) == 5 and O.lin(3, 2) == 5 and O.lin(1, 1) == 1
