@@ -83,7 +83,8 @@ typedef struct {
     double  glob_par15;         /* solve2 orbital-energy shift for mode >= 2      */
     double  glob_par17;
     int64_t split3_iters;       /* PREC_MIXED: leading iterations whose products use the
-                                   three-plane bf16 split (~24 bits); 0 = all, -1 = none */
+                                   three-plane bf16 split (~24 bits); 0 = all, -1 = none
+                                   (the default: the refinement rounds make them unnecessary) */
     int64_t fp64_slices;        /* PREC_MIXED: 6..8 -> the FP64 products around the purification
                                    (orthogonalisation, cleanup, commutator, back-transform) run on
                                    the int8 tensor cores with that many 7-bit slices per operand;
@@ -193,6 +194,20 @@ int ptbgpu_tc_purify_device(ptbgpu_ctx* ctx, int64_t ndim, int64_t nel,
 int ptbgpu_tc_purify_batch(ptbgpu_ctx* ctx, int64_t ninst, const int64_t* ndim, const int64_t* nel,
                            const double* const* Hpk, const double* const* Spk, double* const* Ppk,
                            int64_t workers, const ptbgpu_opts* opts, ptbgpu_stats* st, double* wall_ms);
+
+/* The same systems purified together: bucketed by ndim rounded up to 256 and
+ * padded within a bucket (decoupled padding: unit overlap, orthogonalised
+ * diagonal at the system's upper spectral bound), stacked, and every step run
+ * as one launch over all systems of a bucket (split-bf16 tcgen05 products over
+ * the stacked planes, batched cuBLAS / cuSOLVER for the FP64 steps, per-system
+ * branch and stop decisions on the device).  Results agree with
+ * ptbgpu_tc_purify to the same tolerances (not bit for bit: the padded FP64
+ * steps round differently).  A system the grouped path cannot finish is redone
+ * by ptbgpu_tc_purify in FP64 (stats.fp64_fallback).  Per-system stats carry
+ * iterations, refinement rounds and flops; wall_ms the host time of the call. */
+int ptbgpu_tc_purify_grouped(ptbgpu_ctx* ctx, int64_t ninst, const int64_t* ndim, const int64_t* nel,
+                             const double* const* Hpk, const double* const* Spk, double* const* Ppk,
+                             const ptbgpu_opts* opts, ptbgpu_stats* st, double* wall_ms);
 
 /* solve2(mode,ndim,nel,nopen,homo,et,focc,H,S,P,e,U,fail), source/pgtb.f90:1066-1170:
  * dense generalized eigensolve + Fermi smearing, the check-mode oracle.

@@ -67,7 +67,8 @@ class _Stats(C.Structure):
 
 EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_default_settings",
             "ptbgpu_default_opts", "ptbgpu_filter_packed", "ptbgpu_check_density", "ptbgpu_sm_density",
-            "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_tc_purify_batch", "ptbgpu_solve2",
+            "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_tc_purify_batch", "ptbgpu_tc_purify_grouped",
+            "ptbgpu_solve2",
             "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_symsq_split", "ptbgpu_runtime_info",
             "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm", "ptbgpu_mlpop14", "ptbgpu_mlpop14_device",
             "ptbgpu_mlpop2", "ptbgpu_mlpop2_device", "ptbgpu_kmeans_partition", "ptbgpu_sm_plan",
@@ -113,6 +114,8 @@ def load_library():
                                             P(_Stats)]
     lib.ptbgpu_tc_purify_batch.argtypes = [C.c_void_p, i64, P(i64), P(i64), P(d), P(d), P(d), i64, P(_Opts),
                                            P(_Stats), d]
+    lib.ptbgpu_tc_purify_grouped.argtypes = [C.c_void_p, i64, P(i64), P(i64), P(d), P(d), P(d), P(_Opts),
+                                             P(_Stats), d]
     lib.ptbgpu_solve2.argtypes = [C.c_void_p, i64, i64, i64, i64, d, d, d, d, d, P(_Opts), P(_Stats)]
     lib.ptbgpu_xc_damping.argtypes = [C.c_void_p, i64, i64, P(i64), d, d, d, d, d, d, d]
     lib.ptbgpu_xc_damping_device.argtypes = [C.c_void_p, i64, i64, P(i64), d, d, d, d, C.c_void_p, C.c_void_p, d]
@@ -205,7 +208,7 @@ class Options:
     electronic_temp: float = 300.0
     glob_par15: float = 0.0
     glob_par17: float = 0.0
-    split3_iters: int = 8
+    split3_iters: int = -1
     fp64_slices: int = 8
     refine_rounds: int = 4
     refine_tol: float = 1e-7
@@ -414,6 +417,25 @@ class Context:
                                                        _dptr(_f64(rad)), _dptr(_f64(hao)), _dptr(_f64(xdiag)),
                                                        C.c_void_p(dP), C.c_void_p(dH), C.byref(ms)))
         return ms.value
+
+    def tc_purify_grouped(self, systems, opts: Options | None = None):
+        """tc_purify over many systems grouped into stacked launches per size
+        bucket, `systems` a sequence of (ndim, nel, H, S).  Returns ([Pvec],
+        [Stats], wall milliseconds)."""
+        n = len(systems)
+        m = max(n, 1)
+        ndim = (C.c_int64 * m)(*[int(s[0]) for s in systems])
+        nel = (C.c_int64 * m)(*[int(s[1]) for s in systems])
+        Hs = [_f64(s[2]) for s in systems]
+        Ss = [_f64(s[3]) for s in systems]
+        Ps = [np.zeros(npacked(int(s[0]))) for s in systems]
+        arr = lambda xs: (C.POINTER(C.c_double) * m)(*[_dptr(x) for x in xs])
+        st = (_Stats * m)()
+        wall = C.c_double(0.0)
+        o = (opts or Options()).to_c()
+        self._check(self._lib.ptbgpu_tc_purify_grouped(self._h, n, ndim, nel, arr(Hs), arr(Ss), arr(Ps), C.byref(o),
+                                                       st, C.byref(wall)))
+        return Ps, [Stats.from_c(st[i]) for i in range(n)], wall.value
 
     def solve2(self, mode: int, ndim: int, nel: int, nopen: int, H: np.ndarray, S: np.ndarray,
                opts: Options | None = None):

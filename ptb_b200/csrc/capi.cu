@@ -29,6 +29,9 @@ void mlpop14_device(ptbgpu_ctx* c, int64_t n, const double* dSpk, double x, floa
 void mlpop2_diag_device(ptbgpu_ctx* c, int64_t n, const double* dPpk, const float* s1, const float* s2, double* xd);
 float xc_damping_device(ptbgpu_ctx* c, int64_t nat, int64_t ndim, const int64_t* aoat, const double* rab,
                         const double* rad, const double* hao, const double* xdiag, const double* dP, double* dH);
+void tc_purify_grouped(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const int64_t* nel,
+                       const double* const* Hpk, const double* const* Spk, double* const* Ppk, const ptbgpu_opts* o,
+                       ptbgpu_stats* st, std::vector<int>& redo);
 void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int variant, int tri_a, int tri_b, bool sym,
                    const double* hA,
                    const double* hB, double* hC);
@@ -292,6 +295,36 @@ int ptbgpu_tc_purify_batch(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, co
     if (wall_ms) *wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     const int rc = first_rc.load();
     c->last_error = rc == PTBGPU_OK ? std::string() : err_msg;
+    return rc;
+}
+
+int ptbgpu_tc_purify_grouped(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const int64_t* nel,
+                             const double* const* Hpk, const double* const* Spk, double* const* Ppk,
+                             const ptbgpu_opts* opts, ptbgpu_stats* st, double* wall_ms) {
+    if (!c) return PTBGPU_EINVAL;
+    if (ninst < 0 || (ninst > 0 && (!ndim || !nel || !Hpk || !Spk || !Ppk))) {
+        c->last_error = "bad arguments";
+        return PTBGPU_EINVAL;
+    }
+    ptbgpu_opts def;
+    ptbgpu_default_opts(&def);
+    const ptbgpu_opts* o = opts ? opts : &def;
+    if (st)
+        for (int64_t i = 0; i < ninst; ++i) clear_stats(&st[i]);
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<int> redo;
+    int rc = guarded(c, [&] { tc_purify_grouped(c, ninst, ndim, nel, Hpk, Spk, Ppk, o, st, redo); });
+    // systems the grouped path left (pass 1 not converged, refinement short of its
+    // tolerance, NaN): the single-system path in FP64, the same as its own fallback
+    for (int64_t i = 0; rc == PTBGPU_OK && i < ninst; ++i) {
+        if (!redo[i]) continue;
+        ptbgpu_opts o64 = *o;
+        o64.precision = PTBGPU_PREC_FP64;
+        rc = ptbgpu_tc_purify(c, ndim[i], nel[i], Hpk[i], Spk[i], Ppk[i], &o64, st ? &st[i] : nullptr);
+        if (rc != PTBGPU_OK) c->last_error = "system " + std::to_string(i) + ": " + c->last_error;
+        else if (st && o->precision != PTBGPU_PREC_FP64) st[i].fp64_fallback = 1;
+    }
+    if (wall_ms) *wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
 }
 

@@ -121,6 +121,7 @@ enum BufId {
     B_SM0, B_SM1, B_SM2, B_SM3, B_SM4, B_SM5, B_SM6, B_SM7,
     B_OZ0, B_OZ1, B_OZE0, B_OZE1, B_OZR, B_OZT, B_OZS,  // int8 slices, row exponents, scratch of the
                                                         // emulated FP64 products
+    B_G0, B_G1, B_G2, B_G3, B_G4, B_G5, B_G6, B_G7, B_G8, B_G9, B_G10,   // grouped purification (released after)
     B_COUNT
 };
 

@@ -171,7 +171,7 @@ void ptbgpu_default_opts(ptbgpu_opts* o) {
     o->print_level = 0;
     o->max_iter = 100;
     o->electronic_temp = 300.0;
-    o->split3_iters = 8;
+    o->split3_iters = -1;
     o->fp64_slices = 8;
     o->refine_rounds = 4;
     o->refine_tol = 1e-7;

@@ -39,31 +39,12 @@
 
 #include "common.cuh"
 #include "oz_gemm.cuh"
+#include "sp2_state.cuh"
 #include "tc_gemm.cuh"
 
 namespace ptb {
 
 namespace {
-
-constexpr int kMaxIt = 255;
-// Contraction of the refinement rounds per unit response gain g of the first
-// round (measured bounds, see sp2_mixed): the first round leaves at most
-// kRho1 * g of its correction, every later one at most kRho2 * g of its own.
-constexpr double kRho1 = 6.5e-5;
-constexpr double kRho2 = 2.6e-4;
-
-struct SP2State {
-    int active;      // 1 while pass 1 runs; product/decision launches are no-ops at 0
-    int next;        // index of the iterate the next decision evaluates
-    int converged;
-    int status;      // 0 or a PTBGPU_E* code
-    int sq_cur;      // branch for the step about to run
-    int pad[3];
-    double trX[kMaxIt + 1];
-    double trX2[kMaxIt + 1];
-    double err[kMaxIt + 1];
-    int sq[kMaxIt + 1];
-};
 
 // ---------------------------------------------------------------------------
 // kernels
@@ -141,42 +122,7 @@ __global__ void k_decide(SP2State* st, const double* __restrict__ stats, int npa
         __syncthreads();
     }
     if (threadIdx.x != 0) return;
-    const int k = st->next;
-    const double trX = sh[0][0], trX2 = sh[1][0];
-    const double e = trX - trX2;
-    st->trX[k] = trX;
-    st->trX2[k] = trX2;
-    st->err[k] = e;
-    if (!(e == e)) {
-        st->status = PTBGPU_ENAN;
-        st->active = 0;
-        return;
-    }
-    const int sq = fabs(trX2 - N) <= fabs(2.0 * trX - trX2 - N) ? 1 : 0;
-    st->sq[k] = sq;
-    st->sq_cur = sq;
-    const double ae = fabs(e);
-    // Rounding floor: in the asymptotic regime (every eigenvalue within ~0.1 of
-    // 0 or 1, which e < e_asym implies) two exact steps always lower e, so no
-    // decrease over two steps means rounding; above e_asym states near a small
-    // gap can hold e level for a step or two, so there only six steps that all
-    // stay above the best error before them count (for floors above e_asym).
-    bool conv = ae < tol_abs || (k >= 2 && ae < e_asym && ae >= fabs(st->err[k - 2]));
-    if (!conv && k >= 8 && ae < e_stag) {
-        double before = fabs(st->err[0]), window = ae;
-        for (int j = 1; j <= k - 6; ++j) before = fmin(before, fabs(st->err[j]));
-        for (int j = k - 5; j < k; ++j) window = fmin(window, fabs(st->err[j]));
-        conv = window >= before;
-    }
-    if (conv) {
-        st->converged = 1;
-        st->active = 0;
-    } else if (k >= maxit || k >= kMaxIt) {
-        st->status = PTBGPU_EITER;
-        st->active = 0;
-    } else {
-        st->next = k + 1;
-    }
+    sp2_decide(st, sh[0][0], sh[1][0], N, tol_abs, e_asym, e_stag, maxit);
 }
 
 // out(i,j) = alpha (W_ij + W_ji) + beta X_ij over the ldp x ldp FP32 planes
@@ -724,7 +670,6 @@ bool sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
             // int8-sliced squares, X updated in place (the epilogue reads X(r,c), c >= r,
             // before writing it; the mirrored lower triangle is never read); the error
             // of each iterate is checked before its square is taken
-            const oz::Operand opX = oz_operand(c, 1, n, S);
             DevBuf& bst = c->buf(B_OZS);
             // per-tile partials: at most (rows / 128) x ceil(cols / 48) tiles for either kernel variant
             bst.reserve(sizeof(double) * 2 * (size_t)(oz::padded(n) / oz::BM) * (size_t)((oz::padded(n) + 47) / 48));
@@ -739,6 +684,10 @@ bool sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
                 log_line(prl, 2, " SP2 (int8 FP64 cleanup) %d  err %.3e", nclean, err);
                 if (e < 1e-13 * (double)n || (hist.size() > 2 && e >= hist[hist.size() - 3]) || nclean >= 8) break;
                 const bool sq = std::fabs(trX2 - N) <= std::fabs(2.0 * trX - trX2 - N);
+                // while the iterate is still far from idempotent its square needs no
+                // more than 6 slices (42 bits): the last digits only matter in the
+                // final squares, which take the full slice count
+                const oz::Operand opX = oz_operand(c, 1, n, e > 1e-4 ? std::min(S, 6) : S);
                 oz_slice(c, X, 1, n, n, oz::TRI_NONE, opX);
                 oz::OzEpi es;
                 es.n = n;

@@ -94,7 +94,11 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
                                             int* abort_flag, double* red, int bi, int bj, int q, int lane,
                                             int stat_index) {
     const int64_t ld = ep.ld;
-    const int64_t r = (int64_t)bi * BM + q * 32 + lane;
+    const int64_t r = (int64_t)bi * BM + q * 32 + lane;    // row of the (stacked) planes
+    // stacked systems: the tile's system starts at row rb; rows and columns
+    // below are local to it (rb = 0 for a single system)
+    const int64_t rb = ep.stacked ? ((int64_t)bi * BM / ld) * ld : 0;
+    const int64_t rl = r - rb;
     double tr = 0.0, ss = 0.0;
     const bool ok = __all_sync(0xffffffffu, mbar_wait(accum_bar, 0));
     if (!ok && lane == 0) {
@@ -104,12 +108,12 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
     const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
     tc_fence_after();
     if (ok && !aborted) {
-        const bool square = (EPI == EPI_SP2) ? (*ep.sq_flag != 0) : true;
+        const bool square = (EPI == EPI_SP2) ? (ep.sq_flag[rb / ld] != 0) : true;
         for (int c0 = 0; c0 < BN; c0 += 32) {
             uint32_t v[32];
             __syncwarp();   // lanes may have taken different paths in the previous chunk
             tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
-            const int64_t cbase = (int64_t)bj * BN + c0;
+            const int64_t cbase = (int64_t)bj * BN - rb + c0;   // local column
             if (EPI == EPI_FULL) {
                 float4* dst = reinterpret_cast<float4*>(ep.out + r * ld + cbase);
 #pragma unroll
@@ -118,8 +122,8 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
                                          __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]));
                 continue;
             }
-            if (cbase + 31 < r) continue;       // chunk entirely below the diagonal
-            if (cbase >= r) {
+            if (cbase + 31 < rl) continue;      // chunk entirely below the diagonal
+            if (cbase >= rl) {
                 // whole chunk in the upper triangle: vector path
                 const float4* xin = reinterpret_cast<const float4*>(ep.xcur + r * ld + cbase);
                 float4* xo = reinterpret_cast<float4*>(ep.out + r * ld + cbase);
@@ -142,15 +146,16 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
                         split_bf16(val[t], hh[t], mm[t], ll[t]);
                         const int64_t c = cbase + 8 * j8 + t;
                         const double dv = (double)val[t];
-                        if (c == r) {
+                        if (c == rl) {
                             tr += dv;
                             ss += dv * dv;
                         } else {
+                            const int64_t m = (rb + c) * ld + rl;   // mirrored element
                             ss += 2.0 * dv * dv;
-                            ep.out[c * ld + r] = val[t];
-                            ep.hi[c * ld + r] = hh[t];
-                            ep.lo[c * ld + r] = mm[t];
-                            ep.lo2[c * ld + r] = ll[t];
+                            ep.out[m] = val[t];
+                            ep.hi[m] = hh[t];
+                            ep.lo[m] = mm[t];
+                            ep.lo2[m] = ll[t];
                         }
                     }
                     xo[2 * j8] = make_float4(val[0], val[1], val[2], val[3]);
@@ -164,7 +169,7 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
 #pragma unroll 4
                 for (int j = 0; j < 32; ++j) {
                     const int64_t c = cbase + j;
-                    if (c < r) continue;
+                    if (c < rl) continue;
                     const float cv = __uint_as_float(v[j]);
                     const float val = square ? cv : 2.0f * ep.xcur[r * ld + c] - cv;
                     __nv_bfloat16 h, m, l;
@@ -174,15 +179,16 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
                     ep.hi[r * ld + c] = h;
                     ep.lo[r * ld + c] = m;
                     ep.lo2[r * ld + c] = l;
-                    if (c == r) {
+                    if (c == rl) {
                         tr += dv;
                         ss += dv * dv;
                     } else {
+                        const int64_t mi = (rb + c) * ld + rl;   // mirrored element
                         ss += 2.0 * dv * dv;
-                        ep.out[c * ld + r] = val;
-                        ep.hi[c * ld + r] = h;
-                        ep.lo[c * ld + r] = m;
-                        ep.lo2[c * ld + r] = l;
+                        ep.out[mi] = val;
+                        ep.hi[mi] = h;
+                        ep.lo[mi] = m;
+                        ep.lo2[mi] = l;
                     }
                 }
             }
@@ -209,7 +215,8 @@ template <int EPI, int BN, int NP, int KB>
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_product(const __grid_constant__ TmaPlanes maps, const ProdList prods, const int2* __restrict__ tiles,
                  int nk, EpiParams ep) {
-    if (ep.active && *ep.active == 0) return;   // uniform early exit (converged iteration)
+    // early exit of a converged system (uniform over the CTA)
+    if (ep.active && ep.active[ep.stacked ? (int64_t)tiles[blockIdx.x].x * BM / ep.ld : 0] == 0) return;
     using C = Cfg<BN, NP, KB>;
     constexpr int STAGE_BYTES = C::STAGE_BYTES;
     constexpr int STAGES = C::STAGES;
@@ -350,7 +357,8 @@ template <int EPI, int NP, int KB>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
     k_tc_product_pair(const __grid_constant__ TmaPlanes maps, const ProdList prods, const int2* __restrict__ pairs,
                       int nk, EpiParams ep) {
-    if (ep.active && *ep.active == 0) return;   // uniform over the grid: both CTAs of a pair return
+    // early exit of a converged system: both CTAs of a pair hold rows of the same system
+    if (ep.active && ep.active[ep.stacked ? (int64_t)pairs[blockIdx.x >> 1].x * 256 / ep.ld : 0] == 0) return;
     using C = CfgPair<NP, KB>;
     constexpr int STAGE_BYTES = C::STAGE_BYTES;
     constexpr int STAGES = C::STAGES;
@@ -478,10 +486,10 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     return fn;
 }
 
-void encode_plane(CUtensorMap* map, const void* plane, int64_t ld, int box_rows, int kb) {
+void encode_plane(CUtensorMap* map, const void* plane, int64_t ld, int64_t rows, int box_rows, int kb) {
     PTB_CHECK(((uintptr_t)plane & 15) == 0, PTBGPU_EINVAL, "operand plane not 16-byte aligned");
     PTB_CHECK(ld % 256 == 0, PTBGPU_EINVAL, "operand leading dimension must be a multiple of 256");
-    cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)ld};
+    cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
     cuuint32_t box[2] = {(cuuint32_t)kb, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
@@ -571,20 +579,23 @@ void launch_epi(cudaStream_t s, int np, int kb, bool pair, const TmaPlanes& maps
 // outputs, so running them all is harmless -- times them with CUDA events and
 // keeps the fastest for the rest of the process.
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, long long>, int> g_tuned;
+std::map<std::tuple<int, int, int, long long, long long>, int> g_tuned;
 }  // namespace
 
-int tuned_kblock(int epi, int np, long long ld) {
+int tuned_kblock(int epi, int np, long long ld, long long rows) {
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    auto it = g_tuned.find(std::make_tuple(dev, epi, np, ld));
+    auto it = g_tuned.find(std::make_tuple(dev, epi, np, ld, rows == 0 ? ld : rows));
     return it == g_tuned.end() ? 0 : it->second;
 }
 
 int launch_product(cudaStream_t s, int epi, int np, long long ld, const void* const* a, const void* const* b,
                    const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep, int kblock,
-                   const int2* pairs_dev, int npairs) {
+                   const int2* pairs_dev, int npairs, long long rows) {
+    if (rows == 0) rows = ld;
+    PTB_CHECK(rows % ld == 0 && (ep.stacked || rows == ld), PTBGPU_EINVAL,
+              "stacked planes: rows must be a multiple of ld and the epilogue told so");
     PTB_CHECK(np == 2 || np == 3, PTBGPU_EINVAL, "unsupported plane count %d", np);
     PTB_CHECK(kblock == 0 || kblock == 32 || kblock == 64 || kblock == kPairKernel + 32 ||
                   kblock == kPairKernel + 64,
@@ -603,8 +614,8 @@ int launch_product(cudaStream_t s, int epi, int np, long long ld, const void* co
         const int kb = pair ? choice - kPairKernel : choice;
         TmaPlanes maps;
         for (int p = 0; p < np; ++p) {
-            encode_plane(&maps.a[p], a[p], ld, BM, kb);
-            encode_plane(&maps.b[p], b[p], ld, pair ? 128 : bn, kb);
+            encode_plane(&maps.a[p], a[p], ld, rows, BM, kb);
+            encode_plane(&maps.b[p], b[p], ld, rows, pair ? 128 : bn, kb);
         }
         const int nk = (int)(ld / kb);
         const int2* t = pair ? pairs_dev : tiles_dev;
@@ -614,7 +625,7 @@ int launch_product(cudaStream_t s, int epi, int np, long long ld, const void* co
         PTB_CUDA(cudaGetLastError());
         return pair ? 2 * npairs : ntiles;
     };
-    if (kblock == 0) kblock = tuned_kblock(epi, np, ld);
+    if (kblock == 0) kblock = tuned_kblock(epi, np, ld, rows);
     if (kblock != 0 && (kblock < kPairKernel || pairs_dev)) return run(kblock);
     std::vector<int> cand = {64, 32};
     if (np == 2 && pairs_dev) {
@@ -644,7 +655,7 @@ int launch_product(cudaStream_t s, int epi, int np, long long ld, const void* co
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    g_tuned[std::make_tuple(dev, epi, np, ld)] = best;
+    g_tuned[std::make_tuple(dev, epi, np, ld, rows)] = best;
     return parts;   // the buffers hold the last candidate's results
 }
 

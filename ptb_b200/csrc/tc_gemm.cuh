@@ -29,8 +29,12 @@ struct ProdList {
 };
 
 struct EpiParams {
-    const int* active;        // device flag; 0 -> the launch does nothing (may be null)
+    const int* active;        // device flag(s); 0 -> the tile does nothing (may be null)
     const int* sq_flag;       // EPI_SP2: 1 -> X' = X^2, 0 -> X' = 2X - X^2
+    // stacked != 0: the planes hold systems of ld x ld stacked along the rows
+    // (row-major, ld columns); tiles carry global row blocks, output columns
+    // are local to the tile's system, and active / sq_flag are per system
+    int stacked;
     int* err;                 // device error word (bounded waits)
     long long ld;             // leading dimension of every plane / matrix (multiple of 256)
     const float* xcur;        // EPI_SP2: current iterate (FP32)
@@ -50,10 +54,11 @@ std::vector<int2> make_pair_tiles(long long ld, bool upper_only);
 // planes and pairs_dev), or 0 = the autotuned choice for this shape (every
 // candidate is timed on its first launch).  Returns the number of per-CTA
 // stats partials written (EPI_SP2 reduces that many).
+// rows: rows of every plane (0 = ld; a multiple of ld for stacked systems).
 int launch_product(cudaStream_t s, int epi, int np, long long ld, const void* const* a, const void* const* b,
                    const ProdList& prods, const int2* tiles_dev, int ntiles, const EpiParams& ep, int kblock = 0,
-                   const int2* pairs_dev = nullptr, int npairs = 0);
-int tuned_kblock(int epi, int np, long long ld);   // 0 until the shape has been tuned
+                   const int2* pairs_dev = nullptr, int npairs = 0, long long rows = 0);
+int tuned_kblock(int epi, int np, long long ld, long long rows = 0);   // 0 until the shape has been tuned
 
 }  // namespace tc
 }  // namespace ptb
