@@ -235,12 +235,17 @@ def run_batch(args, rank, world, local, pg):
             walls.append(wall)
     clocks = clk.summary()
     ms = reduce_max(pg, statistics.median(walls))
-    extra = {}
+    extra, grouped = {}, None
     if args.compare_fp64 and rank == 0:
         P64, st64, wall64 = ctx.tc_purify_batch(args_b, Options(precision=PREC_FP64), workers=args.workers)
         extra = {"s_per_step": wall64 / 1e3,
                  "max_abs_dP_mixed_vs_fp64": float(max(np.max(np.abs(a - b)) for a, b in zip(Ps, P64))),
                  "speedup_mixed_vs_fp64": wall64 / ms}
+        # the same systems through the grouped entry (one launch per step per size bucket)
+        Pg, stg, wallg = ctx.tc_purify_grouped(args_b, opts)
+        grouped = {"entry": "ptbgpu_tc_purify_grouped", "s_per_step": wallg / 1e3,
+                   "max_abs_dP_vs_fp64": float(max(np.max(np.abs(a - b)) for a, b in zip(Pg, P64))),
+                   "fp64_fallbacks": sum(x.fp64_fallback for x in stg)}
     if rank != 0:
         ctx.close()
         return
@@ -285,6 +290,8 @@ def run_batch(args, rank, world, local, pg):
     }
     if extra:
         line["fp64_gpu"] = extra
+    if grouped:
+        line["grouped"] = grouped
     print(json.dumps(line), flush=True)
     ctx.close()
 
