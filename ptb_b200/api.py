@@ -358,10 +358,18 @@ class Context:
                                             C.byref(o), C.byref(st)))
         return P, Stats.from_c(st)
 
-    def tc_purify(self, ndim: int, nel: int, H: np.ndarray, S: np.ndarray, opts: Options | None = None):
-        """Trace-correcting purification (FP64 or bf16x3 + FP64 refinement).  Returns (Pvec, Stats)."""
+    def tc_purify(self, ndim: int, nel: int, H: np.ndarray, S: np.ndarray, opts: Options | None = None,
+                  out: np.ndarray | None = None):
+        """Trace-correcting purification (FP64 or bf16x3 + FP64 refinement).  Returns (Pvec, Stats).
+        out: a preallocated contiguous float64 array of npacked(ndim) elements for P (e.g. in
+        pinned memory, which the device-to-host copy needs for full speed)."""
         Hh, Sh = _f64(H), _f64(S)
-        P = np.zeros(npacked(ndim))
+        if out is not None:
+            if out.dtype != np.float64 or out.size != npacked(ndim) or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous float64 array of npacked(ndim) elements")
+            P = out
+        else:
+            P = np.empty(npacked(ndim))
         st = _Stats()
         o = (opts or Options()).to_c()
         self._check(self._lib.ptbgpu_tc_purify(self._h, int(ndim), int(nel), _dptr(Hh), _dptr(Sh), _dptr(P),
