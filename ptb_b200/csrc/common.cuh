@@ -91,6 +91,8 @@ struct ptbgpu_ctx {
     // submatrix method between its phases (plan, prepare, nel, finish): kept
     // until the next plan or the context's end; its destructor frees its buffers
     std::shared_ptr<void> sm_plan;
+    // side streams and handles of the submatrix method's large eigensolves
+    std::shared_ptr<void> sm_side;
     // worker contexts of the multi-instance batch (same device, own streams and buffers)
     std::vector<ptbgpu_ctx*> workers;
     // launches of this library's kernels since the last call started

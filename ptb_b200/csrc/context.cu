@@ -107,6 +107,7 @@ int ptbgpu_finalize(ptbgpu_ctx* c) {
     if (!c) return PTBGPU_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->sm_plan.reset();
+    c->sm_side.reset();
     for (ptbgpu_ctx* w : c->workers) ptbgpu_finalize(w);
     c->workers.clear();
     for (auto& b : c->bufs) b.release();

@@ -24,7 +24,9 @@
 #include <chrono>
 #include <cmath>
 #include <map>
+#include <mutex>
 #include <numeric>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -538,6 +540,49 @@ struct Bucket {
     DevBuf probs, U, w;
 };
 
+// Side streams for the large submatrices (one generalized eigensolve each):
+// cuSOLVER's dsygvd at these sizes is latency-bound (tridiagonalisation), so
+// several run at once, each on its own stream and handles, driven by its own
+// host thread.  Kept on the context between calls.
+struct SidePool {
+    static constexpr int kStreams = 4;
+    int device = 0;
+    cudaStream_t st[kStreams] = {};
+    cusolverDnHandle_t sol[kStreams] = {};
+    cublasHandle_t blas[kStreams] = {};
+    cudaEvent_t done[kStreams] = {};
+    DevBuf ws[kStreams], sk[kStreams], tb[kStreams];
+    ~SidePool() {
+        for (int i = 0; i < kStreams; ++i) {
+            if (st[i]) cudaStreamSynchronize(st[i]);
+            ws[i].release();
+            sk[i].release();
+            tb[i].release();
+            if (sol[i]) cusolverDnDestroy(sol[i]);
+            if (blas[i]) cublasDestroy(blas[i]);
+            if (done[i]) cudaEventDestroy(done[i]);
+            if (st[i]) cudaStreamDestroy(st[i]);
+        }
+    }
+};
+
+SidePool& side_pool(ptbgpu_ctx* c) {
+    if (!c->sm_side) {
+        auto sp = std::make_shared<SidePool>();
+        sp->device = c->device;
+        for (int i = 0; i < SidePool::kStreams; ++i) {
+            PTB_CUDA(cudaStreamCreateWithFlags(&sp->st[i], cudaStreamNonBlocking));
+            PTB_CUSOLVER(cusolverDnCreate(&sp->sol[i]));
+            PTB_CUSOLVER(cusolverDnSetStream(sp->sol[i], sp->st[i]));
+            PTB_CUBLAS(cublasCreate(&sp->blas[i]));
+            PTB_CUBLAS(cublasSetStream(sp->blas[i], sp->st[i]));
+            PTB_CUDA(cudaEventCreateWithFlags(&sp->done[i], cudaEventDisableTiming));
+        }
+        c->sm_side = sp;
+    }
+    return *static_cast<SidePool*>(c->sm_side.get());
+}
+
 // __global__ helper: nel(mu) = sum fe_q occ(e_q, mu) over the prepared
 // eigenpairs, one block of 1024 threads with the same partition and reduction
 // order as k_mu_bisect (so a one-rank host bisection reproduces it exactly).
@@ -581,6 +626,134 @@ struct SmPlan {
 };
 
 namespace {
+
+// ---- size-bucket schedule of the batched eigensolver -----------------------
+// The batched cuSOLVER eigensolver costs about L(M) + p(M) B for B problems
+// padded to M (a launch/latency term that does not shrink with B, and a
+// per-problem term): fine buckets of a few problems each pay L many times.
+// The cost model is measured once per device and padded size (random symmetric
+// test matrices, B = 1 and B = 16), and the problems, sorted by size, are cut
+// into contiguous buckets by dynamic programming on the modelled cost.
+struct EigCost {
+    double L = 0.0, p = 0.0;   // ms
+};
+
+__global__ void k_fill_test(int M, int B, double* __restrict__ A) {
+    const int64_t total = (int64_t)B * M * M;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = t / ((int64_t)M * M), r = t % ((int64_t)M * M);
+        const int64_t i = r % M, j = r / M;
+        const uint64_t lo = (uint64_t)(i < j ? i : j), hi = (uint64_t)(i < j ? j : i);
+        uint64_t h = (lo * 0x9E3779B97F4A7C15ull) ^ (hi * 0xC2B2AE3D27D4EB4Full) ^ ((uint64_t)b * 0x165667B19E3779F9ull);
+        h ^= h >> 31;
+        h *= 0xD6E8FEB86659FD93ull;
+        h ^= h >> 32;
+        A[t] = (double)(h >> 11) * (1.0 / 9007199254740992.0) - 0.5 + (i == j ? 2.0 : 0.0);
+    }
+}
+
+std::mutex g_eig_mu;
+std::map<std::pair<int, int>, EigCost> g_eig_cost;
+
+// Measured cost of the batched eigensolver at padded size M (cached per device).
+// Returns false when the batched routine is unavailable at this size.
+bool eig_cost(ptbgpu_ctx* c, cusolverDnParams_t params, int M, EigCost* out) {
+    std::lock_guard<std::mutex> lock(g_eig_mu);
+    const auto key = std::make_pair(c->device, M);
+    auto it = g_eig_cost.find(key);
+    if (it != g_eig_cost.end()) {
+        *out = it->second;
+        return true;
+    }
+    constexpr int Bt = 16;
+    cudaStream_t s = c->stream;
+    DevBuf a, w, ws, info;
+    a.reserve(sizeof(double) * (size_t)Bt * M * M);
+    w.reserve(sizeof(double) * (size_t)Bt * M);
+    info.reserve(sizeof(int) * Bt);
+    size_t wsd = 0, wsh = 0;
+    if (cusolverDnXsyevBatched_bufferSize(c->solver, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, M,
+                                          CUDA_R_64F, a.ptr, M, CUDA_R_64F, w.ptr, CUDA_R_64F, &wsd, &wsh, Bt) !=
+        CUSOLVER_STATUS_SUCCESS)
+        return false;
+    ws.reserve(std::max<size_t>(wsd, 16));
+    std::vector<char> hws(std::max<size_t>(wsh, 16));
+    cudaEvent_t e0 = c->take_event(), e1 = c->take_event();
+    auto run = [&](int B) -> float {
+        k_fill_test<<<592, 256, 0, s>>>(M, B, a.as<double>());
+        PTB_CUDA(cudaGetLastError());
+        PTB_CUDA(cudaEventRecord(e0, s));
+        PTB_CUSOLVER(cusolverDnXsyevBatched(c->solver, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, M,
+                                            CUDA_R_64F, a.ptr, M, CUDA_R_64F, w.ptr, CUDA_R_64F, ws.ptr, wsd,
+                                            hws.data(), wsh, info.as<int>(), B));
+        PTB_CUDA(cudaEventRecord(e1, s));
+        PTB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        PTB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms;
+    };
+    run(1);   // first call of this size: one-time setup inside the library
+    const float t1 = std::min(run(1), run(1));
+    const float tb = run(Bt);
+    EigCost ec;
+    ec.p = std::max(0.0, (double)(tb - t1) / (Bt - 1));
+    ec.L = std::max(0.0, (double)t1 - ec.p);
+    g_eig_cost[key] = ec;
+    *out = ec;
+    return true;
+}
+
+// Contiguous buckets of the problems sorted by size, padded to multiples of 32,
+// with the least modelled cost.  Returns (padded size, problems) per bucket.
+std::vector<std::pair<int, std::vector<Prob>>> tuned_buckets(ptbgpu_ctx* c, cusolverDnParams_t params,
+                                                             std::vector<Prob> probs, int prl) {
+    std::vector<std::pair<int, std::vector<Prob>>> out;
+    if (probs.empty()) return out;
+    std::stable_sort(probs.begin(), probs.end(), [](const Prob& a, const Prob& b) { return a.m < b.m; });
+    const int P = (int)probs.size();
+    std::map<int, EigCost> cost;
+    for (const Prob& p : probs) {
+        const int M = (int)round_up(p.m, 32);
+        if (cost.count(M)) continue;
+        EigCost ec;
+        if (!eig_cost(c, params, M, &ec)) {   // no batched routine: fine buckets
+            std::map<int, std::vector<Prob>> fine;
+            for (const Prob& q : probs) fine[(int)round_up(q.m, 32)].push_back(q);
+            for (auto& kv : fine) out.push_back({kv.first, kv.second});
+            return out;
+        }
+        cost[M] = ec;
+    }
+    std::vector<double> best(P + 1, 0.0);
+    std::vector<int> from(P + 1, 0);
+    for (int j = 1; j <= P; ++j) {
+        const int M = (int)round_up(probs[j - 1].m, 32);
+        const EigCost& ec = cost[M];
+        best[j] = INFINITY;
+        for (int i = 1; i <= j; ++i) {
+            const double v = best[i - 1] + ec.L + ec.p * (double)(j - i + 1);
+            if (v < best[j]) {
+                best[j] = v;
+                from[j] = i;
+            }
+        }
+    }
+    for (int j = P; j > 0; j = from[j] - 1) {
+        const int i = from[j];
+        out.push_back({(int)round_up(probs[j - 1].m, 32), std::vector<Prob>(probs.begin() + (i - 1), probs.begin() + j)});
+    }
+    std::reverse(out.begin(), out.end());
+    if (prl >= 2) {
+        std::string line;
+        char buf[64];
+        for (const auto& b : out) {
+            snprintf(buf, sizeof(buf), " %dx%zu", b.first, b.second.size());
+            line += buf;
+        }
+        log_line(prl, 2, " * submatrix bucket schedule (M x problems):%s  modelled %.1f ms", line.c_str(), best[P]);
+    }
+    return out;
+}
 
 SmPlan& plan_of(ptbgpu_ctx* c) {
     PTB_CHECK(c->sm_plan != nullptr, PTBGPU_EINVAL, "no submatrix plan on this context (call the plan phase first)");
@@ -715,25 +888,30 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
     };
 
     constexpr int kBatchMax = 1024;
-    std::map<int, std::vector<Prob>> buckets;
-    std::vector<Prob> large;
+    std::vector<Prob> small, large;
     int64_t eoff = 0;
     for (int k : ids) {
         Prob p{k, pl.counts[k], pl.moff[k], eoff};
         eoff += pl.counts[k];
         if (pl.counts[k] > kBatchMax) large.push_back(p);
-        else buckets[(int)round_up(pl.counts[k], 32)].push_back(p);
+        else small.push_back(p);
     }
     pl.total = eoff;
     DevBuf& be = c->buf(B_MISC0);
     DevBuf& bfe = c->buf(B_MISC1);
     be.reserve(sizeof(double) * std::max<int64_t>(eoff, 1));
     bfe.reserve(sizeof(double) * std::max<int64_t>(eoff, 1));
-    pl.bks.resize(buckets.size() + large.size());
-
     DevBuf sb, ptrs, infos, ws, tbuf;
     cusolverDnParams_t params;
     PTB_CUSOLVER(cusolverDnCreateParams(&params));
+    std::vector<std::pair<int, std::vector<Prob>>> buckets;
+    try {
+        buckets = tuned_buckets(c, params, small, prl);
+    } catch (...) {
+        cusolverDnDestroyParams(params);
+        throw;
+    }
+    pl.bks.resize(buckets.size() + large.size());
     auto cleanup = [&] {
         cusolverDnDestroyParams(params);
         sb.release();
@@ -827,39 +1005,100 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
             for (const Prob& p : pv) pl.flops += 9.0 * std::pow((double)p.m, 3);
             log_line(prl, 2, " * submatrix bucket M=%d: %d problems", M, B);
         }
-        // large submatrices: one generalized eigensolve each (dsygvd), fe from T = S_k U
-        for (const Prob& p : large) {
-            Bucket& bk = pl.bks[bi++];
-            bk.is_large = true;
-            bk.single = p;
-            const int m = p.m;
-            bk.M = m;
-            bk.count = 1;
-            bk.probs.reserve(sizeof(Prob));
-            PTB_CUDA(cudaMemcpyAsync(bk.probs.ptr, &p, sizeof(Prob), cudaMemcpyHostToDevice, s));
-            bk.U.reserve(sizeof(double) * (size_t)m * m);
-            bk.w.reserve(sizeof(double) * (size_t)m);
-            sb.reserve(sizeof(double) * (size_t)m * m);
-            tbuf.reserve(sizeof(double) * (size_t)m * m);
-            double* U = bk.U.as<double>();
-            double* Sk = sb.as<double>();
-            dim3 gg((m + 31) / 32, 64, 1);
-            k_gather<<<gg, dim3(32, 8), 0, s>>>(m, bk.probs.as<Prob>(), d_maps, n, H, S, U, Sk);
-            count_launch();
-            PTB_CUDA(cudaGetLastError());
-            const int info = dsygvd(c, m, m, U, Sk, bk.w.as<double>());
-            PTB_CHECK(info == 0, PTBGPU_ENOTSPD, "dsygvd failed on submatrix %d (info=%d)", p.k + 1, info);
-            k_gather<<<gg, dim3(32, 8), 0, s>>>(m, bk.probs.as<Prob>(), d_maps, n, H, S, tbuf.as<double>(), Sk);
-            count_launch();
-            PTB_CUDA(cudaGetLastError());
-            PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &one, Sk, m, U, m, &zero,
-                                   tbuf.as<double>(), m));
-            k_fe_large<<<(m + 255) / 256, 256, 0, s>>>(m, tbuf.as<double>(), U, d_own_cols, pl.own_off[p.k],
-                                                       pl.own_off[p.k + 1], d_ipos, bk.w.as<double>(),
-                                                       be.as<double>() + p.eoff, bfe.as<double>() + p.eoff);
-            count_launch();
-            PTB_CUDA(cudaGetLastError());
-            pl.flops += 9.0 * std::pow((double)m, 3);
+        // large submatrices: one generalized eigensolve each (dsygvd), fe from T = S_k U,
+        // spread over the side streams (largest first), each driven by its own host thread
+        if (!large.empty()) {
+            SidePool& sp = side_pool(c);
+            std::vector<size_t> order(large.size());
+            std::iota(order.begin(), order.end(), 0);
+            std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return large[a].m > large[b].m; });
+            std::vector<Bucket*> lb(large.size());
+            for (size_t q = 0; q < large.size(); ++q) {
+                const Prob& p = large[q];
+                Bucket& bk = pl.bks[bi++];
+                bk.is_large = true;
+                bk.single = p;
+                bk.M = p.m;
+                bk.count = 1;
+                bk.probs.reserve(sizeof(Prob));
+                PTB_CUDA(cudaMemcpyAsync(bk.probs.ptr, &p, sizeof(Prob), cudaMemcpyHostToDevice, s));
+                bk.U.reserve(sizeof(double) * (size_t)p.m * p.m);
+                bk.w.reserve(sizeof(double) * (size_t)p.m);
+                lb[q] = &bk;
+                pl.flops += 9.0 * std::pow((double)p.m, 3);
+            }
+            infos.reserve(sizeof(int) * large.size());
+            PTB_CUDA(cudaMemsetAsync(infos.ptr, 0, sizeof(int) * large.size(), s));
+            cudaEvent_t ready = c->take_event();
+            PTB_CUDA(cudaEventRecord(ready, s));
+            const int nw = (int)std::min<size_t>(SidePool::kStreams, large.size());
+            std::atomic<size_t> next{0};
+            std::vector<std::string> errs(nw);
+            std::vector<int64_t> launches(nw, 0);
+            auto work = [&](int w) {
+                try {
+                    PTB_CUDA(cudaSetDevice(c->device));
+                    cudaStream_t st = sp.st[w];
+                    PTB_CUDA(cudaStreamWaitEvent(st, ready, 0));
+                    for (size_t t = next++; t < order.size(); t = next++) {
+                        const size_t q = order[t];
+                        const Prob& p = large[q];
+                        Bucket& bk = *lb[q];
+                        const int m = p.m;
+                        sp.sk[w].reserve(sizeof(double) * (size_t)m * m);
+                        sp.tb[w].reserve(sizeof(double) * (size_t)m * m);
+                        double* U = bk.U.as<double>();
+                        double* Sk = sp.sk[w].as<double>();
+                        double* T = sp.tb[w].as<double>();
+                        dim3 gg((m + 31) / 32, 64, 1);
+                        k_gather<<<gg, dim3(32, 8), 0, st>>>(m, bk.probs.as<Prob>(), d_maps, n, H, S, U, Sk);
+                        PTB_CUDA(cudaGetLastError());
+                        int lwork = 0;
+                        PTB_CUSOLVER(cusolverDnDsygvd_bufferSize(sp.sol[w], CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                                                 CUBLAS_FILL_MODE_UPPER, m, U, m, Sk, m,
+                                                                 bk.w.as<double>(), &lwork));
+                        sp.ws[w].reserve(sizeof(double) * (size_t)std::max(lwork, 1));
+                        PTB_CUSOLVER(cusolverDnDsygvd(sp.sol[w], CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                                      CUBLAS_FILL_MODE_UPPER, m, U, m, Sk, m, bk.w.as<double>(),
+                                                      sp.ws[w].as<double>(), lwork, infos.as<int>() + q));
+                        k_gather<<<gg, dim3(32, 8), 0, st>>>(m, bk.probs.as<Prob>(), d_maps, n, H, S, T, Sk);
+                        PTB_CUDA(cudaGetLastError());
+                        PTB_CUBLAS(cublasDgemm(sp.blas[w], CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &one, Sk, m, U, m,
+                                               &zero, T, m));
+                        k_fe_large<<<(m + 255) / 256, 256, 0, st>>>(m, T, U, d_own_cols, pl.own_off[p.k],
+                                                                   pl.own_off[p.k + 1], d_ipos, bk.w.as<double>(),
+                                                                   be.as<double>() + p.eoff,
+                                                                   bfe.as<double>() + p.eoff);
+                        PTB_CUDA(cudaGetLastError());
+                        launches[w] += 3;
+                    }
+                    PTB_CUDA(cudaEventRecord(sp.done[w], st));
+                } catch (const Error& e) {
+                    errs[w] = e.msg;
+                } catch (const std::exception& e) {
+                    errs[w] = e.what();
+                }
+            };
+            std::vector<std::thread> pool;
+            for (int w = 0; w < nw; ++w) pool.emplace_back(work, w);
+            for (auto& t : pool) t.join();
+            for (int w = 0; w < nw; ++w)
+                if (!errs[w].empty()) {
+                    // let every side stream drain before the shared buffers can be released
+                    for (int v = 0; v < nw; ++v) cudaStreamSynchronize(sp.st[v]);
+                    fail(PTBGPU_ECUDA, "large submatrix eigensolve: %s", errs[w].c_str());
+                }
+            for (int w = 0; w < nw; ++w) {
+                PTB_CUDA(cudaStreamWaitEvent(s, sp.done[w], 0));
+                count_launch((int)launches[w]);
+            }
+            std::vector<int> hinfo(large.size());
+            PTB_CUDA(cudaMemcpyAsync(hinfo.data(), infos.ptr, sizeof(int) * hinfo.size(), cudaMemcpyDeviceToHost, s));
+            PTB_CUDA(cudaStreamSynchronize(s));
+            for (size_t q = 0; q < large.size(); ++q)
+                PTB_CHECK(hinfo[q] == 0, PTBGPU_ENOTSPD, "dsygvd failed on submatrix %d (info=%d)", large[q].k + 1,
+                          hinfo[q]);
+            mark("large eigensolves (side streams)");
         }
         PTB_CUDA(cudaStreamSynchronize(s));
     } catch (...) {
