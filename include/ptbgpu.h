@@ -338,6 +338,14 @@ int ptbgpu_xc_damping_device(ptbgpu_ctx* ctx, int64_t nat, int64_t ndim, const i
                              const double* rad, const double* hao, const double* xdiag, const double* dPpk,
                              double* dHpk, double* ms_update);
 
+/* ---- self-test ------------------------------------------------------------ */
+/* No counterpart in the reference.  Runs one bounded device wait on a flag that
+ * nothing sets, with a limit of limit_us (1..2e6) microseconds, through the
+ * same error path as the library's kernels' waits: returns PTBGPU_ETIMEOUT with
+ * a message naming the site, and leaves the context usable.  For testing the
+ * failure path without faulting or hanging a GPU. */
+int ptbgpu_selftest_bounded_wait(ptbgpu_ctx* ctx, int64_t limit_us);
+
 #ifdef __cplusplus
 }
 #endif

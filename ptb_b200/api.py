@@ -73,7 +73,7 @@ EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_defau
             "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm", "ptbgpu_mlpop14", "ptbgpu_mlpop14_device",
             "ptbgpu_mlpop2", "ptbgpu_mlpop2_device", "ptbgpu_kmeans_partition", "ptbgpu_sm_plan",
             "ptbgpu_sm_prepare", "ptbgpu_sm_nel", "ptbgpu_sm_finish", "ptbgpu_xc_damping",
-            "ptbgpu_xc_damping_device")
+            "ptbgpu_xc_damping_device", "ptbgpu_selftest_bounded_wait")
 
 
 def library_path() -> Path:
@@ -117,6 +117,7 @@ def load_library():
     lib.ptbgpu_tc_purify_grouped.argtypes = [C.c_void_p, i64, P(i64), P(i64), P(d), P(d), P(d), P(_Opts),
                                              P(_Stats), d]
     lib.ptbgpu_solve2.argtypes = [C.c_void_p, i64, i64, i64, i64, d, d, d, d, d, P(_Opts), P(_Stats)]
+    lib.ptbgpu_selftest_bounded_wait.argtypes = [C.c_void_p, i64]
     lib.ptbgpu_xc_damping.argtypes = [C.c_void_p, i64, i64, P(i64), d, d, d, d, d, d, d]
     lib.ptbgpu_xc_damping_device.argtypes = [C.c_void_p, i64, i64, P(i64), d, d, d, d, C.c_void_p, C.c_void_p, d]
     lib.ptbgpu_symsq_bf16x3.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
@@ -444,6 +445,11 @@ class Context:
         self._check(self._lib.ptbgpu_tc_purify_grouped(self._h, n, ndim, nel, arr(Hs), arr(Ss), arr(Ps), C.byref(o),
                                                        st, C.byref(wall)))
         return Ps, [Stats.from_c(st[i]) for i in range(n)], wall.value
+
+    def selftest_bounded_wait(self, limit_us: int = 20000):
+        """One bounded device wait on a flag nothing sets: raises PtbGpuError with
+        code ETIMEOUT through the library's device-error path."""
+        self._check(self._lib.ptbgpu_selftest_bounded_wait(self._h, int(limit_us)))
 
     def solve2(self, mode: int, ndim: int, nel: int, nopen: int, H: np.ndarray, S: np.ndarray,
                opts: Options | None = None):

@@ -545,7 +545,7 @@ struct Bucket {
 // several run at once, each on its own stream and handles, driven by its own
 // host thread.  Kept on the context between calls.
 struct SidePool {
-    static constexpr int kStreams = 4;
+    static constexpr int kStreams = 8;
     int device = 0;
     cudaStream_t st[kStreams] = {};
     cusolverDnHandle_t sol[kStreams] = {};

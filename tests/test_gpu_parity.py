@@ -262,3 +262,19 @@ def test_tc_purify_errors(ctx, water8):
     # the context stays usable after errors
     P, st = ctx.tc_purify(s.ndim, s.nel, s.Hvec, s.Svec, Options(precision=PREC_MIXED))
     assert abs(st.ms_total) > 0
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(ctx, water8):
+    """A device wait on a flag that nothing sets gives up after its limit and
+    comes back as ETIMEOUT (the path every tensor-core pipeline wait takes);
+    the same context then runs a purification normally."""
+    with pytest.raises(PtbGpuError) as ei:
+        ctx.selftest_bounded_wait(20000)
+    assert ei.value.code == api.ETIMEOUT
+    assert "site 90" in str(ei.value)
+    s = water8
+    P, st = ctx.tc_purify(s.ndim, s.nel, s.Hvec, s.Svec, Options(precision=PREC_FP64))
+    assert st.iterations > 5
+    with pytest.raises(PtbGpuError) as ei:
+        ctx.selftest_bounded_wait(0)
+    assert ei.value.code == api.EINVAL
