@@ -75,7 +75,7 @@ __global__ void k_x0_init(int64_t n, int64_t ldp, const double* __restrict__ A, 
             const __nv_bfloat16 m = __float2bfloat16_rn(r);
             hi[k] = h;
             mid[k] = m;
-            lo[k] = __float2bfloat16_rn(r - __bfloat162float(m));
+            if (lo) lo[k] = __float2bfloat16_rn(r - __bfloat162float(m));
             const double dv = v;
             if (i == j) tr += dv;
             ss += dv * dv;
@@ -532,17 +532,22 @@ bool sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
     const size_t plane = sizeof(__nv_bfloat16) * (size_t)ldp * ldp;
     const size_t fplane = sizeof(float) * (size_t)ldp * ldp;
 
-    // trajectory slots (hi, mid, lo planes per iterate), bounded by free memory
+    // trajectory slots, bounded by free memory: hi and mid planes per iterate (the
+    // bf16x3 products and the replay read these), plus the lo plane only when
+    // three-plane products run
+    const int tp = split3_iters >= 0 ? 3 : 2;
     size_t free_b = 0, total_b = 0;
     PTB_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t other = 6 * fplane + 4 * plane + (size_t)(64 << 20);
     int slots = (int)std::min<int64_t>(maxit + 1, kMaxIt + 1);
-    if (free_b > other) slots = (int)std::min<size_t>(slots, (free_b - other) * 6 / 10 / (3 * plane));
+    if (free_b > other) slots = (int)std::min<size_t>(slots, (free_b - other) * 6 / 10 / (tp * plane));
     PTB_CHECK(slots >= std::min(8, maxit + 1), PTBGPU_ENOMEM,
               "not enough device memory for the purification trajectory");
     DevBuf& btraj = c->buf(B_TRAJ);
-    btraj.reserve(3 * plane * (size_t)slots);
-    auto traj = [&](int k, int j) { return (__nv_bfloat16*)((char*)btraj.ptr + plane * (3 * (size_t)k + j)); };
+    btraj.reserve(tp * plane * (size_t)slots);
+    auto traj = [&](int k, int j) {
+        return j < tp ? (__nv_bfloat16*)((char*)btraj.ptr + plane * (tp * (size_t)k + j)) : nullptr;
+    };
     auto traj_hi = [&](int k) { return traj(k, 0); };
     auto traj_lo = [&](int k) { return traj(k, 1); };
     c->buf(B_XF0).reserve(fplane);
@@ -613,7 +618,7 @@ bool sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
         ep.out = xf[(k + 1) & 1];
         ep.hi = traj(k + 1, 0);
         ep.lo = traj(k + 1, 1);
-        ep.lo2 = traj(k + 1, 2);
+        ep.lo2 = traj(k + 1, 2);   // null with two planes
         const void* pl[3] = {traj(k, 0), traj(k, 1), traj(k, 2)};
         const bool three = three_planes(k);
         const int ntl = three ? timed_product(c, tc::EPI_SP2, 3, ldp, pl, pl, split6, tiles_up3, n6, ep)

@@ -154,7 +154,7 @@ __global__ void k_x0(int64_t B, const double* __restrict__ A, const double* __re
         xf[base + l] = v;
         hi[base + l] = h;
         mid[base + l] = m;
-        lo[base + l] = q;
+        if (lo) lo[base + l] = q;
         if (i == j) tr += v;
         ss += (double)v * v;
     }
@@ -384,6 +384,7 @@ void run_chunk(ptbgpu_ctx* c, const Chunk& ch, const int64_t* ndim, const int64_
     const int refine_rounds = o->refine_rounds > 0 ? (int)o->refine_rounds : 4;
     const double refine_tol = o->refine_tol > 0.0 ? o->refine_tol : 1e-7;
     const int prl = (int)o->print_level;
+    const int tp = o->split3_iters >= 0 ? 3 : 2;   // bf16 planes per trajectory iterate
     // phase times of the chunk (print level >= 2; host clock after a stream synchronisation)
     auto tclock = std::chrono::steady_clock::now();
     std::vector<std::pair<const char*, double>> tph;
@@ -413,7 +414,7 @@ void run_chunk(ptbgpu_ctx* c, const Chunk& ch, const int64_t* ndim, const int64_
         bC.reserve(8 * (size_t)nb * BB);
         bF.reserve(4 * 5 * (size_t)nb * BB);
         bP.reserve(2 * 8 * (size_t)nb * BB);
-        bT.reserve(2 * 3 * (size_t)slots * nb * BB);
+        bT.reserve(2 * (size_t)tp * slots * nb * BB);
     }
     double* A = bA.as<double>();
     double* L = bL.as<double>();
@@ -431,7 +432,7 @@ void run_chunk(ptbgpu_ctx* c, const Chunk& ch, const int64_t* ndim, const int64_
     bf16* clo = plane(5);
     bf16* phi = plane(6);
     bf16* plo = plane(7);
-    auto traj = [&](int k, int j) { return bT.as<bf16>() + (size_t)(3 * k + j) * nb * BB; };
+    auto traj = [&](int k, int j) { return j < tp ? bT.as<bf16>() + (size_t)(tp * k + j) * nb * BB : nullptr; };
 
     // ---- unpack, pad, Cholesky, A = L^-1 H L^-T ----
     PTB_CUDA(cudaMemsetAsync(A, 0, 8 * (size_t)nb * BB, s));
@@ -962,7 +963,8 @@ void tc_purify_grouped(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const 
     std::vector<Chunk> chunks;
     for (size_t p = 0; p < idx.size();) {
         const int64_t B = round_up(ndim[idx[p]], 256);
-        const double per = (double)B * B * (mixed ? 88.0 + 6.0 * slots : 40.0) + 24.0 * (double)B * B;
+        const double per = (double)B * B * (mixed ? 88.0 + 2.0 * (o->split3_iters >= 0 ? 3 : 2) * slots : 40.0) +
+                           24.0 * (double)B * B;
         Chunk ch{B, {}};
         while (p < idx.size() && round_up(ndim[idx[p]], 256) == B &&
                (ch.ids.empty() || (double)(ch.ids.size() + 1) * per <= budget)) {

@@ -109,6 +109,7 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
     tc_fence_after();
     if (ok && !aborted) {
         const bool square = (EPI == EPI_SP2) ? (ep.sq_flag[rb / ld] != 0) : true;
+        const bool w3 = ep.lo2 != nullptr;   // third plane written (kept only for three-plane products)
         for (int c0 = 0; c0 < BN; c0 += 32) {
             uint32_t v[32];
             __syncwarp();   // lanes may have taken different paths in the previous chunk
@@ -129,7 +130,7 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
                 float4* xo = reinterpret_cast<float4*>(ep.out + r * ld + cbase);
                 uint4* ho = reinterpret_cast<uint4*>(ep.hi + r * ld + cbase);
                 uint4* mo = reinterpret_cast<uint4*>(ep.lo + r * ld + cbase);
-                uint4* lo = reinterpret_cast<uint4*>(ep.lo2 + r * ld + cbase);
+                uint4* lo = w3 ? reinterpret_cast<uint4*>(ep.lo2 + r * ld + cbase) : nullptr;
 #pragma unroll
                 for (int j8 = 0; j8 < 4; ++j8) {
                     float val[8];
@@ -155,14 +156,14 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
                             ep.out[m] = val[t];
                             ep.hi[m] = hh[t];
                             ep.lo[m] = mm[t];
-                            ep.lo2[m] = ll[t];
+                            if (w3) ep.lo2[m] = ll[t];
                         }
                     }
                     xo[2 * j8] = make_float4(val[0], val[1], val[2], val[3]);
                     xo[2 * j8 + 1] = make_float4(val[4], val[5], val[6], val[7]);
                     ho[j8] = *reinterpret_cast<const uint4*>(hh);
                     mo[j8] = *reinterpret_cast<const uint4*>(mm);
-                    lo[j8] = *reinterpret_cast<const uint4*>(ll);
+                    if (w3) lo[j8] = *reinterpret_cast<const uint4*>(ll);
                 }
             } else {
                 // chunk straddles the diagonal: scalar path, c >= r only
@@ -178,7 +179,7 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
                     ep.out[r * ld + c] = val;
                     ep.hi[r * ld + c] = h;
                     ep.lo[r * ld + c] = m;
-                    ep.lo2[r * ld + c] = l;
+                    if (w3) ep.lo2[r * ld + c] = l;
                     if (c == rl) {
                         tr += dv;
                         ss += dv * dv;
@@ -188,7 +189,7 @@ __device__ __forceinline__ void tc_epilogue(const EpiParams& ep, uint32_t tmem, 
                         ep.out[mi] = val;
                         ep.hi[mi] = h;
                         ep.lo[mi] = m;
-                        ep.lo2[mi] = l;
+                        if (w3) ep.lo2[mi] = l;
                     }
                 }
             }
@@ -606,8 +607,8 @@ int launch_product(cudaStream_t s, int epi, int np, long long ld, const void* co
     const int bn = np == 2 ? 256 : 128;
     for (int p = 0; p < prods.n; ++p)
         PTB_CHECK(prods.a[p] < np && prods.b[p] < np, PTBGPU_EINVAL, "product references a missing plane");
-    PTB_CHECK(epi != EPI_SP2 || (ep.lo2 != nullptr && ep.lo != nullptr), PTBGPU_EINVAL,
-              "the SP2 epilogue writes three planes");
+    PTB_CHECK(epi != EPI_SP2 || (ep.hi != nullptr && ep.lo != nullptr), PTBGPU_EINVAL,
+              "the SP2 epilogue writes at least two planes");
     // returns the number of per-CTA stats partials the launch writes
     auto run = [&](int choice) {
         const bool pair = choice >= kPairKernel;

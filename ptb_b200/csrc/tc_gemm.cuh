@@ -41,7 +41,7 @@ struct EpiParams {
     float* out;               // EPI_FULL: C;  EPI_SP2: next iterate (FP32)
     __nv_bfloat16* hi;        // EPI_SP2: next iterate, bf16 hi plane
     __nv_bfloat16* lo;        // EPI_SP2: next iterate, bf16 mid plane  (x - hi)
-    __nv_bfloat16* lo2;       // EPI_SP2: next iterate, bf16 lo plane   (x - hi - mid)
+    __nv_bfloat16* lo2;       // EPI_SP2: next iterate, bf16 lo plane   (x - hi - mid); null: not written
     double* stats;            // EPI_SP2: per-CTA {trace, sum of squares}
 };
 

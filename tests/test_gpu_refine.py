@@ -79,3 +79,17 @@ def test_refine_options_validated(ctx, water8):
         ctx.tc_purify(s.ndim, s.nel, s.Hvec, s.Svec, Options(precision=PREC_MIXED, refine_rounds=17))
     with pytest.raises(PtbGpuError, match="refine_rounds"):
         ctx.tc_purify(s.ndim, s.nel, s.Hvec, s.Svec, Options(precision=PREC_MIXED, refine_tol=-1.0))
+
+
+@pytest.mark.parametrize("split3", [-1, 0, 4])
+def test_three_plane_leading_iterations(ctx, split3):
+    """Pass 1 with no, all, or the first four iterations on three-plane products
+    (the trajectory then keeps a third bf16 plane per iterate): every variant
+    meets the tolerances, single-system and grouped."""
+    s = synth.lattice_instance(2)
+    Hf, Sf, Pd = _dense(s)
+    o = Options(precision=PREC_MIXED, split3_iters=split3)
+    P, st = ctx.tc_purify(s.ndim, s.nel, s.Hvec, s.Svec, o)
+    _check(s, P, Hf, Sf, Pd)
+    Ps, _, _ = ctx.tc_purify_grouped([(s.ndim, s.nel, s.Hvec, s.Svec)], o)
+    _check(s, Ps[0], Hf, Sf, Pd)
