@@ -380,6 +380,40 @@ Prologue orthogonalise(ptbgpu_ctx* c, int64_t n, const double* dHpk, const doubl
     return p;
 }
 
+// L^-1 in place (lower triangle, column-major, leading dimension ld) by
+// recursive halving, L^-1 = [L11^-1 0; -L22^-1 L21 L11^-1  L22^-1]: where the
+// halves are equal and at least 2048, the two products of the off-diagonal
+// block run on the int8 tensor cores (S slices, triangular operands masked and
+// their zero K blocks skipped, written in place); smaller or uneven blocks go
+// to the FP64 routine (cuBLAS trmm, cuSOLVER trtri leaves).
+void trtri_oz(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A, int S) {
+    const int64_t n1 = (n / 2 + 127) / 128 * 128, n2 = n - n1;
+    if (n < 4096 || n1 != n2 || !oz::supported(n1, S)) {
+        dtrtri_lower(c, n, ld, A);
+        return;
+    }
+    double* L11 = A;
+    double* L21 = A + n1;
+    double* L22 = A + n1 + n1 * ld;
+    trtri_oz(c, n1, ld, L11, S);
+    trtri_oz(c, n2, ld, L22, S);
+    const oz::Operand opA = oz_operand(c, 0, n1, S), opB = oz_operand(c, 1, n1, S);
+    oz::OzEpi ep;
+    ep.n = n1;
+    ep.out = L21;
+    ep.ors = 1;
+    ep.ocs = ld;
+    // T = L21 L11^-1: rows of L21 times rows of L11^-T (upper triangular)
+    oz_slice(c, L21, 1, ld, n1, oz::TRI_NONE, opA);
+    oz_slice(c, L11, ld, 1, n1, oz::TRI_UPPER, opB);
+    oz_product(c, oz::OZ_OUT, opA, opB, false, oz::TRI_NONE, oz::TRI_UPPER, ep);
+    // L21 <- -L22^-1 T: rows of L22^-1 (lower triangular) times rows of T^T
+    oz_slice(c, L22, 1, ld, n1, oz::TRI_LOWER, opA);
+    oz_slice(c, L21, ld, 1, n1, oz::TRI_NONE, opB);
+    ep.alpha = -1.0;
+    oz_product(c, oz::OZ_OUT, opA, opB, false, oz::TRI_LOWER, oz::TRI_NONE, ep);
+}
+
 // The same on the int8 tensor cores: L^-1 by cuSOLVER trtri (in place in B_S,
 // lower triangle), T = L^-1 H (lower-triangular A operand: K blocks past the
 // diagonal are skipped), A = T L^-T (symmetric: upper tiles, mirrored).
@@ -399,7 +433,7 @@ Prologue orthogonalise_oz(ptbgpu_ctx* c, int64_t n, const double* dHpk, const do
     const int info = dpotrf_lower(c, n, n, L);
     PTB_CHECK(info == 0, PTBGPU_ENOTSPD, "overlap matrix not positive definite (potrf info=%d)", info);
     phase("potrf");
-    dtrtri_lower(c, n, n, L);
+    trtri_oz(c, n, n, L, S);
     phase("trtri");
     const oz::Operand opL = oz_operand(c, 0, n, S), op1 = oz_operand(c, 1, n, S);
     oz_slice(c, L, 1, n, n, oz::TRI_LOWER, opL);   // rows of L^-1 (column-major storage)

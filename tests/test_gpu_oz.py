@@ -145,3 +145,18 @@ def test_oz_gemm_tmem_a_variant_is_bit_exact(ctx, S, kblock):
         C1 = ctx.oz_gemm(M, N, slices=S, kblock=kblock, variant=1, **kw)
         C2 = ctx.oz_gemm(M, N, slices=S, kblock=kblock, variant=2, **kw)
         assert np.array_equal(C1, C2), kw
+
+
+def test_mixed_path_with_int8_triangular_inverse(ctx):
+    """ndim 5888 = 2 x 2944: the triangular inverse of the Cholesky factor takes
+    its top-level off-diagonal products on the int8 tensor cores.  The mixed
+    result agrees with the library's FP64 path (itself checked against the
+    oracle at smaller sizes) to the mixed-precision tolerances."""
+    s = synth.water_cluster(256, seed=2)
+    assert s.ndim == 5888
+    P, st = ctx.tc_purify(s.ndim, s.nel, s.Hvec, s.Svec, Options(filter=1e-5, precision=PREC_MIXED))
+    P64, _ = ctx.tc_purify(s.ndim, s.nel, s.Hvec, s.Svec, Options(filter=1e-5, precision=PREC_FP64))
+    assert np.max(np.abs(P - P64)) <= 1e-6
+    chk = ctx.check_density(s.ndim, P, ctx.filter_matrix_sym(s.Svec, s.ndim, 1e-5),
+                            ctx.filter_matrix_sym(s.Hvec, s.ndim, 1e-5))
+    assert abs(chk.nel - s.nel) <= 1e-8
