@@ -215,16 +215,30 @@ def build_hs(symbols, xyz, seed: int, amp: float = DEFAULT_AMP, name: str = "sys
     rng = np.random.default_rng(seed + 7919)
     at = aoat - 1
     d = np.sqrt(np.sum((xyz[:, None, :] - xyz[None, :, :]) ** 2, axis=-1))
-    r, c = np.tril_indices(n)                       # packed order: col r, row c <= r
-    rab = d[at[r], at[c]]
-    u = rng.uniform(-1.0, 1.0, size=r.shape[0])
-    hvec = amp * np.exp(-rab) * u
-    diag = r == c
+    npk = n * (n + 1) // 2
+    hvec = np.empty(npk)
+    svec = np.empty(npk)
+    # packed order: column r, rows c <= r; built in column blocks of about 2^24
+    # elements so that large systems fit in host memory (the uniform draws come
+    # from the one generator in order, so the values do not depend on the blocking)
+    r0 = 0
+    while r0 < n:
+        r1 = r0 + 1
+        while r1 < n and (r1 + 1) * (r1 + 2) // 2 - r0 * (r0 + 1) // 2 <= (1 << 24):
+            r1 += 1
+        k0, k1 = r0 * (r0 + 1) // 2, r1 * (r1 + 1) // 2
+        r = np.repeat(np.arange(r0, r1), np.arange(r0 + 1, r1 + 1))
+        c = np.arange(k0, k1) - r * (r + 1) // 2
+        rab = d[at[r], at[c]]
+        u = rng.uniform(-1.0, 1.0, size=k1 - k0)
+        hvec[k0:k1] = amp * np.exp(-rab) * u
+        same_slot = (slots[r] == slots[c]) & (at[r] != at[c])
+        svec[k0:k1] = np.where(same_slot, np.exp(-0.5 * rab * rab), 0.0)
+        r0 = r1
+    dk = np.arange(1, n + 1) * np.arange(2, n + 2) // 2 - 1   # diagonal positions
     onsite = np.where(occ, rng.normal(-0.5, 0.1, size=n), rng.normal(0.3, 0.1, size=n))
-    hvec[diag] = onsite[r[diag]]
-    same_slot = (slots[r] == slots[c]) & (at[r] != at[c])
-    svec = np.where(same_slot, np.exp(-0.5 * rab * rab), 0.0)
-    svec[diag] = 1.0
+    hvec[dk] = onsite
+    svec[dk] = 1.0
     nel = 2 * int(occ.sum())
     return System(name, list(symbols), np.asarray(xyz, dtype=np.float64), aoat, slots, occ,
                   np.ascontiguousarray(hvec), np.ascontiguousarray(svec), nel)
