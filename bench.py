@@ -305,23 +305,54 @@ def run_sm(args, rank, world, local, pg):
     part = None
     if cols == 4:   # the library's seeded k-means (also what the call itself runs without a partition)
         part, _, _ = ctx.kmeans_partition(s.ndim, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, seed=42, opts=o)
-    call = lambda: ctx.sm_stupid_simple(s.ndim, s.nel, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, cols, 2, None, o)
+    if world == 1:
+        call = lambda: ctx.sm_stupid_simple(s.ndim, s.nel, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, cols, 2, None, o)
+    else:
+        # one system over the ranks: a size-balanced share of the submatrices per GPU,
+        # one all-reduce of the electron count per bisection step, one of P at the end
+        from ptb_b200.distributed import DeviceShard, sm_stupid_simple_sharded
+
+        class Shard(DeviceShard):
+            launches = 0
+
+            def prepare(self, ids):
+                st_ = super().prepare(ids)
+                Shard.launches = int(st_.kernel_launches)
+                return st_
+
+        shard = Shard(ctx)
+        call = lambda: sm_stupid_simple_sharded(shard, s.ndim, s.nel, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, cols, 2,
+                                                None, o)
     for _ in range(args.warmup):
         call()
     barrier(pg)
-    stats, walls = [], []
+    stats, walls, evms = [], [], []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
+            torch.cuda.synchronize()
+            barrier(pg)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             t0 = time.perf_counter()
+            e0.record()
             P, st = call()
+            e1.record()
+            torch.cuda.synchronize()
             walls.append(time.perf_counter() - t0)
+            evms.append(e0.elapsed_time(e1))
             stats.append(st)
     clocks = clk.summary()
-    ms = reduce_max(pg, statistics.median(x.ms_solve for x in stats))
+    # one GPU: the library's device time of the call; several: the whole sharded
+    # call between events (the ranks wait on each other inside it), max over ranks
+    ms = reduce_max(pg, statistics.median(x.ms_solve for x in stats) if world == 1 else statistics.median(evms))
     wall = reduce_max(pg, statistics.median(walls))
     if rank != 0:
         ctx.close()
         return
+    if world > 1:
+        info = stats[-1]
+        stats = [type("S", (), {"nsm": info.nsm, "sum_dims": int(np.sum(info.dims)), "max_dim": int(np.max(info.dims)),
+                                "mu_iterations": len(info.trace), "kernel_launches": Shard.launches,
+                                "mu": info.mu, "nel": info.nel})()]
     dims = ctx.sm_plan(s.ndim, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, cols, 2, part, o)
     feig = float(np.sum(7.0 * np.asarray(dims, dtype=np.float64) ** 3))
     cpu, acc = None, {}
@@ -335,9 +366,11 @@ def run_sm(args, rank, world, local, pg):
     npk = s.ndim * (s.ndim + 1) // 2
     line = {
         "metric": METRIC, "value": ms / 1e3, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak" if world == 1 else "strong",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc, "global_batch": world, "seq_len": s.ndim, "parallelism": f"replicas x{world}",
+        "config": {"workload": desc, "global_batch": 1, "seq_len": s.ndim,
+                   "parallelism": "one GPU" if world == 1 else f"submatrices sharded over {world} ranks",
                    "l2": "per call the packed inputs are copied in and unpacked afresh"},
         "submatrices": {"nsm": int(last.nsm), "sum_dims": int(last.sum_dims), "max_dim": int(last.max_dim),
                         "mu_iterations": int(last.mu_iterations)},
