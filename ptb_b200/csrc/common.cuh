@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "ptbgpu.h"
@@ -172,6 +173,10 @@ struct EventTimer {
 };
 
 void log_line(int level, int want, const char* fmt, ...);
+// The reference's timer block (source/timer.f90:194-215 layout: the total under
+// `total_tag`, then "* tag" lines, seconds with 9 decimals), printed from print level 1.
+void log_timer_block(int level, const char* total_tag, double total_s,
+                     const std::vector<std::pair<const char*, double>>& items);
 
 // Launches of this library's kernels by the calling host thread (a context is
 // driven by one thread at a time); the C-ABI layer resets it per call.

@@ -49,6 +49,15 @@ void log_line(int level, int want, const char* fmt, ...) {
     fflush(stdout);
 }
 
+void log_timer_block(int level, const char* total_tag, double total_s,
+                     const std::vector<std::pair<const char*, double>>& items) {
+    if (level < 1) return;
+    fprintf(stdout, "\n%-40s   %15.9f sec\n", total_tag, total_s);
+    for (const auto& it : items) fprintf(stdout, "* %-40s %15.9f sec\n", it.first, it.second);
+    fputc('\n', stdout);
+    fflush(stdout);
+}
+
 }  // namespace ptb
 
 cudaEvent_t ptbgpu_ctx::take_event() {

@@ -1,6 +1,7 @@
 // Dense FP64 density step (the reference's check-mode oracle, solve2) and the
 // density checks of source/metrics.f90, on the device.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <vector>
 
@@ -93,9 +94,16 @@ void solve2_device(ptbgpu_ctx* c, int64_t mode, int64_t n, int64_t nel, int64_t 
     bv.reserve(sizeof(double) * n);
     double* U = bh.as<double>();
     double* B = bs.as<double>();
+    using clk = std::chrono::steady_clock;
+    const int prl = o ? (int)o->print_level : 0;
+    PTB_CUDA(cudaStreamSynchronize(s));
+    const auto t0 = clk::now();
     unpack_sym(s, n, n, dH, U, filter);
     unpack_sym(s, n, n, dS, B, filter);
+    PTB_CUDA(cudaStreamSynchronize(s));
+    const auto t1 = clk::now();
     const int info = dsygvd(c, n, n, U, B, bv.as<double>());
+    const auto t2 = clk::now();
     std::vector<double> e(n);
     PTB_CUDA(cudaMemcpy(e.data(), bv.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost));
     if (mode >= 2) {
@@ -120,6 +128,9 @@ void solve2_device(ptbgpu_ctx* c, int64_t mode, int64_t n, int64_t nel, int64_t 
                            (int)n, &zero, B, (int)n));
     pack_cols(s, n, n, B, dP);
     PTB_CUDA(cudaStreamSynchronize(s));
+    // the reference's closing timer block of solve2 (source/pgtb.f90:1108-1168)
+    log_timer_block(prl, "Total solve2", std::chrono::duration<double>(clk::now() - t0).count(),
+                    {{"sygvd solver", std::chrono::duration<double>(t2 - t1).count()}});
     if (he) std::copy(e.begin(), e.end(), he);
     if (hfocc) std::copy(focc.begin(), focc.end(), hfocc);
     if (st) {

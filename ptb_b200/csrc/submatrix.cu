@@ -1179,11 +1179,16 @@ void sm_finish(ptbgpu_ctx* c, SmPlan& pl, double mu, double* dP) {
 void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* dH, const double* dS, double* dP,
                        int64_t nat, const double* xyz, const int64_t* aoat, int64_t columns, int64_t mode,
                        const int64_t* partition, const ptbgpu_opts* o, ptbgpu_stats* st) {
+    using clk = std::chrono::steady_clock;
+    auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+    const auto t0 = clk::now();
     SmPlan& pl = sm_plan(c, n, dH, dS, nat, xyz, aoat, columns, mode, partition, o);
+    const auto t1 = clk::now();
     const int prl = pl.prl;
     std::vector<int> all(pl.nsm);
     std::iota(all.begin(), all.end(), 0);
     sm_prepare(c, pl, all);
+    const auto t2 = clk::now();
     cudaStream_t s = c->stream;
     DevBuf bmu;
     bmu.reserve(sizeof(MuResult));
@@ -1201,7 +1206,14 @@ void sm_density_device(ptbgpu_ctx* c, int64_t n, int64_t nelref, const double* d
                  (long long)nelref);
     PTB_CHECK(mr.converged, PTBGPU_EITER, "chemical potential bisection did not converge");
     log_line(prl, 1, " iteration of chemical potential converged");
+    const auto t3 = clk::now();
     sm_finish(c, pl, mr.mu, dP);
+    PTB_CUDA(cudaStreamSynchronize(s));
+    const auto t4 = clk::now();
+    // the reference's closing timer block (source/sm.f90:408), its tags in its slot order
+    log_timer_block(prl, "Submatrix", secs(t0, t4),
+                    {{"submatrix combination", secs(t0, t1)}, {"mu iter", secs(t2, t3)},
+                     {"submatrix eigendecomp", secs(t1, t2)}, {"submatrix final iter", secs(t3, t4)}});
     if (st) {
         st->mu = mr.mu;
         st->nel = mr.nel;

@@ -278,3 +278,22 @@ def test_bounded_wait_reports_timeout_and_context_survives(ctx, water8):
     with pytest.raises(PtbGpuError) as ei:
         ctx.selftest_bounded_wait(0)
     assert ei.value.code == api.EINVAL
+
+
+def test_progress_output_parses_like_the_reference(ctx, water8, capfd):
+    """At print level 1 the submatrix step and solve2 print the lines the
+    reference's result collector reads (collect_and_plot_results.py): the
+    'number of submatrices=' line and the closing 'Submatrix' and
+    '* sygvd solver' timer lines in the reference's timer layout."""
+    s = water8
+    P, st = ctx.sm_stupid_simple(s.ndim, s.nel, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, 2, 2, None,
+                                 Options(filter=1e-4, print_level=1))
+    ctx.solve2(1, s.ndim, s.nel, 0, s.Hvec, s.Svec, Options(filter=1e-4, print_level=1))
+    out = capfd.readouterr().out.splitlines()
+    nsm = [int(l.split()[3]) for l in out if l.startswith(" number of submatrices=")]
+    tsm = [float(l.split()[1]) for l in out if l.startswith("Submatrix ")]
+    tsy = [float(l.split()[3]) for l in out if l.startswith("* sygvd solver")]
+    tso = [float(l.split()[2]) for l in out if l.startswith("Total solve2")]
+    assert nsm == [st.nsm]
+    assert len(tsm) == 1 and tsm[0] > 0.0
+    assert len(tsy) == 1 and len(tso) == 1 and 0.0 < tsy[0] <= tso[0]
