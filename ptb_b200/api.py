@@ -489,7 +489,9 @@ class Context:
         """C = A B in FP64 on the int8 tensor cores (4 or 6..8 slices per
         operand row); tri_*: 0 full, 1 lower, 2 upper triangular operand;
         symmetric: only the upper triangle of C is computed and mirrored;
-        variant: 0 default, 1 A from shared memory, 2 A in tensor memory.
+        variant: 0 default, 1 A from shared memory, 2 A in tensor memory,
+        3 A from shared memory on a CTA pair (256-row tiles), 4 128-column
+        tiles summed in two passes over K (kblock 0 or 32).
         timed: returns (C, device milliseconds of the product kernel)."""
         Ah, Bh = _f64(A), _f64(B)
         n = Ah.shape[0]

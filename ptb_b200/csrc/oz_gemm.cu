@@ -21,6 +21,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <climits>
 #include <mutex>
 
 #include "common.cuh"
@@ -37,7 +38,6 @@ using namespace tc::ptx;
 constexpr int THREADS = 256;
 constexpr int kSmemBudget = 196608;
 constexpr int kTmemCols = 512;
-constexpr int kDefaultVariant = V_SMEM_A;
 
 template <int S, int RB>
 struct OzCfg {
@@ -180,6 +180,10 @@ __device__ __forceinline__ void tmem_ldw(uint32_t taddr, uint32_t (&v)[W]) {
     else tmem_ld16(taddr, v);
 }
 
+template <int EPI, int W>
+__device__ __forceinline__ void oz_write(const OzEpi& ep, int64_t r, int64_t cb, const double (&acc)[W], int er,
+                                         const int* __restrict__ eb, double& tr, double& ss);
+
 // W columns [c0, c0 + W) of the tile: combine the S group accumulators
 // (columns g * NT + c0 ..) in FP64, smallest group first, rescale by
 // 2^(e_r + f_c) and write the fused output.
@@ -187,7 +191,6 @@ template <int EPI, int S, int NT, int W>
 __device__ __forceinline__ void oz_epilogue_chunk(const OzEpi& ep, uint32_t tmem, int bi, int bj, int q4, int lane,
                                                   int c0, bool empty_k, int er, const int* __restrict__ eb,
                                                   double& tr, double& ss) {
-    const int64_t n = ep.n;
     const int64_t r = (int64_t)bi * BM + q4 * 32 + lane;
     double acc[W];
 #pragma unroll
@@ -205,8 +208,18 @@ __device__ __forceinline__ void oz_epilogue_chunk(const OzEpi& ep, uint32_t tmem
 #pragma unroll
         for (int j = 0; j < W; ++j) acc[j] = 0.0;
     }
+    oz_write<EPI, W>(ep, r, (int64_t)bj * NT + c0, acc, er, eb, tr, ss);
+}
+
+// Fused output of W finished FP64 sums of row r, columns cb.. (the caller has
+// combined the groups): rescale by 2^(e_r + f_c), general strides (OZ_OUT) or
+// the upper triangle mirrored with the optional SP2 update and the trace /
+// sum-of-squares partials (OZ_SYM).
+template <int EPI, int W>
+__device__ __forceinline__ void oz_write(const OzEpi& ep, int64_t r, int64_t cb, const double (&acc)[W], int er,
+                                         const int* __restrict__ eb, double& tr, double& ss) {
+    const int64_t n = ep.n;
     if (r >= n) return;
-    const int64_t cb = (int64_t)bj * NT + c0;
     if (EPI == OZ_OUT) {
 #pragma unroll
         for (int j = 0; j < W; ++j) {
@@ -539,6 +552,451 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
 }
 
+// CTA-pair variant (cta_group::2, cluster of two): one 256 x 64 tile per pair,
+// UMMA 256x64x32 int8 issued by the leader CTA.  CTA r holds rows 128r..128r+127
+// of the A slices and of the accumulators, and rows 32r..32r+31 of the 64 B
+// rows, so each SM reads its A slice and half the B slice per MMA (5 KB instead
+// of 6 KB of shared memory for 32 tensor cycles of the SM).  Both CTAs' TMA
+// loads count on the leader's "full" mbarrier, which the leader arms with both
+// CTAs' bytes; the leader's commits arrive on the "empty" and accumulator
+// barriers of both CTAs (tcgen05.commit multicast; no multicast loads).  The
+// epilogue is the one-CTA epilogue on each CTA's own 128 rows.  Tiles
+// {pair row block, bj, k0, k1}: the K range covers both halves.
+template <int S, int RB>
+struct OzPairCfg {
+    static constexpr int A_TILE = BM * RB;
+    static constexpr int B_TILE = (BN / 2) * RB;
+    static constexpr int STAGE = S * (A_TILE + B_TILE);
+    static constexpr int STAGES = (kSmemBudget / STAGE) > 4 ? 4 : (kSmemBudget / STAGE);
+    static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+    static constexpr uint32_t LAYOUT = RB == 64 ? 4u : 6u;
+    static constexpr uint32_t SBO = 8u * RB;
+    // kind::i8: D s32, A and B s8, K-major, N = 64, M = 256 (the pair)
+    static constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                      ((uint32_t)(256 >> 4) << 24);
+    static_assert(RB == 64 || RB == 32, "64- or 32-byte K blocks");
+    static_assert(S >= 2 && S * BN <= kTmemCols, "S accumulators of 64 columns fit in tensor memory");
+    static_assert(STAGES >= 2, "at least two pipeline stages");
+    static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0, "tiles keep the swizzle atoms aligned");
+};
+
+template <int EPI, int S, int RB>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
+    k_oz_product_pair(const __grid_constant__ OzMaps maps, const int4* __restrict__ pairs,
+                      const int* __restrict__ ea, const int* __restrict__ eb, OzEpi ep) {
+    using C = OzPairCfg<S, RB>;
+    constexpr int STAGE = C::STAGE;
+    constexpr int STAGES = C::STAGES;
+
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t base_raw = smem_u32(smem_raw);
+    const uint32_t base = (base_raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - base_raw);
+    const uint32_t bar0 = base + STAGES * STAGE;
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+    const uint32_t accum_bar = bar0 + 8u * (2 * STAGES);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + STAGES * STAGE + 8 * (2 * STAGES + 1));
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+    double* red = reinterpret_cast<double*>(gbase + STAGES * STAGE + 128);   // 8 doubles
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const int4 pt = pairs[blockIdx.x >> 1];
+    const int bi = 2 * pt.x + (int)rank, bj = pt.y;
+    const int kb0 = pt.z / RB;
+    const int nk = (pt.w - pt.z) / RB;
+    // an odd row-block count leaves the second half of the last pair past the
+    // operand: it loads the first half's rows again and writes nothing
+    const int nbi = (int)(ep.ldp / BM);
+    const int abi = bi < nbi ? bi : nbi - 1;
+
+    auto a_tile = [&](int s, int p) { return base + s * STAGE + p * C::A_TILE; };
+    auto b_tile = [&](int s, int q) { return base + s * STAGE + S * C::A_TILE + q * C::B_TILE; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(accum_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"((uint32_t)kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();   // both CTAs' barriers are initialised before any remote arrive
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer (both CTAs) ----------------
+        int issued_phase[STAGES];
+        for (int s = 0; s < STAGES; ++s) issued_phase[s] = -1;
+        for (int it = 0; it < nk; ++it) {
+            const int s = it % STAGES, round = it / STAGES;
+            if (round > 0 && !mbar_wait(empty_bar(s), (round - 1) & 1)) {
+                set_err(ep.err, 141);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            if (rank == 0) mbar_expect_tx(full_bar(s), 2 * STAGE);   // both CTAs' bytes
+            const uint32_t fb = mapa_shared(full_bar(s), 0);
+            const int kx = (kb0 + it) * RB;
+            for (int p = 0; p < S; ++p)
+                tma_load_2d_pair(a_tile(s, p), &maps.a, fb, kx, (int)(p * ep.ldp) + abi * BM);
+            for (int q = 0; q < S; ++q)
+                tma_load_2d_pair(b_tile(s, q), &maps.b, fb, kx, (int)(q * ep.ldp) + bj * BN + (int)rank * (BN / 2));
+            issued_phase[s] = round & 1;
+        }
+        // drain: the leader sees every copy of the pair land on its full barriers;
+        // the peer's copies have landed once the leader's MMAs consumed them,
+        // which its accumulator barrier (waited by the epilogue) certifies
+        if (rank == 0)
+            for (int s = 0; s < STAGES; ++s)
+                if (issued_phase[s] >= 0 && !mbar_wait(full_bar(s), (uint32_t)issued_phase[s])) set_err(ep.err, 142);
+    } else if (warp == 1 && lane == 0 && rank == 0) {
+        // ---------------- MMA issuer (leader CTA) ----------------
+        bool ok = true;
+        for (int it = 0; it < nk; ++it) {
+            const int s = it % STAGES, round = it / STAGES;
+            if (!mbar_wait(full_bar(s), round & 1)) {
+                set_err(ep.err, 151);
+                *(volatile int*)abort_flag = 1;
+                ok = false;
+                break;
+            }
+            if (*(volatile int*)abort_flag) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+#pragma unroll
+            for (int k = 0; k < RB / 32; ++k) {
+#pragma unroll
+                for (int p = 0; p < S; ++p) {
+                    const uint64_t ad = sdesc(a_tile(s, p) + k * 32, C::SBO, C::LAYOUT);
+#pragma unroll
+                    for (int q = 0; q < S - p; ++q) {
+                        const uint64_t bd = sdesc(b_tile(s, q) + k * 32, C::SBO, C::LAYOUT);
+                        umma_i8_pair(tmem + (uint32_t)((p + q) * BN), ad, bd, C::IDESC, (it | k | p) != 0);
+                    }
+                }
+            }
+            umma_commit_pair(empty_bar(s), (uint16_t)0x3);
+        }
+        umma_commit_pair(accum_bar, (uint16_t)0x3);   // also on abort so both epilogues' waits end
+        if (!ok) mbar_wait(accum_bar, 0);
+    } else if (warp >= 4) {
+        oz_epilogue<EPI, S, BN>(ep, tmem, accum_bar, abort_flag, red, bi, bj, warp - 4, lane, nk, ea, eb);
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();   // the leader's MMAs have finished reading the peer's shared memory
+    tc_fence_after();
+    if (warp == 2) {
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTmemCols));
+    }
+}
+
+// Wide variant: one CTA per 128 x 128 tile, UMMA 128x128x32 int8.  Every
+// tcgen05.mma instruction costs the tensor pipe a fixed ~17 cycles besides its
+// math (32 cycles at N = 64, 64 at N = 128: measured as tensor-pipe activity of
+// 51 % against 80 % for the issuing pipe in the 64-column kernels), so N = 128
+// halves that overhead per flop.  Eight 128-column int32 accumulators do not
+// fit the 512 TMEM columns, so the groups are split over two passes over K:
+// pass 1 sums the slice pairs of groups GS..S-1 (GS = S - 4, the low-weight
+// groups) and its epilogue combines them in FP64, smallest group first, and
+// parks the partial sum in the output's own storage (OZ_OUT: the element
+// itself; OZ_SYM: the mirrored lower-triangle element, which nothing reads,
+// and a register for the diagonal); pass 2 sums groups 0..GS-1 into the freed
+// columns and the epilogue continues the same FP64 sum from the parked value.
+// The result is bit-identical to the 64-column kernel.  Pass 2 loads only the
+// slices 0..GS-1; its loads overlap the pass-1 epilogue.  K blocks of 32 bytes
+// (32B swizzle): a stage holds S A slices and S B slices of 4 KB each.
+template <int S>
+struct OzWideCfg {
+    static constexpr int NT = 128;
+    static constexpr int RB = 32;
+    static constexpr int GS = S > 4 ? S - 4 : 0;   // first group of pass 1 (0: one pass)
+    static constexpr int A_TILE = BM * RB;
+    static constexpr int B_TILE = NT * RB;
+    static constexpr int STAGE = S * (A_TILE + B_TILE);
+    static constexpr int STAGES = (kSmemBudget / STAGE) > 4 ? 4 : (kSmemBudget / STAGE);
+    static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+    static constexpr uint32_t LAYOUT = 6u;   // SWIZZLE_32B
+    static constexpr uint32_t SBO = 8u * RB;
+    // kind::i8: D s32, A and B s8, K-major, N = 128, M = 128
+    static constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) |
+                                      ((uint32_t)(BM >> 4) << 24);
+    static_assert((S - GS) * NT <= kTmemCols, "one pass's accumulators fit in tensor memory");
+    static_assert(STAGES >= 2, "at least two pipeline stages");
+    static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0, "tiles keep the swizzle atoms aligned");
+};
+
+// Bounded wait that also ends when the abort flag is raised; true when the phase completed.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t bar, uint32_t parity, const int* abort_flag) {
+    const uint64_t t0 = gtimer();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*(volatile const int*)abort_flag) return false;
+        if (gtimer() - t0 > kTimeoutNs) return false;
+    }
+}
+
+// Sum of groups g = g_hi down to g_lo (accumulator of g at column (g - gc) * 128)
+// of 32 columns [c0, c0 + 32) into acc, smallest group first.
+__device__ __forceinline__ void oz_wide_groups(uint32_t tmem, int q4, int c0, int g_hi, int g_lo, int gc,
+                                               double (&acc)[32]) {
+#pragma unroll 1
+    for (int g = g_hi; g >= g_lo; --g) {
+        uint32_t v[32];
+        __syncwarp();
+        tmem_ld32(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)((g - gc) * 128 + c0), v);
+        const double w = pow2i(-7 * (g + 2));
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[j] += (double)(int)v[j] * w;
+    }
+}
+
+template <int EPI, int S>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_oz_product_w(const __grid_constant__ OzMaps maps, const int4* __restrict__ tiles, const int* __restrict__ ea,
+                   const int* __restrict__ eb, OzEpi ep) {
+    using C = OzWideCfg<S>;
+    constexpr int STAGE = C::STAGE;
+    constexpr int STAGES = C::STAGES;
+    constexpr int GS = C::GS;
+    constexpr int NT = C::NT;
+
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t base_raw = smem_u32(smem_raw);
+    const uint32_t base = (base_raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - base_raw);
+    const uint32_t bar0 = base + STAGES * STAGE;
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+    const uint32_t accum_bar = bar0 + 8u * (2 * STAGES);
+    const uint32_t free_bar = bar0 + 8u * (2 * STAGES + 1);   // pass-1 accumulators drained
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + STAGES * STAGE + 8 * (2 * STAGES + 2));
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+    double* red = reinterpret_cast<double*>(gbase + STAGES * STAGE + 128);   // 8 doubles
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int4 tile = tiles[blockIdx.x];
+    const int bi = tile.x, bj = tile.y;
+    const int kb0 = tile.z / C::RB;
+    const int nk = (tile.w - tile.z) / C::RB;         // K steps of one pass
+    const int ntot = GS > 0 ? 2 * nk : nk;            // both passes
+
+    auto a_tile = [&](int s, int p) { return base + s * STAGE + p * C::A_TILE; };
+    auto b_tile = [&](int s, int q) { return base + s * STAGE + S * C::A_TILE + q * C::B_TILE; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(accum_bar, 1);
+        mbar_init(free_bar, 4);   // one arrival per epilogue warp
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"((uint32_t)kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer: pass 1 (all S slices), pass 2 (slices 0..GS-1) ----------------
+        int issued_phase[STAGES];
+        for (int s = 0; s < STAGES; ++s) issued_phase[s] = -1;
+        for (int it = 0; it < ntot; ++it) {
+            const int s = it % STAGES, round = it / STAGES;
+            if (round > 0 && !mbar_wait(empty_bar(s), (round - 1) & 1)) {
+                set_err(ep.err, 161);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            const int ns = it < nk ? S : GS;
+            mbar_expect_tx(full_bar(s), (uint32_t)(ns * (C::A_TILE + C::B_TILE)));
+            const int kx = (kb0 + (it < nk ? it : it - nk)) * C::RB;
+            for (int p = 0; p < ns; ++p)
+                tma_load_2d(a_tile(s, p), &maps.a, full_bar(s), kx, (int)(p * ep.ldp) + bi * BM);
+            for (int q = 0; q < ns; ++q)
+                tma_load_2d(b_tile(s, q), &maps.b, full_bar(s), kx, (int)(q * ep.ldp) + bj * NT);
+            issued_phase[s] = round & 1;
+        }
+        for (int s = 0; s < STAGES; ++s)
+            if (issued_phase[s] >= 0 && !mbar_wait(full_bar(s), (uint32_t)issued_phase[s])) set_err(ep.err, 162);
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer ----------------
+        int commits = 0;
+        for (int it = 0; it < ntot; ++it) {
+            const int s = it % STAGES, round = it / STAGES;
+            const bool pass2 = GS > 0 && it >= nk;
+            if (GS > 0 && it == nk) {
+                // end of pass 1: hand the accumulators to the epilogue, wait until drained
+                umma_commit(accum_bar);
+                ++commits;
+                if (!mbar_wait_or_abort(free_bar, 0, abort_flag)) {
+                    set_err(ep.err, 173);
+                    *(volatile int*)abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+            }
+            if (!mbar_wait(full_bar(s), round & 1)) {
+                set_err(ep.err, 171);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            tc_fence_after();
+            const int itp = pass2 ? it - nk : it;
+            if (!pass2) {
+#pragma unroll
+                for (int p = 0; p < S; ++p) {
+                    const uint64_t ad = sdesc(a_tile(s, p), C::SBO, C::LAYOUT);
+#pragma unroll
+                    for (int q = (GS - p > 0 ? GS - p : 0); q < S - p; ++q) {
+                        const uint64_t bd = sdesc(b_tile(s, q), C::SBO, C::LAYOUT);
+                        // p = 0 opens every accumulator of the pass on its first K step
+                        umma_i8(tmem + (uint32_t)((p + q - GS) * NT), ad, bd, C::IDESC, (itp | p) != 0);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int p = 0; p < GS; ++p) {
+                    const uint64_t ad = sdesc(a_tile(s, p), C::SBO, C::LAYOUT);
+#pragma unroll
+                    for (int q = 0; q < GS - p; ++q) {
+                        const uint64_t bd = sdesc(b_tile(s, q), C::SBO, C::LAYOUT);
+                        umma_i8(tmem + (uint32_t)((p + q) * NT), ad, bd, C::IDESC, (itp | p) != 0);
+                    }
+                }
+            }
+            umma_commit(empty_bar(s));
+        }
+        if (GS > 0 && nk == 0) {   // empty K range: both epilogue phases still complete
+            umma_commit(accum_bar);
+            ++commits;
+            if (!mbar_wait_or_abort(free_bar, 0, abort_flag)) set_err(ep.err, 174);
+        }
+        umma_commit(accum_bar);
+        ++commits;
+        // every MMA of the tile has completed before the block tears down
+        if (!mbar_wait(accum_bar, (uint32_t)((commits - 1) & 1))) set_err(ep.err, 175);
+    } else if (warp >= 4) {
+        // ---------------- epilogue: warp w drains TMEM lanes 32 (w - 4) .. ----------------
+        const int q4 = warp - 4;
+        const int64_t n = ep.n, r = (int64_t)bi * BM + q4 * 32 + lane;
+        const int64_t ld = ep.ors;
+        double tr = 0.0, ss = 0.0, dlo = 0.0;
+        bool live = true;
+        if constexpr (GS > 0) {
+            const bool ok = __all_sync(0xffffffffu, mbar_wait_or_abort(accum_bar, 0, abort_flag));
+            const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
+            tc_fence_after();
+            if (!ok && !aborted && lane == 0) set_err(ep.err, 180);
+            live = ok && !aborted;
+            if (live) {
+#pragma unroll 1
+                for (int c0 = 0; c0 < NT; c0 += 32) {
+                    double acc[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                    oz_wide_groups(tmem, q4, c0, S - 1, GS, GS, acc);
+                    const int64_t cb = (int64_t)bj * NT + c0;
+                    if (r < n) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int64_t c = cb + j;
+                            if (c >= n) continue;
+                            if (EPI == OZ_OUT) ep.out[r * ep.ors + c * ep.ocs] = acc[j];
+                            else if (c > r) ep.out[c + r * ld] = acc[j];
+                            else if (c == r) dlo = acc[j];
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(free_bar) : "memory");
+        }
+        if (live) {
+            const uint32_t par = GS > 0 ? 1u : 0u;
+            const bool ok = __all_sync(0xffffffffu, mbar_wait_or_abort(accum_bar, par, abort_flag));
+            const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
+            tc_fence_after();
+            if (!ok && !aborted && lane == 0) set_err(ep.err, 181);
+            if (ok && !aborted) {
+                const int er = r < n ? ea[r] : 0;
+#pragma unroll 1
+                for (int c0 = 0; c0 < NT; c0 += 32) {
+                    double acc[32];
+                    const int64_t cb = (int64_t)bj * NT + c0;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int64_t c = cb + j;
+                        double v = 0.0;
+                        if (GS > 0 && r < n && c < n) {
+                            if (EPI == OZ_OUT) v = ep.out[r * ep.ors + c * ep.ocs];
+                            else if (c > r) v = ep.out[c + r * ld];
+                            else if (c == r) v = dlo;
+                        }
+                        acc[j] = v;
+                    }
+                    if (GS > 0) oz_wide_groups(tmem, q4, c0, GS - 1, 0, 0, acc);
+                    else oz_wide_groups(tmem, q4, c0, S - 1, 0, 0, acc);
+                    if (nk == 0) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                    }
+                    oz_write<EPI, 32>(ep, r, cb, acc, er, eb, tr, ss);
+                }
+            }
+        }
+        if (EPI == OZ_SYM && ep.stats) {
+            for (int o = 16; o > 0; o >>= 1) {
+                tr += __shfl_xor_sync(0xffffffffu, tr, o);
+                ss += __shfl_xor_sync(0xffffffffu, ss, o);
+            }
+            if (lane == 0) {
+                red[2 * q4] = tr;
+                red[2 * q4 + 1] = ss;
+            }
+            asm volatile("bar.sync 1, 128;" ::: "memory");   // epilogue warps only
+            if (q4 == 0 && lane == 0) {
+                ep.stats[2 * blockIdx.x] = red[0] + red[2] + red[4] + red[6];
+                ep.stats[2 * blockIdx.x + 1] = red[1] + red[3] + red[5] + red[7];
+            }
+        }
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 2) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTmemCols));
+    }
+}
+
 // ---- host side ---------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -582,6 +1040,33 @@ void launch_t(cudaStream_t s, const OzMaps& maps, const int4* tiles, int ntiles,
     count_launch();
 }
 
+template <int EPI, int S, int RB>
+void launch_p(cudaStream_t s, const OzMaps& maps, const int4* pairs, int npairs, const Operand& a,
+              const Operand& b, const OzEpi& ep) {
+    using C = OzPairCfg<S, RB>;
+    static const bool attr = [] {   // thread-safe one-time setup
+        PTB_CUDA(cudaFuncSetAttribute(k_oz_product_pair<EPI, S, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      C::SMEM));
+        return true;
+    }();
+    (void)attr;
+    k_oz_product_pair<EPI, S, RB><<<2 * npairs, THREADS, C::SMEM, s>>>(maps, pairs, a.exps, b.exps, ep);
+    count_launch();
+}
+
+template <int EPI, int S>
+void launch_w(cudaStream_t s, const OzMaps& maps, const int4* tiles, int ntiles, const Operand& a,
+              const Operand& b, const OzEpi& ep) {
+    using C = OzWideCfg<S>;
+    static const bool attr = [] {   // thread-safe one-time setup
+        PTB_CUDA(cudaFuncSetAttribute(k_oz_product_w<EPI, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+        return true;
+    }();
+    (void)attr;
+    k_oz_product_w<EPI, S><<<ntiles, THREADS, C::SMEM, s>>>(maps, tiles, a.exps, b.exps, ep);
+    count_launch();
+}
+
 constexpr int ta_tile_n(int S) { return S >= 7 ? 48 : 64; }
 
 template <int EPI, int S, int RB>
@@ -607,6 +1092,11 @@ void launch_s(cudaStream_t s, int rb, int variant, const OzMaps& maps, const int
     if (variant == V_TMEM_A) {
         if (rb == 64) launch_ta<EPI, S, 64>(s, maps, tiles, ntiles, a, b, ep);
         else launch_ta<EPI, S, 32>(s, maps, tiles, ntiles, a, b, ep);
+    } else if (variant == V_PAIR) {
+        if (rb == 64) launch_p<EPI, S, 64>(s, maps, tiles, ntiles, a, b, ep);
+        else launch_p<EPI, S, 32>(s, maps, tiles, ntiles, a, b, ep);
+    } else if (variant == V_WIDE) {
+        launch_w<EPI, S>(s, maps, tiles, ntiles, a, b, ep);
     } else {
         if (rb == 64) launch_t<EPI, S, 64>(s, maps, tiles, ntiles, a, b, ep);
         else launch_t<EPI, S, 32>(s, maps, tiles, ntiles, a, b, ep);
@@ -651,12 +1141,20 @@ void slice(cudaStream_t s, const double* M, int64_t rs, int64_t cs, int64_t n, i
     PTB_CUDA(cudaGetLastError());
 }
 
-int resolve_variant(int variant) { return variant == V_DEFAULT ? kDefaultVariant : variant; }
+int resolve_variant(int variant, int S, int rb) {
+    if (variant != V_DEFAULT) return variant;
+    // 128-column tiles measured 5-15 % faster with 7 or 8 slices at ndim 4096-11776
+    // (N = 128 MMAs), within 1 % either way with 6; they take 32-byte K blocks only
+    return S >= 7 && rb != 64 ? V_WIDE : V_SMEM_A;
+}
 
-int tile_n(int S, int variant) { return resolve_variant(variant) == V_TMEM_A ? ta_tile_n(S) : BN; }
+int tile_n(int S, int variant) {
+    PTB_CHECK(variant != V_DEFAULT, PTBGPU_EINVAL, "kernel variant not resolved");
+    return variant == V_TMEM_A ? ta_tile_n(S) : variant == V_WIDE ? 128 : BN;
+}
 
 std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int bn) {
-    PTB_CHECK(bn == 64 || bn == 48, PTBGPU_EINVAL, "tile width must be 64 or 48");
+    PTB_CHECK(bn == 128 || bn == 64 || bn == 48, PTBGPU_EINVAL, "tile width must be 128, 64 or 48");
     // column tiles may overhang ldp (the operand rows there are padding or the
     // next plane; those columns are never written)
     const int nbi = (int)(ldp / BM), nbj = (int)((ldp + bn - 1) / bn);
@@ -679,10 +1177,50 @@ std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int 
     return t;
 }
 
+std::vector<int4> make_pair_tiles(int64_t ldp, bool upper, int a_tri, int b_tri) {
+    const std::vector<int4> one = make_tiles(ldp, upper, a_tri, b_tri, BN);
+    const int nbi = (int)(ldp / BM), nbj = (int)(ldp / BN), np = (nbi + 1) / 2;
+    // K range of each (pair, bj) over the halves make_tiles keeps; k1 = 0: none kept
+    std::vector<int2> kr((size_t)np * nbj, make_int2(INT_MAX, 0));
+    for (const int4& x : one) {
+        int2& r = kr[(size_t)(x.x / 2) * nbj + x.y];
+        r.x = std::min(r.x, x.z);
+        r.y = std::max(r.y, x.w);
+    }
+    std::vector<int4> t;
+    const int G = 8;   // pair blocks per column sweep (16 row blocks, as make_tiles)
+    for (int g0 = 0; g0 < np; g0 += G)
+        for (int bj = 0; bj < nbj; ++bj)
+            for (int p = g0; p < std::min(np, g0 + G); ++p) {
+                const int2 r = kr[(size_t)p * nbj + bj];
+                if (r.y > 0) t.push_back(make_int4(p, bj, r.x, r.y));
+            }
+    std::stable_sort(t.begin(), t.end(), [](const int4& x, const int4& y) { return x.w - x.z > y.w - y.z; });
+    return t;
+}
+
+std::vector<int4> build_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int S, int variant) {
+    return variant == V_PAIR ? make_pair_tiles(ldp, upper, a_tri, b_tri)
+                             : make_tiles(ldp, upper, a_tri, b_tri, tile_n(S, variant));
+}
+
+int grid_ctas(int ntiles, int variant) { return variant == V_PAIR ? 2 * ntiles : ntiles; }
+
+double tile_ops(const std::vector<int4>& tiles, int S, int variant) {
+    double kk = 0.0;
+    for (const int4& x : tiles) kk += (double)(x.w - x.z);
+    const int rows = variant == V_PAIR ? 2 * BM : BM;
+    return 2.0 * rows * tile_n(S, variant) * kk * (double)(S * (S + 1) / 2);
+}
+
 void product(cudaStream_t s, int epi, const Operand& a, const Operand& b, const int4* tiles_dev, int ntiles,
              const OzEpi& ep, int rb, int variant) {
-    variant = resolve_variant(variant);
-    PTB_CHECK(variant == V_SMEM_A || variant == V_TMEM_A, PTBGPU_EINVAL, "bad kernel variant %d", variant);
+    PTB_CHECK(variant == V_SMEM_A || variant == V_TMEM_A || variant == V_PAIR || variant == V_WIDE, PTBGPU_EINVAL,
+              "bad kernel variant %d", variant);
+    if (variant == V_WIDE) {
+        PTB_CHECK(rb == 0 || rb == 32, PTBGPU_EINVAL, "the 128-column kernel takes 32-byte K blocks");
+        rb = 32;
+    }
     if (rb == 0) rb = 64;   // measured faster than 32 at ndim 11776 (S = 7 and 8)
     PTB_CHECK(rb == 32 || rb == 64, PTBGPU_EINVAL, "K block must be 32 or 64 bytes");
     PTB_CHECK(a.S == b.S && a.ldp == b.ldp && a.ldp == ep.ldp, PTBGPU_EINVAL, "operands do not match");
@@ -692,7 +1230,8 @@ void product(cudaStream_t s, int epi, const Operand& a, const Operand& b, const 
     if (ntiles == 0) return;
     OzMaps maps;
     encode_planes(&maps.a, a, BM, rb);
-    encode_planes(&maps.b, b, tile_n(a.S, variant), rb);
+    // a CTA pair splits the 64 B rows of a tile between its two CTAs
+    encode_planes(&maps.b, b, variant == V_PAIR ? BN / 2 : tile_n(a.S, variant), rb);
     if (epi == OZ_OUT) launch_e<OZ_OUT>(s, a.S, rb, variant, maps, tiles_dev, ntiles, a, b, ep);
     else launch_e<OZ_SYM>(s, a.S, rb, variant, maps, tiles_dev, ntiles, a, b, ep);
     PTB_CUDA(cudaGetLastError());

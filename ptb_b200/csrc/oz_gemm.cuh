@@ -66,9 +66,15 @@ void slice(cudaStream_t s, const double* M, int64_t rs, int64_t cs, int64_t n, i
 
 // Kernel variants: A slices re-read from shared memory by every MMA (64-column
 // tiles), or copied once per K step into tensor memory (48-column tiles for 7
-// or 8 slices, 64 for fewer).  Both give bit-identical results.
-enum Variant : int { V_DEFAULT = 0, V_SMEM_A = 1, V_TMEM_A = 2 };
-int tile_n(int S, int variant = V_DEFAULT);   // output columns per tile
+// or 8 slices, 64 for fewer), or the shared-memory variant on a CTA pair
+// (cta_group::2: 256-row tiles, each SM loads half of the 64 B rows), or
+// 128-column tiles whose accumulator groups are summed in two passes over K
+// (32-byte K blocks only).  All give bit-identical results.
+enum Variant : int { V_DEFAULT = 0, V_SMEM_A = 1, V_TMEM_A = 2, V_PAIR = 3, V_WIDE = 4 };
+// The variant V_DEFAULT stands for with S slices and rb-byte K blocks (0 = the
+// variant's default); the functions below take resolved variants only.
+int resolve_variant(int variant, int S, int rb);
+int tile_n(int S, int variant);   // output columns per tile
 
 // Tiles {bi, bj, k0, k1}: 128-row blocks of ldp by bn-column blocks (the last
 // may overhang), all or only those touching the upper triangle; the K range of
@@ -76,11 +82,24 @@ int tile_n(int S, int variant = V_DEFAULT);   // output columns per tile
 // (rows of A) or B (rows of B).  Longest K ranges first.
 std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int bn);
 
-// C(i,j) = sum_k A(i,k) B(j,k) over the listed tiles, which must be built
-// with tile_n(S, variant).  rb: K bytes per stage, 64 (64B swizzle) or 32
-// (32B swizzle); 0 = the default.
+// CTA-pair tiles {pair row block p (rows 256p..256p+255), bj, k0, k1}: pairs
+// with a half that touches the upper triangle (when `upper`), K range = the
+// union of the ranges of those halves (the extra blocks of a triangular operand
+// are zero slices).  Longest K ranges first.
+std::vector<int4> make_pair_tiles(int64_t ldp, bool upper, int a_tri, int b_tri);
+
+// The tile list `product` expects for `variant`, the CTAs it launches for it
+// (one per tile entry, two per pair entry; OZ_SYM writes one stats pair per
+// CTA), and the int8 multiply-adds x 2 the tiles execute.
+std::vector<int4> build_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int S, int variant);
+int grid_ctas(int ntiles, int variant);
+double tile_ops(const std::vector<int4>& tiles, int S, int variant);
+
+// C(i,j) = sum_k A(i,k) B(j,k) over the listed tiles, which must be built by
+// build_tiles for the same (resolved) variant.  rb: K bytes per stage, 64 (64B
+// swizzle) or 32 (32B swizzle); 0 = the variant's default.
 void product(cudaStream_t s, int epi, const Operand& a, const Operand& b, const int4* tiles_dev, int ntiles,
-             const OzEpi& ep, int rb = 0, int variant = V_DEFAULT);
+             const OzEpi& ep, int rb, int variant);
 
 }  // namespace oz
 }  // namespace ptb

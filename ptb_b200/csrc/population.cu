@@ -160,8 +160,8 @@ void mlpop2_diag_device(ptbgpu_ctx* c, int64_t n, const double* dPpk, const floa
     oa.S = ob.S = S;
     oz::slice(s, P, 1, n, n, oz::TRI_NONE, oa, brm.as<unsigned long long>());
     oz::slice(s, S1, n, 1, n, oz::TRI_NONE, ob, brm.as<unsigned long long>());
-    const int bn = oz::tile_n(S);
-    const std::vector<int4> t = oz::make_tiles(ldp, false, oz::TRI_NONE, oz::TRI_NONE, bn);
+    const int variant = oz::resolve_variant(oz::V_DEFAULT, S, 0);
+    const std::vector<int4> t = oz::build_tiles(ldp, false, oz::TRI_NONE, oz::TRI_NONE, S, variant);
     DevBuf& bt = c->buf(B_OZT);
     bt.reserve(sizeof(int4) * t.size());
     PTB_CUDA(cudaMemcpyAsync(bt.ptr, t.data(), sizeof(int4) * t.size(), cudaMemcpyHostToDevice, s));
@@ -175,12 +175,10 @@ void mlpop2_diag_device(ptbgpu_ctx* c, int64_t n, const double* dPpk, const floa
     PTB_CUDA(cudaMemsetAsync(&c->flags->timeout, 0, sizeof(int), s));
     cudaEvent_t e0 = c->take_event(), e1 = c->take_event();
     PTB_CUDA(cudaEventRecord(e0, s));
-    oz::product(s, oz::OZ_OUT, oa, ob, bt.as<int4>(), (int)t.size(), ep);
+    oz::product(s, oz::OZ_OUT, oa, ob, bt.as<int4>(), (int)t.size(), ep, 0, variant);
     PTB_CUDA(cudaEventRecord(e1, s));
     c->timed.push_back({2, e0, e1});
-    double kk = 0.0;
-    for (const int4& x : t) kk += (double)(x.w - x.z);
-    c->oz_ops += 2.0 * oz::BM * bn * kk * (double)(S * (S + 1) / 2);
+    c->oz_ops += oz::tile_ops(t, S, variant);
     k_diag_s2c<<<(unsigned)((n + 31) / 32), dim3(32, 8), 0, s>>>(n, s2, Cm, bxd.as<double>());
     count_launch();
     PTB_CUDA(cudaGetLastError());

@@ -311,25 +311,23 @@ void oz_slice(ptbgpu_ctx* c, const double* M, int64_t rs, int64_t cs, int64_t n,
 }
 
 // One product over a freshly uploaded tile list, bracketed by CUDA events.
-// Returns the tile count (the number of per-tile stats of OZ_SYM).
+// Returns the CTA count (the number of per-CTA stats of OZ_SYM).
 int oz_product(ptbgpu_ctx* c, int epi, const oz::Operand& a, const oz::Operand& b, bool upper, int tri_a,
                int tri_b, oz::OzEpi ep, int rb = 0, int variant = oz::V_DEFAULT) {
-    const int bn = oz::tile_n(a.S, variant);
-    const std::vector<int4> t = oz::make_tiles(a.ldp, upper, tri_a, tri_b, bn);
+    variant = oz::resolve_variant(variant, a.S, rb);
+    const std::vector<int4> t = oz::build_tiles(a.ldp, upper, tri_a, tri_b, a.S, variant);
     DevBuf& bt = c->buf(B_OZT);
     bt.reserve(sizeof(int4) * t.size());
     PTB_CUDA(cudaMemcpyAsync(bt.ptr, t.data(), sizeof(int4) * t.size(), cudaMemcpyHostToDevice, c->stream));
     ep.ldp = a.ldp;
     if (!ep.err) ep.err = &c->flags->timeout;
-    double kk = 0.0;
-    for (const int4& x : t) kk += (double)(x.w - x.z);
-    c->oz_ops += 2.0 * oz::BM * bn * kk * (double)(a.S * (a.S + 1) / 2);
+    c->oz_ops += oz::tile_ops(t, a.S, variant);
     cudaEvent_t e0 = c->take_event(), e1 = c->take_event();
     PTB_CUDA(cudaEventRecord(e0, c->stream));
     oz::product(c->stream, epi, a, b, bt.as<int4>(), (int)t.size(), ep, rb, variant);
     PTB_CUDA(cudaEventRecord(e1, c->stream));
     c->timed.push_back({2, e0, e1});
-    return (int)t.size();
+    return oz::grid_ctas((int)t.size(), variant);
 }
 
 // Slices of the orthogonalisation products: one fewer than the cleanup squares
@@ -710,8 +708,9 @@ bool sp2_mixed(ptbgpu_ctx* c, int64_t n, int64_t nel, const Prologue& pro, int m
             // before writing it; the mirrored lower triangle is never read); the error
             // of each iterate is checked before its square is taken
             DevBuf& bst = c->buf(B_OZS);
-            // per-tile partials: at most (rows / 128) x ceil(cols / 48) tiles for either kernel variant
-            bst.reserve(sizeof(double) * 2 * (size_t)(oz::padded(n) / oz::BM) * (size_t)((oz::padded(n) + 47) / 48));
+            // per-CTA partials: at most (rows / 128 + 1) x ceil(cols / 48) CTAs for any kernel variant
+            bst.reserve(sizeof(double) * 2 * (size_t)(oz::padded(n) / oz::BM + 1) *
+                        (size_t)((oz::padded(n) + 47) / 48));
             std::vector<double> hst;
             double trX = trace_dev(c, n, n, X);
             const double f0 = frob_dev(c, n, n, X);

@@ -147,6 +147,49 @@ def test_oz_gemm_tmem_a_variant_is_bit_exact(ctx, S, kblock):
         assert np.array_equal(C1, C2), kw
 
 
+@pytest.mark.parametrize("S", [4, 6, 7, 8])
+@pytest.mark.parametrize("kblock", [32, 64])
+@pytest.mark.parametrize("n", [300, 700])
+def test_oz_gemm_pair_variant_is_bit_exact(ctx, S, kblock, n):
+    """The CTA-pair kernel (256-row tiles, K ranges merged over both halves)
+    sums the same exact int32 products as the one-CTA kernel; n = 300 gives an
+    odd count of 128-row blocks, so the last pair has a half past the operand."""
+    rng = np.random.default_rng(S * 1000 + kblock + n)
+    A = rng.standard_normal((n, n))
+    B = rng.standard_normal((n, n))
+    X = 0.5 * (A + A.T)
+    for kw in ({}, {"symmetric": True}, {"tri_a": 1, "tri_b": 2}, {"tri_a": 2}, {"tri_b": 1},
+               {"tri_a": 1, "symmetric": True}):
+        M = X if kw.get("symmetric") else A
+        N = X if kw.get("symmetric") else B
+        C1 = ctx.oz_gemm(M, N, slices=S, kblock=kblock, variant=1, **kw)
+        C3 = ctx.oz_gemm(M, N, slices=S, kblock=kblock, variant=3, **kw)
+        assert np.array_equal(C1, C3), kw
+
+
+@pytest.mark.parametrize("S", [4, 6, 7, 8])
+@pytest.mark.parametrize("n", [300, 700, 1000])
+def test_oz_gemm_wide_variant_is_bit_exact(ctx, S, n):
+    """The 128-column kernel sums the low-weight accumulator groups in a first
+    pass over K, parks their FP64 sum in the output and continues it with the
+    other groups in a second pass: the same FP64 sum in the same order as the
+    64-column kernel, so bit-identical results, for general, symmetric and
+    triangular products."""
+    rng = np.random.default_rng(S * 7 + n)
+    A = rng.standard_normal((n, n)) * np.exp2(rng.integers(-20, 20, size=(n, 1)))
+    B = rng.standard_normal((n, n))
+    X = 0.5 * (A + A.T)
+    for kw in ({}, {"symmetric": True}, {"tri_a": 1, "tri_b": 2}, {"tri_a": 2}, {"tri_b": 1},
+               {"tri_a": 1, "symmetric": True}):
+        M = X if kw.get("symmetric") else A
+        N = X if kw.get("symmetric") else B
+        C1 = ctx.oz_gemm(M, N, slices=S, kblock=64, variant=1, **kw)
+        C4 = ctx.oz_gemm(M, N, slices=S, variant=4, **kw)
+        assert np.array_equal(C1, C4), kw
+    with pytest.raises(PtbGpuError):
+        ctx.oz_gemm(A, B, slices=S, kblock=64, variant=4)
+
+
 def test_mixed_path_with_int8_triangular_inverse(ctx):
     """ndim 5888 = 2 x 2944: the triangular inverse of the Cholesky factor takes
     its top-level off-diagonal products on the int8 tensor cores.  The mixed
