@@ -170,8 +170,10 @@ __global__ void k_oz_slice(const double* __restrict__ M, int64_t rs, int64_t cs,
 
 // ---- product ---------------------------------------------------------------
 struct OzMaps {
-    CUtensorMap a;   // S stacked A planes
-    CUtensorMap b;   // S stacked B planes
+    CUtensorMap a;    // S stacked A planes
+    CUtensorMap b;    // S stacked B planes
+    CUtensorMap a2;   // the same planes with 64-byte K boxes (second pass of the 128-column kernel)
+    CUtensorMap b2;
 };
 
 template <int W>
@@ -720,8 +722,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
 // and a register for the diagonal); pass 2 sums groups 0..GS-1 into the freed
 // columns and the epilogue continues the same FP64 sum from the parked value.
 // The result is bit-identical to the 64-column kernel.  Pass 2 loads only the
-// slices 0..GS-1; its loads overlap the pass-1 epilogue.  K blocks of 32 bytes
-// (32B swizzle): a stage holds S A slices and S B slices of 4 KB each.
+// slices 0..GS-1; its loads overlap the pass-1 epilogue.  Pass 1 takes K
+// blocks of 32 bytes (32B swizzle: a stage holds S A slices and S B slices of
+// 4 KB each), pass 2 blocks of 64 bytes (64B swizzle, GS slices of 8 KB each in
+// the same stage buffers), so that its few MMAs per K byte still see two K32
+// steps of work per stage.
 template <int S>
 struct OzWideCfg {
     static constexpr int NT = 128;
@@ -734,12 +739,20 @@ struct OzWideCfg {
     static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
     static constexpr uint32_t LAYOUT = 6u;   // SWIZZLE_32B
     static constexpr uint32_t SBO = 8u * RB;
+    static constexpr int RB2 = 64;          // pass 2
+    static constexpr int A2_TILE = BM * RB2;
+    static constexpr int B2_TILE = NT * RB2;
+    static constexpr uint32_t LAYOUT2 = 4u;   // SWIZZLE_64B
+    static constexpr uint32_t SBO2 = 8u * RB2;
     // kind::i8: D s32, A and B s8, K-major, N = 128, M = 128
     static constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) |
                                       ((uint32_t)(BM >> 4) << 24);
     static_assert((S - GS) * NT <= kTmemCols, "one pass's accumulators fit in tensor memory");
     static_assert(STAGES >= 2, "at least two pipeline stages");
     static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0, "tiles keep the swizzle atoms aligned");
+    static_assert(GS * (A2_TILE + B2_TILE) <= STAGE, "pass-2 slices fit a stage");
+    // one resident CTA per SM whatever else runs there (TMEM: all 512 columns)
+    static_assert(SMEM > 232448 / 2, "shared memory keeps the kernel at one CTA per SM");
 };
 
 // Bounded wait that also ends when the abort flag is raised; true when the phase completed.
@@ -793,12 +806,14 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int4 tile = tiles[blockIdx.x];
     const int bi = tile.x, bj = tile.y;
-    const int kb0 = tile.z / C::RB;
-    const int nk = (tile.w - tile.z) / C::RB;         // K steps of one pass
-    const int ntot = GS > 0 ? 2 * nk : nk;            // both passes
+    const int nk = (tile.w - tile.z) / C::RB;                  // K steps of pass 1
+    const int nk2 = GS > 0 ? (tile.w - tile.z) / C::RB2 : 0;   // K steps of pass 2
+    const int ntot = nk + nk2;
 
     auto a_tile = [&](int s, int p) { return base + s * STAGE + p * C::A_TILE; };
     auto b_tile = [&](int s, int q) { return base + s * STAGE + S * C::A_TILE + q * C::B_TILE; };
+    auto a2_tile = [&](int s, int p) { return base + s * STAGE + p * C::A2_TILE; };
+    auto b2_tile = [&](int s, int q) { return base + s * STAGE + GS * C::A2_TILE + q * C::B2_TILE; };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -833,13 +848,21 @@ __global__ void __launch_bounds__(THREADS, 1)
                 break;
             }
             if (*(volatile int*)abort_flag) break;
-            const int ns = it < nk ? S : GS;
-            mbar_expect_tx(full_bar(s), (uint32_t)(ns * (C::A_TILE + C::B_TILE)));
-            const int kx = (kb0 + (it < nk ? it : it - nk)) * C::RB;
-            for (int p = 0; p < ns; ++p)
-                tma_load_2d(a_tile(s, p), &maps.a, full_bar(s), kx, (int)(p * ep.ldp) + bi * BM);
-            for (int q = 0; q < ns; ++q)
-                tma_load_2d(b_tile(s, q), &maps.b, full_bar(s), kx, (int)(q * ep.ldp) + bj * NT);
+            if (it < nk) {
+                mbar_expect_tx(full_bar(s), (uint32_t)(S * (C::A_TILE + C::B_TILE)));
+                const int kx = tile.z + it * C::RB;
+                for (int p = 0; p < S; ++p)
+                    tma_load_2d(a_tile(s, p), &maps.a, full_bar(s), kx, (int)(p * ep.ldp) + bi * BM);
+                for (int q = 0; q < S; ++q)
+                    tma_load_2d(b_tile(s, q), &maps.b, full_bar(s), kx, (int)(q * ep.ldp) + bj * NT);
+            } else {
+                mbar_expect_tx(full_bar(s), (uint32_t)(GS * (C::A2_TILE + C::B2_TILE)));
+                const int kx = tile.z + (it - nk) * C::RB2;
+                for (int p = 0; p < GS; ++p)
+                    tma_load_2d(a2_tile(s, p), &maps.a2, full_bar(s), kx, (int)(p * ep.ldp) + bi * BM);
+                for (int q = 0; q < GS; ++q)
+                    tma_load_2d(b2_tile(s, q), &maps.b2, full_bar(s), kx, (int)(q * ep.ldp) + bj * NT);
+            }
             issued_phase[s] = round & 1;
         }
         for (int s = 0; s < STAGES; ++s)
@@ -882,12 +905,15 @@ __global__ void __launch_bounds__(THREADS, 1)
                 }
             } else {
 #pragma unroll
-                for (int p = 0; p < GS; ++p) {
-                    const uint64_t ad = sdesc(a_tile(s, p), C::SBO, C::LAYOUT);
+                for (int k = 0; k < C::RB2 / 32; ++k) {
 #pragma unroll
-                    for (int q = 0; q < GS - p; ++q) {
-                        const uint64_t bd = sdesc(b_tile(s, q), C::SBO, C::LAYOUT);
-                        umma_i8(tmem + (uint32_t)((p + q) * NT), ad, bd, C::IDESC, (itp | p) != 0);
+                    for (int p = 0; p < GS; ++p) {
+                        const uint64_t ad = sdesc(a2_tile(s, p) + k * 32, C::SBO2, C::LAYOUT2);
+#pragma unroll
+                        for (int q = 0; q < GS - p; ++q) {
+                            const uint64_t bd = sdesc(b2_tile(s, q) + k * 32, C::SBO2, C::LAYOUT2);
+                            umma_i8(tmem + (uint32_t)((p + q) * NT), ad, bd, C::IDESC, (itp | k | p) != 0);
+                        }
                     }
                 }
             }
@@ -1143,9 +1169,9 @@ void slice(cudaStream_t s, const double* M, int64_t rs, int64_t cs, int64_t n, i
 
 int resolve_variant(int variant, int S, int rb) {
     if (variant != V_DEFAULT) return variant;
-    // 128-column tiles measured 5-15 % faster with 7 or 8 slices at ndim 4096-11776
-    // (N = 128 MMAs), within 1 % either way with 6; they take 32-byte K blocks only
-    return S >= 7 && rb != 64 ? V_WIDE : V_SMEM_A;
+    // 128-column tiles measured x1.09-1.22 faster than 128 x 64 tiles with 6, 7 or
+    // 8 slices at ndim 4096-11776 (N = 128 MMAs); they take 32-byte K blocks only
+    return S >= 6 && rb != 64 ? V_WIDE : V_SMEM_A;
 }
 
 int tile_n(int S, int variant) {
@@ -1228,10 +1254,14 @@ void product(cudaStream_t s, int epi, const Operand& a, const Operand& b, const 
               (long long)a.ldp, a.S);
     PTB_CHECK(epi == OZ_OUT || epi == OZ_SYM, PTBGPU_EINVAL, "bad epilogue");
     if (ntiles == 0) return;
-    OzMaps maps;
+    OzMaps maps{};
     encode_planes(&maps.a, a, BM, rb);
     // a CTA pair splits the 64 B rows of a tile between its two CTAs
     encode_planes(&maps.b, b, variant == V_PAIR ? BN / 2 : tile_n(a.S, variant), rb);
+    if (variant == V_WIDE) {   // the second pass takes 64-byte K blocks
+        encode_planes(&maps.a2, a, BM, 64);
+        encode_planes(&maps.b2, b, tile_n(a.S, variant), 64);
+    }
     if (epi == OZ_OUT) launch_e<OZ_OUT>(s, a.S, rb, variant, maps, tiles_dev, ntiles, a, b, ep);
     else launch_e<OZ_SYM>(s, a.S, rb, variant, maps, tiles_dev, ntiles, a, b, ep);
     PTB_CUDA(cudaGetLastError());
