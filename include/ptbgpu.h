@@ -306,12 +306,12 @@ int ptbgpu_symsq_split(ptbgpu_ctx* ctx, int64_t n, int64_t planes, int64_t kbloc
                        double* ms);   /* ms (may be NULL): device time of the product launch(es) */
 /* C = A * B for n x n FP64 row-major host matrices, on the int8 tensor cores
  * with `slices` (6..8) 7-bit slices per operand row and an int32-exact K loop;
- * kblock 32 or 64 bytes (0 = default); variant 0 default (4 for 6 to 8
+ * kblock 32 or 64 bytes (0 = default); variant 0 default (5 for 6 to 8
  * slices unless kblock is 64, else 1), 1 A slices read from shared memory by
  * every MMA, 2 A slices copied into tensor memory once per K step, 3 variant 1
  * on a CTA pair (256-row tiles, cta_group::2), 4 128-column tiles with the
- * accumulator groups summed in two passes over K (kblock 0 or 32), all
- * bit-identical.  tri_a / tri_b: 0 full, 1 lower, 2 upper
+ * accumulator groups summed in two passes over K (kblock 0 or 32), 5 variant 4
+ * on a CTA pair (256 x 128 tiles), all bit-identical.  tri_a / tri_b: 0 full, 1 lower, 2 upper
  * triangular (the other part is read as zero and its K blocks are skipped);
  * symmetric != 0: only the upper triangle of C is computed and mirrored.
  * n <= (2^31 - 1) / (slices * 127^2) rounded down to a multiple of 128.

@@ -491,7 +491,8 @@ class Context:
         symmetric: only the upper triangle of C is computed and mirrored;
         variant: 0 default, 1 A from shared memory, 2 A in tensor memory,
         3 A from shared memory on a CTA pair (256-row tiles), 4 128-column
-        tiles summed in two passes over K (kblock 0 or 32).
+        tiles summed in two passes over K (kblock 0 or 32), 5 variant 4 on a
+        CTA pair (256 x 128 tiles).
         timed: returns (C, device milliseconds of the product kernel)."""
         Ah, Bh = _f64(A), _f64(B)
         n = Ah.shape[0]

@@ -535,7 +535,7 @@ int ptbgpu_oz_gemm(ptbgpu_ctx* c, int64_t n, int64_t slices, int64_t kblock, int
                    int64_t tri_b, int64_t symmetric, const double* A, const double* B, double* Cout, double* ms) {
     return guarded(c, [&] {
         PTB_CHECK(n > 0 && A && B && Cout && (slices == 4 || (slices >= 6 && slices <= 8)) &&
-                      (kblock == 0 || kblock == 32 || kblock == 64) && variant >= 0 && variant <= 4 &&
+                      (kblock == 0 || kblock == 32 || kblock == 64) && variant >= 0 && variant <= 5 &&
                       tri_a >= 0 && tri_a <= 2 && tri_b >= 0 && tri_b <= 2,
                   PTBGPU_EINVAL, "bad arguments");
         oz_gemm_entry(c, n, (int)slices, (int)kblock, (int)variant, (int)tri_a, (int)tri_b, symmetric != 0, A, B,

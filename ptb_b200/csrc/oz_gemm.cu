@@ -780,6 +780,105 @@ __device__ __forceinline__ void oz_wide_groups(uint32_t tmem, int q4, int c0, in
     }
 }
 
+// Epilogue warps 4..7 of the 128-column kernels (q4 = TMEM lane quarter): pass 1
+// drain into the parked partial sums, one arrival per warp on the "free" barrier
+// (of the leader CTA, a shared::cluster address, when CLUSTER_ARRIVE), pass 2
+// drain continuing the parked sums, fused output and per-CTA stats.
+template <int EPI, int S, bool CLUSTER_ARRIVE>
+__device__ __forceinline__ void oz_wide_epilogue(const OzEpi& ep, uint32_t tmem, uint32_t accum_bar, uint32_t free_bar,
+                                                 int* abort_flag, double* red, int bi, int bj, int q4, int lane,
+                                                 int nk, const int* __restrict__ ea, const int* __restrict__ eb) {
+    constexpr int GS = OzWideCfg<S>::GS;
+    constexpr int NT = OzWideCfg<S>::NT;
+    const int64_t n = ep.n, r = (int64_t)bi * BM + q4 * 32 + lane;
+    const int64_t ld = ep.ors;
+    double tr = 0.0, ss = 0.0, dlo = 0.0;
+    bool live = true;
+    if constexpr (GS > 0) {
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_or_abort(accum_bar, 0, abort_flag));
+        const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
+        tc_fence_after();
+        if (!ok && !aborted && lane == 0) set_err(ep.err, 180);
+        live = ok && !aborted;
+        if (live) {
+#pragma unroll 1
+            for (int c0 = 0; c0 < NT; c0 += 32) {
+                double acc[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                oz_wide_groups(tmem, q4, c0, S - 1, GS, GS, acc);
+                const int64_t cb = (int64_t)bj * NT + c0;
+                if (r < n) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int64_t c = cb + j;
+                        if (c >= n) continue;
+                        if (EPI == OZ_OUT) ep.out[r * ep.ors + c * ep.ocs] = acc[j];
+                        else if (c > r) ep.out[c + r * ld] = acc[j];
+                        else if (c == r) dlo = acc[j];
+                    }
+                }
+            }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) {
+            if constexpr (CLUSTER_ARRIVE)
+                asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(free_bar) : "memory");
+            else
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(free_bar) : "memory");
+        }
+    }
+    if (live) {
+        const uint32_t par = GS > 0 ? 1u : 0u;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_or_abort(accum_bar, par, abort_flag));
+        const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
+        tc_fence_after();
+        if (!ok && !aborted && lane == 0) set_err(ep.err, 181);
+        if (ok && !aborted) {
+            const int er = r < n ? ea[r] : 0;
+#pragma unroll 1
+            for (int c0 = 0; c0 < NT; c0 += 32) {
+                double acc[32];
+                const int64_t cb = (int64_t)bj * NT + c0;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int64_t c = cb + j;
+                    double v = 0.0;
+                    if (GS > 0 && r < n && c < n) {
+                        if (EPI == OZ_OUT) v = ep.out[r * ep.ors + c * ep.ocs];
+                        else if (c > r) v = ep.out[c + r * ld];
+                        else if (c == r) v = dlo;
+                    }
+                    acc[j] = v;
+                }
+                if (GS > 0) oz_wide_groups(tmem, q4, c0, GS - 1, 0, 0, acc);
+                else oz_wide_groups(tmem, q4, c0, S - 1, 0, 0, acc);
+                if (nk == 0) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                }
+                oz_write<EPI, 32>(ep, r, cb, acc, er, eb, tr, ss);
+            }
+        }
+    }
+    if (EPI == OZ_SYM && ep.stats) {
+        for (int o = 16; o > 0; o >>= 1) {
+            tr += __shfl_xor_sync(0xffffffffu, tr, o);
+            ss += __shfl_xor_sync(0xffffffffu, ss, o);
+        }
+        if (lane == 0) {
+            red[2 * q4] = tr;
+            red[2 * q4 + 1] = ss;
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");   // epilogue warps only
+        if (q4 == 0 && lane == 0) {
+            ep.stats[2 * blockIdx.x] = red[0] + red[2] + red[4] + red[6];
+            ep.stats[2 * blockIdx.x + 1] = red[1] + red[3] + red[5] + red[7];
+        }
+    }
+}
+
 template <int EPI, int S>
 __global__ void __launch_bounds__(THREADS, 1)
     k_oz_product_w(const __grid_constant__ OzMaps maps, const int4* __restrict__ tiles, const int* __restrict__ ea,
@@ -929,90 +1028,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         // every MMA of the tile has completed before the block tears down
         if (!mbar_wait(accum_bar, (uint32_t)((commits - 1) & 1))) set_err(ep.err, 175);
     } else if (warp >= 4) {
-        // ---------------- epilogue: warp w drains TMEM lanes 32 (w - 4) .. ----------------
-        const int q4 = warp - 4;
-        const int64_t n = ep.n, r = (int64_t)bi * BM + q4 * 32 + lane;
-        const int64_t ld = ep.ors;
-        double tr = 0.0, ss = 0.0, dlo = 0.0;
-        bool live = true;
-        if constexpr (GS > 0) {
-            const bool ok = __all_sync(0xffffffffu, mbar_wait_or_abort(accum_bar, 0, abort_flag));
-            const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
-            tc_fence_after();
-            if (!ok && !aborted && lane == 0) set_err(ep.err, 180);
-            live = ok && !aborted;
-            if (live) {
-#pragma unroll 1
-                for (int c0 = 0; c0 < NT; c0 += 32) {
-                    double acc[32];
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-                    oz_wide_groups(tmem, q4, c0, S - 1, GS, GS, acc);
-                    const int64_t cb = (int64_t)bj * NT + c0;
-                    if (r < n) {
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int64_t c = cb + j;
-                            if (c >= n) continue;
-                            if (EPI == OZ_OUT) ep.out[r * ep.ors + c * ep.ocs] = acc[j];
-                            else if (c > r) ep.out[c + r * ld] = acc[j];
-                            else if (c == r) dlo = acc[j];
-                        }
-                    }
-                }
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(free_bar) : "memory");
-        }
-        if (live) {
-            const uint32_t par = GS > 0 ? 1u : 0u;
-            const bool ok = __all_sync(0xffffffffu, mbar_wait_or_abort(accum_bar, par, abort_flag));
-            const int aborted = __shfl_sync(0xffffffffu, *(volatile int*)abort_flag, 0);
-            tc_fence_after();
-            if (!ok && !aborted && lane == 0) set_err(ep.err, 181);
-            if (ok && !aborted) {
-                const int er = r < n ? ea[r] : 0;
-#pragma unroll 1
-                for (int c0 = 0; c0 < NT; c0 += 32) {
-                    double acc[32];
-                    const int64_t cb = (int64_t)bj * NT + c0;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int64_t c = cb + j;
-                        double v = 0.0;
-                        if (GS > 0 && r < n && c < n) {
-                            if (EPI == OZ_OUT) v = ep.out[r * ep.ors + c * ep.ocs];
-                            else if (c > r) v = ep.out[c + r * ld];
-                            else if (c == r) v = dlo;
-                        }
-                        acc[j] = v;
-                    }
-                    if (GS > 0) oz_wide_groups(tmem, q4, c0, GS - 1, 0, 0, acc);
-                    else oz_wide_groups(tmem, q4, c0, S - 1, 0, 0, acc);
-                    if (nk == 0) {
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-                    }
-                    oz_write<EPI, 32>(ep, r, cb, acc, er, eb, tr, ss);
-                }
-            }
-        }
-        if (EPI == OZ_SYM && ep.stats) {
-            for (int o = 16; o > 0; o >>= 1) {
-                tr += __shfl_xor_sync(0xffffffffu, tr, o);
-                ss += __shfl_xor_sync(0xffffffffu, ss, o);
-            }
-            if (lane == 0) {
-                red[2 * q4] = tr;
-                red[2 * q4 + 1] = ss;
-            }
-            asm volatile("bar.sync 1, 128;" ::: "memory");   // epilogue warps only
-            if (q4 == 0 && lane == 0) {
-                ep.stats[2 * blockIdx.x] = red[0] + red[2] + red[4] + red[6];
-                ep.stats[2 * blockIdx.x + 1] = red[1] + red[3] + red[5] + red[7];
-            }
-        }
+        oz_wide_epilogue<EPI, S, false>(ep, tmem, accum_bar, free_bar, abort_flag, red, bi, bj, warp - 4, lane, nk, ea,
+                                        eb);
     }
     __syncwarp();
     tc_fence_before();
@@ -1020,6 +1037,214 @@ __global__ void __launch_bounds__(THREADS, 1)
     tc_fence_after();
     if (warp == 2) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTmemCols));
+    }
+}
+
+// The 128-column two-pass kernel on a CTA pair (cta_group::2, cluster of two):
+// one 256 x 128 tile per pair, UMMA 256x128x32 int8 issued by the leader CTA.
+// CTA r holds rows 128r..128r+127 of the A slices and of the accumulators and
+// rows 64r..64r+63 of the 128 B rows, so each SM loads its A slices and half
+// the B slices: 6 KB instead of 8 KB per slice pair and K32 step, which the
+// one-CTA form draws from L2 at up to ~60 % of its throughput.  Both CTAs' TMA
+// loads count on the leader's "full" barrier (armed with both CTAs' bytes), the
+// leader's commits arrive on both CTAs' "empty" and accumulator barriers, and
+// both CTAs' epilogue warps arrive on the leader's "free" barrier after the
+// pass-1 drain (8 arrivals) before the leader starts pass 2.  Same passes,
+// parking and FP64 order as the one-CTA form: bit-identical results.
+template <int S>
+struct OzWidePairCfg {
+    static constexpr int NT = 128;
+    static constexpr int RB = 32, RB2 = 64;
+    static constexpr int GS = OzWideCfg<S>::GS;
+    static constexpr int A_TILE = BM * RB;
+    static constexpr int B_TILE = (NT / 2) * RB;
+    static constexpr int A2_TILE = BM * RB2;
+    static constexpr int B2_TILE = (NT / 2) * RB2;
+    static constexpr int STAGE = S * (A_TILE + B_TILE);
+    static constexpr int STAGES = (kSmemBudget / STAGE) > 4 ? 4 : (kSmemBudget / STAGE);
+    static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+    static constexpr uint32_t LAYOUT = 6u, SBO = 8u * RB;      // SWIZZLE_32B
+    static constexpr uint32_t LAYOUT2 = 4u, SBO2 = 8u * RB2;   // SWIZZLE_64B
+    // kind::i8: D s32, A and B s8, K-major, N = 128, M = 256 (the pair)
+    static constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) |
+                                      ((uint32_t)(256 >> 4) << 24);
+    static_assert((S - GS) * NT <= kTmemCols, "one pass's accumulators fit in tensor memory");
+    static_assert(STAGES >= 2, "at least two pipeline stages");
+    static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0 && B2_TILE % 1024 == 0, "swizzle atoms aligned");
+    static_assert(GS * (A2_TILE + B2_TILE) <= STAGE, "pass-2 slices fit a stage");
+};
+
+template <int EPI, int S>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
+    k_oz_product_wp(const __grid_constant__ OzMaps maps, const int4* __restrict__ pairs,
+                    const int* __restrict__ ea, const int* __restrict__ eb, OzEpi ep) {
+    using C = OzWidePairCfg<S>;
+    constexpr int STAGE = C::STAGE;
+    constexpr int STAGES = C::STAGES;
+    constexpr int GS = C::GS;
+    constexpr int NT = C::NT;
+
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t base_raw = smem_u32(smem_raw);
+    const uint32_t base = (base_raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - base_raw);
+    const uint32_t bar0 = base + STAGES * STAGE;
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+    const uint32_t accum_bar = bar0 + 8u * (2 * STAGES);
+    const uint32_t free_bar = bar0 + 8u * (2 * STAGES + 1);   // the leader's: pass-1 accumulators drained
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + STAGES * STAGE + 8 * (2 * STAGES + 2));
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+    double* red = reinterpret_cast<double*>(gbase + STAGES * STAGE + 128);   // 8 doubles
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const int4 pt = pairs[blockIdx.x >> 1];
+    const int bi = 2 * pt.x + (int)rank, bj = pt.y;
+    // an odd row-block count leaves the second half of the last pair past the
+    // operand: it loads the first half's rows again and writes nothing
+    const int nbi = (int)(ep.ldp / BM);
+    const int abi = bi < nbi ? bi : nbi - 1;
+    const int nk = (pt.w - pt.z) / C::RB;                  // K steps of pass 1
+    const int nk2 = GS > 0 ? (pt.w - pt.z) / C::RB2 : 0;   // K steps of pass 2
+    const int ntot = nk + nk2;
+
+    auto a_tile = [&](int s, int p) { return base + s * STAGE + p * C::A_TILE; };
+    auto b_tile = [&](int s, int q) { return base + s * STAGE + S * C::A_TILE + q * C::B_TILE; };
+    auto a2_tile = [&](int s, int p) { return base + s * STAGE + p * C::A2_TILE; };
+    auto b2_tile = [&](int s, int q) { return base + s * STAGE + GS * C::A2_TILE + q * C::B2_TILE; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(accum_bar, 1);
+        mbar_init(free_bar, 8);   // four epilogue warps of each CTA (the leader's barrier is used)
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"((uint32_t)kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();   // both CTAs' barriers are initialised before any remote arrive
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer (both CTAs) ----------------
+        int issued_phase[STAGES];
+        for (int s = 0; s < STAGES; ++s) issued_phase[s] = -1;
+        for (int it = 0; it < ntot; ++it) {
+            const int s = it % STAGES, round = it / STAGES;
+            if (round > 0 && !mbar_wait(empty_bar(s), (round - 1) & 1)) {
+                set_err(ep.err, 191);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            const uint32_t fb = mapa_shared(full_bar(s), 0);
+            if (it < nk) {
+                if (rank == 0) mbar_expect_tx(full_bar(s), (uint32_t)(2 * S * (C::A_TILE + C::B_TILE)));
+                const int kx = pt.z + it * C::RB;
+                for (int p = 0; p < S; ++p)
+                    tma_load_2d_pair(a_tile(s, p), &maps.a, fb, kx, (int)(p * ep.ldp) + abi * BM);
+                for (int q = 0; q < S; ++q)
+                    tma_load_2d_pair(b_tile(s, q), &maps.b, fb, kx,
+                                     (int)(q * ep.ldp) + bj * NT + (int)rank * (NT / 2));
+            } else {
+                if (rank == 0) mbar_expect_tx(full_bar(s), (uint32_t)(2 * GS * (C::A2_TILE + C::B2_TILE)));
+                const int kx = pt.z + (it - nk) * C::RB2;
+                for (int p = 0; p < GS; ++p)
+                    tma_load_2d_pair(a2_tile(s, p), &maps.a2, fb, kx, (int)(p * ep.ldp) + abi * BM);
+                for (int q = 0; q < GS; ++q)
+                    tma_load_2d_pair(b2_tile(s, q), &maps.b2, fb, kx,
+                                     (int)(q * ep.ldp) + bj * NT + (int)rank * (NT / 2));
+            }
+            issued_phase[s] = round & 1;
+        }
+        // drain: the leader sees every copy of the pair land on its full barriers;
+        // the peer's copies have landed once the leader's MMAs consumed them,
+        // which its accumulator barrier (waited by the epilogue) certifies
+        if (rank == 0)
+            for (int s = 0; s < STAGES; ++s)
+                if (issued_phase[s] >= 0 && !mbar_wait(full_bar(s), (uint32_t)issued_phase[s])) set_err(ep.err, 192);
+    } else if (warp == 1 && lane == 0 && rank == 0) {
+        // ---------------- MMA issuer (leader CTA) ----------------
+        int commits = 0;
+        for (int it = 0; it < ntot; ++it) {
+            const int s = it % STAGES, round = it / STAGES;
+            const bool pass2 = GS > 0 && it >= nk;
+            if (GS > 0 && it == nk) {
+                // end of pass 1: hand the accumulators to both epilogues, wait until both drained
+                umma_commit_pair(accum_bar, (uint16_t)0x3);
+                ++commits;
+                if (!mbar_wait_or_abort(free_bar, 0, abort_flag)) {
+                    set_err(ep.err, 203);
+                    *(volatile int*)abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+            }
+            if (!mbar_wait(full_bar(s), round & 1)) {
+                set_err(ep.err, 201);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            tc_fence_after();
+            const int itp = pass2 ? it - nk : it;
+            if (!pass2) {
+#pragma unroll
+                for (int p = 0; p < S; ++p) {
+                    const uint64_t ad = sdesc(a_tile(s, p), C::SBO, C::LAYOUT);
+#pragma unroll
+                    for (int q = (GS - p > 0 ? GS - p : 0); q < S - p; ++q) {
+                        const uint64_t bd = sdesc(b_tile(s, q), C::SBO, C::LAYOUT);
+                        umma_i8_pair(tmem + (uint32_t)((p + q - GS) * NT), ad, bd, C::IDESC, (itp | p) != 0);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < C::RB2 / 32; ++k) {
+#pragma unroll
+                    for (int p = 0; p < GS; ++p) {
+                        const uint64_t ad = sdesc(a2_tile(s, p) + k * 32, C::SBO2, C::LAYOUT2);
+#pragma unroll
+                        for (int q = 0; q < GS - p; ++q) {
+                            const uint64_t bd = sdesc(b2_tile(s, q) + k * 32, C::SBO2, C::LAYOUT2);
+                            umma_i8_pair(tmem + (uint32_t)((p + q) * NT), ad, bd, C::IDESC, (itp | k | p) != 0);
+                        }
+                    }
+                }
+            }
+            umma_commit_pair(empty_bar(s), (uint16_t)0x3);
+        }
+        if (GS > 0 && nk == 0) {   // empty K range: both epilogue phases still complete
+            umma_commit_pair(accum_bar, (uint16_t)0x3);
+            ++commits;
+            if (!mbar_wait_or_abort(free_bar, 0, abort_flag)) set_err(ep.err, 204);
+        }
+        umma_commit_pair(accum_bar, (uint16_t)0x3);
+        ++commits;
+        // every MMA of the pair has completed before either CTA tears down
+        if (!mbar_wait(accum_bar, (uint32_t)((commits - 1) & 1))) set_err(ep.err, 205);
+    } else if (warp >= 4) {
+        oz_wide_epilogue<EPI, S, true>(ep, tmem, accum_bar, mapa_shared(free_bar, 0), abort_flag, red, bi, bj,
+                                       warp - 4, lane, nk, ea, eb);
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();   // the leader's MMAs have finished with the peer's shared and tensor memory
+    tc_fence_after();
+    if (warp == 2) {
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTmemCols));
     }
 }
 
@@ -1093,6 +1318,19 @@ void launch_w(cudaStream_t s, const OzMaps& maps, const int4* tiles, int ntiles,
     count_launch();
 }
 
+template <int EPI, int S>
+void launch_wp(cudaStream_t s, const OzMaps& maps, const int4* pairs, int npairs, const Operand& a,
+               const Operand& b, const OzEpi& ep) {
+    using C = OzWidePairCfg<S>;
+    static const bool attr = [] {   // thread-safe one-time setup
+        PTB_CUDA(cudaFuncSetAttribute(k_oz_product_wp<EPI, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+        return true;
+    }();
+    (void)attr;
+    k_oz_product_wp<EPI, S><<<2 * npairs, THREADS, C::SMEM, s>>>(maps, pairs, a.exps, b.exps, ep);
+    count_launch();
+}
+
 constexpr int ta_tile_n(int S) { return S >= 7 ? 48 : 64; }
 
 template <int EPI, int S, int RB>
@@ -1123,6 +1361,8 @@ void launch_s(cudaStream_t s, int rb, int variant, const OzMaps& maps, const int
         else launch_p<EPI, S, 32>(s, maps, tiles, ntiles, a, b, ep);
     } else if (variant == V_WIDE) {
         launch_w<EPI, S>(s, maps, tiles, ntiles, a, b, ep);
+    } else if (variant == V_WPAIR) {
+        launch_wp<EPI, S>(s, maps, tiles, ntiles, a, b, ep);
     } else {
         if (rb == 64) launch_t<EPI, S, 64>(s, maps, tiles, ntiles, a, b, ep);
         else launch_t<EPI, S, 32>(s, maps, tiles, ntiles, a, b, ep);
@@ -1169,14 +1409,15 @@ void slice(cudaStream_t s, const double* M, int64_t rs, int64_t cs, int64_t n, i
 
 int resolve_variant(int variant, int S, int rb) {
     if (variant != V_DEFAULT) return variant;
-    // 128-column tiles measured x1.09-1.22 faster than 128 x 64 tiles with 6, 7 or
-    // 8 slices at ndim 4096-11776 (N = 128 MMAs); they take 32-byte K blocks only
-    return S >= 6 && rb != 64 ? V_WIDE : V_SMEM_A;
+    // 128-column tiles on a CTA pair measured x1.21-1.29 faster than 128 x 64 tiles
+    // with 6, 7 or 8 slices at ndim 4096-11776 (N = 128 MMAs: x1.09-1.22 on one CTA;
+    // the pair halves the B loads per SM); they take 32-byte K blocks only
+    return S >= 6 && rb != 64 ? V_WPAIR : V_SMEM_A;
 }
 
 int tile_n(int S, int variant) {
     PTB_CHECK(variant != V_DEFAULT, PTBGPU_EINVAL, "kernel variant not resolved");
-    return variant == V_TMEM_A ? ta_tile_n(S) : variant == V_WIDE ? 128 : BN;
+    return variant == V_TMEM_A ? ta_tile_n(S) : (variant == V_WIDE || variant == V_WPAIR) ? 128 : BN;
 }
 
 std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int bn) {
@@ -1203,9 +1444,10 @@ std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int 
     return t;
 }
 
-std::vector<int4> make_pair_tiles(int64_t ldp, bool upper, int a_tri, int b_tri) {
-    const std::vector<int4> one = make_tiles(ldp, upper, a_tri, b_tri, BN);
-    const int nbi = (int)(ldp / BM), nbj = (int)(ldp / BN), np = (nbi + 1) / 2;
+std::vector<int4> make_pair_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int bn) {
+    PTB_CHECK(bn == 64 || bn == 128, PTBGPU_EINVAL, "pair tiles are 64 or 128 columns wide");
+    const std::vector<int4> one = make_tiles(ldp, upper, a_tri, b_tri, bn);
+    const int nbi = (int)(ldp / BM), nbj = (int)(ldp / bn), np = (nbi + 1) / 2;
     // K range of each (pair, bj) over the halves make_tiles keeps; k1 = 0: none kept
     std::vector<int2> kr((size_t)np * nbj, make_int2(INT_MAX, 0));
     for (const int4& x : one) {
@@ -1226,24 +1468,25 @@ std::vector<int4> make_pair_tiles(int64_t ldp, bool upper, int a_tri, int b_tri)
 }
 
 std::vector<int4> build_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int S, int variant) {
-    return variant == V_PAIR ? make_pair_tiles(ldp, upper, a_tri, b_tri)
-                             : make_tiles(ldp, upper, a_tri, b_tri, tile_n(S, variant));
+    return (variant == V_PAIR || variant == V_WPAIR) ? make_pair_tiles(ldp, upper, a_tri, b_tri, tile_n(S, variant))
+                                                     : make_tiles(ldp, upper, a_tri, b_tri, tile_n(S, variant));
 }
 
-int grid_ctas(int ntiles, int variant) { return variant == V_PAIR ? 2 * ntiles : ntiles; }
+int grid_ctas(int ntiles, int variant) { return (variant == V_PAIR || variant == V_WPAIR) ? 2 * ntiles : ntiles; }
 
 double tile_ops(const std::vector<int4>& tiles, int S, int variant) {
     double kk = 0.0;
     for (const int4& x : tiles) kk += (double)(x.w - x.z);
-    const int rows = variant == V_PAIR ? 2 * BM : BM;
+    const int rows = (variant == V_PAIR || variant == V_WPAIR) ? 2 * BM : BM;
     return 2.0 * rows * tile_n(S, variant) * kk * (double)(S * (S + 1) / 2);
 }
 
 void product(cudaStream_t s, int epi, const Operand& a, const Operand& b, const int4* tiles_dev, int ntiles,
              const OzEpi& ep, int rb, int variant) {
-    PTB_CHECK(variant == V_SMEM_A || variant == V_TMEM_A || variant == V_PAIR || variant == V_WIDE, PTBGPU_EINVAL,
-              "bad kernel variant %d", variant);
-    if (variant == V_WIDE) {
+    PTB_CHECK(variant == V_SMEM_A || variant == V_TMEM_A || variant == V_PAIR || variant == V_WIDE ||
+                  variant == V_WPAIR,
+              PTBGPU_EINVAL, "bad kernel variant %d", variant);
+    if (variant == V_WIDE || variant == V_WPAIR) {
         PTB_CHECK(rb == 0 || rb == 32, PTBGPU_EINVAL, "the 128-column kernel takes 32-byte K blocks");
         rb = 32;
     }
@@ -1256,11 +1499,13 @@ void product(cudaStream_t s, int epi, const Operand& a, const Operand& b, const 
     if (ntiles == 0) return;
     OzMaps maps{};
     encode_planes(&maps.a, a, BM, rb);
-    // a CTA pair splits the 64 B rows of a tile between its two CTAs
-    encode_planes(&maps.b, b, variant == V_PAIR ? BN / 2 : tile_n(a.S, variant), rb);
-    if (variant == V_WIDE) {   // the second pass takes 64-byte K blocks
+    // a CTA pair splits the B rows of a tile between its two CTAs
+    const bool pair = variant == V_PAIR || variant == V_WPAIR;
+    const int brows = pair ? tile_n(a.S, variant) / 2 : tile_n(a.S, variant);
+    encode_planes(&maps.b, b, brows, rb);
+    if (variant == V_WIDE || variant == V_WPAIR) {   // the second pass takes 64-byte K blocks
         encode_planes(&maps.a2, a, BM, 64);
-        encode_planes(&maps.b2, b, tile_n(a.S, variant), 64);
+        encode_planes(&maps.b2, b, brows, 64);
     }
     if (epi == OZ_OUT) launch_e<OZ_OUT>(s, a.S, rb, variant, maps, tiles_dev, ntiles, a, b, ep);
     else launch_e<OZ_SYM>(s, a.S, rb, variant, maps, tiles_dev, ntiles, a, b, ep);

@@ -69,8 +69,9 @@ void slice(cudaStream_t s, const double* M, int64_t rs, int64_t cs, int64_t n, i
 // or 8 slices, 64 for fewer), or the shared-memory variant on a CTA pair
 // (cta_group::2: 256-row tiles, each SM loads half of the 64 B rows), or
 // 128-column tiles whose accumulator groups are summed in two passes over K
-// (32-byte K blocks only).  All give bit-identical results.
-enum Variant : int { V_DEFAULT = 0, V_SMEM_A = 1, V_TMEM_A = 2, V_PAIR = 3, V_WIDE = 4 };
+// (32-byte K blocks only), or those on a CTA pair (256 x 128 tiles).  All give
+// bit-identical results.
+enum Variant : int { V_DEFAULT = 0, V_SMEM_A = 1, V_TMEM_A = 2, V_PAIR = 3, V_WIDE = 4, V_WPAIR = 5 };
 // The variant V_DEFAULT stands for with S slices and rb-byte K blocks (0 = the
 // variant's default); the functions below take resolved variants only.
 int resolve_variant(int variant, int S, int rb);
@@ -82,11 +83,11 @@ int tile_n(int S, int variant);   // output columns per tile
 // (rows of A) or B (rows of B).  Longest K ranges first.
 std::vector<int4> make_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int bn);
 
-// CTA-pair tiles {pair row block p (rows 256p..256p+255), bj, k0, k1}: pairs
-// with a half that touches the upper triangle (when `upper`), K range = the
-// union of the ranges of those halves (the extra blocks of a triangular operand
-// are zero slices).  Longest K ranges first.
-std::vector<int4> make_pair_tiles(int64_t ldp, bool upper, int a_tri, int b_tri);
+// CTA-pair tiles {pair row block p (rows 256p..256p+255), bj (bn columns), k0,
+// k1}: pairs with a half that touches the upper triangle (when `upper`), K
+// range = the union of the ranges of those halves (the extra blocks of a
+// triangular operand are zero slices).  Longest K ranges first.
+std::vector<int4> make_pair_tiles(int64_t ldp, bool upper, int a_tri, int b_tri, int bn);
 
 // The tile list `product` expects for `variant`, the CTAs it launches for it
 // (one per tile entry, two per pair entry; OZ_SYM writes one stats pair per

@@ -167,14 +167,16 @@ def test_oz_gemm_pair_variant_is_bit_exact(ctx, S, kblock, n):
         assert np.array_equal(C1, C3), kw
 
 
+@pytest.mark.parametrize("variant", [4, 5])
 @pytest.mark.parametrize("S", [4, 6, 7, 8])
 @pytest.mark.parametrize("n", [300, 700, 1000])
-def test_oz_gemm_wide_variant_is_bit_exact(ctx, S, n):
-    """The 128-column kernel sums the low-weight accumulator groups in a first
-    pass over K, parks their FP64 sum in the output and continues it with the
-    other groups in a second pass: the same FP64 sum in the same order as the
-    64-column kernel, so bit-identical results, for general, symmetric and
-    triangular products."""
+def test_oz_gemm_wide_variant_is_bit_exact(ctx, S, n, variant):
+    """The 128-column kernel (variant 4; variant 5 on a CTA pair, 256 x 128
+    tiles) sums the low-weight accumulator groups in a first pass over K,
+    parks their FP64 sum in the output and continues it with the other groups
+    in a second pass: the same FP64 sum in the same order as the 64-column
+    kernel, so bit-identical results, for general, symmetric and triangular
+    products; n = 300 leaves the last CTA pair with a half past the operand."""
     rng = np.random.default_rng(S * 7 + n)
     A = rng.standard_normal((n, n)) * np.exp2(rng.integers(-20, 20, size=(n, 1)))
     B = rng.standard_normal((n, n))
@@ -184,10 +186,10 @@ def test_oz_gemm_wide_variant_is_bit_exact(ctx, S, n):
         M = X if kw.get("symmetric") else A
         N = X if kw.get("symmetric") else B
         C1 = ctx.oz_gemm(M, N, slices=S, kblock=64, variant=1, **kw)
-        C4 = ctx.oz_gemm(M, N, slices=S, variant=4, **kw)
+        C4 = ctx.oz_gemm(M, N, slices=S, variant=variant, **kw)
         assert np.array_equal(C1, C4), kw
     with pytest.raises(PtbGpuError):
-        ctx.oz_gemm(A, B, slices=S, kblock=64, variant=4)
+        ctx.oz_gemm(A, B, slices=S, kblock=64, variant=variant)
 
 
 def test_mixed_path_with_int8_triangular_inverse(ctx):
