@@ -316,6 +316,17 @@ int ptbgpu_symsq_split(ptbgpu_ctx* ctx, int64_t n, int64_t planes, int64_t kbloc
  * symmetric != 0: only the upper triangle of C is computed and mirrored.
  * n <= (2^31 - 1) / (slices * 127^2) rounded down to a multiple of 128.
  * ms (may be NULL) receives the device time of the product kernel. */
+/* The tile list that ptbgpu_oz_gemm's product launches for the same n, slices,
+ * kblock and variant (host logic only: no context, no device).  a_tri / b_tri
+ * mask the rows of the two K-major operands (rows of A and of B^T): 0 none,
+ * 1 k <= i, 2 k >= i.  symmetric != 0: only tiles touching the upper triangle.
+ * Writes min(cap, count) tiles as int32 {row block (pair row block for the
+ * CTA-pair variants), column block, k0, k1} into tiles, the count into
+ * *ntiles, and info[0] = the resolved variant, info[1] = columns per tile,
+ * info[2] = CTAs launched, info[3] = rows per tile entry.  No counterpart in
+ * the reference. */
+int ptbgpu_oz_tiles(int64_t n, int64_t slices, int64_t kblock, int64_t variant, int64_t a_tri, int64_t b_tri,
+                    int64_t symmetric, int32_t* tiles, int64_t cap, int64_t* ntiles, int64_t* info);
 int ptbgpu_oz_gemm(ptbgpu_ctx* ctx, int64_t n, int64_t slices, int64_t kblock, int64_t variant, int64_t tri_a,
                    int64_t tri_b, int64_t symmetric, const double* A, const double* B, double* C, double* ms);
 

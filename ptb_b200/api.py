@@ -73,7 +73,7 @@ EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_defau
             "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm", "ptbgpu_mlpop14", "ptbgpu_mlpop14_device",
             "ptbgpu_mlpop2", "ptbgpu_mlpop2_device", "ptbgpu_kmeans_partition", "ptbgpu_sm_plan",
             "ptbgpu_sm_prepare", "ptbgpu_sm_nel", "ptbgpu_sm_finish", "ptbgpu_xc_damping",
-            "ptbgpu_xc_damping_device", "ptbgpu_selftest_bounded_wait")
+            "ptbgpu_xc_damping_device", "ptbgpu_selftest_bounded_wait", "ptbgpu_oz_tiles")
 
 
 def library_path() -> Path:
@@ -124,6 +124,7 @@ def load_library():
     lib.ptbgpu_symsq_bf16x6.argtypes = [C.c_void_p, i64, d, P(C.c_float)]
     lib.ptbgpu_symsq_split.argtypes = [C.c_void_p, i64, i64, i64, d, P(C.c_float), d]
     lib.ptbgpu_oz_gemm.argtypes = [C.c_void_p, i64, i64, i64, i64, i64, i64, i64, d, d, d, d]
+    lib.ptbgpu_oz_tiles.argtypes = [i64, i64, i64, i64, i64, i64, i64, P(C.c_int32), i64, P(i64), P(i64)]
     lib.ptbgpu_kmeans_partition.argtypes = [C.c_void_p, i64, d, d, i64, d, P(i64), C.c_uint64, P(_Opts), P(i64),
                                             P(i64), d]
     lib.ptbgpu_sm_plan.argtypes = [C.c_void_p, i64, d, d, i64, d, P(i64), i64, i64, P(i64), P(_Opts), P(i64),
@@ -566,6 +567,28 @@ def density_traces_noalloc(device: int, ndim: int, dP: int, dS: int, dH: int | N
     if rc != OK:
         raise PtbGpuError(rc, err.value.decode(errors="replace"))
     return float(out[0]), float(out[1])
+
+
+def oz_tiles(n: int, slices: int = 8, kblock: int = 0, variant: int = 0, a_tri: int = 0, b_tri: int = 0,
+             symmetric: bool = False) -> tuple[np.ndarray, dict]:
+    """Tile list of the int8-sliced product (ptbgpu_oz_tiles; host logic, no
+    device): an (m, 4) int32 array of {row block (pair row block for the
+    CTA-pair variants), column block, k0, k1} and a dict with the resolved
+    variant, columns per tile, CTAs launched and rows per tile entry.  a_tri /
+    b_tri mask the rows of A and of B^T: 0 none, 1 k <= i, 2 k >= i."""
+    lib = load_library()
+    cnt = C.c_int64(0)
+    info = np.zeros(4, dtype=np.int64)
+    args = (int(n), int(slices), int(kblock), int(variant), int(a_tri), int(b_tri), int(bool(symmetric)))
+    ip = info.ctypes.data_as(C.POINTER(C.c_int64))
+    rc = lib.ptbgpu_oz_tiles(*args, None, 0, C.byref(cnt), ip)
+    if rc != OK:
+        raise PtbGpuError(rc, "ptbgpu_oz_tiles: bad arguments")
+    tiles = np.zeros((cnt.value, 4), dtype=np.int32)
+    rc = lib.ptbgpu_oz_tiles(*args, tiles.ctypes.data_as(C.POINTER(C.c_int32)), cnt.value, C.byref(cnt), ip)
+    if rc != OK:
+        raise PtbGpuError(rc, "ptbgpu_oz_tiles failed")
+    return tiles, {"variant": int(info[0]), "tile_n": int(info[1]), "ctas": int(info[2]), "rows": int(info[3])}
 
 
 # module-level conveniences with the reference's names -----------------------

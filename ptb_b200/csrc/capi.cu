@@ -10,6 +10,7 @@
 #include <thread>
 
 #include "common.cuh"
+#include "oz_gemm.cuh"
 #include "tc_gemm.cuh"
 
 namespace ptb {
@@ -529,6 +530,38 @@ int ptbgpu_xc_damping_device(ptbgpu_ctx* c, int64_t nat, int64_t ndim, const int
         const float ms = xc_damping_device(c, nat, ndim, aoat, rab, rad, hao, xdiag, dPpk, dHpk);
         if (ms_update) *ms_update = ms;
     });
+}
+
+int ptbgpu_oz_tiles(int64_t n, int64_t slices, int64_t kblock, int64_t variant, int64_t a_tri, int64_t b_tri,
+                    int64_t symmetric, int32_t* tiles, int64_t cap, int64_t* ntiles, int64_t* info) {
+    if (n <= 0 || !(slices == 4 || (slices >= 6 && slices <= 8)) || !(kblock == 0 || kblock == 32 || kblock == 64) ||
+        variant < 0 || variant > 5 || a_tri < 0 || a_tri > 2 || b_tri < 0 || b_tri > 2 || cap < 0 ||
+        (cap > 0 && !tiles) || !ntiles || !info)
+        return PTBGPU_EINVAL;
+    try {
+        const int S = (int)slices;
+        const int v = oz::resolve_variant((int)variant, S, (int)kblock);
+        PTB_CHECK(!((v == oz::V_WIDE || v == oz::V_WPAIR) && kblock == 64), PTBGPU_EINVAL,
+                  "the 128-column kernels take 32-byte K blocks");
+        const std::vector<int4> t =
+            oz::build_tiles(oz::padded(n), symmetric != 0, (int)a_tri, (int)b_tri, S, v);
+        *ntiles = (int64_t)t.size();
+        for (int64_t i = 0; i < std::min<int64_t>(cap, (int64_t)t.size()); ++i) {
+            tiles[4 * i] = t[i].x;
+            tiles[4 * i + 1] = t[i].y;
+            tiles[4 * i + 2] = t[i].z;
+            tiles[4 * i + 3] = t[i].w;
+        }
+        info[0] = v;
+        info[1] = oz::tile_n(S, v);
+        info[2] = oz::grid_ctas((int)t.size(), v);
+        info[3] = (v == oz::V_PAIR || v == oz::V_WPAIR) ? 2 * oz::BM : oz::BM;
+        return PTBGPU_OK;
+    } catch (const Error& e) {
+        return e.code;
+    } catch (const std::exception&) {
+        return PTBGPU_EINVAL;
+    }
 }
 
 int ptbgpu_oz_gemm(ptbgpu_ctx* c, int64_t n, int64_t slices, int64_t kblock, int64_t variant, int64_t tri_a,
