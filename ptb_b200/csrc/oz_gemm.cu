@@ -38,6 +38,13 @@ using namespace tc::ptx;
 constexpr int THREADS = 256;
 constexpr int kSmemBudget = 196608;
 constexpr int kTmemCols = 512;
+// Dynamic shared memory that keeps a kernel at one resident CTA per SM (more
+// than half of the 227 KB a block may use).  The CTA-pair kernels hold all 512
+// TMEM columns of both SMs of a pair: two pair CTAs resident on the same SMs
+// could each hold one SM's columns while their peers wait in tcgen05.alloc for
+// the other's, and neither pair would finish.
+constexpr int kSmemMax = 232448;
+constexpr int kOneCtaPerSm = kSmemMax / 2 + 1024;
 
 template <int S, int RB>
 struct OzCfg {
@@ -570,7 +577,8 @@ struct OzPairCfg {
     static constexpr int B_TILE = (BN / 2) * RB;
     static constexpr int STAGE = S * (A_TILE + B_TILE);
     static constexpr int STAGES = (kSmemBudget / STAGE) > 4 ? 4 : (kSmemBudget / STAGE);
-    static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+    static constexpr int SMEM = STAGES * STAGE + 1024 + 256 > kOneCtaPerSm ? STAGES * STAGE + 1024 + 256
+                                                                          : kOneCtaPerSm;
     static constexpr uint32_t LAYOUT = RB == 64 ? 4u : 6u;
     static constexpr uint32_t SBO = 8u * RB;
     // kind::i8: D s32, A and B s8, K-major, N = 64, M = 256 (the pair)
@@ -580,6 +588,7 @@ struct OzPairCfg {
     static_assert(S >= 2 && S * BN <= kTmemCols, "S accumulators of 64 columns fit in tensor memory");
     static_assert(STAGES >= 2, "at least two pipeline stages");
     static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0, "tiles keep the swizzle atoms aligned");
+    static_assert(SMEM >= kOneCtaPerSm && SMEM <= kSmemMax, "one resident CTA per SM");
 };
 
 template <int EPI, int S, int RB>
@@ -751,8 +760,8 @@ struct OzWideCfg {
     static_assert(STAGES >= 2, "at least two pipeline stages");
     static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0, "tiles keep the swizzle atoms aligned");
     static_assert(GS * (A2_TILE + B2_TILE) <= STAGE, "pass-2 slices fit a stage");
-    // one resident CTA per SM whatever else runs there (TMEM: all 512 columns)
-    static_assert(SMEM > 232448 / 2, "shared memory keeps the kernel at one CTA per SM");
+    // one resident CTA per SM (all 512 TMEM columns: a second CTA would only wait in tcgen05.alloc)
+    static_assert(SMEM >= kOneCtaPerSm && SMEM <= kSmemMax, "shared memory keeps the kernel at one CTA per SM");
 };
 
 // Bounded wait that also ends when the abort flag is raised; true when the phase completed.
@@ -1062,7 +1071,8 @@ struct OzWidePairCfg {
     static constexpr int B2_TILE = (NT / 2) * RB2;
     static constexpr int STAGE = S * (A_TILE + B_TILE);
     static constexpr int STAGES = (kSmemBudget / STAGE) > 4 ? 4 : (kSmemBudget / STAGE);
-    static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+    static constexpr int SMEM = STAGES * STAGE + 1024 + 256 > kOneCtaPerSm ? STAGES * STAGE + 1024 + 256
+                                                                          : kOneCtaPerSm;
     static constexpr uint32_t LAYOUT = 6u, SBO = 8u * RB;      // SWIZZLE_32B
     static constexpr uint32_t LAYOUT2 = 4u, SBO2 = 8u * RB2;   // SWIZZLE_64B
     // kind::i8: D s32, A and B s8, K-major, N = 128, M = 256 (the pair)
@@ -1072,6 +1082,7 @@ struct OzWidePairCfg {
     static_assert(STAGES >= 2, "at least two pipeline stages");
     static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0 && B2_TILE % 1024 == 0, "swizzle atoms aligned");
     static_assert(GS * (A2_TILE + B2_TILE) <= STAGE, "pass-2 slices fit a stage");
+    static_assert(SMEM >= kOneCtaPerSm && SMEM <= kSmemMax, "one resident CTA per SM");
 };
 
 template <int EPI, int S>
