@@ -55,15 +55,16 @@ class PurificationSettings:
     # initialize_purification, source/purification_settings.f90:91-218
     def read(self, text: str) -> "PurificationSettings":
         for raw in text.splitlines():
-            toks = raw.split()
-            if not toks:
+            strs, floats = _readline(raw)
+            if not strs and not floats:
                 continue
-            arg1 = toks[0]
+            arg1 = strs[0] if strs else ""
             if arg1.startswith("!"):
                 continue
-            if len(toks) >= 2 and toks[1] == "=":
-                arg3 = toks[2] if len(toks) > 2 else ""
-                num = _first_float(toks[2:])
+            arg2 = strs[1] if len(strs) > 1 else ""
+            if arg2 == "=":
+                arg3 = strs[2] if len(strs) > 2 else ""
+                num = floats[0] if floats else None
                 if arg1 == "mode":
                     self.mode = _pick(_MODE, arg3, "Error: .PUR contains invalid type definition")
                 elif arg1 == "submatrix_columns":
@@ -103,10 +104,32 @@ def _pick(table, key, msg):
     return table[key]
 
 
-def _first_float(toks):
-    for t in toks:
-        try:
-            return float(t.replace("d", "e").replace("D", "e"))
-        except ValueError:
+def _readline(raw: str):
+    """Tokens of one settings line as source/readline.f90:1-64 splits them.
+
+    The record is read into an 80-character variable (the rest is dropped),
+    split at blanks and tabs, and each token is classed by checktype
+    (source/readl2.f90:52-90): a number if it reads as a real, a logical if it
+    is exactly ``true`` or ``false`` (dropped here: no setting reads them), a
+    string otherwise.  Strings and numbers are numbered separately, so in
+    ``cycles = 40`` the value is the first number and ``arg3`` is empty.
+    """
+    strs, floats = [], []
+    for tok in raw[:80].replace("\t", " ").split(" "):
+        if not tok:
             continue
-    return None
+        num = _checktype_number(tok)
+        if num is not None:
+            floats.append(num)
+        elif tok not in ("true", "false"):
+            strs.append(tok)
+    return strs, floats
+
+
+def _checktype_number(tok: str):
+    # a Fortran real field: digits with an optional point and an exponent
+    # introduced by e or d (either case)
+    try:
+        return float(tok.replace("d", "e").replace("D", "e"))
+    except ValueError:
+        return None
