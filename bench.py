@@ -24,6 +24,11 @@ C200H402 chain with per-atom columns, the 512-H2O box with seeded k-means
 columns, all with filter 1e-4; value = device time of the call (inputs copied
 in first), e2e = the whole host call.
 
+--workload purify_types measures the reference's full-matrix purification
+module (dormant in twoscf: McWeeny, Pade, Newton-Schulz and eigen-sign solvers
+with the chemical-potential search, source/purification.f90) in FP64 on the
+32-H2O cluster, one call per solver type; the oracle is the CPU baseline.
+
 --workload lattice256 measures the uneven multi-instance batch instead: 256
 synthetic cubic-lattice systems (20-400 atoms, ndim 153-3064) purified by
 ptbgpu_tc_purify_batch (host worker threads, one stream each); one step = the
@@ -185,6 +190,27 @@ def run_reference(args, rank):
             "config": {"workload": desc, "global_batch": 1, "seq_len": sysobj.ndim, "parallelism": "replicas"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
+    if args.workload == "purify_types":
+        s = synth.make_config(0)
+        times = []
+        for i in range(args.warmup + args.steps):
+            t = sum(purify_oracle(s, pt, me, it)[0] for pt, me, it, _ in PURIFY_TYPES)
+            if i >= args.warmup:
+                times.append(t)
+        v = statistics.median(times)
+        cores = os.cpu_count()
+        line = {
+            "impl": "reference", "metric": METRIC, "value": v, "unit": PURIFY_UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": PURIFY_DESC, "global_batch": 1, "seq_len": s.ndim, "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": PURIFY_UNIT, "cores": cores, "kind": "port",
+                             "sample": "oracle purification (numpy / scipy OpenBLAS), one call per type, "
+                                       "whole workload"},
+            "e2e": {"value": v, "unit": PURIFY_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line), flush=True)
         return
@@ -385,6 +411,105 @@ def run_sm(args, rank, world, local, pg):
     }
     if acc:
         line["accuracy"] = acc
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+# The solver types of the reference's full-matrix purification module
+# (source/purification_settings.f90:6-27): type, metric, iterative metric, label.
+PURIFY_TYPES = [
+    (1, 2, False, "mcweeny, inverse_sqrt"),
+    (1, 1, False, "mcweeny, inverse"),
+    (2, 2, False, "pade, inverse_sqrt"),
+    (3, 2, False, "newton, inverse_sqrt"),
+    (3, 1, True, "newton, inverse, iterative_inversion"),
+    (4, 2, False, "diag, inverse_sqrt"),
+]
+PURIFY_DESC = ("full-matrix purification module (mu search with McWeeny / Pade / Newton-Schulz / eigen-sign "
+               "solvers), 32-H2O cluster (96 atoms, ndim 736, nel 256), filter 1e-4, one call per solver type")
+PURIFY_UNIT = "s/sweep-of-6-types"
+
+
+def purify_oracle(s, ptype, metric, it):
+    """One oracle call of the purification module with the workload's filter."""
+    from oracle import ptb_oracle as O
+    pur = O.PurificationSettings(type=ptype, metric_type=metric, metric_iterative=it, nel=s.nel)
+    t0 = time.perf_counter()
+    P, mu, steps = O.purification(pur, s.ndim, O.filter_matrix_sym(s.Hvec, SM_FILTER),
+                                  O.filter_matrix_sym(s.Svec, SM_FILTER))
+    return time.perf_counter() - t0, P, mu, steps
+
+
+def run_purify_types(args, rank, world, local, pg):
+    """The reference's dormant full-matrix purification (purification_wrapper,
+    source/purification.f90:28-782) in FP64 on the device, once per solver type;
+    one step = the six calls.  N > 1 runs replicas."""
+    import torch
+
+    from ptb_b200 import Context, Options, PurificationSettings, synth
+
+    s = synth.make_config(0)
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    o = Options(filter=SM_FILTER)
+    npk = s.ndim * (s.ndim + 1) // 2
+    per, step_ms, step_wall, launches, flops = [], 0.0, 0.0, 0, 0.0
+    with ClockSampler(local) as clk:
+        for ptype, metric, it, label in PURIFY_TYPES:
+            pur = PurificationSettings(type=ptype, metric_type=metric, metric_iterative=it, nel=s.nel)
+            for _ in range(args.warmup):
+                ctx.purification(pur, s.ndim, s.Hvec, s.Svec, o)
+            ms, walls, sts = [], [], []
+            for _ in range(args.steps):
+                torch.cuda.synchronize()
+                barrier(pg)
+                t0 = time.perf_counter()
+                P, st = ctx.purification(pur, s.ndim, s.Hvec, s.Svec, o)
+                walls.append(time.perf_counter() - t0)
+                ms.append(st.ms_solve)
+                sts.append(st)
+            m = reduce_max(pg, statistics.median(ms))
+            w = reduce_max(pg, statistics.median(walls))
+            step_ms += m
+            step_wall += w
+            launches += sum(x.kernel_launches for x in sts)
+            flops += sts[-1].flops
+            per.append({"type": label, "ms": m, "mu_steps": int(sts[-1].mu_iterations),
+                        "sign_iterations": int(sts[-1].iterations), "mu": sts[-1].mu,
+                        "dgemm_tflops": sts[-1].flops / (m / 1e3) / 1e12, "P": P})
+    clocks = clk.summary()
+    if rank != 0:
+        ctx.close()
+        return
+    cpu_s = 0.0
+    if not args.no_cpu_baseline:
+        for (ptype, metric, it, _), d in zip(PURIFY_TYPES, per):
+            t, Pref, mu, steps = purify_oracle(s, ptype, metric, it)
+            cpu_s += t
+            d.update({"oracle_s": t, "max_abs_dP_vs_oracle": float(np.max(np.abs(d["P"] - Pref))),
+                      "mu_oracle": mu, "mu_steps_oracle": int(steps)})
+    for d in per:
+        d.pop("P")
+    tf = flops / (step_ms / 1e3) / 1e12
+    line = {
+        "metric": METRIC, "value": step_ms / 1e3, "unit": PURIFY_UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": PURIFY_DESC, "global_batch": 1, "seq_len": s.ndim,
+                   "parallelism": "one GPU" if world == 1 else f"replicas x{world}",
+                   "l2": "small case: inputs (4.3 MB packed) fit in L2; latency-bound"},
+        "e2e": {"value": step_wall, "unit": PURIFY_UNIT, "h2d_bytes_per_step": len(PURIFY_TYPES) * 2 * npk * 8,
+                "d2h_bytes_per_step": len(PURIFY_TYPES) * npk * 8},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp64", "kernel": "cuBLAS DGEMM / cuSOLVER DSYEVD with the library's kernels",
+                     "achieved": tf, "peak": 37.0, "unit": "TFLOP/s", "frac": tf / 37.0, "traffic": None,
+                     "peak_kind": "nominal B200 FP64 (no measured FP64 figure on this pool)",
+                     "work": "2 n^3 per DGEMM issued, eigensolves not counted, over the six calls' device time"},
+        "cpu_baseline": ({"value": cpu_s, "unit": PURIFY_UNIT, "cores": os.cpu_count(), "kind": "port",
+                          "sample": "oracle purification (numpy / scipy OpenBLAS), one call per type, whole workload"}
+                         if cpu_s else None),
+        "clocks": clocks, "types": per,
+    }
     print(json.dumps(line), flush=True)
     ctx.close()
 
@@ -612,7 +737,8 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--no-compare-fp64", dest="compare_fp64", action="store_false")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["water512", "lattice256"] + sorted(SM_WORKLOADS), default="water512")
+    ap.add_argument("--workload", choices=["water512", "lattice256", "purify_types"] + sorted(SM_WORKLOADS),
+                    default="water512")
     ap.add_argument("--workers", type=int, default=8, help="worker streams of the lattice256 batch")
     ap.add_argument("--nmol", type=int, default=512,
                     help="water molecules in the box (512 = the benchmark workload; smaller boxes for profiling)")
@@ -631,6 +757,8 @@ def main():
             run_batch(args, rank, world, local, pg)
         elif args.workload in SM_WORKLOADS:
             run_sm(args, rank, world, local, pg)
+        elif args.workload == "purify_types":
+            run_purify_types(args, rank, world, local, pg)
         else:
             run_ours(args, rank, world, local, pg)
     finally:

@@ -67,6 +67,7 @@ struct Ctx {
     int prl;
     DevBuf scratch[8];
     double* m[8];
+    double gemm_flops = 0.0;   // 2n^3 per DGEMM issued (eigensolves not counted)
     Ctx(ptbgpu_ctx* cc, int64_t nn, int p) : c(cc), n(nn), thr(thresholds(nn)), prl(p) {
         for (int k = 0; k < 8; ++k) {
             scratch[k].reserve(sizeof(double) * nn * nn);
@@ -80,6 +81,7 @@ struct Ctx {
         const double beta = 0.0;
         PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, transb ? CUBLAS_OP_T : CUBLAS_OP_N, (int)n, (int)n, (int)n,
                                &alpha, A, (int)n, B, (int)n, &beta, C, (int)n));
+        gemm_flops += 2.0 * (double)n * (double)n * (double)n;
     }
     double frob(const double* a) { return frob_dev(c, n, n, a); }
     void nan_check(const double* a, const char* msg) {
@@ -389,6 +391,7 @@ void purify_ref_device(ptbgpu_ctx* c, const ptbgpu_pur_settings& pur, int64_t n,
         st->mu = chempot;
         st->mu_iterations = steps;
         st->iterations = iters;
+        st->flops = x.gemm_flops;
     }
 }
 
