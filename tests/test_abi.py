@@ -41,6 +41,62 @@ def test_struct_layouts_match_header(cname, pyclass):
     assert ctypes.sizeof(pyclass) == 8 * len(pyclass._fields_)
 
 
+C_CALLER = r"""
+#include <stdio.h>
+#include <string.h>
+#include "ptbgpu.h"
+
+int main(void) {
+    ptbgpu_pur_settings s;
+    ptbgpu_opts o;
+    ptbgpu_stats st;
+    int32_t tiles[4 * 64];
+    int64_t nt = 0, info[4];
+    ptbgpu_ctx* c = NULL;
+    int rc;
+    ptbgpu_default_settings(&s);
+    ptbgpu_default_opts(&o);
+    memset(&st, 0, sizeof st);
+    if (s.type != PTBGPU_TYPE_DIAG || s.cycles != 40 || s.chempot_cycles != 60 || s.chempot_guess != -1.5)
+        return 2;
+    if (o.precision != PTBGPU_PREC_MIXED) return 3;
+    rc = ptbgpu_oz_tiles(256, 8, 64, 0, 0, 0, 0, tiles, 64, &nt, info);
+    if (rc != PTBGPU_OK || nt <= 0) return 4;
+    if (ptbgpu_oz_tiles(0, 8, 64, 0, 0, 0, 0, tiles, 64, &nt, info) != PTBGPU_EINVAL) return 5;
+    rc = ptbgpu_init(0, &c);
+    printf("init %d tiles %lld\n", rc, (long long)nt);
+    if (rc == PTBGPU_OK) ptbgpu_finalize(c);
+    return 0;
+}
+"""
+
+
+def test_header_compiles_as_c99_and_links(tmp_path):
+    """A C caller (what the Fortran ISO_C_BINDING shim binds to) compiles against
+    the header with -std=c99 -pedantic -Werror, links libptbgpu and makes the
+    host-only calls; without a GPU, ptbgpu_init returns a status instead of
+    failing the process."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    lib = api.library_path()
+    src = tmp_path / "caller.c"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    cmd = [gcc, "-std=c99", "-pedantic", "-Wall", "-Wextra", "-Werror", f"-I{HEADER.parent}", str(src),
+           f"-L{lib.parent}", "-l:" + lib.name, f"-Wl,-rpath,{lib.parent}", "-Wl,--allow-shlib-undefined",
+           "-o", str(exe)]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    rc = int(out.stdout.split()[1])
+    import torch
+    if not torch.cuda.is_available():
+        assert rc != api.OK
+
+
 def test_init_fails_cleanly_without_gpu():
     import torch
     if torch.cuda.is_available():
