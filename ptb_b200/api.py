@@ -165,6 +165,25 @@ def npacked(n: int) -> int:
     return n * (n + 1) // 2
 
 
+# The C-ABI takes bare pointers and reads as many elements as the sizes say, so
+# the lengths of the host arrays are checked here, before any call.
+def _packed(a, ndim: int, what: str) -> np.ndarray:
+    """A packed symmetric matrix of order ndim as a contiguous float64 array."""
+    x = _f64(a)
+    if x.size != npacked(max(int(ndim), 0)):
+        raise PtbGpuError(EINVAL, f"{what} has {x.size} elements; a packed matrix of order {ndim} has "
+                                  f"{npacked(max(int(ndim), 0))}")
+    return x
+
+
+def _vec(a, count: int, what: str, conv=None) -> np.ndarray:
+    """An array of exactly count elements (float64, or int64 with conv=_i64)."""
+    x = (conv or _f64)(a)
+    if x.size != max(int(count), 0):
+        raise PtbGpuError(EINVAL, f"{what} has {x.size} elements, expected {max(int(count), 0)}")
+    return x
+
+
 @dataclass
 class Stats:
     mu: float = 0.0
@@ -265,15 +284,15 @@ class Context:
     # ---- reference entry points ------------------------------------------
     def filter_matrix_sym(self, A: np.ndarray, n: int, filter: float) -> np.ndarray:
         """source/pgtb.f90:1532-1547, returns the filtered packed copy."""
-        out = _f64(A).copy()
+        out = _packed(A, n, "A").copy()
         self._check(self._lib.ptbgpu_filter_packed(self._h, int(n), _dptr(out), float(filter)))
         return out
 
     def check_density(self, ndim: int, P: np.ndarray, S: np.ndarray, H: np.ndarray | None = None) -> Stats:
         """get_nel, band_structure and idempotent (source/metrics.f90:144-360) on packed data."""
         st = _Stats()
-        P, S = _f64(P), _f64(S)
-        Hp = _dptr(_f64(H)) if H is not None else None
+        P, S = _packed(P, ndim, "P"), _packed(S, ndim, "S")
+        Hp = _dptr(_packed(H, ndim, "H")) if H is not None else None
         self._check(self._lib.ptbgpu_check_density(self._h, int(ndim), _dptr(P), _dptr(S), Hp, C.byref(st)))
         return Stats.from_c(st)
 
@@ -281,10 +300,10 @@ class Context:
                          xyz: np.ndarray, aoat: np.ndarray, submatrix_columns: int, submatrix_mode: int,
                          partition: np.ndarray | None = None, opts: Options | None = None):
         """Submatrix density step, source/sm.f90:34-409.  Returns (Pvec, Stats)."""
-        H, S = _f64(Hvec), _f64(Svec)
+        H, S = _packed(Hvec, ndim, "Hvec"), _packed(Svec, ndim, "Svec")
         P = np.zeros(npacked(ndim))
-        xyz_a = _f64(xyz)
-        ao = _i64(aoat)
+        xyz_a = _vec(xyz, 3 * n, "xyz")
+        ao = _vec(aoat, ndim, "aoat", _i64)
         part = _i64(partition) if partition is not None else None
         st = _Stats()
         o = (opts or Options()).to_c()
@@ -303,11 +322,13 @@ class Context:
         nsm = C.c_int64(0)
         dims = np.zeros(ndim, dtype=np.int64)
         o = (opts or Options()).to_c()
-        ao = _i64(aoat)
+        H, S = _packed(Hvec, ndim, "Hvec"), _packed(Svec, ndim, "Svec")
+        xyz_a = _vec(xyz, 3 * n, "xyz")
+        ao = _vec(aoat, ndim, "aoat", _i64)
         part = _i64(partition) if partition is not None else None
         ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
         self._check(self._lib.ptbgpu_sm_plan(
-            self._h, int(ndim), _dptr(_f64(Hvec)), _dptr(_f64(Svec)), int(n), _dptr(_f64(xyz)), ip(ao),
+            self._h, int(ndim), _dptr(H), _dptr(S), int(n), _dptr(xyz_a), ip(ao),
             int(submatrix_columns), int(submatrix_mode), ip(part) if part is not None else None, C.byref(o),
             C.byref(nsm), ip(dims)))
         return dims[:nsm.value].copy()
@@ -341,9 +362,11 @@ class Context:
         nsm = C.c_int64(0)
         eff = C.c_double(0.0)
         o = (opts or Options()).to_c()
-        ao = _i64(aoat)
+        H, S = _packed(Hvec, ndim, "Hvec"), _packed(Svec, ndim, "Svec")
+        xyz_a = _vec(xyz, 3 * n, "xyz")
+        ao = _vec(aoat, ndim, "aoat", _i64)
         self._check(self._lib.ptbgpu_kmeans_partition(
-            self._h, int(ndim), _dptr(_f64(Hvec)), _dptr(_f64(Svec)), int(n), _dptr(_f64(xyz)),
+            self._h, int(ndim), _dptr(H), _dptr(S), int(n), _dptr(xyz_a),
             ao.ctypes.data_as(C.POINTER(C.c_int64)), C.c_uint64(seed), C.byref(o),
             part.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(nsm), C.byref(eff)))
         return part, int(nsm.value), float(eff.value)
@@ -351,7 +374,7 @@ class Context:
     def purification(self, pur: PurificationSettings, ndim: int, H: np.ndarray, S: np.ndarray,
                      opts: Options | None = None):
         """purification_wrapper, source/purification.f90:28-80.  Returns (Pvec, Stats)."""
-        Hh, Sh = _f64(H), _f64(S)
+        Hh, Sh = _packed(H, ndim, "H"), _packed(S, ndim, "S")
         P = np.zeros(npacked(ndim))
         st = _Stats()
         cs = pur.to_c(_Settings)
@@ -365,7 +388,7 @@ class Context:
         """Trace-correcting purification (FP64 or bf16x3 + FP64 refinement).  Returns (Pvec, Stats).
         out: a preallocated contiguous float64 array of npacked(ndim) elements for P (e.g. in
         pinned memory, which the device-to-host copy needs for full speed)."""
-        Hh, Sh = _f64(H), _f64(S)
+        Hh, Sh = _packed(H, ndim, "H"), _packed(S, ndim, "S")
         if out is not None:
             if out.dtype != np.float64 or out.size != npacked(ndim) or not out.flags.c_contiguous:
                 raise ValueError("out must be a contiguous float64 array of npacked(ndim) elements")
@@ -394,8 +417,8 @@ class Context:
         m = max(n, 1)
         ndim = (C.c_int64 * m)(*[int(s[0]) for s in systems])
         nel = (C.c_int64 * m)(*[int(s[1]) for s in systems])
-        Hs = [_f64(s[2]) for s in systems]
-        Ss = [_f64(s[3]) for s in systems]
+        Hs = [_packed(s[2], s[0], f"H of system {i}") for i, s in enumerate(systems)]
+        Ss = [_packed(s[3], s[0], f"S of system {i}") for i, s in enumerate(systems)]
         Ps = [np.zeros(npacked(int(s[0]))) for s in systems]
         arr = lambda xs: (C.POINTER(C.c_double) * m)(*[_dptr(x) for x in xs])
         st = (_Stats * max(n, 1))()
@@ -409,22 +432,27 @@ class Context:
                    timed: bool = False):
         """Iteration-2 XC long-range damping, source/pgtb.f90:482-513: returns H + the
         P-dependent term (packed); timed: (H, device ms of the AO-pair update)."""
-        a = np.ascontiguousarray(aoat, dtype=np.int64)
-        Hout = _f64(H).copy()
+        a = _vec(aoat, ndim, "aoat", _i64)
+        Hout = _packed(H, ndim, "H").copy()
+        rab_, rad_ = _packed(rab, nat, "rab"), _vec(rad, nat, "rad")
+        hao_, xd_ = _vec(hao, ndim, "hao"), _vec(xdiag, ndim, "xdiag")
+        Pp = _packed(P, ndim, "P")
         ms = C.c_double(0.0)
         self._check(self._lib.ptbgpu_xc_damping(self._h, int(nat), int(ndim), a.ctypes.data_as(C.POINTER(C.c_int64)),
-                                                _dptr(_f64(rab)), _dptr(_f64(rad)), _dptr(_f64(hao)),
-                                                _dptr(_f64(xdiag)), _dptr(_f64(P)), _dptr(Hout), C.byref(ms)))
+                                                _dptr(rab_), _dptr(rad_), _dptr(hao_), _dptr(xd_), _dptr(Pp),
+                                                _dptr(Hout), C.byref(ms)))
         return (Hout, ms.value) if timed else Hout
 
     def xc_damping_device(self, nat: int, ndim: int, aoat, rab, rad, hao, xdiag, dP: int, dH: int) -> float:
         """Same on device-resident packed P and H (raw device pointers, H updated in
         place); returns the device ms of the AO-pair update."""
-        a = np.ascontiguousarray(aoat, dtype=np.int64)
+        a = _vec(aoat, ndim, "aoat", _i64)
+        rab_, rad_ = _packed(rab, nat, "rab"), _vec(rad, nat, "rad")
+        hao_, xd_ = _vec(hao, ndim, "hao"), _vec(xdiag, ndim, "xdiag")
         ms = C.c_double(0.0)
         self._check(self._lib.ptbgpu_xc_damping_device(self._h, int(nat), int(ndim),
-                                                       a.ctypes.data_as(C.POINTER(C.c_int64)), _dptr(_f64(rab)),
-                                                       _dptr(_f64(rad)), _dptr(_f64(hao)), _dptr(_f64(xdiag)),
+                                                       a.ctypes.data_as(C.POINTER(C.c_int64)), _dptr(rab_),
+                                                       _dptr(rad_), _dptr(hao_), _dptr(xd_),
                                                        C.c_void_p(dP), C.c_void_p(dH), C.byref(ms)))
         return ms.value
 
@@ -436,8 +464,8 @@ class Context:
         m = max(n, 1)
         ndim = (C.c_int64 * m)(*[int(s[0]) for s in systems])
         nel = (C.c_int64 * m)(*[int(s[1]) for s in systems])
-        Hs = [_f64(s[2]) for s in systems]
-        Ss = [_f64(s[3]) for s in systems]
+        Hs = [_packed(s[2], s[0], f"H of system {i}") for i, s in enumerate(systems)]
+        Ss = [_packed(s[3], s[0], f"S of system {i}") for i, s in enumerate(systems)]
         Ps = [np.zeros(npacked(int(s[0]))) for s in systems]
         arr = lambda xs: (C.POINTER(C.c_double) * m)(*[_dptr(x) for x in xs])
         st = (_Stats * m)()
@@ -457,7 +485,7 @@ class Context:
         """Dense FP64 diagonalisation + Fermi smearing, source/pgtb.f90:1066-1170.
 
         Returns (Pvec, e, focc, Stats)."""
-        Hh, Sh = _f64(H), _f64(S)
+        Hh, Sh = _packed(H, ndim, "H"), _packed(S, ndim, "S")
         P = np.zeros(npacked(ndim))
         e = np.zeros(ndim)
         focc = np.zeros(ndim)
@@ -511,7 +539,8 @@ class Context:
         s34 = np.zeros((nao, nao), dtype=np.float32, order="F")
         s14 = np.zeros((nao, nao), dtype=np.float32, order="F")
         fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
-        self._check(self._lib.ptbgpu_mlpop14(self._h, int(nao), _dptr(_f64(Svec)), float(x), fp(s34), fp(s14)))
+        Sp = _packed(Svec, nao, "Svec")
+        self._check(self._lib.ptbgpu_mlpop14(self._h, int(nao), _dptr(Sp), float(x), fp(s34), fp(s14)))
         return s34, s14
 
     def mlpop2(self, n: int, nao: int, Pvec: np.ndarray, s1: np.ndarray, s2: np.ndarray, aoat: np.ndarray,
@@ -521,13 +550,17 @@ class Context:
         indexed [row, col]; aoat / shell2ao 1-based."""
         f1 = np.asfortranarray(s1, dtype=np.float32)
         f2 = np.asfortranarray(s2, dtype=np.float32)
+        for name, f in (("s1", f1), ("s2", f2)):
+            if f.shape != (nao, nao):
+                raise PtbGpuError(EINVAL, f"{name} has shape {f.shape}, expected ({nao}, {nao})")
         q = np.zeros(n)
         qsh = np.zeros((n, 10))
         st = _Stats()
         fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
         ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
-        a, sh = _i64(aoat), _i64(shell2ao)
-        self._check(self._lib.ptbgpu_mlpop2(self._h, int(n), int(nao), _dptr(_f64(Pvec)), fp(f1), fp(f2), ip(a),
+        a, sh = _vec(aoat, nao, "aoat", _i64), _vec(shell2ao, nao, "shell2ao", _i64)
+        Pp = _packed(Pvec, nao, "Pvec")
+        self._check(self._lib.ptbgpu_mlpop2(self._h, int(n), int(nao), _dptr(Pp), fp(f1), fp(f2), ip(a),
                                             ip(sh), _dptr(q), _dptr(qsh), C.byref(st)))
         return q, qsh, Stats.from_c(st)
 
@@ -539,7 +572,7 @@ class Context:
         qsh = np.zeros((n, 10))
         st = _Stats()
         ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
-        a, sh = _i64(aoat), _i64(shell2ao)
+        a, sh = _vec(aoat, nao, "aoat", _i64), _vec(shell2ao, nao, "shell2ao", _i64)
         self._check(self._lib.ptbgpu_mlpop2_device(self._h, int(n), int(nao), C.c_void_p(dP), C.c_void_p(ds1),
                                                    C.c_void_p(ds2), ip(a), ip(sh), _dptr(q), _dptr(qsh),
                                                    C.byref(st)))

@@ -103,3 +103,51 @@ def test_init_fails_cleanly_without_gpu():
         pytest.skip("a GPU is present")
     with pytest.raises(api.PtbGpuError):
         api.Context(0)
+
+
+class _NoCalls:
+    """Stands in for the loaded library: any C call fails the test."""
+
+    def __getattr__(self, name):
+        raise AssertionError(f"{name} was called with arrays of the wrong length")
+
+
+def _unbound_context():
+    ctx = api.Context.__new__(api.Context)
+    ctx._lib, ctx._h, ctx.device = _NoCalls(), None, 0
+    return ctx
+
+
+def test_wrong_array_lengths_are_rejected_before_the_c_call():
+    import numpy as np
+    ctx = _unbound_context()
+    n, nat = 10, 4
+    pk, short = np.zeros(n * (n + 1) // 2), np.zeros(n * (n + 1) // 2 - 1)
+    aoat, xyz = np.repeat(np.arange(1, nat + 1), [3, 3, 2, 2]), np.zeros((nat, 3))
+    calls = [
+        lambda: ctx.filter_matrix_sym(short, n, 1e-5),
+        lambda: ctx.check_density(n, pk, short),
+        lambda: ctx.check_density(n, pk, pk, short),
+        lambda: ctx.sm_stupid_simple(n, 8, short, pk, nat, xyz, aoat, 2, 2),
+        lambda: ctx.sm_stupid_simple(n, 8, pk, pk, nat, xyz[:3], aoat, 2, 2),
+        lambda: ctx.sm_stupid_simple(n, 8, pk, pk, nat, xyz, aoat[:-1], 2, 2),
+        lambda: ctx.sm_plan(n, pk, short, nat, xyz, aoat, 2, 2),
+        lambda: ctx.kmeans_partition(n, pk, pk, nat, xyz, aoat[1:]),
+        lambda: ctx.purification(api.PurificationSettings(), n, pk, short),
+        lambda: ctx.tc_purify(n, 8, short, pk),
+        lambda: ctx.tc_purify(n + 1, 8, pk, pk),
+        lambda: ctx.tc_purify_batch([(n, 8, pk, pk), (n, 8, pk, short)]),
+        lambda: ctx.tc_purify_grouped([(n, 8, short, pk)]),
+        lambda: ctx.solve2(1, n, 8, 0, pk, short),
+        lambda: ctx.mlpop14(n, short),
+        lambda: ctx.mlpop2(nat, n, short, np.eye(n), np.eye(n), aoat, aoat),
+        lambda: ctx.mlpop2(nat, n, pk, np.eye(n - 1), np.eye(n), aoat, aoat),
+        lambda: ctx.mlpop2(nat, n, pk, np.eye(n), np.eye(n), aoat, aoat[:-2]),
+        lambda: ctx.xc_damping(nat, n, aoat, np.zeros(10), np.zeros(nat), np.zeros(n), np.zeros(n), short, pk),
+        lambda: ctx.xc_damping(nat, n, aoat, np.zeros(9), np.zeros(nat), np.zeros(n), np.zeros(n), pk, pk),
+        lambda: ctx.xc_damping_device(nat, n, aoat, np.zeros(10), np.zeros(nat + 1), np.zeros(n), np.zeros(n), 0, 0),
+    ]
+    for k, call in enumerate(calls):
+        with pytest.raises(api.PtbGpuError) as ei:
+            call()
+        assert ei.value.code == api.EINVAL, k
