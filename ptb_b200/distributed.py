@@ -6,8 +6,15 @@ electron count summed over all submatrices (source/sm.f90:322-340).  Here each
 rank plans the whole system (grouping, pattern scan: cheap and identical on
 every rank), prepares a size-balanced share of the submatrices on its own
 device, and every rank runs the same bisection with one all-reduce of the
-8-byte partial electron count per step.  The owned columns of P are disjoint
-between ranks, so one all-reduce (sum) of the packed P assembles the result.
+partial electron count per step.  The owned columns of P are disjoint between
+ranks, so one all-reduce (sum) of the packed P assembles the result.
+
+Errors are collective: each all-reduce also carries one status word per rank
+(0, or the failing rank's PTBGPU_E* code; -1 for a host exception).  A rank
+whose plan or prepare phase fails still joins the first bisection all-reduce,
+one whose finish phase fails joins the all-reduce of P, and after that
+collective every rank raises.  No rank is left waiting in a collective that a
+failed peer will never join.
 
 The per-rank device work goes through the C-ABI phases (ptbgpu_sm_plan /
 _prepare / _nel / _finish); anything with the same four methods can stand in
@@ -19,7 +26,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .api import EITER, Context, Options, PtbGpuError
+from .api import EINVAL, EITER, Context, Options, PtbGpuError
 
 # REAL(4) literals of the reference's stop test, source/sm.f90:191-192
 TOL_MU = float(np.float32(1e-3))
@@ -85,6 +92,25 @@ class DeviceShard:
         return self.ctx.sm_finish(ndim, mu)
 
 
+def _status_code(err) -> int:
+    if err is None:
+        return 0
+    return int(err.code) if isinstance(err, PtbGpuError) else -1
+
+
+def _raise_failures(status, err, phase: str):
+    """Raises on every rank when any rank's status word is set: the failing rank
+    re-raises its own error, the others a PtbGpuError naming the first failing
+    rank and its code (EINVAL for a host exception)."""
+    failed = [(r, int(c)) for r, c in enumerate(status) if c != 0]
+    if not failed:
+        return
+    if err is not None:
+        raise err
+    r, c = failed[0]
+    raise PtbGpuError(c if c > 0 else EINVAL, f"rank {r} failed in the {phase} phase (status {c})")
+
+
 @dataclass
 class ShardInfo:
     mu: float
@@ -106,28 +132,56 @@ def sm_stupid_simple_sharded(shard, ndim: int, nelref: int, Hvec: np.ndarray, Sv
 
     world = dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
     rank = dist.get_rank(group) if world > 1 else 0
-    dims = np.asarray(shard.plan(ndim, Hvec, Svec, n, xyz, aoat, submatrix_columns, submatrix_mode, partition,
-                                 opts or Options()))
-    ids = assign_submatrices(dims, world)[rank]
-    shard.prepare(ids)
+    dims, ids, err = np.zeros(0, dtype=np.int64), [], None
+    try:
+        dims = np.asarray(shard.plan(ndim, Hvec, Svec, n, xyz, aoat, submatrix_columns, submatrix_mode, partition,
+                                     opts or Options()))
+        ids = assign_submatrices(dims, world)[rank]
+        shard.prepare(ids)
+    except Exception as e:   # noqa: BLE001 -- reported to the peers, then re-raised
+        if world == 1:
+            raise
+        err = e
     dev = torch.device("cpu")
     if world > 1 and dist.get_backend(group) == "nccl":
         dev = torch.device("cuda", torch.cuda.current_device())
+    phase = ["plan, prepare or first bisection step"]
 
     def nel_total(mu: float) -> float:
-        v = shard.nel(mu)
+        nonlocal err
         if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
+            return shard.nel(mu)
+        v = 0.0
+        if err is None:
+            try:
+                v = shard.nel(mu)
+            except Exception as e:   # noqa: BLE001
+                err = e
+        t = torch.zeros(1 + world, dtype=torch.float64, device=dev)
+        t[0] = v
+        t[1 + rank] = _status_code(err)
         dist.all_reduce(t, group=group)
-        return float(t.item())
+        h = t.cpu().tolist()
+        _raise_failures(h[1:], err, phase[0])
+        phase[0] = "bisection"   # later failures happen in a bisection step
+        return h[0]
 
     mu, nel, trace, ok = mu_bisect(nel_total, float(nelref))
     if not ok:
         raise PtbGpuError(EITER, "chemical potential bisection did not converge")
-    P = shard.finish(ndim, mu)
-    if world > 1:
-        t = torch.from_numpy(P).to(dev)
-        dist.all_reduce(t, group=group)
-        P = t.cpu().numpy()
-    return P, ShardInfo(mu, nel, int(dims.shape[0]), ids, dims, trace)
+    if world == 1:
+        return shard.finish(ndim, mu), ShardInfo(mu, nel, int(dims.shape[0]), ids, dims, trace)
+    npk = ndim * (ndim + 1) // 2
+    P = np.zeros(npk)
+    try:
+        P = shard.finish(ndim, mu)
+    except Exception as e:   # noqa: BLE001
+        err = e
+    t = torch.zeros(npk + world, dtype=torch.float64, device=dev)
+    if err is None:
+        t[:npk] = torch.from_numpy(np.ascontiguousarray(P, dtype=np.float64)).to(dev)
+    t[npk + rank] = _status_code(err)
+    dist.all_reduce(t, group=group)
+    h = t.cpu().numpy()
+    _raise_failures(h[npk:], err, "finish")
+    return h[:npk].copy(), ShardInfo(mu, nel, int(dims.shape[0]), ids, dims, trace)

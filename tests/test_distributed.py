@@ -86,3 +86,75 @@ def test_two_gloo_ranks_match_oracle():
     assert len(ids0) > 0 and len(ids1) > 0 and not set(ids0) & set(ids1)
     assert np.array_equal(P0, P1) and mu0[0] == mu1[0]
     assert np.max(np.abs(P0 - ref.Pvec)) < 1e-12
+
+
+class _FailingShard(OracleShard):
+    """The oracle shard with a planted failure on one rank (host-side error
+    injection: the failing phase raises the library's exception type)."""
+
+    def __init__(self, rank, fail_rank, where):
+        self.rank, self.fail_rank, self.where, self.calls = rank, fail_rank, where, 0
+
+    def _maybe_fail(self, where):
+        if self.rank == self.fail_rank and self.where == where:
+            from ptb_b200.api import ENOTSPD, PtbGpuError
+            raise PtbGpuError(ENOTSPD, f"planted failure in {where}")
+
+    def prepare(self, ids):
+        self._maybe_fail("prepare")
+        return super().prepare(ids)
+
+    def nel(self, mu):
+        self.calls += 1
+        if self.calls == 3:
+            self._maybe_fail("nel")
+        return super().nel(mu)
+
+    def finish(self, ndim, mu):
+        self._maybe_fail("finish")
+        return super().finish(ndim, mu)
+
+
+def _failing_worker(rank, world, port, out, where):
+    import datetime
+
+    import torch.distributed as dist
+    from ptb_b200.api import PtbGpuError
+    # a short timeout: a rank left waiting in a collective ends the test with an error, not a hang
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        s = _system()
+        try:
+            sm_stupid_simple_sharded(_FailingShard(rank, 1, where), s.ndim, s.nel, s.Hvec, s.Svec, s.nat, s.xyz,
+                                     s.aoat, 1, 2, opts=Options(filter=FILTER))
+            msg = "no error"
+        except PtbGpuError as e:
+            msg = f"{e.code}|{e}"
+        with open(os.path.join(out, f"r{rank}.txt"), "w") as f:
+            f.write(msg)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("where", ["prepare", "nel", "finish"])
+def test_a_failing_rank_fails_every_rank(where):
+    """A failure on rank 1 in any phase reaches rank 0 through the protocol's own
+    all-reduces: rank 1 raises its own error, rank 0 a PtbGpuError with the same
+    code naming rank 1, and neither waits for the process-group timeout."""
+    import time
+
+    import torch.multiprocessing as mp
+    from ptb_b200.api import ENOTSPD
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    t0 = time.perf_counter()
+    with tempfile.TemporaryDirectory() as out:
+        mp.spawn(_failing_worker, args=(2, port, out, where), nprocs=2, join=True)
+        r0 = open(os.path.join(out, "r0.txt")).read()
+        r1 = open(os.path.join(out, "r1.txt")).read()
+    assert time.perf_counter() - t0 < 50.0
+    assert r1.startswith(f"{ENOTSPD}|") and "planted failure" in r1
+    assert r0.startswith(f"{ENOTSPD}|") and "rank 1 failed" in r0
