@@ -38,3 +38,36 @@ def test_oracle_dense_and_sp2_match_golden():
     # full_matrix partition == dense (the invariant of the reference's full_matrix runs)
     assert np.max(np.abs(G["P_sm3"] - G["P_dense"])) < 1e-11
     assert np.max(np.abs(G["P_solve2"] - G["P_dense"])) < 1e-11
+
+
+@pytest.mark.parametrize("ptype", [1, 2, 3, 4])
+def test_oracle_purification_types_match_golden(ptype):
+    """The four solver types of the purification module (McWeeny with the inverse
+    metric, Pade / Newton-Schulz / eigen-sign with the inverse square root), with
+    the chemical potential and the number of search steps."""
+    n = G["aoat"].shape[0]
+    pur = O.PurificationSettings(type=ptype, metric_type=O.INV if ptype == 1 else O.INV_SQRT, nel=int(G["nel"]),
+                                 cycles=100)
+    P, mu, steps = O.purification(pur, n, G["Hvec"], G["Svec"])
+    assert mu == G[f"mu_pur{ptype}"][0] and steps == int(G[f"mu_pur{ptype}"][1])
+    assert np.max(np.abs(P - G[f"P_pur{ptype}"])) < 1e-12
+
+
+def test_oracle_solve2_and_electron_counts_match_golden():
+    n = G["aoat"].shape[0]
+    H = O.filter_matrix_sym(G["Hvec"], float(G["filter"]))
+    S = O.filter_matrix_sym(G["Svec"], float(G["filter"]))
+    P2, e2, focc, fail = O.solve2(1, n, int(G["nel"]), 0, 300.0, H, S)
+    assert np.max(np.abs(P2 - G["P_solve2"])) < 1e-12
+    assert np.max(np.abs(focc - G["focc_solve2"])) < 1e-12
+    # the bisection's stop rule (source/sm.f90:191-192,370): on [-10, 10] the bracket is
+    # narrower than 1e-3 after 15 halvings, so a trace stops at 16 steps even with the
+    # electron count unconverged (single and atom columns here), or earlier once
+    # |nel - nelref| < 1e-5 (the full matrix)
+    tol_mu, tol_nel, nelref = float(np.float32(1e-3)), float(np.float32(1e-5)), int(G["nel"])
+    for cols, by_count in ((1, False), (2, False), (3, True)):
+        nel, mu = G[f"nel_sm{cols}"], G[f"mu_sm{cols}"]
+        assert (abs(nel[-1] - nelref) < tol_nel) == by_count
+        if not by_count:
+            assert len(mu) == 16 and 20.0 / 2 ** 15 < tol_mu <= 20.0 / 2 ** 14
+            assert abs(nel[-1] - nelref) > 1e-3
