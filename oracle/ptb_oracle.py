@@ -107,6 +107,25 @@ def analyse_matrix_sym(packed: np.ndarray, n: int) -> dict:
 # ----------------------------------------------------------------------------
 # LAPACK drivers with the reference's arguments
 # ----------------------------------------------------------------------------
+# Thread count of the small per-submatrix LAPACK/BLAS calls.  Multithreaded
+# OpenBLAS on matrices of order ~100-500, alternating dsygvd with a small
+# dgemm, runs dsygvd about 7x slower than one thread does (thread hand-over
+# between routines); MKL, which the reference links, lowers its thread count
+# for such sizes by itself.  Below this order the submatrix loop runs its
+# calls on one thread, so the timed CPU baseline is not inflated.
+SMALL_LAPACK_ORDER = 512
+_TPC = None
+
+
+def _blas_threads(m: int):
+    """Context: one BLAS/LAPACK thread for a submatrix of order m < SMALL_LAPACK_ORDER."""
+    global _TPC
+    if _TPC is None:
+        from threadpoolctl import ThreadpoolController
+        _TPC = ThreadpoolController()
+    return _TPC.limit(limits=1 if m < SMALL_LAPACK_ORDER else None)
+
+
 def sygvd(a: np.ndarray, b: np.ndarray):
     """dsygvd(itype=1,'V','U'); source/lapack_eig.f90:305-368. Returns (w, U, info)."""
     w, v, info = _lapack.dsygvd(a, b, itype=1, jobz="V", uplo="U")
@@ -344,8 +363,9 @@ def sm_stupid_simple(ndim: int, nelref: int, Hvec: np.ndarray, Svec: np.ndarray,
         imap[mp] = np.arange(m)
         Hs = H[np.ix_(mp, mp)]
         Ss = S[np.ix_(mp, mp)]
-        e, U, info = sygvd(Hs, Ss)
-        Psm = Ss @ U
+        with _blas_threads(m):
+            e, U, info = sygvd(Hs, Ss)
+            Psm = Ss @ U
         io = imap[owned]
         fe = np.sum(Psm[io, :] * U[io, :], axis=0)
         eig.append((mp, imap, owned, e, U, fe))
@@ -367,7 +387,8 @@ def sm_stupid_simple(ndim: int, nelref: int, Hvec: np.ndarray, Svec: np.ndarray,
             occ = np.where(e < mu, 2.0, np.where(e == mu, 1.0, 0.0))
             nel += float(np.sum(fe * occ))
             if finaliter:
-                Psm = dmat(occ, U)
+                with _blas_threads(len(mp)):
+                    Psm = dmat(occ, U)
                 P[np.ix_(mp, owned)] = Psm[:, imap[owned]]
         if finaliter:
             break
