@@ -151,3 +151,29 @@ def test_wrong_array_lengths_are_rejected_before_the_c_call():
         with pytest.raises(api.PtbGpuError) as ei:
             call()
         assert ei.value.code == api.EINVAL, k
+
+
+def _fortran_fields(name):
+    """Field list of a bind(C) derived type in INTEGRATION.md's Fortran module."""
+    doc = (HEADER.parent.parent / "INTEGRATION.md").read_text()
+    m = re.search(r"type, bind\(C\) :: " + name + r"\n(.*?)end type", doc, re.S)
+    assert m, name
+    out = []
+    for line in m.group(1).splitlines():
+        mm = re.match(r"\s*(real\(c_double\)|integer\(c_int64_t\))\s*::\s*(.*)", line.split("!")[0])
+        if mm:
+            kind = "double" if mm.group(1).startswith("real") else "int64_t"
+            out += [(kind, v.split("=")[0].strip()) for v in mm.group(2).split(",")]
+    return out
+
+
+@pytest.mark.parametrize("name", ["ptbgpu_opts", "ptbgpu_stats"])
+def test_fortran_binding_types_match_header(name):
+    """The bind(C) types a Fortran maintainer copies from INTEGRATION.md have the
+    header's fields in the header's order and kinds (a mismatch would shift every
+    later field of the struct the library writes)."""
+    text = HEADER.read_text()
+    m = re.search(r"typedef struct \{([^{}]*)\}\s*" + name + ";", text)
+    body = re.sub(r"/\*.*?\*/", "", m.group(1), flags=re.S)
+    c_fields = re.findall(r"\b(int64_t|double)\s+(\w+)\s*;", body)
+    assert _fortran_fields(name) == c_fields
