@@ -156,7 +156,7 @@ def test_wrong_array_lengths_are_rejected_before_the_c_call():
 def _fortran_fields(name):
     """Field list of a bind(C) derived type in INTEGRATION.md's Fortran module."""
     doc = (HEADER.parent.parent / "INTEGRATION.md").read_text()
-    m = re.search(r"type, bind\(C\) :: " + name + r"\n(.*?)end type", doc, re.S)
+    m = re.search(r"type, bind\(C\) :: " + name + r"\b[^\n]*\n(.*?)end type", doc, re.S)
     assert m, name
     out = []
     for line in m.group(1).splitlines():
@@ -167,7 +167,7 @@ def _fortran_fields(name):
     return out
 
 
-@pytest.mark.parametrize("name", ["ptbgpu_opts", "ptbgpu_stats"])
+@pytest.mark.parametrize("name", ["ptbgpu_opts", "ptbgpu_stats", "ptbgpu_pur_settings"])
 def test_fortran_binding_types_match_header(name):
     """The bind(C) types a Fortran maintainer copies from INTEGRATION.md have the
     header's fields in the header's order and kinds (a mismatch would shift every
