@@ -158,3 +158,24 @@ def test_a_failing_rank_fails_every_rank(where):
     assert time.perf_counter() - t0 < 50.0
     assert r1.startswith(f"{ENOTSPD}|") and "planted failure" in r1
     assert r0.startswith(f"{ENOTSPD}|") and "rank 1 failed" in r0
+
+
+def test_a_rank_with_an_empty_share():
+    """The full-matrix grouping has one submatrix: on two ranks one of them prepares
+    nothing, still takes every collective step, and both return the oracle's P."""
+    import torch.multiprocessing as mp
+    columns = 3
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    with tempfile.TemporaryDirectory() as out:
+        mp.spawn(_worker, args=(2, port, out, columns), nprocs=2, join=True)
+        P0, P1 = np.load(os.path.join(out, "P0.npy")), np.load(os.path.join(out, "P1.npy"))
+        ids = [np.load(os.path.join(out, f"ids{r}.npy")) for r in (0, 1)]
+    s = _system()
+    ref = O.sm_stupid_simple(s.ndim, s.nel, O.filter_matrix_sym(s.Hvec, FILTER), O.filter_matrix_sym(s.Svec, FILTER),
+                             s.nat, s.xyz, s.aoat, columns, 2)
+    assert sorted(len(x) for x in ids) == [0, 1]
+    assert np.array_equal(P0, P1)
+    assert np.max(np.abs(P0 - ref.Pvec)) < 1e-12
