@@ -156,3 +156,28 @@ def test_to_c_carries_every_field():
                              chempot_guess=-0.25, chempot_increment=2.0)
     c = s.to_c(api._Settings)
     assert [getattr(c, f) for f, _ in api._Settings._fields_] == [2, 3, 11, 0, 64, 1, 4, 1, 7, 1, 9, -0.25, 2.0]
+
+
+def test_arbitrary_lines_parse_or_raise_the_settings_error():
+    """Any text made of the parser's keywords, values, numbers and junk either
+    parses or raises PurSettingsError (the reference's error stop), nothing else."""
+    from hypothesis import given, settings as hsettings, strategies as st
+
+    words = st.sampled_from(["mode", "type", "metric", "cycles", "pr", "chempot_cycles", "chempot_increment",
+                             "submatrix_mode", "submatrix_columns", "=", "!", "!x", "full", "submatrix", "pade",
+                             "newton", "diag", "mcweeny", "inverse", "sqrt", "inverse_sqrt", "single_columns",
+                             "kmeans_r_heuristic", "submatrix_sygv", "check", "dev", "iterative_inversion", "true",
+                             "false", "1", "2.5", "-3", "1e-5", "1d-3", "nan", "inf", "x=y", "", "\t"])
+    line = st.lists(words, max_size=6).map(" ".join)
+    text = st.lists(line, max_size=8).map("\n".join)
+
+    @hsettings(max_examples=300, deadline=None)
+    @given(text)
+    def check(t):
+        try:
+            s = PurificationSettings().read(t)
+        except PurSettingsError:
+            return
+        assert s.mode in (ps.FULL, ps.SUBMATRIX) and 1 <= s.type <= 4 and 1 <= s.metric_type <= 3
+
+    check()
