@@ -7,6 +7,7 @@ invalid values, and the same quirk that ``chempot_increment`` is truncated by
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass
 
 FULL, SUBMATRIX = 1, 2
@@ -76,13 +77,13 @@ class PurificationSettings:
                 elif arg1 == "metric":
                     self.metric_type = _pick(_METRIC, arg3, "Error: .PUR contains invalid metric definition.")
                 elif arg1 == "cycles" and num is not None:
-                    self.cycles = int(num)
+                    self.cycles = _int_value(num)
                 elif arg1 == "chempot_cycles" and num is not None:
-                    self.chempot_cycles = int(num)
+                    self.chempot_cycles = _int_value(num)
                 elif arg1 == "chempot_increment" and num is not None:
-                    self.chempot_increment = float(int(num))
+                    self.chempot_increment = float(_int_value(num))
                 elif arg1 == "pr" and num is not None:
-                    self.prlvl = int(num)
+                    self.prlvl = _int_value(num)
             else:
                 if arg1 == "dev":
                     self.dev = True
@@ -128,8 +129,17 @@ def _readline(raw: str):
 
 def _checktype_number(tok: str):
     # a Fortran real field: digits with an optional point and an exponent
-    # introduced by e or d (either case)
+    # introduced by e or d (either case).  nan and inf are not taken as numbers:
+    # the reference's int() of them is undefined, here they count as strings.
     try:
-        return float(tok.replace("d", "e").replace("D", "e"))
+        v = float(tok.replace("d", "e").replace("D", "e"))
     except ValueError:
         return None
+    return v if math.isfinite(v) else None
+
+
+def _int_value(num: float) -> int:
+    """int(floats(1)) of the reference, for a value that fits its 8-byte default integer."""
+    if not -2.0 ** 63 <= num < 2.0 ** 63:
+        raise PurSettingsError(f"Error: .PUR value {num!r} does not fit an integer setting")
+    return int(num)

@@ -107,6 +107,15 @@ def test_numeric_keys_truncate_like_int():
 def test_numeric_key_without_a_number_keeps_the_default():
     s = PurificationSettings().read("cycles = many\npr =\n")
     assert (s.cycles, s.prlvl) == (40, 1)
+    # nan / inf are not numbers here (the reference's int() of them is undefined)
+    s = PurificationSettings().read("cycles = nan\nchempot_cycles = inf\npr = -inf\n")
+    assert (s.cycles, s.chempot_cycles, s.prlvl) == (40, 60, 1)
+
+
+def test_integer_settings_out_of_range_raise_the_settings_error():
+    for line in ("cycles = 1e30", "pr = -1e19", "chempot_increment = 9.3e18"):
+        with pytest.raises(PurSettingsError):
+            PurificationSettings().read(line)
 
 
 def test_strings_and_numbers_are_counted_apart():
