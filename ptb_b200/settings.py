@@ -93,6 +93,54 @@ class PurificationSettings:
                     self.metric_iterative = True
         return self
 
+    # print_settings, source/purification_settings.f90:222-300
+    def format_settings(self, thrs_normal: float) -> str:
+        """The settings block the reference prints, edit descriptor by edit
+        descriptor.  Its quirk is kept: the 'Calculation mode' line selects on
+        the solver type, not on the mode (type 1 prints 'Full matrix', type 2
+        'Submatrix method', types 3 and 4 nothing), and because that line is a
+        non-advancing write, an unmatched case leaves the record open so that
+        the 'Purification type' label continues on the same line."""
+        out = ["", "*" * 72, "*" * 26 + " PURIFICATION MODE " + "*" * 27, "*" * 72,
+               "  __SETTINGS__", "  __general__"]
+        rec = "  Calculation mode :            " + " " * 6          # (2x,a,6x), advance='no'
+        mode_text = {FULL: "Full matrix", SUBMATRIX: "Submatrix method"}.get(self.type)
+        if mode_text is not None:
+            out.append(rec + mode_text)
+            rec = ""
+        rec += "  Purification type:            " + " " * 6         # (2x,a,6x), advance='no'
+        cycles = "  Iteration Cycles:           " + " " * 8 + str(self.cycles)
+        type_text = {MCWEENY: "McWeeny Grand Canonical Purification", SIGN_ITER_PADE: "Iterative Sign: Pade",
+                     SIGN_DIAGONALIZATION: "Sign Diagonalization",
+                     SIGN_ITER_NEWTON: "Iterative Sign: Newton-Schulz"}.get(self.type)
+        if type_text is not None:
+            out.append(rec + type_text)
+            rec = ""
+            if self.type != SIGN_DIAGONALIZATION and self.prlvl > 0:
+                out.append(cycles)
+        lead = rec   # an open record (no type matched) is continued by the next write
+        if self.prlvl > 1:
+            out.append(lead + "  Development Mode:              " + " " * 5 + ("T" if self.dev else "F"))
+            lead = ""
+        out.append(lead + "  Print Level:                   " + " " * 5 + str(self.prlvl))
+        if self.prlvl > 0:
+            out += ["", "  __metric__"]
+            rec = "  S power:                      " + " " * 5       # (2x,a,5x), advance='no'
+            power = {INV: "-1", SQRT_: "0.5", INV_SQRT: "-0.5"}.get(self.metric_type)
+            it_line = "  Iterative metric evaluation:  " + " " * 6 + ("T" if self.metric_iterative else "F")
+            if power is not None:
+                out += [rec + power, it_line]
+            else:
+                out.append(rec + it_line)
+            if self.metric_iterative and self.prlvl > 1:
+                out.append("  Number of cycles:             " + " " * 5 + str(self.metric_cycles))
+            out += ["", "  __chempot__", "  Initial Chemical Potential:   " + " " * 3 + f"{self.chempot_guess:13.8f}"]
+            if self.prlvl > 1:
+                out.append("  Number of cycles:             " + " " * 5 + str(self.chempot_cycles))
+            out += ["", "  __thresholds_", "  Threshold:                      " + " " * 3 + _fortran_e(thrs_normal, 13, 6)]
+        out += ["", "*" * 72, ""]
+        return "\n".join(out) + "\n"
+
     @classmethod
     def from_file(cls, path) -> "PurificationSettings":
         with open(path) as f:
@@ -143,3 +191,13 @@ def _int_value(num: float) -> int:
     if not -2.0 ** 63 <= num < 2.0 ** 63:
         raise PurSettingsError(f"Error: .PUR value {num!r} does not fit an integer setting")
     return int(num)
+
+
+def _fortran_e(x: float, w: int, d: int) -> str:
+    """Fortran Ew.d output: 0.<d digits>E<sign><two digits>, right-justified in w columns."""
+    if x == 0.0:
+        s = "0." + "0" * d + "E+00"
+    else:
+        m, e = f"{abs(x):.{d - 1}e}".split("e")
+        s = ("-" if x < 0 else "") + "0." + m.replace(".", "") + f"E{int(e) + 1:+03d}"
+    return s.rjust(w)

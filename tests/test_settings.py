@@ -190,3 +190,34 @@ def test_arbitrary_lines_parse_or_raise_the_settings_error():
         assert s.mode in (ps.FULL, ps.SUBMATRIX) and 1 <= s.type <= 4 and 1 <= s.metric_type <= 3
 
     check()
+
+
+def test_print_settings_layout_and_mode_line_quirk():
+    thr = float(__import__("numpy").float32(1e-4))   # thrs%normal for 2000 <= ndim < 15000
+    s = PurificationSettings(type=ps.MCWEENY, mode=ps.SUBMATRIX)
+    lines = s.format_settings(thr).splitlines()
+    assert lines[0] == "" and lines[1] == "*" * 72 and lines[2] == "*" * 26 + " PURIFICATION MODE " + "*" * 27
+    # the mode line selects on the type: McWeeny (1) prints 'Full matrix' although mode is submatrix
+    assert lines[6] == "  Calculation mode :            " + " " * 6 + "Full matrix"
+    assert lines[7] == "  Purification type:            " + " " * 6 + "McWeeny Grand Canonical Purification"
+    assert lines[8] == "  Iteration Cycles:           " + " " * 8 + "40"
+    text = s.format_settings(thr)
+    # (2x,a,3x,f13.8) and (2x,a,3x,e13.6) after the reference's padded labels
+    assert "\n  Initial Chemical Potential:   " + " " * 3 + "  -1.50000000\n" in text
+    assert "\n  Threshold:                      " + " " * 3 + " 0.100000E-03\n" in text
+    assert text.endswith("\n" + "*" * 72 + "\n\n")
+    # Newton (3): no mode text, so the open record continues with the type label
+    t = PurificationSettings(type=ps.SIGN_ITER_NEWTON).format_settings(thr).splitlines()
+    assert t[6] == ("  Calculation mode :            " + " " * 6 + "  Purification type:            " + " " * 6
+                    + "Iterative Sign: Newton-Schulz")
+    # print level 0: no metric, chempot or threshold blocks
+    q = PurificationSettings(prlvl=0).format_settings(thr)
+    assert "__metric__" not in q and "Threshold" not in q and "Print Level:" in q
+
+
+def test_fortran_e_format():
+    from ptb_b200.settings import _fortran_e
+    assert _fortran_e(9.999999747378752e-05, 13, 6) == " 0.100000E-03"
+    assert _fortran_e(1e-3, 13, 6) == " 0.100000E-02"
+    assert _fortran_e(-123.456, 13, 6) == "-0.123456E+03"
+    assert _fortran_e(0.0, 13, 6) == " 0.000000E+00"
