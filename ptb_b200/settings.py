@@ -3,7 +3,8 @@
 Follows source/purification_settings.f90:6-218: the same mode codes and
 defaults, the same ``key = value`` / bare-flag grammar, the same errors on
 invalid values, and the same quirk that ``chempot_increment`` is truncated by
-``int()`` (source/purification_settings.f90:193-195).
+``int()`` (source/purification_settings.f90:193-195).  format_settings
+restates print_settings (source/purification_settings.f90:222-300).
 """
 from __future__ import annotations
 
