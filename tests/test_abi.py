@@ -153,10 +153,14 @@ def test_wrong_array_lengths_are_rejected_before_the_c_call():
         assert ei.value.code == api.EINVAL, k
 
 
+FORTRAN_MODULE = HEADER.parent / "ptbgpu_c.f90"
+FORTRAN_SHIMS = HEADER.parent / "ptbgpu_shims.f90"
+
+
 def _fortran_fields(name):
-    """Field list of a bind(C) derived type in INTEGRATION.md's Fortran module."""
-    doc = (HEADER.parent.parent / "INTEGRATION.md").read_text()
-    m = re.search(r"type, bind\(C\) :: " + name + r"\b[^\n]*\n(.*?)end type", doc, re.S)
+    """Field list of a bind(C) derived type in the Fortran module include/ptbgpu_c.f90."""
+    src = FORTRAN_MODULE.read_text()
+    m = re.search(r"type, bind\(C\) :: " + name + r"\b[^\n]*\n(.*?)end type", src, re.S)
     assert m, name
     out = []
     for line in m.group(1).splitlines():
@@ -169,11 +173,35 @@ def _fortran_fields(name):
 
 @pytest.mark.parametrize("name", ["ptbgpu_opts", "ptbgpu_stats", "ptbgpu_pur_settings"])
 def test_fortran_binding_types_match_header(name):
-    """The bind(C) types a Fortran maintainer copies from INTEGRATION.md have the
-    header's fields in the header's order and kinds (a mismatch would shift every
-    later field of the struct the library writes)."""
+    """The bind(C) types of include/ptbgpu_c.f90 have the header's fields in the
+    header's order and kinds (a mismatch would shift every later field of the
+    struct the library writes)."""
     text = HEADER.read_text()
     m = re.search(r"typedef struct \{([^{}]*)\}\s*" + name + ";", text)
     body = re.sub(r"/\*.*?\*/", "", m.group(1), flags=re.S)
     c_fields = re.findall(r"\b(int64_t|double)\s+(\w+)\s*;", body)
     assert _fortran_fields(name) == c_fields
+
+
+def test_fortran_interfaces_bind_declared_exports():
+    """Every bind(C, name=...) interface of the Fortran module names a function the
+    header declares and the library exports, with as many dummy arguments as the
+    C prototype has parameters; every function the shims call is bound."""
+    src = FORTRAN_MODULE.read_text()
+    header = HEADER.read_text()
+    lib = api.load_library()
+    binds = re.findall(r"function\s+(ptbgpu_\w+)\s*\(([^)]*)\)[^\n]*?(?:&\s*\n\s*)?[^\n]*?bind\(C, name=\"(\w+)\"\)",
+                       src, re.S)
+    assert len(binds) >= 6
+    for fname, dummies, cname in binds:
+        assert fname == cname
+        assert hasattr(lib, cname), cname
+        proto = re.search(r"\b" + cname + r"\s*\(([^)]*)\)\s*;", header)
+        assert proto, cname
+        n_c = len([a for a in proto.group(1).split(",") if a.strip() and a.strip() != "void"])
+        n_f = len([a for a in dummies.replace("&", " ").split(",") if a.strip()])
+        assert n_f == n_c, (cname, n_f, n_c)
+    bound = {c for _, _, c in binds}
+    called = set(re.findall(r"\b(ptbgpu_[a-z0-9_]+)\s*\(", FORTRAN_SHIMS.read_text()))
+    called -= {"ptbgpu_pur_settings"}   # the derived type's structure constructor
+    assert called and called <= bound, called - bound
