@@ -224,11 +224,17 @@ int ptbgpu_solve2(ptbgpu_ctx* ctx, int64_t mode, int64_t ndim, int64_t nel, int6
  * cudaMalloc/cudaFree.  No counterpart in the reference.  out (host, 2 doubles)
  * = {tr(PS), tr(PH)}; dHpk may be NULL (out[1] = 0).  Working memory is a
  * fixed 1 MB array in the library's device image: ndim <= 65536, larger sizes
- * are rejected with PTBGPU_EINVAL.  The first call on a device looks up that
- * array's device address; make it before any stream capture.  Calls share the
- * array: calls whose kernels overlap on the GPU race.  stream is a cudaStream_t
- * (NULL: the legacy default stream); the call returns after the stream has
- * finished.  err (may be NULL) receives the message of a failure. */
+ * are rejected with PTBGPU_EINVAL.  The CUDA runtime loads device code lazily
+ * by default, so the first call on a device places this code and its 1 MB
+ * array there and looks up the array's device address: a caller that will run
+ * with the device full makes its first call early (or sets
+ * CUDA_MODULE_LOADING=EAGER), and makes it before any stream capture.  After a
+ * cudaDeviceReset of a device the kept address is stale: do not call again on
+ * that device.  Calls share the array: calls whose kernels overlap on the GPU
+ * race.  stream is a cudaStream_t (NULL: the legacy default stream); the call
+ * returns after the stream has finished.  The caller's current device is the
+ * same after the call as before.  err (may be NULL) receives the message of a
+ * failure. */
 int ptbgpu_density_traces_noalloc(int device, int64_t ndim, const double* dPpk, const double* dSpk,
                                   const double* dHpk, double* out, void* stream, char* err, size_t errlen);
 

@@ -10,11 +10,23 @@
 // device pointers; its only working memory is the fixed array below.
 //
 // Scratch: kNoAllocMaxDim column partial pairs plus the two results, 1 MB per
-// device that loads the library, held until the process exits.  Every call
+// device that loads this code, held until the process exits.  Every call
 // writes all slots it later reads, so nothing has to start at zero; calls on
 // the same device share the array, so calls whose kernels overlap on the GPU
 // (different streams or host threads without ordering) race and must be
 // serialised by the caller.
+//
+// When the array comes into being: the CUDA runtime loads a library's device
+// code lazily (CUDA_MODULE_LOADING=LAZY is the default since CUDA 12.2), so
+// this file's kernels and the 1 MB array are placed on a device by the first
+// call on that device, which looks up the array's address.  A caller that will
+// later run with the device full makes its first call early (or runs with
+// CUDA_MODULE_LOADING=EAGER, which loads the code when the context is
+// created), and makes it before any stream capture.  The address is kept per
+// device for the life of the process; a caller that resets a device
+// (cudaDeviceReset) discards the loaded code, and later calls on that device
+// would use a stale address, so such a caller must not call this entry point
+// on that device again.
 #include <mutex>
 
 #include "common.cuh"
@@ -95,6 +107,28 @@ void set_msg(char* err, size_t len, const char* fmt, ...) {
 
 }  // namespace
 
+namespace {
+
+// Makes `device` current for the call and gives the caller's current device
+// back on every return path.
+struct CurrentDevice {
+    int saved = -1;
+    cudaError_t set(int device) {
+        cudaError_t e = cudaGetDevice(&saved);
+        if (e != cudaSuccess) {
+            saved = -1;
+            return e;
+        }
+        return saved == device ? cudaSuccess : cudaSetDevice(device);
+    }
+    ~CurrentDevice() {
+        int now = -1;
+        if (saved >= 0 && cudaGetDevice(&now) == cudaSuccess && now != saved) cudaSetDevice(saved);
+    }
+};
+
+}  // namespace
+
 extern "C" int ptbgpu_density_traces_noalloc(int device, int64_t ndim, const double* dPpk, const double* dSpk,
                                              const double* dHpk, double* out, void* stream, char* err,
                                              size_t errlen) {
@@ -112,7 +146,8 @@ extern "C" int ptbgpu_density_traces_noalloc(int device, int64_t ndim, const dou
         set_msg(err, errlen, "device %d out of range", device);
         return PTBGPU_EINVAL;
     }
-    cudaError_t e = cudaSetDevice(device);
+    CurrentDevice cur;
+    cudaError_t e = cur.set(device);
     if (e != cudaSuccess) {
         set_msg(err, errlen, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
         return PTBGPU_ECUDA;
