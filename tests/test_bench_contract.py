@@ -37,3 +37,25 @@ def test_reference_arm_other_ranks_print_nothing():
                "--warmup", "0")
     assert out.returncode == 0, out.stderr[-2000:]
     assert not [l for l in out.stdout.splitlines() if l.startswith("{")]
+
+
+def test_reference_arm_reports_the_calls_it_timed():
+    """With a budget smaller than one call, exactly one whole call is timed and
+    the line says so (steps 1, the request kept beside it); no scaled sample."""
+    out = _run({}, "--workload", "sm_water32", "--steps", "5", "--warmup", "0", "--ref-budget", "0.001")
+    assert out.returncode == 0, out.stderr[-2000:]
+    d = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][0])
+    assert d["steps"] == 1 and d["requested_steps"] == 5
+    assert len(d["timed_calls_s"]) == 1 and d["value"] == d["timed_calls_s"][0]
+    assert "whole" in d["cpu_baseline"]["sample"] and "scaled" not in d["cpu_baseline"]["sample"]
+
+
+def test_timed_calls_stops_at_the_budget_or_the_steps():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    calls = []
+    times, w = bench.timed_calls(lambda: calls.append(1), 4, lambda: None, 2, 1e9)
+    assert len(times) == 4 and w == 2 and len(calls) == 4
+    import time as _t
+    times, _ = bench.timed_calls(lambda: _t.sleep(0.05), 10, lambda: None, 0, 0.12)
+    assert 1 <= len(times) < 10
