@@ -336,6 +336,22 @@ int ptbgpu_oz_tiles(int64_t n, int64_t slices, int64_t kblock, int64_t variant, 
 int ptbgpu_oz_gemm(ptbgpu_ctx* ctx, int64_t n, int64_t slices, int64_t kblock, int64_t variant, int64_t tri_a,
                    int64_t tri_b, int64_t symmetric, const double* A, const double* B, double* C, double* ms);
 
+/* The batched FP64 generalized eigensolver of the submatrix method on dense
+ * host problems (kernel-level entry for tests and measurements; it replaces,
+ * for submatrices of order <= 1024, the per-submatrix la_sygvd and the S_k U
+ * product of source/sm.f90:296-310).  nprob problems of orders dims[k]
+ * (1..1024): H and S hold their column-major dims[k]^2 blocks one after
+ * another; owned holds nown[k] (0-based, local) owned indices per problem, one
+ * list after another.  Out: e and fe (sum of dims each, per problem in the
+ * solver's order, not sorted): the eigenvalues of H c = e S c and the weights
+ * fe_j = sum_c (S U)_{c,j} U_{c,j} over the owned rows c.  With Pcols non-NULL
+ * also the owned columns of P = U occ U^T with occ = 2 / 1 / 0 for e < / = / > mu
+ * (dims[k] x nown[k] column-major per problem, one after another).  ENOTSPD
+ * if an S block is not positive definite. */
+int ptbgpu_sygv_batched(ptbgpu_ctx* ctx, int64_t nprob, const int64_t* dims, const double* H, const double* S,
+                        const int64_t* nown, const int64_t* owned, double mu, double* e, double* fe,
+                        double* Pcols);
+
 /* ---- consumer of P in the next SCF iteration ---------------------------- */
 /* The iteration-2 XC long-range damping of twoscf (source/pgtb.f90:482-513) on
  * the packed arrays: xab(lin(a,b)) = (1 + erf(-1.8 (rab - r)/r))/2 with

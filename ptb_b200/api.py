@@ -73,7 +73,8 @@ EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_defau
             "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm", "ptbgpu_mlpop14", "ptbgpu_mlpop14_device",
             "ptbgpu_mlpop2", "ptbgpu_mlpop2_device", "ptbgpu_kmeans_partition", "ptbgpu_sm_plan",
             "ptbgpu_sm_prepare", "ptbgpu_sm_nel", "ptbgpu_sm_finish", "ptbgpu_xc_damping",
-            "ptbgpu_xc_damping_device", "ptbgpu_selftest_bounded_wait", "ptbgpu_oz_tiles")
+            "ptbgpu_xc_damping_device", "ptbgpu_selftest_bounded_wait", "ptbgpu_oz_tiles",
+            "ptbgpu_sygv_batched")
 
 
 def library_path() -> Path:
@@ -125,6 +126,7 @@ def load_library():
     lib.ptbgpu_symsq_split.argtypes = [C.c_void_p, i64, i64, i64, d, P(C.c_float), d]
     lib.ptbgpu_oz_gemm.argtypes = [C.c_void_p, i64, i64, i64, i64, i64, i64, i64, d, d, d, d]
     lib.ptbgpu_oz_tiles.argtypes = [i64, i64, i64, i64, i64, i64, i64, P(C.c_int32), i64, P(i64), P(i64)]
+    lib.ptbgpu_sygv_batched.argtypes = [C.c_void_p, i64, P(i64), d, d, P(i64), P(i64), C.c_double, d, d, d]
     lib.ptbgpu_kmeans_partition.argtypes = [C.c_void_p, i64, d, d, i64, d, P(i64), C.c_uint64, P(_Opts), P(i64),
                                             P(i64), d]
     lib.ptbgpu_sm_plan.argtypes = [C.c_void_p, i64, d, d, i64, d, P(i64), i64, i64, P(i64), P(_Opts), P(i64),
@@ -531,6 +533,38 @@ class Context:
                                              int(tri_b), int(bool(symmetric)), _dptr(Ah), _dptr(Bh), _dptr(out),
                                              C.byref(ms)))
         return (out, ms.value) if timed else out
+
+    def sygv_batched(self, problems, mu: float | None = None):
+        """The submatrix method's batched generalized eigensolver on dense problems
+        (ptbgpu_sygv_batched): problems = [(H_k, S_k, owned_k)] with (m, m) arrays
+        and 0-based local owned indices.  Returns per problem (e, fe) (the
+        solver's order), and with mu given also the owned columns of
+        P = U occ U^T as an (m, len(owned)) array."""
+        dims = np.array([np.asarray(h).shape[0] for h, _, _ in problems], dtype=np.int64)
+        for (h, s_, o), m in zip(problems, dims):
+            if np.asarray(h).shape != (m, m) or np.asarray(s_).shape != (m, m) or len(o) == 0:
+                raise PtbGpuError(EINVAL, "problem arrays must be (m, m) with at least one owned index")
+        H = np.concatenate([np.asarray(h, dtype=np.float64).ravel(order="F") for h, _, _ in problems])
+        S = np.concatenate([np.asarray(s_, dtype=np.float64).ravel(order="F") for _, s_, _ in problems])
+        nown = np.array([len(o) for _, _, o in problems], dtype=np.int64)
+        owned = np.concatenate([np.asarray(o, dtype=np.int64) for _, _, o in problems])
+        tot = int(dims.sum())
+        e = np.zeros(tot)
+        fe = np.zeros(tot)
+        pc = np.zeros(int(np.sum(dims * nown))) if mu is not None else None
+        self._check(self._lib.ptbgpu_sygv_batched(
+            self._h, len(problems), dims.ctypes.data_as(C.POINTER(C.c_int64)), _dptr(H), _dptr(S),
+            nown.ctypes.data_as(C.POINTER(C.c_int64)), owned.ctypes.data_as(C.POINTER(C.c_int64)),
+            float(mu if mu is not None else 0.0), _dptr(e), _dptr(fe), _dptr(pc) if pc is not None else None))
+        out, o0, p0 = [], 0, 0
+        for m, no in zip(dims, nown):
+            item = [e[o0:o0 + m], fe[o0:o0 + m]]
+            if pc is not None:
+                item.append(pc[p0:p0 + m * no].reshape((m, no), order="F"))
+            out.append(tuple(item))
+            o0 += m
+            p0 += m * no
+        return out
 
     # ---- population analysis (source/mlpop.f) ----
     def mlpop14(self, nao: int, Svec: np.ndarray, x: float = MULL_LOEW14):

@@ -10,6 +10,7 @@
 #include <thread>
 
 #include "common.cuh"
+#include "sm_eig.cuh"
 #include "oz_gemm.cuh"
 #include "tc_gemm.cuh"
 
@@ -581,6 +582,15 @@ int ptbgpu_oz_gemm(ptbgpu_ctx* c, int64_t n, int64_t slices, int64_t kblock, int
                 *ms += x;
             }
         }
+    });
+}
+
+int ptbgpu_sygv_batched(ptbgpu_ctx* c, int64_t nprob, const int64_t* dims, const double* H, const double* S,
+                        const int64_t* nown, const int64_t* owned, double mu, double* e, double* fe,
+                        double* Pcols) {
+    return guarded(c, [&] {
+        PTB_CHECK(nprob > 0 && dims && H && S && nown && owned && e && fe, PTBGPU_EINVAL, "bad arguments");
+        sygv_batched_entry(c, nprob, dims, H, S, nown, owned, mu, e, fe, Pcols);
     });
 }
 

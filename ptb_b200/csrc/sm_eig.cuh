@@ -1,0 +1,48 @@
+// Batched FP64 generalized eigensolver of the submatrix method (sm_eig.cu).
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+
+namespace ptb {
+
+// Largest submatrix the batched solver takes (its per-problem shared-memory
+// vectors are sized for it); larger ones go to the side-stream path.
+constexpr int kEigBatchMax = 1024;
+
+// One submatrix as the host plan describes it.
+struct EigProbHost {
+    int k;          // submatrix index
+    int m;          // dimension
+    int nown;       // owned columns
+    int64_t moff;   // offset of its row map in the maps array
+    int64_t eoff;   // offset of its eigenpairs in the flat e / fe arrays
+    int64_t o0;     // offset of its owned columns in the owned-column list
+    int64_t gbase = 0;   // its H / S element (i, j) at gbase + map(i) + map(j) gld
+    int64_t gld = -1;    // -1: the system's ndim
+};
+
+struct EigBatch;
+
+// Gather, Cholesky, reduction, tridiagonalisation, implicit QL, owned rows of
+// U and S U, and the (e, fe) pairs into d_e / d_fe at each problem's eoff.
+// Raises ENOTSPD (overlap block not positive definite) or EITER (QL did not
+// converge).  Returns null for an empty list.
+std::shared_ptr<EigBatch> eig_batch_prepare(ptbgpu_ctx* c, int64_t n, const double* H, const double* S,
+                                            const std::vector<EigProbHost>& probs, const int* d_maps,
+                                            const int* d_own_cols, const int* d_ipos, double* d_e, double* d_fe,
+                                            int prl, double* flops);
+
+// The owned columns of P_k = U occ U^T at mu for every prepared problem,
+// written into the packed result (rows map(i) <= c of column c), or with
+// dPdense non-null as m x nown column-major blocks, one after another.
+void eig_batch_final(ptbgpu_ctx* c, EigBatch& eb, double mu, int64_t n, const int* d_maps,
+                     const int* d_own_cols, double* dP, double* dPdense = nullptr);
+
+// Kernel-level entry of ptbgpu_sygv_batched (dense host problems).
+void sygv_batched_entry(ptbgpu_ctx* c, int64_t np, const int64_t* dims, const double* H, const double* S,
+                        const int64_t* nown, const int64_t* owned, double mu, double* e, double* fe, double* Pcols);
+
+}  // namespace ptb

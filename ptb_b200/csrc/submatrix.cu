@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -31,6 +32,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "sm_eig.cuh"
 
 namespace ptb {
 
@@ -616,6 +618,7 @@ struct SmPlan {
     int64_t total = 0;     // prepared eigenpairs
     double flops = 0.0;
     bool prepared = false;
+    std::shared_ptr<EigBatch> eig;   // submatrices of the batched eigensolver
     ~SmPlan() {
         for (Bucket& bk : bks) {
             bk.probs.release();
@@ -864,6 +867,7 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
         bk.w.release();
     }
     pl.bks.clear();
+    pl.eig.reset();
     pl.prepared = false;
     pl.flops = 0.0;
     std::vector<char> seen(pl.nsm, 0);
@@ -887,7 +891,7 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
         t_last = now;
     };
 
-    constexpr int kBatchMax = 1024;
+    constexpr int kBatchMax = kEigBatchMax;
     std::vector<Prob> small, large;
     int64_t eoff = 0;
     for (int k : ids) {
@@ -901,6 +905,24 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
     DevBuf& bfe = c->buf(B_MISC1);
     be.reserve(sizeof(double) * std::max<int64_t>(eoff, 1));
     bfe.reserve(sizeof(double) * std::max<int64_t>(eoff, 1));
+    // submatrices up to kEigBatchMax: the library's batched eigensolver (one
+    // CTA per submatrix); PTBGPU_SM_EIG=library sends them through cuSOLVER's
+    // batched routines in tuned size buckets instead (kept for comparison)
+    static const bool use_library = [] {
+        const char* v = getenv("PTBGPU_SM_EIG");
+        return v != nullptr && std::string(v) == "library";
+    }();
+    if (!use_library && !small.empty()) {
+        std::vector<EigProbHost> eh;
+        eh.reserve(small.size());
+        for (const Prob& p : small)
+            eh.push_back({p.k, p.m, (int)(pl.own_off[p.k + 1] - pl.own_off[p.k]), p.moff, p.eoff, pl.own_off[p.k]});
+        pl.eig = eig_batch_prepare(c, n, H, S, eh, d_maps, d_own_cols, d_ipos, be.as<double>(), bfe.as<double>(),
+                                   prl, &pl.flops);
+        mark("batched eigensolver");
+        log_line(prl, 2, " * submatrix batched eigensolver: %zu problems", small.size());
+        small.clear();
+    }
     DevBuf sb, ptrs, infos, ws, tbuf;
     cusolverDnParams_t params;
     PTB_CUSOLVER(cusolverDnCreateParams(&params));
@@ -1137,6 +1159,7 @@ void sm_finish(ptbgpu_ctx* c, SmPlan& pl, double mu, double* dP) {
     const int* d_ipos = c->buf(B_SM7).as<int>();
     const double one = 1.0, zero = 0.0;
     PTB_CUDA(cudaMemsetAsync(dP, 0, sizeof(double) * (size_t)npacked(n), s));
+    if (pl.eig) eig_batch_final(c, *pl.eig, mu, n, d_maps, d_own_cols, dP);
     DevBuf tbuf;
     try {
         for (Bucket& bk : pl.bks) {

@@ -1,0 +1,89 @@
+"""The submatrix method's batched generalized eigensolver (ptbgpu_sygv_batched)
+against LAPACK (scipy's dsygvd, the routine the reference calls per submatrix,
+source/sm.f90:296-299), stage by stage through what leaves the solver:
+
+* eigenvalues of H c = e S c (the solver's order is not sorted: compared sorted),
+* fe_j = sum_c (S U)_{c,j} U_{c,j} over the owned rows (source/sm.f90:305-310),
+* the owned columns of P = U occ U^T with occ 2 / 1 / 0 for e < / = / > mu
+  (source/sm.f90:322-362).
+
+Orders 1 to 1024 (the solver's limit) in one batch, uneven owned counts, an
+exactly degenerate spectrum, and a non-positive-definite overlap.  FP64
+throughout: eigenvalues to 1e-11 of the spectral range, fe and P to 1e-10.
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sl
+
+from ptb_b200 import PtbGpuError, api
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1, 2, 3, 5, 31, 32, 33, 64, 65, 100, 257, 600, 1024]
+
+
+def _problem(m, rng, nown):
+    A = rng.standard_normal((m, m))
+    S = A @ A.T / m + np.eye(m)                # SPD, condition ~ 5
+    H = rng.uniform(-1, 1, (m, m))
+    H = 0.5 * (H + H.T) + np.diag(rng.uniform(-2, 2, m))
+    own = np.sort(rng.choice(m, size=min(nown, m), replace=False))
+    return H, S, own
+
+
+def _reference(H, S, own, mu):
+    e, U = sl.eigh(H, S)                       # S-orthonormal eigenvectors, ascending
+    fe = np.sum((S @ U)[own, :] * U[own, :], axis=0)
+    occ = np.where(e < mu, 2.0, np.where(e == mu, 1.0, 0.0))
+    P = (U * occ) @ U[own, :].T
+    return e, fe, P
+
+
+def test_batched_eigensolver_matches_lapack(ctx):
+    rng = np.random.default_rng(17)
+    probs = [_problem(m, rng, 1 + (m % 13)) for m in SIZES]
+    mu = 0.05
+    out = ctx.sygv_batched(probs, mu=mu)
+    for (H, S, own), (e, fe, Pc) in zip(probs, out):
+        m = H.shape[0]
+        er, fer, Pr = _reference(H, S, own, mu)
+        order = np.argsort(e, kind="stable")
+        scale = max(1.0, np.max(np.abs(er)))
+        assert np.max(np.abs(e[order] - er)) <= 1e-11 * scale * max(1.0, np.sqrt(m)), m
+        assert np.max(np.abs(fe[order] - fer)) <= 1e-10, m
+        assert np.max(np.abs(Pc - Pr)) <= 1e-10, m
+        assert abs(np.sum(fe) - len(own)) <= 1e-10 * m    # sum_j fe_j = number of owned rows
+
+
+def test_degenerate_spectrum(ctx):
+    """Repeated identical blocks give exactly repeated eigenvalues; the owned
+    columns of P depend only on the occupied subspace, which must come out
+    right whichever basis of each degenerate cluster the solver lands on."""
+    rng = np.random.default_rng(5)
+    b = 40
+    Hb = rng.uniform(-1, 1, (b, b))
+    Hb = 0.5 * (Hb + Hb.T)
+    Ab = rng.standard_normal((b, b))
+    Sb = Ab @ Ab.T / b + np.eye(b)
+    H = np.kron(np.eye(4), Hb)
+    S = np.kron(np.eye(4), Sb)
+    own = np.array([0, 3, 41, 100, 159])
+    e_b = sl.eigh(Hb, Sb, eigvals_only=True)
+    mu = 0.5 * (e_b[17] + e_b[18])             # between two quadruplets
+    (e, fe, Pc), = ctx.sygv_batched([(H, S, own)], mu=mu)
+    er, fer, Pr = _reference(H, S, own, mu)
+    assert np.max(np.abs(np.sort(e) - er)) <= 1e-12 * max(1.0, np.max(np.abs(er))) * 10
+    assert np.max(np.abs(Pc - Pr)) <= 1e-10
+    # per cluster of four equal eigenvalues the fe sums are basis independent
+    occ_fe = np.sum(fe[e < mu])
+    assert abs(occ_fe - np.sum(fer[er < mu])) <= 1e-10
+
+
+def test_non_positive_definite_overlap_is_reported(ctx):
+    rng = np.random.default_rng(2)
+    H, S, own = _problem(70, rng, 3)
+    S = S.copy()
+    S[40, 40] = -5.0
+    with pytest.raises(PtbGpuError) as ei:
+        ctx.sygv_batched([_problem(30, rng, 2), (H, S, own)])
+    assert ei.value.code == api.ENOTSPD and "submatrix 2" in str(ei.value)
