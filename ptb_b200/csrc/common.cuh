@@ -94,6 +94,8 @@ struct ptbgpu_ctx {
     std::shared_ptr<void> sm_plan;
     // side streams and handles of the submatrix method's large eigensolves
     std::shared_ptr<void> sm_side;
+    // device tile lists of the int8-sliced FP64 products of the module code
+    std::shared_ptr<void> oz_tile_cache;
     // worker contexts of the multi-instance batch (same device, own streams and buffers)
     std::vector<ptbgpu_ctx*> workers;
     // launches of this library's kernels since the last call started
@@ -161,6 +163,13 @@ int  dpotrf_lower(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A);             
 void dtrtri_lower(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A);
 void dsyevd(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A, double* w);
 int  dsygvd(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A, double* B, double* w);
+
+// FP64-class product on the int8 tensor cores (sp2.cu): C = alpha op(A) op(B),
+// column-major n x n device matrices, S slices; oz_check raises ETIMEOUT if a
+// product's bounded waits gave up (it synchronises the stream).
+void oz_dgemm(ptbgpu_ctx* c, int64_t n, double alpha, const double* A, bool ta, const double* B, bool tb,
+              double* C, int S = 8);
+void oz_check(ptbgpu_ctx* c, const char* what);
 
 // timing helpers
 struct EventTimer {

@@ -3,13 +3,16 @@
 // metric X = S^-1 or S^-1/2 (eigendecomposition or Newton-Schulz), the guess,
 // McWeeny / Pade / Newton-Schulz sign / eigen-sign solvers and the outer
 // chemical-potential search, with the reference's thresholds, stop rules and
-// quirks (documented beside each routine).  Dense column-major matrices,
-// cuBLAS DGEMM / cuSOLVER DSYEVD for the products and eigensolves.
+// quirks (documented beside each routine).  Dense column-major matrices; the
+// products run on the int8 tensor cores as FP64-class sliced products
+// (oz_dgemm), the eigendecompositions of the metric and of the eigen-sign
+// solver on cuSOLVER DSYEVD.
 #include <algorithm>
 #include <cmath>
 #include <vector>
 
 #include "common.cuh"
+#include "oz_gemm.cuh"
 
 namespace ptb {
 
@@ -77,12 +80,19 @@ struct Ctx {
     ~Ctx() {
         for (auto& b : scratch) b.release();
     }
+    // The module's products on the int8 tensor cores (8 slices, FP64 class);
+    // beyond the exact int32 range of the slice sums (n > 16643) cuBLAS DGEMM.
     void gemm(const double* A, const double* B, double* C, double alpha = 1.0, bool transb = false) {
-        const double beta = 0.0;
-        PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, transb ? CUBLAS_OP_T : CUBLAS_OP_N, (int)n, (int)n, (int)n,
-                               &alpha, A, (int)n, B, (int)n, &beta, C, (int)n));
+        if (oz::supported(n, kSlices)) {
+            oz_dgemm(c, n, alpha, A, false, B, transb, C, kSlices);
+        } else {
+            const double beta = 0.0;
+            PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, transb ? CUBLAS_OP_T : CUBLAS_OP_N, (int)n, (int)n,
+                                   (int)n, &alpha, A, (int)n, B, (int)n, &beta, C, (int)n));
+        }
         gemm_flops += 2.0 * (double)n * (double)n * (double)n;
     }
+    static constexpr int kSlices = 8;
     double frob(const double* a) { return frob_dev(c, n, n, a); }
     void nan_check(const double* a, const char* msg) {
         PTB_CHECK(!has_nan_dev(c, n * n, a), PTBGPU_ENAN, "%s", msg);
@@ -386,6 +396,7 @@ void purify_ref_device(ptbgpu_ctx* c, const ptbgpu_pur_settings& pur, int64_t n,
         bisection = is_lower && is_upper;
         incr *= 2.0;
     }
+    oz_check(c, "int8 product (purification module)");
     pack_cols(s, n, n, P, dP);
     if (st) {
         st->mu = chempot;

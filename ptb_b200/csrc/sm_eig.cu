@@ -1,5 +1,5 @@
-// Batched FP64 generalized eigensolver of the submatrix method: one CTA per
-// submatrix for the dense stages, one warp per submatrix for the QL chase.
+// Batched FP64 generalized eigensolver of the submatrix method, one CTA per
+// submatrix.
 //
 // The reference solves H_k U = S_k U diag(e) with LAPACK dsygvd per submatrix
 // (la_sygvd, source/sm.f90:296-299), forms S_k U for the electron-count
@@ -12,21 +12,14 @@
 //   C   = L^-1 H_k L^-T              two blocked triangular solves (k_eig_reduce)
 //   C   = Q T Q^T                    Householder tridiagonalisation, lower,
 //                                    Q = H_0 H_1 ... H_{m-3} (k_eig_sytrd)
-//   T   = Z diag(e) Z^T              implicit QL with Wilkinson shifts; Z is
-//                                    the product of the Givens rotations in the
-//                                    order they are made, which are stored
-//                                    (k_eig_ql)
+//   T   = Z diag(e) Z^T              divide and conquer (k_eig_dc)
 //   U   = L^-T Q Z                   never formed:
 //     rows c of U    = (L^-T)[c,:] Q Z,  rows c of S U = L[c,:] Q Z  for the
 //     owned columns c (k_eig_rows), so fe_j = sum_c (SU)[c,j] U[c,j];
-//     P_k[:,c] = U (occ o U[c,:]^T) = L^-T (Q (Z w)) with Z w applying the
-//     stored rotations in reverse (k_eig_final).
+//     P_k[:,c] = U (occ o U[c,:]^T) = L^-T (Q (Z w)) (k_eig_final).
 //
-// The QL iteration is the implicit QL algorithm with a Wilkinson shift for
-// symmetric tridiagonal matrices (Bowdler, Martin, Reinsch and Wilkinson 1968,
-// the tql2 procedure), restated here with its rotations recorded instead of
-// accumulated into an m x m matrix.  Each step's quantities are summed in a
-// fixed order, so results do not depend on scheduling.
+// Each step's quantities are summed in a fixed order, so results do not depend
+// on scheduling.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -37,16 +30,14 @@ namespace ptb {
 
 namespace {
 
-constexpr int kT = 256;           // threads of the per-problem CTAs
+constexpr int kT = 512;           // threads of the per-problem CTAs (16 warps)
 constexpr int NB = 32;            // panel width of the blocked stages
 constexpr int TS = 64;            // output tile of the blocked updates
-constexpr int kQlWarps = 4;       // problems per CTA of the QL kernel
-constexpr int kQlMaxIter = 30;    // QL sweeps per eigenvalue before giving up (as LAPACK's dsteqr)
+constexpr int kQlMaxIter = 30;    // QL sweeps per eigenvalue of a leaf before giving up (as LAPACK's dsteqr)
 
 // Status words per problem.
 constexpr int kStOk = 0;
-constexpr int kStNoConv = -1;     // QL sweeps exhausted
-constexpr int kStRotCap = -2;     // rotation / sweep storage exhausted (retried with more)
+constexpr int kStNoConv = -1;     // a leaf's QL sweeps exhausted
 // > 0: leading minor of that order of S_k is not positive definite
 
 struct EigProb {
@@ -54,16 +45,14 @@ struct EigProb {
     int64_t moff, eoff, o0;
     int64_t gbase, gld;   // the problem's H / S: element (i, j) at gbase + map(i) + map(j) gld
     int64_t poff;         // dense output of the owned columns of P (m x nown, column-major)
-    int64_t aoff;     // C and L arenas (m x m, column-major, ld = m)
+    int64_t aoff;     // C, L, Z and merge-workspace arenas (m x m, column-major, ld = m)
     int64_t voff;     // d, e, tau, eigenvalue arenas (m)
-    int64_t boff;     // owned-row arena (2 nown x m, row-major)
-    int64_t roff, rcap;   // rotations (double2)
-    int64_t soff, scap;   // sweeps (int4: l, mm, count, first rotation)
+    int64_t boff;     // owned-row arena (4 nown x m)
 };
 
 // ---------------------------------------------------------------------------
 // C[r0+i, c0+j] -= sum_{k < kk} A(i,k) B(k,j) on one TS x TS tile (mr x nc
-// valid), 256 threads with 4 x 4 outputs each.
+// valid), 512 threads with 4 x 2 outputs each.
 //   A(i,k) = A[(r0+i) + k lda]
 //   B(k,j) = BT ? B[(c0+j) + k ldb] : B[k + (c0+j) ldb]
 // LOWER: only elements on or below the diagonal of C are written.
@@ -88,33 +77,45 @@ __device__ void tile_update(double* __restrict__ C, int ldc, int r0, int c0, int
         }
     }
     __syncthreads();
-    const int tx = tid & 15, ty = tid >> 4;
-    double acc[4][4];
+    const int tx = tid & 15, ty = tid >> 4;   // 16 x 32 threads, 4 x 2 outputs each
+    double acc[4][2];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+        for (int b = 0; b < 2; ++b) acc[a][b] = 0.0;
     for (int k = 0; k < kk; ++k) {
-        double av[4], bv[4];
+        double av[4], bv[2];
 #pragma unroll
         for (int a = 0; a < 4; ++a) av[a] = sA[k * (TS + 1) + tx + 16 * a];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) bv[b] = sB[k * (TS + 1) + ty + 16 * b];
+        for (int b = 0; b < 2; ++b) bv[b] = sB[k * (TS + 1) + ty + 32 * b];
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+            for (int b = 0; b < 2; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
     }
+    // read-modify-write of the C tile: all loads issued before any store (the
+    // stores could alias later loads as far as the compiler knows, which would
+    // otherwise serialise the round trips to memory)
+    double cv[4][2];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        const int j = ty + 16 * b;
-        if (j >= nc) continue;
+    for (int b = 0; b < 2; ++b) {
+        const int j = ty + 32 * b;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             const int i = tx + 16 * a;
-            if (i >= mr || (LOWER && r0 + i < c0 + j)) continue;
-            double* p = C + (int64_t)(r0 + i) + (int64_t)(c0 + j) * ldc;
-            *p -= acc[a][b];
+            const bool ok = j < nc && i < mr && !(LOWER && r0 + i < c0 + j);
+            cv[a][b] = ok ? C[(int64_t)(r0 + i) + (int64_t)(c0 + j) * ldc] : 0.0;
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+        const int j = ty + 32 * b;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = tx + 16 * a;
+            const bool ok = j < nc && i < mr && !(LOWER && r0 + i < c0 + j);
+            if (ok) C[(int64_t)(r0 + i) + (int64_t)(c0 + j) * ldc] = cv[a][b] - acc[a][b];
         }
     }
     __syncthreads();
@@ -312,6 +313,7 @@ __global__ void __launch_bounds__(kT) k_eig_reduce(const EigProb* __restrict__ p
 // written once per column.  Output: d (m), e (m-1), tau, and v_j in C's column
 // j below the subdiagonal.
 constexpr int kSyRows = (kEigBatchMax + kT - 1) / kT;   // rows per thread
+constexpr int kSyChunk = 8;                              // columns per batch of loads
 
 __global__ void __launch_bounds__(kT) k_eig_sytrd(const EigProb* __restrict__ probs, double* __restrict__ Ca,
                                                   double* __restrict__ Da, double* __restrict__ Ea,
@@ -403,17 +405,33 @@ __global__ void __launch_bounds__(kT) k_eig_sytrd(const EigProb* __restrict__ pr
             vr[q] = (r < m) ? vc[r] : 0.0;
             wr[q] = (r < m) ? wc[r] : 0.0;
         }
-        for (int k = r0; k < m; ++k) {
-            const double vk = vc[k], wk = wc[k], nk = vn[k];
-            double* col = A + (int64_t)k * m;
+        // columns in chunks of kSyChunk: every load of a chunk is issued before
+        // its stores, so the pass streams instead of waiting on each element
+        for (int k0 = r0; k0 < m; k0 += kSyChunk) {
+            double a[kSyChunk][kSyRows];
 #pragma unroll
-            for (int q = 0; q < kSyRows; ++q) {
-                const int r = r0 + tid + q * kT;
-                if (r < m) {
-                    double a = col[r];
-                    a -= vr[q] * wk + wr[q] * vk;
-                    col[r] = a;
-                    acc[q] = fma(a, nk, acc[q]);
+            for (int u = 0; u < kSyChunk; ++u) {
+                const int k = k0 + u;
+#pragma unroll
+                for (int q = 0; q < kSyRows; ++q) {
+                    const int r = r0 + tid + q * kT;
+                    a[u][q] = (k < m && r < m) ? A[r + (int64_t)k * m] : 0.0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kSyChunk; ++u) {
+                const int k = k0 + u;
+                if (k < m) {
+                    const double vk = vc[k], wk = wc[k], nk = vn[k];
+#pragma unroll
+                    for (int q = 0; q < kSyRows; ++q) {
+                        const int r = r0 + tid + q * kT;
+                        if (r < m) {
+                            const double x = a[u][q] - (vr[q] * wk + wr[q] * vk);
+                            A[r + (int64_t)k * m] = x;
+                            acc[q] = fma(x, nk, acc[q]);
+                        }
+                    }
                 }
             }
         }
@@ -447,130 +465,655 @@ __global__ void __launch_bounds__(kT) k_eig_sytrd(const EigProb* __restrict__ pr
 }
 
 // ---------------------------------------------------------------------------
-// Implicit QL with Wilkinson shift on (d, e); lane 0 of a warp per problem
-// chases, with d and e in shared memory.  Rotation q of a sweep over [l, mm]
-// acts on indices (i, i+1), i = mm-1-q, with (c, s): columns of Z transform as
-// z_{i+1} <- s z_i + c z_{i+1}, z_i <- c z_i - s z_{i+1}.
-__global__ void k_eig_ql(int nprob, const EigProb* __restrict__ probs, const double* __restrict__ Da,
-                         const double* __restrict__ Ea, double* __restrict__ Wa, double2* __restrict__ cs,
-                         int4* __restrict__ sw, int* __restrict__ nsw_out, int* __restrict__ status, int maxm,
-                         int only_capped) {
-    extern __shared__ double sm[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int pi = blockIdx.x * kQlWarps + warp;
-    if (pi >= nprob) return;
-    if (only_capped ? status[pi] != kStRotCap : status[pi] != kStOk) return;
-    const EigProb p = probs[pi];
-    const int m = p.m;
-    double* d = sm + (size_t)warp * 2 * maxm;
-    double* e = d + maxm;
-    for (int i = lane; i < m; i += 32) {
-        d[i] = Da[p.voff + i];
-        e[i] = (i < m - 1) ? Ea[p.voff + i] : 0.0;
-    }
-    __syncwarp();
-    if (lane == 0) {
-        const double eps = 2.220446049250313e-16;
-        double2* rot = cs + p.roff;
-        int4* swp = sw + p.soff;
-        int64_t nrot = 0;
-        int nsw = 0, st = kStOk;
-        for (int l = 0; l < m && st == kStOk; ++l) {
-            int iter = 0;
-            for (;;) {
-                int mm = l;
-                for (; mm < m - 1; ++mm) {
-                    const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
-                    if (fabs(e[mm]) <= eps * dd) break;
+// C[ro(i), co(j)] = sum_k A(i, kx(k)) B(k, j) on one TS x TS output tile, the
+// K range in NB chunks, 256 threads with 4 x 4 outputs each:
+//   A(i, k) = AT ? A[k + (r0+i) lda] : A[(r0+i) + k lda]
+//   B(k, j) = B[kxb(k) + (c0+j) ldb]
+//   kx, kxb: optional K index maps (shared memory), crow: output row offset,
+//   ccol: optional output column map (shared memory) else c0 + j.
+template <bool AT>
+__device__ void tile_gemm(double* __restrict__ C, int64_t ldc, int crow, const int* ccol, int r0, int c0, int mr,
+                          int nc, const double* __restrict__ A, int64_t lda, const int* kx,
+                          const double* __restrict__ B, int64_t ldb, const int* kxb, int K, double* sA, double* sB) {
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;   // 16 x 32 threads, 4 x 2 outputs each
+    double acc[4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) acc[a][b] = 0.0;
+    for (int k0 = 0; k0 < K; k0 += NB) {
+        const int kk = min(NB, K - k0);
+        if (AT) {
+            for (int t = tid; t < TS * NB; t += kT) {
+                const int k = t % NB, i = t / NB;
+                double v = 0.0;
+                if (i < mr && k < kk) {
+                    const int64_t kg = kx ? kx[k0 + k] : (k0 + k);
+                    v = A[kg + (int64_t)(r0 + i) * lda];
                 }
-                if (mm == l) break;
-                if (++iter > kQlMaxIter) {
-                    st = kStNoConv;
-                    break;
+                sA[k * (TS + 1) + i] = v;
+            }
+        } else {
+            for (int t = tid; t < TS * NB; t += kT) {
+                const int i = t % TS, k = t / TS;
+                double v = 0.0;
+                if (i < mr && k < kk) {
+                    const int64_t kg = kx ? kx[k0 + k] : (k0 + k);
+                    v = A[(int64_t)(r0 + i) + kg * lda];
                 }
-                if (nsw >= p.scap || nrot + (mm - l) > p.rcap) {
-                    st = kStRotCap;
-                    break;
-                }
-                double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-                double r = hypot(g, 1.0);
-                g = d[mm] - d[l] + e[l] / (g + copysign(r, g));
-                double s = 1.0, c = 1.0, pp = 0.0;
-                const int64_t first = nrot;
-                bool underflow = false;
-                for (int i = mm - 1; i >= l; --i) {
-                    const double f = s * e[i], b = c * e[i];
-                    // r = |(f, g)|, (s, c) = (f, g) / r from one reciprocal square
-                    // root (the chase is a chain of dependent operations; this
-                    // is its longest link)
-                    const double q = fma(f, f, g * g);
-                    if (q == 0.0) {
-                        e[i + 1] = 0.0;
-                        d[i + 1] -= pp;
-                        e[mm] = 0.0;
-                        underflow = true;
-                        break;
-                    }
-                    const double rq = rsqrt(q);
-                    e[i + 1] = q * rq;
-                    s = f * rq;
-                    c = g * rq;
-                    g = d[i + 1] - pp;
-                    r = (d[i] - g) * s + 2.0 * c * b;
-                    pp = s * r;
-                    d[i + 1] = g + pp;
-                    g = c * r - b;
-                    rot[nrot++] = make_double2(c, s);
-                }
-                swp[nsw++] = make_int4(l, mm, (int)(nrot - first), (int)first);
-                if (underflow) continue;
-                d[l] -= pp;
-                e[l] = g;
-                e[mm] = 0.0;
+                sA[k * (TS + 1) + i] = v;
             }
         }
-        nsw_out[pi] = nsw;
-        status[pi] = st;
+        for (int t = tid; t < TS * NB; t += kT) {
+            const int k = t % NB, j = t / NB;
+            double v = 0.0;
+            if (j < nc && k < kk) {
+                const int64_t kg = kxb ? kxb[k0 + k] : (k0 + k);
+                v = B[kg + (int64_t)(c0 + j) * ldb];
+            }
+            sB[k * (TS + 1) + j] = v;
+        }
+        __syncthreads();
+        for (int k = 0; k < kk; ++k) {
+            double av[4], bv[2];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) av[a] = sA[k * (TS + 1) + tx + 16 * a];
+#pragma unroll
+            for (int b = 0; b < 2; ++b) bv[b] = sB[k * (TS + 1) + ty + 32 * b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        }
+        __syncthreads();
     }
-    __syncwarp();
-    for (int i = lane; i < m; i += 32) Wa[p.voff + i] = d[i];
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+        const int j = ty + 32 * b;
+        if (j >= nc) continue;
+        const int64_t col = ccol ? ccol[c0 + j] : (c0 + j);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = tx + 16 * a;
+            if (i < mr) C[(int64_t)(crow + r0 + i) + col * ldc] = acc[a][b];
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
-// Owned rows of S U and U, fe and the eigenpairs.  B holds 2 nown rows of
-// length m (row-major): rows t < nown are L[c_t,:] -> (S U)[c_t,:], rows
-// nown + t are (L^-T)[c_t,:] -> U[c_t,:].
+// Divide and conquer for the tridiagonal eigenproblem T = Z diag(w) Z^T
+// (Cuppen's split T = diag(T1, T2) + |beta| u u^T, u = e_last + sign(beta)
+// e_first; Gu and Eisenstat's recomputed z for orthogonal eigenvectors), one
+// CTA per problem.  Leaves of at most 32 rows are solved by a warp with the
+// implicit QL iteration (every lane runs the same scalar iteration and applies
+// each rotation to its own row of the leaf's Z); the merges run bottom-up over
+// a balanced tree, one at a time with the whole CTA:
+//   z = [last row of Z1, sign(beta) first row of Z2] / sqrt 2, rho = 2|beta|;
+//   sort the block eigenvalues (merge of two sorted lists);
+//   deflate: rho |z_j| <= tol -> eigenpair (d_j, q_j); two close d's -> a Givens
+//   rotation zeroes one z entry (LAPACK's dlaed2 rules, tol = 8 eps max(|d|, rho));
+//   secular roots lambda_i = d_org + tau in (d_i, d_i+1), each step modelling the
+//   left and right sums by one pole each;
+//   zhat_j^2 = (lambda_j - d_j) prod_{i != j} (lambda_i - d_j)/(d_i - d_j) / rho;
+//   v_i = (zhat_j / (d_j - lambda_i))_j normalised; Z_new = Q v in two GEMMs
+//   (rows of block 1 against the columns that touch it, rows of block 2 likewise).
+// Output: w ascending, Z in the Z arena (column-major, ld m).
+constexpr int kDcLeaf = 32;
+
+struct DcSmem {
+    // per-element arrays of the merge (kEigBatchMax each)
+    double *D, *Ds, *zs, *dk, *zk, *tau, *zh, *val;
+    int *perm, *org, *sec, *dl, *rank, *cls, *ktop, *kbot;
+    int2* rpair;
+    double2* rcs;
+};
+
+__device__ DcSmem dc_smem(unsigned char* base) {
+    DcSmem s;
+    double* d = reinterpret_cast<double*>(base);
+    s.D = d;
+    s.Ds = d + kEigBatchMax;
+    s.zs = d + 2 * kEigBatchMax;
+    s.dk = d + 3 * kEigBatchMax;
+    s.zk = d + 4 * kEigBatchMax;
+    s.tau = d + 5 * kEigBatchMax;
+    s.zh = d + 6 * kEigBatchMax;
+    s.val = d + 7 * kEigBatchMax;
+    s.rcs = reinterpret_cast<double2*>(d + 8 * kEigBatchMax);
+    int* ip = reinterpret_cast<int*>(s.rcs + kEigBatchMax);
+    s.perm = ip;
+    s.org = ip + kEigBatchMax;
+    s.sec = ip + 2 * kEigBatchMax;
+    s.dl = ip + 3 * kEigBatchMax;
+    s.rank = ip + 4 * kEigBatchMax;
+    s.cls = ip + 5 * kEigBatchMax;
+    s.ktop = ip + 6 * kEigBatchMax;
+    s.kbot = ip + 7 * kEigBatchMax;
+    s.rpair = reinterpret_cast<int2*>(ip + 8 * kEigBatchMax);
+    return s;
+}
+constexpr size_t kDcSmemMerge = sizeof(double) * 8 * kEigBatchMax + sizeof(double2) * kEigBatchMax +
+                                sizeof(int) * 8 * kEigBatchMax + sizeof(int2) * kEigBatchMax;
+constexpr size_t kDcSmem = kDcSmemMerge;
+
+// Leaf: implicit QL on d[0..s), e[0..s-1) with Z = I accumulated.  Every
+// lane runs the same scalar iteration on its own copies of d and e and rotates
+// its own row z of Z (lane r holds row r), so no lane reads another's data.
+__device__ bool dc_leaf(int s, double* d, double* e, double* z, int lane) {
+    const double eps = 2.220446049250313e-16;
+    for (int c = 0; c < kDcLeaf; ++c) z[c] = (c == lane) ? 1.0 : 0.0;
+    for (int l = 0; l < s; ++l) {
+        int iter = 0;
+        for (;;) {
+            int mm = l;
+            for (; mm < s - 1; ++mm)
+                if (fabs(e[mm]) <= eps * (fabs(d[mm]) + fabs(d[mm + 1]))) break;
+            if (mm == l) break;
+            if (++iter > kQlMaxIter) return false;
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = hypot(g, 1.0);
+            g = d[mm] - d[l] + e[l] / (g + copysign(r, g));
+            double sn = 1.0, c = 1.0, pp = 0.0;
+            bool underflow = false;
+            for (int i = mm - 1; i >= l; --i) {
+                const double f = sn * e[i], b = c * e[i];
+                r = hypot(f, g);
+                e[i + 1] = r;
+                if (r == 0.0) {
+                    d[i + 1] -= pp;
+                    e[mm] = 0.0;
+                    underflow = true;
+                    break;
+                }
+                sn = f / r;
+                c = g / r;
+                g = d[i + 1] - pp;
+                r = (d[i] - g) * sn + 2.0 * c * b;
+                pp = sn * r;
+                d[i + 1] = g + pp;
+                g = c * r - b;
+                const double zi = z[i], zi1 = z[i + 1];
+                z[i + 1] = sn * zi + c * zi1;
+                z[i] = c * zi - sn * zi1;
+            }
+            if (underflow) continue;
+            d[l] -= pp;
+            e[l] = g;
+            e[mm] = 0.0;
+        }
+    }
+    return true;
+}
+
+// Root i of 1 + rho sum_t z_t^2 / (dk_t - lambda) = 0 (dk ascending, k roots):
+// returns tau with lambda = dk[*org] + tau.
+__device__ double dc_secular(int k, const double* dk, const double* zk, double rho, int i, int* org_out) {
+    const double eps = 2.220446049250313e-16;
+    int org;
+    double lo, hi;
+    if (i < k - 1) {
+        const double mid = 0.5 * (dk[i + 1] - dk[i]);
+        double f = 1.0;
+        for (int t = 0; t < k; ++t) f += rho * zk[t] * zk[t] / ((dk[t] - dk[i]) - mid);
+        if (f >= 0.0) {
+            org = i;
+            lo = 0.0;
+            hi = mid;
+        } else {
+            org = i + 1;
+            lo = -mid;
+            hi = 0.0;
+        }
+    } else {
+        double z2 = 0.0;
+        for (int t = 0; t < k; ++t) z2 += zk[t] * zk[t];
+        org = i;
+        lo = 0.0;
+        hi = rho * z2;
+    }
+    const double dorg = dk[org];
+    const double a = dk[i] - dorg;
+    const double b = (i < k - 1) ? dk[i + 1] - dorg : 0.0;
+    double tau = 0.5 * (lo + hi);
+    for (int it = 0; it < 100; ++it) {
+        double psi = 0.0, phi = 0.0, dpsi = 0.0, dphi = 0.0;
+        for (int t = 0; t < k; ++t) {
+            const double den = (dk[t] - dorg) - tau;
+            const double q = rho * zk[t] * zk[t] / den;
+            if (t <= i) {
+                psi += q;
+                dpsi += q / den;
+            } else {
+                phi += q;
+                dphi += q / den;
+            }
+        }
+        const double f = 1.0 + psi + phi;
+        if (f > 0.0) hi = tau;
+        else if (f < 0.0) lo = tau;
+        else break;
+        if (fabs(f) <= 16.0 * eps * (1.0 + fabs(psi) + fabs(phi))) break;
+        const double B = dpsi * (a - tau) * (a - tau);
+        const double A = psi - B / (a - tau);
+        double nt;
+        if (i < k - 1) {
+            const double E = dphi * (b - tau) * (b - tau);
+            const double Cc = phi - E / (b - tau);
+            const double c0 = 1.0 + A + Cc;
+            const double qb = -(c0 * (a + b) + B + E);
+            const double qc = c0 * a * b + B * b + E * a;
+            if (c0 == 0.0) {
+                nt = -qc / qb;
+            } else {
+                const double disc = fmax(qb * qb - 4.0 * c0 * qc, 0.0);
+                const double r1 = (-qb - copysign(sqrt(disc), qb)) / (2.0 * c0);
+                const double r2 = (r1 != 0.0) ? qc / (c0 * r1) : r1;
+                nt = (lo < r1 && r1 < hi) ? r1 : r2;
+            }
+        } else {
+            const double c0 = 1.0 + A + phi;
+            nt = (c0 != 0.0) ? a + B / c0 : 0.5 * (lo + hi);
+        }
+        if (!(lo < nt && nt < hi)) nt = 0.5 * (lo + hi);
+        if (fabs(nt - tau) <= 2.0 * eps * fabs(nt)) {
+            tau = nt;
+            break;
+        }
+        tau = nt;
+    }
+    *org_out = org;
+    return tau;
+}
+
+__global__ void __launch_bounds__(kT) k_eig_dc(const EigProb* __restrict__ probs, const double* __restrict__ Da,
+                                               const double* __restrict__ Ea, double* __restrict__ Wa,
+                                               double* __restrict__ Za, double* __restrict__ Qa,
+                                               double* __restrict__ Va, int* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double sA[NB * (TS + 1)], sB[NB * (TS + 1)];
+    __shared__ int s_k, s_nd, s_nrot, s_ntop, s_nbot, s_fail;
+    if (status[blockIdx.x] != kStOk) return;
+    const EigProb p = probs[blockIdx.x];
+    const int m = p.m;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* Z = Za + p.aoff;
+    double* Qp = Qa + p.aoff;
+    double* V = Va + p.aoff;
+    const double* eo = Ea + p.voff;
+    DcSmem S = dc_smem(smraw);
+    int L = 0;
+    while (((m + (1 << L) - 1) >> L) > kDcLeaf) ++L;
+    const int nleaf = 1 << L;
+    for (int i = tid; i < m; i += kT) S.D[i] = Da[p.voff + i];
+    if (tid == 0) s_fail = 0;
+    __syncthreads();
+    if (tid == 0)
+        for (int q = 1; q < nleaf; ++q) {
+            const int pos = (int)(((int64_t)q * m) >> L);
+            const double ab = fabs(eo[pos - 1]);
+            S.D[pos - 1] -= ab;
+            S.D[pos] -= ab;
+        }
+    __syncthreads();
+    // leaves: a warp each
+    for (int q = warp; q < nleaf; q += kT / 32) {
+        const int lo = (int)(((int64_t)q * m) >> L), hi = (int)(((int64_t)(q + 1) * m) >> L), s = hi - lo;
+        double dl[kDcLeaf], el[kDcLeaf], zl[kDcLeaf];
+        for (int i = 0; i < kDcLeaf; ++i) {
+            dl[i] = (i < s) ? S.D[lo + i] : 0.0;
+            el[i] = (i < s - 1) ? eo[lo + i] : 0.0;
+        }
+        const bool ok = dc_leaf(s, dl, el, zl, lane);
+        if (!ok && lane == 0) s_fail = 1;
+        // eigenvalues ascending (ties by index) and the columns in that order
+        int rk = 0;
+        if (lane < s) {
+            const double x = dl[lane];
+            for (int c = 0; c < s; ++c) rk += (dl[c] < x || (dl[c] == x && c < lane)) ? 1 : 0;
+        }
+        for (int c = 0; c < s; ++c) {
+            const int rc = __shfl_sync(0xffffffffu, rk, c);
+            if (lane < s) Z[(int64_t)(lo + lane) + (int64_t)(lo + rc) * m] = zl[c];
+        }
+        __syncwarp();
+        if (lane < s) S.D[lo + rk] = dl[lane];
+        __syncwarp();
+    }
+    __syncthreads();
+    if (s_fail) {
+        if (tid == 0) status[blockIdx.x] = kStNoConv;
+        return;
+    }
+    const double eps = 2.220446049250313e-16;
+    for (int lev = L - 1; lev >= 0; --lev) {
+        for (int q = 0; q < (1 << lev); ++q) {
+            const int lo = (int)(((int64_t)q * m) >> lev), hi = (int)(((int64_t)(q + 1) * m) >> lev);
+            const int mid = (int)(((int64_t)(2 * q + 1) * m) >> (lev + 1));
+            const int n1 = mid - lo, n2 = hi - mid, n = n1 + n2;
+            const double beta = eo[mid - 1];
+            const double rho = 2.0 * fabs(beta);
+            const double sgn = beta >= 0.0 ? 1.0 : -1.0;
+            const double rs2 = 0.70710678118654752440;
+            // (a) merged order of the two sorted blocks
+            for (int j = tid; j < n; j += kT) {
+                int r;
+                if (j < n1) {
+                    const double x = S.D[lo + j];
+                    int a = 0, b = n2;
+                    while (a < b) {
+                        const int c = (a + b) >> 1;
+                        if (S.D[mid + c] < x) a = c + 1;
+                        else b = c;
+                    }
+                    r = j + a;
+                } else {
+                    const double x = S.D[mid + j - n1];
+                    int a = 0, b = n1;
+                    while (a < b) {
+                        const int c = (a + b) >> 1;
+                        if (S.D[lo + c] <= x) a = c + 1;
+                        else b = c;
+                    }
+                    r = (j - n1) + a;
+                }
+                S.perm[r] = j;
+            }
+            __syncthreads();
+            // (b) sorted d, z and column classes; (c) Q with the block columns in that order
+            for (int r = tid; r < n; r += kT) {
+                const int j = S.perm[r];
+                if (j < n1) {
+                    S.Ds[r] = S.D[lo + j];
+                    S.zs[r] = Z[(int64_t)(mid - 1) + (int64_t)(lo + j) * m] * rs2;
+                    S.cls[r] = 1;
+                } else {
+                    S.Ds[r] = S.D[mid + j - n1];
+                    S.zs[r] = sgn * Z[(int64_t)mid + (int64_t)(mid + j - n1) * m] * rs2;
+                    S.cls[r] = 2;
+                }
+            }
+            for (int64_t t = tid; t < (int64_t)n * n; t += kT) {
+                const int i = (int)(t % n), r = (int)(t / n);
+                const int j = S.perm[r];
+                double v = 0.0;
+                if (j < n1) {
+                    if (i < n1) v = Z[(int64_t)(lo + i) + (int64_t)(lo + j) * m];
+                } else if (i >= n1) {
+                    v = Z[(int64_t)(lo + i) + (int64_t)(mid + j - n1) * m];
+                }
+                Qp[t] = v;
+            }
+            __syncthreads();
+            // (d) deflation (one thread, in sorted order)
+            if (tid == 0) {
+                double dmax = 0.0;
+                for (int r = 0; r < n; ++r) dmax = fmax(dmax, fabs(S.Ds[r]));
+                const double tol = 8.0 * eps * fmax(dmax, rho);
+                int k = 0, nd = 0, nrot = 0, pj = -1;
+                for (int r = 0; r < n; ++r) {
+                    if (rho * fabs(S.zs[r]) <= tol) {
+                        S.dl[nd++] = r;
+                        continue;
+                    }
+                    if (pj < 0) {
+                        pj = r;
+                        continue;
+                    }
+                    double sn = S.zs[pj], c = S.zs[r];
+                    const double t = hypot(c, sn);
+                    const double dd = S.Ds[r] - S.Ds[pj];
+                    c /= t;
+                    sn = -sn / t;
+                    if (fabs(dd * c * sn) <= tol) {
+                        S.zs[r] = t;
+                        S.zs[pj] = 0.0;
+                        S.rpair[nrot] = make_int2(pj, r);
+                        S.rcs[nrot] = make_double2(c, sn);
+                        ++nrot;
+                        const double t2 = S.Ds[pj] * c * c + S.Ds[r] * sn * sn;
+                        S.Ds[r] = S.Ds[pj] * sn * sn + S.Ds[r] * c * c;
+                        S.Ds[pj] = t2;
+                        S.cls[r] |= S.cls[pj];
+                        S.dl[nd++] = pj;
+                        pj = r;
+                    } else {
+                        S.sec[k++] = pj;
+                        pj = r;
+                    }
+                }
+                if (pj >= 0) S.sec[k++] = pj;
+                // secular columns that touch block 1 / block 2 (the K lists of the two GEMMs)
+                int nt = 0, nb = 0;
+                for (int t = 0; t < k; ++t) {
+                    const int c = S.cls[S.sec[t]];
+                    if (c & 1) S.ktop[nt++] = t;
+                    if (c & 2) S.kbot[nb++] = t;
+                }
+                s_k = k;
+                s_nd = nd;
+                s_nrot = nrot;
+                s_ntop = nt;
+                s_nbot = nb;
+            }
+            __syncthreads();
+            const int k = s_k, nd = s_nd, nrot = s_nrot;
+            // (e) deflation rotations on the columns of Q (thread per row)
+            if (nrot > 0)
+                for (int i = tid; i < n; i += kT)
+                    for (int q2 = 0; q2 < nrot; ++q2) {
+                        const int2 pr = S.rpair[q2];
+                        const double2 cs = S.rcs[q2];
+                        const double a = Qp[i + (int64_t)pr.x * n], b = Qp[i + (int64_t)pr.y * n];
+                        Qp[i + (int64_t)pr.x * n] = cs.x * a + cs.y * b;
+                        Qp[i + (int64_t)pr.y * n] = -cs.y * a + cs.x * b;
+                    }
+            for (int t = tid; t < k; t += kT) {
+                S.dk[t] = S.Ds[S.sec[t]];
+                S.zk[t] = S.zs[S.sec[t]];
+            }
+            __syncthreads();
+            // (f) secular roots
+            for (int i = tid; i < k; i += kT) S.tau[i] = dc_secular(k, S.dk, S.zk, rho, i, &S.org[i]);
+            __syncthreads();
+            // (g) recomputed z
+            for (int j = tid; j < k; j += kT) {
+                const double dj = S.dk[j];
+                double w = (S.dk[S.org[j]] - dj) + S.tau[j];
+                for (int i = 0; i < k; ++i) {
+                    if (i == j) continue;
+                    w *= ((S.dk[S.org[i]] - dj) + S.tau[i]) / (S.dk[i] - dj);
+                }
+                S.zh[j] = copysign(sqrt(fmax(w / rho, 0.0)), S.zk[j]);
+            }
+            __syncthreads();
+            // (h) eigenvectors of the rank-one problem (columns of V, k x k) and the new eigenvalues
+            for (int i = tid; i < k; i += kT) {
+                const double dorg = S.dk[S.org[i]], ti = S.tau[i];
+                double nrm = 0.0;
+                for (int j = 0; j < k; ++j) {
+                    const double v = S.zh[j] / ((S.dk[j] - dorg) - ti);
+                    nrm = fma(v, v, nrm);
+                }
+                const double sc = 1.0 / sqrt(nrm);
+                for (int j = 0; j < k; ++j) V[j + (int64_t)i * k] = sc * (S.zh[j] / ((S.dk[j] - dorg) - ti));
+                S.val[i] = dorg + ti;
+            }
+            for (int q2 = tid; q2 < nd; q2 += kT) S.val[k + q2] = S.Ds[S.dl[q2]];
+            __syncthreads();
+            // (i) positions of the n new eigenvalues in ascending order
+            for (int a = tid; a < n; a += kT) {
+                const double x = S.val[a];
+                int r = 0;
+                for (int b2 = 0; b2 < n; ++b2) r += (S.val[b2] < x || (S.val[b2] == x && b2 < a)) ? 1 : 0;
+                S.rank[a] = lo + r;
+            }
+            __syncthreads();
+            // (j) Z block = Q [V | deflated columns]: block-1 rows against the columns
+            // touching block 1, block-2 rows against those touching block 2
+            // gathered K lists: columns of Q (sec[ktop[t]]) against rows ktop[t] of V
+            for (int t = tid; t < s_ntop; t += kT) S.perm[t] = S.sec[S.ktop[t]];
+            __syncthreads();
+            // rows of block 1: Z[lo + r, rank[c]] = sum_t Q[r, sec[ktop[t]]] V[ktop[t], c]
+            for (int c0 = 0; c0 < k; c0 += TS)
+                for (int r0 = 0; r0 < n1; r0 += TS)
+                    tile_gemm<false>(Z, m, lo, S.rank, r0, c0, min(TS, n1 - r0), min(TS, k - c0), Qp, n, S.perm, V, k,
+                                     S.ktop, s_ntop, sA, sB);
+            __syncthreads();
+            for (int t = tid; t < s_nbot; t += kT) S.perm[t] = S.sec[S.kbot[t]];
+            __syncthreads();
+            // rows of block 2 against the columns that touch block 2
+            for (int c0 = 0; c0 < k; c0 += TS)
+                for (int r0 = n1; r0 < n; r0 += TS)
+                    tile_gemm<false>(Z, m, lo, S.rank, r0, c0, min(TS, n - r0), min(TS, k - c0), Qp, n, S.perm, V, k,
+                                     S.kbot, s_nbot, sA, sB);
+            // deflated columns: copies of Q's columns
+            for (int64_t t = tid; t < (int64_t)nd * n; t += kT) {
+                const int i = (int)(t % n), q2 = (int)(t / n);
+                Z[(int64_t)(lo + i) + (int64_t)S.rank[k + q2] * m] = Qp[i + (int64_t)S.dl[q2] * n];
+            }
+            for (int a = tid; a < n; a += kT) S.D[S.rank[a]] = S.val[a];
+            __syncthreads();
+        }
+    }
+    for (int i = tid; i < m; i += kT) Wa[p.voff + i] = S.D[i];
+}
+
+// ---------------------------------------------------------------------------
+// Q = H_0 H_1 ... H_{m-3} applied to nv vectors x_t of length m (x_t at
+// X + t m): trans -> x <- Q^T x (panels of 32 reflectors in order), else
+// x <- Q x (panels in reverse).  A panel's reflectors act together as
+// I - V T V^T (compact WY: T upper triangular, T_qq = tau_q,
+// T[0:q, q] = -tau_q T[0:q, 0:q] V[:, 0:q]^T v_q), so each panel costs three
+// small products and a handful of barriers instead of two barriers per
+// reflector.  v_j: 1 at j+1, C[r + j m] for r >= j+2, zero above.
+struct WySmem {
+    double* G;   // NB x (NB+1): Gram V^T V, then T
+    double* Xs;  // NB x kWyChunk: V^T x, then T(^T) V^T x
+};
+constexpr int kWyChunk = 64;
+static_assert(NB * (NB + 1) <= NB * (TS + 1) && NB * kWyChunk <= NB * (TS + 1), "WY scratch fits the tile staging");
+
+__device__ __forceinline__ double wy_v(const double* C, int m, int j, int r) {
+    return (r == j + 1) ? 1.0 : (r > j + 1 ? C[r + (int64_t)j * m] : 0.0);
+}
+
+__device__ void wy_apply(const double* __restrict__ C, int m, const double* __restrict__ tau, double* X, int nv,
+                         bool trans, WySmem sm) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nref = m - 2;   // reflectors 0..m-3
+    if (nref <= 0) return;
+    const int npan = (nref + NB - 1) / NB;
+    for (int pp = 0; pp < npan; ++pp) {
+        const int pan = trans ? pp : npan - 1 - pp;
+        const int j0 = pan * NB, nb = min(NB, nref - j0);
+        // Gram of the panel's vectors (rows j0+1 .. m-1): a warp per pair, lanes
+        // over the rows (coalesced), fixed-order sums
+        for (int q = warp; q < NB * NB; q += kT / 32) {
+            const int a = q % NB, b = q / NB;
+            double g = 0.0;
+            if (a < nb && b < nb && a <= b) {
+                for (int r = j0 + 1 + b + lane; r < m; r += 32)
+                    g = fma(wy_v(C, m, j0 + a, r), wy_v(C, m, j0 + b, r), g);
+                g = warp_sum(g);
+            }
+            if (lane == 0) sm.G[a + b * (NB + 1)] = g;
+        }
+        __syncthreads();
+        // T in place of the Gram's upper triangle (one warp, column by column)
+        if (warp == 0) {
+            for (int b = 0; b < nb; ++b) {
+                const double tb = tau[j0 + b];
+                // T[a][b] = -tb * sum_{a <= c < b} T[a][c] G[c][b] for a < b (lane a)
+                double acc = 0.0;
+                if (lane < b)
+                    for (int c2 = lane; c2 < b; ++c2) acc = fma(sm.G[lane + c2 * (NB + 1)], sm.G[c2 + b * (NB + 1)], acc);
+                __syncwarp();
+                if (lane < b) sm.G[lane + b * (NB + 1)] = -tb * acc;
+                if (lane == b) sm.G[b + b * (NB + 1)] = tb;
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int t0 = 0; t0 < nv; t0 += kWyChunk) {
+            const int nc = min(kWyChunk, nv - t0);
+            // Xs = V^T x: a warp per (reflector, vector), lanes over the rows
+            for (int q = warp; q < NB * nc; q += kT / 32) {
+                const int a = q % NB, t = q / NB;
+                double g = 0.0;
+                if (a < nb) {
+                    const double* x = X + (int64_t)(t0 + t) * m;
+                    for (int r = j0 + 1 + a + lane; r < m; r += 32) g = fma(wy_v(C, m, j0 + a, r), x[r], g);
+                    g = warp_sum(g);
+                }
+                if (lane == 0) sm.Xs[a + t * NB] = g;
+            }
+            __syncthreads();
+            // Xs <- T Xs or T^T Xs (thread per column t, in registers)
+            for (int t = tid; t < nc; t += kT) {
+                double xv[NB], yv[NB];
+                for (int a = 0; a < NB; ++a) xv[a] = sm.Xs[a + t * NB];
+                for (int a = 0; a < NB; ++a) {
+                    double y = 0.0;
+                    if (a < nb) {
+                        if (trans) {   // (T^T x)_a = sum_{c <= a} T[c][a] x_c
+                            for (int c2 = 0; c2 <= a; ++c2) y = fma(sm.G[c2 + a * (NB + 1)], xv[c2], y);
+                        } else {       // (T x)_a = sum_{c >= a} T[a][c] x_c
+                            for (int c2 = a; c2 < nb; ++c2) y = fma(sm.G[a + c2 * (NB + 1)], xv[c2], y);
+                        }
+                    }
+                    yv[a] = y;
+                }
+                for (int a = 0; a < NB; ++a) sm.Xs[a + t * NB] = yv[a];
+            }
+            __syncthreads();
+            // x <- x - V Xs
+            for (int64_t q = tid; q < (int64_t)nc * (m - j0 - 1); q += kT) {
+                const int t = (int)(q / (m - j0 - 1)), r = j0 + 1 + (int)(q % (m - j0 - 1));
+                double s = 0.0;
+                for (int a = 0; a < nb; ++a) s = fma(wy_v(C, m, j0 + a, r), sm.Xs[a + t * NB], s);
+                X[(int64_t)(t0 + t) * m + r] -= s;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Owned rows of S U and U, fe and the eigenpairs.  R holds 2 nown rows of
+// length m (row-major, i.e. the column-major m x 2nown matrix R^T): rows
+// t < nown are L[c_t,:] -> (S U)[c_t,:], rows nown + t are (L^-T)[c_t,:] ->
+// U[c_t,:].  The final product with Z goes into the third block G (R Z).
 __global__ void __launch_bounds__(kT) k_eig_rows(const EigProb* __restrict__ probs, const double* __restrict__ Ca,
                                                  const double* __restrict__ La, const double* __restrict__ Ta,
-                                                 const double* __restrict__ Wa, const double2* __restrict__ cs,
-                                                 const int4* __restrict__ sw, const int* __restrict__ nsw,
+                                                 const double* __restrict__ Wa, const double* __restrict__ Za,
                                                  const int* __restrict__ own_cols, const int* __restrict__ ipos,
                                                  double* __restrict__ Ba, double* __restrict__ e_out,
                                                  double* __restrict__ fe_out, const int* __restrict__ status) {
-    __shared__ double v[kEigBatchMax];
+    __shared__ double sA[NB * (TS + 1)], sB[NB * (TS + 1)];
     if (status[blockIdx.x] != kStOk) return;
     const EigProb p = probs[blockIdx.x];
     const int m = p.m, no = p.nown, nb2 = 2 * no;
     const double* C = Ca + p.aoff;
     const double* L = La + p.aoff;
+    const double* Z = Za + p.aoff;
     const double* tau = Ta + p.voff;
-    double* B = Ba + p.boff;
-    double* B2 = B + (int64_t)no * m;
+    double* R = Ba + p.boff;                     // 2 nown rows
+    double* R2 = R + (int64_t)no * m;
+    double* G = R + (int64_t)nb2 * m;            // 2 nown rows of R Z
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = kT / 32;
-    // (1) L rows and unit vectors
     for (int t = 0; t < no; ++t) {
         const int ct = ipos[own_cols[p.o0 + t]];
         for (int r = tid; r < m; r += kT) {
-            B[(int64_t)t * m + r] = (r <= ct) ? L[ct + (int64_t)r * m] : 0.0;
-            B2[(int64_t)t * m + r] = (r == ct) ? 1.0 : 0.0;
+            R[(int64_t)t * m + r] = (r <= ct) ? L[ct + (int64_t)r * m] : 0.0;
+            R2[(int64_t)t * m + r] = (r == ct) ? 1.0 : 0.0;
         }
     }
     __syncthreads();
-    // (2) rows of L^-T: x_t = L^-1 e_{c_t}, 32-row blocks
+    // rows of L^-T: x_t = L^-1 e_{c_t}, 32-row blocks
     for (int i0 = 0; i0 < m; i0 += NB) {
         const int nb = min(NB, m - i0), i1 = i0 + nb;
         for (int t = warp; t < no; t += nwarp) {
-            double* x = B2 + (int64_t)t * m;
+            double* x = R2 + (int64_t)t * m;
             double xv = (lane < nb) ? x[i0 + lane] : 0.0;
             for (int k = 0; k < nb; ++k) {
                 if (lane == k) xv /= L[(i0 + k) + (int64_t)(i0 + k) * m];
@@ -582,129 +1125,72 @@ __global__ void __launch_bounds__(kT) k_eig_rows(const EigProb* __restrict__ pro
         __syncthreads();
         for (int64_t q = tid; q < (int64_t)no * (m - i1); q += kT) {
             const int t = (int)(q / (m - i1)), r = i1 + (int)(q % (m - i1));
-            double* x = B2 + (int64_t)t * m;
+            double* x = R2 + (int64_t)t * m;
             double s = 0.0;
             for (int k = 0; k < nb; ++k) s = fma(L[r + (int64_t)(i0 + k) * m], x[i0 + k], s);
             x[r] -= s;
         }
         __syncthreads();
     }
-    // (3) B <- B Q = B H_0 H_1 ... H_{m-3}
-    for (int k = 0; k + 2 < m; ++k) {
-        const double tk = tau[k];
-        if (tk == 0.0) continue;
-        for (int r = k + 1 + tid; r < m; r += kT) v[r] = (r == k + 1) ? 1.0 : C[r + (int64_t)k * m];
-        __syncthreads();
-        for (int b = warp; b < nb2; b += nwarp) {
-            double* row = B + (int64_t)b * m;
-            double s = 0.0;
-            for (int r = k + 1 + lane; r < m; r += 32) s = fma(row[r], v[r], s);
-            s = warp_sum(s) * tk;
-            for (int r = k + 1 + lane; r < m; r += 32) row[r] -= s * v[r];
-        }
-        __syncthreads();
-    }
-    // (4) B <- B Z: the stored rotations in the order they were made
-    const double2* rot = cs + p.roff;
-    const int4* swp = sw + p.soff;
-    const int ns = nsw[blockIdx.x];
-    for (int b = tid; b < nb2; b += kT) {
-        double* row = B + (int64_t)b * m;
-        for (int q = 0; q < ns; ++q) {
-            const int4 h = swp[q];
-            const int mm = h.y, cnt = h.z;
-            const double2* rr = rot + h.w;
-            double hi = row[mm];
-            for (int u = 0; u < cnt; ++u) {
-                const int i = mm - 1 - u;
-                const double2 g = rr[u];
-                const double lo = row[i];
-                row[i + 1] = g.y * lo + g.x * hi;
-                hi = g.x * lo - g.y * hi;
-            }
-            row[mm - cnt] = hi;
-        }
-    }
+    // R <- R Q: each row x becomes Q^T x (the tiles' staging space as scratch)
+    wy_apply(C, m, tau, R, nb2, true, WySmem{sA, sB});
+    // G^T = Z^T R^T (m x 2nown, column-major = G row-major)
+    for (int c0 = 0; c0 < nb2; c0 += TS)
+        for (int r0 = 0; r0 < m; r0 += TS)
+            tile_gemm<true>(G, m, 0, nullptr, r0, c0, min(TS, m - r0), min(TS, nb2 - c0), Z, m, nullptr, R, m, nullptr, m,
+                            sA, sB);
     __syncthreads();
-    // (5) fe_j = sum_t (SU)[c_t, j] U[c_t, j]; eigenvalues
+    const double* G2 = G + (int64_t)no * m;
     for (int j = tid; j < m; j += kT) {
         double f = 0.0;
-        for (int t = 0; t < no; ++t) f = fma(B[(int64_t)t * m + j], B2[(int64_t)t * m + j], f);
+        for (int t = 0; t < no; ++t) f = fma(G[(int64_t)t * m + j], G2[(int64_t)t * m + j], f);
         e_out[p.eoff + j] = Wa[p.voff + j];
         fe_out[p.eoff + j] = f;
     }
 }
 
 // ---------------------------------------------------------------------------
-// Owned columns of P_k at mu: w_t = occ o U[c_t,:]^T, w <- Z w (rotations in
-// reverse), w <- Q w (reflectors in reverse), w <- L^-T w; scattered into the
-// packed result, rows map(i) <= c_t of column c_t.
+// Owned columns of P_k at mu: w_t = occ o U[c_t,:]^T, w <- Z w, w <- Q w
+// (reflectors in reverse), w <- L^-T w; scattered into the packed result,
+// rows map(i) <= c_t of column c_t (or written dense).
 __global__ void __launch_bounds__(kT) k_eig_final(const EigProb* __restrict__ probs, const double* __restrict__ Ca,
                                                   const double* __restrict__ La, const double* __restrict__ Ta,
-                                                  const double* __restrict__ Wa, const double2* __restrict__ cs,
-                                                  const int4* __restrict__ sw, const int* __restrict__ nsw,
+                                                  const double* __restrict__ Wa, const double* __restrict__ Za,
                                                   const int* __restrict__ maps, const int* __restrict__ own_cols,
                                                   double* __restrict__ Ba, double mu, double* __restrict__ Ppk,
                                                   double* __restrict__ Pdense) {
-    __shared__ double v[kEigBatchMax];
+    __shared__ double sA[NB * (TS + 1)], sB[NB * (TS + 1)];
     const EigProb p = probs[blockIdx.x];
     const int m = p.m, no = p.nown;
     const double* C = Ca + p.aoff;
     const double* L = La + p.aoff;
+    const double* Z = Za + p.aoff;
     const double* tau = Ta + p.voff;
     const double* ev = Wa + p.voff;
-    double* W = Ba + p.boff;                    // reuses the (S U) rows
-    const double* U2 = W + (int64_t)no * m;     // U[c_t, :]
+    double* W0 = Ba + p.boff;                       // (S U) rows block: free after the prepare step
+    const double* U2 = Ba + p.boff + 3 * (int64_t)no * m;   // U[c_t, :] (second half of G)
+    double* W = Ba + p.boff + (int64_t)no * m;      // m x nown, column-major
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = kT / 32;
     for (int64_t q = tid; q < (int64_t)no * m; q += kT) {
         const int j = (int)(q % m);
         const double e = ev[j];
         const double occ = e < mu ? 2.0 : (e == mu ? 1.0 : 0.0);
-        W[q] = occ * U2[q];
+        W0[q] = occ * U2[q];
     }
     __syncthreads();
-    // Z w: rotations in reverse order
-    const double2* rot = cs + p.roff;
-    const int4* swp = sw + p.soff;
-    const int ns = nsw[blockIdx.x];
-    for (int t = tid; t < no; t += kT) {
-        double* w = W + (int64_t)t * m;
-        for (int q = ns - 1; q >= 0; --q) {
-            const int4 h = swp[q];
-            const int mm = h.y, cnt = h.z;
-            const double2* rr = rot + h.w;
-            int i = mm - cnt;
-            double lo = w[i];
-            for (int u = cnt - 1; u >= 0; --u, ++i) {
-                const double2 g = rr[u];
-                const double hi = w[i + 1];
-                w[i] = g.x * lo + g.y * hi;
-                lo = g.x * hi - g.y * lo;
-            }
-            w[i] = lo;
-        }
-    }
+    // W = Z W0
+    for (int c0 = 0; c0 < no; c0 += TS)
+        for (int r0 = 0; r0 < m; r0 += TS)
+            tile_gemm<false>(W, m, 0, nullptr, r0, c0, min(TS, m - r0), min(TS, no - c0), Z, m, nullptr, W0, m, nullptr, m,
+                             sA, sB);
     __syncthreads();
-    // Q w = H_0 (H_1 (... H_{m-3} w))
-    for (int k = m - 3; k >= 0; --k) {
-        const double tk = tau[k];
-        if (tk == 0.0) continue;
-        for (int r = k + 1 + tid; r < m; r += kT) v[r] = (r == k + 1) ? 1.0 : C[r + (int64_t)k * m];
-        __syncthreads();
-        for (int t = warp; t < no; t += nwarp) {
-            double* w = W + (int64_t)t * m;
-            double s = 0.0;
-            for (int r = k + 1 + lane; r < m; r += 32) s = fma(v[r], w[r], s);
-            s = warp_sum(s) * tk;
-            for (int r = k + 1 + lane; r < m; r += 32) w[r] -= s * v[r];
-        }
-        __syncthreads();
-    }
+    // Q W (the tiles' staging space as scratch)
+    wy_apply(C, m, tau, W, no, false, WySmem{sA, sB});
     // L^-T w: back substitution, warp per column
     for (int t = warp; t < no; t += nwarp) {
         double* w = W + (int64_t)t * m;
         for (int i = m - 1; i >= 0; --i) {
-            const double* li = L + (int64_t)i * m;   // column i of L: L[k, i], k > i
+            const double* li = L + (int64_t)i * m;
             double s = 0.0;
             for (int k = i + 1 + lane; k < m; k += 32) s = fma(li[k], w[k], s);
             s = warp_sum(s);
@@ -732,9 +1218,9 @@ struct EigBatch {
     int nprob = 0;
     int maxm = 0;
     std::vector<EigProb> hp;
-    DevBuf probs, Ca, La, Da, Ea, Ta, Wa, Ba, cs, sw, nsw, status;
+    DevBuf probs, Ca, La, Za, Qa, Va, Da, Ea, Ta, Wa, Ba, status;
     ~EigBatch() {
-        for (DevBuf* b : {&probs, &Ca, &La, &Da, &Ea, &Ta, &Wa, &Ba, &cs, &sw, &nsw, &status}) b->release();
+        for (DevBuf* b : {&probs, &Ca, &La, &Za, &Qa, &Va, &Da, &Ea, &Ta, &Wa, &Ba, &status}) b->release();
     }
 };
 
@@ -746,20 +1232,11 @@ void eig_setup_attrs() {
     static const bool done = [] {
         PTB_CUDA(cudaFuncSetAttribute(k_eig_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBlocked));
         PTB_CUDA(cudaFuncSetAttribute(k_eig_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBlocked));
-        PTB_CUDA(cudaFuncSetAttribute(k_eig_ql, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(sizeof(double) * 2 * kEigBatchMax * kQlWarps)));
+        PTB_CUDA(cudaFuncSetAttribute(k_eig_dc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDcSmem));
         return true;
     }();
     (void)done;
 }
-
-// Rotation and sweep capacities: about m^2 rotations are typical; the first
-// pass reserves 1.5 m^2 + 64 m, a problem that needs more is redone with the
-// bound kQlMaxIter m^2 (kQlMaxIter sweeps of at most m rotations per eigenvalue).
-int64_t rot_cap(int m, bool full) {
-    return full ? (int64_t)kQlMaxIter * m * m + 64 : (int64_t)(1.5 * m * m) + 64 * (int64_t)m;
-}
-int64_t sweep_cap(int m, bool full) { return full ? (int64_t)kQlMaxIter * m + 8 : 4 * (int64_t)m + 8; }
 
 }  // namespace
 
@@ -767,12 +1244,13 @@ std::shared_ptr<EigBatch> eig_batch_prepare(ptbgpu_ctx* c, int64_t n, const doub
                                             const std::vector<EigProbHost>& probs, const int* d_maps,
                                             const int* d_own_cols, const int* d_ipos, double* d_e, double* d_fe,
                                             int prl, double* flops) {
+    (void)prl;
     if (probs.empty()) return nullptr;
     eig_setup_attrs();
     cudaStream_t s = c->stream;
     auto eb = std::make_shared<EigBatch>();
     eb->nprob = (int)probs.size();
-    int64_t asz = 0, vsz = 0, bsz = 0, rsz = 0, ssz = 0, psz = 0;
+    int64_t asz = 0, vsz = 0, bsz = 0, psz = 0;
     for (const EigProbHost& q : probs) {
         PTB_CHECK(q.m >= 1 && q.m <= kEigBatchMax, PTBGPU_EINVAL, "submatrix %d of order %d outside the batched solver",
                   q.k + 1, q.m);
@@ -790,31 +1268,18 @@ std::shared_ptr<EigBatch> eig_batch_prepare(ptbgpu_ctx* c, int64_t n, const doub
         p.aoff = asz;
         p.voff = vsz;
         p.boff = bsz;
-        p.roff = rsz;
-        p.rcap = rot_cap(q.m, false);
-        p.soff = ssz;
-        p.scap = sweep_cap(q.m, false);
         asz += (int64_t)q.m * q.m;
         vsz += q.m;
-        bsz += 2 * (int64_t)q.nown * q.m;
-        rsz += p.rcap;
-        ssz += p.scap;
+        bsz += 4 * (int64_t)q.nown * q.m;
         eb->maxm = std::max(eb->maxm, q.m);
         eb->hp.push_back(p);
         if (flops) *flops += 7.0 * std::pow((double)q.m, 3);
     }
     const int np = eb->nprob;
     eb->probs.reserve(sizeof(EigProb) * np);
-    eb->Ca.reserve(sizeof(double) * asz);
-    eb->La.reserve(sizeof(double) * asz);
-    eb->Da.reserve(sizeof(double) * vsz);
-    eb->Ea.reserve(sizeof(double) * vsz);
-    eb->Ta.reserve(sizeof(double) * vsz);
-    eb->Wa.reserve(sizeof(double) * vsz);
+    for (DevBuf* b : {&eb->Ca, &eb->La, &eb->Za, &eb->Qa, &eb->Va}) b->reserve(sizeof(double) * asz);
+    for (DevBuf* b : {&eb->Da, &eb->Ea, &eb->Ta, &eb->Wa}) b->reserve(sizeof(double) * vsz);
     eb->Ba.reserve(sizeof(double) * std::max<int64_t>(bsz, 1));
-    eb->cs.reserve(sizeof(double2) * rsz);
-    eb->sw.reserve(sizeof(int4) * ssz);
-    eb->nsw.reserve(sizeof(int) * np);
     eb->status.reserve(sizeof(int) * np);
     PTB_CUDA(cudaMemcpyAsync(eb->probs.ptr, eb->hp.data(), sizeof(EigProb) * np, cudaMemcpyHostToDevice, s));
     PTB_CUDA(cudaMemsetAsync(eb->status.ptr, 0, sizeof(int) * np, s));
@@ -826,10 +1291,8 @@ std::shared_ptr<EigBatch> eig_batch_prepare(ptbgpu_ctx* c, int64_t n, const doub
     k_eig_reduce<<<np, kT, kSmemBlocked, s>>>(dp, eb->La.as<double>(), eb->Ca.as<double>(), dst);
     k_eig_sytrd<<<np, kT, 0, s>>>(dp, eb->Ca.as<double>(), eb->Da.as<double>(), eb->Ea.as<double>(),
                                   eb->Ta.as<double>(), dst);
-    const size_t ql_smem = sizeof(double) * 2 * eb->maxm * kQlWarps;
-    k_eig_ql<<<(np + kQlWarps - 1) / kQlWarps, 32 * kQlWarps, ql_smem, s>>>(
-        np, dp, eb->Da.as<double>(), eb->Ea.as<double>(), eb->Wa.as<double>(), eb->cs.as<double2>(),
-        eb->sw.as<int4>(), eb->nsw.as<int>(), dst, eb->maxm, 0);
+    k_eig_dc<<<np, kT, kDcSmem, s>>>(dp, eb->Da.as<double>(), eb->Ea.as<double>(), eb->Wa.as<double>(),
+                                     eb->Za.as<double>(), eb->Qa.as<double>(), eb->Va.as<double>(), dst);
     count_launch(5);
     PTB_CUDA(cudaGetLastError());
     std::vector<int> hst(np);
@@ -838,53 +1301,12 @@ std::shared_ptr<EigBatch> eig_batch_prepare(ptbgpu_ctx* c, int64_t n, const doub
     for (int q = 0; q < np; ++q)
         PTB_CHECK(hst[q] <= 0, PTBGPU_ENOTSPD, "overlap submatrix %d not positive definite (leading minor %d)",
                   eb->hp[q].k + 1, hst[q]);
-    // problems whose rotations did not fit: redo them with the full bound
-    std::vector<int> redo;
     for (int q = 0; q < np; ++q)
-        if (hst[q] == kStRotCap) redo.push_back(q);
-    if (!redo.empty()) {
-        int64_t extra = 0, extra_s = 0;
-        for (int q : redo) {
-            extra += rot_cap(eb->hp[q].m, true);
-            extra_s += sweep_cap(eb->hp[q].m, true);
-        }
-        DevBuf cs2, sw2;
-        cs2.reserve(sizeof(double2) * (rsz + extra));
-        sw2.reserve(sizeof(int4) * (ssz + extra_s));
-        PTB_CUDA(cudaMemcpyAsync(cs2.ptr, eb->cs.ptr, sizeof(double2) * rsz, cudaMemcpyDeviceToDevice, s));
-        PTB_CUDA(cudaMemcpyAsync(sw2.ptr, eb->sw.ptr, sizeof(int4) * ssz, cudaMemcpyDeviceToDevice, s));
-        int64_t ro = rsz, so = ssz;
-        for (int q : redo) {
-            EigProb& p = eb->hp[q];
-            p.roff = ro;
-            p.rcap = rot_cap(p.m, true);
-            p.soff = so;
-            p.scap = sweep_cap(p.m, true);
-            ro += p.rcap;
-            so += p.scap;
-        }
-        PTB_CUDA(cudaStreamSynchronize(s));
-        std::swap(eb->cs, cs2);
-        std::swap(eb->sw, sw2);
-        cs2.release();
-        sw2.release();
-        PTB_CUDA(cudaMemcpyAsync(eb->probs.ptr, eb->hp.data(), sizeof(EigProb) * np, cudaMemcpyHostToDevice, s));
-        // the kernel only redoes the problems still marked kStRotCap
-        k_eig_ql<<<(np + kQlWarps - 1) / kQlWarps, 32 * kQlWarps, ql_smem, s>>>(
-            np, dp, eb->Da.as<double>(), eb->Ea.as<double>(), eb->Wa.as<double>(), eb->cs.as<double2>(),
-            eb->sw.as<int4>(), eb->nsw.as<int>(), dst, eb->maxm, 1);
-        count_launch();
-        PTB_CUDA(cudaGetLastError());
-        PTB_CUDA(cudaMemcpyAsync(hst.data(), dst, sizeof(int) * np, cudaMemcpyDeviceToHost, s));
-        PTB_CUDA(cudaStreamSynchronize(s));
-        log_line(prl, 2, " * submatrix QL: %zu problems redone with the full rotation bound", redo.size());
-    }
-    for (int q = 0; q < np; ++q)
-        PTB_CHECK(hst[q] == kStOk, PTBGPU_EITER, "tridiagonal QL iteration did not converge on submatrix %d",
+        PTB_CHECK(hst[q] == kStOk, PTBGPU_EITER, "tridiagonal eigensolver did not converge on submatrix %d",
                   eb->hp[q].k + 1);
     k_eig_rows<<<np, kT, 0, s>>>(dp, eb->Ca.as<double>(), eb->La.as<double>(), eb->Ta.as<double>(),
-                                 eb->Wa.as<double>(), eb->cs.as<double2>(), eb->sw.as<int4>(), eb->nsw.as<int>(),
-                                 d_own_cols, d_ipos, eb->Ba.as<double>(), d_e, d_fe, dst);
+                                 eb->Wa.as<double>(), eb->Za.as<double>(), d_own_cols, d_ipos, eb->Ba.as<double>(),
+                                 d_e, d_fe, dst);
     count_launch();
     PTB_CUDA(cudaGetLastError());
     return eb;
@@ -896,9 +1318,8 @@ void eig_batch_final(ptbgpu_ctx* c, EigBatch& eb, double mu, int64_t n, const in
     if (eb.nprob == 0) return;
     cudaStream_t s = c->stream;
     k_eig_final<<<eb.nprob, kT, 0, s>>>(eb.probs.as<EigProb>(), eb.Ca.as<double>(), eb.La.as<double>(),
-                                        eb.Ta.as<double>(), eb.Wa.as<double>(), eb.cs.as<double2>(),
-                                        eb.sw.as<int4>(), eb.nsw.as<int>(), d_maps, d_own_cols, eb.Ba.as<double>(),
-                                        mu, dP, dPdense);
+                                        eb.Ta.as<double>(), eb.Wa.as<double>(), eb.Za.as<double>(), d_maps,
+                                        d_own_cols, eb.Ba.as<double>(), mu, dP, dPdense);
     count_launch();
     PTB_CUDA(cudaGetLastError());
 }

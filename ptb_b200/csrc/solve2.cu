@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "oz_gemm.cuh"
 
 namespace ptb {
 
@@ -122,10 +123,16 @@ void solve2_device(ptbgpu_ctx* c, int64_t mode, int64_t n, int64_t nel, int64_t 
     k_scale_cols2<<<g1(n), 256, 0, s>>>(n, U, bv.as<double>(), Ptmp);
     count_launch();
     PTB_CUDA(cudaGetLastError());
-    const double one = 1.0, zero = 0.0;
-    // P = C diag(focc) C^T
-    PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)n, (int)n, (int)n, &one, U, (int)n, Ptmp,
-                           (int)n, &zero, B, (int)n));
+    // P = C diag(focc) C^T (dmat, source/solve.f:263-283): FP64-class product on
+    // the int8 tensor cores; beyond its exact range (n > 16643) cuBLAS DGEMM
+    if (oz::supported(n, 8)) {
+        oz_dgemm(c, n, 1.0, U, false, Ptmp, true, B, 8);
+        oz_check(c, "int8 product (density matrix)");
+    } else {
+        const double one = 1.0, zero = 0.0;
+        PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)n, (int)n, (int)n, &one, U, (int)n, Ptmp,
+                               (int)n, &zero, B, (int)n));
+    }
     pack_cols(s, n, n, B, dP);
     PTB_CUDA(cudaStreamSynchronize(s));
     // the reference's closing timer block of solve2 (source/pgtb.f90:1108-1168)
@@ -161,11 +168,19 @@ void check_density_device(ptbgpu_ctx* c, int64_t n, const double* dP, const doub
         unpack_sym(s, n, n, dH, M, 0.0);
         st->band_energy = trace_prod_dev(c, n, n, P, M);
     }
-    const double one = 1.0, half = 0.5, zero = 0.0;
-    PTB_CUBLAS(cublasDsymm(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, (int)n, (int)n, &one, P, (int)n, S,
-                           (int)n, &zero, M, (int)n));                  // P S
-    PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, (int)n, (int)n, &half, M, (int)n, P, (int)n,
-                           &zero, Q, (int)n));                          // 1/2 P S P
+    // 1/2 P S P: FP64-class products on the int8 tensor cores (beyond their
+    // exact range, n > 16643, cuBLAS)
+    if (oz::supported(n, 8)) {
+        oz_dgemm(c, n, 1.0, P, false, S, false, M, 8);                 // P S
+        oz_dgemm(c, n, 0.5, M, false, P, false, Q, 8);                 // 1/2 P S P
+        oz_check(c, "int8 product (idempotency)");
+    } else {
+        const double one = 1.0, half = 0.5, zero = 0.0;
+        PTB_CUBLAS(cublasDsymm(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, (int)n, (int)n, &one, P, (int)n,
+                               S, (int)n, &zero, M, (int)n));
+        PTB_CUBLAS(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, (int)n, (int)n, &half, M, (int)n, P,
+                               (int)n, &zero, Q, (int)n));
+    }
     axpby_diag(s, n, n, -1.0, P, 1.0, Q, 0.0);                         // mm2 - P
     st->idempotency_ref = std::fabs(sum_dev(c, n * n, Q));
     st->idempotency_frob = frob_dev(c, n, n, Q);

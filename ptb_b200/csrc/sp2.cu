@@ -34,6 +34,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <vector>
 
@@ -1099,5 +1100,63 @@ void oz_gemm_entry(ptbgpu_ctx* c, int64_t n, int S, int kblock, int variant, int
     PTB_CUDA(cudaMemcpyAsync(hC, bc.ptr, sizeof(double) * n * n, cudaMemcpyDeviceToHost, s));
     check_timeout(c, "int8 product");
 }
+
+// ---------------------------------------------------------------------------
+// General FP64-class products on the int8 tensor cores for the module code
+// (purification module, metrics): C = alpha op(A) op(B) for column-major
+// n x n device matrices, S slices (8: about 53 bits relative to the row and
+// column maxima).  The device tile list of each (n, S) is kept on the context,
+// so a product is two slicings and one launch with no host round trip.
+namespace {
+struct OzTiles {
+    DevBuf buf;
+    int count = 0;
+    double ops = 0.0;
+};
+struct OzTileCache {
+    std::map<std::pair<int64_t, int>, OzTiles> lists;
+    ~OzTileCache() {
+        for (auto& kv : lists) kv.second.buf.release();
+    }
+};
+}  // namespace
+
+void oz_dgemm(ptbgpu_ctx* c, int64_t n, double alpha, const double* A, bool ta, const double* B, bool tb,
+              double* C, int S) {
+    PTB_CHECK(oz::supported(n, S), PTBGPU_EINVAL, "n = %lld is too large for exact int32 sums with %d slices",
+              (long long)n, S);
+    if (!c->oz_tile_cache) c->oz_tile_cache = std::make_shared<OzTileCache>();
+    OzTileCache& tc = *static_cast<OzTileCache*>(c->oz_tile_cache.get());
+    const oz::Operand opA = oz_operand(c, 0, n, S), opB = oz_operand(c, 1, n, S);
+    const int variant = oz::resolve_variant(oz::V_DEFAULT, S, 0);
+    auto key = std::make_pair(n, S);
+    auto it = tc.lists.find(key);
+    if (it == tc.lists.end()) {
+        const std::vector<int4> t = oz::build_tiles(opA.ldp, false, oz::TRI_NONE, oz::TRI_NONE, S, variant);
+        OzTiles e;
+        e.buf.reserve(sizeof(int4) * t.size());
+        e.count = (int)t.size();
+        e.ops = oz::tile_ops(t, S, variant);
+        PTB_CUDA(cudaMemcpy(e.buf.ptr, t.data(), sizeof(int4) * t.size(), cudaMemcpyHostToDevice));
+        it = tc.lists.emplace(key, e).first;
+    }
+    c->oz_ops += it->second.ops;
+    // rows i of op(A): A(i,k) = A[i + k n], A^T(i,k) = A[k + i n]
+    oz_slice(c, A, ta ? n : 1, ta ? 1 : n, n, oz::TRI_NONE, opA);
+    // rows j of op(B)^T, i.e. op(B)(k, j): B[k + j n], or B^T: B[j + k n]
+    oz_slice(c, B, tb ? 1 : n, tb ? n : 1, n, oz::TRI_NONE, opB);
+    oz::OzEpi ep;
+    ep.n = n;
+    ep.alpha = alpha;
+    ep.out = C;
+    ep.ors = 1;
+    ep.ocs = n;
+    ep.ldp = opA.ldp;
+    ep.err = &c->flags->timeout;
+    oz::product(c->stream, oz::OZ_OUT, opA, opB, it->second.buf.as<int4>(), it->second.count, ep, 0, variant);
+    count_launch();
+}
+
+void oz_check(ptbgpu_ctx* c, const char* what) { check_timeout(c, what); }
 
 }  // namespace ptb
