@@ -393,8 +393,10 @@ def run_sm(args, rank, world, local, pg):
                         "mu_iterations": int(last.mu_iterations)},
         "e2e": {"value": wall, "unit": UNIT, "h2d_bytes_per_step": 2 * npk * 8, "d2h_bytes_per_step": npk * 8},
         "gpu_launches": int(sum(x.kernel_launches for x in stats)),
-        "roofline": {"bound": "fp64", "kernel": "generalized eigensolves (cuSOLVER batched syev / sygvd) and the "
-                     "library's gather, fe and bisection kernels", "achieved": feig / (ms / 1e3) / 1e12,
+        "roofline": {"bound": "fp64", "kernel": "k_eig_fused (the library's batched generalized eigensolver, one "
+                     "persistent launch: Cholesky, reduction, tridiagonalisation, divide and conquer, owned rows; "
+                     "submatrices of order <= 1024) and cuSOLVER dsygvd for larger ones on side streams",
+                     "achieved": feig / (ms / 1e3) / 1e12,
                      "peak": 37.0, "unit": "TFLOP/s", "frac": feig / (ms / 1e3) / 1e12 / 37.0, "traffic": None,
                      "peak_kind": "nominal B200 FP64 (no measured FP64 figure on this pool)",
                      "work": "7 m^3 per submatrix (dsygvd with vectors), the whole call's device time"},
@@ -667,10 +669,15 @@ def run_ours(args, rank, world, local, pg):
     executed = last.tc_flops   # every product of the split, every tile that ran (reported by the library)
     achieved = alg / (last.ms_tc_sp2 + last.ms_tc_full) / 1e9 if (last.ms_tc_sp2 + last.ms_tc_full) > 0 else 0.0
     exec_tf = executed / (last.ms_tc_sp2 + last.ms_tc_full) / 1e9 if (last.ms_tc_sp2 + last.ms_tc_full) > 0 else 0.0
+    # measured DRAM bytes per launch of each epilogue (ncu at ndim 11776), weighted
+    # by this step's launches of each; only for the workload they were measured on
     traffic = None
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
-        traffic = json.loads(tp.read_text()).get("tc_product_bytes_per_launch")
+        tj = json.loads(tp.read_text())
+        if tj.get("ndim") == n and (last.n_tc_sp2 + last.n_tc_full) > 0:
+            traffic = (last.n_tc_sp2 * tj["sp2_bytes_per_launch"] + last.n_tc_full * tj["full_bytes_per_launch"]) / (
+                last.n_tc_sp2 + last.n_tc_full)
     # the FP64-class products of the mixed path on the int8 tensor cores (Ozaki slices)
     oz = None
     if last.n_oz > 0 and last.ms_oz > 0:

@@ -142,12 +142,22 @@ __device__ double warp_sum(double v) {
 }
 
 // ---------------------------------------------------------------------------
+// Shared memory of the stages, carved from one dynamic buffer: the tile
+// staging (sA, sB), the diagonal block of the blocked factorisations (sD), a
+// union region (the tridiagonalisation's vectors or the divide and conquer's
+// per-element arrays, M = the largest order of the batch) and a few scalars.
+struct StageSmem {
+    double *sA, *sB, *sD;
+    unsigned char* uni;
+    int* ints;      // 16
+    double* dsc;    // 2 + kT / 32
+    int M;
+};
+
+// ---------------------------------------------------------------------------
 // Gather H_k, S_k (source/sm.f90:240-246) into the C and L arenas.
-__global__ void __launch_bounds__(kT) k_eig_gather(const EigProb* __restrict__ probs, const int* __restrict__ maps,
-                                                   const double* __restrict__ H,
-                                                   const double* __restrict__ S, double* __restrict__ Ca,
-                                                   double* __restrict__ La) {
-    const EigProb p = probs[blockIdx.x];
+__device__ void stage_gather(const EigProb& p, const int* __restrict__ maps, const double* __restrict__ H,
+                             const double* __restrict__ S, double* __restrict__ Ca, double* __restrict__ La) {
     const int m = p.m;
     const int* mp = maps + p.moff;
     double* C = Ca + p.aoff;
@@ -164,15 +174,13 @@ __global__ void __launch_bounds__(kT) k_eig_gather(const EigProb* __restrict__ p
 
 // ---------------------------------------------------------------------------
 // S_k = L L^T in place (lower), right-looking with 32-wide panels; the strict
-// upper triangle is zeroed.  status = order of the first non-positive pivot.
-__global__ void __launch_bounds__(kT) k_eig_potrf(const EigProb* __restrict__ probs, double* __restrict__ La,
-                                                  int* __restrict__ status) {
-    extern __shared__ double sm[];
-    double* sA = sm;                       // NB x (TS+1)
-    double* sB = sA + NB * (TS + 1);       // NB x (TS+1)
-    double* sD = sB + NB * (TS + 1);       // NB x (NB+1), sD[i + j*(NB+1)]
-    __shared__ int fail;
-    const EigProb p = probs[blockIdx.x];
+// upper triangle is zeroed.  Returns the order of the first non-positive
+// pivot (0: positive definite).
+__device__ int stage_potrf(const EigProb& p, double* __restrict__ La, const StageSmem& sh) {
+    double* sA = sh.sA;
+    double* sB = sh.sB;
+    double* sD = sh.sD;   // sD[i + j*(NB+1)]
+    int& fail = sh.ints[0];
     const int m = p.m;
     double* L = La + p.aoff;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -236,10 +244,12 @@ __global__ void __launch_bounds__(kT) k_eig_potrf(const EigProb* __restrict__ pr
                                         L + (int64_t)kb * m, m, nb, sA, sB);
     }
     __syncthreads();
-    if (tid == 0) status[blockIdx.x] = fail;
-    if (fail) return;
+    const int f = fail;
+    __syncthreads();
+    if (f) return f;
     for (int j = 1; j < m; ++j)
         for (int i = tid; i < j; i += kT) L[(int64_t)i + (int64_t)j * m] = 0.0;
+    return 0;
 }
 
 // X <- L^-1 X (L lower, m x m; X m x m), blocked by 32 rows.
@@ -273,14 +283,11 @@ __device__ void trsm_left_lower(const double* __restrict__ L, double* __restrict
 
 // C <- L^-1 H_k L^-T: C <- L^-1 C, transpose, C <- L^-1 C, then the lower
 // triangle copied to the upper one (exactly symmetric).
-__global__ void __launch_bounds__(kT) k_eig_reduce(const EigProb* __restrict__ probs, const double* __restrict__ La,
-                                                   double* __restrict__ Ca, const int* __restrict__ status) {
-    extern __shared__ double sm[];
-    double* sA = sm;
-    double* sB = sA + NB * (TS + 1);
-    double* sD = sB + NB * (TS + 1);
-    if (status[blockIdx.x] != kStOk) return;
-    const EigProb p = probs[blockIdx.x];
+__device__ void stage_reduce(const EigProb& p, const double* __restrict__ La, double* __restrict__ Ca,
+                             const StageSmem& sh) {
+    double* sA = sh.sA;
+    double* sB = sh.sB;
+    double* sD = sh.sD;
     const int m = p.m;
     const double* L = La + p.aoff;
     double* C = Ca + p.aoff;
@@ -315,14 +322,14 @@ __global__ void __launch_bounds__(kT) k_eig_reduce(const EigProb* __restrict__ p
 constexpr int kSyRows = (kEigBatchMax + kT - 1) / kT;   // rows per thread
 constexpr int kSyChunk = 8;                              // columns per batch of loads
 
-__global__ void __launch_bounds__(kT) k_eig_sytrd(const EigProb* __restrict__ probs, double* __restrict__ Ca,
-                                                  double* __restrict__ Da, double* __restrict__ Ea,
-                                                  double* __restrict__ Ta, const int* __restrict__ status) {
-    __shared__ double vc[kEigBatchMax], wc[kEigBatchMax], vn[kEigBatchMax];
-    __shared__ double red[kT / 32];
-    __shared__ double sh_tau, sh_alpha;
-    if (status[blockIdx.x] != kStOk) return;
-    const EigProb p = probs[blockIdx.x];
+__device__ void stage_sytrd(const EigProb& p, double* __restrict__ Ca, double* __restrict__ Da,
+                            double* __restrict__ Ea, double* __restrict__ Ta, const StageSmem& sh) {
+    double* vc = reinterpret_cast<double*>(sh.uni);
+    double* wc = vc + sh.M;
+    double* vn = wc + sh.M;
+    double* red = sh.dsc + 2;
+    double& sh_tau = sh.dsc[0];
+    double& sh_alpha = sh.dsc[1];
     const int m = p.m;
     double* A = Ca + p.aoff;
     double* d = Da + p.voff;
@@ -406,8 +413,10 @@ __global__ void __launch_bounds__(kT) k_eig_sytrd(const EigProb* __restrict__ pr
             wr[q] = (r < m) ? wc[r] : 0.0;
         }
         // columns in chunks of kSyChunk: every load of a chunk is issued before
-        // its stores, so the pass streams instead of waiting on each element
-        for (int k0 = r0; k0 < m; k0 += kSyChunk) {
+        // its stores, so the pass streams instead of waiting on each element;
+        // threads without a row in the trailing block skip the pass
+        const bool has_row = r0 + tid < m;
+        for (int k0 = has_row ? r0 : m; k0 < m; k0 += kSyChunk) {
             double a[kSyChunk][kSyRows];
 #pragma unroll
             for (int u = 0; u < kSyChunk; ++u) {
@@ -568,33 +577,35 @@ struct DcSmem {
     double2* rcs;
 };
 
-__device__ DcSmem dc_smem(unsigned char* base) {
+// Per-element arrays of capacity M (a multiple of 2, so every block stays
+// 16-byte aligned).
+__device__ DcSmem dc_smem(unsigned char* base, int M) {
     DcSmem s;
     double* d = reinterpret_cast<double*>(base);
     s.D = d;
-    s.Ds = d + kEigBatchMax;
-    s.zs = d + 2 * kEigBatchMax;
-    s.dk = d + 3 * kEigBatchMax;
-    s.zk = d + 4 * kEigBatchMax;
-    s.tau = d + 5 * kEigBatchMax;
-    s.zh = d + 6 * kEigBatchMax;
-    s.val = d + 7 * kEigBatchMax;
-    s.rcs = reinterpret_cast<double2*>(d + 8 * kEigBatchMax);
-    int* ip = reinterpret_cast<int*>(s.rcs + kEigBatchMax);
+    s.Ds = d + M;
+    s.zs = d + 2 * M;
+    s.dk = d + 3 * M;
+    s.zk = d + 4 * M;
+    s.tau = d + 5 * M;
+    s.zh = d + 6 * M;
+    s.val = d + 7 * M;
+    s.rcs = reinterpret_cast<double2*>(d + 8 * M);
+    int* ip = reinterpret_cast<int*>(s.rcs + M);
     s.perm = ip;
-    s.org = ip + kEigBatchMax;
-    s.sec = ip + 2 * kEigBatchMax;
-    s.dl = ip + 3 * kEigBatchMax;
-    s.rank = ip + 4 * kEigBatchMax;
-    s.cls = ip + 5 * kEigBatchMax;
-    s.ktop = ip + 6 * kEigBatchMax;
-    s.kbot = ip + 7 * kEigBatchMax;
-    s.rpair = reinterpret_cast<int2*>(ip + 8 * kEigBatchMax);
+    s.org = ip + M;
+    s.sec = ip + 2 * M;
+    s.dl = ip + 3 * M;
+    s.rank = ip + 4 * M;
+    s.cls = ip + 5 * M;
+    s.ktop = ip + 6 * M;
+    s.kbot = ip + 7 * M;
+    s.rpair = reinterpret_cast<int2*>(ip + 8 * M);
     return s;
 }
-constexpr size_t kDcSmemMerge = sizeof(double) * 8 * kEigBatchMax + sizeof(double2) * kEigBatchMax +
-                                sizeof(int) * 8 * kEigBatchMax + sizeof(int2) * kEigBatchMax;
-constexpr size_t kDcSmem = kDcSmemMerge;
+__host__ __device__ constexpr size_t dc_smem_bytes(int M) {
+    return (sizeof(double) * 8 + sizeof(double2) + sizeof(int) * 8 + sizeof(int2)) * (size_t)M;
+}
 
 // Leaf: implicit QL on d[0..s), e[0..s-1) with Z = I accumulated.  Every
 // lane runs the same scalar iteration on its own copies of d and e and rotates
@@ -725,22 +736,24 @@ __device__ double dc_secular(int k, const double* dk, const double* zk, double r
     return tau;
 }
 
-__global__ void __launch_bounds__(kT) k_eig_dc(const EigProb* __restrict__ probs, const double* __restrict__ Da,
-                                               const double* __restrict__ Ea, double* __restrict__ Wa,
-                                               double* __restrict__ Za, double* __restrict__ Qa,
-                                               double* __restrict__ Va, int* __restrict__ status) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    __shared__ double sA[NB * (TS + 1)], sB[NB * (TS + 1)];
-    __shared__ int s_k, s_nd, s_nrot, s_ntop, s_nbot, s_fail;
-    if (status[blockIdx.x] != kStOk) return;
-    const EigProb p = probs[blockIdx.x];
+__device__ bool stage_dc(const EigProb& p, const double* __restrict__ Da, const double* __restrict__ Ea,
+                         double* __restrict__ Wa, double* __restrict__ Za, double* __restrict__ Qa,
+                         double* __restrict__ Va, const StageSmem& sh) {
+    double* sA = sh.sA;
+    double* sB = sh.sB;
+    int& s_k = sh.ints[1];
+    int& s_nd = sh.ints[2];
+    int& s_nrot = sh.ints[3];
+    int& s_ntop = sh.ints[4];
+    int& s_nbot = sh.ints[5];
+    int& s_fail = sh.ints[6];
     const int m = p.m;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double* Z = Za + p.aoff;
     double* Qp = Qa + p.aoff;
     double* V = Va + p.aoff;
     const double* eo = Ea + p.voff;
-    DcSmem S = dc_smem(smraw);
+    DcSmem S = dc_smem(sh.uni, sh.M);
     int L = 0;
     while (((m + (1 << L) - 1) >> L) > kDcLeaf) ++L;
     const int nleaf = 1 << L;
@@ -780,10 +793,7 @@ __global__ void __launch_bounds__(kT) k_eig_dc(const EigProb* __restrict__ probs
         __syncwarp();
     }
     __syncthreads();
-    if (s_fail) {
-        if (tid == 0) status[blockIdx.x] = kStNoConv;
-        return;
-    }
+    if (s_fail) return false;
     const double eps = 2.220446049250313e-16;
     for (int lev = L - 1; lev >= 0; --lev) {
         for (int q = 0; q < (1 << lev); ++q) {
@@ -976,6 +986,7 @@ __global__ void __launch_bounds__(kT) k_eig_dc(const EigProb* __restrict__ probs
         }
     }
     for (int i = tid; i < m; i += kT) Wa[p.voff + i] = S.D[i];
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -1083,15 +1094,13 @@ __device__ void wy_apply(const double* __restrict__ C, int m, const double* __re
 // length m (row-major, i.e. the column-major m x 2nown matrix R^T): rows
 // t < nown are L[c_t,:] -> (S U)[c_t,:], rows nown + t are (L^-T)[c_t,:] ->
 // U[c_t,:].  The final product with Z goes into the third block G (R Z).
-__global__ void __launch_bounds__(kT) k_eig_rows(const EigProb* __restrict__ probs, const double* __restrict__ Ca,
-                                                 const double* __restrict__ La, const double* __restrict__ Ta,
-                                                 const double* __restrict__ Wa, const double* __restrict__ Za,
-                                                 const int* __restrict__ own_cols, const int* __restrict__ ipos,
-                                                 double* __restrict__ Ba, double* __restrict__ e_out,
-                                                 double* __restrict__ fe_out, const int* __restrict__ status) {
-    __shared__ double sA[NB * (TS + 1)], sB[NB * (TS + 1)];
-    if (status[blockIdx.x] != kStOk) return;
-    const EigProb p = probs[blockIdx.x];
+__device__ void stage_rows(const EigProb& p, const double* __restrict__ Ca, const double* __restrict__ La,
+                           const double* __restrict__ Ta, const double* __restrict__ Wa,
+                           const double* __restrict__ Za, const int* __restrict__ own_cols,
+                           const int* __restrict__ ipos, double* __restrict__ Ba, double* __restrict__ e_out,
+                           double* __restrict__ fe_out, const StageSmem& sh) {
+    double* sA = sh.sA;
+    double* sB = sh.sB;
     const int m = p.m, no = p.nown, nb2 = 2 * no;
     const double* C = Ca + p.aoff;
     const double* L = La + p.aoff;
@@ -1146,6 +1155,68 @@ __global__ void __launch_bounds__(kT) k_eig_rows(const EigProb* __restrict__ pro
         for (int t = 0; t < no; ++t) f = fma(G[(int64_t)t * m + j], G2[(int64_t)t * m + j], f);
         e_out[p.eoff + j] = Wa[p.voff + j];
         fe_out[p.eoff + j] = f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One persistent launch for every submatrix of the step: each CTA takes the
+// next submatrix (largest first) from a device counter and runs all stages on
+// it - gather, Cholesky, reduction, tridiagonalisation, divide and conquer,
+// owned rows and fe - so the uneven sizes balance over the SMs without a
+// launch per stage or per size bucket.  status[pi]: 0, the order of a
+// non-positive pivot of S_k, or kStNoConv.
+__host__ __device__ constexpr size_t stage_smem_bytes(int M) {
+    return sizeof(double) * (2 * NB * (TS + 1) + NB * (NB + 1)) + dc_smem_bytes(M) + sizeof(int) * 16 +
+           sizeof(double) * (2 + kT / 32) + 16;
+}
+
+__device__ StageSmem stage_smem(unsigned char* base, int M) {
+    StageSmem sh;
+    double* d = reinterpret_cast<double*>(base);
+    sh.sA = d;
+    sh.sB = d + NB * (TS + 1);
+    sh.sD = d + 2 * NB * (TS + 1);
+    sh.uni = reinterpret_cast<unsigned char*>(d + 2 * NB * (TS + 1) + NB * (NB + 1));
+    sh.ints = reinterpret_cast<int*>(sh.uni + dc_smem_bytes(M));
+    sh.dsc = reinterpret_cast<double*>(sh.ints + 16);
+    sh.M = M;
+    return sh;
+}
+
+__global__ void __launch_bounds__(kT, 1) k_eig_fused(
+    const EigProb* __restrict__ probs, const int* __restrict__ order, int np, int* __restrict__ counter, int M,
+    const int* __restrict__ maps, const double* __restrict__ H, const double* __restrict__ S,
+    double* __restrict__ Ca, double* __restrict__ La, double* __restrict__ Za, double* __restrict__ Qa,
+    double* __restrict__ Va, double* __restrict__ Da, double* __restrict__ Ea, double* __restrict__ Ta,
+    double* __restrict__ Wa, double* __restrict__ Ba, const int* __restrict__ own_cols,
+    const int* __restrict__ ipos, double* __restrict__ e_out, double* __restrict__ fe_out,
+    int* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const StageSmem sh = stage_smem(smraw, M);
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) sh.ints[15] = atomicAdd(counter, 1);
+        __syncthreads();
+        const int q = sh.ints[15];
+        __syncthreads();
+        if (q >= np) break;
+        const int pi = order[q];
+        const EigProb p = probs[pi];
+        stage_gather(p, maps, H, S, Ca, La);
+        __syncthreads();
+        int st = stage_potrf(p, La, sh);
+        __syncthreads();
+        if (st == kStOk) {
+            stage_reduce(p, La, Ca, sh);
+            __syncthreads();
+            stage_sytrd(p, Ca, Da, Ea, Ta, sh);
+            __syncthreads();
+            if (!stage_dc(p, Da, Ea, Wa, Za, Qa, Va, sh)) st = kStNoConv;
+            __syncthreads();
+            if (st == kStOk) stage_rows(p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, e_out, fe_out, sh);
+        }
+        if (tid == 0) status[pi] = st;
+        __syncthreads();
     }
 }
 
@@ -1218,21 +1289,19 @@ struct EigBatch {
     int nprob = 0;
     int maxm = 0;
     std::vector<EigProb> hp;
-    DevBuf probs, Ca, La, Za, Qa, Va, Da, Ea, Ta, Wa, Ba, status;
+    DevBuf probs, order, counter, Ca, La, Za, Qa, Va, Da, Ea, Ta, Wa, Ba, status;
     ~EigBatch() {
-        for (DevBuf* b : {&probs, &Ca, &La, &Za, &Qa, &Va, &Da, &Ea, &Ta, &Wa, &Ba, &status}) b->release();
+        for (DevBuf* b : {&probs, &order, &counter, &Ca, &La, &Za, &Qa, &Va, &Da, &Ea, &Ta, &Wa, &Ba, &status})
+            b->release();
     }
 };
 
 namespace {
 
-constexpr size_t kSmemBlocked = sizeof(double) * (2 * NB * (TS + 1) + NB * (NB + 1));
-
 void eig_setup_attrs() {
     static const bool done = [] {
-        PTB_CUDA(cudaFuncSetAttribute(k_eig_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBlocked));
-        PTB_CUDA(cudaFuncSetAttribute(k_eig_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBlocked));
-        PTB_CUDA(cudaFuncSetAttribute(k_eig_dc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDcSmem));
+        PTB_CUDA(cudaFuncSetAttribute(k_eig_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)stage_smem_bytes(kEigBatchMax)));
         return true;
     }();
     (void)done;
@@ -1240,8 +1309,8 @@ void eig_setup_attrs() {
 
 }  // namespace
 
-std::shared_ptr<EigBatch> eig_batch_prepare(ptbgpu_ctx* c, int64_t n, const double* H, const double* S,
-                                            const std::vector<EigProbHost>& probs, const int* d_maps,
+std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const double* H, const double* S,
+                                           const std::vector<EigProbHost>& probs, const int* d_maps,
                                             const int* d_own_cols, const int* d_ipos, double* d_e, double* d_fe,
                                             int prl, double* flops) {
     (void)prl;
@@ -1286,30 +1355,38 @@ std::shared_ptr<EigBatch> eig_batch_prepare(ptbgpu_ctx* c, int64_t n, const doub
     const EigProb* dp = eb->probs.as<EigProb>();
     int* dst = eb->status.as<int>();
 
-    k_eig_gather<<<np, kT, 0, s>>>(dp, d_maps, H, S, eb->Ca.as<double>(), eb->La.as<double>());
-    k_eig_potrf<<<np, kT, kSmemBlocked, s>>>(dp, eb->La.as<double>(), dst);
-    k_eig_reduce<<<np, kT, kSmemBlocked, s>>>(dp, eb->La.as<double>(), eb->Ca.as<double>(), dst);
-    k_eig_sytrd<<<np, kT, 0, s>>>(dp, eb->Ca.as<double>(), eb->Da.as<double>(), eb->Ea.as<double>(),
-                                  eb->Ta.as<double>(), dst);
-    k_eig_dc<<<np, kT, kDcSmem, s>>>(dp, eb->Da.as<double>(), eb->Ea.as<double>(), eb->Wa.as<double>(),
-                                     eb->Za.as<double>(), eb->Qa.as<double>(), eb->Va.as<double>(), dst);
-    count_launch(5);
-    PTB_CUDA(cudaGetLastError());
-    std::vector<int> hst(np);
-    PTB_CUDA(cudaMemcpyAsync(hst.data(), dst, sizeof(int) * np, cudaMemcpyDeviceToHost, s));
-    PTB_CUDA(cudaStreamSynchronize(s));
-    for (int q = 0; q < np; ++q)
-        PTB_CHECK(hst[q] <= 0, PTBGPU_ENOTSPD, "overlap submatrix %d not positive definite (leading minor %d)",
-                  eb->hp[q].k + 1, hst[q]);
-    for (int q = 0; q < np; ++q)
-        PTB_CHECK(hst[q] == kStOk, PTBGPU_EITER, "tridiagonal eigensolver did not converge on submatrix %d",
-                  eb->hp[q].k + 1);
-    k_eig_rows<<<np, kT, 0, s>>>(dp, eb->Ca.as<double>(), eb->La.as<double>(), eb->Ta.as<double>(),
-                                 eb->Wa.as<double>(), eb->Za.as<double>(), d_own_cols, d_ipos, eb->Ba.as<double>(),
-                                 d_e, d_fe, dst);
+    // largest first, so that the small submatrices fill in around the large ones
+    std::vector<int> ord(np);
+    for (int q = 0; q < np; ++q) ord[q] = q;
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return eb->hp[a].m > eb->hp[b].m; });
+    eb->order.reserve(sizeof(int) * np);
+    eb->counter.reserve(sizeof(int));
+    PTB_CUDA(cudaMemcpyAsync(eb->order.ptr, ord.data(), sizeof(int) * np, cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemsetAsync(eb->counter.ptr, 0, sizeof(int), s));
+    const int M = (eb->maxm + 1) & ~1;
+    const int grid = std::min(np, c->num_sms > 0 ? c->num_sms : 148);
+    k_eig_fused<<<grid, kT, stage_smem_bytes(M), s>>>(
+        dp, eb->order.as<int>(), np, eb->counter.as<int>(), M, d_maps, H, S, eb->Ca.as<double>(),
+        eb->La.as<double>(), eb->Za.as<double>(), eb->Qa.as<double>(), eb->Va.as<double>(), eb->Da.as<double>(),
+        eb->Ea.as<double>(), eb->Ta.as<double>(), eb->Wa.as<double>(), eb->Ba.as<double>(), d_own_cols, d_ipos, d_e,
+        d_fe, dst);
     count_launch();
     PTB_CUDA(cudaGetLastError());
     return eb;
+}
+
+void eig_batch_check(ptbgpu_ctx* c, EigBatch& eb) {
+    cudaStream_t s = c->stream;
+    const int np = eb.nprob;
+    std::vector<int> hst(np);
+    PTB_CUDA(cudaMemcpyAsync(hst.data(), eb.status.ptr, sizeof(int) * np, cudaMemcpyDeviceToHost, s));
+    PTB_CUDA(cudaStreamSynchronize(s));
+    for (int q = 0; q < np; ++q)
+        PTB_CHECK(hst[q] <= 0, PTBGPU_ENOTSPD, "overlap submatrix %d not positive definite (leading minor %d)",
+                  eb.hp[q].k + 1, hst[q]);
+    for (int q = 0; q < np; ++q)
+        PTB_CHECK(hst[q] == kStOk, PTBGPU_EITER, "tridiagonal eigensolver did not converge on submatrix %d",
+                  eb.hp[q].k + 1);
 }
 
 void eig_batch_final(ptbgpu_ctx* c, EigBatch& eb, double mu, int64_t n, const int* d_maps, const int* d_own_cols,
@@ -1382,8 +1459,9 @@ void sygv_batched_entry(ptbgpu_ctx* c, int64_t np, const int64_t* dims, const do
     PTB_CUDA(cudaMemcpyAsync(b.own.ptr, own.data(), sizeof(int) * osum, cudaMemcpyHostToDevice, st));
     PTB_CUDA(cudaMemcpyAsync(b.ipos.ptr, ipos.data(), sizeof(int) * nsum, cudaMemcpyHostToDevice, st));
     std::shared_ptr<EigBatch> eb =
-        eig_batch_prepare(c, 0, b.h.as<double>(), b.s.as<double>(), probs, b.maps.as<int>(), b.own.as<int>(),
-                          b.ipos.as<int>(), b.e.as<double>(), b.fe.as<double>(), 0, nullptr);
+        eig_batch_launch(c, 0, b.h.as<double>(), b.s.as<double>(), probs, b.maps.as<int>(), b.own.as<int>(),
+                         b.ipos.as<int>(), b.e.as<double>(), b.fe.as<double>(), 0, nullptr);
+    eig_batch_check(c, *eb);
     PTB_CUDA(cudaMemcpyAsync(e, b.e.ptr, sizeof(double) * nsum, cudaMemcpyDeviceToHost, st));
     PTB_CUDA(cudaMemcpyAsync(fe, b.fe.ptr, sizeof(double) * nsum, cudaMemcpyDeviceToHost, st));
     if (Pcols) {

@@ -26,14 +26,17 @@ struct EigProbHost {
 
 struct EigBatch;
 
-// Gather, Cholesky, reduction, tridiagonalisation, implicit QL, owned rows of
-// U and S U, and the (e, fe) pairs into d_e / d_fe at each problem's eoff.
-// Raises ENOTSPD (overlap block not positive definite) or EITER (QL did not
-// converge).  Returns null for an empty list.
-std::shared_ptr<EigBatch> eig_batch_prepare(ptbgpu_ctx* c, int64_t n, const double* H, const double* S,
-                                            const std::vector<EigProbHost>& probs, const int* d_maps,
-                                            const int* d_own_cols, const int* d_ipos, double* d_e, double* d_fe,
-                                            int prl, double* flops);
+// Launches (on the context's stream, no host synchronisation) the gather,
+// Cholesky, reduction, tridiagonalisation, divide and conquer, and the owned
+// rows of U and S U with the (e, fe) pairs into d_e / d_fe at each problem's
+// eoff.  Returns null for an empty list.  eig_batch_check waits for the stream
+// and raises ENOTSPD (an overlap block not positive definite) or EITER (a
+// leaf's QL iteration did not converge).
+std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const double* H, const double* S,
+                                           const std::vector<EigProbHost>& probs, const int* d_maps,
+                                           const int* d_own_cols, const int* d_ipos, double* d_e, double* d_fe,
+                                           int prl, double* flops);
+void eig_batch_check(ptbgpu_ctx* c, EigBatch& eb);
 
 // The owned columns of P_k = U occ U^T at mu for every prepared problem,
 // written into the packed result (rows map(i) <= c of column c), or with

@@ -912,17 +912,22 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
         const char* v = getenv("PTBGPU_SM_EIG");
         return v != nullptr && std::string(v) == "library";
     }();
+    // launched on the context's stream after the side streams' start event, so
+    // that it runs while the large submatrices are solved on the side streams
+    std::vector<EigProbHost> own_probs;
     if (!use_library && !small.empty()) {
-        std::vector<EigProbHost> eh;
-        eh.reserve(small.size());
+        own_probs.reserve(small.size());
         for (const Prob& p : small)
-            eh.push_back({p.k, p.m, (int)(pl.own_off[p.k + 1] - pl.own_off[p.k]), p.moff, p.eoff, pl.own_off[p.k]});
-        pl.eig = eig_batch_prepare(c, n, H, S, eh, d_maps, d_own_cols, d_ipos, be.as<double>(), bfe.as<double>(),
-                                   prl, &pl.flops);
-        mark("batched eigensolver");
-        log_line(prl, 2, " * submatrix batched eigensolver: %zu problems", small.size());
+            own_probs.push_back(
+                {p.k, p.m, (int)(pl.own_off[p.k + 1] - pl.own_off[p.k]), p.moff, p.eoff, pl.own_off[p.k]});
         small.clear();
     }
+    auto launch_own = [&] {
+        if (own_probs.empty() || pl.eig) return;
+        pl.eig = eig_batch_launch(c, n, H, S, own_probs, d_maps, d_own_cols, d_ipos, be.as<double>(),
+                                  bfe.as<double>(), prl, &pl.flops);
+        log_line(prl, 2, " * submatrix batched eigensolver: %zu problems launched", own_probs.size());
+    };
     DevBuf sb, ptrs, infos, ws, tbuf;
     cusolverDnParams_t params;
     PTB_CUSOLVER(cusolverDnCreateParams(&params));
@@ -1053,6 +1058,7 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
             PTB_CUDA(cudaMemsetAsync(infos.ptr, 0, sizeof(int) * large.size(), s));
             cudaEvent_t ready = c->take_event();
             PTB_CUDA(cudaEventRecord(ready, s));
+            launch_own();
             const int nw = (int)std::min<size_t>(SidePool::kStreams, large.size());
             std::atomic<size_t> next{0};
             std::vector<std::string> errs(nw);
@@ -1121,6 +1127,11 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
                 PTB_CHECK(hinfo[q] == 0, PTBGPU_ENOTSPD, "dsygvd failed on submatrix %d (info=%d)", large[q].k + 1,
                           hinfo[q]);
             mark("large eigensolves (side streams)");
+        }
+        launch_own();   // no large submatrices
+        if (pl.eig) {
+            eig_batch_check(c, *pl.eig);
+            mark("batched eigensolver");
         }
         PTB_CUDA(cudaStreamSynchronize(s));
     } catch (...) {

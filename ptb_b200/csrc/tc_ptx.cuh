@@ -105,7 +105,10 @@ __device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t adesc, 
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 // arrive on the mbarrier at this shared-memory offset in every CTA of `mask`
-// once the pair's prior tcgen05 operations have completed
+// once the pair's prior tcgen05 operations have completed.  The multicast
+// here is of the completion signal (an mbarrier arrive in the CTAs of this
+// GPU's own cluster), not of data: no load in this library, TMA or bulk, uses
+// cluster multicast, and every TMA source is this GPU's own memory.
 __device__ __forceinline__ void umma_commit_pair(uint32_t bar, uint16_t mask) {
     asm volatile(
         "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
