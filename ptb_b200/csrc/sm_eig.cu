@@ -414,8 +414,29 @@ __device__ void stage_sytrd(const EigProb& p, double* __restrict__ Ca, double* _
         }
         // columns in chunks of kSyChunk: every load of a chunk is issued before
         // its stores, so the pass streams instead of waiting on each element;
-        // threads without a row in the trailing block skip the pass
+        // threads without a row in the trailing block skip the pass, and while
+        // the block has at most kT rows each thread carries one row only
         const bool has_row = r0 + tid < m;
+        if (m - r0 <= kT) {
+            double* colbase = A + r0 + tid;
+            for (int k0 = has_row ? r0 : m; k0 < m; k0 += kSyChunk) {
+                double a1[kSyChunk];
+#pragma unroll
+                for (int u = 0; u < kSyChunk; ++u) {
+                    const int k = k0 + u;
+                    a1[u] = (k < m) ? colbase[(int64_t)k * m] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kSyChunk; ++u) {
+                    const int k = k0 + u;
+                    if (k < m) {
+                        const double x = a1[u] - (vr[0] * wc[k] + wr[0] * vc[k]);
+                        colbase[(int64_t)k * m] = x;
+                        acc[0] = fma(x, vn[k], acc[0]);
+                    }
+                }
+            }
+        } else
         for (int k0 = has_row ? r0 : m; k0 < m; k0 += kSyChunk) {
             double a[kSyChunk][kSyRows];
 #pragma unroll
