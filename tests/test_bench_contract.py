@@ -59,3 +59,14 @@ def test_timed_calls_stops_at_the_budget_or_the_steps():
     import time as _t
     times, _ = bench.timed_calls(lambda: _t.sleep(0.05), 10, lambda: None, 0, 0.12)
     assert 1 <= len(times) < 10
+
+
+def test_reference_arm_unavailable_where_the_oracle_does_not_fit():
+    """The 2048-H2O submatrix workload has no CPU restatement run (full 47104 x 47104
+    matrices): the arm prints one 'unavailable' line and exits 0 without building it."""
+    out = _run({}, "--workload", "sm_water2048", "--steps", "1", "--warmup", "0")
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and "host memory" in d["unavailable"]
