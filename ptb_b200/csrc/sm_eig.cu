@@ -9,7 +9,7 @@
 // them are reached without forming U:
 //
 //   S_k = L L^T                      Cholesky, blocked (k_eig_potrf)
-//   C   = L^-1 H_k L^-T              L^-1 by a blocked solve, then two tile GEMMs
+//   C   = L^-1 H_k L^-T              two blocked triangular solves
 //   C   = Q T Q^T                    Householder tridiagonalisation, lower,
 //                                    Q = H_0 H_1 ... H_{m-3} (k_eig_sytrd)
 //   T   = Z diag(e) Z^T              divide and conquer (k_eig_dc)
@@ -252,6 +252,64 @@ __device__ int stage_potrf(const EigProb& p, double* __restrict__ La, const Stag
     return 0;
 }
 
+// X <- L^-1 X (L lower, m x m; X m x m), blocked by 32 rows.
+__device__ void trsm_left_lower(const double* __restrict__ L, double* __restrict__ X, int m, double* sA, double* sB,
+                                double* sD) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i0 = 0; i0 < m; i0 += NB) {
+        const int nb = min(NB, m - i0), i1 = i0 + nb;
+        for (int t = tid; t < NB * NB; t += kT) {
+            const int i = t % NB, j = t / NB;
+            sD[i + j * (NB + 1)] = (i < nb && j < nb) ? L[(int64_t)(i0 + i) + (int64_t)(i0 + j) * m] : 0.0;
+        }
+        __syncthreads();
+        // diagonal block: warp per column of X, lanes over its rows
+        for (int j = warp; j < m; j += kT / 32) {
+            double x = (lane < nb) ? X[(int64_t)(i0 + lane) + (int64_t)j * m] : 0.0;
+            for (int k = 0; k < nb; ++k) {
+                if (lane == k) x /= sD[k + k * (NB + 1)];
+                const double xk = __shfl_sync(0xffffffffu, x, k);
+                if (lane > k && lane < nb) x -= sD[lane + k * (NB + 1)] * xk;
+            }
+            if (lane < nb) X[(int64_t)(i0 + lane) + (int64_t)j * m] = x;
+        }
+        __syncthreads();
+        for (int c0 = 0; c0 < m; c0 += TS)
+            for (int r0 = i1; r0 < m; r0 += TS)
+                tile_update<false, false>(X, m, r0, c0, min(TS, m - r0), min(TS, m - c0), L + (int64_t)i0 * m, m,
+                                          X + i0, m, nb, sA, sB);
+    }
+}
+
+// C <- L^-1 H_k L^-T: C <- L^-1 C, transpose, C <- L^-1 C, then the lower
+// triangle copied to the upper one (exactly symmetric).
+__device__ void stage_reduce(const EigProb& p, const double* __restrict__ La, double* __restrict__ Ca,
+                             const StageSmem& sh) {
+    double* sA = sh.sA;
+    double* sB = sh.sB;
+    double* sD = sh.sD;
+    const int m = p.m;
+    const double* L = La + p.aoff;
+    double* C = Ca + p.aoff;
+    trsm_left_lower(L, C, m, sA, sB, sD);
+    __syncthreads();
+    for (int64_t t = threadIdx.x; t < (int64_t)m * m; t += kT) {
+        const int i = (int)(t % m), j = (int)(t / m);
+        if (i > j) {
+            const double a = C[i + (int64_t)j * m], b = C[j + (int64_t)i * m];
+            C[i + (int64_t)j * m] = b;
+            C[j + (int64_t)i * m] = a;
+        }
+    }
+    __syncthreads();
+    trsm_left_lower(L, C, m, sA, sB, sD);
+    __syncthreads();
+    for (int64_t t = threadIdx.x; t < (int64_t)m * m; t += kT) {
+        const int i = (int)(t % m), j = (int)(t / m);
+        if (i > j) C[j + (int64_t)i * m] = C[i + (int64_t)j * m];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Householder tridiagonalisation of C (lower).  Iteration j applies the
 // previous reflector's rank-2 update to column j, forms reflector j from it
@@ -453,51 +511,62 @@ __device__ void tile_gemm(double* __restrict__ C, int64_t ldc, int crow, const i
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 2; ++b) acc[a][b] = 0.0;
+    // K chunks double-buffered through registers: the next chunk's loads are in
+    // flight while the current one is multiplied out of shared memory
+    constexpr int kPer = TS * NB / kT;   // staged elements of A (and of B) per thread
+    double ra[kPer], rb[kPer];
+    auto fetch = [&](int k0) {
+        const int kk = min(NB, K - k0);
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int t = tid + q * kT;
+            int i, k;
+            if (AT) {
+                k = t % NB;
+                i = t / NB;
+            } else {
+                i = t % TS;
+                k = t / TS;
+            }
+            double v = 0.0;
+            if (i < mr && k < kk) {
+                const int64_t kg = kx ? kx[k0 + k] : (k0 + k);
+                v = AT ? A[kg + (int64_t)(r0 + i) * lda] : A[(int64_t)(r0 + i) + kg * lda];
+            }
+            ra[q] = v;
+            int j, kb;
+            if (BT) {
+                j = t % TS;
+                kb = t / TS;
+            } else {
+                kb = t % NB;
+                j = t / NB;
+            }
+            double w = 0.0;
+            if (j < nc && kb < kk) {
+                const int64_t kg = kxb ? kxb[k0 + kb] : (k0 + kb);
+                w = BT ? B[(int64_t)(c0 + j) + kg * ldb] : B[kg + (int64_t)(c0 + j) * ldb];
+            }
+            rb[q] = w;
+        }
+    };
+    auto stash = [&]() {
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int t = tid + q * kT;
+            const int i = AT ? t / NB : t % TS, k = AT ? t % NB : t / TS;
+            sA[k * (TS + 1) + i] = ra[q];
+            const int j = BT ? t % TS : t / NB, kb = BT ? t / TS : t % NB;
+            sB[kb * (TS + 1) + j] = rb[q];
+        }
+    };
+    fetch(0);
+    stash();
+    __syncthreads();
     for (int k0 = 0; k0 < K; k0 += NB) {
         const int kk = min(NB, K - k0);
-        if (AT) {
-            for (int t = tid; t < TS * NB; t += kT) {
-                const int k = t % NB, i = t / NB;
-                double v = 0.0;
-                if (i < mr && k < kk) {
-                    const int64_t kg = kx ? kx[k0 + k] : (k0 + k);
-                    v = A[kg + (int64_t)(r0 + i) * lda];
-                }
-                sA[k * (TS + 1) + i] = v;
-            }
-        } else {
-            for (int t = tid; t < TS * NB; t += kT) {
-                const int i = t % TS, k = t / TS;
-                double v = 0.0;
-                if (i < mr && k < kk) {
-                    const int64_t kg = kx ? kx[k0 + k] : (k0 + k);
-                    v = A[(int64_t)(r0 + i) + kg * lda];
-                }
-                sA[k * (TS + 1) + i] = v;
-            }
-        }
-        if (BT) {
-            for (int t = tid; t < TS * NB; t += kT) {
-                const int j = t % TS, k = t / TS;
-                double v = 0.0;
-                if (j < nc && k < kk) {
-                    const int64_t kg = kxb ? kxb[k0 + k] : (k0 + k);
-                    v = B[(int64_t)(c0 + j) + kg * ldb];
-                }
-                sB[k * (TS + 1) + j] = v;
-            }
-        } else {
-            for (int t = tid; t < TS * NB; t += kT) {
-                const int k = t % NB, j = t / NB;
-                double v = 0.0;
-                if (j < nc && k < kk) {
-                    const int64_t kg = kxb ? kxb[k0 + k] : (k0 + k);
-                    v = B[kg + (int64_t)(c0 + j) * ldb];
-                }
-                sB[k * (TS + 1) + j] = v;
-            }
-        }
-        __syncthreads();
+        const bool more = k0 + NB < K;
+        if (more) fetch(k0 + NB);
         for (int k = 0; k < kk; ++k) {
             double av[4], bv[2];
 #pragma unroll
@@ -510,6 +579,10 @@ __device__ void tile_gemm(double* __restrict__ C, int64_t ldc, int crow, const i
                 for (int b = 0; b < 2; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
         }
         __syncthreads();
+        if (more) {
+            stash();
+            __syncthreads();
+        }
     }
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
@@ -521,67 +594,6 @@ __device__ void tile_gemm(double* __restrict__ C, int64_t ldc, int crow, const i
             const int i = tx + 16 * a;
             if (i < mr) C[(int64_t)(crow + r0 + i) + col * ldc] = acc[a][b];
         }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// C <- L^-1 H_k L^-T.  X = L^-1 by a blocked solve of L X = I (X lower
-// triangular: block row I only has columns < its end, so the updates skip the
-// zero columns), then W = X H and the lower tiles of C = X W^T as tile GEMMs
-// over the nonzero K range of X (each output accumulated in registers and
-// written once), then the lower triangle copied to the upper one (exactly
-// symmetric).  X and W live in the Z and Q arenas, free at this stage.
-__device__ void stage_reduce(const EigProb& p, const double* __restrict__ La, double* __restrict__ Ca,
-                             double* __restrict__ Xa, double* __restrict__ Wa2, const StageSmem& sh) {
-    double* sA = sh.sA;
-    double* sB = sh.sB;
-    double* sD = sh.sD;
-    const int m = p.m;
-    const double* L = La + p.aoff;
-    double* C = Ca + p.aoff;
-    double* X = Xa + p.aoff;
-    double* W = Wa2 + p.aoff;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int64_t t = tid; t < (int64_t)m * m; t += kT) X[t] = ((t % m) == (t / m)) ? 1.0 : 0.0;
-    __syncthreads();
-    for (int i0 = 0; i0 < m; i0 += NB) {
-        const int nb = min(NB, m - i0), i1 = i0 + nb;
-        for (int t = tid; t < NB * NB; t += kT) {
-            const int i = t % NB, j = t / NB;
-            sD[i + j * (NB + 1)] = (i < nb && j < nb) ? L[(int64_t)(i0 + i) + (int64_t)(i0 + j) * m] : 0.0;
-        }
-        __syncthreads();
-        for (int j = warp; j < i1; j += kT / 32) {
-            double x = (lane < nb) ? X[(int64_t)(i0 + lane) + (int64_t)j * m] : 0.0;
-            for (int k = 0; k < nb; ++k) {
-                if (lane == k) x /= sD[k + k * (NB + 1)];
-                const double xk = __shfl_sync(0xffffffffu, x, k);
-                if (lane > k && lane < nb) x -= sD[lane + k * (NB + 1)] * xk;
-            }
-            if (lane < nb) X[(int64_t)(i0 + lane) + (int64_t)j * m] = x;
-        }
-        __syncthreads();
-        for (int c0 = 0; c0 < i1; c0 += TS)
-            for (int r0 = i1; r0 < m; r0 += TS)
-                tile_update<false, false>(X, m, r0, c0, min(TS, m - r0), min(TS, i1 - c0), L + (int64_t)i0 * m, m,
-                                          X + i0, m, nb, sA, sB);
-    }
-    __syncthreads();
-    // W = X H (X(i, k) = 0 for k > i)
-    for (int r0 = 0; r0 < m; r0 += TS)
-        for (int c0 = 0; c0 < m; c0 += TS)
-            tile_gemm<false>(W, m, 0, nullptr, r0, c0, min(TS, m - r0), min(TS, m - c0), X, m, nullptr, C, m,
-                             nullptr, min(m, r0 + TS), sA, sB);
-    __syncthreads();
-    // lower tiles of C = X W^T
-    for (int r0 = 0; r0 < m; r0 += TS)
-        for (int c0 = 0; c0 <= r0; c0 += TS)
-            tile_gemm<false, true>(C, m, 0, nullptr, r0, c0, min(TS, m - r0), min(TS, m - c0), X, m, nullptr, W, m,
-                                   nullptr, min(m, r0 + TS), sA, sB);
-    __syncthreads();
-    for (int64_t t = tid; t < (int64_t)m * m; t += kT) {
-        const int i = (int)(t % m), j = (int)(t / m);
-        if (i > j) C[j + (int64_t)i * m] = C[i + (int64_t)j * m];
     }
 }
 
@@ -1038,6 +1050,7 @@ struct WySmem {
     double* Xs;  // NB x kWyChunk: V^T x, then T(^T) V^T x
 };
 constexpr int kWyChunk = 64;
+static_assert(TS * NB % kT == 0, "tile staging divides over the CTA");
 static_assert(NB * (NB + 1) <= NB * (TS + 1) && NB * kWyChunk <= NB * (TS + 1), "WY scratch fits the tile staging");
 
 __device__ __forceinline__ double wy_v(const double* C, int m, int j, int r) {
@@ -1243,7 +1256,7 @@ __global__ void __launch_bounds__(kT, 1) k_eig_fused(
         int st = stage_potrf(p, La, sh);
         __syncthreads();
         if (st == kStOk) {
-            stage_reduce(p, La, Ca, Za, Qa, sh);
+            stage_reduce(p, La, Ca, sh);
             __syncthreads();
             stage_sytrd(p, Ca, Da, Ea, Ta, sh);
             __syncthreads();
