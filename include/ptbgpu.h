@@ -337,10 +337,11 @@ int ptbgpu_oz_gemm(ptbgpu_ctx* ctx, int64_t n, int64_t slices, int64_t kblock, i
                    int64_t tri_b, int64_t symmetric, const double* A, const double* B, double* C, double* ms);
 
 /* The batched FP64 generalized eigensolver of the submatrix method on dense
- * host problems (kernel-level entry for tests and measurements; it replaces,
- * for submatrices of order <= 1024, the per-submatrix la_sygvd and the S_k U
- * product of source/sm.f90:296-310).  nprob problems of orders dims[k]
- * (1..1024): H and S hold their column-major dims[k]^2 blocks one after
+ * host problems (kernel-level entry for tests and measurements; it replaces the
+ * per-submatrix la_sygvd and the S_k U product of source/sm.f90:296-310).
+ * Orders up to 1024 run one CTA per problem in a persistent launch, larger ones
+ * one thread-block cluster per problem.  nprob problems of orders dims[k]
+ * (1..10240): H and S hold their column-major dims[k]^2 blocks one after
  * another; owned holds nown[k] (0-based, local) owned indices per problem, one
  * list after another.  Out: e and fe (sum of dims each, per problem in the
  * solver's order, not sorted): the eigenvalues of H c = e S c and the weights

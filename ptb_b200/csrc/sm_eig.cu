@@ -20,13 +20,18 @@
 //
 // Each step's quantities are summed in a fixed order, so results do not depend
 // on scheduling.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "sm_eig.cuh"
 
 namespace ptb {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -48,77 +53,151 @@ struct EigProb {
     int64_t aoff;     // C, L, Z and merge-workspace arenas (m x m, column-major, ld = m)
     int64_t voff;     // d, e, tau, eigenvalue arenas (m)
     int64_t boff;     // owned-row arena (4 nown x m)
+    int64_t xoff;     // cluster solver scratch (orders above kEigBatchMax)
 };
 
 // ---------------------------------------------------------------------------
+// Tile products on the FP64 tensor cores: one TS x TS output tile per CTA, the
+// K range staged through shared memory in NB-deep chunks (the next chunk's
+// loads in flight in registers while the current one is multiplied), each of
+// the 16 warps owning a 16 x 16 block of the tile as 2 x 2 fragments of
+// mma.m8n8k4.f64 (A fragment: lane holds A[g][t4]; B fragment: B[t4][g];
+// accumulator: C[g][2 t4 + h], g = lane / 4, t4 = lane % 4).
+//   A(i, k) = AT ? A[kg + (r0+i) lda] : A[(r0+i) + kg lda],   kg = kx ? kx[k] : k
+//   B(k, j) = BT ? B[(c0+j) + kg ldb] : B[kg + (c0+j) ldb],   kg = kxb ? kxb[k] : k
+//   MMA_SET: C[crow + r0 + i, col] = sum_k A(i,k) B(k,j); MMA_SUB: C[...] -= sum;
+//   col = ccol ? ccol[c0+j] : c0+j; LOWER: only r0+i >= c0+j is written.
+// Staged layouts keep both the stores (contiguous global runs) and the
+// fragment reads free of bank conflicts: the operand whose global run is along
+// the tile edge is stored k-major with row stride 68, the other edge-major with
+// stride 36 (both = 4 mod 16 doubles).
+constexpr int kStageOp = 2304;   // doubles of one staged operand chunk (max of 32 x 68 and 64 x 36)
+enum { MMA_SET = 0, MMA_SUB = 1 };
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+template <bool AT>
+__device__ __forceinline__ int sa_idx(int i, int k) {
+    return AT ? i * 36 + k : k * 68 + i;
+}
+template <bool BT>
+__device__ __forceinline__ int sb_idx(int k, int j) {
+    return BT ? k * 68 + j : j * 36 + k;
+}
+
+template <bool AT, bool BT, int MODE, bool LOWER>
+__device__ void tile_mma(double* __restrict__ C, int64_t ldc, int crow, const int* ccol, int r0, int c0, int mr,
+                         int nc, const double* __restrict__ A, int64_t lda, const int* kx,
+                         const double* __restrict__ B, int64_t ldb, const int* kxb, int K, double* sA, double* sB) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int wr = (warp & 3) * 16, wc = (warp >> 2) * 16;
+    double acc[2][2][2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    constexpr int kPer = TS * NB / kT;   // staged elements of A (and of B) per thread
+    double ra[kPer], rb[kPer];
+    auto fetch = [&](int k0) {
+        const int kk = min(NB, K - k0);
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int t = tid + q * kT;
+            const int i = AT ? t / NB : t % TS, k = AT ? t % NB : t / TS;
+            double v = 0.0;
+            if (i < mr && k < kk) {
+                const int64_t kg = kx ? kx[k0 + k] : (k0 + k);
+                v = AT ? A[kg + (int64_t)(r0 + i) * lda] : A[(int64_t)(r0 + i) + kg * lda];
+            }
+            ra[q] = v;
+            const int j = BT ? t % TS : t / NB, kb = BT ? t / TS : t % NB;
+            double w = 0.0;
+            if (j < nc && kb < kk) {
+                const int64_t kg = kxb ? kxb[k0 + kb] : (k0 + kb);
+                w = BT ? B[(int64_t)(c0 + j) + kg * ldb] : B[kg + (int64_t)(c0 + j) * ldb];
+            }
+            rb[q] = w;
+        }
+    };
+    auto stash = [&]() {
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int t = tid + q * kT;
+            const int i = AT ? t / NB : t % TS, k = AT ? t % NB : t / TS;
+            sA[sa_idx<AT>(i, k)] = ra[q];
+            const int j = BT ? t % TS : t / NB, kb = BT ? t / TS : t % NB;
+            sB[sb_idx<BT>(kb, j)] = rb[q];
+        }
+    };
+    fetch(0);
+    stash();
+    __syncthreads();
+    for (int k0 = 0; k0 < K; k0 += NB) {
+        const bool more = k0 + NB < K;
+        if (more) fetch(k0 + NB);
+        const int ksteps = (min(NB, K - k0) + 3) >> 2;
+        for (int ks = 0; ks < ksteps; ++ks) {
+            const int k = ks * 4 + t4;
+            const double a0 = sA[sa_idx<AT>(wr + g, k)], a1 = sA[sa_idx<AT>(wr + 8 + g, k)];
+            const double b0 = sB[sb_idx<BT>(k, wc + g)], b1 = sB[sb_idx<BT>(k, wc + 8 + g)];
+            dmma(acc[0][0][0], acc[0][0][1], a0, b0);
+            dmma(acc[0][1][0], acc[0][1][1], a0, b1);
+            dmma(acc[1][0][0], acc[1][0][1], a1, b0);
+            dmma(acc[1][1][0], acc[1][1][1], a1, b1);
+        }
+        __syncthreads();
+        if (more) {
+            stash();
+            __syncthreads();
+        }
+    }
+    // accumulator acc[a][b][h] is C(wr + 8a + g, wc + 8b + 2 t4 + h); for a
+    // read-modify-write every load is issued before any store
+    double cv[2][2][2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = wr + 8 * a + g, j = wc + 8 * b + 2 * t4 + h;
+                const bool ok = i < mr && j < nc && !(LOWER && r0 + i < c0 + j);
+                cv[a][b][h] = 0.0;
+                if (MODE == MMA_SUB && ok) {
+                    const int64_t col = ccol ? ccol[c0 + j] : (c0 + j);
+                    cv[a][b][h] = C[(int64_t)(crow + r0 + i) + col * ldc];
+                }
+            }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = wr + 8 * a + g, j = wc + 8 * b + 2 * t4 + h;
+                const bool ok = i < mr && j < nc && !(LOWER && r0 + i < c0 + j);
+                if (ok) {
+                    const int64_t col = ccol ? ccol[c0 + j] : (c0 + j);
+                    C[(int64_t)(crow + r0 + i) + col * ldc] =
+                        (MODE == MMA_SUB) ? cv[a][b][h] - acc[a][b][h] : acc[a][b][h];
+                }
+            }
+    __syncthreads();
+}
+
 // C[r0+i, c0+j] -= sum_{k < kk} A(i,k) B(k,j) on one TS x TS tile (mr x nc
-// valid), 512 threads with 4 x 2 outputs each.
-//   A(i,k) = A[(r0+i) + k lda]
-//   B(k,j) = BT ? B[(c0+j) + k ldb] : B[k + (c0+j) ldb]
+// valid):  A(i,k) = A[(r0+i) + k lda],  B(k,j) = BT ? B[(c0+j) + k ldb] : B[k + (c0+j) ldb].
 // LOWER: only elements on or below the diagonal of C are written.
 template <bool BT, bool LOWER>
 __device__ void tile_update(double* __restrict__ C, int ldc, int r0, int c0, int mr, int nc,
                             const double* __restrict__ A, int lda, const double* __restrict__ B, int ldb, int kk,
                             double* sA, double* sB) {
-    const int tid = threadIdx.x;
-    for (int t = tid; t < TS * NB; t += kT) {
-        const int i = t % TS, k = t / TS;
-        sA[k * (TS + 1) + i] = (i < mr && k < kk) ? A[(int64_t)(r0 + i) + (int64_t)k * lda] : 0.0;
-    }
-    if (BT) {
-        for (int t = tid; t < TS * NB; t += kT) {
-            const int j = t % TS, k = t / TS;
-            sB[k * (TS + 1) + j] = (j < nc && k < kk) ? B[(int64_t)(c0 + j) + (int64_t)k * ldb] : 0.0;
-        }
-    } else {
-        for (int t = tid; t < TS * NB; t += kT) {
-            const int k = t % NB, j = t / NB;
-            sB[k * (TS + 1) + j] = (j < nc && k < kk) ? B[(int64_t)k + (int64_t)(c0 + j) * ldb] : 0.0;
-        }
-    }
-    __syncthreads();
-    const int tx = tid & 15, ty = tid >> 4;   // 16 x 32 threads, 4 x 2 outputs each
-    double acc[4][2];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) acc[a][b] = 0.0;
-    for (int k = 0; k < kk; ++k) {
-        double av[4], bv[2];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) av[a] = sA[k * (TS + 1) + tx + 16 * a];
-#pragma unroll
-        for (int b = 0; b < 2; ++b) bv[b] = sB[k * (TS + 1) + ty + 32 * b];
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
-    }
-    // read-modify-write of the C tile: all loads issued before any store (the
-    // stores could alias later loads as far as the compiler knows, which would
-    // otherwise serialise the round trips to memory)
-    double cv[4][2];
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-        const int j = ty + 32 * b;
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int i = tx + 16 * a;
-            const bool ok = j < nc && i < mr && !(LOWER && r0 + i < c0 + j);
-            cv[a][b] = ok ? C[(int64_t)(r0 + i) + (int64_t)(c0 + j) * ldc] : 0.0;
-        }
-    }
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-        const int j = ty + 32 * b;
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int i = tx + 16 * a;
-            const bool ok = j < nc && i < mr && !(LOWER && r0 + i < c0 + j);
-            if (ok) C[(int64_t)(r0 + i) + (int64_t)(c0 + j) * ldc] = cv[a][b] - acc[a][b];
-        }
-    }
-    __syncthreads();
+    tile_mma<false, BT, MMA_SUB, LOWER>(C, ldc, 0, nullptr, r0, c0, mr, nc, A, lda, nullptr, B, ldb, nullptr, kk,
+                                        sA, sB);
 }
 
 // Fixed-order sum over the CTA (every thread gets the result).
@@ -495,106 +574,13 @@ __device__ void stage_sytrd(const EigProb& p, double* __restrict__ Ca, double* _
 }
 
 // ---------------------------------------------------------------------------
-// C[ro(i), co(j)] = sum_k A(i, kx(k)) B(k, j) on one TS x TS output tile, the
-// K range in NB chunks, 256 threads with 4 x 4 outputs each:
-//   A(i, k) = AT ? A[k + (r0+i) lda] : A[(r0+i) + k lda]
-//   B(k, j) = BT ? B[(c0+j) + kxb(k) ldb] : B[kxb(k) + (c0+j) ldb]
-//   kx, kxb: optional K index maps (shared memory), crow: output row offset,
-//   ccol: optional output column map (shared memory) else c0 + j.
+// C[crow + r0 + i, col(c0 + j)] = sum_k A(i, kx(k)) B(kxb(k), j) on one TS x TS
+// output tile (tile_mma, MMA_SET).
 template <bool AT, bool BT = false>
 __device__ void tile_gemm(double* __restrict__ C, int64_t ldc, int crow, const int* ccol, int r0, int c0, int mr,
                           int nc, const double* __restrict__ A, int64_t lda, const int* kx,
                           const double* __restrict__ B, int64_t ldb, const int* kxb, int K, double* sA, double* sB) {
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;   // 16 x 32 threads, 4 x 2 outputs each
-    double acc[4][2];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) acc[a][b] = 0.0;
-    // K chunks double-buffered through registers: the next chunk's loads are in
-    // flight while the current one is multiplied out of shared memory
-    constexpr int kPer = TS * NB / kT;   // staged elements of A (and of B) per thread
-    double ra[kPer], rb[kPer];
-    auto fetch = [&](int k0) {
-        const int kk = min(NB, K - k0);
-#pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            const int t = tid + q * kT;
-            int i, k;
-            if (AT) {
-                k = t % NB;
-                i = t / NB;
-            } else {
-                i = t % TS;
-                k = t / TS;
-            }
-            double v = 0.0;
-            if (i < mr && k < kk) {
-                const int64_t kg = kx ? kx[k0 + k] : (k0 + k);
-                v = AT ? A[kg + (int64_t)(r0 + i) * lda] : A[(int64_t)(r0 + i) + kg * lda];
-            }
-            ra[q] = v;
-            int j, kb;
-            if (BT) {
-                j = t % TS;
-                kb = t / TS;
-            } else {
-                kb = t % NB;
-                j = t / NB;
-            }
-            double w = 0.0;
-            if (j < nc && kb < kk) {
-                const int64_t kg = kxb ? kxb[k0 + kb] : (k0 + kb);
-                w = BT ? B[(int64_t)(c0 + j) + kg * ldb] : B[kg + (int64_t)(c0 + j) * ldb];
-            }
-            rb[q] = w;
-        }
-    };
-    auto stash = [&]() {
-#pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            const int t = tid + q * kT;
-            const int i = AT ? t / NB : t % TS, k = AT ? t % NB : t / TS;
-            sA[k * (TS + 1) + i] = ra[q];
-            const int j = BT ? t % TS : t / NB, kb = BT ? t / TS : t % NB;
-            sB[kb * (TS + 1) + j] = rb[q];
-        }
-    };
-    fetch(0);
-    stash();
-    __syncthreads();
-    for (int k0 = 0; k0 < K; k0 += NB) {
-        const int kk = min(NB, K - k0);
-        const bool more = k0 + NB < K;
-        if (more) fetch(k0 + NB);
-        for (int k = 0; k < kk; ++k) {
-            double av[4], bv[2];
-#pragma unroll
-            for (int a = 0; a < 4; ++a) av[a] = sA[k * (TS + 1) + tx + 16 * a];
-#pragma unroll
-            for (int b = 0; b < 2; ++b) bv[b] = sB[k * (TS + 1) + ty + 32 * b];
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 2; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
-        }
-        __syncthreads();
-        if (more) {
-            stash();
-            __syncthreads();
-        }
-    }
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-        const int j = ty + 32 * b;
-        if (j >= nc) continue;
-        const int64_t col = ccol ? ccol[c0 + j] : (c0 + j);
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int i = tx + 16 * a;
-            if (i < mr) C[(int64_t)(crow + r0 + i) + col * ldc] = acc[a][b];
-        }
-    }
+    tile_mma<AT, BT, MMA_SET, false>(C, ldc, crow, ccol, r0, c0, mr, nc, A, lda, kx, B, ldb, kxb, K, sA, sB);
 }
 
 // ---------------------------------------------------------------------------
@@ -1051,7 +1037,7 @@ struct WySmem {
 };
 constexpr int kWyChunk = 64;
 static_assert(TS * NB % kT == 0, "tile staging divides over the CTA");
-static_assert(NB * (NB + 1) <= NB * (TS + 1) && NB * kWyChunk <= NB * (TS + 1), "WY scratch fits the tile staging");
+static_assert(NB * (NB + 1) <= kStageOp && NB * kWyChunk <= kStageOp, "WY scratch fits the tile staging");
 
 __device__ __forceinline__ double wy_v(const double* C, int m, int j, int r) {
     return (r == j + 1) ? 1.0 : (r > j + 1 ? C[r + (int64_t)j * m] : 0.0);
@@ -1139,6 +1125,142 @@ __device__ void wy_apply(const double* __restrict__ C, int m, const double* __re
 }
 
 // ---------------------------------------------------------------------------
+constexpr int kWyMmaMin = 160;   // orders from which the reflectors are applied as tile products
+
+// Q = H_0 ... H_{m-3} applied to nv vectors (X, ld m) on the FP64 tensor
+// cores, a panel of NB reflectors at a time as I - V T V^T: Vp = the panel's
+// reflectors written out (rows j0+1.., unit and zeros in place), its Gram
+// matrix by one tile product, T from the Gram as in wy_apply, then
+// Y = V^T X, Y2 = T^T Y (trans) or T Y, X -= V Y2 as tile products.  Vp
+// (m x NB) and Y (2 NB x nv + NB x NB) are global scratch, T is NB x (NB+1)
+// shared.
+__device__ void wy_apply_mma(const double* __restrict__ C, int m, const double* __restrict__ tau, double* X, int nv,
+                             bool trans, double* Vp, double* Y, double* T, double* sA, double* sB) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nref = m - 2;
+    if (nref <= 0 || nv <= 0) return;
+    const int npan = (nref + NB - 1) / NB;
+    double* Gg = Y + (int64_t)NB * nv;
+    double* Y2 = Gg + NB * NB;
+    for (int pp = 0; pp < npan; ++pp) {
+        const int pan = trans ? pp : npan - 1 - pp;
+        const int j0 = pan * NB, nb = min(NB, nref - j0);
+        const int r0 = j0 + 1, len = m - r0;
+        for (int64_t q = tid; q < (int64_t)len * NB; q += kT) {
+            const int i = (int)(q % len), a = (int)(q / len);
+            Vp[q] = (a < nb) ? wy_v(C, m, j0 + a, r0 + i) : 0.0;
+        }
+        __syncthreads();
+        tile_mma<true, false, MMA_SET, false>(Gg, NB, 0, nullptr, 0, 0, NB, NB, Vp, len, nullptr, Vp, len, nullptr, len,
+                                              sA, sB);
+        for (int q = tid; q < NB * NB; q += kT) {
+            const int a = q % NB, b = q / NB;
+            T[a + b * (NB + 1)] = (a <= b && a < nb && b < nb) ? Gg[a + b * NB] : 0.0;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            for (int b = 0; b < nb; ++b) {
+                const double tb = tau[j0 + b];
+                double acc = 0.0;
+                if (lane < b)
+                    for (int c2 = lane; c2 < b; ++c2) acc = fma(T[lane + c2 * (NB + 1)], T[c2 + b * (NB + 1)], acc);
+                __syncwarp();
+                if (lane < b) T[lane + b * (NB + 1)] = -tb * acc;
+                if (lane == b) T[b + b * (NB + 1)] = tb;
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int c0 = 0; c0 < nv; c0 += TS)
+            tile_mma<true, false, MMA_SET, false>(Y, NB, 0, nullptr, 0, c0, NB, min(TS, nv - c0), Vp, len, nullptr,
+                                                  X + r0, m, nullptr, len, sA, sB);
+        for (int64_t q = tid; q < (int64_t)NB * nv; q += kT) {
+            const int a = (int)(q % NB), t = (int)(q / NB);
+            const double* yc = Y + (int64_t)t * NB;
+            double y = 0.0;
+            if (trans) {
+                for (int c2 = 0; c2 <= a; ++c2) y = fma(T[c2 + a * (NB + 1)], yc[c2], y);
+            } else {
+                for (int c2 = a; c2 < NB; ++c2) y = fma(T[a + c2 * (NB + 1)], yc[c2], y);
+            }
+            Y2[q] = y;
+        }
+        __syncthreads();
+        for (int c0 = 0; c0 < nv; c0 += TS)
+            for (int i0 = 0; i0 < len; i0 += TS)
+                tile_mma<false, false, MMA_SUB, false>(X + r0, m, 0, nullptr, i0, c0, min(TS, len - i0),
+                                                       min(TS, nv - c0), Vp, len, nullptr, Y2, NB, nullptr, nb, sA, sB);
+    }
+}
+
+// X <- L^-1 X (lower = true) or X <- L^-T X (lower = false) for the columns
+// [c_begin, c_end) of X (ld ldx), L lower (ld m): over 64-row blocks (from the
+// top, or from the bottom for L^-T), the earlier blocks' contribution as one
+// tile product per 64-column block, then the diagonal block's substitution
+// (warp per column, two rows per lane).  One CTA; sD holds TS x (TS+1).
+__device__ void trsm_cols(bool lower, const double* __restrict__ L, int m, double* X, int64_t ldx, int c_begin,
+                          int c_end, double* sD, double* sA, double* sB) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nrb = (m + TS - 1) / TS;
+    for (int c0 = c_begin; c0 < c_end; c0 += TS) {
+        const int nc = min(TS, c_end - c0);
+        for (int q = 0; q < nrb; ++q) {
+            const int rb = lower ? q : nrb - 1 - q;
+            const int i0 = rb * TS, mr = min(TS, m - i0), i1 = i0 + mr;
+            if (lower) {
+                if (i0 > 0)
+                    tile_mma<false, false, MMA_SUB, false>(X, ldx, 0, nullptr, i0, c0, mr, nc, L, m, nullptr, X, ldx,
+                                                           nullptr, i0, sA, sB);
+            } else if (i1 < m) {
+                // (L^T)[i, k] = L[k, i] for k >= i1
+                tile_mma<true, false, MMA_SUB, false>(X, ldx, 0, nullptr, i0, c0, mr, nc, L + i1, m, nullptr, X + i1,
+                                                      ldx, nullptr, m - i1, sA, sB);
+            }
+            for (int t = tid; t < TS * TS; t += kT) {
+                const int i = t % TS, j = t / TS;
+                sD[i + j * (TS + 1)] = (i < mr && j < mr && i >= j) ? L[(int64_t)(i0 + i) + (int64_t)(i0 + j) * m] : 0.0;
+            }
+            __syncthreads();
+            for (int jc = warp; jc < nc; jc += kT / 32) {
+                double* x = X + (int64_t)(c0 + jc) * ldx + i0;
+                double x0 = lane < mr ? x[lane] : 0.0, x1 = lane + 32 < mr ? x[lane + 32] : 0.0;
+                if (lower) {
+                    for (int k = 0; k < mr; ++k) {
+                        double xk;
+                        if (k < 32) {
+                            if (lane == k) x0 /= sD[k + k * (TS + 1)];
+                            xk = __shfl_sync(0xffffffffu, x0, k);
+                        } else {
+                            if (lane == k - 32) x1 /= sD[k + k * (TS + 1)];
+                            xk = __shfl_sync(0xffffffffu, x1, k - 32);
+                        }
+                        if (lane > k && lane < mr) x0 -= sD[lane + k * (TS + 1)] * xk;
+                        if (lane + 32 > k && lane + 32 < mr) x1 -= sD[lane + 32 + k * (TS + 1)] * xk;
+                    }
+                } else {
+                    // L_bb^T x = b: back substitution, (L^T)[i, k] = sD[k + i (TS+1)] for k > i
+                    for (int k = mr - 1; k >= 0; --k) {
+                        double xk;
+                        if (k < 32) {
+                            if (lane == k) x0 /= sD[k + k * (TS + 1)];
+                            xk = __shfl_sync(0xffffffffu, x0, k);
+                        } else {
+                            if (lane == k - 32) x1 /= sD[k + k * (TS + 1)];
+                            xk = __shfl_sync(0xffffffffu, x1, k - 32);
+                        }
+                        if (lane < k) x0 -= sD[k + lane * (TS + 1)] * xk;
+                        if (lane + 32 < k) x1 -= sD[k + (lane + 32) * (TS + 1)] * xk;
+                    }
+                }
+                if (lane < mr) x[lane] = x0;
+                if (lane + 32 < mr) x[lane + 32] = x1;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Owned rows of S U and U, fe and the eigenpairs.  R holds 2 nown rows of
 // length m (row-major, i.e. the column-major m x 2nown matrix R^T): rows
 // t < nown are L[c_t,:] -> (S U)[c_t,:], rows nown + t are (L^-T)[c_t,:] ->
@@ -1146,8 +1268,9 @@ __device__ void wy_apply(const double* __restrict__ C, int m, const double* __re
 __device__ void stage_rows(const EigProb& p, const double* __restrict__ Ca, const double* __restrict__ La,
                            const double* __restrict__ Ta, const double* __restrict__ Wa,
                            const double* __restrict__ Za, const int* __restrict__ own_cols,
-                           const int* __restrict__ ipos, double* __restrict__ Ba, double* __restrict__ e_out,
-                           double* __restrict__ fe_out, const StageSmem& sh) {
+                           const int* __restrict__ ipos, double* __restrict__ Ba, double* __restrict__ Qa,
+                           double* __restrict__ Va, double* __restrict__ e_out, double* __restrict__ fe_out,
+                           const StageSmem& sh) {
     double* sA = sh.sA;
     double* sB = sh.sB;
     const int m = p.m, no = p.nown, nb2 = 2 * no;
@@ -1167,31 +1290,39 @@ __device__ void stage_rows(const EigProb& p, const double* __restrict__ Ca, cons
         }
     }
     __syncthreads();
-    // rows of L^-T: x_t = L^-1 e_{c_t}, 32-row blocks
-    for (int i0 = 0; i0 < m; i0 += NB) {
-        const int nb = min(NB, m - i0), i1 = i0 + nb;
-        for (int t = warp; t < no; t += nwarp) {
-            double* x = R2 + (int64_t)t * m;
-            double xv = (lane < nb) ? x[i0 + lane] : 0.0;
-            for (int k = 0; k < nb; ++k) {
-                if (lane == k) xv /= L[(i0 + k) + (int64_t)(i0 + k) * m];
-                const double xk = __shfl_sync(0xffffffffu, xv, k);
-                if (lane > k && lane < nb) xv -= L[(i0 + lane) + (int64_t)(i0 + k) * m] * xk;
+    // rows of L^-T: x_t = L^-1 e_{c_t}; blocked on the tensor cores when the
+    // divide and conquer's (now free) arrays hold a 64 x 65 diagonal block
+    if (dc_smem_bytes(sh.M) >= sizeof(double) * TS * (TS + 1)) {
+        trsm_cols(true, L, m, R2, m, 0, no, reinterpret_cast<double*>(sh.uni), sA, sB);
+    } else {
+        for (int i0 = 0; i0 < m; i0 += NB) {
+            const int nb = min(NB, m - i0), i1 = i0 + nb;
+            for (int t = warp; t < no; t += nwarp) {
+                double* x = R2 + (int64_t)t * m;
+                double xv = (lane < nb) ? x[i0 + lane] : 0.0;
+                for (int k = 0; k < nb; ++k) {
+                    if (lane == k) xv /= L[(i0 + k) + (int64_t)(i0 + k) * m];
+                    const double xk = __shfl_sync(0xffffffffu, xv, k);
+                    if (lane > k && lane < nb) xv -= L[(i0 + lane) + (int64_t)(i0 + k) * m] * xk;
+                }
+                if (lane < nb) x[i0 + lane] = xv;
             }
-            if (lane < nb) x[i0 + lane] = xv;
+            __syncthreads();
+            for (int64_t q = tid; q < (int64_t)no * (m - i1); q += kT) {
+                const int t = (int)(q / (m - i1)), r = i1 + (int)(q % (m - i1));
+                double* x = R2 + (int64_t)t * m;
+                double s = 0.0;
+                for (int k = 0; k < nb; ++k) s = fma(L[r + (int64_t)(i0 + k) * m], x[i0 + k], s);
+                x[r] -= s;
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        for (int64_t q = tid; q < (int64_t)no * (m - i1); q += kT) {
-            const int t = (int)(q / (m - i1)), r = i1 + (int)(q % (m - i1));
-            double* x = R2 + (int64_t)t * m;
-            double s = 0.0;
-            for (int k = 0; k < nb; ++k) s = fma(L[r + (int64_t)(i0 + k) * m], x[i0 + k], s);
-            x[r] -= s;
-        }
-        __syncthreads();
     }
-    // R <- R Q: each row x becomes Q^T x (the tiles' staging space as scratch)
-    wy_apply(C, m, tau, R, nb2, true, WySmem{sA, sB});
+    // R <- R Q: each row x becomes Q^T x (from order 160 on the tensor cores, the
+    // divide and conquer's Q and V arenas as scratch)
+    if (m >= kWyMmaMin) wy_apply_mma(C, m, tau, R, nb2, true, Qa + p.aoff, Va + p.aoff, sh.sD, sA, sB);
+    else wy_apply(C, m, tau, R, nb2, true, WySmem{sA, sB});
+    __syncthreads();
     // G^T = Z^T R^T (m x 2nown, column-major = G row-major)
     for (int c0 = 0; c0 < nb2; c0 += TS)
         for (int r0 = 0; r0 < m; r0 += TS)
@@ -1215,7 +1346,7 @@ __device__ void stage_rows(const EigProb& p, const double* __restrict__ Ca, cons
 // launch per stage or per size bucket.  status[pi]: 0, the order of a
 // non-positive pivot of S_k, or kStNoConv.
 __host__ __device__ constexpr size_t stage_smem_bytes(int M) {
-    return sizeof(double) * (2 * NB * (TS + 1) + NB * (NB + 1)) + dc_smem_bytes(M) + sizeof(int) * 16 +
+    return sizeof(double) * (2 * kStageOp + NB * (NB + 1)) + dc_smem_bytes(M) + sizeof(int) * 16 +
            sizeof(double) * (2 + kT / 32) + 16;
 }
 
@@ -1223,9 +1354,9 @@ __device__ StageSmem stage_smem(unsigned char* base, int M) {
     StageSmem sh;
     double* d = reinterpret_cast<double*>(base);
     sh.sA = d;
-    sh.sB = d + NB * (TS + 1);
-    sh.sD = d + 2 * NB * (TS + 1);
-    sh.uni = reinterpret_cast<unsigned char*>(d + 2 * NB * (TS + 1) + NB * (NB + 1));
+    sh.sB = d + kStageOp;
+    sh.sD = d + 2 * kStageOp;
+    sh.uni = reinterpret_cast<unsigned char*>(d + 2 * kStageOp + NB * (NB + 1));
     sh.ints = reinterpret_cast<int*>(sh.uni + dc_smem_bytes(M));
     sh.dsc = reinterpret_cast<double*>(sh.ints + 16);
     sh.M = M;
@@ -1262,7 +1393,7 @@ __global__ void __launch_bounds__(kT, 1) k_eig_fused(
             __syncthreads();
             if (!stage_dc(p, Da, Ea, Wa, Za, Qa, Va, sh)) st = kStNoConv;
             __syncthreads();
-            if (st == kStOk) stage_rows(p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, e_out, fe_out, sh);
+            if (st == kStOk) stage_rows(p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, Qa, Va, e_out, fe_out, sh);
         }
         if (tid == 0) status[pi] = st;
         __syncthreads();
@@ -1273,14 +1404,24 @@ __global__ void __launch_bounds__(kT, 1) k_eig_fused(
 // Owned columns of P_k at mu: w_t = occ o U[c_t,:]^T, w <- Z w, w <- Q w
 // (reflectors in reverse), w <- L^-T w; scattered into the packed result,
 // rows map(i) <= c_t of column c_t (or written dense).
-__global__ void __launch_bounds__(kT) k_eig_final(const EigProb* __restrict__ probs, const double* __restrict__ Ca,
+// Shared memory of the final-column kernels: tile staging, a 64 x 65 diagonal
+// block of L and the panel's T.
+constexpr size_t kFinalSmem = sizeof(double) * (2 * kStageOp + TS * (TS + 1) + NB * (NB + 1));
+
+__global__ void __launch_bounds__(kT) k_eig_final(const EigProb* __restrict__ probs, const int* __restrict__ order,
+                                                  const double* __restrict__ Ca,
                                                   const double* __restrict__ La, const double* __restrict__ Ta,
                                                   const double* __restrict__ Wa, const double* __restrict__ Za,
+                                                  double* __restrict__ Qa, double* __restrict__ Va,
                                                   const int* __restrict__ maps, const int* __restrict__ own_cols,
                                                   double* __restrict__ Ba, double mu, double* __restrict__ Ppk,
                                                   double* __restrict__ Pdense) {
-    __shared__ double sA[NB * (TS + 1)], sB[NB * (TS + 1)];
-    const EigProb p = probs[blockIdx.x];
+    extern __shared__ __align__(16) unsigned char smf[];
+    double* sA = reinterpret_cast<double*>(smf);
+    double* sB = sA + kStageOp;
+    double* sD = sB + kStageOp;
+    double* sT = sD + TS * (TS + 1);
+    const EigProb p = probs[order[blockIdx.x]];
     const int m = p.m, no = p.nown;
     const double* C = Ca + p.aoff;
     const double* L = La + p.aoff;
@@ -1290,7 +1431,7 @@ __global__ void __launch_bounds__(kT) k_eig_final(const EigProb* __restrict__ pr
     double* W0 = Ba + p.boff;                       // (S U) rows block: free after the prepare step
     const double* U2 = Ba + p.boff + 3 * (int64_t)no * m;   // U[c_t, :] (second half of G)
     double* W = Ba + p.boff + (int64_t)no * m;      // m x nown, column-major
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = kT / 32;
+    const int tid = threadIdx.x;
     for (int64_t q = tid; q < (int64_t)no * m; q += kT) {
         const int j = (int)(q % m);
         const double e = ev[j];
@@ -1304,21 +1445,12 @@ __global__ void __launch_bounds__(kT) k_eig_final(const EigProb* __restrict__ pr
             tile_gemm<false>(W, m, 0, nullptr, r0, c0, min(TS, m - r0), min(TS, no - c0), Z, m, nullptr, W0, m, nullptr, m,
                              sA, sB);
     __syncthreads();
-    // Q W (the tiles' staging space as scratch)
-    wy_apply(C, m, tau, W, no, false, WySmem{sA, sB});
-    // L^-T w: back substitution, warp per column
-    for (int t = warp; t < no; t += nwarp) {
-        double* w = W + (int64_t)t * m;
-        for (int i = m - 1; i >= 0; --i) {
-            const double* li = L + (int64_t)i * m;
-            double s = 0.0;
-            for (int k = i + 1 + lane; k < m; k += 32) s = fma(li[k], w[k], s);
-            s = warp_sum(s);
-            if (lane == 0) w[i] = (w[i] - s) / li[i];
-            __syncwarp();
-        }
-    }
+    // Q W (from order 160 as tile products, the divide and conquer's arenas as scratch)
+    if (m >= kWyMmaMin) wy_apply_mma(C, m, tau, W, no, false, Qa + p.aoff, Va + p.aoff, sT, sA, sB);
+    else wy_apply(C, m, tau, W, no, false, WySmem{sA, sB});
     __syncthreads();
+    // L^-T W: blocked back substitution
+    trsm_cols(false, L, m, W, m, 0, no, sD, sA, sB);
     if (Pdense) {
         for (int64_t q = tid; q < (int64_t)no * m; q += kT) Pdense[p.poff + q] = W[q];
         return;
@@ -1332,16 +1464,1029 @@ __global__ void __launch_bounds__(kT) k_eig_final(const EigProb* __restrict__ pr
     }
 }
 
+
+// ===========================================================================
+// Submatrices above kEigBatchMax (the k-means columns of large boxes): the
+// same stages on a thread-block cluster of G CTAs per submatrix, one cluster
+// barrier (barrier.cluster) between dependent steps and every intermediate in
+// global memory (L2-resident for the vectors and panels).
+//   gather       columns split over the CTAs
+//   Cholesky     32-wide panels: the diagonal block factored by every CTA (same
+//                data, same arithmetic, same result), panel rows and lower
+//                trailing tiles split over the CTAs
+//   reduction    C = L^-1 H L^-T: left-looking triangular solves over 64-row
+//                blocks, each CTA owning 64-column blocks of C (no barrier
+//                inside a solve)
+//   tridiag.     blocked Householder with lazy updates (LAPACK's latrd
+//                scheme): per column the panel's earlier reflectors update that
+//                column, the reflector is formed, and y = A v runs over the
+//                lower 64 x 64 tiles of the not yet updated trailing block (each
+//                tile read once for both its row and its column contribution),
+//                corrected by V (W^T v) + W (V^T v); w = tau (y - tau/2 (y.v) v);
+//                after 32 columns the trailing block gets A -= V W^T + W V^T.
+//                Rows are owned in 32-row chunks, partial sums go through
+//                per-CTA slots summed in CTA order, so results do not depend on
+//                scheduling.  Two cluster barriers per column.
+//   D&C          leaves and the lower merges one CTA each, merges with fewer
+//                problems than CTAs by the whole cluster
+//   owned rows   vectors split over the CTAs, then one tiled product with Z
+// ===========================================================================
+constexpr int kLargeMax = kEigLargeMax;   // largest order the cluster solver takes (its vectors live in shared memory)
+constexpr int kRedW = 2 * NB + 4;         // per-CTA partial sums of the tridiagonalisation
+constexpr int kRedVAv = 2 * NB + 1;       // slot of the partial v^T A v
+constexpr int kSyB = 4;                   // trailing tiles per round of the tridiagonalisation's A v
+static_assert(kSyB * (kT / 32 + 1) * TS <= 2 * kStageOp, "A v round buffers fit the tile staging");
+constexpr int kLgStages = 6;              // stage timestamps per problem: start, Cholesky, reduction, tridiag., D&C, rows
+
+struct Grp {
+    int rank, size;
+    __device__ __forceinline__ void sync() const { cg::this_cluster().sync(); }
+};
+
+// Per-problem scratch of a cluster solve (offsets in doubles from p.xoff).
+struct LgLayout {
+    int64_t ypart, red, V, W, dc, scal, total;
+};
+__host__ __device__ inline LgLayout lg_layout(int m, int G) {
+    LgLayout L;
+    int64_t o = 0;
+    L.ypart = o;
+    o += (int64_t)G * m;
+    L.red = o;
+    o += (int64_t)G * kRedW;
+    L.V = o;
+    o += (int64_t)m * NB;
+    L.W = o;
+    o += (int64_t)m * NB;
+    o = (o + 1) & ~int64_t(1);
+    L.dc = o;
+    o += (int64_t)((dc_smem_bytes((m + 1) & ~1) + 15) / 16) * 2;
+    L.scal = o;
+    o += ((int64_t)m + 64) / 2 + 2;   // 8 ints per merge of the widest level (at most m / 16 merges)
+    L.total = (o + 1) & ~int64_t(1);
+    return L;
+}
+
+struct LgSmem {
+    double *sA, *sB;           // tile staging
+    double* sD;                // diagonal blocks (TS x (TS+1)), union with the vectors below
+    double *v, *y;             // tridiagonalisation: reflector and partial product (M each)
+    double *rowbuf, *colbuf;   // 16 x TS row partials, TS column sums of one tile
+    double *pw, *pv, *wtv, *vtv, *wj, *vj;   // NB each
+    double* red;               // kT / 32 + 2
+    double* dsc;               // scalars
+    int* ints;                 // 16
+};
+__host__ __device__ constexpr size_t lg_union_doubles(int M) {
+    return (size_t)2 * M + 16 * TS + TS + 6 * NB + kT / 32 + 2 + 8 > (size_t)TS * (TS + 1)
+               ? (size_t)2 * M + 16 * TS + TS + 6 * NB + kT / 32 + 2 + 8
+               : (size_t)TS * (TS + 1);
+}
+__host__ __device__ constexpr size_t lg_smem_bytes(int M) {
+    return sizeof(double) * (2 * kStageOp + lg_union_doubles(M)) + sizeof(int) * 16;
+}
+__device__ LgSmem lg_smem(unsigned char* base, int M) {
+    LgSmem s;
+    double* d = reinterpret_cast<double*>(base);
+    s.sA = d;
+    s.sB = d + kStageOp;
+    double* u = d + 2 * kStageOp;
+    s.sD = u;
+    s.v = u;
+    s.y = u + M;
+    s.rowbuf = s.y + M;
+    s.colbuf = s.rowbuf + 16 * TS;
+    s.pw = s.colbuf + TS;
+    s.pv = s.pw + NB;
+    s.wtv = s.pv + NB;
+    s.vtv = s.wtv + NB;
+    s.wj = s.vtv + NB;
+    s.vj = s.wj + NB;
+    s.red = s.vj + NB;
+    s.dsc = s.red + kT / 32 + 2;
+    s.ints = reinterpret_cast<int*>(u + lg_union_doubles(M));
+    return s;
+}
+
+// Lower-triangle tile index -> (row block, column block), rb >= cb.
+__device__ __forceinline__ void tri_decode(int64_t idx, int& rb, int& cb) {
+    int r = (int)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+    while ((int64_t)(r + 1) * (r + 2) / 2 <= idx) ++r;
+    while ((int64_t)r * (r + 1) / 2 > idx) --r;
+    rb = r;
+    cb = (int)(idx - (int64_t)r * (r + 1) / 2);
+}
+
+__device__ void lg_gather(const Grp& g, const EigProb& p, const int* __restrict__ maps, const double* __restrict__ H,
+                          const double* __restrict__ S, double* __restrict__ Ca, double* __restrict__ La) {
+    const int m = p.m;
+    const int* mp = maps + p.moff;
+    double* C = Ca + p.aoff;
+    double* L = La + p.aoff;
+    for (int j = g.rank; j < m; j += g.size) {
+        const int64_t gj = p.gbase + (int64_t)mp[j] * p.gld;
+        for (int i = threadIdx.x; i < m; i += kT) {
+            const int64_t q = (int64_t)mp[i] + gj;
+            C[i + (int64_t)j * m] = H[q];
+            L[i + (int64_t)j * m] = S[q];
+        }
+    }
+}
+
+// S_k = L L^T (lower) on the cluster; returns the order of the first
+// non-positive pivot (0: positive definite), the same on every CTA.
+__device__ int lg_potrf(const Grp& g, int m, double* __restrict__ L, const LgSmem& sh) {
+    double* sD = sh.sD;   // sD[i + j*(NB+1)]
+    int& fail = sh.ints[0];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) fail = 0;
+    __syncthreads();
+    for (int kb = 0; kb < m; kb += NB) {
+        const int nb = min(NB, m - kb);
+        for (int t = tid; t < NB * NB; t += kT) {
+            const int i = t % NB, j = t / NB;
+            sD[i + j * (NB + 1)] = (i < nb && j < nb) ? L[(int64_t)(kb + i) + (int64_t)(kb + j) * m] : 0.0;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            for (int jj = 0; jj < nb; ++jj) {
+                if (lane == jj) {
+                    const double piv = sD[jj + jj * (NB + 1)];
+                    if (!(piv > 0.0)) fail = kb + jj + 1;
+                    else sD[jj + jj * (NB + 1)] = sqrt(piv);
+                }
+                __syncwarp();
+                if (fail) break;
+                const double djj = sD[jj + jj * (NB + 1)];
+                if (lane > jj && lane < nb) sD[lane + jj * (NB + 1)] /= djj;
+                __syncwarp();
+                if (lane > jj && lane < nb) {
+                    const double lij = sD[lane + jj * (NB + 1)];
+                    for (int k = jj + 1; k <= lane; ++k) sD[lane + k * (NB + 1)] -= lij * sD[k + jj * (NB + 1)];
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        if (fail) break;   // every CTA factored the same block: the same decision everywhere
+        if (g.rank == 0)
+            for (int t = tid; t < nb * nb; t += kT) {
+                const int i = t % nb, j = t / nb;
+                if (i >= j) L[(int64_t)(kb + i) + (int64_t)(kb + j) * m] = sD[i + j * (NB + 1)];
+            }
+        for (int r = kb + nb + g.rank * kT + tid; r < m; r += g.size * kT) {
+            double x[NB];
+#pragma unroll
+            for (int j = 0; j < NB; ++j) x[j] = (j < nb) ? L[(int64_t)r + (int64_t)(kb + j) * m] : 0.0;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                if (j < nb) {
+                    double v = x[j];
+                    for (int k = 0; k < j; ++k) v -= x[k] * sD[j + k * (NB + 1)];
+                    x[j] = v / sD[j + j * (NB + 1)];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < nb) L[(int64_t)r + (int64_t)(kb + j) * m] = x[j];
+        }
+        g.sync();
+        const int t0 = kb + nb;
+        const int nt = (m - t0 + TS - 1) / TS;
+        const int64_t ntile = (int64_t)nt * (nt + 1) / 2;
+        for (int64_t idx = g.rank; idx < ntile; idx += g.size) {
+            int rb, cb;
+            tri_decode(idx, rb, cb);
+            const int r0 = t0 + rb * TS, c0 = t0 + cb * TS;
+            tile_update<true, true>(L, m, r0, c0, min(TS, m - r0), min(TS, m - c0), L + (int64_t)kb * m, m,
+                                    L + (int64_t)kb * m, m, nb, sh.sA, sh.sB);
+        }
+        g.sync();
+    }
+    __syncthreads();
+    const int f = fail;
+    __syncthreads();
+    if (f) return f;
+    for (int j = 1 + g.rank; j < m; j += g.size)
+        for (int i = tid; i < j; i += kT) L[(int64_t)i + (int64_t)j * m] = 0.0;
+    return 0;
+}
+
+// X <- L^-1 X for the 64-column blocks cb = rank, rank + G, ... of X (m x m):
+// left-looking over 64-row blocks, X_i -= L[i, <i] X[<i] as one tile product,
+// then the diagonal block's forward substitution (warp per column, two rows per
+// lane).  The column blocks are independent, so no cluster barrier is needed.
+__device__ void lg_trsm_cols(const Grp& g, const double* __restrict__ L, double* X, int m, const LgSmem& sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* sD = sh.sD;   // sD[i + j*(TS+1)]
+    const int ncb = (m + TS - 1) / TS;
+    for (int cb = g.rank; cb < ncb; cb += g.size) {
+        const int c0 = cb * TS, nc = min(TS, m - c0);
+        for (int i0 = 0; i0 < m; i0 += TS) {
+            const int mr = min(TS, m - i0);
+            if (i0 > 0)
+                tile_mma<false, false, MMA_SUB, false>(X, m, 0, nullptr, i0, c0, mr, nc, L, m, nullptr, X, m, nullptr,
+                                                       i0, sh.sA, sh.sB);
+            for (int t = tid; t < TS * TS; t += kT) {
+                const int i = t % TS, j = t / TS;
+                sD[i + j * (TS + 1)] = (i < mr && j < mr && i >= j) ? L[(int64_t)(i0 + i) + (int64_t)(i0 + j) * m] : 0.0;
+            }
+            __syncthreads();
+            for (int jc = warp; jc < nc; jc += kT / 32) {
+                double* x = X + (int64_t)(c0 + jc) * m + i0;
+                double x0 = lane < mr ? x[lane] : 0.0, x1 = lane + 32 < mr ? x[lane + 32] : 0.0;
+                for (int k = 0; k < mr; ++k) {
+                    double xk;
+                    if (k < 32) {
+                        if (lane == k) x0 /= sD[k + k * (TS + 1)];
+                        xk = __shfl_sync(0xffffffffu, x0, k);
+                    } else {
+                        if (lane == k - 32) x1 /= sD[k + k * (TS + 1)];
+                        xk = __shfl_sync(0xffffffffu, x1, k - 32);
+                    }
+                    if (lane > k && lane < mr) x0 -= sD[lane + k * (TS + 1)] * xk;
+                    if (lane + 32 > k && lane + 32 < mr) x1 -= sD[lane + 32 + k * (TS + 1)] * xk;
+                }
+                if (lane < mr) x[lane] = x0;
+                if (lane + 32 < mr) x[lane + 32] = x1;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// C <- L^-1 H_k L^-T: C <- L^-1 C, transpose, C <- L^-1 C (only the lower
+// triangle is read afterwards).
+__device__ void lg_reduce(const Grp& g, const EigProb& p, const double* __restrict__ La, double* Ca,
+                          const LgSmem& sh) {
+    const int m = p.m;
+    const double* L = La + p.aoff;
+    double* C = Ca + p.aoff;
+    lg_trsm_cols(g, L, C, m, sh);
+    g.sync();
+    const int64_t mm = (int64_t)m * m;
+    for (int64_t t = (int64_t)g.rank * kT + threadIdx.x; t < mm; t += (int64_t)g.size * kT) {
+        const int i = (int)(t % m), j = (int)(t / m);
+        if (i > j) {
+            const double a = C[i + (int64_t)j * m], b = C[j + (int64_t)i * m];
+            C[i + (int64_t)j * m] = b;
+            C[j + (int64_t)i * m] = a;
+        }
+    }
+    g.sync();
+    lg_trsm_cols(g, L, C, m, sh);
+    g.sync();
+}
+
+// w of reflector jp (column j - 1 of the panel's first column j0 = j - 1 - jp)
+// on this CTA's rows r >= j, from the summed partial products; the reflector
+// itself goes into column j - 1 below its leading 1.  Returns w at row j
+// (every CTA computes it).
+__device__ double lg_finish_w(const Grp& g, int m, int j, int jp, double* __restrict__ A, double* __restrict__ V,
+                              double* __restrict__ W, const double* __restrict__ yp, const double* __restrict__ red,
+                              const LgSmem& sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double tp = sh.dsc[0];
+    double vAv = 0.0;
+    for (int q = 0; q < g.size; ++q) vAv += red[q * kRedW + kRedVAv];
+    double vw = 0.0;
+    for (int q = 0; q < jp; ++q) vw = fma(sh.vtv[q], sh.wtv[q], vw);
+    const double ytv = vAv - 2.0 * vw;
+    const double hc = 0.5 * tp * ytv;
+    auto w_at = [&](int r) {
+        double y = 0.0;
+        for (int q = 0; q < g.size; ++q) y += yp[(int64_t)q * m + r];
+        for (int q = 0; q < jp; ++q) y -= V[r + (int64_t)q * m] * sh.wtv[q] + W[r + (int64_t)q * m] * sh.vtv[q];
+        return tp * (y - hc * sh.v[r]);
+    };
+    for (int ch = g.rank + g.size * warp; ch * 32 < m; ch += g.size * (kT / 32)) {
+        const int r = ch * 32 + lane;
+        if (r >= j && r < m) {
+            W[r + (int64_t)jp * m] = w_at(r);
+            if (r >= j + 1) A[r + (int64_t)(j - 1) * m] = sh.v[r];
+        }
+    }
+    if (j < m) {
+        if (tid == 0) sh.dsc[2] = w_at(j);
+    }
+    __syncthreads();
+    const double wr = sh.dsc[2];
+    __syncthreads();
+    return wr;
+}
+
+__device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca, double* __restrict__ Da,
+                         double* __restrict__ Ea, double* __restrict__ Ta, double* __restrict__ X, const LgSmem& sh) {
+    const int m = p.m, G = g.size, rk = g.rank;
+    double* A = Ca + p.aoff;
+    double* d = Da + p.voff;
+    double* e = Ea + p.voff;
+    double* tau = Ta + p.voff;
+    const LgLayout lay = lg_layout(m, G);
+    double* yp = X + lay.ypart;
+    double* red = X + lay.red;
+    double* V = X + lay.V;
+    double* W = X + lay.W;
+    double* v = sh.v;
+    double* yl = sh.y;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nT = (m + TS - 1) / TS;
+    for (int j0 = 0; j0 < m - 1; j0 += NB) {
+        const int nb = min(NB, m - 1 - j0);
+        for (int jj = 0; jj < nb; ++jj) {
+            const int j = j0 + jj;
+            // ---- phase A: finish w of the previous column, update column j on own rows
+            double wrow = 0.0;
+            if (jj > 0) wrow = lg_finish_w(g, m, j, jj - 1, A, V, W, yp, red, sh);
+            if (tid < jj) {
+                const int q = tid;
+                sh.wj[q] = (q == jj - 1) ? wrow : W[j + (int64_t)q * m];
+                sh.vj[q] = V[j + (int64_t)q * m];
+            }
+            __syncthreads();
+            for (int ch = rk + G * warp; ch * 32 < m; ch += G * (kT / 32)) {
+                const int r = ch * 32 + lane;
+                if (r >= j && r < m) {
+                    double a = A[r + (int64_t)j * m];
+                    for (int q = 0; q < jj; ++q)
+                        a -= V[r + (int64_t)q * m] * sh.wj[q] + W[r + (int64_t)q * m] * sh.vj[q];
+                    A[r + (int64_t)j * m] = a;
+                    yl[r] = a;
+                }
+            }
+            __syncthreads();
+            {
+                double part = 0.0;
+                for (int ch = rk + G * warp; ch * 32 < m; ch += G * (kT / 32)) {
+                    const int r = ch * 32 + lane;
+                    if (r >= j + 2 && r < m) part = fma(yl[r], yl[r], part);
+                }
+                part = cta_sum(part, sh.red);
+                if (tid == 0) red[rk * kRedW + 0] = part;
+            }
+            for (int q = warp; q < 2 * jj; q += kT / 32) {
+                const double* col = (q < jj) ? W + (int64_t)q * m : V + (int64_t)(q - jj) * m;
+                double part = 0.0;
+                for (int ch = rk; ch * 32 < m; ch += G) {
+                    const int r = ch * 32 + lane;
+                    if (r >= j + 2 && r < m) part = fma(col[r], yl[r], part);
+                }
+                part = warp_sum(part);
+                if (lane == 0) red[rk * kRedW + ((q < jj) ? 1 + q : 1 + NB + (q - jj))] = part;
+            }
+            g.sync();
+            // ---- phase B: reflector, then y = A v over the trailing lower tiles
+            if (tid < jj) {
+                double a = 0.0, b = 0.0;
+                for (int q = 0; q < G; ++q) {
+                    a += red[q * kRedW + 1 + tid];
+                    b += red[q * kRedW + 1 + NB + tid];
+                }
+                sh.pw[tid] = a;
+                sh.pv[tid] = b;
+            }
+            if (tid == 32) {
+                double xn2 = 0.0;
+                for (int q = 0; q < G; ++q) xn2 += red[q * kRedW + 0];
+                const double alpha = A[(j + 1) + (int64_t)j * m];
+                const double dj = A[j + (int64_t)j * m];
+                double t, beta;
+                if (xn2 == 0.0) {
+                    t = 0.0;
+                    beta = alpha;
+                } else {
+                    beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+                    t = (beta - alpha) / beta;
+                }
+                sh.dsc[0] = t;
+                sh.dsc[1] = (t == 0.0) ? 0.0 : 1.0 / (alpha - beta);
+                if (rk == 0) {
+                    d[j] = dj;
+                    e[j] = beta;
+                    tau[j] = t;
+                }
+            }
+            __syncthreads();
+            const double sc = sh.dsc[1];
+            for (int r = tid; r < m; r += kT) {
+                double vr;
+                if (r <= j) vr = 0.0;
+                else if (r == j + 1) vr = 1.0;
+                else vr = (sc == 0.0) ? 0.0 : A[r + (int64_t)j * m] * sc;
+                v[r] = vr;
+            }
+            if (tid < jj) {
+                sh.wtv[tid] = W[(j + 1) + (int64_t)tid * m] + sc * sh.pw[tid];
+                sh.vtv[tid] = V[(j + 1) + (int64_t)tid * m] + sc * sh.pv[tid];
+            }
+            const int s = j + 1;
+            for (int r = s + tid; r < m; r += kT) yl[r] = 0.0;
+            __syncthreads();
+            for (int ch = rk + G * warp; ch * 32 < m; ch += G * (kT / 32)) {
+                const int r = ch * 32 + lane;
+                if (r >= s && r < m) V[r + (int64_t)jj * m] = v[r];
+            }
+            const int I0 = s / TS, nbt = nT - I0;
+            const int64_t ntiles = (int64_t)nbt * (nbt + 1) / 2;
+            // kSyB tiles per round: every load of the round is issued before any
+            // arithmetic, then one barrier; the per-tile row and column sums are
+            // added by 64 threads, thread t only ever touching positions = t mod 64
+            // (tile origins are multiples of 64), in tile order: no two threads
+            // write one position and the sums do not depend on scheduling
+            double* rowbuf = sh.sA;                        // [kSyB][16][TS], in the tile staging
+            double* colbuf = sh.sA + kSyB * (kT / 32) * TS;   // [kSyB][TS]
+            for (int64_t base = rk; base < ntiles; base += (int64_t)G * kSyB) {
+                double a0[kSyB][4], a1[kSyB][4];
+                int rbs[kSyB], cbs[kSyB];
+#pragma unroll
+                for (int b = 0; b < kSyB; ++b) {
+                    const int64_t idx = base + (int64_t)b * G;
+                    int I = -1, J = -1;
+                    if (idx < ntiles) {
+                        int bi, bj;
+                        tri_decode(idx, bi, bj);
+                        I = I0 + bi;
+                        J = I0 + bj;
+                    }
+                    rbs[b] = I * TS;
+                    cbs[b] = J * TS;
+                    const bool diag = (I == J);
+                    const int ra = I * TS + lane, rb = ra + 32;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int c = J * TS + warp * 4 + u;
+                        a0[b][u] = 0.0;
+                        a1[b][u] = 0.0;
+                        if (I >= 0 && c < m && c >= s) {
+                            if (ra < m && (!diag || ra >= c)) a0[b][u] = A[ra + (int64_t)c * m];
+                            if (rb < m && (!diag || rb >= c)) a1[b][u] = A[rb + (int64_t)c * m];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < kSyB; ++b) {
+                    if (rbs[b] < 0) continue;
+                    const bool diag = rbs[b] == cbs[b];
+                    const int ra = rbs[b] + lane, rb = ra + 32;
+                    const double va = (ra < m) ? v[ra] : 0.0, vb = (rb < m) ? v[rb] : 0.0;
+                    double rp0 = 0.0, rp1 = 0.0;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int c = cbs[b] + warp * 4 + u;
+                        const double vc = (c < m) ? v[c] : 0.0;
+                        rp0 = fma(a0[b][u], vc, rp0);
+                        rp1 = fma(a1[b][u], vc, rp1);
+                        double cp = ((diag && ra == c) ? 0.0 : a0[b][u] * va) + ((diag && rb == c) ? 0.0 : a1[b][u] * vb);
+                        cp = warp_sum(cp);
+                        if (lane == 0) colbuf[b * TS + warp * 4 + u] = cp;
+                    }
+                    rowbuf[(b * (kT / 32) + warp) * TS + lane] = rp0;
+                    rowbuf[(b * (kT / 32) + warp) * TS + lane + 32] = rp1;
+                }
+                __syncthreads();
+                if (tid < TS) {
+                    for (int b = 0; b < kSyB; ++b) {
+                        if (rbs[b] < 0) break;
+                        double acc = 0.0;
+                        for (int w2 = 0; w2 < kT / 32; ++w2) acc += rowbuf[(b * (kT / 32) + w2) * TS + tid];
+                        const bool diag = rbs[b] == cbs[b];
+                        if (diag) acc += colbuf[b * TS + tid];
+                        const int r = rbs[b] + tid;
+                        if (r >= s && r < m) yl[r] += acc;
+                        if (!diag) {
+                            const int c = cbs[b] + tid;
+                            if (c >= s && c < m) yl[c] += colbuf[b * TS + tid];
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            {
+                double part = 0.0;
+                for (int r = s + tid; r < m; r += kT) part = fma(v[r], yl[r], part);
+                part = cta_sum(part, sh.red);
+                if (tid == 0) red[rk * kRedW + kRedVAv] = part;
+            }
+            for (int r = s + tid; r < m; r += kT) yp[(int64_t)rk * m + r] = yl[r];
+            g.sync();
+        }
+        // ---- panel end: w of the last column, then the trailing block
+        const int j1 = j0 + nb;
+        lg_finish_w(g, m, j1, nb - 1, A, V, W, yp, red, sh);
+        g.sync();
+        if (j1 < m) {
+            const int nt = (m - j1 + TS - 1) / TS;
+            const int64_t ntile = (int64_t)nt * (nt + 1) / 2;
+            for (int64_t idx = rk; idx < ntile; idx += G) {
+                int rb, cb;
+                tri_decode(idx, rb, cb);
+                const int r0 = j1 + rb * TS, c0 = j1 + cb * TS;
+                const int mr = min(TS, m - r0), nc = min(TS, m - c0);
+                tile_update<true, true>(A, m, r0, c0, mr, nc, V, m, W, m, nb, sh.sA, sh.sB);
+                tile_update<true, true>(A, m, r0, c0, mr, nc, W, m, V, m, nb, sh.sA, sh.sB);
+            }
+        }
+        g.sync();
+    }
+    if (rk == 0 && tid == 0) {
+        d[m - 1] = A[(m - 1) + (int64_t)(m - 1) * m];
+        tau[m - 1] = 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Divide and conquer on a cluster.  A merge is run by one CTA (Split{0, 1,
+// false}) or by the whole cluster (Split{rank, G, true}); its per-element
+// arrays sit at offset lo of the problem's arrays, its Q and V blocks at
+// column lo of the Q and V arenas, so merges of one level never overlap.
+struct Split {
+    int part, nparts;
+    bool coop;
+    __device__ __forceinline__ void sync() const {
+        if (coop) cg::this_cluster().sync();
+        else __syncthreads();
+    }
+    __device__ __forceinline__ int first() const { return part * kT + (int)threadIdx.x; }
+    __device__ __forceinline__ int step() const { return nparts * kT; }
+    __device__ __forceinline__ bool lead() const { return part == 0 && threadIdx.x == 0; }
+};
+
+__device__ DcSmem dc_shift(const DcSmem& S, int lo) {
+    DcSmem q = S;
+    q.Ds += lo;
+    q.zs += lo;
+    q.dk += lo;
+    q.zk += lo;
+    q.tau += lo;
+    q.zh += lo;
+    q.val += lo;
+    q.perm += lo;
+    q.org += lo;
+    q.sec += lo;
+    q.dl += lo;
+    q.rank += lo;
+    q.cls += lo;
+    q.ktop += lo;
+    q.kbot += lo;
+    q.rpair += lo;
+    q.rcs += lo;
+    return q;
+}
+
+__device__ void dc_merge(const Split& sp, int m, int lo, int mid, int hi, double beta, const DcSmem& S,
+                         double* __restrict__ Z, double* __restrict__ Qp, double* __restrict__ V, int* sc, double* sA,
+                         double* sB) {
+    const DcSmem Q = dc_shift(S, lo);
+    const int n1 = mid - lo, n2 = hi - mid, n = n1 + n2;
+    const double rho = 2.0 * fabs(beta);
+    const double sgn = beta >= 0.0 ? 1.0 : -1.0;
+    const double rs2 = 0.70710678118654752440;
+    const double eps = 2.220446049250313e-16;
+    const int f0 = sp.first(), st = sp.step();
+    // (a) merged order of the two sorted blocks
+    for (int j = f0; j < n; j += st) {
+        int r;
+        if (j < n1) {
+            const double x = S.D[lo + j];
+            int a = 0, b = n2;
+            while (a < b) {
+                const int c = (a + b) >> 1;
+                if (S.D[mid + c] < x) a = c + 1;
+                else b = c;
+            }
+            r = j + a;
+        } else {
+            const double x = S.D[mid + j - n1];
+            int a = 0, b = n1;
+            while (a < b) {
+                const int c = (a + b) >> 1;
+                if (S.D[lo + c] <= x) a = c + 1;
+                else b = c;
+            }
+            r = (j - n1) + a;
+        }
+        Q.perm[r] = j;
+    }
+    sp.sync();
+    // (b) sorted d, z and column classes; (c) Q with the block columns in that order
+    for (int r = f0; r < n; r += st) {
+        const int j = Q.perm[r];
+        if (j < n1) {
+            Q.Ds[r] = S.D[lo + j];
+            Q.zs[r] = Z[(int64_t)(mid - 1) + (int64_t)(lo + j) * m] * rs2;
+            Q.cls[r] = 1;
+        } else {
+            Q.Ds[r] = S.D[mid + j - n1];
+            Q.zs[r] = sgn * Z[(int64_t)mid + (int64_t)(mid + j - n1) * m] * rs2;
+            Q.cls[r] = 2;
+        }
+    }
+    for (int64_t t = f0; t < (int64_t)n * n; t += st) {
+        const int i = (int)(t % n), r = (int)(t / n);
+        const int j = Q.perm[r];
+        double v = 0.0;
+        if (j < n1) {
+            if (i < n1) v = Z[(int64_t)(lo + i) + (int64_t)(lo + j) * m];
+        } else if (i >= n1) {
+            v = Z[(int64_t)(lo + i) + (int64_t)(mid + j - n1) * m];
+        }
+        Qp[t] = v;
+    }
+    sp.sync();
+    // (d) deflation (one thread, in sorted order)
+    if (sp.lead()) {
+        double dmax = 0.0;
+        for (int r = 0; r < n; ++r) dmax = fmax(dmax, fabs(Q.Ds[r]));
+        const double tol = 8.0 * eps * fmax(dmax, rho);
+        int k = 0, nd = 0, nrot = 0, pj = -1;
+        for (int r = 0; r < n; ++r) {
+            if (rho * fabs(Q.zs[r]) <= tol) {
+                Q.dl[nd++] = r;
+                continue;
+            }
+            if (pj < 0) {
+                pj = r;
+                continue;
+            }
+            double sn = Q.zs[pj], c = Q.zs[r];
+            const double t = hypot(c, sn);
+            const double dd = Q.Ds[r] - Q.Ds[pj];
+            c /= t;
+            sn = -sn / t;
+            if (fabs(dd * c * sn) <= tol) {
+                Q.zs[r] = t;
+                Q.zs[pj] = 0.0;
+                Q.rpair[nrot] = make_int2(pj, r);
+                Q.rcs[nrot] = make_double2(c, sn);
+                ++nrot;
+                const double t2 = Q.Ds[pj] * c * c + Q.Ds[r] * sn * sn;
+                Q.Ds[r] = Q.Ds[pj] * sn * sn + Q.Ds[r] * c * c;
+                Q.Ds[pj] = t2;
+                Q.cls[r] |= Q.cls[pj];
+                Q.dl[nd++] = pj;
+                pj = r;
+            } else {
+                Q.sec[k++] = pj;
+                pj = r;
+            }
+        }
+        if (pj >= 0) Q.sec[k++] = pj;
+        int nt = 0, nb = 0;
+        for (int t = 0; t < k; ++t) {
+            const int c = Q.cls[Q.sec[t]];
+            if (c & 1) Q.ktop[nt++] = t;
+            if (c & 2) Q.kbot[nb++] = t;
+        }
+        sc[0] = k;
+        sc[1] = nd;
+        sc[2] = nrot;
+        sc[3] = nt;
+        sc[4] = nb;
+    }
+    sp.sync();
+    const volatile int* vsc = sc;
+    const int k = vsc[0], nd = vsc[1], nrot = vsc[2], ntop = vsc[3], nbot = vsc[4];
+    // (e) deflation rotations on the columns of Q (thread per row)
+    if (nrot > 0)
+        for (int i = f0; i < n; i += st)
+            for (int q2 = 0; q2 < nrot; ++q2) {
+                const int2 pr = Q.rpair[q2];
+                const double2 cs = Q.rcs[q2];
+                const double a = Qp[i + (int64_t)pr.x * n], b = Qp[i + (int64_t)pr.y * n];
+                Qp[i + (int64_t)pr.x * n] = cs.x * a + cs.y * b;
+                Qp[i + (int64_t)pr.y * n] = -cs.y * a + cs.x * b;
+            }
+    for (int t = f0; t < k; t += st) {
+        Q.dk[t] = Q.Ds[Q.sec[t]];
+        Q.zk[t] = Q.zs[Q.sec[t]];
+    }
+    sp.sync();
+    // (f) secular roots
+    for (int i = f0; i < k; i += st) Q.tau[i] = dc_secular(k, Q.dk, Q.zk, rho, i, &Q.org[i]);
+    sp.sync();
+    // (g) recomputed z
+    for (int j = f0; j < k; j += st) {
+        const double dj = Q.dk[j];
+        double w = (Q.dk[Q.org[j]] - dj) + Q.tau[j];
+        for (int i = 0; i < k; ++i) {
+            if (i == j) continue;
+            w *= ((Q.dk[Q.org[i]] - dj) + Q.tau[i]) / (Q.dk[i] - dj);
+        }
+        Q.zh[j] = copysign(sqrt(fmax(w / rho, 0.0)), Q.zk[j]);
+    }
+    sp.sync();
+    // (h) eigenvectors of the rank-one problem (columns of V, k x k) and the new eigenvalues
+    for (int i = f0; i < k; i += st) {
+        const double dorg = Q.dk[Q.org[i]], ti = Q.tau[i];
+        double nrm = 0.0;
+        for (int j = 0; j < k; ++j) {
+            const double v = Q.zh[j] / ((Q.dk[j] - dorg) - ti);
+            nrm = fma(v, v, nrm);
+        }
+        const double scl = 1.0 / sqrt(nrm);
+        for (int j = 0; j < k; ++j) V[j + (int64_t)i * k] = scl * (Q.zh[j] / ((Q.dk[j] - dorg) - ti));
+        Q.val[i] = dorg + ti;
+    }
+    for (int q2 = f0; q2 < nd; q2 += st) Q.val[k + q2] = Q.Ds[Q.dl[q2]];
+    sp.sync();
+    // (i) positions of the n new eigenvalues in ascending order
+    for (int a = f0; a < n; a += st) {
+        const double x = Q.val[a];
+        int r = 0;
+        for (int b2 = 0; b2 < n; ++b2) r += (Q.val[b2] < x || (Q.val[b2] == x && b2 < a)) ? 1 : 0;
+        Q.rank[a] = lo + r;
+    }
+    for (int t = f0; t < ntop; t += st) Q.perm[t] = Q.sec[Q.ktop[t]];
+    sp.sync();
+    // (j) Z block = Q [V | deflated columns], block-1 rows against the columns touching block 1
+    {
+        const int ntr = (n1 + TS - 1) / TS, ntc = (k + TS - 1) / TS;
+        for (int tt = sp.part; tt < ntr * ntc; tt += sp.nparts) {
+            const int r0 = (tt % ntr) * TS, c0 = (tt / ntr) * TS;
+            tile_gemm<false>(Z, m, lo, Q.rank, r0, c0, min(TS, n1 - r0), min(TS, k - c0), Qp, n, Q.perm, V, k, Q.ktop,
+                             ntop, sA, sB);
+        }
+    }
+    sp.sync();
+    for (int t = f0; t < nbot; t += st) Q.perm[t] = Q.sec[Q.kbot[t]];
+    sp.sync();
+    {
+        const int ntr = (n2 + TS - 1) / TS, ntc = (k + TS - 1) / TS;
+        for (int tt = sp.part; tt < ntr * ntc; tt += sp.nparts) {
+            const int r0 = n1 + (tt % ntr) * TS, c0 = (tt / ntr) * TS;
+            tile_gemm<false>(Z, m, lo, Q.rank, r0, c0, min(TS, n - r0), min(TS, k - c0), Qp, n, Q.perm, V, k, Q.kbot,
+                             nbot, sA, sB);
+        }
+    }
+    for (int64_t t = f0; t < (int64_t)nd * n; t += st) {
+        const int i = (int)(t % n), q2 = (int)(t / n);
+        Z[(int64_t)(lo + i) + (int64_t)Q.rank[k + q2] * m] = Qp[i + (int64_t)Q.dl[q2] * n];
+    }
+    for (int a = f0; a < n; a += st) S.D[Q.rank[a]] = Q.val[a];
+    sp.sync();
+}
+
+__device__ bool lg_dc(const Grp& g, const EigProb& p, const double* __restrict__ Da, const double* __restrict__ Ea,
+                      double* __restrict__ Wa, double* __restrict__ Za, double* __restrict__ Qa,
+                      double* __restrict__ Va, double* __restrict__ X, const LgSmem& sh) {
+    const int m = p.m;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const LgLayout lay = lg_layout(m, g.size);
+    const DcSmem S = dc_smem(reinterpret_cast<unsigned char*>(X + lay.dc), (m + 1) & ~1);
+    int* scal = reinterpret_cast<int*>(X + lay.scal);
+    double* Z = Za + p.aoff;
+    const double* eo = Ea + p.voff;
+    int L = 0;
+    while (((m + (1 << L) - 1) >> L) > kDcLeaf) ++L;
+    const int nleaf = 1 << L;
+    for (int i = g.rank * kT + tid; i < m; i += g.size * kT) S.D[i] = Da[p.voff + i];
+    if (g.rank == 0 && tid == 0) scal[7] = 0;
+    g.sync();
+    if (g.rank == 0 && tid == 0)
+        for (int q = 1; q < nleaf; ++q) {
+            const int pos = (int)(((int64_t)q * m) >> L);
+            const double ab = fabs(eo[pos - 1]);
+            S.D[pos - 1] -= ab;
+            S.D[pos] -= ab;
+        }
+    g.sync();
+    // leaves: a warp each over the whole cluster
+    for (int q = g.rank * (kT / 32) + warp; q < nleaf; q += g.size * (kT / 32)) {
+        const int lo = (int)(((int64_t)q * m) >> L), hi = (int)(((int64_t)(q + 1) * m) >> L), s = hi - lo;
+        double dl[kDcLeaf], el[kDcLeaf], zl[kDcLeaf];
+        for (int i = 0; i < kDcLeaf; ++i) {
+            dl[i] = (i < s) ? S.D[lo + i] : 0.0;
+            el[i] = (i < s - 1) ? eo[lo + i] : 0.0;
+        }
+        const bool ok = dc_leaf(s, dl, el, zl, lane);
+        if (!ok && lane == 0) atomicExch(&scal[7], 1);
+        int rk = 0;
+        if (lane < s) {
+            const double x = dl[lane];
+            for (int c = 0; c < s; ++c) rk += (dl[c] < x || (dl[c] == x && c < lane)) ? 1 : 0;
+        }
+        for (int c = 0; c < s; ++c) {
+            const int rc = __shfl_sync(0xffffffffu, rk, c);
+            if (lane < s) Z[(int64_t)(lo + lane) + (int64_t)(lo + rc) * m] = zl[c];
+        }
+        __syncwarp();
+        if (lane < s) S.D[lo + rk] = dl[lane];
+        __syncwarp();
+    }
+    g.sync();
+    if (((volatile int*)scal)[7] != 0) return false;
+    for (int lev = L - 1; lev >= 0; --lev) {
+        const int nm = 1 << lev;
+        if (nm >= g.size) {
+            for (int q = g.rank; q < nm; q += g.size) {
+                const int lo = (int)(((int64_t)q * m) >> lev), hi = (int)(((int64_t)(q + 1) * m) >> lev);
+                const int mid = (int)(((int64_t)(2 * q + 1) * m) >> (lev + 1));
+                dc_merge(Split{0, 1, false}, m, lo, mid, hi, eo[mid - 1], S, Z, Qa + p.aoff + (int64_t)lo * m,
+                         Va + p.aoff + (int64_t)lo * m, scal + 8 + 8 * q, sh.sA, sh.sB);
+            }
+        } else {
+            for (int q = 0; q < nm; ++q) {
+                const int lo = (int)(((int64_t)q * m) >> lev), hi = (int)(((int64_t)(q + 1) * m) >> lev);
+                const int mid = (int)(((int64_t)(2 * q + 1) * m) >> (lev + 1));
+                dc_merge(Split{g.rank, g.size, true}, m, lo, mid, hi, eo[mid - 1], S, Z,
+                         Qa + p.aoff + (int64_t)lo * m, Va + p.aoff + (int64_t)lo * m, scal + 8 + 8 * q, sh.sA, sh.sB);
+            }
+        }
+        g.sync();
+    }
+    for (int i = g.rank * kT + tid; i < m; i += g.size * kT) Wa[p.voff + i] = S.D[i];
+    return true;
+}
+
+// Owned rows of S U and U, fe and the eigenpairs on the cluster: CTA rk takes a
+// contiguous range of the 2 nown vectors (L rows, then L^-T rows by forward
+// substitution), applies Q^T to them, and the product with Z is tiled over
+// the cluster.
+// Per-CTA scratch of the tile-product reflectors in the Q arena (free after the
+// divide and conquer): V panel (m x NB), Y and T Y (NB x nv each) and the
+// panel's Gram.
+__host__ __device__ inline int64_t lg_wy_stride(int m, int nv) {
+    return ((int64_t)NB * m + 2 * (int64_t)NB * nv + NB * NB + 1) & ~int64_t(1);
+}
+
+__device__ void lg_rows(const Grp& g, const EigProb& p, const double* __restrict__ Ca,
+                        const double* __restrict__ La, const double* __restrict__ Ta, const double* __restrict__ Wa,
+                        const double* __restrict__ Za, const int* __restrict__ own_cols, const int* __restrict__ ipos,
+                        double* __restrict__ Ba, double* __restrict__ Qa, double* __restrict__ e_out,
+                        double* __restrict__ fe_out, const LgSmem& sh) {
+    const int m = p.m, no = p.nown, nb2 = 2 * no;
+    const double* C = Ca + p.aoff;
+    const double* L = La + p.aoff;
+    const double* Z = Za + p.aoff;
+    const double* tau = Ta + p.voff;
+    double* R = Ba + p.boff;
+    double* G2 = R + (int64_t)nb2 * m;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = kT / 32;
+    const int per = (nb2 + g.size - 1) / g.size;
+    const int u0 = min(nb2, g.rank * per), u1 = min(nb2, u0 + per);
+    for (int u = u0; u < u1; ++u) {
+        const int t = u < no ? u : u - no;
+        const int ct = ipos[own_cols[p.o0 + t]];
+        double* x = R + (int64_t)u * m;
+        for (int r = tid; r < m; r += kT)
+            x[r] = (u < no) ? ((r <= ct) ? L[ct + (int64_t)r * m] : 0.0) : ((r == ct) ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    const int s0 = max(u0, no);
+    if (s0 < u1) trsm_cols(true, L, m, R + (int64_t)s0 * m, m, 0, u1 - s0, sh.sD, sh.sA, sh.sB);
+    if (u1 > u0) {
+        double* scr = Qa + p.aoff + (int64_t)g.rank * lg_wy_stride(m, per);
+        wy_apply_mma(C, m, tau, R + (int64_t)u0 * m, u1 - u0, true, scr, scr + (int64_t)NB * m,
+                     sh.sD + TS * (TS + 1), sh.sA, sh.sB);
+    }
+    g.sync();
+    {
+        const int ntr = (m + TS - 1) / TS, ntc = (nb2 + TS - 1) / TS;
+        for (int tt = g.rank; tt < ntr * ntc; tt += g.size) {
+            const int r0 = (tt % ntr) * TS, c0 = (tt / ntr) * TS;
+            tile_gemm<true>(G2, m, 0, nullptr, r0, c0, min(TS, m - r0), min(TS, nb2 - c0), Z, m, nullptr, R, m,
+                            nullptr, m, sh.sA, sh.sB);
+        }
+    }
+    g.sync();
+    const double* G3 = G2 + (int64_t)no * m;
+    for (int j = g.rank * kT + tid; j < m; j += g.size * kT) {
+        double f = 0.0;
+        for (int t = 0; t < no; ++t) f = fma(G2[(int64_t)t * m + j], G3[(int64_t)t * m + j], f);
+        e_out[p.eoff + j] = Wa[p.voff + j];
+        fe_out[p.eoff + j] = f;
+    }
+}
+
+// One cluster per submatrix above kEigBatchMax (order[] largest first).
+__global__ void __launch_bounds__(kT, 1) k_eig_cluster(
+    const EigProb* __restrict__ probs, const int* __restrict__ order, int M, const int* __restrict__ maps,
+    const double* __restrict__ H, const double* __restrict__ S, double* __restrict__ Ca, double* __restrict__ La,
+    double* __restrict__ Za, double* __restrict__ Qa, double* __restrict__ Va, double* __restrict__ Da,
+    double* __restrict__ Ea, double* __restrict__ Ta, double* __restrict__ Wa, double* __restrict__ Ba,
+    double* __restrict__ Xa, const int* __restrict__ own_cols, const int* __restrict__ ipos,
+    double* __restrict__ e_out, double* __restrict__ fe_out, int* __restrict__ status,
+    unsigned long long* __restrict__ tstage) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const LgSmem sh = lg_smem(smraw, M);
+    cg::cluster_group cl = cg::this_cluster();
+    const Grp g{(int)cl.block_rank(), (int)cl.num_blocks()};
+    const int pi = order[blockIdx.x / g.size];
+    const EigProb p = probs[pi];
+    double* X = Xa + p.xoff;
+    // stage boundaries (global timer, ns) for the print-level-2 stage summary
+    auto mark = [&](int q) {
+        if (tstage && g.rank == 0 && threadIdx.x == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            tstage[(int64_t)pi * kLgStages + q] = t;
+        }
+    };
+    mark(0);
+    lg_gather(g, p, maps, H, S, Ca, La);
+    g.sync();
+    int st = lg_potrf(g, p.m, La + p.aoff, sh);
+    g.sync();
+    mark(1);
+    if (st == kStOk) {
+        lg_reduce(g, p, La, Ca, sh);
+        mark(2);
+        lg_sytrd(g, p, Ca, Da, Ea, Ta, X, sh);
+        g.sync();
+        mark(3);
+        if (!lg_dc(g, p, Da, Ea, Wa, Za, Qa, Va, X, sh)) st = kStNoConv;
+        g.sync();
+        mark(4);
+        if (st == kStOk) lg_rows(g, p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, Qa, e_out, fe_out, sh);
+    }
+    mark(5);
+    if (g.rank == 0 && threadIdx.x == 0) status[pi] = st;
+}
+
+// Owned columns of P_k at mu on the cluster (the large-submatrix form of
+// k_eig_final): W0 = occ o U[c,:], W = Z W0 tiled over the cluster, then each
+// CTA takes a contiguous range of the columns for Q w, L^-T w and the scatter.
+__global__ void __launch_bounds__(kT, 1) k_eig_final_cluster(
+    const EigProb* __restrict__ probs, const int* __restrict__ order, const double* __restrict__ Ca,
+    const double* __restrict__ La, const double* __restrict__ Ta, const double* __restrict__ Wa,
+    const double* __restrict__ Za, double* __restrict__ Qa, const int* __restrict__ maps,
+    const int* __restrict__ own_cols, double* __restrict__ Ba, double mu, double* __restrict__ Ppk,
+    double* __restrict__ Pdense) {
+    extern __shared__ __align__(16) unsigned char smf[];
+    double* sA = reinterpret_cast<double*>(smf);
+    double* sB = sA + kStageOp;
+    double* sD = sB + kStageOp;
+    double* sT = sD + TS * (TS + 1);
+    cg::cluster_group cl = cg::this_cluster();
+    const Grp g{(int)cl.block_rank(), (int)cl.num_blocks()};
+    const EigProb p = probs[order[blockIdx.x / g.size]];
+    const int m = p.m, no = p.nown;
+    const double* C = Ca + p.aoff;
+    const double* L = La + p.aoff;
+    const double* Z = Za + p.aoff;
+    const double* tau = Ta + p.voff;
+    const double* ev = Wa + p.voff;
+    double* W0 = Ba + p.boff;
+    const double* U2 = Ba + p.boff + 3 * (int64_t)no * m;
+    double* W = Ba + p.boff + (int64_t)no * m;
+    const int tid = threadIdx.x;
+    for (int64_t q = (int64_t)g.rank * kT + tid; q < (int64_t)no * m; q += (int64_t)g.size * kT) {
+        const int j = (int)(q % m);
+        const double e = ev[j];
+        const double occ = e < mu ? 2.0 : (e == mu ? 1.0 : 0.0);
+        W0[q] = occ * U2[q];
+    }
+    g.sync();
+    {
+        const int ntr = (m + TS - 1) / TS, ntc = (no + TS - 1) / TS;
+        for (int tt = g.rank; tt < ntr * ntc; tt += g.size) {
+            const int r0 = (tt % ntr) * TS, c0 = (tt / ntr) * TS;
+            tile_gemm<false>(W, m, 0, nullptr, r0, c0, min(TS, m - r0), min(TS, no - c0), Z, m, nullptr, W0, m,
+                             nullptr, m, sA, sB);
+        }
+    }
+    g.sync();
+    const int per = (no + g.size - 1) / g.size;
+    const int t0 = min(no, g.rank * per), t1 = min(no, t0 + per);
+    if (t1 > t0) {
+        double* scr = Qa + p.aoff + (int64_t)g.rank * lg_wy_stride(m, per);
+        wy_apply_mma(C, m, tau, W + (int64_t)t0 * m, t1 - t0, false, scr, scr + (int64_t)NB * m, sT, sA, sB);
+        __syncthreads();
+        trsm_cols(false, L, m, W + (int64_t)t0 * m, m, 0, t1 - t0, sD, sA, sB);
+    }
+    if (Pdense) {
+        for (int64_t q = (int64_t)t0 * m + tid; q < (int64_t)t1 * m; q += kT) Pdense[p.poff + q] = W[q];
+        return;
+    }
+    const int* mp = maps + p.moff;
+    for (int64_t q = (int64_t)t0 * m + tid; q < (int64_t)t1 * m; q += kT) {
+        const int t = (int)(q / m), i = (int)(q % m);
+        const int64_t cgl = own_cols[p.o0 + t];
+        const int64_t gi = mp[i];
+        if (gi <= cgl) Ppk[cgl * (cgl + 1) / 2 + gi] = W[q];
+    }
+}
+
 }  // namespace
 
 struct EigBatch {
     int nprob = 0;
     int maxm = 0;
+    int G = 1;                    // CTAs per cluster of the large-submatrix solver
+    int nsmall = 0, nlarge = 0;
     std::vector<EigProb> hp;
-    DevBuf probs, order, counter, Ca, La, Za, Qa, Va, Da, Ea, Ta, Wa, Ba, status;
+    DevBuf probs, order, order_l, counter, Ca, La, Za, Qa, Va, Da, Ea, Ta, Wa, Ba, Xa, status, tstage;
+    int prl = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~EigBatch() {
-        for (DevBuf* b : {&probs, &order, &counter, &Ca, &La, &Za, &Qa, &Va, &Da, &Ea, &Ta, &Wa, &Ba, &status})
+        if (side) cudaStreamSynchronize(side);
+        for (DevBuf* b : {&probs, &order, &order_l, &counter, &Ca, &La, &Za, &Qa, &Va, &Da, &Ea, &Ta, &Wa, &Ba, &Xa,
+                          &status, &tstage})
             b->release();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (side) cudaStreamDestroy(side);
     }
 };
 
@@ -1351,9 +2496,78 @@ void eig_setup_attrs() {
     static const bool done = [] {
         PTB_CUDA(cudaFuncSetAttribute(k_eig_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)stage_smem_bytes(kEigBatchMax)));
+        PTB_CUDA(cudaFuncSetAttribute(k_eig_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)lg_smem_bytes(kLargeMax)));
+        PTB_CUDA(cudaFuncSetAttribute(k_eig_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        PTB_CUDA(cudaFuncSetAttribute(k_eig_final_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        PTB_CUDA(cudaFuncSetAttribute(k_eig_final_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinalSmem));
+        PTB_CUDA(cudaFuncSetAttribute(k_eig_final, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinalSmem));
         return true;
     }();
     (void)done;
+}
+
+// CTAs per cluster of the large-submatrix solver: 16 when clusters of 16 keep
+// at least 80 % of the SMs busy (one 512-thread CTA each), else 8, else the
+// size among 4 and 2 that keeps the most SMs busy; a submatrix's stages
+// shorten with the cluster, and the longest submatrix sets the step.
+// PTBGPU_EIG_CLUSTER overrides it.
+int eig_cluster_size(ptbgpu_ctx* c) {
+    static int cached[64] = {};
+    const int dev = c->device & 63;
+    if (cached[dev]) return cached[dev];
+    int best = 1, best_ctas = 0;
+    if (const char* e = getenv("PTBGPU_EIG_CLUSTER")) {
+        const int v = atoi(e);
+        if (v == 1 || v == 2 || v == 4 || v == 8 || v == 16) best = v;
+    } else {
+        const int nsm = c->num_sms > 0 ? c->num_sms : 148;
+        for (int G : {16, 8, 4, 2}) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = G;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(G * 64);
+            cfg.blockDim = dim3(kT);
+            cfg.dynamicSmemBytes = lg_smem_bytes(kLargeMax);
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int ncl = 0;
+            if (cudaOccupancyMaxActiveClusters(&ncl, (void*)k_eig_cluster, &cfg) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            if (G >= 8 && ncl * G * 5 >= nsm * 4) {
+                best = G;
+                break;
+            }
+            if (ncl * G > best_ctas) {
+                best_ctas = ncl * G;
+                best = G;
+            }
+        }
+    }
+    cached[dev] = best;
+    return best;
+}
+
+template <class K, class... Args>
+void launch_clustered(K kern, int nclusters, int G, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = G;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(nclusters * G);
+    cfg.blockDim = dim3(kT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    PTB_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
 }
 
 }  // namespace
@@ -1362,16 +2576,20 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
                                            const std::vector<EigProbHost>& probs, const int* d_maps,
                                             const int* d_own_cols, const int* d_ipos, double* d_e, double* d_fe,
                                             int prl, double* flops) {
-    (void)prl;
     if (probs.empty()) return nullptr;
     eig_setup_attrs();
     cudaStream_t s = c->stream;
     auto eb = std::make_shared<EigBatch>();
     eb->nprob = (int)probs.size();
-    int64_t asz = 0, vsz = 0, bsz = 0, psz = 0;
+    eb->prl = prl;
+    bool any_large = false;
+    for (const EigProbHost& q : probs) any_large = any_large || q.m > kEigBatchMax;
+    eb->G = any_large ? eig_cluster_size(c) : 1;
+    int64_t asz = 0, vsz = 0, bsz = 0, psz = 0, xsz = 0;
+    std::vector<int> ord_s, ord_l;
     for (const EigProbHost& q : probs) {
-        PTB_CHECK(q.m >= 1 && q.m <= kEigBatchMax, PTBGPU_EINVAL, "submatrix %d of order %d outside the batched solver",
-                  q.k + 1, q.m);
+        PTB_CHECK(q.m >= 1 && q.m <= kLargeMax, PTBGPU_EINVAL, "submatrix %d of order %d outside the eigensolver (1..%d)",
+                  q.k + 1, q.m, kLargeMax);
         EigProb p{};
         p.k = q.k;
         p.m = q.m;
@@ -1386,18 +2604,28 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
         p.aoff = asz;
         p.voff = vsz;
         p.boff = bsz;
+        p.xoff = xsz;
         asz += (int64_t)q.m * q.m;
         vsz += q.m;
         bsz += 4 * (int64_t)q.nown * q.m;
+        if (q.m > kEigBatchMax) {
+            xsz += lg_layout(q.m, eb->G).total;
+            ord_l.push_back((int)eb->hp.size());
+        } else {
+            ord_s.push_back((int)eb->hp.size());
+        }
         eb->maxm = std::max(eb->maxm, q.m);
         eb->hp.push_back(p);
         if (flops) *flops += 7.0 * std::pow((double)q.m, 3);
     }
     const int np = eb->nprob;
+    eb->nsmall = (int)ord_s.size();
+    eb->nlarge = (int)ord_l.size();
     eb->probs.reserve(sizeof(EigProb) * np);
     for (DevBuf* b : {&eb->Ca, &eb->La, &eb->Za, &eb->Qa, &eb->Va}) b->reserve(sizeof(double) * asz);
     for (DevBuf* b : {&eb->Da, &eb->Ea, &eb->Ta, &eb->Wa}) b->reserve(sizeof(double) * vsz);
     eb->Ba.reserve(sizeof(double) * std::max<int64_t>(bsz, 1));
+    eb->Xa.reserve(sizeof(double) * std::max<int64_t>(xsz, 2));
     eb->status.reserve(sizeof(int) * np);
     PTB_CUDA(cudaMemcpyAsync(eb->probs.ptr, eb->hp.data(), sizeof(EigProb) * np, cudaMemcpyHostToDevice, s));
     PTB_CUDA(cudaMemsetAsync(eb->status.ptr, 0, sizeof(int) * np, s));
@@ -1405,22 +2633,57 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
     int* dst = eb->status.as<int>();
 
     // largest first, so that the small submatrices fill in around the large ones
-    std::vector<int> ord(np);
-    for (int q = 0; q < np; ++q) ord[q] = q;
-    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return eb->hp[a].m > eb->hp[b].m; });
-    eb->order.reserve(sizeof(int) * np);
+    auto by_size = [&](int a, int b) { return eb->hp[a].m > eb->hp[b].m; };
+    std::stable_sort(ord_s.begin(), ord_s.end(), by_size);
+    std::stable_sort(ord_l.begin(), ord_l.end(), by_size);
+    eb->order.reserve(sizeof(int) * std::max<size_t>(ord_s.size(), 1));
+    eb->order_l.reserve(sizeof(int) * std::max<size_t>(ord_l.size(), 1));
     eb->counter.reserve(sizeof(int));
-    PTB_CUDA(cudaMemcpyAsync(eb->order.ptr, ord.data(), sizeof(int) * np, cudaMemcpyHostToDevice, s));
+    if (!ord_s.empty())
+        PTB_CUDA(cudaMemcpyAsync(eb->order.ptr, ord_s.data(), sizeof(int) * ord_s.size(), cudaMemcpyHostToDevice, s));
+    if (!ord_l.empty())
+        PTB_CUDA(cudaMemcpyAsync(eb->order_l.ptr, ord_l.data(), sizeof(int) * ord_l.size(), cudaMemcpyHostToDevice, s));
     PTB_CUDA(cudaMemsetAsync(eb->counter.ptr, 0, sizeof(int), s));
-    const int M = (eb->maxm + 1) & ~1;
-    const int grid = std::min(np, c->num_sms > 0 ? c->num_sms : 148);
-    k_eig_fused<<<grid, kT, stage_smem_bytes(M), s>>>(
-        dp, eb->order.as<int>(), np, eb->counter.as<int>(), M, d_maps, H, S, eb->Ca.as<double>(),
-        eb->La.as<double>(), eb->Za.as<double>(), eb->Qa.as<double>(), eb->Va.as<double>(), eb->Da.as<double>(),
-        eb->Ea.as<double>(), eb->Ta.as<double>(), eb->Wa.as<double>(), eb->Ba.as<double>(), d_own_cols, d_ipos, d_e,
-        d_fe, dst);
-    count_launch();
-    PTB_CUDA(cudaGetLastError());
+    // the large submatrices on their clusters (a side stream, launched first so
+    // their clusters find free SMs), the small ones in the persistent launch
+    if (eb->nlarge > 0) {
+        PTB_CUDA(cudaStreamCreateWithFlags(&eb->side, cudaStreamNonBlocking));
+        PTB_CUDA(cudaEventCreateWithFlags(&eb->ev0, cudaEventDisableTiming));
+        PTB_CUDA(cudaEventCreateWithFlags(&eb->ev1, cudaEventDisableTiming));
+        unsigned long long* dts = nullptr;
+        if (prl >= 2) {
+            eb->tstage.reserve(sizeof(unsigned long long) * kLgStages * np);
+            PTB_CUDA(cudaMemsetAsync(eb->tstage.ptr, 0, sizeof(unsigned long long) * kLgStages * np, s));
+            dts = eb->tstage.as<unsigned long long>();
+        }
+        PTB_CUDA(cudaEventRecord(eb->ev0, s));
+        PTB_CUDA(cudaStreamWaitEvent(eb->side, eb->ev0, 0));
+        launch_clustered(k_eig_cluster, eb->nlarge, eb->G, lg_smem_bytes(kLargeMax), eb->side, dp,
+                         (const int*)eb->order_l.as<int>(), kLargeMax, d_maps, H, S, eb->Ca.as<double>(),
+                         eb->La.as<double>(), eb->Za.as<double>(), eb->Qa.as<double>(), eb->Va.as<double>(),
+                         eb->Da.as<double>(), eb->Ea.as<double>(), eb->Ta.as<double>(), eb->Wa.as<double>(),
+                         eb->Ba.as<double>(), eb->Xa.as<double>(), d_own_cols, d_ipos, d_e, d_fe, dst, dts);
+        count_launch();
+        PTB_CUDA(cudaEventRecord(eb->ev1, eb->side));
+        log_line(prl, 2, " * submatrix cluster eigensolver: %d problems above order %d, clusters of %d CTAs",
+                 eb->nlarge, kEigBatchMax, eb->G);
+    }
+    if (eb->nsmall > 0) {
+        const int M = (std::min(eb->maxm, kEigBatchMax) + 1) & ~1;
+        int Msmall = 0;
+        for (int q : ord_s) Msmall = std::max(Msmall, eb->hp[q].m);
+        const int Ms = (Msmall + 1) & ~1;
+        (void)M;
+        const int grid = std::min(eb->nsmall, c->num_sms > 0 ? c->num_sms : 148);
+        k_eig_fused<<<grid, kT, stage_smem_bytes(Ms), s>>>(
+            dp, eb->order.as<int>(), eb->nsmall, eb->counter.as<int>(), Ms, d_maps, H, S, eb->Ca.as<double>(),
+            eb->La.as<double>(), eb->Za.as<double>(), eb->Qa.as<double>(), eb->Va.as<double>(), eb->Da.as<double>(),
+            eb->Ea.as<double>(), eb->Ta.as<double>(), eb->Wa.as<double>(), eb->Ba.as<double>(), d_own_cols, d_ipos,
+            d_e, d_fe, dst);
+        count_launch();
+        PTB_CUDA(cudaGetLastError());
+    }
+    if (eb->nlarge > 0) PTB_CUDA(cudaStreamWaitEvent(s, eb->ev1, 0));
     return eb;
 }
 
@@ -1436,6 +2699,31 @@ void eig_batch_check(ptbgpu_ctx* c, EigBatch& eb) {
     for (int q = 0; q < np; ++q)
         PTB_CHECK(hst[q] == kStOk, PTBGPU_EITER, "tridiagonal eigensolver did not converge on submatrix %d",
                   eb.hp[q].k + 1);
+    if (eb.prl >= 2 && eb.nlarge > 0 && eb.tstage.ptr) {
+        // per stage: summed over the large submatrices and the longest one, then
+        // the span from the first cluster's start to the last one's end
+        std::vector<unsigned long long> ts((size_t)kLgStages * np);
+        PTB_CUDA(cudaMemcpy(ts.data(), eb.tstage.ptr, sizeof(unsigned long long) * ts.size(), cudaMemcpyDeviceToHost));
+        static const char* names[kLgStages - 1] = {"gather + Cholesky", "reduction", "tridiagonalisation",
+                                                   "divide and conquer", "owned rows"};
+        double sum[kLgStages - 1] = {}, mx[kLgStages - 1] = {};
+        unsigned long long t_lo = ~0ull, t_hi = 0;
+        for (int q = 0; q < np; ++q) {
+            if (eb.hp[q].m <= kEigBatchMax) continue;
+            const unsigned long long* t = &ts[(size_t)q * kLgStages];
+            t_lo = std::min(t_lo, t[0]);
+            t_hi = std::max(t_hi, t[kLgStages - 1]);
+            for (int k = 0; k + 1 < kLgStages; ++k) {
+                const double d = (t[k + 1] >= t[k] && t[k] != 0) ? (double)(t[k + 1] - t[k]) * 1e-6 : 0.0;
+                sum[k] += d;
+                mx[k] = std::max(mx[k], d);
+            }
+        }
+        for (int k = 0; k + 1 < kLgStages; ++k)
+            log_line(eb.prl, 2, " * cluster eigensolver %-22s sum %10.3f ms, longest %9.3f ms", names[k], sum[k], mx[k]);
+        log_line(eb.prl, 2, " * cluster eigensolver span %10.3f ms (%d submatrices, clusters of %d)",
+                 t_hi > t_lo ? (double)(t_hi - t_lo) * 1e-6 : 0.0, eb.nlarge, eb.G);
+    }
 }
 
 void eig_batch_final(ptbgpu_ctx* c, EigBatch& eb, double mu, int64_t n, const int* d_maps, const int* d_own_cols,
@@ -1443,11 +2731,23 @@ void eig_batch_final(ptbgpu_ctx* c, EigBatch& eb, double mu, int64_t n, const in
     (void)n;
     if (eb.nprob == 0) return;
     cudaStream_t s = c->stream;
-    k_eig_final<<<eb.nprob, kT, 0, s>>>(eb.probs.as<EigProb>(), eb.Ca.as<double>(), eb.La.as<double>(),
-                                        eb.Ta.as<double>(), eb.Wa.as<double>(), eb.Za.as<double>(), d_maps,
-                                        d_own_cols, eb.Ba.as<double>(), mu, dP, dPdense);
-    count_launch();
-    PTB_CUDA(cudaGetLastError());
+    if (eb.nsmall > 0) {
+        eig_setup_attrs();
+        k_eig_final<<<eb.nsmall, kT, kFinalSmem, s>>>(eb.probs.as<EigProb>(), eb.order.as<int>(), eb.Ca.as<double>(),
+                                                      eb.La.as<double>(), eb.Ta.as<double>(), eb.Wa.as<double>(),
+                                                      eb.Za.as<double>(), eb.Qa.as<double>(), eb.Va.as<double>(),
+                                                      d_maps, d_own_cols, eb.Ba.as<double>(), mu, dP, dPdense);
+        count_launch();
+        PTB_CUDA(cudaGetLastError());
+    }
+    if (eb.nlarge > 0) {
+        launch_clustered(k_eig_final_cluster, eb.nlarge, eb.G, kFinalSmem, s, (const EigProb*)eb.probs.as<EigProb>(),
+                         (const int*)eb.order_l.as<int>(), (const double*)eb.Ca.as<double>(),
+                         (const double*)eb.La.as<double>(), (const double*)eb.Ta.as<double>(),
+                         (const double*)eb.Wa.as<double>(), (const double*)eb.Za.as<double>(), eb.Qa.as<double>(),
+                         d_maps, d_own_cols, eb.Ba.as<double>(), mu, dP, dPdense);
+        count_launch();
+    }
 }
 
 // Kernel-level entry: dense host problems through the same stages.  Problem k's
@@ -1467,9 +2767,9 @@ void sygv_batched_entry(ptbgpu_ctx* c, int64_t np, const int64_t* dims, const do
     int64_t hsz = 0, nsum = 0, osum = 0, psz = 0;
     for (int64_t k = 0; k < np; ++k) {
         const int m = (int)dims[k];
-        PTB_CHECK(dims[k] >= 1 && dims[k] <= kEigBatchMax && nown[k] >= 1 && nown[k] <= dims[k], PTBGPU_EINVAL,
+        PTB_CHECK(dims[k] >= 1 && dims[k] <= kLargeMax && nown[k] >= 1 && nown[k] <= dims[k], PTBGPU_EINVAL,
                   "problem %lld: order %lld (1..%d) or owned count %lld out of range", (long long)k,
-                  (long long)dims[k], kEigBatchMax, (long long)nown[k]);
+                  (long long)dims[k], kLargeMax, (long long)nown[k]);
         EigProbHost q{};
         q.k = (int)k;
         q.m = m;

@@ -11,6 +11,10 @@ namespace ptb {
 // Largest submatrix the batched solver takes (its per-problem shared-memory
 // vectors are sized for it); larger ones go to the side-stream path.
 constexpr int kEigBatchMax = 1024;
+// Largest submatrix the library's eigensolver takes at all: orders above
+// kEigBatchMax run on a thread-block cluster each, whose tridiagonalisation
+// keeps two vectors of this length in shared memory.
+constexpr int kEigLargeMax = 10240;
 
 // One submatrix as the host plan describes it.
 struct EigProbHost {

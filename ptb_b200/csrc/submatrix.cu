@@ -905,9 +905,10 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
     DevBuf& bfe = c->buf(B_MISC1);
     be.reserve(sizeof(double) * std::max<int64_t>(eoff, 1));
     bfe.reserve(sizeof(double) * std::max<int64_t>(eoff, 1));
-    // submatrices up to kEigBatchMax: the library's batched eigensolver (one
-    // CTA per submatrix); PTBGPU_SM_EIG=library sends them through cuSOLVER's
-    // batched routines in tuned size buckets instead (kept for comparison)
+    // every submatrix through the library's eigensolver: up to kEigBatchMax one
+    // CTA each in a persistent launch, above it one thread-block cluster each;
+    // PTBGPU_SM_EIG=library sends them through cuSOLVER instead (batched routines
+    // in tuned size buckets, dsygvd above kEigBatchMax; kept for comparison)
     static const bool use_library = [] {
         const char* v = getenv("PTBGPU_SM_EIG");
         return v != nullptr && std::string(v) == "library";
@@ -915,12 +916,22 @@ void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
     // launched on the context's stream after the side streams' start event, so
     // that it runs while the large submatrices are solved on the side streams
     std::vector<EigProbHost> own_probs;
-    if (!use_library && !small.empty()) {
-        own_probs.reserve(small.size());
+    if (!use_library) {
+        own_probs.reserve(small.size() + large.size());
         for (const Prob& p : small)
             own_probs.push_back(
                 {p.k, p.m, (int)(pl.own_off[p.k + 1] - pl.own_off[p.k]), p.moff, p.eoff, pl.own_off[p.k]});
         small.clear();
+        // above kEigBatchMax: one thread-block cluster per submatrix, up to kEigLargeMax
+        std::vector<Prob> rest;
+        for (const Prob& p : large) {
+            if (p.m <= kEigLargeMax)
+                own_probs.push_back(
+                    {p.k, p.m, (int)(pl.own_off[p.k + 1] - pl.own_off[p.k]), p.moff, p.eoff, pl.own_off[p.k]});
+            else
+                rest.push_back(p);
+        }
+        large.swap(rest);
     }
     auto launch_own = [&] {
         if (own_probs.empty() || pl.eig) return;

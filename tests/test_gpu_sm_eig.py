@@ -7,9 +7,11 @@ source/sm.f90:296-299), stage by stage through what leaves the solver:
 * the owned columns of P = U occ U^T with occ 2 / 1 / 0 for e < / = / > mu
   (source/sm.f90:322-362).
 
-Orders 1 to 1024 (the solver's limit) in one batch, uneven owned counts, an
-exactly degenerate spectrum, and a non-positive-definite overlap.  FP64
-throughout: eigenvalues to 1e-11 of the spectral range, fe and P to 1e-10.
+Orders 1 to 1024 (one CTA per problem) in one batch, uneven owned counts, an
+exactly degenerate spectrum, and a non-positive-definite overlap; orders above
+1024 (one thread-block cluster per problem) alone and mixed with small ones,
+with a degenerate spectrum and a non-positive-definite overlap of their own.
+FP64 throughout: eigenvalues to 1e-11 of the spectral range, fe and P to 1e-10.
 """
 import numpy as np
 import pytest
@@ -86,4 +88,75 @@ def test_non_positive_definite_overlap_is_reported(ctx):
     S[40, 40] = -5.0
     with pytest.raises(PtbGpuError) as ei:
         ctx.sygv_batched([_problem(30, rng, 2), (H, S, own)])
+    assert ei.value.code == api.ENOTSPD and "submatrix 2" in str(ei.value)
+
+
+LARGE = [1025, 1100, 1537, 2100]
+
+
+def test_cluster_orders_match_lapack(ctx):
+    """Orders above 1024 go to the cluster solver (Cholesky, reduction,
+    tridiagonalisation, divide and conquer and owned rows each spread over the
+    CTAs of a cluster); owned counts as the k-means partitions have them (one to
+    a few hundred columns)."""
+    rng = np.random.default_rng(23)
+    nowns = [1, 37, 310, 120]
+    probs = [_problem(m, rng, no) for m, no in zip(LARGE, nowns)]
+    mu = -0.1
+    out = ctx.sygv_batched(probs, mu=mu)
+    for (H, S, own), (e, fe, Pc) in zip(probs, out):
+        m = H.shape[0]
+        er, fer, Pr = _reference(H, S, own, mu)
+        order = np.argsort(e, kind="stable")
+        scale = max(1.0, np.max(np.abs(er)))
+        assert np.max(np.abs(e[order] - er)) <= 1e-11 * scale * np.sqrt(m), m
+        assert np.max(np.abs(fe[order] - fer)) <= 1e-10, m
+        assert np.max(np.abs(Pc - Pr)) <= 1e-10, m
+        assert abs(np.sum(fe) - len(own)) <= 1e-10 * m
+
+
+def test_cluster_and_batched_orders_in_one_call(ctx):
+    """Small and large problems of one call run on both solvers at once (the
+    persistent launch and the clusters side by side); each result lands at its
+    own offsets."""
+    rng = np.random.default_rng(29)
+    sizes = [700, 1300, 33, 1030, 256]
+    probs = [_problem(m, rng, 1 + (m % 29)) for m in sizes]
+    out = ctx.sygv_batched(probs, mu=0.2)
+    for (H, S, own), (e, fe, Pc) in zip(probs, out):
+        er, fer, Pr = _reference(H, S, own, 0.2)
+        order = np.argsort(e, kind="stable")
+        assert np.max(np.abs(e[order] - er)) <= 1e-11 * max(1.0, np.max(np.abs(er))) * np.sqrt(len(e))
+        assert np.max(np.abs(fe[order] - fer)) <= 1e-10
+        assert np.max(np.abs(Pc - Pr)) <= 1e-10
+
+
+def test_cluster_degenerate_spectrum(ctx):
+    """Four identical 300-blocks: every eigenvalue four times, so the top merges
+    of the divide and conquer (run by the whole cluster) deflate by rotations."""
+    rng = np.random.default_rng(31)
+    b = 300
+    Hb = rng.uniform(-1, 1, (b, b))
+    Hb = 0.5 * (Hb + Hb.T)
+    Ab = rng.standard_normal((b, b))
+    Sb = Ab @ Ab.T / b + np.eye(b)
+    H = np.kron(np.eye(4), Hb)
+    S = np.kron(np.eye(4), Sb)
+    own = np.array([0, 7, 299, 300, 650, 1199])
+    e_b = sl.eigh(Hb, Sb, eigvals_only=True)
+    mu = 0.5 * (e_b[140] + e_b[141])
+    (e, fe, Pc), = ctx.sygv_batched([(H, S, own)], mu=mu)
+    er, fer, Pr = _reference(H, S, own, mu)
+    assert np.max(np.abs(np.sort(e) - er)) <= 1e-11 * max(1.0, np.max(np.abs(er))) * 40
+    assert np.max(np.abs(Pc - Pr)) <= 1e-10
+    assert abs(np.sum(fe[e < mu]) - np.sum(fer[er < mu])) <= 1e-10
+
+
+def test_cluster_non_positive_definite_overlap_is_reported(ctx):
+    rng = np.random.default_rng(3)
+    H, S, own = _problem(1200, rng, 5)
+    S = S.copy()
+    S[900, 900] = -5.0
+    with pytest.raises(PtbGpuError) as ei:
+        ctx.sygv_batched([_problem(40, rng, 2), (H, S, own)])
     assert ei.value.code == api.ENOTSPD and "submatrix 2" in str(ei.value)
