@@ -9,6 +9,7 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "sm_eig.cuh"
 
 namespace ptb {
 
@@ -498,7 +499,14 @@ void trtri_rec(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A) {
 // triangle is not referenced.
 void dtrtri_lower(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A) { trtri_rec(c, n, ld, A); }
 
+// All eigenpairs of a symmetric matrix (upper triangle read, eigenvectors over
+// A, w ascending): the library's eigensolver up to order kEigLargeMax, cuSOLVER
+// above it.
 void dsyevd(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A, double* w) {
+    if (n <= kEigLargeMax && ld == n) {
+        eig_full_upper(c, n, A, nullptr, w);
+        return;
+    }
     int lwork = 0;
     PTB_CUSOLVER(cusolverDnDsyevd_bufferSize(c->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER,
                                              (int)n, A, (int)ld, w, &lwork));
@@ -512,7 +520,19 @@ void dsyevd(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A, double* w) {
     PTB_CHECK(info == 0, PTBGPU_ECUDA, "dsyevd info=%d", info);
 }
 
+// H U = S U diag(w) (upper triangles read, U over A with U^T S U = I, w
+// ascending): the library's eigensolver up to order kEigLargeMax, cuSOLVER above
+// it.  Returns 0, or n + the order of S's first non-positive leading minor.
 int dsygvd(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A, double* B, double* w) {
+    if (n <= kEigLargeMax && ld == n) {
+        try {
+            eig_full_upper(c, n, A, B, w);
+        } catch (const Error& e) {
+            if (e.code != PTBGPU_ENOTSPD) throw;
+            return (int)n + 1;
+        }
+        return 0;
+    }
     int lwork = 0;
     PTB_CUSOLVER(cusolverDnDsygvd_bufferSize(c->solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
                                              CUBLAS_FILL_MODE_UPPER, (int)n, A, (int)ld, B, (int)ld, w,

@@ -46,7 +46,8 @@ constexpr int kStNoConv = -1;     // a leaf's QL sweeps exhausted
 // > 0: leading minor of that order of S_k is not positive definite
 
 struct EigProb {
-    int k, m, nown, pad;
+    int k, m, nown;
+    int kind;             // 0: H U = S U e; 1: standard problem (S not read, L = I)
     int64_t moff, eoff, o0;
     int64_t gbase, gld;   // the problem's H / S: element (i, j) at gbase + map(i) + map(j) gld
     int64_t poff;         // dense output of the owned columns of P (m x nown, column-major)
@@ -54,6 +55,7 @@ struct EigProb {
     int64_t voff;     // d, e, tau, eigenvalue arenas (m)
     int64_t boff;     // owned-row arena (4 nown x m)
     int64_t xoff;     // cluster solver scratch (orders above kEigBatchMax)
+    int64_t koff;     // T of the compact WY panels (t_panels(m) x NB^2)
 };
 
 // ---------------------------------------------------------------------------
@@ -88,7 +90,12 @@ __device__ __forceinline__ int sb_idx(int k, int j) {
     return BT ? k * 68 + j : j * 36 + k;
 }
 
-template <bool AT, bool BT, int MODE, bool LOWER>
+// AREF / BREF: the operand is a panel of Householder reflectors stored as
+// below, read with its implicit structure (1 where the row equals the
+// reflector's index, the stored value below it, 0 above): A(i, k) is reflector
+// r0+i at row k when AT, row r0+i of reflector k otherwise; B(k, j) is row k of
+// reflector c0+j.
+template <bool AT, bool BT, int MODE, bool LOWER, bool AREF = false, bool BREF = false>
 __device__ void tile_mma(double* __restrict__ C, int64_t ldc, int crow, const int* ccol, int r0, int c0, int mr,
                          int nc, const double* __restrict__ A, int64_t lda, const int* kx,
                          const double* __restrict__ B, int64_t ldb, const int* kxb, int K, double* sA, double* sB) {
@@ -111,14 +118,25 @@ __device__ void tile_mma(double* __restrict__ C, int64_t ldc, int crow, const in
             double v = 0.0;
             if (i < mr && k < kk) {
                 const int64_t kg = kx ? kx[k0 + k] : (k0 + k);
-                v = AT ? A[kg + (int64_t)(r0 + i) * lda] : A[(int64_t)(r0 + i) + kg * lda];
+                if (AREF) {
+                    const int64_t ig = r0 + i;   // AT: reflector ig at row kg; else row ig of reflector kg
+                    const int64_t row = AT ? kg : ig, refl = AT ? ig : kg;
+                    v = (row == refl) ? 1.0 : (row > refl ? A[row + refl * lda] : 0.0);
+                } else {
+                    v = AT ? A[kg + (int64_t)(r0 + i) * lda] : A[(int64_t)(r0 + i) + kg * lda];
+                }
             }
             ra[q] = v;
             const int j = BT ? t % TS : t / NB, kb = BT ? t / TS : t % NB;
             double w = 0.0;
             if (j < nc && kb < kk) {
                 const int64_t kg = kxb ? kxb[k0 + kb] : (k0 + kb);
-                w = BT ? B[(int64_t)(c0 + j) + kg * ldb] : B[kg + (int64_t)(c0 + j) * ldb];
+                if (BREF) {
+                    const int64_t refl = c0 + j;
+                    w = (kg == refl) ? 1.0 : (kg > refl ? B[kg + refl * ldb] : 0.0);
+                } else {
+                    w = BT ? B[(int64_t)(c0 + j) + kg * ldb] : B[kg + (int64_t)(c0 + j) * ldb];
+                }
             }
             rb[q] = w;
         }
@@ -1125,37 +1143,30 @@ __device__ void wy_apply(const double* __restrict__ C, int m, const double* __re
 }
 
 // ---------------------------------------------------------------------------
-constexpr int kWyMmaMin = 160;   // orders from which the reflectors are applied as tile products
+constexpr int kWyMmaMin = 64;   // orders from which the reflectors are applied as tile products
 
-// Q = H_0 ... H_{m-3} applied to nv vectors (X, ld m) on the FP64 tensor
-// cores, a panel of NB reflectors at a time as I - V T V^T: Vp = the panel's
-// reflectors written out (rows j0+1.., unit and zeros in place), its Gram
-// matrix by one tile product, T from the Gram as in wy_apply, then
-// Y = V^T X, Y2 = T^T Y (trans) or T Y, X -= V Y2 as tile products.  Vp
-// (m x NB) and Y (2 NB x nv + NB x NB) are global scratch, T is NB x (NB+1)
-// shared.
-__device__ void wy_apply_mma(const double* __restrict__ C, int m, const double* __restrict__ tau, double* X, int nv,
-                             bool trans, double* Vp, double* Y, double* T, double* sA, double* sB) {
+__host__ __device__ constexpr int64_t t_panels(int m) { return m > 2 ? (m - 2 + NB - 1) / NB : 0; }
+
+// T of the compact WY form I - V T V^T of every panel of NB reflectors of
+// Q = H_0 ... H_{m-3} (panels p = first, first + step, ...): the panel's
+// Gram V^T V as one tile product reading the reflectors in place, then T
+// column by column (T_bb = tau_b, T[0:b, b] = -tau_b T[0:b, 0:b] G[0:b, b])
+// by one warp.  Tall + p NB^2 holds panel p's T (NB x NB, column-major, zero
+// outside the panel's nb x nb upper triangle).  Gg: NB^2 global scratch;
+// T: NB x (NB+1) shared.
+__device__ void build_T(const double* __restrict__ C, int m, const double* __restrict__ tau, double* __restrict__ Tall,
+                        int first, int step, double* Gg, double* T, double* sA, double* sB) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nref = m - 2;
-    if (nref <= 0 || nv <= 0) return;
-    const int npan = (nref + NB - 1) / NB;
-    double* Gg = Y + (int64_t)NB * nv;
-    double* Y2 = Gg + NB * NB;
-    for (int pp = 0; pp < npan; ++pp) {
-        const int pan = trans ? pp : npan - 1 - pp;
-        const int j0 = pan * NB, nb = min(NB, nref - j0);
-        const int r0 = j0 + 1, len = m - r0;
-        for (int64_t q = tid; q < (int64_t)len * NB; q += kT) {
-            const int i = (int)(q % len), a = (int)(q / len);
-            Vp[q] = (a < nb) ? wy_v(C, m, j0 + a, r0 + i) : 0.0;
-        }
-        __syncthreads();
-        tile_mma<true, false, MMA_SET, false>(Gg, NB, 0, nullptr, 0, 0, NB, NB, Vp, len, nullptr, Vp, len, nullptr, len,
-                                              sA, sB);
+    const int npan = (int)t_panels(m);
+    for (int pan = first; pan < npan; pan += step) {
+        const int j0 = pan * NB, nb = min(NB, nref - j0), r0 = j0 + 1, len = m - r0;
+        const double* Vb = C + r0 + (int64_t)j0 * m;
+        tile_mma<true, false, MMA_SET, false, true, true>(Gg, NB, 0, nullptr, 0, 0, nb, nb, Vb, m, nullptr, Vb, m,
+                                                          nullptr, len, sA, sB);
         for (int q = tid; q < NB * NB; q += kT) {
             const int a = q % NB, b = q / NB;
-            T[a + b * (NB + 1)] = (a <= b && a < nb && b < nb) ? Gg[a + b * NB] : 0.0;
+            T[a + b * (NB + 1)] = (a <= b && b < nb) ? Gg[a + b * NB] : 0.0;
         }
         __syncthreads();
         if (warp == 0) {
@@ -1171,25 +1182,53 @@ __device__ void wy_apply_mma(const double* __restrict__ C, int m, const double* 
             }
         }
         __syncthreads();
+        double* Tp = Tall + (int64_t)pan * NB * NB;
+        for (int q = tid; q < NB * NB; q += kT) {
+            const int a = q % NB, b = q / NB;
+            Tp[q] = (a < nb && b < nb) ? T[a + b * (NB + 1)] : 0.0;
+        }
+        __syncthreads();
+    }
+}
+
+// Q = H_0 ... H_{m-3} applied to nv vectors (X, ld m) on the FP64 tensor
+// cores, a panel of NB reflectors at a time as I - V T V^T with the panels' T
+// from build_T: Y = V^T X, Y2 = T^T Y (trans: panels in order) or T Y (panels
+// in reverse), X -= V Y2, the reflectors read in place from C.  Y and Y2 are
+// NB x nv global scratch each.
+__device__ void wy_apply_t(const double* __restrict__ C, int m, const double* __restrict__ Tall, double* X, int nv,
+                           bool trans, double* Y, double* Y2, double* sA, double* sB) {
+    const int tid = threadIdx.x;
+    const int nref = m - 2;
+    const int npan = (int)t_panels(m);
+    if (npan == 0 || nv <= 0) return;
+    for (int pp = 0; pp < npan; ++pp) {
+        const int pan = trans ? pp : npan - 1 - pp;
+        const int j0 = pan * NB, nb = min(NB, nref - j0), r0 = j0 + 1, len = m - r0;
+        const double* Vb = C + r0 + (int64_t)j0 * m;
+        const double* Tp = Tall + (int64_t)pan * NB * NB;
         for (int c0 = 0; c0 < nv; c0 += TS)
-            tile_mma<true, false, MMA_SET, false>(Y, NB, 0, nullptr, 0, c0, NB, min(TS, nv - c0), Vp, len, nullptr,
-                                                  X + r0, m, nullptr, len, sA, sB);
+            tile_mma<true, false, MMA_SET, false, true, false>(Y, NB, 0, nullptr, 0, c0, nb, min(TS, nv - c0), Vb, m,
+                                                               nullptr, X + r0, m, nullptr, len, sA, sB);
         for (int64_t q = tid; q < (int64_t)NB * nv; q += kT) {
             const int a = (int)(q % NB), t = (int)(q / NB);
             const double* yc = Y + (int64_t)t * NB;
             double y = 0.0;
-            if (trans) {
-                for (int c2 = 0; c2 <= a; ++c2) y = fma(T[c2 + a * (NB + 1)], yc[c2], y);
-            } else {
-                for (int c2 = a; c2 < NB; ++c2) y = fma(T[a + c2 * (NB + 1)], yc[c2], y);
+            if (a < nb) {
+                if (trans) {
+                    for (int c2 = 0; c2 <= a; ++c2) y = fma(Tp[c2 + a * NB], yc[c2], y);
+                } else {
+                    for (int c2 = a; c2 < nb; ++c2) y = fma(Tp[a + c2 * NB], yc[c2], y);
+                }
             }
             Y2[q] = y;
         }
         __syncthreads();
         for (int c0 = 0; c0 < nv; c0 += TS)
             for (int i0 = 0; i0 < len; i0 += TS)
-                tile_mma<false, false, MMA_SUB, false>(X + r0, m, 0, nullptr, i0, c0, min(TS, len - i0),
-                                                       min(TS, nv - c0), Vp, len, nullptr, Y2, NB, nullptr, nb, sA, sB);
+                tile_mma<false, false, MMA_SUB, false, true, false>(X + r0, m, 0, nullptr, i0, c0, min(TS, len - i0),
+                                                                    min(TS, nv - c0), Vb, m, nullptr, Y2, NB, nullptr,
+                                                                    nb, sA, sB);
     }
 }
 
@@ -1269,8 +1308,8 @@ __device__ void stage_rows(const EigProb& p, const double* __restrict__ Ca, cons
                            const double* __restrict__ Ta, const double* __restrict__ Wa,
                            const double* __restrict__ Za, const int* __restrict__ own_cols,
                            const int* __restrict__ ipos, double* __restrict__ Ba, double* __restrict__ Qa,
-                           double* __restrict__ Va, double* __restrict__ e_out, double* __restrict__ fe_out,
-                           const StageSmem& sh) {
+                           double* __restrict__ Va, const double* __restrict__ Ka, double* __restrict__ e_out,
+                           double* __restrict__ fe_out, const StageSmem& sh) {
     double* sA = sh.sA;
     double* sB = sh.sB;
     const int m = p.m, no = p.nown, nb2 = 2 * no;
@@ -1318,9 +1357,9 @@ __device__ void stage_rows(const EigProb& p, const double* __restrict__ Ca, cons
             __syncthreads();
         }
     }
-    // R <- R Q: each row x becomes Q^T x (from order 160 on the tensor cores, the
-    // divide and conquer's Q and V arenas as scratch)
-    if (m >= kWyMmaMin) wy_apply_mma(C, m, tau, R, nb2, true, Qa + p.aoff, Va + p.aoff, sh.sD, sA, sB);
+    // R <- R Q: each row x becomes Q^T x (from order 64 as tile products with the
+    // panels' T, the divide and conquer's Q and V arenas as scratch)
+    if (m >= kWyMmaMin) wy_apply_t(C, m, Ka + p.koff, R, nb2, true, Qa + p.aoff, Va + p.aoff, sA, sB);
     else wy_apply(C, m, tau, R, nb2, true, WySmem{sA, sB});
     __syncthreads();
     // G^T = Z^T R^T (m x 2nown, column-major = G row-major)
@@ -1368,7 +1407,7 @@ __global__ void __launch_bounds__(kT, 1) k_eig_fused(
     const int* __restrict__ maps, const double* __restrict__ H, const double* __restrict__ S,
     double* __restrict__ Ca, double* __restrict__ La, double* __restrict__ Za, double* __restrict__ Qa,
     double* __restrict__ Va, double* __restrict__ Da, double* __restrict__ Ea, double* __restrict__ Ta,
-    double* __restrict__ Wa, double* __restrict__ Ba, const int* __restrict__ own_cols,
+    double* __restrict__ Wa, double* __restrict__ Ba, double* __restrict__ Ka, const int* __restrict__ own_cols,
     const int* __restrict__ ipos, double* __restrict__ e_out, double* __restrict__ fe_out,
     int* __restrict__ status) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -1393,7 +1432,11 @@ __global__ void __launch_bounds__(kT, 1) k_eig_fused(
             __syncthreads();
             if (!stage_dc(p, Da, Ea, Wa, Za, Qa, Va, sh)) st = kStNoConv;
             __syncthreads();
-            if (st == kStOk) stage_rows(p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, Qa, Va, e_out, fe_out, sh);
+            if (st == kStOk) {
+                if (p.m >= kWyMmaMin)
+                    build_T(Ca + p.aoff, p.m, Ta + p.voff, Ka + p.koff, 0, 1, Va + p.aoff, sh.sD, sh.sA, sh.sB);
+                stage_rows(p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, Qa, Va, Ka, e_out, fe_out, sh);
+            }
         }
         if (tid == 0) status[pi] = st;
         __syncthreads();
@@ -1413,6 +1456,7 @@ __global__ void __launch_bounds__(kT) k_eig_final(const EigProb* __restrict__ pr
                                                   const double* __restrict__ La, const double* __restrict__ Ta,
                                                   const double* __restrict__ Wa, const double* __restrict__ Za,
                                                   double* __restrict__ Qa, double* __restrict__ Va,
+                                                  const double* __restrict__ Ka,
                                                   const int* __restrict__ maps, const int* __restrict__ own_cols,
                                                   double* __restrict__ Ba, double mu, double* __restrict__ Ppk,
                                                   double* __restrict__ Pdense) {
@@ -1445,8 +1489,8 @@ __global__ void __launch_bounds__(kT) k_eig_final(const EigProb* __restrict__ pr
             tile_gemm<false>(W, m, 0, nullptr, r0, c0, min(TS, m - r0), min(TS, no - c0), Z, m, nullptr, W0, m, nullptr, m,
                              sA, sB);
     __syncthreads();
-    // Q W (from order 160 as tile products, the divide and conquer's arenas as scratch)
-    if (m >= kWyMmaMin) wy_apply_mma(C, m, tau, W, no, false, Qa + p.aoff, Va + p.aoff, sT, sA, sB);
+    // Q W (from order 64 as tile products, the divide and conquer's arenas as scratch)
+    if (m >= kWyMmaMin) wy_apply_t(C, m, Ka + p.koff, W, no, false, Qa + p.aoff, Va + p.aoff, sA, sB);
     else wy_apply(C, m, tau, W, no, false, WySmem{sA, sB});
     __syncthreads();
     // L^-T W: blocked back substitution
@@ -1494,24 +1538,89 @@ __global__ void __launch_bounds__(kT) k_eig_final(const EigProb* __restrict__ pr
 constexpr int kLargeMax = kEigLargeMax;   // largest order the cluster solver takes (its vectors live in shared memory)
 constexpr int kRedW = 2 * NB + 4;         // per-CTA partial sums of the tridiagonalisation
 constexpr int kRedVAv = 2 * NB + 1;       // slot of the partial v^T A v
-constexpr int kSyB = 4;                   // trailing tiles per round of the tridiagonalisation's A v
-static_assert(kSyB * (kT / 32 + 1) * TS <= 2 * kStageOp, "A v round buffers fit the tile staging");
 constexpr int kLgStages = 6;              // stage timestamps per problem: start, Cholesky, reduction, tridiag., D&C, rows
+constexpr int kLgSub = 7;                 // tridiagonalisation phase times per problem (ns, summed over its columns)
+constexpr int kLgStride = kLgStages + kLgSub;
 
+// Phase clock of one thread (rank 0, thread 0 of a cluster when stage times are
+// requested): lap(q) adds the time since the previous lap to acc[q].
+struct PhaseClock {
+    unsigned long long* acc;
+    unsigned long long t;
+    __device__ __forceinline__ static unsigned long long now() {
+        unsigned long long v;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+        return v;
+    }
+    __device__ __forceinline__ void start() {
+        if (acc) t = now();
+    }
+    __device__ __forceinline__ void lap(int q) {
+        if (acc) {
+            const unsigned long long n = now();
+            acc[q] += n - t;
+            t = n;
+        }
+    }
+};
+
+// Software barrier over the CTAs of a cooperative launch (all resident):
+// bar[0] counts arrivals, bar[1] is the generation.  The wait is bounded: after
+// kGridSpin polls the CTA records the failure in *err and goes on, and every
+// later barrier returns at once, so a kernel whose barrier gave up still ends
+// (its results are then discarded by the host, which reports the timeout).
+constexpr long long kGridSpin = 1ll << 24;
+
+__device__ void grid_barrier(unsigned* bar, int nblocks, int* err) {
+    __syncthreads();
+    if (threadIdx.x == 0 && *(volatile int*)err == 0) {
+        volatile unsigned* vb = bar;
+        const unsigned gen = vb[1];
+        __threadfence();
+        if (atomicAdd(&bar[0], 1u) == (unsigned)nblocks - 1) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            long long it = 0;
+            while (vb[1] == gen) {
+                if (++it > kGridSpin) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// The CTAs that solve one problem together: a thread-block cluster (bar null,
+// hardware barrier) or the whole grid of a cooperative launch (software barrier).
 struct Grp {
     int rank, size;
-    __device__ __forceinline__ void sync() const { cg::this_cluster().sync(); }
+    unsigned* bar;
+    int* err;
+    __device__ __forceinline__ void sync() const {
+        if (!bar) cg::this_cluster().sync();
+        else grid_barrier(bar, size, err);
+    }
 };
 
 // Per-problem scratch of a cluster solve (offsets in doubles from p.xoff).
 struct LgLayout {
-    int64_t ypart, red, V, W, dc, scal, total;
+    int64_t rowp, colp, red, V, W, dc, scal, total;
 };
+constexpr int kSegW = 64;    // columns of one A v work unit of the tridiagonalisation
+constexpr int kAvGrp = 8;    // columns whose loads are issued together in the A v units
 __host__ __device__ inline LgLayout lg_layout(int m, int G) {
     LgLayout L;
     int64_t o = 0;
-    L.ypart = o;
-    o += (int64_t)G * m;
+    L.rowp = o;   // row sums of the A v units: [segment][m]
+    o += (int64_t)((m + kSegW - 1) / kSegW + 1) * m;
+    L.colp = o;   // column sums of the A v units: [64-row block][m]
+    o += (int64_t)((m + TS - 1) / TS) * m;
     L.red = o;
     o += (int64_t)G * kRedW;
     L.V = o;
@@ -1530,21 +1639,20 @@ __host__ __device__ inline LgLayout lg_layout(int m, int G) {
 struct LgSmem {
     double *sA, *sB;           // tile staging
     double* sD;                // diagonal blocks (TS x (TS+1)), union with the vectors below
-    double *v, *y;             // tridiagonalisation: reflector and partial product (M each)
-    double *rowbuf, *colbuf;   // 16 x TS row partials, TS column sums of one tile
+    double *v, *y;             // tridiagonalisation: reflector and updated column (M each)
     double *pw, *pv, *wtv, *vtv, *wj, *vj;   // NB each
     double* red;               // kT / 32 + 2
     double* dsc;               // scalars
     int* ints;                 // 16
 };
 __host__ __device__ constexpr size_t lg_union_doubles(int M) {
-    return (size_t)2 * M + 16 * TS + TS + 6 * NB + kT / 32 + 2 + 8 > (size_t)TS * (TS + 1)
-               ? (size_t)2 * M + 16 * TS + TS + 6 * NB + kT / 32 + 2 + 8
-               : (size_t)TS * (TS + 1);
+    return (size_t)2 * M + 6 * NB + kT / 32 + 2 + 8 > (size_t)TS * (TS + 1) ? (size_t)2 * M + 6 * NB + kT / 32 + 2 + 8
+                                                                            : (size_t)TS * (TS + 1);
 }
 __host__ __device__ constexpr size_t lg_smem_bytes(int M) {
     return sizeof(double) * (2 * kStageOp + lg_union_doubles(M)) + sizeof(int) * 16;
 }
+static_assert(lg_smem_bytes(kLargeMax) <= 232448, "cluster solver shared memory within the per-CTA limit");
 __device__ LgSmem lg_smem(unsigned char* base, int M) {
     LgSmem s;
     double* d = reinterpret_cast<double*>(base);
@@ -1554,9 +1662,7 @@ __device__ LgSmem lg_smem(unsigned char* base, int M) {
     s.sD = u;
     s.v = u;
     s.y = u + M;
-    s.rowbuf = s.y + M;
-    s.colbuf = s.rowbuf + 16 * TS;
-    s.pw = s.colbuf + TS;
+    s.pw = s.y + M;
     s.pv = s.pw + NB;
     s.wtv = s.pv + NB;
     s.vtv = s.wtv + NB;
@@ -1588,7 +1694,7 @@ __device__ void lg_gather(const Grp& g, const EigProb& p, const int* __restrict_
         for (int i = threadIdx.x; i < m; i += kT) {
             const int64_t q = (int64_t)mp[i] + gj;
             C[i + (int64_t)j * m] = H[q];
-            L[i + (int64_t)j * m] = S[q];
+            if (p.kind == 0) L[i + (int64_t)j * m] = S[q];
         }
     }
 }
@@ -1742,9 +1848,15 @@ __device__ void lg_reduce(const Grp& g, const EigProb& p, const double* __restri
 // on this CTA's rows r >= j, from the summed partial products; the reflector
 // itself goes into column j - 1 below its leading 1.  Returns w at row j
 // (every CTA computes it).
+// Units of the A v pass for the trailing block from row/column s: tile rows
+// I in [s/64, nT), each cut into kSegW-column segments from column 64 (s/64).
+__device__ __forceinline__ int av_nseg(int I, int cstart) {
+    return ((I + 1) * TS - cstart + kSegW - 1) / kSegW;
+}
+
 __device__ double lg_finish_w(const Grp& g, int m, int j, int jp, double* __restrict__ A, double* __restrict__ V,
-                              double* __restrict__ W, const double* __restrict__ yp, const double* __restrict__ red,
-                              const LgSmem& sh) {
+                              double* __restrict__ W, const double* __restrict__ rowp,
+                              const double* __restrict__ colp, const double* __restrict__ red, const LgSmem& sh) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double tp = sh.dsc[0];
     double vAv = 0.0;
@@ -1753,9 +1865,15 @@ __device__ double lg_finish_w(const Grp& g, int m, int j, int jp, double* __rest
     for (int q = 0; q < jp; ++q) vw = fma(sh.vtv[q], sh.wtv[q], vw);
     const double ytv = vAv - 2.0 * vw;
     const double hc = 0.5 * tp * ytv;
+    const int cstart = (j / TS) * TS, nT = (m + TS - 1) / TS;
     auto w_at = [&](int r) {
+        // y_r = its row sums over the segments of its tile row, then its column
+        // sums over the tile rows at and below its own, in that fixed order
+        const int Ir = r / TS;
         double y = 0.0;
-        for (int q = 0; q < g.size; ++q) y += yp[(int64_t)q * m + r];
+        const int ns = av_nseg(Ir, cstart);
+        for (int q = 0; q < ns; ++q) y += rowp[(int64_t)q * m + r];
+        for (int I = Ir; I < nT; ++I) y += colp[(int64_t)I * m + r];
         for (int q = 0; q < jp; ++q) y -= V[r + (int64_t)q * m] * sh.wtv[q] + W[r + (int64_t)q * m] * sh.vtv[q];
         return tp * (y - hc * sh.v[r]);
     };
@@ -1776,14 +1894,18 @@ __device__ double lg_finish_w(const Grp& g, int m, int j, int jp, double* __rest
 }
 
 __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca, double* __restrict__ Da,
-                         double* __restrict__ Ea, double* __restrict__ Ta, double* __restrict__ X, const LgSmem& sh) {
+                         double* __restrict__ Ea, double* __restrict__ Ta, double* __restrict__ X, const LgSmem& sh,
+                         unsigned long long* tsub) {
     const int m = p.m, G = g.size, rk = g.rank;
+    PhaseClock pc{(g.rank == 0 && threadIdx.x == 0) ? tsub : nullptr, 0};
+    pc.start();
     double* A = Ca + p.aoff;
     double* d = Da + p.voff;
     double* e = Ea + p.voff;
     double* tau = Ta + p.voff;
     const LgLayout lay = lg_layout(m, G);
-    double* yp = X + lay.ypart;
+    double* rowp = X + lay.rowp;
+    double* colp = X + lay.colp;
     double* red = X + lay.red;
     double* V = X + lay.V;
     double* W = X + lay.W;
@@ -1797,7 +1919,7 @@ __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca
             const int j = j0 + jj;
             // ---- phase A: finish w of the previous column, update column j on own rows
             double wrow = 0.0;
-            if (jj > 0) wrow = lg_finish_w(g, m, j, jj - 1, A, V, W, yp, red, sh);
+            if (jj > 0) wrow = lg_finish_w(g, m, j, jj - 1, A, V, W, rowp, colp, red, sh);
             if (tid < jj) {
                 const int q = tid;
                 sh.wj[q] = (q == jj - 1) ? wrow : W[j + (int64_t)q * m];
@@ -1834,7 +1956,9 @@ __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca
                 part = warp_sum(part);
                 if (lane == 0) red[rk * kRedW + ((q < jj) ? 1 + q : 1 + NB + (q - jj))] = part;
             }
+            pc.lap(0);
             g.sync();
+            pc.lap(1);
             // ---- phase B: reflector, then y = A v over the trailing lower tiles
             if (tid < jj) {
                 double a = 0.0, b = 0.0;
@@ -1886,93 +2010,77 @@ __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca
                 const int r = ch * 32 + lane;
                 if (r >= s && r < m) V[r + (int64_t)jj * m] = v[r];
             }
-            const int I0 = s / TS, nbt = nT - I0;
-            const int64_t ntiles = (int64_t)nbt * (nbt + 1) / 2;
-            // kSyB tiles per round: every load of the round is issued before any
-            // arithmetic, then one barrier; the per-tile row and column sums are
-            // added by 64 threads, thread t only ever touching positions = t mod 64
-            // (tile origins are multiples of 64), in tile order: no two threads
-            // write one position and the sums do not depend on scheduling
-            double* rowbuf = sh.sA;                        // [kSyB][16][TS], in the tile staging
-            double* colbuf = sh.sA + kSyB * (kT / 32) * TS;   // [kSyB][TS]
-            for (int64_t base = rk; base < ntiles; base += (int64_t)G * kSyB) {
-                double a0[kSyB][4], a1[kSyB][4];
-                int rbs[kSyB], cbs[kSyB];
-#pragma unroll
-                for (int b = 0; b < kSyB; ++b) {
-                    const int64_t idx = base + (int64_t)b * G;
-                    int I = -1, J = -1;
-                    if (idx < ntiles) {
-                        int bi, bj;
-                        tri_decode(idx, bi, bj);
-                        I = I0 + bi;
-                        J = I0 + bj;
-                    }
-                    rbs[b] = I * TS;
-                    cbs[b] = J * TS;
-                    const bool diag = (I == J);
-                    const int ra = I * TS + lane, rb = ra + 32;
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int c = J * TS + warp * 4 + u;
-                        a0[b][u] = 0.0;
-                        a1[b][u] = 0.0;
-                        if (I >= 0 && c < m && c >= s) {
-                            if (ra < m && (!diag || ra >= c)) a0[b][u] = A[ra + (int64_t)c * m];
-                            if (rb < m && (!diag || rb >= c)) a1[b][u] = A[rb + (int64_t)c * m];
-                        }
-                    }
-                }
-#pragma unroll
-                for (int b = 0; b < kSyB; ++b) {
-                    if (rbs[b] < 0) continue;
-                    const bool diag = rbs[b] == cbs[b];
-                    const int ra = rbs[b] + lane, rb = ra + 32;
-                    const double va = (ra < m) ? v[ra] : 0.0, vb = (rb < m) ? v[rb] : 0.0;
-                    double rp0 = 0.0, rp1 = 0.0;
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int c = cbs[b] + warp * 4 + u;
-                        const double vc = (c < m) ? v[c] : 0.0;
-                        rp0 = fma(a0[b][u], vc, rp0);
-                        rp1 = fma(a1[b][u], vc, rp1);
-                        double cp = ((diag && ra == c) ? 0.0 : a0[b][u] * va) + ((diag && rb == c) ? 0.0 : a1[b][u] * vb);
-                        cp = warp_sum(cp);
-                        if (lane == 0) colbuf[b * TS + warp * 4 + u] = cp;
-                    }
-                    rowbuf[(b * (kT / 32) + warp) * TS + lane] = rp0;
-                    rowbuf[(b * (kT / 32) + warp) * TS + lane + 32] = rp1;
-                }
-                __syncthreads();
-                if (tid < TS) {
-                    for (int b = 0; b < kSyB; ++b) {
-                        if (rbs[b] < 0) break;
-                        double acc = 0.0;
-                        for (int w2 = 0; w2 < kT / 32; ++w2) acc += rowbuf[(b * (kT / 32) + w2) * TS + tid];
-                        const bool diag = rbs[b] == cbs[b];
-                        if (diag) acc += colbuf[b * TS + tid];
-                        const int r = rbs[b] + tid;
-                        if (r >= s && r < m) yl[r] += acc;
-                        if (!diag) {
-                            const int c = cbs[b] + tid;
-                            if (c >= s && c < m) yl[c] += colbuf[b * TS + tid];
-                        }
-                    }
-                }
-                __syncthreads();
-            }
+            pc.lap(2);
+            // A v over the trailing lower triangle, one pass: every warp streams
+            // its own units (64 rows x kSegW columns of one tile row) without a
+            // barrier, lane holding rows I*64 + lane and + 32: the row sums stay
+            // in registers for the unit, each column's sum is a warp reduction;
+            // both go to their own slots (rowp[segment][r], colp[tile row][c]),
+            // summed in a fixed order when w is formed.  v^T A v comes from the
+            // same sums.
             {
-                double part = 0.0;
-                for (int r = s + tid; r < m; r += kT) part = fma(v[r], yl[r], part);
-                part = cta_sum(part, sh.red);
+                const int I0 = s / TS, cstart = I0 * TS;
+                const int gw = rk * (kT / 32) + warp, nw = G * (kT / 32);
+                double vav = 0.0;
+                int I = I0, ubase = 0;
+                for (int u = gw;; u += nw) {
+                    while (I < nT && u >= ubase + av_nseg(I, cstart)) {
+                        ubase += av_nseg(I, cstart);
+                        ++I;
+                    }
+                    if (I >= nT) break;
+                    const int seg = u - ubase;
+                    const int c_lo = cstart + seg * kSegW;
+                    const int c_hi = min(min(c_lo + kSegW, (I + 1) * TS), m);
+                    const int r0 = I * TS + lane, r1 = r0 + 32;
+                    const double v0 = (r0 < m) ? v[r0] : 0.0, v1 = (r1 < m) ? v[r1] : 0.0;
+                    const double* A0 = A + r0;
+                    const double* A1 = A + r1;
+                    double rp0 = 0.0, rp1 = 0.0;
+                    for (int cb = c_lo; cb < c_hi; cb += 32) {
+                        double mycol = 0.0;
+#pragma unroll 1
+                        for (int g8 = 0; g8 < 32; g8 += kAvGrp) {
+                            double a0[kAvGrp], a1[kAvGrp];
+#pragma unroll
+                            for (int u8 = 0; u8 < kAvGrp; ++u8) {
+                                const int c = cb + g8 + u8;
+                                const bool cok = c < c_hi && c >= s;
+                                a0[u8] = (cok && r0 < m && c <= r0) ? A0[(int64_t)c * m] : 0.0;
+                                a1[u8] = (cok && r1 < m && c <= r1) ? A1[(int64_t)c * m] : 0.0;
+                            }
+#pragma unroll
+                            for (int u8 = 0; u8 < kAvGrp; ++u8) {
+                                const int c = cb + g8 + u8;
+                                const double vc = (c < c_hi) ? v[c] : 0.0;
+                                rp0 = fma(a0[u8], vc, rp0);
+                                rp1 = fma(a1[u8], vc, rp1);
+                                double cp = ((c < r0) ? a0[u8] * v0 : 0.0) + ((c < r1) ? a1[u8] * v1 : 0.0);
+                                cp = warp_sum(cp);
+                                if (lane == g8 + u8) mycol = cp;
+                            }
+                        }
+                        const int c = cb + lane;
+                        if (c < c_hi) {
+                            colp[(int64_t)I * m + c] = mycol;
+                            vav = fma(v[c], mycol, vav);
+                        }
+                    }
+                    if (r0 < m) rowp[(int64_t)seg * m + r0] = rp0;
+                    if (r1 < m) rowp[(int64_t)seg * m + r1] = rp1;
+                    vav = fma(v0, rp0, fma(v1, rp1, vav));
+                }
+                pc.lap(3);
+                const double part = cta_sum(vav, sh.red);
                 if (tid == 0) red[rk * kRedW + kRedVAv] = part;
             }
-            for (int r = s + tid; r < m; r += kT) yp[(int64_t)rk * m + r] = yl[r];
+            pc.lap(4);
             g.sync();
+            pc.lap(5);
         }
         // ---- panel end: w of the last column, then the trailing block
         const int j1 = j0 + nb;
-        lg_finish_w(g, m, j1, nb - 1, A, V, W, yp, red, sh);
+        lg_finish_w(g, m, j1, nb - 1, A, V, W, rowp, colp, red, sh);
         g.sync();
         if (j1 < m) {
             const int nt = (m - j1 + TS - 1) / TS;
@@ -1987,6 +2095,7 @@ __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca
             }
         }
         g.sync();
+        pc.lap(6);
     }
     if (rk == 0 && tid == 0) {
         d[m - 1] = A[(m - 1) + (int64_t)(m - 1) * m];
@@ -1996,14 +2105,15 @@ __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca
 
 // ---------------------------------------------------------------------------
 // Divide and conquer on a cluster.  A merge is run by one CTA (Split{0, 1,
-// false}) or by the whole cluster (Split{rank, G, true}); its per-element
+// false}) or by the whole group (Split{rank, G, true}); its per-element
 // arrays sit at offset lo of the problem's arrays, its Q and V blocks at
 // column lo of the Q and V arenas, so merges of one level never overlap.
 struct Split {
     int part, nparts;
     bool coop;
+    const Grp* g;
     __device__ __forceinline__ void sync() const {
-        if (coop) cg::this_cluster().sync();
+        if (coop) g->sync();
         else __syncthreads();
     }
     __device__ __forceinline__ int first() const { return part * kT + (int)threadIdx.x; }
@@ -2281,14 +2391,14 @@ __device__ bool lg_dc(const Grp& g, const EigProb& p, const double* __restrict__
             for (int q = g.rank; q < nm; q += g.size) {
                 const int lo = (int)(((int64_t)q * m) >> lev), hi = (int)(((int64_t)(q + 1) * m) >> lev);
                 const int mid = (int)(((int64_t)(2 * q + 1) * m) >> (lev + 1));
-                dc_merge(Split{0, 1, false}, m, lo, mid, hi, eo[mid - 1], S, Z, Qa + p.aoff + (int64_t)lo * m,
+                dc_merge(Split{0, 1, false, &g}, m, lo, mid, hi, eo[mid - 1], S, Z, Qa + p.aoff + (int64_t)lo * m,
                          Va + p.aoff + (int64_t)lo * m, scal + 8 + 8 * q, sh.sA, sh.sB);
             }
         } else {
             for (int q = 0; q < nm; ++q) {
                 const int lo = (int)(((int64_t)q * m) >> lev), hi = (int)(((int64_t)(q + 1) * m) >> lev);
                 const int mid = (int)(((int64_t)(2 * q + 1) * m) >> (lev + 1));
-                dc_merge(Split{g.rank, g.size, true}, m, lo, mid, hi, eo[mid - 1], S, Z,
+                dc_merge(Split{g.rank, g.size, true, &g}, m, lo, mid, hi, eo[mid - 1], S, Z,
                          Qa + p.aoff + (int64_t)lo * m, Va + p.aoff + (int64_t)lo * m, scal + 8 + 8 * q, sh.sA, sh.sB);
             }
         }
@@ -2303,17 +2413,14 @@ __device__ bool lg_dc(const Grp& g, const EigProb& p, const double* __restrict__
 // substitution), applies Q^T to them, and the product with Z is tiled over
 // the cluster.
 // Per-CTA scratch of the tile-product reflectors in the Q arena (free after the
-// divide and conquer): V panel (m x NB), Y and T Y (NB x nv each) and the
-// panel's Gram.
-__host__ __device__ inline int64_t lg_wy_stride(int m, int nv) {
-    return ((int64_t)NB * m + 2 * (int64_t)NB * nv + NB * NB + 1) & ~int64_t(1);
-}
+// divide and conquer): Y and T Y, NB x nv each.
+__host__ __device__ inline int64_t lg_wy_stride(int nv) { return 2 * (int64_t)NB * nv; }
 
 __device__ void lg_rows(const Grp& g, const EigProb& p, const double* __restrict__ Ca,
                         const double* __restrict__ La, const double* __restrict__ Ta, const double* __restrict__ Wa,
                         const double* __restrict__ Za, const int* __restrict__ own_cols, const int* __restrict__ ipos,
-                        double* __restrict__ Ba, double* __restrict__ Qa, double* __restrict__ e_out,
-                        double* __restrict__ fe_out, const LgSmem& sh) {
+                        double* __restrict__ Ba, double* __restrict__ Qa, const double* __restrict__ Ka,
+                        double* __restrict__ e_out, double* __restrict__ fe_out, const LgSmem& sh) {
     const int m = p.m, no = p.nown, nb2 = 2 * no;
     const double* C = Ca + p.aoff;
     const double* L = La + p.aoff;
@@ -2335,9 +2442,9 @@ __device__ void lg_rows(const Grp& g, const EigProb& p, const double* __restrict
     const int s0 = max(u0, no);
     if (s0 < u1) trsm_cols(true, L, m, R + (int64_t)s0 * m, m, 0, u1 - s0, sh.sD, sh.sA, sh.sB);
     if (u1 > u0) {
-        double* scr = Qa + p.aoff + (int64_t)g.rank * lg_wy_stride(m, per);
-        wy_apply_mma(C, m, tau, R + (int64_t)u0 * m, u1 - u0, true, scr, scr + (int64_t)NB * m,
-                     sh.sD + TS * (TS + 1), sh.sA, sh.sB);
+        double* scr = Qa + p.aoff + (int64_t)g.rank * lg_wy_stride(per);
+        wy_apply_t(C, m, Ka + p.koff, R + (int64_t)u0 * m, u1 - u0, true, scr, scr + (int64_t)NB * per, sh.sA,
+                   sh.sB);
     }
     g.sync();
     {
@@ -2358,49 +2465,107 @@ __device__ void lg_rows(const Grp& g, const EigProb& p, const double* __restrict
     }
 }
 
+// Every stage of one problem on a group of CTAs.  mode 0: the submatrix
+// method's eigenvalues, fe weights and owned rows of U (lg_rows); mode 1: all
+// eigenvectors U = L^-T Q Z into Uout (m x m, column-major; L = I for the
+// standard problem) and the eigenvalues into wout (ascending).
+__device__ void eig_group_solve(const Grp& g, int pi, const EigProb& p, const LgSmem& sh, int mode,
+                                const int* __restrict__ maps, const double* __restrict__ H,
+                                const double* __restrict__ S, double* __restrict__ Ca, double* __restrict__ La,
+                                double* __restrict__ Za, double* __restrict__ Qa, double* __restrict__ Va,
+                                double* __restrict__ Da, double* __restrict__ Ea, double* __restrict__ Ta,
+                                double* __restrict__ Wa, double* __restrict__ Ba, double* __restrict__ Ka,
+                                double* __restrict__ Xa, const int* __restrict__ own_cols, const int* __restrict__ ipos,
+                                double* __restrict__ e_out, double* __restrict__ fe_out, double* __restrict__ Uout,
+                                double* __restrict__ wout, int* __restrict__ status,
+                                unsigned long long* __restrict__ tstage) {
+    double* X = Xa + p.xoff;
+    const int m = p.m;
+    // stage boundaries (global timer, ns) for the print-level-2 stage summary
+    auto mark = [&](int q) {
+        if (tstage && g.rank == 0 && threadIdx.x == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            tstage[(int64_t)pi * kLgStride + q] = t;
+        }
+    };
+    mark(0);
+    lg_gather(g, p, maps, H, S, Ca, La);
+    g.sync();
+    int st = kStOk;
+    if (p.kind == 0) st = lg_potrf(g, m, La + p.aoff, sh);
+    g.sync();
+    mark(1);
+    if (st == kStOk) {
+        if (p.kind == 0) lg_reduce(g, p, La, Ca, sh);
+        mark(2);
+        lg_sytrd(g, p, Ca, Da, Ea, Ta, X, sh, tstage ? tstage + (int64_t)pi * kLgStride + kLgStages : nullptr);
+        g.sync();
+        mark(3);
+        if (!lg_dc(g, p, Da, Ea, Wa, Za, Qa, Va, X, sh)) st = kStNoConv;
+        g.sync();
+        mark(4);
+        if (st == kStOk) {
+            build_T(Ca + p.aoff, m, Ta + p.voff, Ka + p.koff, g.rank, g.size, Va + p.aoff + (int64_t)g.rank * NB * NB,
+                    sh.sD, sh.sA, sh.sB);
+            g.sync();
+            if (mode == 0) {
+                lg_rows(g, p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, Qa, Ka, e_out, fe_out, sh);
+            } else {
+                const int per = (m + g.size - 1) / g.size;
+                const int t0 = min(m, g.rank * per), t1 = min(m, t0 + per);
+                for (int64_t q = (int64_t)t0 * m + threadIdx.x; q < (int64_t)t1 * m; q += kT) Uout[q] = Za[p.aoff + q];
+                __syncthreads();
+                if (t1 > t0) {
+                    double* scr = Qa + p.aoff + (int64_t)g.rank * lg_wy_stride(per);
+                    wy_apply_t(Ca + p.aoff, m, Ka + p.koff, Uout + (int64_t)t0 * m, t1 - t0, false, scr,
+                               scr + (int64_t)NB * per, sh.sA, sh.sB);
+                    __syncthreads();
+                    if (p.kind == 0)
+                        trsm_cols(false, La + p.aoff, m, Uout + (int64_t)t0 * m, m, 0, t1 - t0, sh.sD, sh.sA, sh.sB);
+                }
+                for (int j = g.rank * kT + threadIdx.x; j < m; j += g.size * kT) wout[j] = Wa[p.voff + j];
+            }
+        }
+    }
+    mark(5);
+    if (g.rank == 0 && threadIdx.x == 0) status[pi] = st;
+}
+
 // One cluster per submatrix above kEigBatchMax (order[] largest first).
 __global__ void __launch_bounds__(kT, 1) k_eig_cluster(
     const EigProb* __restrict__ probs, const int* __restrict__ order, int M, const int* __restrict__ maps,
     const double* __restrict__ H, const double* __restrict__ S, double* __restrict__ Ca, double* __restrict__ La,
     double* __restrict__ Za, double* __restrict__ Qa, double* __restrict__ Va, double* __restrict__ Da,
     double* __restrict__ Ea, double* __restrict__ Ta, double* __restrict__ Wa, double* __restrict__ Ba,
-    double* __restrict__ Xa, const int* __restrict__ own_cols, const int* __restrict__ ipos,
+    double* __restrict__ Ka, double* __restrict__ Xa, const int* __restrict__ own_cols, const int* __restrict__ ipos,
     double* __restrict__ e_out, double* __restrict__ fe_out, int* __restrict__ status,
-    unsigned long long* __restrict__ tstage) {
+    unsigned long long* __restrict__ tstage, int mode, double* __restrict__ Uout, double* __restrict__ wout) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const LgSmem sh = lg_smem(smraw, M);
     cg::cluster_group cl = cg::this_cluster();
-    const Grp g{(int)cl.block_rank(), (int)cl.num_blocks()};
+    const Grp g{(int)cl.block_rank(), (int)cl.num_blocks(), nullptr, nullptr};
     const int pi = order[blockIdx.x / g.size];
     const EigProb p = probs[pi];
-    double* X = Xa + p.xoff;
-    // stage boundaries (global timer, ns) for the print-level-2 stage summary
-    auto mark = [&](int q) {
-        if (tstage && g.rank == 0 && threadIdx.x == 0) {
-            unsigned long long t;
-            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-            tstage[(int64_t)pi * kLgStages + q] = t;
-        }
-    };
-    mark(0);
-    lg_gather(g, p, maps, H, S, Ca, La);
-    g.sync();
-    int st = lg_potrf(g, p.m, La + p.aoff, sh);
-    g.sync();
-    mark(1);
-    if (st == kStOk) {
-        lg_reduce(g, p, La, Ca, sh);
-        mark(2);
-        lg_sytrd(g, p, Ca, Da, Ea, Ta, X, sh);
-        g.sync();
-        mark(3);
-        if (!lg_dc(g, p, Da, Ea, Wa, Za, Qa, Va, X, sh)) st = kStNoConv;
-        g.sync();
-        mark(4);
-        if (st == kStOk) lg_rows(g, p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, Qa, e_out, fe_out, sh);
-    }
-    mark(5);
-    if (g.rank == 0 && threadIdx.x == 0) status[pi] = st;
+    eig_group_solve(g, pi, p, sh, mode, maps, H, S, Ca, La, Za, Qa, Va, Da, Ea, Ta, Wa, Ba, Ka, Xa, own_cols, ipos,
+                    e_out, fe_out, Uout, wout, status, tstage);
+}
+
+// One problem on the whole grid of a cooperative launch (software barrier).
+__global__ void __launch_bounds__(kT, 1) k_eig_grid(
+    const EigProb* __restrict__ probs, int pi, int M, int mode, const int* __restrict__ maps,
+    const double* __restrict__ H, const double* __restrict__ S, double* __restrict__ Ca, double* __restrict__ La,
+    double* __restrict__ Za, double* __restrict__ Qa, double* __restrict__ Va, double* __restrict__ Da,
+    double* __restrict__ Ea, double* __restrict__ Ta, double* __restrict__ Wa, double* __restrict__ Ba,
+    double* __restrict__ Ka, double* __restrict__ Xa, const int* __restrict__ own_cols, const int* __restrict__ ipos,
+    double* __restrict__ e_out, double* __restrict__ fe_out, double* __restrict__ Uout, double* __restrict__ wout,
+    int* __restrict__ status, unsigned* __restrict__ bar, int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const LgSmem sh = lg_smem(smraw, M);
+    const Grp g{(int)blockIdx.x, (int)gridDim.x, bar, err};
+    const EigProb p = probs[pi];
+    eig_group_solve(g, pi, p, sh, mode, maps, H, S, Ca, La, Za, Qa, Va, Da, Ea, Ta, Wa, Ba, Ka, Xa, own_cols, ipos,
+                    e_out, fe_out, Uout, wout, status, nullptr);
 }
 
 // Owned columns of P_k at mu on the cluster (the large-submatrix form of
@@ -2409,16 +2574,16 @@ __global__ void __launch_bounds__(kT, 1) k_eig_cluster(
 __global__ void __launch_bounds__(kT, 1) k_eig_final_cluster(
     const EigProb* __restrict__ probs, const int* __restrict__ order, const double* __restrict__ Ca,
     const double* __restrict__ La, const double* __restrict__ Ta, const double* __restrict__ Wa,
-    const double* __restrict__ Za, double* __restrict__ Qa, const int* __restrict__ maps,
-    const int* __restrict__ own_cols, double* __restrict__ Ba, double mu, double* __restrict__ Ppk,
-    double* __restrict__ Pdense) {
+    const double* __restrict__ Za, double* __restrict__ Qa, const double* __restrict__ Ka,
+    const int* __restrict__ maps, const int* __restrict__ own_cols, double* __restrict__ Ba, double mu,
+    double* __restrict__ Ppk, double* __restrict__ Pdense) {
     extern __shared__ __align__(16) unsigned char smf[];
     double* sA = reinterpret_cast<double*>(smf);
     double* sB = sA + kStageOp;
     double* sD = sB + kStageOp;
     double* sT = sD + TS * (TS + 1);
     cg::cluster_group cl = cg::this_cluster();
-    const Grp g{(int)cl.block_rank(), (int)cl.num_blocks()};
+    const Grp g{(int)cl.block_rank(), (int)cl.num_blocks(), nullptr, nullptr};
     const EigProb p = probs[order[blockIdx.x / g.size]];
     const int m = p.m, no = p.nown;
     const double* C = Ca + p.aoff;
@@ -2449,8 +2614,8 @@ __global__ void __launch_bounds__(kT, 1) k_eig_final_cluster(
     const int per = (no + g.size - 1) / g.size;
     const int t0 = min(no, g.rank * per), t1 = min(no, t0 + per);
     if (t1 > t0) {
-        double* scr = Qa + p.aoff + (int64_t)g.rank * lg_wy_stride(m, per);
-        wy_apply_mma(C, m, tau, W + (int64_t)t0 * m, t1 - t0, false, scr, scr + (int64_t)NB * m, sT, sA, sB);
+        double* scr = Qa + p.aoff + (int64_t)g.rank * lg_wy_stride(per);
+        wy_apply_t(C, m, Ka + p.koff, W + (int64_t)t0 * m, t1 - t0, false, scr, scr + (int64_t)NB * per, sA, sB);
         __syncthreads();
         trsm_cols(false, L, m, W + (int64_t)t0 * m, m, 0, t1 - t0, sD, sA, sB);
     }
@@ -2475,14 +2640,14 @@ struct EigBatch {
     int G = 1;                    // CTAs per cluster of the large-submatrix solver
     int nsmall = 0, nlarge = 0;
     std::vector<EigProb> hp;
-    DevBuf probs, order, order_l, counter, Ca, La, Za, Qa, Va, Da, Ea, Ta, Wa, Ba, Xa, status, tstage;
+    DevBuf probs, order, order_l, counter, Ca, La, Za, Qa, Va, Da, Ea, Ta, Wa, Ba, Xa, Ka, status, tstage;
     int prl = 0;
     cudaStream_t side = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~EigBatch() {
         if (side) cudaStreamSynchronize(side);
         for (DevBuf* b : {&probs, &order, &order_l, &counter, &Ca, &La, &Za, &Qa, &Va, &Da, &Ea, &Ta, &Wa, &Ba, &Xa,
-                          &status, &tstage})
+                          &Ka, &status, &tstage})
             b->release();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -2501,6 +2666,8 @@ void eig_setup_attrs() {
         PTB_CUDA(cudaFuncSetAttribute(k_eig_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         PTB_CUDA(cudaFuncSetAttribute(k_eig_final_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         PTB_CUDA(cudaFuncSetAttribute(k_eig_final_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinalSmem));
+        PTB_CUDA(cudaFuncSetAttribute(k_eig_grid, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)lg_smem_bytes(kLargeMax)));
         PTB_CUDA(cudaFuncSetAttribute(k_eig_final, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinalSmem));
         return true;
     }();
@@ -2585,7 +2752,7 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
     bool any_large = false;
     for (const EigProbHost& q : probs) any_large = any_large || q.m > kEigBatchMax;
     eb->G = any_large ? eig_cluster_size(c) : 1;
-    int64_t asz = 0, vsz = 0, bsz = 0, psz = 0, xsz = 0;
+    int64_t asz = 0, vsz = 0, bsz = 0, psz = 0, xsz = 0, ksz = 0;
     std::vector<int> ord_s, ord_l;
     for (const EigProbHost& q : probs) {
         PTB_CHECK(q.m >= 1 && q.m <= kLargeMax, PTBGPU_EINVAL, "submatrix %d of order %d outside the eigensolver (1..%d)",
@@ -2605,6 +2772,8 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
         p.voff = vsz;
         p.boff = bsz;
         p.xoff = xsz;
+        p.koff = ksz;
+        ksz += t_panels(q.m) * NB * NB;
         asz += (int64_t)q.m * q.m;
         vsz += q.m;
         bsz += 4 * (int64_t)q.nown * q.m;
@@ -2626,6 +2795,7 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
     for (DevBuf* b : {&eb->Da, &eb->Ea, &eb->Ta, &eb->Wa}) b->reserve(sizeof(double) * vsz);
     eb->Ba.reserve(sizeof(double) * std::max<int64_t>(bsz, 1));
     eb->Xa.reserve(sizeof(double) * std::max<int64_t>(xsz, 2));
+    eb->Ka.reserve(sizeof(double) * std::max<int64_t>(ksz, 2));
     eb->status.reserve(sizeof(int) * np);
     PTB_CUDA(cudaMemcpyAsync(eb->probs.ptr, eb->hp.data(), sizeof(EigProb) * np, cudaMemcpyHostToDevice, s));
     PTB_CUDA(cudaMemsetAsync(eb->status.ptr, 0, sizeof(int) * np, s));
@@ -2652,8 +2822,8 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
         PTB_CUDA(cudaEventCreateWithFlags(&eb->ev1, cudaEventDisableTiming));
         unsigned long long* dts = nullptr;
         if (prl >= 2) {
-            eb->tstage.reserve(sizeof(unsigned long long) * kLgStages * np);
-            PTB_CUDA(cudaMemsetAsync(eb->tstage.ptr, 0, sizeof(unsigned long long) * kLgStages * np, s));
+            eb->tstage.reserve(sizeof(unsigned long long) * kLgStride * np);
+            PTB_CUDA(cudaMemsetAsync(eb->tstage.ptr, 0, sizeof(unsigned long long) * kLgStride * np, s));
             dts = eb->tstage.as<unsigned long long>();
         }
         PTB_CUDA(cudaEventRecord(eb->ev0, s));
@@ -2662,7 +2832,8 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
                          (const int*)eb->order_l.as<int>(), kLargeMax, d_maps, H, S, eb->Ca.as<double>(),
                          eb->La.as<double>(), eb->Za.as<double>(), eb->Qa.as<double>(), eb->Va.as<double>(),
                          eb->Da.as<double>(), eb->Ea.as<double>(), eb->Ta.as<double>(), eb->Wa.as<double>(),
-                         eb->Ba.as<double>(), eb->Xa.as<double>(), d_own_cols, d_ipos, d_e, d_fe, dst, dts);
+                         eb->Ba.as<double>(), eb->Ka.as<double>(), eb->Xa.as<double>(), d_own_cols, d_ipos, d_e, d_fe,
+                         dst, dts, 0, (double*)nullptr, (double*)nullptr);
         count_launch();
         PTB_CUDA(cudaEventRecord(eb->ev1, eb->side));
         log_line(prl, 2, " * submatrix cluster eigensolver: %d problems above order %d, clusters of %d CTAs",
@@ -2678,8 +2849,8 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
         k_eig_fused<<<grid, kT, stage_smem_bytes(Ms), s>>>(
             dp, eb->order.as<int>(), eb->nsmall, eb->counter.as<int>(), Ms, d_maps, H, S, eb->Ca.as<double>(),
             eb->La.as<double>(), eb->Za.as<double>(), eb->Qa.as<double>(), eb->Va.as<double>(), eb->Da.as<double>(),
-            eb->Ea.as<double>(), eb->Ta.as<double>(), eb->Wa.as<double>(), eb->Ba.as<double>(), d_own_cols, d_ipos,
-            d_e, d_fe, dst);
+            eb->Ea.as<double>(), eb->Ta.as<double>(), eb->Wa.as<double>(), eb->Ba.as<double>(), eb->Ka.as<double>(),
+            d_own_cols, d_ipos, d_e, d_fe, dst);
         count_launch();
         PTB_CUDA(cudaGetLastError());
     }
@@ -2702,7 +2873,7 @@ void eig_batch_check(ptbgpu_ctx* c, EigBatch& eb) {
     if (eb.prl >= 2 && eb.nlarge > 0 && eb.tstage.ptr) {
         // per stage: summed over the large submatrices and the longest one, then
         // the span from the first cluster's start to the last one's end
-        std::vector<unsigned long long> ts((size_t)kLgStages * np);
+        std::vector<unsigned long long> ts((size_t)kLgStride * np);
         PTB_CUDA(cudaMemcpy(ts.data(), eb.tstage.ptr, sizeof(unsigned long long) * ts.size(), cudaMemcpyDeviceToHost));
         static const char* names[kLgStages - 1] = {"gather + Cholesky", "reduction", "tridiagonalisation",
                                                    "divide and conquer", "owned rows"};
@@ -2710,7 +2881,7 @@ void eig_batch_check(ptbgpu_ctx* c, EigBatch& eb) {
         unsigned long long t_lo = ~0ull, t_hi = 0;
         for (int q = 0; q < np; ++q) {
             if (eb.hp[q].m <= kEigBatchMax) continue;
-            const unsigned long long* t = &ts[(size_t)q * kLgStages];
+            const unsigned long long* t = &ts[(size_t)q * kLgStride];
             t_lo = std::min(t_lo, t[0]);
             t_hi = std::max(t_hi, t[kLgStages - 1]);
             for (int k = 0; k + 1 < kLgStages; ++k) {
@@ -2721,6 +2892,14 @@ void eig_batch_check(ptbgpu_ctx* c, EigBatch& eb) {
         }
         for (int k = 0; k + 1 < kLgStages; ++k)
             log_line(eb.prl, 2, " * cluster eigensolver %-22s sum %10.3f ms, longest %9.3f ms", names[k], sum[k], mx[k]);
+        static const char* sub[kLgSub] = {"column update", "barrier 1", "reflector", "A v tiles", "A v partials",
+                                          "barrier 2", "panel end"};
+        for (int k = 0; k < kLgSub; ++k) {
+            double t = 0.0;
+            for (int q = 0; q < np; ++q)
+                if (eb.hp[q].m > kEigBatchMax) t += (double)ts[(size_t)q * kLgStride + kLgStages + k] * 1e-6;
+            log_line(eb.prl, 2, " *   tridiagonalisation %-14s sum %10.3f ms", sub[k], t);
+        }
         log_line(eb.prl, 2, " * cluster eigensolver span %10.3f ms (%d submatrices, clusters of %d)",
                  t_hi > t_lo ? (double)(t_hi - t_lo) * 1e-6 : 0.0, eb.nlarge, eb.G);
     }
@@ -2736,7 +2915,8 @@ void eig_batch_final(ptbgpu_ctx* c, EigBatch& eb, double mu, int64_t n, const in
         k_eig_final<<<eb.nsmall, kT, kFinalSmem, s>>>(eb.probs.as<EigProb>(), eb.order.as<int>(), eb.Ca.as<double>(),
                                                       eb.La.as<double>(), eb.Ta.as<double>(), eb.Wa.as<double>(),
                                                       eb.Za.as<double>(), eb.Qa.as<double>(), eb.Va.as<double>(),
-                                                      d_maps, d_own_cols, eb.Ba.as<double>(), mu, dP, dPdense);
+                                                      eb.Ka.as<double>(), d_maps, d_own_cols, eb.Ba.as<double>(), mu, dP,
+                                                      dPdense);
         count_launch();
         PTB_CUDA(cudaGetLastError());
     }
@@ -2745,9 +2925,137 @@ void eig_batch_final(ptbgpu_ctx* c, EigBatch& eb, double mu, int64_t n, const in
                          (const int*)eb.order_l.as<int>(), (const double*)eb.Ca.as<double>(),
                          (const double*)eb.La.as<double>(), (const double*)eb.Ta.as<double>(),
                          (const double*)eb.Wa.as<double>(), (const double*)eb.Za.as<double>(), eb.Qa.as<double>(),
-                         d_maps, d_own_cols, eb.Ba.as<double>(), mu, dP, dPdense);
+                         (const double*)eb.Ka.as<double>(), d_maps, d_own_cols, eb.Ba.as<double>(), mu, dP, dPdense);
         count_launch();
     }
+}
+
+// Matrix with both triangles set from the upper one: out[i + j n] = a[min(i,j) + max(i,j) n].
+__global__ void k_sym_from_upper(int64_t n, const double* __restrict__ a, double* __restrict__ out) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * n; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = q % n, j = q / n;
+        out[q] = (i <= j) ? a[i + j * n] : a[j + i * n];
+    }
+}
+
+constexpr int kGridRows = 64;   // rows per CTA of a cooperative-grid solve
+constexpr int kGridMax = 64;    // CTAs of a cooperative-grid solve at most
+constexpr int kGridMin = 4096;  // orders solved by one cluster instead
+
+void eig_full(ptbgpu_ctx* c, int64_t n, const double* H, const double* S, double* w, double* U) {
+    PTB_CHECK(n >= 1 && n <= kLargeMax, PTBGPU_EINVAL, "eigenproblem of order %lld outside the eigensolver (1..%d)",
+              (long long)n, kLargeMax);
+    eig_setup_attrs();
+    cudaStream_t s = c->stream;
+    const int m = (int)n;
+    int per_sm = 0;
+    PTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_eig_grid, kT, lg_smem_bytes(kLargeMax)));
+    PTB_CHECK(per_sm >= 1, PTBGPU_ECUDA, "eigensolver kernel does not fit an SM");
+    const int nsm = c->num_sms > 0 ? c->num_sms : 148;
+    // up to order kGridMin one thread-block cluster (hardware barrier), above it
+    // a cooperative grid of one CTA per kGridRows rows, at most kGridMax CTAs
+    // (the software barrier's latency grows with the CTA count)
+    const bool cluster = m <= kGridMin;
+    int G = cluster ? eig_cluster_size(c) : std::min({nsm * per_sm, kGridMax, std::max(1, m / kGridRows)});
+    EigBatch eb;
+    eb.nprob = 1;
+    eb.G = G;
+    EigProb p{};
+    p.m = m;
+    p.kind = S ? 0 : 1;
+    p.gld = n;
+    eb.hp.push_back(p);
+    const int64_t mm = (int64_t)m * m;
+    const int per = (m + G - 1) / G;
+    const LgLayout lay = lg_layout(m, G);
+    for (DevBuf* b : {&eb.Ca, &eb.La, &eb.Za}) b->reserve(sizeof(double) * mm);
+    eb.Qa.reserve(sizeof(double) * std::max<int64_t>(mm, (int64_t)G * lg_wy_stride(per) + 2));
+    eb.Va.reserve(sizeof(double) * std::max<int64_t>(mm, (int64_t)G * NB * NB + 2));
+    for (DevBuf* b : {&eb.Da, &eb.Ea, &eb.Ta, &eb.Wa}) b->reserve(sizeof(double) * n);
+    eb.Ka.reserve(sizeof(double) * std::max<int64_t>(t_panels(m) * NB * NB, 2));
+    eb.Xa.reserve(sizeof(double) * lay.total);
+    eb.Ba.reserve(sizeof(double) * 2);
+    eb.probs.reserve(sizeof(EigProb));
+    eb.status.reserve(sizeof(int) * 4);
+    eb.order.reserve(sizeof(int) * n);   // the identity row map
+    std::vector<int> ident(n);
+    for (int i = 0; i < m; ++i) ident[i] = i;
+    PTB_CUDA(cudaMemcpyAsync(eb.order.ptr, ident.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemcpyAsync(eb.probs.ptr, &p, sizeof(EigProb), cudaMemcpyHostToDevice, s));
+    PTB_CUDA(cudaMemsetAsync(eb.status.ptr, 0, sizeof(int) * 4, s));
+    unsigned* bar = reinterpret_cast<unsigned*>(eb.status.as<int>() + 1);   // status, bar[0], bar[1], err
+    int* err = eb.status.as<int>() + 3;
+    const EigProb* dp = eb.probs.as<EigProb>();
+    int pi = 0, M = kLargeMax, mode = 1;
+    const int* maps = eb.order.as<int>();
+    double *Ca = eb.Ca.as<double>(), *La = eb.La.as<double>(), *Za = eb.Za.as<double>(), *Qa = eb.Qa.as<double>(),
+           *Va = eb.Va.as<double>(), *Da = eb.Da.as<double>(), *Ea = eb.Ea.as<double>(), *Ta = eb.Ta.as<double>(),
+           *Wa = eb.Wa.as<double>(), *Ba = eb.Ba.as<double>(), *Ka = eb.Ka.as<double>(), *Xa = eb.Xa.as<double>();
+    const int* own = nullptr;
+    const int* ipos = nullptr;
+    double *e_out = nullptr, *fe_out = nullptr;
+    int* status = eb.status.as<int>();
+    // PTBGPU_EIG_STAGES=1: stage and tridiagonalisation phase times on stderr
+    static const bool stages = getenv("PTBGPU_EIG_STAGES") != nullptr;
+    if (cluster) {
+        const int* order = eb.order.as<int>() + 0;   // identity map: order[0] = 0
+        unsigned long long* ts = nullptr;
+        if (stages) {
+            eb.tstage.reserve(sizeof(unsigned long long) * kLgStride);
+            PTB_CUDA(cudaMemsetAsync(eb.tstage.ptr, 0, sizeof(unsigned long long) * kLgStride, s));
+            ts = eb.tstage.as<unsigned long long>();
+        }
+        launch_clustered(k_eig_cluster, 1, G, lg_smem_bytes(kLargeMax), s, dp, order, M, maps, H, S, Ca, La, Za, Qa,
+                         Va, Da, Ea, Ta, Wa, Ba, Ka, Xa, own, ipos, e_out, fe_out, status, ts, mode, U, w);
+        if (stages) {
+            unsigned long long t[kLgStride];
+            PTB_CUDA(cudaMemcpyAsync(t, ts, sizeof(t), cudaMemcpyDeviceToHost, s));
+            PTB_CUDA(cudaStreamSynchronize(s));
+            fprintf(stderr, "eig_full n=%d cluster %d: stages", m, G);
+            for (int k = 0; k + 1 < kLgStages; ++k) fprintf(stderr, " %.3f", (double)(t[k + 1] - t[k]) * 1e-6);
+            fprintf(stderr, " ms; tridiag phases");
+            for (int k = 0; k < kLgSub; ++k) fprintf(stderr, " %.3f", (double)t[kLgStages + k] * 1e-6);
+            fprintf(stderr, " ms\n");
+        }
+    } else {
+        void* args[] = {&dp, &pi, &M, &mode, &maps, &H, &S, &Ca, &La, &Za, &Qa, &Va, &Da, &Ea, &Ta, &Wa, &Ba, &Ka, &Xa,
+                        &own, &ipos, &e_out, &fe_out, &U, &w, &status, &bar, &err};
+        PTB_CUDA(cudaLaunchCooperativeKernel((void*)k_eig_grid, dim3(G), dim3(kT), args, lg_smem_bytes(kLargeMax), s));
+    }
+    count_launch();
+    int hs[4];
+    PTB_CUDA(cudaMemcpyAsync(hs, eb.status.ptr, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
+    PTB_CUDA(cudaStreamSynchronize(s));
+    PTB_CHECK(hs[3] == 0, PTBGPU_ETIMEOUT, "eigensolver: a grid barrier gave up waiting");
+    PTB_CHECK(hs[0] <= 0, PTBGPU_ENOTSPD, "overlap matrix not positive definite (leading minor %d)", hs[0]);
+    PTB_CHECK(hs[0] == kStOk, PTBGPU_EITER, "tridiagonal eigensolver did not converge");
+}
+
+void eig_full_upper(ptbgpu_ctx* c, int64_t n, double* A, double* B, double* w) {
+    cudaStream_t s = c->stream;
+    DevBuf h, b, u;
+    struct Rel {
+        DevBuf *x, *y, *z;
+        ~Rel() {
+            x->release();
+            y->release();
+            z->release();
+        }
+    } rel{&h, &b, &u};
+    h.reserve(sizeof(double) * n * n);
+    u.reserve(sizeof(double) * n * n);
+    const int grid = (int)std::min<int64_t>((n * n + 255) / 256, 148 * 16);
+    k_sym_from_upper<<<grid, 256, 0, s>>>(n, A, h.as<double>());
+    count_launch();
+    if (B) {
+        b.reserve(sizeof(double) * n * n);
+        k_sym_from_upper<<<grid, 256, 0, s>>>(n, B, b.as<double>());
+        count_launch();
+    }
+    PTB_CUDA(cudaGetLastError());
+    eig_full(c, n, h.as<double>(), B ? b.as<double>() : nullptr, w, u.as<double>());
+    PTB_CUDA(cudaMemcpyAsync(A, u.ptr, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
+    PTB_CUDA(cudaStreamSynchronize(s));
 }
 
 // Kernel-level entry: dense host problems through the same stages.  Problem k's

@@ -14,7 +14,7 @@ constexpr int kEigBatchMax = 1024;
 // Largest submatrix the library's eigensolver takes at all: orders above
 // kEigBatchMax run on a thread-block cluster each, whose tridiagonalisation
 // keeps two vectors of this length in shared memory.
-constexpr int kEigLargeMax = 10240;
+constexpr int kEigLargeMax = 12032;
 
 // One submatrix as the host plan describes it.
 struct EigProbHost {
@@ -47,6 +47,16 @@ void eig_batch_check(ptbgpu_ctx* c, EigBatch& eb);
 // dPdense non-null as m x nown column-major blocks, one after another.
 void eig_batch_final(ptbgpu_ctx* c, EigBatch& eb, double mu, int64_t n, const int* d_maps,
                      const int* d_own_cols, double* dP, double* dPdense = nullptr);
+
+// All eigenpairs of a dense problem on the device with the same solver on the
+// whole GPU (one cooperative launch): H U = S U diag(w) (S null: the standard
+// problem), H and S full symmetric (n x n, ld n; only the lower triangles are
+// read), w ascending, U column-major with U^T S U = I.  Orders up to
+// kEigLargeMax.
+void eig_full(ptbgpu_ctx* c, int64_t n, const double* H, const double* S, double* w, double* U);
+// The same with LAPACK's dsyevd / dsygvd argument convention ('V', upper
+// triangles read): A (and B) n x n, ld n; A is overwritten by the eigenvectors.
+void eig_full_upper(ptbgpu_ctx* c, int64_t n, double* A, double* B, double* w);
 
 // Kernel-level entry of ptbgpu_sygv_batched (dense host problems).
 void sygv_batched_entry(ptbgpu_ctx* c, int64_t np, const int64_t* dims, const double* H, const double* S,

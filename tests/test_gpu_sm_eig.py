@@ -160,3 +160,21 @@ def test_cluster_non_positive_definite_overlap_is_reported(ctx):
     with pytest.raises(PtbGpuError) as ei:
         ctx.sygv_batched([_problem(40, rng, 2), (H, S, own)])
     assert ei.value.code == api.ENOTSPD and "submatrix 2" in str(ei.value)
+
+
+def test_dense_solve2_on_the_whole_gpu(ctx):
+    """solve2's generalized eigensolve (source/pgtb.f90:1066-1170) runs the same
+    solver on the whole GPU (one cooperative launch, a grid barrier between
+    dependent steps): P, the eigenvalues and the Fermi occupations of an 80-H2O
+    cluster (ndim 1840) against the oracle's dsygvd."""
+    from oracle import ptb_oracle as O
+    from ptb_b200 import Options, synth
+
+    s = synth.water_cluster(80, seed=3)
+    n = s.ndim
+    P, e, focc, st = ctx.solve2(1, n, s.nel, 0, s.Hvec, s.Svec, Options(filter=1e-4))
+    ref, e_ref, f_ref, _ = O.solve2(1, n, s.nel, 0, 300.0, O.filter_matrix_sym(s.Hvec, 1e-4),
+                                    O.filter_matrix_sym(s.Svec, 1e-4))
+    assert np.max(np.abs(e - e_ref)) < 1e-10
+    assert np.max(np.abs(focc - f_ref)) < 1e-10
+    assert np.max(np.abs(P - ref)) < 1e-10
