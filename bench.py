@@ -404,9 +404,10 @@ def run_sm(args, rank, world, local, pg):
                         "mu_iterations": int(last.mu_iterations)},
         "e2e": {"value": wall, "unit": UNIT, "h2d_bytes_per_step": 2 * npk * 8, "d2h_bytes_per_step": npk * 8},
         "gpu_launches": int(sum(x.kernel_launches for x in stats)),
-        "roofline": {"bound": "fp64", "kernel": "k_eig_fused (the library's batched generalized eigensolver, one "
-                     "persistent launch: Cholesky, reduction, tridiagonalisation, divide and conquer, owned rows; "
-                     "submatrices of order <= 1024) and cuSOLVER dsygvd for larger ones on side streams",
+        "roofline": {"bound": "fp64", "kernel": "the library's FP64 generalized eigensolver (Cholesky, reduction, "
+                     "tridiagonalisation, divide and conquer, owned rows; DMMA tile products): k_eig_fused, one "
+                     "persistent launch for submatrices of order <= 1024, and k_eig_cluster, one thread-block "
+                     "cluster per larger submatrix, side by side",
                      "achieved": feig / (ms / 1e3) / 1e12,
                      "peak": 37.0, "unit": "TFLOP/s", "frac": feig / (ms / 1e3) / 1e12 / 37.0, "traffic": None,
                      "peak_kind": "nominal B200 FP64 (no measured FP64 figure on this pool)",
@@ -505,10 +506,12 @@ def run_purify_types(args, rank, world, local, pg):
         "e2e": {"value": step_wall, "unit": PURIFY_UNIT, "h2d_bytes_per_step": len(PURIFY_TYPES) * 2 * npk * 8,
                 "d2h_bytes_per_step": len(PURIFY_TYPES) * npk * 8},
         "gpu_launches": launches,
-        "roofline": {"bound": "fp64", "kernel": "cuBLAS DGEMM / cuSOLVER DSYEVD with the library's kernels",
+        "roofline": {"bound": "fp64", "kernel": "FP64-class products on the int8 tensor cores (oz_dgemm) and the "
+                     "library's eigensolver (eig_full) with the library's kernels",
                      "achieved": tf, "peak": 37.0, "unit": "TFLOP/s", "frac": tf / 37.0, "traffic": None,
                      "peak_kind": "nominal B200 FP64 (no measured FP64 figure on this pool)",
-                     "work": "2 n^3 per DGEMM issued, eigensolves not counted, over the six calls' device time"},
+                     "work": "2 n^3 per FP64-class product issued, eigensolves not counted, over the six calls' "
+                             "device time"},
         "cpu_baseline": ({"value": cpu_s, "unit": PURIFY_UNIT, "cores": os.cpu_count(), "kind": "port",
                           "sample": "oracle purification (numpy / scipy OpenBLAS), one call per type, whole workload"}
                          if cpu_s else None),
@@ -551,6 +554,20 @@ def run_batch(args, rank, world, local, pg):
         grouped = {"entry": "ptbgpu_tc_purify_grouped", "s_per_step": wallg / 1e3,
                    "max_abs_dP_vs_fp64": float(max(np.max(np.abs(a - b)) for a, b in zip(Pg, P64))),
                    "fp64_fallbacks": sum(x.fp64_fallback for x in stg)}
+        # and through the FP64 eigensolver, all 256 systems in one launch (the dense
+        # projector per system: one CTA each up to order 1024, one cluster each above)
+        ctx.eig_density_batch(args_b)
+        ew = []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            Pe, ste, walle = ctx.eig_density_batch(args_b)
+            ew.append(time.perf_counter() - t0)
+        eig_batch = {"entry": "ptbgpu_eig_density_batch", "s_per_step": statistics.median(ew),
+                     "note": "host wall clock of the whole call with the packed host arrays (copies inside), "
+                             "median of the timed calls",
+                     "max_abs_dP_vs_fp64": float(max(np.max(np.abs(a - b)) for a, b in zip(Pe, P64))),
+                     "gpu_launches_per_step": int(sum(x.kernel_launches for x in ste)) or None}
+        extra["eig_batch"] = eig_batch
     if rank != 0:
         ctx.close()
         return

@@ -195,6 +195,19 @@ int ptbgpu_tc_purify_batch(ptbgpu_ctx* ctx, int64_t ninst, const int64_t* ndim, 
                            const double* const* Hpk, const double* const* Spk, double* const* Ppk,
                            int64_t workers, const ptbgpu_opts* opts, ptbgpu_stats* st, double* wall_ms);
 
+/* The density step of many independent systems in one launch of the library's
+ * FP64 eigensolver: per system the filtered generalized eigenproblem
+ * H_k U = S_k U e and P_k = 2 sum_{i < nel_k/2} u_i u_i^T (the dense projector
+ * at T = 0, i.e. the reference's solve2, source/pgtb.f90:1066-1170, without the
+ * Fermi smearing), P_k formed in the same launch.  Systems up to order 1024 run
+ * one CTA each in a persistent launch (largest first), larger ones (up to 12032)
+ * one thread-block cluster each, beside them.  opts->filter is applied to H and
+ * S (filter_matrix_sym).  Per-system stats carry flops; wall_ms the host time of
+ * the call.  ENOTSPD names the first system whose S is not positive definite. */
+int ptbgpu_eig_density_batch(ptbgpu_ctx* ctx, int64_t ninst, const int64_t* ndim, const int64_t* nel,
+                             const double* const* Hpk, const double* const* Spk, double* const* Ppk,
+                             const ptbgpu_opts* opts, ptbgpu_stats* st, double* wall_ms);
+
 /* The same systems purified together: bucketed by ndim rounded up to 256 and
  * padded within a bucket (decoupled padding: unit overlap, orthogonalised
  * diagonal at the system's upper spectral bound), stacked, and every step run

@@ -68,6 +68,7 @@ class _Stats(C.Structure):
 EXPORTED = ("ptbgpu_init", "ptbgpu_finalize", "ptbgpu_last_error", "ptbgpu_default_settings",
             "ptbgpu_default_opts", "ptbgpu_filter_packed", "ptbgpu_check_density", "ptbgpu_sm_density",
             "ptbgpu_purify", "ptbgpu_tc_purify", "ptbgpu_tc_purify_device", "ptbgpu_tc_purify_batch", "ptbgpu_tc_purify_grouped",
+            "ptbgpu_eig_density_batch",
             "ptbgpu_solve2",
             "ptbgpu_symsq_bf16x3", "ptbgpu_symsq_bf16x6", "ptbgpu_symsq_split", "ptbgpu_runtime_info",
             "ptbgpu_density_traces_noalloc", "ptbgpu_oz_gemm", "ptbgpu_mlpop14", "ptbgpu_mlpop14_device",
@@ -116,6 +117,8 @@ def load_library():
     lib.ptbgpu_tc_purify_batch.argtypes = [C.c_void_p, i64, P(i64), P(i64), P(d), P(d), P(d), i64, P(_Opts),
                                            P(_Stats), d]
     lib.ptbgpu_tc_purify_grouped.argtypes = [C.c_void_p, i64, P(i64), P(i64), P(d), P(d), P(d), P(_Opts),
+                                             P(_Stats), d]
+    lib.ptbgpu_eig_density_batch.argtypes = [C.c_void_p, i64, P(i64), P(i64), P(d), P(d), P(d), P(_Opts),
                                              P(_Stats), d]
     lib.ptbgpu_solve2.argtypes = [C.c_void_p, i64, i64, i64, i64, d, d, d, d, d, P(_Opts), P(_Stats)]
     lib.ptbgpu_selftest_bounded_wait.argtypes = [C.c_void_p, i64]
@@ -428,6 +431,27 @@ class Context:
         o = (opts or Options()).to_c()
         self._check(self._lib.ptbgpu_tc_purify_batch(self._h, n, ndim, nel, arr(Hs), arr(Ss), arr(Ps),
                                                      int(workers), C.byref(o), st, C.byref(wall)))
+        return Ps, [Stats.from_c(st[i]) for i in range(n)], wall.value
+
+    def eig_density_batch(self, systems, opts: Options | None = None):
+        """The density step of many independent systems in one launch of the
+        FP64 eigensolver (ptbgpu_eig_density_batch): `systems` a sequence of
+        (ndim, nel, H, S) packed; P = 2 sum of the nel/2 lowest generalized
+        eigenvectors' outer products (opts.filter applied to H and S).  Returns
+        ([Pvec], [Stats], wall milliseconds)."""
+        n = len(systems)
+        m = max(n, 1)
+        ndim = (C.c_int64 * m)(*[int(s[0]) for s in systems])
+        nel = (C.c_int64 * m)(*[int(s[1]) for s in systems])
+        Hs = [_packed(s[2], s[0], f"H of system {i}") for i, s in enumerate(systems)]
+        Ss = [_packed(s[3], s[0], f"S of system {i}") for i, s in enumerate(systems)]
+        Ps = [np.zeros(npacked(int(s[0]))) for s in systems]
+        arr = lambda xs: (C.POINTER(C.c_double) * m)(*[_dptr(x) for x in xs])
+        st = (_Stats * m)()
+        wall = C.c_double(0.0)
+        o = (opts or Options()).to_c()
+        self._check(self._lib.ptbgpu_eig_density_batch(self._h, n, ndim, nel, arr(Hs), arr(Ss), arr(Ps),
+                                                       C.byref(o), st, C.byref(wall)))
         return Ps, [Stats.from_c(st[i]) for i in range(n)], wall.value
 
     def xc_damping(self, nat: int, ndim: int, aoat, rab, rad, hao, xdiag, P: np.ndarray, H: np.ndarray,

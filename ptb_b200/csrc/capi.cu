@@ -249,6 +249,22 @@ int ptbgpu_tc_purify_device(ptbgpu_ctx* c, int64_t ndim, int64_t nel, const doub
     });
 }
 
+int ptbgpu_eig_density_batch(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const int64_t* nel,
+                             const double* const* Hpk, const double* const* Spk, double* const* Ppk,
+                             const ptbgpu_opts* opts, ptbgpu_stats* st, double* wall_ms) {
+    if (st)
+        for (int64_t i = 0; i < ninst; ++i) clear_stats(&st[i]);
+    return guarded(c, [&] {
+        PTB_CHECK(ninst >= 0 && (ninst == 0 || (ndim && nel && Hpk && Spk && Ppk)), PTBGPU_EINVAL, "bad arguments");
+        const auto t0 = std::chrono::steady_clock::now();
+        eig_density_batch(c, ninst, ndim, nel, Hpk, Spk, Ppk, opts ? opts->filter : 0.0,
+                          opts ? (int)opts->print_level : 0, st);
+        if (st && ninst > 0) st[0].kernel_launches = launch_counter();   // the whole call's launches
+        if (wall_ms)
+            *wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    });
+}
+
 int ptbgpu_tc_purify_batch(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const int64_t* nel,
                            const double* const* Hpk, const double* const* Spk, double* const* Ppk, int64_t workers,
                            const ptbgpu_opts* opts, ptbgpu_stats* st, double* wall_ms) {

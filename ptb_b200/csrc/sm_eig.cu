@@ -48,6 +48,8 @@ constexpr int kStNoConv = -1;     // a leaf's QL sweeps exhausted
 struct EigProb {
     int k, m, nown;
     int kind;             // 0: H U = S U e; 1: standard problem (S not read, L = I)
+    int mode;             // 0: eigenvalues, fe, owned rows; 2: density 2 U_occ U_occ^T (m x m at boff)
+    int nocc;             // mode 2: occupied eigenvectors (the lowest)
     int64_t moff, eoff, o0;
     int64_t gbase, gld;   // the problem's H / S: element (i, j) at gbase + map(i) + map(j) gld
     int64_t poff;         // dense output of the owned columns of P (m x nown, column-major)
@@ -1378,6 +1380,53 @@ __device__ void stage_rows(const EigProb& p, const double* __restrict__ Ca, cons
 }
 
 // ---------------------------------------------------------------------------
+// Density of one system on one CTA (mode 2): U = L^-T Q Z in place of Z (Q as
+// WY tile products, L^-T by blocked back substitution, or one warp per column
+// when the divide and conquer's arrays are too small for the 64 x 65 block),
+// then the upper tiles of U_occ U_occ^T (K = nocc, the lowest eigenvectors:
+// the divide and conquer leaves them ascending) into Ba + boff; the factor 2
+// is applied when packing.
+__device__ void stage_density(const EigProb& p, const double* __restrict__ Ca, const double* __restrict__ La,
+                              const double* __restrict__ Ta, double* __restrict__ Za, double* __restrict__ Qa,
+                              double* __restrict__ Va, const double* __restrict__ Ka, double* __restrict__ Ba,
+                              const StageSmem& sh) {
+    const int m = p.m, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int no = p.nocc;   // only the occupied eigenvectors enter P
+    const double* C = Ca + p.aoff;
+    const double* L = La + p.aoff;
+    double* U = Za + p.aoff;
+    if (no == 0) return;
+    if (m >= kWyMmaMin) wy_apply_t(C, m, Ka + p.koff, U, no, false, Qa + p.aoff, Va + p.aoff, sh.sA, sh.sB);
+    else wy_apply(C, m, Ta + p.voff, U, no, false, WySmem{sh.sA, sh.sB});
+    __syncthreads();
+    if (p.kind == 0) {
+        if (dc_smem_bytes(sh.M) >= sizeof(double) * TS * (TS + 1)) {
+            trsm_cols(false, L, m, U, m, 0, no, reinterpret_cast<double*>(sh.uni), sh.sA, sh.sB);
+        } else {
+            for (int t = warp; t < no; t += kT / 32) {
+                double* w = U + (int64_t)t * m;
+                for (int i = m - 1; i >= 0; --i) {
+                    const double* li = L + (int64_t)i * m;
+                    double sum = 0.0;
+                    for (int k = i + 1 + lane; k < m; k += 32) sum = fma(li[k], w[k], sum);
+                    sum = warp_sum(sum);
+                    if (lane == 0) w[i] = (w[i] - sum) / li[i];
+                    __syncwarp();
+                }
+            }
+        }
+    }
+    __syncthreads();
+    double* P = Ba + p.boff;
+    const int nt = (m + TS - 1) / TS;
+    for (int cb = 0; cb < nt; ++cb)
+        for (int rb = 0; rb <= cb; ++rb)
+            tile_mma<false, true, MMA_SET, false>(P, m, 0, nullptr, rb * TS, cb * TS, min(TS, m - rb * TS),
+                                                  min(TS, m - cb * TS), U, m, nullptr, U, m, nullptr, p.nocc, sh.sA,
+                                                  sh.sB);
+}
+
+// ---------------------------------------------------------------------------
 // One persistent launch for every submatrix of the step: each CTA takes the
 // next submatrix (largest first) from a device counter and runs all stages on
 // it - gather, Cholesky, reduction, tridiagonalisation, divide and conquer,
@@ -1435,7 +1484,12 @@ __global__ void __launch_bounds__(kT, 1) k_eig_fused(
             if (st == kStOk) {
                 if (p.m >= kWyMmaMin)
                     build_T(Ca + p.aoff, p.m, Ta + p.voff, Ka + p.koff, 0, 1, Va + p.aoff, sh.sD, sh.sA, sh.sB);
-                stage_rows(p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, Qa, Va, Ka, e_out, fe_out, sh);
+                if (p.mode == 2) {
+                    for (int j = threadIdx.x; j < p.m; j += kT) e_out[p.eoff + j] = Wa[p.voff + j];
+                    stage_density(p, Ca, La, Ta, Za, Qa, Va, Ka, Ba, sh);
+                } else {
+                    stage_rows(p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, Qa, Va, Ka, e_out, fe_out, sh);
+                }
             }
         }
         if (tid == 0) status[pi] = st;
@@ -2509,7 +2563,35 @@ __device__ void eig_group_solve(const Grp& g, int pi, const EigProb& p, const Lg
             build_T(Ca + p.aoff, m, Ta + p.voff, Ka + p.koff, g.rank, g.size, Va + p.aoff + (int64_t)g.rank * NB * NB,
                     sh.sD, sh.sA, sh.sB);
             g.sync();
-            if (mode == 0) {
+            if (mode == 0 && p.mode == 2) {
+                // density: U_occ = L^-T Q Z_occ in place of Z's occupied (lowest)
+                // columns (column ranges per CTA), then the upper tiles of
+                // U_occ U_occ^T split over the group
+                const int no = p.nocc;
+                const int per = (no + g.size - 1) / g.size;
+                const int t0 = min(no, g.rank * per), t1 = min(no, t0 + per);
+                double* Uz = Za + p.aoff;
+                if (t1 > t0) {
+                    double* scr = Qa + p.aoff + (int64_t)g.rank * lg_wy_stride(per);
+                    wy_apply_t(Ca + p.aoff, m, Ka + p.koff, Uz + (int64_t)t0 * m, t1 - t0, false, scr,
+                               scr + (int64_t)NB * per, sh.sA, sh.sB);
+                    __syncthreads();
+                    if (p.kind == 0)
+                        trsm_cols(false, La + p.aoff, m, Uz + (int64_t)t0 * m, m, 0, t1 - t0, sh.sD, sh.sA, sh.sB);
+                }
+                for (int j = g.rank * kT + threadIdx.x; j < m; j += g.size * kT) e_out[p.eoff + j] = Wa[p.voff + j];
+                g.sync();
+                const int nt = (m + TS - 1) / TS;
+                const int ntile = nt * (nt + 1) / 2;
+                double* P = Ba + p.boff;
+                for (int idx = g.rank; idx < ntile; idx += g.size) {
+                    int cb, rb;
+                    tri_decode(idx, cb, rb);   // cb >= rb: upper tiles
+                    tile_mma<false, true, MMA_SET, false>(P, m, 0, nullptr, rb * TS, cb * TS, min(TS, m - rb * TS),
+                                                          min(TS, m - cb * TS), Uz, m, nullptr, Uz, m, nullptr, p.nocc,
+                                                          sh.sA, sh.sB);
+                }
+            } else if (mode == 0) {
                 lg_rows(g, p, Ca, La, Ta, Wa, Za, own_cols, ipos, Ba, Qa, Ka, e_out, fe_out, sh);
             } else {
                 const int per = (m + g.size - 1) / g.size;
@@ -2766,6 +2848,8 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
         p.o0 = q.o0;
         p.gbase = q.gbase;
         p.gld = q.gld < 0 ? n : q.gld;
+        p.mode = q.mode;
+        p.nocc = q.nocc;
         p.poff = psz;
         psz += (int64_t)q.m * q.nown;
         p.aoff = asz;
@@ -2776,7 +2860,7 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
         ksz += t_panels(q.m) * NB * NB;
         asz += (int64_t)q.m * q.m;
         vsz += q.m;
-        bsz += 4 * (int64_t)q.nown * q.m;
+        bsz += q.mode == 2 ? (int64_t)q.m * q.m : 4 * (int64_t)q.nown * q.m;
         if (q.m > kEigBatchMax) {
             xsz += lg_layout(q.m, eb->G).total;
             ord_l.push_back((int)eb->hp.size());
@@ -3056,6 +3140,91 @@ void eig_full_upper(ptbgpu_ctx* c, int64_t n, double* A, double* B, double* w) {
     eig_full(c, n, h.as<double>(), B ? b.as<double>() : nullptr, w, u.as<double>());
     PTB_CUDA(cudaMemcpyAsync(A, u.ptr, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
     PTB_CUDA(cudaStreamSynchronize(s));
+}
+
+// Packed upper triangle of scale * P (P m x m column-major, read above the diagonal).
+__global__ void k_pack_scaled(int64_t m, const double* __restrict__ P, double scale, double* __restrict__ pk) {
+    const int64_t np = m * (m + 1) / 2;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < np; q += (int64_t)gridDim.x * blockDim.x) {
+        int64_t j = (int64_t)((sqrt(8.0 * (double)q + 1.0) - 1.0) * 0.5);
+        while ((j + 1) * (j + 2) / 2 <= q) ++j;
+        while (j * (j + 1) / 2 > q) --j;
+        const int64_t i = q - j * (j + 1) / 2;
+        pk[q] = scale * P[i + j * m];
+    }
+}
+
+void eig_density_batch(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const int64_t* nel,
+                       const double* const* Hpk, const double* const* Spk, double* const* Ppk, double filter,
+                       int prl, ptbgpu_stats* st) {
+    if (ninst <= 0) return;
+    cudaStream_t s = c->stream;
+    std::vector<EigProbHost> probs;
+    std::vector<int64_t> pkoff((size_t)ninst + 1, 0);
+    int64_t hsz = 0, nsum = 0;
+    for (int64_t k = 0; k < ninst; ++k) {
+        const int64_t m = ndim[k];
+        PTB_CHECK(m >= 1 && m <= kLargeMax, PTBGPU_EINVAL, "system %lld: ndim %lld outside the eigensolver (1..%d)",
+                  (long long)k, (long long)m, kLargeMax);
+        PTB_CHECK(nel[k] >= 0 && nel[k] / 2 <= m && Hpk[k] && Spk[k] && Ppk[k], PTBGPU_EINVAL,
+                  "system %lld: bad electron count or arrays", (long long)k);
+        EigProbHost q{};
+        q.k = (int)k;
+        q.m = (int)m;
+        q.nown = 0;
+        q.moff = nsum;
+        q.eoff = nsum;
+        q.o0 = 0;
+        q.gbase = hsz;
+        q.gld = m;
+        q.mode = 2;
+        q.nocc = (int)(nel[k] / 2);
+        probs.push_back(q);
+        hsz += m * m;
+        nsum += m;
+        pkoff[k + 1] = pkoff[k] + m * (m + 1) / 2;
+    }
+    struct Bufs {
+        DevBuf h, sm, pk, maps, e, dummy;
+        ~Bufs() {
+            for (DevBuf* b : {&h, &sm, &pk, &maps, &e, &dummy}) b->release();
+        }
+    } b;
+    b.h.reserve(sizeof(double) * hsz);
+    b.sm.reserve(sizeof(double) * hsz);
+    b.pk.reserve(sizeof(double) * std::max<int64_t>(2 * pkoff[ninst], 1));
+    b.maps.reserve(sizeof(int) * nsum);
+    b.e.reserve(sizeof(double) * nsum);
+    b.dummy.reserve(64);
+    std::vector<int> maps((size_t)nsum);
+    for (const EigProbHost& q : probs)
+        for (int i = 0; i < q.m; ++i) maps[q.moff + i] = i;
+    PTB_CUDA(cudaMemcpyAsync(b.maps.ptr, maps.data(), sizeof(int) * nsum, cudaMemcpyHostToDevice, s));
+    double* pkH = b.pk.as<double>();
+    double* pkS = pkH + pkoff[ninst];
+    for (int64_t k = 0; k < ninst; ++k) {
+        const int64_t m = ndim[k], np = m * (m + 1) / 2;
+        PTB_CUDA(cudaMemcpyAsync(pkH + pkoff[k], Hpk[k], sizeof(double) * np, cudaMemcpyHostToDevice, s));
+        PTB_CUDA(cudaMemcpyAsync(pkS + pkoff[k], Spk[k], sizeof(double) * np, cudaMemcpyHostToDevice, s));
+        unpack_sym(s, m, m, pkH + pkoff[k], b.h.as<double>() + probs[k].gbase, filter);
+        unpack_sym(s, m, m, pkS + pkoff[k], b.sm.as<double>() + probs[k].gbase, filter);
+    }
+    double flops = 0.0;
+    std::shared_ptr<EigBatch> eb = eig_batch_launch(c, 0, b.h.as<double>(), b.sm.as<double>(), probs,
+                                                    b.maps.as<int>(), b.dummy.as<int>(), b.dummy.as<int>(),
+                                                    b.e.as<double>(), b.e.as<double>(), prl, &flops);
+    eig_batch_check(c, *eb);
+    for (int64_t k = 0; k < ninst; ++k) {
+        const int64_t m = ndim[k], np = m * (m + 1) / 2;
+        const int grid = (int)std::min<int64_t>((np + 255) / 256, 148 * 8);
+        k_pack_scaled<<<grid, 256, 0, s>>>(m, eb->Ba.as<double>() + eb->hp[k].boff, 2.0, pkH + pkoff[k]);
+        count_launch();
+        PTB_CUDA(cudaGetLastError());
+        PTB_CUDA(cudaMemcpyAsync(Ppk[k], pkH + pkoff[k], sizeof(double) * np, cudaMemcpyDeviceToHost, s));
+    }
+    PTB_CUDA(cudaStreamSynchronize(s));
+    if (st)
+        for (int64_t k = 0; k < ninst; ++k) st[k].flops += 7.0 * std::pow((double)ndim[k], 3);
 }
 
 // Kernel-level entry: dense host problems through the same stages.  Problem k's

@@ -26,6 +26,8 @@ struct EigProbHost {
     int64_t o0;     // offset of its owned columns in the owned-column list
     int64_t gbase = 0;   // its H / S element (i, j) at gbase + map(i) + map(j) gld
     int64_t gld = -1;    // -1: the system's ndim
+    int mode = 0;        // 0: eigenvalues, fe and owned rows (submatrix method); 2: density P = 2 U_occ U_occ^T
+    int nocc = 0;        // mode 2: occupied (lowest) eigenvectors
 };
 
 struct EigBatch;
@@ -57,6 +59,14 @@ void eig_full(ptbgpu_ctx* c, int64_t n, const double* H, const double* S, double
 // The same with LAPACK's dsyevd / dsygvd argument convention ('V', upper
 // triangles read): A (and B) n x n, ld n; A is overwritten by the eigenvectors.
 void eig_full_upper(ptbgpu_ctx* c, int64_t n, double* A, double* B, double* w);
+
+// The density step of many independent systems in one launch of the
+// eigensolver (ptbgpu_eig_density_batch): Hpk / Spk / Ppk host packed arrays
+// per system, P_k = 2 sum_{i < nel_k/2} u_i u_i^T of H_k U = S_k U e after the
+// filter; stats per system (may be null).
+void eig_density_batch(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const int64_t* nel,
+                       const double* const* Hpk, const double* const* Spk, double* const* Ppk, double filter,
+                       int prl, ptbgpu_stats* st);
 
 // Kernel-level entry of ptbgpu_sygv_batched (dense host problems).
 void sygv_batched_entry(ptbgpu_ctx* c, int64_t np, const int64_t* dims, const double* H, const double* S,
