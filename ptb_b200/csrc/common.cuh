@@ -161,6 +161,10 @@ void dgemm_nn(ptbgpu_ctx* c, int64_t n, int64_t ld, double alpha, const double* 
 void dsyrk_sq(ptbgpu_ctx* c, int64_t n, int64_t ld, const double* X, double* C);   // C = X X (X symmetric), full C
 int  dpotrf_lower(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A);              // returns info
 void dtrtri_lower(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A);
+// Device-result forms of frob_dev / has_nan_dev (no host synchronisation): the
+// Frobenius norm into a device double; a NaN sets *flag = 1.
+void frob_to_dev(ptbgpu_ctx* c, int64_t n, int64_t ld, const double* a, double* out);
+void nan_flag_dev(ptbgpu_ctx* c, int64_t count, const double* a, int* flag);
 void dsyevd(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A, double* w);
 int  dsygvd(ptbgpu_ctx* c, int64_t n, int64_t ld, double* A, double* B, double* w);
 

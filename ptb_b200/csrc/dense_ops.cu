@@ -337,6 +337,34 @@ double frob_dev(ptbgpu_ctx* c, int64_t n, int64_t ld, const double* a) {
     return std::sqrt(host_reduce(c, p, nb, false));
 }
 
+// Sum of nb partials in index order (as host_reduce), optionally its square
+// root, into a device scalar; or the OR of "sum > 0" into a device flag.
+__global__ void k_sum_partials(const double* __restrict__ p, int nb, double* __restrict__ out, int mode) {
+    double r = 0.0;
+    for (int i = 0; i < nb; ++i) r = r + p[i];
+    if (mode == 0) *out = sqrt(r);
+    else if (mode == 1) *out = r;
+    else if (r > 0.0) *reinterpret_cast<int*>(out) = 1;
+}
+
+void frob_to_dev(ptbgpu_ctx* c, int64_t n, int64_t ld, const double* a, double* out) {
+    int nb = grid_for(n, 1);
+    double* p = partials(c, nb);
+    k_reduce2d<0><<<nb, kThreads, 0, c->stream>>>(n, ld, a, nullptr, p);
+    k_sum_partials<<<1, 1, 0, c->stream>>>(p, nb, out, 0);
+    count_launch(2);
+    PTB_CUDA(cudaGetLastError());
+}
+
+void nan_flag_dev(ptbgpu_ctx* c, int64_t count, const double* a, int* flag) {
+    int nb = grid_for(count);
+    double* p = partials(c, nb);
+    k_reduce1d<2><<<nb, kThreads, 0, c->stream>>>(count, a, nullptr, p);
+    k_sum_partials<<<1, 1, 0, c->stream>>>(p, nb, reinterpret_cast<double*>(flag), 2);
+    count_launch(2);
+    PTB_CUDA(cudaGetLastError());
+}
+
 double trace_prod_dev(ptbgpu_ctx* c, int64_t n, int64_t ld, const double* a, const double* b) {
     int nb = grid_for(n, 1);
     double* p = partials(c, nb);

@@ -63,6 +63,55 @@ __global__ void k_colsq(int64_t n, const double* __restrict__ V, double* __restr
 
 int g1(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(n, 148 * 16)); }
 
+// ---------------------------------------------------------------------------
+// Iteration loops as CUDA graphs: after one eager iteration (which sizes every
+// buffer and tile list the body touches and gives the host its first stop
+// decision), the body of one iteration is captured into the body graph of a
+// conditional WHILE node, and a one-thread kernel at its end applies the
+// loop's stop rule on the device (cudaGraphSetConditional), so the remaining
+// iterations run as one graph launch without a host round trip each.  The
+// norms are summed in the same order as on the host, so the iteration counts
+// and results equal those of the eager loop.
+struct LoopDev {
+    double norm0, norm1;   // the norm the stop rule compares against, the new one
+    long long iters;       // iterations done (the eager one included)
+    int nan;               // a NaN was met in the body
+    int pad;
+};
+
+// sign_iterative's rule (source/purification.f90:587): stop when
+// | ||X||_F - ||X_prev||_F | < thrs%normal, at the cycle cap, or on a NaN.
+// McWeeny's rule (source/purification.f90:496) is the same with the norm
+// carried over to the next iteration.
+__global__ void k_loop_decide(cudaGraphConditionalHandle h, LoopDev* d, double thr, long long cycles, int carry) {
+    d->iters += 1;
+    const bool stop = d->nan != 0 || std::fabs(d->norm1 - d->norm0) < thr || d->iters >= cycles;
+    if (!stop && carry) d->norm0 = d->norm1;
+    cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
+
+struct LoopGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle handle{};
+    int64_t body_launches = 0;
+    double body_flops = 0.0;
+    bool failed = false;
+    ~LoopGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+// PTBGPU_GRAPH_LOOPS=0 runs every iteration eagerly instead.
+bool graph_loops() {
+    static const bool on = [] {
+        const char* v = getenv("PTBGPU_GRAPH_LOOPS");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
 struct Ctx {
     ptbgpu_ctx* c;
     int64_t n;
@@ -93,6 +142,81 @@ struct Ctx {
         gemm_flops += 2.0 * (double)n * (double)n * (double)n;
     }
     static constexpr int kSlices = 8;
+    DevBuf loopdev;
+    LoopGraph sign_loop, mcw_loop;
+    LoopDev* ld() {
+        loopdev.reserve(sizeof(LoopDev));
+        return loopdev.as<LoopDev>();
+    }
+    // Captures body() into a WHILE node's body graph followed by the decision
+    // kernel; false if the stream could not be captured (then the loop runs
+    // eagerly).
+    template <class Body>
+    bool build_loop(LoopGraph& lg, Body body, double thr, long long cycles, int carry) {
+        if (lg.exec) return true;
+        if (lg.failed) return false;
+        cudaStream_t s = c->stream;
+        LoopDev* d = ld();
+        bool ok = cudaGraphCreate(&lg.graph, 0) == cudaSuccess &&
+                  cudaGraphConditionalHandleCreate(&lg.handle, lg.graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+        cudaGraphNode_t node;
+        cudaGraphNodeParams cp = {};
+        cudaGraph_t bodyg = nullptr;
+        if (ok) {
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = lg.handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            ok = cudaGraphAddNode(&node, lg.graph, nullptr, 0, &cp) == cudaSuccess;
+            if (ok) bodyg = cp.conditional.phGraph_out[0];
+        }
+        if (ok) ok = cudaStreamBeginCaptureToGraph(s, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+                     cudaSuccess;
+        if (ok) {
+            const int64_t l0 = launch_counter();
+            const double f0 = gemm_flops;
+            try {
+                body();
+                k_loop_decide<<<1, 1, 0, s>>>(lg.handle, d, thr, cycles, carry);
+                count_launch();
+            } catch (...) {
+                ok = false;
+            }
+            cudaGraph_t out = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(s, &out);
+            ok = ok && e == cudaSuccess;
+            lg.body_launches = launch_counter() - l0;
+            lg.body_flops = gemm_flops - f0;
+            launch_counter() = l0;   // counted per executed iteration after the launch
+            gemm_flops = f0;
+        }
+        if (ok) ok = cudaGraphInstantiate(&lg.exec, lg.graph, 0) == cudaSuccess;
+        if (!ok) {
+            cudaGetLastError();
+            if (lg.exec) cudaGraphExecDestroy(lg.exec);
+            if (lg.graph) cudaGraphDestroy(lg.graph);
+            lg.exec = nullptr;
+            lg.graph = nullptr;
+            lg.failed = true;
+            log_line(prl, 2, " purification loop: CUDA graph capture failed, running eagerly");
+        }
+        return ok;
+    }
+    // One launch of a built loop from the state `init` (iterations done so far
+    // and the norm to compare against); returns the loop's final device state.
+    LoopDev run_loop(LoopGraph& lg, LoopDev init) {
+        cudaStream_t s = c->stream;
+        LoopDev* d = ld();
+        PTB_CUDA(cudaMemcpyAsync(d, &init, sizeof(LoopDev), cudaMemcpyHostToDevice, s));
+        PTB_CUDA(cudaGraphLaunch(lg.exec, s));
+        LoopDev out;
+        PTB_CUDA(cudaMemcpyAsync(&out, d, sizeof(LoopDev), cudaMemcpyDeviceToHost, s));
+        PTB_CUDA(cudaStreamSynchronize(s));
+        const long long ran = out.iters - init.iters;
+        count_launch((int)(ran * lg.body_launches));
+        gemm_flops += (double)ran * lg.body_flops;
+        return out;
+    }
     double frob(const double* a) { return frob_dev(c, n, n, a); }
     void nan_check(const double* a, const char* msg) {
         PTB_CHECK(!has_nan_dev(c, n * n, a), PTBGPU_ENAN, "%s", msg);
@@ -204,17 +328,35 @@ void mcweeny(Ctx& x, const ptbgpu_pur_settings& pur, const double* guess, const 
     copy_mat(s, n, n, guess, n, g);
     double norm = x.frob(g);
     copy_mat(s, n, n, guess, n, P);
-    for (int64_t i = 0; i < pur.cycles; ++i) {
+    auto step = [&] {
         x.gemm(S, g, t1);
         x.gemm(g, t1, t2);
         x.gemm(t2, t1, t3);
         copy_mat(s, n, n, t2, n, P);
         axpby_diag(s, n, n, -2.0, t3, 3.0, P, 0.0);
+    };
+    for (int64_t i = 0; i < pur.cycles; ++i) {
+        step();
         x.nan_check(P, "Error: NaN is encountered during purification");
         const double np = x.frob(P);
         if (std::fabs(np - norm) < x.thr.normal) break;
         copy_mat(s, n, n, P, n, g);
         norm = np;
+        // the remaining iterations as one graph launch (the stop rule on the device)
+        if (i + 1 < pur.cycles && graph_loops()) {
+            LoopDev* d = x.ld();
+            auto body = [&] {
+                step();
+                nan_flag_dev(x.c, n * n, P, &d->nan);
+                frob_to_dev(x.c, n, n, P, &d->norm1);
+                copy_mat(s, n, n, P, n, g);   // the next iteration's input (unused after the last)
+            };
+            if (x.build_loop(x.mcw_loop, body, x.thr.normal, (long long)pur.cycles, 1)) {
+                const LoopDev r = x.run_loop(x.mcw_loop, LoopDev{norm, 0.0, (long long)(i + 1), 0, 0});
+                PTB_CHECK(r.nan == 0, PTBGPU_ENAN, "%s", "Error: NaN is encountered during purification");
+                break;
+            }
+        }
     }
     axpby_diag(s, n, n, 0.0, nullptr, 2.0, P, 0.0);
 }
@@ -248,9 +390,7 @@ void sign_iterative(Ctx& x, const ptbgpu_pur_settings& pur, const double* guess,
     double* t2 = x.m[6];
     double* t3 = x.m[7];
     copy_mat(s, n, n, guess, n, Y);
-    for (int64_t i = 0; i < pur.cycles; ++i) {
-        const double norm = x.frob(Y);
-        ++*iters;
+    auto step = [&] {
         if (pur.type == PTBGPU_TYPE_PADE) {
             x.gemm(Y, Y, t1);
             x.gemm(t1, t1, t2);
@@ -263,8 +403,29 @@ void sign_iterative(Ctx& x, const ptbgpu_pur_settings& pur, const double* guess,
             x.gemm(Y, t1, t2);
             axpby_diag(s, n, n, -0.5, t2, 1.5, Y, 0.0);      // 0.5 (3X - X^3)
         }
+    };
+    for (int64_t i = 0; i < pur.cycles; ++i) {
+        const double norm = x.frob(Y);
+        ++*iters;
+        step();
         x.nan_check(Y, "Error: NaN is encountered during purification");
         if (std::fabs(x.frob(Y) - norm) < x.thr.normal) break;
+        // the remaining iterations as one graph launch (the stop rule on the device)
+        if (i + 1 < pur.cycles && graph_loops()) {
+            LoopDev* d = x.ld();
+            auto body = [&] {
+                frob_to_dev(x.c, n, n, Y, &d->norm0);
+                step();
+                nan_flag_dev(x.c, n * n, Y, &d->nan);
+                frob_to_dev(x.c, n, n, Y, &d->norm1);
+            };
+            if (x.build_loop(x.sign_loop, body, x.thr.normal, (long long)pur.cycles, 0)) {
+                const LoopDev r = x.run_loop(x.sign_loop, LoopDev{0.0, 0.0, (long long)(i + 1), 0, 0});
+                *iters += r.iters - (i + 1);
+                PTB_CHECK(r.nan == 0, PTBGPU_ENAN, "%s", "Error: NaN is encountered during purification");
+                break;
+            }
+        }
     }
     // sign_to_density uses m[6], m[7]; keep Y in m[4]
     sign_to_density(x, pur, Y, X, P);
