@@ -35,9 +35,12 @@ with the chemical-potential search, source/purification.f90) in FP64 on the
 32-H2O cluster, one call per solver type; the oracle is the CPU baseline.
 
 --workload lattice256 measures the uneven multi-instance batch instead: 256
-synthetic cubic-lattice systems (20-400 atoms, ndim 153-3064) purified by
-ptbgpu_tc_purify_batch (host worker threads, one stream each); one step = the
-whole batch, host buffers in and out (value and e2e are the same call).
+synthetic cubic-lattice systems (20-400 atoms, ndim 166-3064), every system's
+dense projector by the FP64 eigensolver in one launch
+(ptbgpu_eig_density_batch); one step = the whole batch, host buffers in and
+out (value and e2e are the same call).  The trace-correcting purification of
+the same systems (ptbgpu_tc_purify_batch, mixed and FP64, host worker threads)
+and the grouped entry are reported beside it.
 """
 from __future__ import annotations
 
@@ -522,59 +525,53 @@ def run_purify_types(args, rank, world, local, pg):
 
 
 def run_batch(args, rank, world, local, pg):
-    """The multi-instance batch: every rank purifies all 256 systems (replicas)."""
+    """The multi-instance batch: every rank solves all 256 systems (replicas).
+    The timed path is the library's FP64 eigensolver with every system in one
+    launch (ptbgpu_eig_density_batch: one CTA per system up to order 1024, one
+    thread-block cluster per larger system, P formed in the same launch); the
+    trace-correcting purification of the same systems (mixed precision and
+    FP64, host worker streams) and the grouped entry are reported beside it."""
     import torch
 
     from ptb_b200 import PREC_FP64, PREC_MIXED, Context, Options, synth
 
     systems = synth.make_config(4)
     args_b = [(s.ndim, s.nel, s.Hvec, s.Svec) for s in systems]
-    prec = PREC_FP64 if args.precision == "fp64" else PREC_MIXED
-    opts = Options(precision=prec)
     torch.cuda.set_device(local)
     ctx = Context(local)
     for _ in range(args.warmup):
-        ctx.tc_purify_batch(args_b, opts, workers=args.workers)
+        ctx.eig_density_batch(args_b)
     barrier(pg)
     walls, stats = [], None
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
-            Ps, stats, wall = ctx.tc_purify_batch(args_b, opts, workers=args.workers)
+            Ps, stats, wall = ctx.eig_density_batch(args_b)
             walls.append(wall)
     clocks = clk.summary()
     ms = reduce_max(pg, statistics.median(walls))
-    extra, grouped = {}, None
+    comparisons = {}
     if args.compare_fp64 and rank == 0:
+        Pm, stm, wallm = ctx.tc_purify_batch(args_b, Options(precision=PREC_MIXED), workers=args.workers)
         P64, st64, wall64 = ctx.tc_purify_batch(args_b, Options(precision=PREC_FP64), workers=args.workers)
-        extra = {"s_per_step": wall64 / 1e3,
-                 "max_abs_dP_mixed_vs_fp64": float(max(np.max(np.abs(a - b)) for a, b in zip(Ps, P64))),
-                 "speedup_mixed_vs_fp64": wall64 / ms}
-        # the same systems through the grouped entry (one launch per step per size bucket)
-        Pg, stg, wallg = ctx.tc_purify_grouped(args_b, opts)
-        grouped = {"entry": "ptbgpu_tc_purify_grouped", "s_per_step": wallg / 1e3,
-                   "max_abs_dP_vs_fp64": float(max(np.max(np.abs(a - b)) for a, b in zip(Pg, P64))),
-                   "fp64_fallbacks": sum(x.fp64_fallback for x in stg)}
-        # and through the FP64 eigensolver, all 256 systems in one launch (the dense
-        # projector per system: one CTA each up to order 1024, one cluster each above)
-        ctx.eig_density_batch(args_b)
-        ew = []
-        for _ in range(max(1, args.steps)):
-            t0 = time.perf_counter()
-            Pe, ste, walle = ctx.eig_density_batch(args_b)
-            ew.append(time.perf_counter() - t0)
-        eig_batch = {"entry": "ptbgpu_eig_density_batch", "s_per_step": statistics.median(ew),
-                     "note": "host wall clock of the whole call with the packed host arrays (copies inside), "
-                             "median of the timed calls",
-                     "max_abs_dP_vs_fp64": float(max(np.max(np.abs(a - b)) for a, b in zip(Pe, P64))),
-                     "gpu_launches_per_step": int(sum(x.kernel_launches for x in ste)) or None}
-        extra["eig_batch"] = eig_batch
+        Pg, stg, wallg = ctx.tc_purify_grouped(args_b, Options(precision=PREC_MIXED))
+        dmax = lambda X, Y: float(max(np.max(np.abs(a - b)) for a, b in zip(X, Y)))
+        comparisons = {
+            "purify_mixed": {"entry": "ptbgpu_tc_purify_batch (bf16x3 trace-correcting purification, FP64-class "
+                                      f"refinement, {args.workers} worker streams)", "s_per_step": wallm / 1e3,
+                             "max_abs_dP_vs_eig_batch": dmax(Pm, Ps),
+                             "refine_rounds": {str(r): sum(1 for x in stm if x.refine_rounds == r) for r in range(6)},
+                             "fp64_fallbacks": sum(x.fp64_fallback for x in stm),
+                             "gpu_launches": int(sum(x.kernel_launches for x in stm))},
+            "purify_fp64": {"entry": "ptbgpu_tc_purify_batch, FP64", "s_per_step": wall64 / 1e3,
+                            "max_abs_dP_vs_eig_batch": dmax(P64, Ps)},
+            "purify_grouped": {"entry": "ptbgpu_tc_purify_grouped", "s_per_step": wallg / 1e3,
+                               "max_abs_dP_vs_eig_batch": dmax(Pg, Ps)},
+            "speedup_eig_batch_vs_purify_mixed": wallm / ms, "speedup_eig_batch_vs_purify_fp64": wall64 / ms,
+        }
     if rank != 0:
         ctx.close()
         return
-    alg = sum(x.n_tc_sp2 * float(s.ndim) ** 3 + x.n_tc_full * 2.0 * float(s.ndim) ** 3 for x, s in zip(stats, systems))
-    tc_ms = sum(x.ms_tc_sp2 + x.ms_tc_full for x in stats)
-    peak_burst, peak_sust, hbm, peak_kind = load_peaks()
-    achieved = alg / tc_ms / 1e9 if tc_ms > 0 else 0.0
+    feig = float(sum(7.0 * float(s.ndim) ** 3 for s in systems))
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         from oracle import ptb_oracle as O
@@ -589,28 +586,28 @@ def run_batch(args, rank, world, local, pg):
     line = {
         "metric": METRIC, "value": ms / 1e3, "unit": "s/batch-of-256", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16x3+i8-sliced-f64+f64" if prec == PREC_MIXED else "f64", "data": "synthetic",
+        "dtype": "f64", "data": "synthetic",
         "config": {"workload": "uneven multi-instance batch: 256 cubic-lattice systems (20-400 atoms, ndim "
-                               f"{min(s.ndim for s in systems)}-{max(s.ndim for s in systems)}), trace-correcting "
-                               f"purification, {args.workers} worker streams",
+                               f"{min(s.ndim for s in systems)}-{max(s.ndim for s in systems)}), dense projector per "
+                               "system by the FP64 eigensolver, all systems in one launch",
                    "global_batch": 256 * world, "seq_len": max(s.ndim for s in systems),
-                   "parallelism": f"replicas x{world}", "l2": "inputs (6.4 GB packed) far larger than L2"},
+                   "parallelism": f"replicas x{world}", "l2": "inputs (6.2 GB packed) far larger than L2"},
         "e2e": {"value": ms / 1e3, "unit": "s/batch-of-256", "h2d_bytes_per_step": 2 * npk * 8,
-                "d2h_bytes_per_step": npk * 8},
-        "gpu_launches": int(sum(x.kernel_launches for x in stats)),
-        "roofline": {"bound": "tensor", "kernel": "k_tc_product (tcgen05 bf16x3)", "achieved": achieved,
-                     "peak": peak_sust, "unit": "TFLOP/s", "frac": achieved / peak_sust if peak_sust else None,
-                     "traffic": None, "peak_kind": f"{peak_kind} bf16 sustained",
-                     "note": "kernel time summed over the worker streams (launches overlap)"},
-        "refine_rounds": {str(r): sum(1 for x in stats if x.refine_rounds == r) for r in range(0, 6)},
-        "fp64_fallbacks": sum(x.fp64_fallback for x in stats),
+                "d2h_bytes_per_step": npk * 8,
+                "timing": "host wall clock of the whole C call (packed host arrays in and out, copies inside), "
+                          "median of the timed calls"},
+        "gpu_launches": int(sum(x.kernel_launches for x in stats)) * args.steps,
+        "roofline": {"bound": "fp64", "kernel": "k_eig_fused / k_eig_cluster (FP64 generalized eigensolver, DMMA "
+                                                "tile products)",
+                     "achieved": feig / (ms / 1e3) / 1e12, "peak": 37.0, "unit": "TFLOP/s",
+                     "frac": feig / (ms / 1e3) / 1e12 / 37.0, "traffic": None,
+                     "peak_kind": "nominal B200 FP64 (no measured FP64 figure on this pool)",
+                     "work": "7 m^3 per system (dsygvd with vectors), the whole call's wall time"},
         "cpu_baseline": cpu,
         "clocks": clocks,
     }
-    if extra:
-        line["fp64_gpu"] = extra
-    if grouped:
-        line["grouped"] = grouped
+    if comparisons:
+        line["comparisons"] = comparisons
     print(json.dumps(line), flush=True)
     ctx.close()
 

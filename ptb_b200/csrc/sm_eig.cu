@@ -2724,6 +2724,7 @@ struct EigBatch {
     std::vector<EigProb> hp;
     DevBuf probs, order, order_l, counter, Ca, La, Za, Qa, Va, Da, Ea, Ta, Wa, Ba, Xa, Ka, status, tstage;
     int prl = 0;
+    const char* what = "submatrix";   // the problems' name in error messages
     cudaStream_t side = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~EigBatch() {
@@ -2824,7 +2825,7 @@ void launch_clustered(K kern, int nclusters, int G, size_t smem, cudaStream_t s,
 std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const double* H, const double* S,
                                            const std::vector<EigProbHost>& probs, const int* d_maps,
                                             const int* d_own_cols, const int* d_ipos, double* d_e, double* d_fe,
-                                            int prl, double* flops) {
+                                            int prl, double* flops, bool join) {
     if (probs.empty()) return nullptr;
     eig_setup_attrs();
     cudaStream_t s = c->stream;
@@ -2938,8 +2939,12 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
         count_launch();
         PTB_CUDA(cudaGetLastError());
     }
-    if (eb->nlarge > 0) PTB_CUDA(cudaStreamWaitEvent(s, eb->ev1, 0));
+    if (eb->nlarge > 0 && join) PTB_CUDA(cudaStreamWaitEvent(s, eb->ev1, 0));
     return eb;
+}
+
+void eig_batch_join(ptbgpu_ctx* c, EigBatch& eb) {
+    if (eb.nlarge > 0 && eb.ev1) PTB_CUDA(cudaStreamWaitEvent(c->stream, eb.ev1, 0));
 }
 
 void eig_batch_check(ptbgpu_ctx* c, EigBatch& eb) {
@@ -2949,10 +2954,10 @@ void eig_batch_check(ptbgpu_ctx* c, EigBatch& eb) {
     PTB_CUDA(cudaMemcpyAsync(hst.data(), eb.status.ptr, sizeof(int) * np, cudaMemcpyDeviceToHost, s));
     PTB_CUDA(cudaStreamSynchronize(s));
     for (int q = 0; q < np; ++q)
-        PTB_CHECK(hst[q] <= 0, PTBGPU_ENOTSPD, "overlap submatrix %d not positive definite (leading minor %d)",
+        PTB_CHECK(hst[q] <= 0, PTBGPU_ENOTSPD, "overlap of %s %d not positive definite (leading minor %d)", eb.what,
                   eb.hp[q].k + 1, hst[q]);
     for (int q = 0; q < np; ++q)
-        PTB_CHECK(hst[q] == kStOk, PTBGPU_EITER, "tridiagonal eigensolver did not converge on submatrix %d",
+        PTB_CHECK(hst[q] == kStOk, PTBGPU_EITER, "tridiagonal eigensolver did not converge on %s %d", eb.what,
                   eb.hp[q].k + 1);
     if (eb.prl >= 2 && eb.nlarge > 0 && eb.tstage.ptr) {
         // per stage: summed over the large submatrices and the longest one, then
@@ -3159,16 +3164,21 @@ void eig_density_batch(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const 
                        int prl, ptbgpu_stats* st) {
     if (ninst <= 0) return;
     cudaStream_t s = c->stream;
-    std::vector<EigProbHost> probs;
+    // The systems above kEigBatchMax are copied in and launched on their
+    // clusters first; the small ones are copied in while those run, then solved
+    // by the persistent launch beside them, and their results copied out while
+    // the clusters finish.
+    std::vector<int64_t> large, small;
     std::vector<int64_t> pkoff((size_t)ninst + 1, 0);
     int64_t hsz = 0, nsum = 0;
+    std::vector<EigProbHost> pr((size_t)ninst);
     for (int64_t k = 0; k < ninst; ++k) {
         const int64_t m = ndim[k];
         PTB_CHECK(m >= 1 && m <= kLargeMax, PTBGPU_EINVAL, "system %lld: ndim %lld outside the eigensolver (1..%d)",
                   (long long)k, (long long)m, kLargeMax);
         PTB_CHECK(nel[k] >= 0 && nel[k] / 2 <= m && Hpk[k] && Spk[k] && Ppk[k], PTBGPU_EINVAL,
                   "system %lld: bad electron count or arrays", (long long)k);
-        EigProbHost q{};
+        EigProbHost& q = pr[k];
         q.k = (int)k;
         q.m = (int)m;
         q.nown = 0;
@@ -3179,10 +3189,10 @@ void eig_density_batch(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const 
         q.gld = m;
         q.mode = 2;
         q.nocc = (int)(nel[k] / 2);
-        probs.push_back(q);
         hsz += m * m;
         nsum += m;
         pkoff[k + 1] = pkoff[k] + m * (m + 1) / 2;
+        (m > kEigBatchMax ? large : small).push_back(k);
     }
     struct Bufs {
         DevBuf h, sm, pk, maps, e, dummy;
@@ -3197,30 +3207,53 @@ void eig_density_batch(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const 
     b.e.reserve(sizeof(double) * nsum);
     b.dummy.reserve(64);
     std::vector<int> maps((size_t)nsum);
-    for (const EigProbHost& q : probs)
+    for (const EigProbHost& q : pr)
         for (int i = 0; i < q.m; ++i) maps[q.moff + i] = i;
     PTB_CUDA(cudaMemcpyAsync(b.maps.ptr, maps.data(), sizeof(int) * nsum, cudaMemcpyHostToDevice, s));
     double* pkH = b.pk.as<double>();
     double* pkS = pkH + pkoff[ninst];
-    for (int64_t k = 0; k < ninst; ++k) {
-        const int64_t m = ndim[k], np = m * (m + 1) / 2;
-        PTB_CUDA(cudaMemcpyAsync(pkH + pkoff[k], Hpk[k], sizeof(double) * np, cudaMemcpyHostToDevice, s));
-        PTB_CUDA(cudaMemcpyAsync(pkS + pkoff[k], Spk[k], sizeof(double) * np, cudaMemcpyHostToDevice, s));
-        unpack_sym(s, m, m, pkH + pkoff[k], b.h.as<double>() + probs[k].gbase, filter);
-        unpack_sym(s, m, m, pkS + pkoff[k], b.sm.as<double>() + probs[k].gbase, filter);
+    auto upload = [&](const std::vector<int64_t>& ids) {
+        for (int64_t k : ids) {
+            const int64_t m = ndim[k], np = m * (m + 1) / 2;
+            PTB_CUDA(cudaMemcpyAsync(pkH + pkoff[k], Hpk[k], sizeof(double) * np, cudaMemcpyHostToDevice, s));
+            PTB_CUDA(cudaMemcpyAsync(pkS + pkoff[k], Spk[k], sizeof(double) * np, cudaMemcpyHostToDevice, s));
+            unpack_sym(s, m, m, pkH + pkoff[k], b.h.as<double>() + pr[k].gbase, filter);
+            unpack_sym(s, m, m, pkS + pkoff[k], b.sm.as<double>() + pr[k].gbase, filter);
+        }
+    };
+    auto launch = [&](const std::vector<int64_t>& ids, bool join) {
+        std::vector<EigProbHost> probs;
+        for (int64_t k : ids) probs.push_back(pr[k]);
+        double flops = 0.0;
+        auto eb = eig_batch_launch(c, 0, b.h.as<double>(), b.sm.as<double>(), probs, b.maps.as<int>(),
+                                   b.dummy.as<int>(), b.dummy.as<int>(), b.e.as<double>(), b.e.as<double>(), prl,
+                                   &flops, join);
+        eb->what = "system";
+        return eb;
+    };
+    auto download = [&](EigBatch& eb, const std::vector<int64_t>& ids) {
+        for (size_t q = 0; q < ids.size(); ++q) {
+            const int64_t k = ids[q], m = ndim[k], np = m * (m + 1) / 2;
+            const int grid = (int)std::min<int64_t>((np + 255) / 256, 148 * 8);
+            k_pack_scaled<<<grid, 256, 0, s>>>(m, eb.Ba.as<double>() + eb.hp[q].boff, 2.0, pkH + pkoff[k]);
+            count_launch();
+            PTB_CUDA(cudaGetLastError());
+            PTB_CUDA(cudaMemcpyAsync(Ppk[k], pkH + pkoff[k], sizeof(double) * np, cudaMemcpyDeviceToHost, s));
+        }
+    };
+    std::shared_ptr<EigBatch> ebl, ebs;   // declared after b: released (side stream drained) before its buffers
+    upload(large);
+    if (!large.empty()) ebl = launch(large, false);
+    upload(small);
+    if (!small.empty()) {
+        ebs = launch(small, true);
+        eig_batch_check(c, *ebs);
+        download(*ebs, small);
     }
-    double flops = 0.0;
-    std::shared_ptr<EigBatch> eb = eig_batch_launch(c, 0, b.h.as<double>(), b.sm.as<double>(), probs,
-                                                    b.maps.as<int>(), b.dummy.as<int>(), b.dummy.as<int>(),
-                                                    b.e.as<double>(), b.e.as<double>(), prl, &flops);
-    eig_batch_check(c, *eb);
-    for (int64_t k = 0; k < ninst; ++k) {
-        const int64_t m = ndim[k], np = m * (m + 1) / 2;
-        const int grid = (int)std::min<int64_t>((np + 255) / 256, 148 * 8);
-        k_pack_scaled<<<grid, 256, 0, s>>>(m, eb->Ba.as<double>() + eb->hp[k].boff, 2.0, pkH + pkoff[k]);
-        count_launch();
-        PTB_CUDA(cudaGetLastError());
-        PTB_CUDA(cudaMemcpyAsync(Ppk[k], pkH + pkoff[k], sizeof(double) * np, cudaMemcpyDeviceToHost, s));
+    if (ebl) {
+        eig_batch_join(c, *ebl);
+        eig_batch_check(c, *ebl);
+        download(*ebl, large);
     }
     PTB_CUDA(cudaStreamSynchronize(s));
     if (st)

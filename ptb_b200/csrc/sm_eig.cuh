@@ -41,7 +41,10 @@ struct EigBatch;
 std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const double* H, const double* S,
                                            const std::vector<EigProbHost>& probs, const int* d_maps,
                                            const int* d_own_cols, const int* d_ipos, double* d_e, double* d_fe,
-                                           int prl, double* flops);
+                                           int prl, double* flops, bool join = true);
+// With join = false the launch's side stream (the clusters of the problems
+// above kEigBatchMax) is not waited for on the context's stream; this does it.
+void eig_batch_join(ptbgpu_ctx* c, EigBatch& eb);
 void eig_batch_check(ptbgpu_ctx* c, EigBatch& eb);
 
 // The owned columns of P_k = U occ U^T at mu for every prepared problem,

@@ -61,7 +61,7 @@ def test_non_positive_definite_overlap_names_the_system(ctx, water8):
     bad[0] = -1.0                                   # S_11 < 0
     with pytest.raises(PtbGpuError) as ei:
         ctx.eig_density_batch([(s.ndim, s.nel, s.Hvec, s.Svec), (s.ndim, s.nel, s.Hvec, bad)])
-    assert ei.value.code == api.ENOTSPD and "submatrix 2" in str(ei.value)
+    assert ei.value.code == api.ENOTSPD and "system 2" in str(ei.value)
 
 
 def test_empty_batch(ctx):
