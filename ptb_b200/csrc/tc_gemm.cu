@@ -265,6 +265,14 @@ __global__ void __launch_bounds__(THREADS, 1)
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
+    // only the planes some product reads are loaded (the bytes the full barrier expects follow)
+    uint32_t amask = 0, bmask = 0;
+    for (int p = 0; p < prods.n; ++p) {
+        amask |= 1u << prods.a[p];
+        bmask |= 1u << prods.b[p];
+    }
+    const uint32_t stage_tx = (uint32_t)(__popc(amask) * A_TILE_BYTES + __popc(bmask) * B_TILE_BYTES);
+
     if (warp == 0 && lane == 0) {
         // ---------------- TMA producer ----------------
         int issued_phase[STAGES];
@@ -277,11 +285,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                 break;
             }
             if (*(volatile int*)abort_flag) break;
-            mbar_expect_tx(full_bar(s), STAGE_BYTES);
+            mbar_expect_tx(full_bar(s), stage_tx);
             for (int p = 0; p < NP; ++p)
-                tma_load_2d(a_tile(s, p), &maps.a[p], full_bar(s), kb * KB, bi * BM);
+                if ((amask >> p) & 1u) tma_load_2d(a_tile(s, p), &maps.a[p], full_bar(s), kb * KB, bi * BM);
             for (int p = 0; p < NP; ++p)
-                tma_load_2d(b_tile(s, p), &maps.b[p], full_bar(s), kb * KB, bj * BN);
+                if ((bmask >> p) & 1u) tma_load_2d(b_tile(s, p), &maps.b[p], full_bar(s), kb * KB, bj * BN);
             issued_phase[s] = round & 1;
         }
         // drain: every copy this thread issued has landed before the CTA may exit
@@ -405,6 +413,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
+    uint32_t amask = 0, bmask = 0;   // planes some product reads (both CTAs: the same list)
+    for (int p = 0; p < prods.n; ++p) {
+        amask |= 1u << prods.a[p];
+        bmask |= 1u << prods.b[p];
+    }
+    const uint32_t stage_tx = (uint32_t)(__popc(amask) * C::A_TILE_BYTES + __popc(bmask) * C::B_TILE_BYTES);
+
     if (warp == 0 && lane == 0) {
         // ---------------- TMA producer (both CTAs) ----------------
         int issued_phase[STAGES];
@@ -417,11 +432,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                 break;
             }
             if (*(volatile int*)abort_flag) break;
-            if (rank == 0) mbar_expect_tx(full_bar(s), 2 * STAGE_BYTES);   // both CTAs' bytes
+            if (rank == 0) mbar_expect_tx(full_bar(s), 2 * stage_tx);   // both CTAs' bytes
             const uint32_t fb = mapa_shared(full_bar(s), 0);
-            for (int p = 0; p < NP; ++p) tma_load_2d_pair(a_tile(s, p), &maps.a[p], fb, kb * KB, bi * BM);
             for (int p = 0; p < NP; ++p)
-                tma_load_2d_pair(b_tile(s, p), &maps.b[p], fb, kb * KB, bj * 256 + (int)rank * 128);
+                if ((amask >> p) & 1u) tma_load_2d_pair(a_tile(s, p), &maps.a[p], fb, kb * KB, bi * BM);
+            for (int p = 0; p < NP; ++p)
+                if ((bmask >> p) & 1u)
+                    tma_load_2d_pair(b_tile(s, p), &maps.b[p], fb, kb * KB, bj * 256 + (int)rank * 128);
             issued_phase[s] = round & 1;
         }
         // drain: the leader sees every copy of the pair land on its full barriers;
@@ -605,8 +622,10 @@ int launch_product(cudaStream_t s, int epi, int np, long long ld, const void* co
               "the CTA-pair kernel needs two planes and pair tiles");
     PTB_CHECK(ld % 256 == 0, PTBGPU_EINVAL, "leading dimension must be a multiple of 256");
     const int bn = np == 2 ? 256 : 128;
+    PTB_CHECK(prods.n >= 1 && prods.n <= 6, PTBGPU_EINVAL, "1 to 6 plane products (got %d)", prods.n);
     for (int p = 0; p < prods.n; ++p)
-        PTB_CHECK(prods.a[p] < np && prods.b[p] < np, PTBGPU_EINVAL, "product references a missing plane");
+        PTB_CHECK(prods.a[p] >= 0 && prods.a[p] < np && prods.b[p] >= 0 && prods.b[p] < np, PTBGPU_EINVAL,
+                  "product references a missing plane");
     PTB_CHECK(epi != EPI_SP2 || (ep.hi != nullptr && ep.lo != nullptr), PTBGPU_EINVAL,
               "the SP2 epilogue writes at least two planes");
     // returns the number of per-CTA stats partials the launch writes
