@@ -6,7 +6,8 @@
 // quirks (documented beside each routine).  Dense column-major matrices; the
 // products run on the int8 tensor cores as FP64-class sliced products
 // (oz_dgemm), the eigendecompositions of the metric and of the eigen-sign
-// solver on cuSOLVER DSYEVD.
+// solver on the library's FP64 eigensolver (dsyevd: one thread-block cluster
+// up to order 4096, a cooperative grid up to 12032, cuSOLVER DSYEVD above).
 #include <algorithm>
 #include <cmath>
 #include <vector>

@@ -2955,11 +2955,9 @@ std::shared_ptr<EigBatch> eig_batch_launch(ptbgpu_ctx* c, int64_t n, const doubl
                  eb->nlarge, kEigBatchMax, eb->G);
     }
     if (eb->nsmall > 0) {
-        const int M = (std::min(eb->maxm, kEigBatchMax) + 1) & ~1;
         int Msmall = 0;
         for (int q : ord_s) Msmall = std::max(Msmall, eb->hp[q].m);
-        const int Ms = (Msmall + 1) & ~1;
-        (void)M;
+        const int Ms = (Msmall + 1) & ~1;   // staging sized for the largest small problem
         const int grid = std::min(eb->nsmall, c->num_sms > 0 ? c->num_sms : 148);
         k_eig_fused<<<grid, kT, stage_smem_bytes(Ms), s>>>(
             dp, eb->order.as<int>(), eb->nsmall, eb->counter.as<int>(), Ms, d_maps, H, S, eb->Ca.as<double>(),

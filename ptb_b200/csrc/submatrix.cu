@@ -542,8 +542,9 @@ struct Bucket {
     DevBuf probs, U, w;
 };
 
-// Side streams for the large submatrices (one generalized eigensolve each):
-// cuSOLVER's dsygvd at these sizes is latency-bound (tridiagonalisation), so
+// Side streams for the large submatrices of the cuSOLVER comparison path
+// (PTBGPU_SM_EIG=library; one generalized eigensolve each): cuSOLVER's dsygvd
+// at these sizes is latency-bound (tridiagonalisation), so
 // several run at once, each on its own stream and handles, driven by its own
 // host thread.  Kept on the context between calls.
 struct SidePool {
@@ -630,8 +631,8 @@ struct SmPlan {
 
 namespace {
 
-// ---- size-bucket schedule of the batched eigensolver -----------------------
-// The batched cuSOLVER eigensolver costs about L(M) + p(M) B for B problems
+// ---- size-bucket schedule of the cuSOLVER comparison path ------------------
+// The batched cuSOLVER eigensolver (PTBGPU_SM_EIG=library) costs about L(M) + p(M) B for B problems
 // padded to M (a launch/latency term that does not shrink with B, and a
 // per-problem term): fine buckets of a few problems each pay L many times.
 // The cost model is measured once per device and padded size (random symmetric
@@ -853,10 +854,11 @@ SmPlan& sm_plan(ptbgpu_ctx* c, int64_t n, const double* dH, const double* dS, in
     return pl;
 }
 
-// (4)-(5): gather, reduction (potrf + 2 trsm), eigensolve and fe weights of
-// the listed submatrices (0-based, each at most once): buckets of padded size
-// <= 1024 through the batched cuSOLVER / cuBLAS calls, larger ones one dsygvd
-// each.  Their eigenpairs replace any earlier prepared set.
+// (4)-(5): gather, reduction, eigensolve and fe weights of the listed
+// submatrices (0-based, each at most once), by the library's eigensolver
+// (sm_eig.cu) or, with PTBGPU_SM_EIG=library, in buckets of padded size <= 1024
+// through the batched cuSOLVER / cuBLAS calls and one dsygvd per larger one.
+// Their eigenpairs replace any earlier prepared set.
 void sm_prepare(ptbgpu_ctx* c, SmPlan& pl, const std::vector<int>& ids) {
     cudaStream_t s = c->stream;
     const int prl = pl.prl;
