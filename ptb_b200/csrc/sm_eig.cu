@@ -2071,10 +2071,12 @@ __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca
             // in registers for the unit, each column's sum is a warp reduction;
             // both go to their own slots (rowp[segment][r], colp[tile row][c]),
             // summed in a fixed order when w is formed.  v^T A v comes from the
-            // same sums.
+            // same sums.  Warps are numbered across the CTAs (warp-major), so
+            // consecutive units land on different SMs: with fewer units than
+            // warps (small orders) every SM's L2 bandwidth still takes part.
             {
                 const int I0 = s / TS, cstart = I0 * TS;
-                const int gw = rk * (kT / 32) + warp, nw = G * (kT / 32);
+                const int gw = warp * G + rk, nw = G * (kT / 32);
                 double vav = 0.0;
                 int I = I0, ubase = 0;
                 for (int u = gw;; u += nw) {
@@ -2414,8 +2416,9 @@ __device__ bool lg_dc(const Grp& g, const EigProb& p, const double* __restrict__
             S.D[pos] -= ab;
         }
     g.sync();
-    // leaves: a warp each over the whole cluster
-    for (int q = g.rank * (kT / 32) + warp; q < nleaf; q += g.size * (kT / 32)) {
+    // leaves: a warp each over the whole cluster, numbered warp-major so that
+    // few leaves still spread over every SM
+    for (int q = warp * g.size + g.rank; q < nleaf; q += g.size * (kT / 32)) {
         const int lo = (int)(((int64_t)q * m) >> L), hi = (int)(((int64_t)(q + 1) * m) >> L), s = hi - lo;
         double dl[kDcLeaf], el[kDcLeaf], zl[kDcLeaf];
         for (int i = 0; i < kDcLeaf; ++i) {
