@@ -1908,9 +1908,12 @@ __device__ __forceinline__ int av_nseg(int I, int cstart) {
     return ((I + 1) * TS - cstart + kSegW - 1) / kSegW;
 }
 
-__device__ double lg_finish_w(const Grp& g, int m, int j, int jp, double* __restrict__ A, double* __restrict__ V,
-                              double* __restrict__ W, const double* __restrict__ rowp,
-                              const double* __restrict__ colp, const double* __restrict__ red, const LgSmem& sh) {
+// w of column jp of the panel (the column before j) on this CTA's rows, with the
+// reflector stored into A's column j-1; w_j itself goes to sh.wj[jp], computed
+// by the last warp beside the row loop.  The caller synchronises the CTA.
+__device__ void lg_finish_w(const Grp& g, int m, int j, int jp, double* __restrict__ A, double* __restrict__ V,
+                            double* __restrict__ W, const double* __restrict__ rowp,
+                            const double* __restrict__ colp, const double* __restrict__ red, const LgSmem& sh) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double tp = sh.dsc[0];
     double vAv = 0.0;
@@ -1931,6 +1934,7 @@ __device__ double lg_finish_w(const Grp& g, int m, int j, int jp, double* __rest
         for (int q = 0; q < jp; ++q) y -= V[r + (int64_t)q * m] * sh.wtv[q] + W[r + (int64_t)q * m] * sh.vtv[q];
         return tp * (y - hc * sh.v[r]);
     };
+    if (tid == kT - 32 && j < m) sh.wj[jp] = w_at(j);
     for (int ch = g.rank + g.size * warp; ch * 32 < m; ch += g.size * (kT / 32)) {
         const int r = ch * 32 + lane;
         if (r >= j && r < m) {
@@ -1938,13 +1942,6 @@ __device__ double lg_finish_w(const Grp& g, int m, int j, int jp, double* __rest
             if (r >= j + 1) A[r + (int64_t)(j - 1) * m] = sh.v[r];
         }
     }
-    if (j < m) {
-        if (tid == 0) sh.dsc[2] = w_at(j);
-    }
-    __syncthreads();
-    const double wr = sh.dsc[2];
-    __syncthreads();
-    return wr;
 }
 
 __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca, double* __restrict__ Da,
@@ -1972,13 +1969,13 @@ __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca
         for (int jj = 0; jj < nb; ++jj) {
             const int j = j0 + jj;
             // ---- phase A: finish w of the previous column, update column j on own rows
-            double wrow = 0.0;
-            if (jj > 0) wrow = lg_finish_w(g, m, j, jj - 1, A, V, W, rowp, colp, red, sh);
+            // (row j of the panel's V and earlier W columns were written before the
+            // last cluster barrier; w_j of the previous column comes from lg_finish_w)
             if (tid < jj) {
-                const int q = tid;
-                sh.wj[q] = (q == jj - 1) ? wrow : W[j + (int64_t)q * m];
-                sh.vj[q] = V[j + (int64_t)q * m];
+                if (tid < jj - 1) sh.wj[tid] = W[j + (int64_t)tid * m];
+                sh.vj[tid] = V[j + (int64_t)tid * m];
             }
+            if (jj > 0) lg_finish_w(g, m, j, jj - 1, A, V, W, rowp, colp, red, sh);
             __syncthreads();
             for (int ch = rk + G * warp; ch * 32 < m; ch += G * (kT / 32)) {
                 const int r = ch * 32 + lane;
