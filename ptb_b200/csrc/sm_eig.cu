@@ -2011,6 +2011,9 @@ __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca
             g.sync();
             pc.lap(1);
             // ---- phase B: reflector, then y = A v over the trailing lower tiles
+            // (column j below the subdiagonal is read into v while the scale is
+            // formed, and scaled in shared memory after the barrier)
+            double wj1 = 0.0, vj1 = 0.0;
             if (tid < jj) {
                 double a = 0.0, b = 0.0;
                 for (int q = 0; q < G; ++q) {
@@ -2019,7 +2022,10 @@ __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca
                 }
                 sh.pw[tid] = a;
                 sh.pv[tid] = b;
+                wj1 = W[(j + 1) + (int64_t)tid * m];
+                vj1 = V[(j + 1) + (int64_t)tid * m];
             }
+            for (int r = j + 2 + tid; r < m; r += kT) v[r] = A[r + (int64_t)j * m];
             if (tid == 32) {
                 double xn2 = 0.0;
                 for (int q = 0; q < G; ++q) xn2 += red[q * kRedW + 0];
@@ -2047,12 +2053,12 @@ __device__ void lg_sytrd(const Grp& g, const EigProb& p, double* __restrict__ Ca
                 double vr;
                 if (r <= j) vr = 0.0;
                 else if (r == j + 1) vr = 1.0;
-                else vr = (sc == 0.0) ? 0.0 : A[r + (int64_t)j * m] * sc;
+                else vr = (sc == 0.0) ? 0.0 : v[r] * sc;
                 v[r] = vr;
             }
             if (tid < jj) {
-                sh.wtv[tid] = W[(j + 1) + (int64_t)tid * m] + sc * sh.pw[tid];
-                sh.vtv[tid] = V[(j + 1) + (int64_t)tid * m] + sc * sh.pv[tid];
+                sh.wtv[tid] = wj1 + sc * sh.pw[tid];
+                sh.vtv[tid] = vj1 + sc * sh.pv[tid];
             }
             const int s = j + 1;
             for (int r = s + tid; r < m; r += kT) yl[r] = 0.0;
