@@ -181,6 +181,17 @@ def _packed(a, ndim: int, what: str) -> np.ndarray:
     return x
 
 
+def _out_packed(out, ndim: int) -> np.ndarray:
+    """A caller-provided output array for a packed matrix of order ndim (for
+    instance in pinned host memory, which the device-to-host copy needs for
+    full speed), or a new one."""
+    if out is None:
+        return np.empty(npacked(ndim))
+    if out.dtype != np.float64 or out.size != npacked(ndim) or not out.flags.c_contiguous:
+        raise ValueError("out must be a contiguous float64 array of npacked(ndim) elements")
+    return out
+
+
 def _vec(a, count: int, what: str, conv=None) -> np.ndarray:
     """An array of exactly count elements (float64, or int64 with conv=_i64)."""
     x = (conv or _f64)(a)
@@ -303,10 +314,13 @@ class Context:
 
     def sm_stupid_simple(self, ndim: int, nelref: int, Hvec: np.ndarray, Svec: np.ndarray, n: int,
                          xyz: np.ndarray, aoat: np.ndarray, submatrix_columns: int, submatrix_mode: int,
-                         partition: np.ndarray | None = None, opts: Options | None = None):
-        """Submatrix density step, source/sm.f90:34-409.  Returns (Pvec, Stats)."""
+                         partition: np.ndarray | None = None, opts: Options | None = None,
+                         out: np.ndarray | None = None):
+        """Submatrix density step, source/sm.f90:34-409.  Returns (Pvec, Stats).
+        out: a preallocated contiguous float64 array of npacked(ndim) elements
+        for P (every element is written)."""
         H, S = _packed(Hvec, ndim, "Hvec"), _packed(Svec, ndim, "Svec")
-        P = np.zeros(npacked(ndim))
+        P = _out_packed(out, ndim)
         xyz_a = _vec(xyz, 3 * n, "xyz")
         ao = _vec(aoat, ndim, "aoat", _i64)
         part = _i64(partition) if partition is not None else None
@@ -394,12 +408,7 @@ class Context:
         out: a preallocated contiguous float64 array of npacked(ndim) elements for P (e.g. in
         pinned memory, which the device-to-host copy needs for full speed)."""
         Hh, Sh = _packed(H, ndim, "H"), _packed(S, ndim, "S")
-        if out is not None:
-            if out.dtype != np.float64 or out.size != npacked(ndim) or not out.flags.c_contiguous:
-                raise ValueError("out must be a contiguous float64 array of npacked(ndim) elements")
-            P = out
-        else:
-            P = np.empty(npacked(ndim))
+        P = _out_packed(out, ndim)
         st = _Stats()
         o = (opts or Options()).to_c()
         self._check(self._lib.ptbgpu_tc_purify(self._h, int(ndim), int(nel), _dptr(Hh), _dptr(Sh), _dptr(P),

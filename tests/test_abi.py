@@ -154,6 +154,23 @@ def test_wrong_array_lengths_are_rejected_before_the_c_call():
         assert ei.value.code == api.EINVAL, k
 
 
+def test_output_arrays_are_checked_before_the_c_call():
+    """A caller-provided P (e.g. in pinned memory) must be contiguous float64
+    of npacked(ndim) elements."""
+    import numpy as np
+    ctx = _unbound_context()
+    n, nat = 10, 4
+    npk = n * (n + 1) // 2
+    pk = np.zeros(npk)
+    aoat, xyz = np.repeat(np.arange(1, nat + 1), [3, 3, 2, 2]), np.zeros((nat, 3))
+    bad = [np.zeros(npk - 1), np.zeros(npk, dtype=np.float32), np.zeros(2 * npk)[::2]]
+    for out in bad:
+        with pytest.raises(ValueError):
+            ctx.sm_stupid_simple(n, 8, pk, pk, nat, xyz, aoat, 2, 2, out=out)
+        with pytest.raises(ValueError):
+            ctx.tc_purify(n, 8, pk, pk, out=out)
+
+
 FORTRAN_MODULE = HEADER.parent / "ptbgpu_c.f90"
 FORTRAN_SHIMS = HEADER.parent / "ptbgpu_shims.f90"
 
