@@ -40,7 +40,9 @@ dense projector by the FP64 eigensolver in one launch
 (ptbgpu_eig_density_batch); one step = the whole batch, host buffers in and
 out (value and e2e are the same call).  The trace-correcting purification of
 the same systems (ptbgpu_tc_purify_batch, mixed and FP64, host worker threads)
-and the grouped entry are reported beside it.
+and the grouped entry are reported beside it.  With N > 1 the 256 systems are
+split over the ranks (size-balanced, no collective) and the batch's time is the
+maximum over ranks.
 """
 from __future__ import annotations
 
@@ -148,6 +150,15 @@ def reduce_max(pg, value: float) -> float:
     import torch
     t = torch.tensor([value], device="cuda", dtype=torch.float64)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], device="cuda", dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -531,17 +542,27 @@ def run_purify_types(args, rank, world, local, pg):
 
 
 def run_batch(args, rank, world, local, pg):
-    """The multi-instance batch: every rank solves all 256 systems (replicas).
-    The timed path is the library's FP64 eigensolver with every system in one
-    launch (ptbgpu_eig_density_batch: one CTA per system up to order 1024, one
-    thread-block cluster per larger system, P formed in the same launch); the
-    trace-correcting purification of the same systems (mixed precision and
-    FP64, host worker streams) and the grouped entry are reported beside it."""
+    """The multi-instance batch of 256 independent systems.  The timed path is
+    the library's FP64 eigensolver with every system in one launch
+    (ptbgpu_eig_density_batch: one CTA per system up to order 1024, one
+    thread-block cluster per larger system, P formed in the same launch).  On
+    one GPU the trace-correcting purification of the same systems (mixed
+    precision and FP64, host worker streams) and the grouped entry are reported
+    beside it.  With N ranks the systems are split size-balanced (decreasing
+    ndim^3 to the least-loaded rank, the submatrix shards' rule) and each rank
+    solves its share in one launch: no collective, the batch's time is the
+    maximum over ranks (strong scaling of the fixed batch)."""
     import torch
 
     from ptb_b200 import PREC_FP64, PREC_MIXED, Context, Options, synth
 
-    systems = synth.make_config(4)
+    all_systems = synth.make_config(4)
+    if world > 1:
+        from ptb_b200.distributed import assign_submatrices
+        share = assign_submatrices([s.ndim for s in all_systems], world)[rank]
+        systems = [all_systems[k] for k in share]
+    else:
+        systems = all_systems
     args_b = [(s.ndim, s.nel, s.Hvec, s.Svec) for s in systems]
     torch.cuda.set_device(local)
     ctx = Context(local)
@@ -556,7 +577,7 @@ def run_batch(args, rank, world, local, pg):
     clocks = clk.summary()
     ms = reduce_max(pg, statistics.median(walls))
     comparisons = {}
-    if args.compare_fp64 and rank == 0:
+    if args.compare_fp64 and world == 1:
         Pm, stm, wallm = ctx.tc_purify_batch(args_b, Options(precision=PREC_MIXED), workers=args.workers)
         P64, st64, wall64 = ctx.tc_purify_batch(args_b, Options(precision=PREC_FP64), workers=args.workers)
         Pg, stg, wallg = ctx.tc_purify_grouped(args_b, Options(precision=PREC_MIXED))
@@ -574,10 +595,11 @@ def run_batch(args, rank, world, local, pg):
                                "max_abs_dP_vs_eig_batch": dmax(Pg, Ps)},
             "speedup_eig_batch_vs_purify_mixed": wallm / ms, "speedup_eig_batch_vs_purify_fp64": wall64 / ms,
         }
+    launches = reduce_sum(pg, float(sum(x.kernel_launches for x in stats)) * args.steps)
     if rank != 0:
         ctx.close()
         return
-    feig = float(sum(7.0 * float(s.ndim) ** 3 for s in systems))
+    feig = float(sum(7.0 * float(s.ndim) ** 3 for s in all_systems))
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         from oracle import ptb_oracle as O
@@ -588,26 +610,31 @@ def run_batch(args, rank, world, local, pg):
         cpu = {"value": t, "unit": "s/batch-of-256", "cores": os.cpu_count(), "kind": "port",
                "sample": f"oracle solve2 (dsygvd + Fermi + C f C^T, scipy OpenBLAS, {os.cpu_count()} threads) on "
                          "all 256 systems, one whole batch"}
-    npk = sum(s.ndim * (s.ndim + 1) // 2 for s in systems)
+    npk = sum(s.ndim * (s.ndim + 1) // 2 for s in all_systems)
     line = {
         "metric": METRIC, "value": ms / 1e3, "unit": "s/batch-of-256", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak" if world == 1 else "strong", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": "uneven multi-instance batch: 256 cubic-lattice systems (20-400 atoms, ndim "
-                               f"{min(s.ndim for s in systems)}-{max(s.ndim for s in systems)}), dense projector per "
-                               "system by the FP64 eigensolver, all systems in one launch",
-                   "global_batch": 256 * world, "seq_len": max(s.ndim for s in systems),
-                   "parallelism": f"replicas x{world}", "l2": "inputs (6.2 GB packed) far larger than L2"},
+                               f"{min(s.ndim for s in all_systems)}-{max(s.ndim for s in all_systems)}), dense "
+                               "projector per system by the FP64 eigensolver, all systems (of a rank's share) in one "
+                               "launch",
+                   "global_batch": 256, "seq_len": max(s.ndim for s in all_systems),
+                   "parallelism": "one GPU" if world == 1 else
+                   f"systems sharded over {world} ranks (size-balanced by ndim^3, no collective)",
+                   "l2": "inputs (6.2 GB packed) far larger than L2"},
         "e2e": {"value": ms / 1e3, "unit": "s/batch-of-256", "h2d_bytes_per_step": 2 * npk * 8,
                 "d2h_bytes_per_step": npk * 8,
                 "timing": "host wall clock of the whole C call (packed host arrays in and out, copies inside), "
                           "median of the timed calls"},
-        "gpu_launches": int(sum(x.kernel_launches for x in stats)) * args.steps,
+        "gpu_launches": int(launches),
         "roofline": {"bound": "fp64", "kernel": "k_eig_fused / k_eig_cluster (FP64 generalized eigensolver, DMMA "
                                                 "tile products)",
-                     "achieved": feig / (ms / 1e3) / 1e12, "peak": 37.0, "unit": "TFLOP/s",
-                     "frac": feig / (ms / 1e3) / 1e12 / 37.0, "traffic": None,
-                     "peak_kind": "nominal B200 FP64 (no measured FP64 figure on this pool)",
+                     "achieved": feig / (ms / 1e3) / 1e12, "peak": 37.0 * world, "unit": "TFLOP/s",
+                     "frac": feig / (ms / 1e3) / 1e12 / (37.0 * world), "traffic": None,
+                     "peak_kind": "nominal B200 FP64 (no measured FP64 figure on this pool)"
+                                  + ("" if world == 1 else f", times {world} GPUs"),
                      "work": "7 m^3 per system (dsygvd with vectors), the whole call's wall time"},
         "cpu_baseline": cpu,
         "clocks": clocks,
