@@ -2763,11 +2763,6 @@ void eig_setup_attrs() {
     (void)done;
 }
 
-// CTAs per cluster of the large-submatrix solver: 16 when clusters of 16 keep
-// at least 80 % of the SMs busy (one 512-thread CTA each), else 8, else the
-// size among 4 and 2 that keeps the most SMs busy; a submatrix's stages
-// shorten with the cluster, and the longest submatrix sets the step.
-// PTBGPU_EIG_CLUSTER overrides it.
 // Clusters of G CTAs of the cluster solver that fit on the device at once.
 int eig_active_clusters(int G) {
     cudaLaunchConfig_t cfg = {};
@@ -2789,9 +2784,12 @@ int eig_active_clusters(int G) {
     return ncl;
 }
 
-// Cluster size for one problem or a few waves of them: the largest size that
-// keeps 80 % of the SMs busy (16 only then, else 8, 4, 2 by the CTAs they keep
-// busy); PTBGPU_EIG_CLUSTER = 1, 2, 4, 8 or 16 overrides it.
+// CTAs per cluster of the large-submatrix solver for one problem or a few
+// waves of them: 16 when clusters of 16 keep at least 80 % of the SMs busy (one
+// 512-thread CTA each), else 8 on the same rule, else the size among 4 and 2
+// that keeps the most SMs busy; a submatrix's stages shorten with the cluster,
+// and the longest submatrix sets the step.  PTBGPU_EIG_CLUSTER = 1, 2, 4, 8 or
+// 16 overrides it.
 int eig_cluster_size(ptbgpu_ctx* c) {
     static int cached[64] = {};
     const int dev = c->device & 63;
