@@ -33,6 +33,26 @@ def test_assignment_covers_and_balances():
         assert parts == assign_submatrices(dims, nr)
 
 
+def test_lattice_batch_split_over_ranks():
+    """The 256-system lattice batch on N ranks (bench.py --workload lattice256
+    --gpus N): every system on exactly one rank, loads within one largest
+    system's ndim^3 of each other, and the split the same on every rank."""
+    ndims = []
+    for i in range(256):   # the sizes of synth.lattice_instance without building H and S
+        rng = np.random.default_rng(11 * 1000003 + i)
+        nat = int(rng.integers(20, 401))
+        sym, _ = synth.lattice_geometry(nat, 11 * 7777 + i)
+        ndims.append(sum(synth.AO_PER_ELEMENT[s] for s in sym))
+    assert min(ndims) == 166 and max(ndims) == 3064
+    for nr in (2, 4, 8):
+        parts = assign_submatrices(ndims, nr)
+        assert sorted(k for p in parts for k in p) == list(range(256))
+        loads = [sum(float(ndims[k]) ** 3 for k in p) for p in parts]
+        assert max(loads) - min(loads) <= float(max(ndims)) ** 3
+        assert max(loads) <= 1.05 * sum(loads) / nr
+        assert parts == assign_submatrices(list(ndims), nr)
+
+
 @pytest.mark.parametrize("columns", [1, 2])
 def test_single_process_matches_oracle(columns):
     s = _system()
