@@ -162,11 +162,11 @@ def test_cluster_non_positive_definite_overlap_is_reported(ctx):
     assert ei.value.code == api.ENOTSPD and "submatrix 2" in str(ei.value)
 
 
-def test_dense_solve2_on_the_whole_gpu(ctx):
+def test_dense_solve2_on_one_cluster(ctx):
     """solve2's generalized eigensolve (source/pgtb.f90:1066-1170) runs the same
-    solver on the whole GPU (one cooperative launch, a grid barrier between
-    dependent steps): P, the eigenvalues and the Fermi occupations of an 80-H2O
-    cluster (ndim 1840) against the oracle's dsygvd."""
+    solver on one thread-block cluster up to order 4096: P, the eigenvalues and
+    the Fermi occupations of an 80-H2O cluster (ndim 1840) against the oracle's
+    dsygvd."""
     from oracle import ptb_oracle as O
     from ptb_b200 import Options, synth
 
@@ -178,3 +178,21 @@ def test_dense_solve2_on_the_whole_gpu(ctx):
     assert np.max(np.abs(e - e_ref)) < 1e-10
     assert np.max(np.abs(focc - f_ref)) < 1e-10
     assert np.max(np.abs(P - ref)) < 1e-10
+
+
+def test_dense_solve2_on_the_whole_gpu(ctx):
+    """Above order 4096 the same solver runs as one cooperative launch over a
+    grid of CTAs (a bounded software barrier between dependent steps): solve2 of
+    a 180-H2O cluster (ndim 4140) against the oracle's dsygvd."""
+    from oracle import ptb_oracle as O
+    from ptb_b200 import Options, synth
+
+    s = synth.water_cluster(180, seed=4)
+    n = s.ndim
+    assert n > 4096
+    P, e, focc, st = ctx.solve2(1, n, s.nel, 0, s.Hvec, s.Svec, Options(filter=1e-4))
+    ref, e_ref, f_ref, _ = O.solve2(1, n, s.nel, 0, 300.0, O.filter_matrix_sym(s.Hvec, 1e-4),
+                                    O.filter_matrix_sym(s.Svec, 1e-4))
+    assert np.max(np.abs(e - e_ref)) < 1e-10
+    assert np.max(np.abs(focc - f_ref)) < 1e-10
+    assert np.max(np.abs(P - ref)) < 1e-9
