@@ -196,3 +196,23 @@ def test_dense_solve2_on_the_whole_gpu(ctx):
     assert np.max(np.abs(e - e_ref)) < 1e-10
     assert np.max(np.abs(focc - f_ref)) < 1e-10
     assert np.max(np.abs(P - ref)) < 1e-9
+
+
+@pytest.mark.parametrize("G", [2, 16])
+def test_cluster_solver_at_other_cluster_sizes(G):
+    """The cluster solver is written for any number of CTAs per cluster: the
+    batch rule picks 2 for many large problems, and 16 is the largest size.  The
+    size is read once per process, so the cluster tests rerun in a child pytest
+    with PTBGPU_EIG_CLUSTER set."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    here = Path(__file__).resolve()
+    env = dict(os.environ, PTBGPU_EIG_CLUSTER=str(G))
+    r = subprocess.run([sys.executable, "-m", "pytest", str(here), "-m", "gpu", "-q", "-p", "no:cacheprovider",
+                        "-k", "cluster_ and not other_cluster_sizes"],
+                       cwd=here.parent.parent, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
+    assert " passed" in r.stdout and "4 passed" in r.stdout, r.stdout[-1000:]
