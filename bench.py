@@ -347,11 +347,17 @@ def run_sm(args, rank, world, local, pg):
     part = None
     if cols == 4:   # the library's seeded k-means (also what the call itself runs without a partition)
         part, _, _ = ctx.kmeans_partition(s.ndim, s.Hvec, s.Svec, s.nat, s.xyz, s.aoat, seed=42, opts=o)
+    pinned = False
     if world == 1:
-        # end to end from pinned host buffers (H, S in, P out), as the dense line
-        hH = torch.from_numpy(s.Hvec).pin_memory().numpy()
-        hS = torch.from_numpy(s.Svec).pin_memory().numpy()
-        hP = torch.empty(s.ndim * (s.ndim + 1) // 2, dtype=torch.float64).pin_memory().numpy()
+        # end to end from pinned host buffers (H, S in, P out), as the dense line;
+        # pageable arrays where the host cannot pin that much (2048 H2O: 3 x 8.9 GB)
+        try:
+            hH = torch.from_numpy(s.Hvec).pin_memory().numpy()
+            hS = torch.from_numpy(s.Svec).pin_memory().numpy()
+            hP = torch.empty(s.ndim * (s.ndim + 1) // 2, dtype=torch.float64).pin_memory().numpy()
+            pinned = True
+        except RuntimeError:
+            hH, hS, hP = s.Hvec, s.Svec, None
         call = lambda: ctx.sm_stupid_simple(s.ndim, s.nel, hH, hS, s.nat, s.xyz, s.aoat, cols, 2, None, o, out=hP)
     else:
         # one system over the ranks: a size-balanced share of the submatrices per GPU,
@@ -422,7 +428,8 @@ def run_sm(args, rank, world, local, pg):
                         "mu_iterations": int(last.mu_iterations)},
         "e2e": {"value": wall, "unit": UNIT, "h2d_bytes_per_step": 2 * npk * 8, "d2h_bytes_per_step": npk * 8,
                 "timing": "host wall clock of the whole call, median of the timed calls; "
-                          + ("pinned host H, S and P" if world == 1 else "pageable host arrays, max over ranks")},
+                          + ("pinned host H, S and P" if pinned else "pageable host arrays")
+                          + ("" if world == 1 else ", max over ranks")},
         "gpu_launches": int(sum(x.kernel_launches for x in stats)),
         "roofline": {"bound": "fp64", "kernel": "the library's FP64 generalized eigensolver (Cholesky, reduction, "
                      "tridiagonalisation, divide and conquer, owned rows; DMMA tile products): k_eig_fused, one "
