@@ -199,7 +199,8 @@ int ptbgpu_tc_purify_batch(ptbgpu_ctx* ctx, int64_t ninst, const int64_t* ndim, 
  * FP64 eigensolver: per system the filtered generalized eigenproblem
  * H_k U = S_k U e and P_k = 2 sum_{i < nel_k/2} u_i u_i^T (the dense projector
  * at T = 0, i.e. the reference's solve2, source/pgtb.f90:1066-1170, without the
- * Fermi smearing), P_k formed in the same launch.  Systems up to order 1024 run
+ * Fermi smearing), P_k formed in the same launch; nel_k must be even (closed
+ * shell: an odd count is EINVAL).  Systems up to order 1024 run
  * one CTA each in a persistent launch (largest first), larger ones (up to 12032)
  * one thread-block cluster each, beside them.  opts->filter is applied to H and
  * S (filter_matrix_sym).  Per-system stats carry flops; wall_ms the host time of

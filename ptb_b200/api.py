@@ -450,6 +450,10 @@ class Context:
         ([Pvec], [Stats], wall milliseconds)."""
         n = len(systems)
         m = max(n, 1)
+        for i, s in enumerate(systems):
+            if int(s[1]) % 2:
+                raise PtbGpuError(EINVAL, f"system {i}: odd electron count {int(s[1])} (the T = 0 projector "
+                                          "here is closed-shell)")
         ndim = (C.c_int64 * m)(*[int(s[0]) for s in systems])
         nel = (C.c_int64 * m)(*[int(s[1]) for s in systems])
         Hs = [_packed(s[2], s[0], f"H of system {i}") for i, s in enumerate(systems)]

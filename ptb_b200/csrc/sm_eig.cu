@@ -3210,6 +3210,9 @@ void eig_density_batch(ptbgpu_ctx* c, int64_t ninst, const int64_t* ndim, const 
                   (long long)k, (long long)m, kLargeMax);
         PTB_CHECK(nel[k] >= 0 && nel[k] / 2 <= m && Hpk[k] && Spk[k] && Ppk[k], PTBGPU_EINVAL,
                   "system %lld: bad electron count or arrays", (long long)k);
+        PTB_CHECK(nel[k] % 2 == 0, PTBGPU_EINVAL,
+                  "system %lld: odd electron count %lld (the T = 0 projector here is closed-shell)", (long long)k,
+                  (long long)nel[k]);
         EigProbHost& q = pr[k];
         q.k = (int)k;
         q.m = (int)m;

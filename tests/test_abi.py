@@ -139,6 +139,7 @@ def test_wrong_array_lengths_are_rejected_before_the_c_call():
         lambda: ctx.tc_purify_batch([(n, 8, pk, pk), (n, 8, pk, short)]),
         lambda: ctx.tc_purify_grouped([(n, 8, short, pk)]),
         lambda: ctx.eig_density_batch([(n, 8, pk, pk), (n, 8, short, pk)]),
+        lambda: ctx.eig_density_batch([(n, 8, pk, pk), (n, 7, pk, pk)]),
         lambda: ctx.solve2(1, n, 8, 0, pk, short),
         lambda: ctx.mlpop14(n, short),
         lambda: ctx.mlpop2(nat, n, short, np.eye(n), np.eye(n), aoat, aoat),
